@@ -1,0 +1,176 @@
+/* sipg_b200.h -- C ABI of the B200-native SIPG pressure/viscous solve path.
+ *
+ * Drop-in boundary for INS-Solver's pressure/viscous linear-solve hot path.
+ * Plain pointers and sizes only; every entry point returns an int status
+ * (SIPG_OK = 0) and never aborts the process; sipg_last_error() describes the
+ * last failure on the calling thread. The reference reports solver failure as
+ * `bool solve(...)` and aborts on setup errors (dg_abort); the C++ shim classes
+ * in include/ins_solver_b200/ map these statuses back to the reference's forms.
+ *
+ * Each declaration names the reference interface it replaces (paths inside
+ * the TobyFlynn/INS-Solver tree). Vectors are FP64, element-major [K][Np]
+ * (the layout of an op_dat with dim Np), components stacked one after another.
+ */
+#ifndef SIPG_B200_H
+#define SIPG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (the reference: bool converged + dg_abort) */
+#define SIPG_OK 0
+#define SIPG_NOT_CONVERGED 1  /* solve(): residual above tolerance after max_iter */
+#define SIPG_BREAKDOWN 2      /* solve(): NaN/Inf or p.Ap <= 0 */
+#define SIPG_INVALID_ARG 3
+#define SIPG_OUT_OF_MEMORY 4  /* also: request rejected by the HBM admission budget */
+#define SIPG_CANCELLED 5      /* served request cancelled or timed out */
+#define SIPG_CUDA_ERROR 6
+#define SIPG_NO_DEVICE 7
+
+typedef struct sipg_mesh sipg_mesh;
+typedef struct sipg_op sipg_op;
+typedef struct sipg_solver sipg_solver;
+typedef struct sipg_server sipg_server;
+
+const char *sipg_last_error(void);
+int sipg_version(void);
+
+/* ---- device memory helpers (plain CUDA runtime calls, for callers without a
+ * CUDA toolkit of their own; the reference owns data through OP2 op_dats) */
+int sipg_device_count(int *n);
+int sipg_dev_alloc(size_t bytes, void **ptr);
+int sipg_dev_free(void *ptr);
+int sipg_memcpy_h2d(void *dst, const void *src, size_t bytes);
+int sipg_memcpy_d2h(void *dst, const void *src, size_t bytes);
+int sipg_device_synchronize(void);
+
+/* ---- reference element tables (replace DGConstants / dg_*_kernel / FMASK of
+ * the unvendored OP2-DG-Toolkit, used e.g. at src/kernels/fvmf_3d_op1_diag.h:2-5).
+ * Matrices are row-major. Any output pointer may be NULL. */
+int sipg_ref_sizes(int dim, int order, int *Np, int *Nfp, int *Nfaces, int *Nperm);
+int sipg_ref_tables(int dim, int order, double *r, double *s, double *t, double *Dr, double *Ds,
+                    double *Dt, double *M, double *MMF, double *EMAT, int *fmask, int *perm_pos);
+/* Prolongation from order q to order p (Np(p) x Np(q)), the p-multigrid transfer. */
+int sipg_interp_matrix(int dim, int q, int p, double *P);
+
+/* ---- synthetic meshes: unit square n x n x 2 triangles, unit cube n^3 x 6
+ * tetrahedra (Kuhn split); interior vertices jittered by +-jitter*h from seed. */
+int sipg_box_mesh_sizes(int dim, int n, int *Nv, int *K);
+int sipg_box_mesh(int dim, int n, double jitter, uint64_t seed, double *vx, int *e2v);
+
+/* ---- mesh: replaces DGMesh3D/DGMesh2D construction and init
+ * (src/ins3d.cpp:154, :203; geof/face data consumed by
+ * src/solvers/3d/slip_matrix/factor_viscous_matrix.cpp:47-92). Builds the
+ * connectivity and geometry on the host and keeps it resident on the GPU. */
+int sipg_mesh_create(int dim, int Nv, const double *vx, int K, const int *e2v, sipg_mesh **out);
+int sipg_mesh_sizes(const sipg_mesh *m, int *K, int *F, int *Kb);
+/* Host copies of the per-order mesh data in the reference's form (any NULL
+ * pointer is skipped): geof K x (10|5); nx, ny, nz, sJ, fscale K x Nf;
+ * face2cells, faceNum F x 2; fmaskL, fmaskR F x Nfp; bface2cell, bfaceNum Kb;
+ * bface_centroid Kb x dim; x, y, z K x Np node coordinates. */
+int sipg_mesh_export(const sipg_mesh *m, int order, double *geof, double *nx, double *ny,
+                     double *nz, double *sJ, double *fscale, int *face2cells, int *faceNum,
+                     int *fmaskL, int *fmaskR, int *bface2cell, int *bfaceNum,
+                     double *bface_centroid, double *x, double *y, double *z);
+int sipg_mesh_device_bytes(const sipg_mesh *m, size_t *bytes);
+void sipg_mesh_destroy(sipg_mesh *m);
+
+/* ---- operator: replaces PoissonMatrixFreeDiag3D / FactorPoissonMatrixFreeDiag3D /
+ * MMPoissonMatrixFree3D / FactorMMPoissonMatrixFreeDiag3D (unvendored; created at
+ * src/solvers/3d/mp_ins_solver.cpp:87, src/solvers/3d/ins_solver.cpp:91,139) and the
+ * vendored FactorViscousMatrix3D / ViscousMatrix3D (ncomp = dim, slip coupling). */
+#define SIPG_MM_NONE 0
+#define SIPG_MM_SCALAR 1
+#define SIPG_MM_NODAL 2
+#define SIPG_BC_DIRICHLET 0
+#define SIPG_BC_NEUMANN 1
+#define SIPG_BC_SLIP 2
+#define SIPG_FP64 64
+#define SIPG_FP32 32
+
+int sipg_op_create(sipg_mesh *m, int order, int ncomp, sipg_op **out);
+/* set_factor(op_dat) (factor_viscous_matrix.cpp:70-72); NULL = constant 1. Host FP64 K x Np. */
+int sipg_op_set_factor(sipg_op *op, const double *factor);
+/* set_mm_factor(op_dat) (:74-76) or MMPoissonMatrixFree3D::set_factor(DG_FP). */
+int sipg_op_set_mm(sipg_op *op, int mode, double scalar, const double *mm);
+/* set_bc_types (:41-45): ncomp x Kb ints, 0 Dirichlet, 1 Neumann, 2 slip. */
+int sipg_op_set_bc_types(sipg_op *op, const int *types);
+/* Pin one DOF (element, node): its row and column become diag * identity. -1 clears. */
+int sipg_op_set_pin(sipg_op *op, int elem, int node);
+/* mult(in, out) (factor_viscous_matrix.cpp:96-310). x, y: device pointers,
+ * ncomp x K x Np of double (SIPG_FP64) or float (SIPG_FP32). stream: cudaStream_t or NULL. */
+int sipg_op_apply(sipg_op *op, int precision, const void *x, void *y, void *stream);
+/* Same with host FP64 buffers (copies in and out inside the call). */
+int sipg_op_apply_host(sipg_op *op, const double *x, double *y);
+/* apply_bc (factor_viscous_matrix.cpp:47-68): rhs += lifted bc data; host buffers,
+ * bc: ncomp x Kb x Nfp, rhs: ncomp x K x Np (updated in place). */
+int sipg_op_apply_bc_host(sipg_op *op, const double *bc, double *rhs);
+/* calc_diag (:312-366) -> host diag ncomp x K x Np. */
+int sipg_op_diag_host(sipg_op *op, double *diag);
+/* calc_inv_block_diag (:368-451) -> host blocks ncomp x K x Np x Np (row-major);
+ * invert != 0 returns the inverses. ref_volume_block != 0 reproduces the
+ * reference's volume block formula (fvmf_3d_op1.h:17-18). */
+int sipg_op_block_diag_host(sipg_op *op, int invert, int ref_volume_block, double *blocks);
+int sipg_op_sizes(const sipg_op *op, int *K, int *Np, int *Nfp, int *ncomp);
+void sipg_op_destroy(sipg_op *op);
+
+/* ---- solver: replaces LinearSolver and its subclasses (src/solvers/3d/
+ * ins_solver_base.cpp:149-184, :1522-1536; solve at mp_ins_solver.cpp:632) and
+ * ViscousSolver3D (src/solvers/3d/slip_matrix/viscous_solver.cpp:63-453). */
+#define SIPG_SOLVER_CG 0             /* ViscousSolver3D, Preconditioners::NONE */
+#define SIPG_SOLVER_INV_MASS 1       /* PETScInvMassSolver / INV_MASS, FACTOR_INV_MASS */
+#define SIPG_SOLVER_JACOBI 2         /* PETScJacobiSolver / JACOBI */
+#define SIPG_SOLVER_BLOCK_JACOBI 3   /* PETScBlockJacobiSolver / BLOCK_JACOBI */
+#define SIPG_SOLVER_PMULTIGRID 4     /* PETScPMultigrid */
+
+typedef struct {
+  int iters;
+  double rel_res;     /* ||b - A x|| / ||b|| (recursive residual) */
+  double abs_res;
+  double true_rel_res;/* recomputed with an explicit FP64 apply at the end */
+  double setup_ms;
+  double solve_ms;
+  int status;
+} sipg_solve_info;
+
+typedef struct {
+  double rel_tol, abs_tol;   /* set_tol_and_iter (ins_solver_base.cpp:153-183) */
+  int max_iter;
+  int nullspace;             /* set_nullspace: project out constants */
+  int precision;             /* preconditioner precision: SIPG_FP64 or SIPG_FP32 (mixed) */
+  double inv_mass_factor;    /* PETScInvMassSolver::setFactor */
+  int ref_volume_block;      /* block Jacobi: reference's volume block formula */
+  /* [p-multigrid] keys (examples/3d/oscillating_droplet/config.ini:24-31) */
+  int n_levels;
+  int orders[4];             /* e.g. 3,2,1 */
+  int cheb_order;            /* Chebyshev degree per smoothing sweep */
+  double eig_safety;         /* eigen_val_saftey_factor */
+  double eig_ratio;          /* lambda_min = lambda_max * safety / eig_ratio */
+  int eig_iters;
+  int coarse_iters;          /* Jacobi-PCG iterations on the coarsest order */
+  int check_every;           /* host convergence check period (iterations) */
+} sipg_solver_opts;
+
+int sipg_solver_default_opts(int kind, sipg_solver_opts *o);
+int sipg_solver_create(sipg_op *op, int kind, const sipg_solver_opts *o, sipg_solver **out);
+/* Re-run the setup that depends on the operator's coefficients (diagonals,
+ * blocks, eigenvalue bounds, coarse operators); call after set_factor. */
+int sipg_solver_setup(sipg_solver *s);
+/* solve(rhs, ans): device FP64 pointers (ncomp x K x Np); x holds the initial guess. */
+int sipg_solver_solve(sipg_solver *s, const double *b, double *x, sipg_solve_info *info);
+/* Same with host buffers, copies inside the call (end-to-end path). */
+int sipg_solver_solve_host(sipg_solver *s, const double *b, double *x, sipg_solve_info *info);
+void sipg_solver_destroy(sipg_solver *s);
+
+/* Number of kernels this library has launched so far in the process
+ * (diagnostics for benchmarks; no reference counterpart). */
+int sipg_launch_count(unsigned long long *n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,97 @@
+// Internal runtime objects behind the C ABI (include/sipg_b200.h).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "mesh.hpp"
+#include "refelem.hpp"
+#include "sipg_apply.cuh"
+#include "sipg_blocks.cuh"
+
+namespace sipg {
+
+// Error carried up to the C ABI as (status, message).
+struct Error : std::runtime_error {
+  int status;
+  Error(int st, const std::string& msg) : std::runtime_error(msg), status(st) {}
+};
+
+void cuda_check(cudaError_t e, const char* what);
+#define SIPG_CUDA(call) ::sipg::cuda_check((call), #call)
+
+// Device allocation owned by a runtime object.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  explicit DevBuf(size_t n);
+  ~DevBuf();
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr; o.bytes = 0; }
+  DevBuf& operator=(DevBuf&& o) noexcept;
+  template <typename T> T* as() const { return static_cast<T*>(p); }
+  void upload(const void* src, size_t n, cudaStream_t s = 0);
+};
+
+// Order-specific reference tables on the device (FP64 and FP32 copies).
+struct DevRef {
+  RefElement ref;
+  DevBuf c64, c32, itab, mf;
+  int Np = 0, Nfp = 0;
+};
+const DevRef& dev_ref(int dim, int order);  // cached per device
+
+int num_sms();
+
+}  // namespace sipg
+
+struct sipg_mesh {
+  int dim = 0, K = 0, Kb = 0, F = 0, Nv = 0;
+  std::vector<double> vx;
+  std::vector<int> e2v;
+  std::map<int, sipg::Mesh> host;  // per-order host tables (lazily built)
+  std::mutex host_mu;
+  sipg::DevBuf geof64, geof32, nbr, fcode, belems;
+  int n_belem = 0;
+  bool device_ready = false;
+  std::mutex dev_mu;
+  const sipg::Mesh& host_order(int order);
+  void ensure_device();  // upload geometry/connectivity on first device use
+};
+
+struct sipg_op {
+  sipg_mesh* mesh = nullptr;
+  int order = 0, ncomp = 1, Np = 0, Nfp = 0;
+  const sipg::DevRef* dref = nullptr;
+  bool has_factor = false;
+  sipg::DevBuf factor64, factor32, tau64, tau32;
+  int mm_mode = 0;
+  double mm_scalar = 0.0;
+  sipg::DevBuf mm64, mm32;
+  sipg::DevBuf bct;           // ncomp x Kb uint8
+  std::vector<int> bct_host;  // ncomp x Kb
+  int pin_elem = -1, pin_node = -1;
+  double pin_scale = 1.0;
+  int eb64 = 0, eb32 = 0;
+  // Apply on device buffers in precision T.
+  template <typename T>
+  void apply(const T* x, T* y, cudaStream_t s, T alpha = T(1), T beta = T(0)) const;
+  void refresh_tau(cudaStream_t s);
+  sipg::BlockArgs block_args(int mode, int ref_volume, double* out, bool with_pin) const;
+  void apply_bc_device(const double* bc, double* rhs, cudaStream_t s) const;
+  void refresh_pin(cudaStream_t s);
+};
+
+namespace sipg {
+std::unique_ptr<sipg_op> create_op(sipg_mesh* m, int order, int ncomp);
+void set_factor_device(sipg_op* op, const double* f64, cudaStream_t s);
+void set_mm_device(sipg_op* op, int mode, double scalar, const double* mm64, cudaStream_t s);
+void set_bc_types_host(sipg_op* op, const std::vector<int>& types);
+}  // namespace sipg

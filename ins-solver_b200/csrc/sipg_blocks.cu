@@ -1,0 +1,325 @@
+// Element diagonal blocks, diagonals, block inverses and boundary lifting.
+//
+// Replaces FactorViscousMatrix3D::calc_diag / calc_inv_block_diag
+// (src/solvers/3d/slip_matrix/factor_viscous_matrix.cpp:312-451: fvmf_3d_op1(_diag),
+// fvmf_3d_op2_(block_)diag, fvmf_3d_mm_(block_)diag, fvmf_3d_bop_(block_)diag and
+// the host Armadillo inverse at :423-450) and apply_bc (:47-68, fvmf_3d_apply_bc.h).
+// One CTA builds one element's Np x Np block in shared memory, FP64 throughout;
+// the inverse is Gauss-Jordan with partial pivoting in shared memory, so the
+// reference's host round trip disappears.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "sipg_blocks.cuh"
+#include "vecops.cuh"
+
+namespace sipg {
+namespace {
+
+template <int DIM>
+__device__ void face_normal_d(const double* g, int f, double n[3], double* sJ) {
+  if (DIM == 3) {
+    for (int d = 0; d < 3; ++d) {
+      double v;
+      if (f == 0) v = -g[6 + d];
+      else if (f == 1) v = -g[3 + d];
+      else if (f == 2) v = (g[d] + g[3 + d]) + g[6 + d];
+      else v = -g[d];
+      n[d] = v;
+    }
+    double len = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+    n[0] /= len; n[1] /= len; n[2] /= len;
+    *sJ = len * g[9];
+  } else {
+    for (int d = 0; d < 2; ++d) {
+      double v;
+      if (f == 0) v = -g[2 + d];
+      else if (f == 1) v = g[d] + g[2 + d];
+      else v = -g[d];
+      n[d] = v;
+    }
+    n[2] = 0.0;
+    double len = sqrt(n[0] * n[0] + n[1] * n[1]);
+    n[0] /= len; n[1] /= len;
+    *sJ = len * g[4];
+  }
+}
+
+// consts64 layout of the apply (Cfg): Dr, Ds, [Dt], M with row stride LD.
+template <int DIM, int P>
+__global__ void __launch_bounds__(128) block_kernel(BlockArgs a) {
+  using C = Cfg<DIM, P>;
+  constexpr int NP = C::NP, NFP = C::NFP, NF = C::NF, LD = C::LD, NG = C::NG, NPP = NP * NP;
+  __shared__ double B[NPP], X[NPP], T[NPP], MF[NF * NFP * NFP];
+  __shared__ double g[NG], fac[NP];
+  __shared__ int fm[NF * NFP];
+  __shared__ int piv_row;
+  __shared__ double fcol[NP];
+  const double* Dm = a.consts + C::OFF_D;
+  const double* Mm = a.consts + C::OFF_M;
+  for (int i = threadIdx.x; i < NF * NFP * NFP; i += blockDim.x) MF[i] = a.mf[i];
+  for (int i = threadIdx.x; i < NF * NFP; i += blockDim.x) fm[i] = a.itab[i];
+  const int total = a.K * a.ncomp;
+  for (int item = blockIdx.x; item < total; item += gridDim.x) {
+    const int e = item % a.K, c = item / a.K;
+    __syncthreads();
+    for (int i = threadIdx.x; i < NG; i += blockDim.x) g[i] = a.geof[(size_t)e * NG + i];
+    for (int i = threadIdx.x; i < NP; i += blockDim.x) fac[i] = a.factor ? a.factor[(size_t)e * NP + i] : 1.0;
+    for (int i = threadIdx.x; i < NPP; i += blockDim.x) B[i] = 0.0;
+    __syncthreads();
+    const double J = g[DIM == 3 ? 9 : 4];
+    // volume: sum_d J Dx_d^T M F Dx_d (fvmf_3d_op1.h / fvmf_3d_op1_diag.h)
+    for (int d = 0; d < DIM; ++d) {
+      for (int i = threadIdx.x; i < NPP; i += blockDim.x) {
+        int r = i / NP, cc = i % NP;
+        double s = 0.0;
+        for (int rr = 0; rr < DIM; ++rr) s += g[rr * DIM + d] * Dm[rr * NP * LD + r * LD + cc];
+        X[i] = s;
+      }
+      __syncthreads();
+      for (int i = threadIdx.x; i < NPP; i += blockDim.x) {
+        int r = i / NP, cc = i % NP;
+        double s = 0.0;
+        if (a.ref_volume && DIM == 2) {
+          for (int k = 0; k < NP; ++k) s += Mm[r * LD + k] * X[k * NP + cc];
+          s *= fac[r];
+        } else {
+          for (int k = 0; k < NP; ++k) s += Mm[r * LD + k] * fac[k] * X[k * NP + cc];
+        }
+        T[i] = J * s;
+      }
+      __syncthreads();
+      for (int i = threadIdx.x; i < NPP; i += blockDim.x) {
+        int r = i / NP, cc = i % NP;
+        double s = 0.0;
+        if (a.ref_volume && DIM == 3)
+          for (int k = 0; k < NP; ++k) s += X[r * NP + k] * T[k * NP + cc];
+        else
+          for (int k = 0; k < NP; ++k) s += X[k * NP + r] * T[k * NP + cc];
+        B[i] += s;
+      }
+      __syncthreads();
+    }
+    // faces (fvmf_3d_op2_block_diag.h, fvmf_3d_bop_block_diag.h)
+    for (int f = 0; f < NF; ++f) {
+      const int nb = a.nbr[(size_t)e * NF + f];
+      double n[3], sJ;
+      face_normal_d<DIM>(g, f, n, &sJ);
+      double scale;
+      if (nb >= 0) {
+        scale = 0.5 * sJ;
+      } else {
+        const int b = -nb - 1;
+        bool all_slip = a.ncomp == DIM;
+        for (int k = 0; k < a.ncomp; ++k) all_slip = all_slip && a.bct[(size_t)k * a.Kb + b] == 2;
+        if (all_slip) scale = sJ * n[c] * n[c];
+        else if (a.bct[(size_t)c * a.Kb + b] == 0) scale = sJ;
+        else continue;  // Neumann
+      }
+      const double gtau = a.tau[(size_t)e * NF + f];
+      // X = D_n: X[i][j] = f_i sum_r (n . grad r) D_r[i][j]
+      double rf[3] = {0.0, 0.0, 0.0};
+      for (int rr = 0; rr < DIM; ++rr)
+        for (int d = 0; d < DIM; ++d) rf[rr] += n[d] * g[rr * DIM + d];
+      __syncthreads();
+      for (int i = threadIdx.x; i < NPP; i += blockDim.x) {
+        int r = i / NP, cc = i % NP;
+        double s = 0.0;
+        for (int rr = 0; rr < DIM; ++rr) s += rf[rr] * Dm[rr * NP * LD + r * LD + cc];
+        X[i] = s * fac[r];
+      }
+      __syncthreads();
+      const double* mf = MF + f * NFP * NFP;
+      const int* fmf = fm + f * NFP;
+      // rows on the face: -scale * (MF D_n)[a][j]; and the penalty on face-face entries
+      for (int i = threadIdx.x; i < NFP * NP; i += blockDim.x) {
+        int aa = i / NP, j = i % NP;
+        double s = 0.0;
+        for (int bb = 0; bb < NFP; ++bb) s += mf[aa * NFP + bb] * X[fmf[bb] * NP + j];
+        B[fmf[aa] * NP + j] -= scale * s;
+      }
+      __syncthreads();
+      // columns on the face: -scale * (D_n^T MF)[i][b]
+      for (int i = threadIdx.x; i < NP * NFP; i += blockDim.x) {
+        int r = i / NFP, bb = i % NFP;
+        double s = 0.0;
+        for (int aa = 0; aa < NFP; ++aa) s += X[fmf[aa] * NP + r] * mf[aa * NFP + bb];
+        B[r * NP + fmf[bb]] -= scale * s;
+      }
+      __syncthreads();
+      for (int i = threadIdx.x; i < NFP * NFP; i += blockDim.x) {
+        int aa = i / NFP, bb = i % NFP;
+        B[fmf[aa] * NP + fmf[bb]] += scale * gtau * mf[i];
+      }
+      __syncthreads();
+    }
+    // mass term (fvmf_3d_mm_block_diag.h: the reference scales rows; the operator scales columns)
+    if (a.mm_mode != 0) {
+      for (int i = threadIdx.x; i < NPP; i += blockDim.x) {
+        int r = i / NP, cc = i % NP;
+        int k = a.ref_volume ? r : cc;
+        double mmv = a.mm_mode == 1 ? a.mm_scalar : a.mm[(size_t)e * NP + k];
+        B[i] += J * Mm[r * LD + cc] * mmv;
+      }
+      __syncthreads();
+    }
+    if (e == a.pin_elem) {
+      const int pn = a.pin_node;
+      for (int i = threadIdx.x; i < NP; i += blockDim.x) {
+        if (i != pn) { B[pn * NP + i] = 0.0; B[i * NP + pn] = 0.0; }
+      }
+      if (threadIdx.x == 0) B[pn * NP + pn] = a.pin_scale;
+      __syncthreads();
+    }
+    double* out_base = a.out + (size_t)item * (a.mode == BLOCK_DIAG_ONLY ? NP : NPP);
+    if (a.mode == BLOCK_DIAG_ONLY) {
+      for (int i = threadIdx.x; i < NP; i += blockDim.x) out_base[i] = B[i * NP + i];
+      continue;
+    }
+    if (a.mode == BLOCK_INVERSE) {
+      // Gauss-Jordan with partial pivoting: B -> I, X -> B^-1
+      for (int i = threadIdx.x; i < NPP; i += blockDim.x) X[i] = (i / NP == i % NP) ? 1.0 : 0.0;
+      __syncthreads();
+      for (int col = 0; col < NP; ++col) {
+        if (threadIdx.x == 0) {
+          int p = col;
+          double best = fabs(B[col * NP + col]);
+          for (int r = col + 1; r < NP; ++r) {
+            double v = fabs(B[r * NP + col]);
+            if (v > best) { best = v; p = r; }
+          }
+          piv_row = p;
+        }
+        __syncthreads();
+        const int p = piv_row;
+        if (p != col)
+          for (int j = threadIdx.x; j < NP; j += blockDim.x) {
+            double t0 = B[col * NP + j]; B[col * NP + j] = B[p * NP + j]; B[p * NP + j] = t0;
+            double t1 = X[col * NP + j]; X[col * NP + j] = X[p * NP + j]; X[p * NP + j] = t1;
+          }
+        __syncthreads();
+        const double dinv = 1.0 / B[col * NP + col];
+        __syncthreads();
+        for (int j = threadIdx.x; j < NP; j += blockDim.x) {
+          B[col * NP + j] *= dinv;
+          X[col * NP + j] *= dinv;
+        }
+        __syncthreads();
+        for (int r = threadIdx.x; r < NP; r += blockDim.x) fcol[r] = B[r * NP + col];
+        __syncthreads();
+        for (int i = threadIdx.x; i < NPP; i += blockDim.x) {
+          int r = i / NP, j = i % NP;
+          if (r == col) continue;
+          B[i] -= fcol[r] * B[col * NP + j];
+          X[i] -= fcol[r] * X[col * NP + j];
+        }
+        __syncthreads();
+      }
+      for (int i = threadIdx.x; i < NPP; i += blockDim.x) out_base[i] = X[i];
+    } else {
+      for (int i = threadIdx.x; i < NPP; i += blockDim.x) out_base[i] = B[i];
+    }
+  }
+}
+
+// Boundary lifting of Dirichlet / Neumann data into the right-hand side
+// (fvmf_3d_apply_bc.h:29-85), one CTA per element that owns boundary faces;
+// an element's faces are applied in order, so the sums are deterministic.
+template <int DIM, int P>
+__global__ void __launch_bounds__(128) apply_bc_kernel(ApplyBcArgs a) {
+  using C = Cfg<DIM, P>;
+  constexpr int NP = C::NP, NFP = C::NFP, NF = C::NF, LD = C::LD, NG = C::NG, NPP = NP * NP;
+  __shared__ double X[NPP], tmp[NP], g[NG], fac[NP], acc[NP];
+  const double* Dm = a.consts + C::OFF_D;
+  for (int item = blockIdx.x; item < a.n_belem * a.ncomp; item += gridDim.x) {
+    const int e = a.belems[item % a.n_belem], c = item / a.n_belem;
+    __syncthreads();
+    for (int i = threadIdx.x; i < NG; i += blockDim.x) g[i] = a.geof[(size_t)e * NG + i];
+    for (int i = threadIdx.x; i < NP; i += blockDim.x) {
+      fac[i] = a.factor ? a.factor[(size_t)e * NP + i] : 1.0;
+      acc[i] = 0.0;
+    }
+    __syncthreads();
+    for (int f = 0; f < NF; ++f) {
+      const int nb = a.nbr[(size_t)e * NF + f];
+      if (nb >= 0) continue;
+      const int b = -nb - 1;
+      const int t = a.bct[(size_t)c * a.Kb + b];
+      if (t != 0 && t != 1) continue;  // slip: nothing
+      double n[3], sJ;
+      face_normal_d<DIM>(g, f, n, &sJ);
+      const double* mf = a.mf + f * NFP * NFP;
+      const int8_t* fmf = a.itab + f * NFP;
+      const double* bc = a.bc + ((size_t)c * a.Kb + b) * NFP;
+      if (t == 1) {
+        for (int i = threadIdx.x; i < NFP; i += blockDim.x) {
+          double s = 0.0;
+          for (int j = 0; j < NFP; ++j) s += mf[i * NFP + j] * bc[j];
+          acc[fmf[i]] += sJ * s;
+        }
+        __syncthreads();
+        continue;
+      }
+      const double gtau = a.tau[(size_t)e * NF + f];
+      double rf[3] = {0.0, 0.0, 0.0};
+      for (int rr = 0; rr < DIM; ++rr)
+        for (int d = 0; d < DIM; ++d) rf[rr] += n[d] * g[rr * DIM + d];
+      for (int i = threadIdx.x; i < NPP; i += blockDim.x) {
+        int r = i / NP, cc = i % NP;
+        double s = 0.0;
+        for (int rr = 0; rr < DIM; ++rr) s += rf[rr] * Dm[rr * NP * LD + r * LD + cc];
+        X[i] = s * fac[r];
+      }
+      for (int i = threadIdx.x; i < NP; i += blockDim.x) tmp[i] = 0.0;
+      __syncthreads();
+      for (int i = threadIdx.x; i < NFP; i += blockDim.x) {
+        double s = 0.0;
+        for (int j = 0; j < NFP; ++j) s += mf[i * NFP + j] * bc[j];
+        tmp[fmf[i]] = sJ * s;
+      }
+      __syncthreads();
+      for (int i = threadIdx.x; i < NP; i += blockDim.x) {
+        double s = gtau * tmp[i];
+        for (int j = 0; j < NP; ++j) s -= X[j * NP + i] * tmp[j];
+        acc[i] += s;
+      }
+      __syncthreads();
+    }
+    for (int i = threadIdx.x; i < NP; i += blockDim.x) a.rhs[((size_t)c * a.K + e) * NP + i] += acc[i];
+  }
+}
+
+}  // namespace
+
+#define SIPG_DISPATCH_B(DIM_, ORDER_, ...)                         \
+  switch ((DIM_) * 10 + (ORDER_)) {                                \
+    case 21: { constexpr int D = 2, P = 1; __VA_ARGS__; }          \
+    case 22: { constexpr int D = 2, P = 2; __VA_ARGS__; }          \
+    case 23: { constexpr int D = 2, P = 3; __VA_ARGS__; }          \
+    case 24: { constexpr int D = 2, P = 4; __VA_ARGS__; }          \
+    case 31: { constexpr int D = 3, P = 1; __VA_ARGS__; }          \
+    case 32: { constexpr int D = 3, P = 2; __VA_ARGS__; }          \
+    case 33: { constexpr int D = 3, P = 3; __VA_ARGS__; }          \
+    case 34: { constexpr int D = 3, P = 4; __VA_ARGS__; }          \
+    default: break;                                                \
+  }
+
+cudaError_t launch_blocks(int dim, int order, const BlockArgs& a, cudaStream_t s) {
+  int total = a.K * a.ncomp;
+  if (total <= 0) return cudaSuccess;
+  int grid = std::min(total, 148 * 16);
+  SIPG_DISPATCH_B(dim, order, block_kernel<D, P><<<grid, 128, 0, s>>>(a); note_launch(); return cudaGetLastError());
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_apply_bc(int dim, int order, const ApplyBcArgs& a, cudaStream_t s) {
+  int total = a.n_belem * a.ncomp;
+  if (total <= 0) return cudaSuccess;
+  int grid = std::min(total, 148 * 16);
+  SIPG_DISPATCH_B(dim, order, apply_bc_kernel<D, P><<<grid, 128, 0, s>>>(a); note_launch(); return cudaGetLastError());
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace sipg

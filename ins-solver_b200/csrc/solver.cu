@@ -1,0 +1,585 @@
+// Krylov solvers and the p-multigrid preconditioner, all on the device.
+//
+// Replaces ViscousSolver3D::conjugate_gradient / preconditioned_conjugate_gradient
+// (src/solvers/3d/slip_matrix/viscous_solver.cpp:89-301) with its preconditioners
+// (:357-453), and the LinearSolver family created at
+// src/solvers/3d/ins_solver_base.cpp:1522-1536 (PETScJacobiSolver,
+// PETScBlockJacobiSolver, PETScInvMassSolver, PETScPMultigrid; unvendored, so the
+// p-multigrid follows its configuration keys [p-multigrid] orders / cheb_orders /
+// eigen_val_saftey_factor, examples/3d/oscillating_droplet/config.ini:24-31).
+//
+// Every scalar of the iteration (alpha, beta, norms) stays on the device; the
+// host reads one FP64 residual norm per iteration to decide termination.
+// Mixed precision: the V-cycle (smoother applies, transfers, coarse CG) runs in
+// FP32 while the outer flexible CG, its residual update, inner products and step
+// lengths, and the final defect r = b - A x stay FP64.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <type_traits>
+#include <vector>
+
+#include "../../include/sipg_b200.h"
+#include "capi_util.hpp"
+#include "runtime.hpp"
+#include "sipg_blocks.cuh"
+#include "vecops.cuh"
+
+using namespace sipg;
+
+namespace {
+
+struct PinnedScalars {
+  double* h = nullptr;
+  PinnedScalars() { SIPG_CUDA(cudaMallocHost(&h, S_COUNT * sizeof(double))); }
+  ~PinnedScalars() { if (h) cudaFreeHost(h); }
+};
+
+struct Level {
+  std::unique_ptr<sipg_op> own;  // levels > 0 own their operator
+  sipg_op* op = nullptr;
+  int order = 0, Np = 0;
+  size_t n = 0;
+  DevBuf dinv64, dinv32, factor64, mm64;
+  double lmax = 0.0;
+  DevBuf P64, P32;               // prolongation from the next level: Np x Np_next
+  // work vectors in the V-cycle precision
+  DevBuf rhs, z, res, d;
+  DevBuf cp, cs, cAp;            // coarse CG
+};
+
+// Per-element interpolation kernel: out_e = I in_e (I: Npo x Npi row-major)
+__global__ void k_interp(double* out, const double* in, const double* I, int K, int Npo, int Npi) {
+  const size_t total = (size_t)K * Npo;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t e = i / Npo;
+    const int r = (int)(i % Npo);
+    double s = 0.0;
+    for (int j = 0; j < Npi; ++j) s += I[r * Npi + j] * in[e * Npi + j];
+    out[i] = s;
+  }
+}
+
+__global__ void k_recip(double* d, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    d[i] = 1.0 / d[i];
+}
+
+__global__ void k_scale(double* v, size_t n, const double* scal, int slot) {
+  const double inv = 1.0 / sqrt(scal[slot]);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    v[i] *= inv;
+}
+
+__global__ void k_mul(double* v, const double* w, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    v[i] *= w[i];
+}
+
+int grid_for(size_t n) { return (int)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, 148 * 16)); }
+
+uint64_t smix(uint64_t* s) {
+  uint64_t z = (*s += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+}  // namespace
+
+struct sipg_solver {
+  sipg_op* op = nullptr;
+  int kind = 0;
+  sipg_solver_opts o{};
+  size_t n = 0;
+  cudaStream_t stream = nullptr;
+  DevBuf r, z, zold, p, Ap, bw, xw, r32, z32;
+  DevBuf scal, partial, counter;
+  RedWork rw;
+  PinnedScalars hs;
+  DevBuf dinv, blocks, minv;
+  std::vector<Level> lv;
+  bool dirty = true;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  double* S() const { return scal.as<double>(); }
+  ~sipg_solver() {
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  double read_scalar(int slot) {
+    SIPG_CUDA(cudaMemcpyAsync(hs.h + slot, S() + slot, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    SIPG_CUDA(cudaStreamSynchronize(stream));
+    return hs.h[slot];
+  }
+
+  void dot(const double* a, const double* b, int slot) {
+    const double* aa[1] = {a};
+    const double* bb[1] = {b};
+    multi_dot<double>(aa, bb, 1, n, S() + slot, 1, rw, stream);
+  }
+
+  void setup();
+  void setup_pmg();
+  template <typename T> void vcycle(int l);
+  template <typename T> void chebyshev(Level& L, bool want_res);
+  template <typename T> void coarse(Level& L);
+  void precondition(const double* rin, double* zout);
+  int solve(const double* b, double* x, sipg_solve_info* info);
+  double power_lmax(sipg_op* lop, const double* dinv64, size_t nl);
+};
+
+// Diagonal of an operator (FP64), with its pinned DOF.
+static void op_diag(sipg_op* op, double* out, cudaStream_t s) {
+  SIPG_CUDA(launch_blocks(op->mesh->dim, op->order, op->block_args(BLOCK_DIAG_ONLY, 0, out, true), s));
+}
+
+double sipg_solver::power_lmax(sipg_op* lop, const double* dinv64, size_t nl) {
+  // Power iteration on D^-1 A from v0_i = U(-1,1), splitmix64 seed 0x5eed.
+  std::vector<double> h(nl);
+  uint64_t st = 0x5eedull;
+  for (size_t i = 0; i < nl; ++i) h[i] = 2.0 * ((smix(&st) >> 11) * (1.0 / 9007199254740992.0)) - 1.0;
+  DevBuf v(nl * sizeof(double)), w(nl * sizeof(double));
+  SIPG_CUDA(cudaMemcpyAsync(v.p, h.data(), nl * sizeof(double), cudaMemcpyHostToDevice, stream));
+  double lam = 0.0;
+  for (int it = 0; it < o.eig_iters; ++it) {
+    const double* a[1] = {v.as<double>()};
+    multi_dot<double>(a, a, 1, nl, S() + S_TMP, 1, rw, stream);
+    k_scale<<<grid_for(nl), 256, 0, stream>>>(v.as<double>(), nl, S(), S_TMP);
+      note_launch();
+    lop->apply<double>(v.as<double>(), w.as<double>(), stream);
+    k_mul<<<grid_for(nl), 256, 0, stream>>>(w.as<double>(), dinv64, nl);
+      note_launch();
+    const double* b[1] = {w.as<double>()};
+    multi_dot<double>(b, b, 1, nl, S() + S_TMP, 1, rw, stream);
+    lam = std::sqrt(read_scalar(S_TMP));
+    std::swap(v, w);
+  }
+  return lam;
+}
+
+void sipg_solver::setup_pmg() {
+  const int nl = o.n_levels;
+  if (nl < 1 || nl > 4) throw Error(SIPG_INVALID_ARG, "n_levels must be 1..4");
+  if (o.orders[0] != op->order) throw Error(SIPG_INVALID_ARG, "orders[0] must equal the operator's order");
+  for (int l = 1; l < nl; ++l)
+    if (o.orders[l] < 1 || o.orders[l] >= o.orders[l - 1]) throw Error(SIPG_INVALID_ARG, "orders must decrease");
+  const bool f32 = o.precision == SIPG_FP32;
+  const size_t ts = f32 ? sizeof(float) : sizeof(double);
+  sipg_mesh* m = op->mesh;
+  const int K = m->K, nc = op->ncomp, dim = m->dim;
+  if (lv.empty()) {
+    lv.resize(nl);
+    for (int l = 0; l < nl; ++l) {
+      Level& L = lv[l];
+      L.order = o.orders[l];
+      if (l == 0) {
+        L.op = op;
+      } else {
+        L.own = create_op(m, L.order, nc);
+        L.op = L.own.get();
+        set_bc_types_host(L.op, op->bct_host);
+      }
+      L.Np = L.op->Np;
+      L.n = (size_t)nc * K * L.Np;
+      L.dinv64 = DevBuf(L.n * sizeof(double));
+      if (f32) L.dinv32 = DevBuf(L.n * sizeof(float));
+      L.rhs = DevBuf(L.n * ts);
+      L.z = DevBuf(L.n * ts);
+      L.res = DevBuf(L.n * ts);
+      L.d = DevBuf(L.n * ts);
+      if (l == nl - 1) {
+        L.cp = DevBuf(L.n * ts);
+        L.cs = DevBuf(L.n * ts);
+        L.cAp = DevBuf(L.n * ts);
+      }
+      if (l < nl - 1) {
+        std::vector<double> P = interp_matrix(dim, o.orders[l + 1], L.order);
+        L.P64 = DevBuf(P.size() * sizeof(double));
+        L.P64.upload(P.data(), P.size() * sizeof(double));
+        std::vector<float> P32(P.begin(), P.end());
+        L.P32 = DevBuf(P32.size() * sizeof(float));
+        L.P32.upload(P32.data(), P32.size() * sizeof(float));
+      }
+    }
+  }
+  // Coefficients of the coarse levels: interpolate the fine nodal factor / mm.
+  for (int l = 1; l < nl; ++l) {
+    Level& L = lv[l];
+    std::vector<double> I = interp_matrix(dim, o.orders[0], L.order);
+    DevBuf Id(I.size() * sizeof(double));
+    Id.upload(I.data(), I.size() * sizeof(double));
+    if (op->has_factor) {
+      if (!L.factor64.p) L.factor64 = DevBuf((size_t)K * L.Np * sizeof(double));
+      k_interp<<<grid_for((size_t)K * L.Np), 256, 0, stream>>>(L.factor64.as<double>(), op->factor64.as<double>(),
+                                                               Id.as<double>(), K, L.Np, op->Np);
+      note_launch();
+      set_factor_device(L.op, L.factor64.as<double>(), stream);
+    } else {
+      L.op->has_factor = false;
+      L.op->refresh_tau(stream);
+    }
+    if (op->mm_mode == SIPG_MM_NODAL) {
+      if (!L.mm64.p) L.mm64 = DevBuf((size_t)K * L.Np * sizeof(double));
+      k_interp<<<grid_for((size_t)K * L.Np), 256, 0, stream>>>(L.mm64.as<double>(), op->mm64.as<double>(),
+                                                               Id.as<double>(), K, L.Np, op->Np);
+      note_launch();
+      set_mm_device(L.op, SIPG_MM_NODAL, 0.0, L.mm64.as<double>(), stream);
+    } else {
+      set_mm_device(L.op, op->mm_mode, op->mm_scalar, nullptr, stream);
+    }
+    if (op->pin_elem >= 0) {
+      L.op->pin_elem = op->pin_elem;
+      L.op->pin_node = op->pin_node < L.Np ? op->pin_node : 0;
+      SIPG_CUDA(cudaStreamSynchronize(stream));
+      L.op->refresh_pin(stream);
+    } else {
+      L.op->pin_elem = -1;
+    }
+    SIPG_CUDA(cudaStreamSynchronize(stream));
+  }
+  for (int l = 0; l < nl; ++l) {
+    Level& L = lv[l];
+    op_diag(L.op, L.dinv64.as<double>(), stream);
+    k_recip<<<grid_for(L.n), 256, 0, stream>>>(L.dinv64.as<double>(), L.n);
+      note_launch();
+    if (f32) to_f32(L.dinv32.as<float>(), L.dinv64.as<double>(), L.n, stream);
+    L.lmax = power_lmax(L.op, L.dinv64.as<double>(), L.n);
+  }
+}
+
+void sipg_solver::setup() {
+  n = (size_t)op->ncomp * op->mesh->K * op->Np;
+  if (!r.p) {
+    size_t b = n * sizeof(double);
+    r = DevBuf(b); z = DevBuf(b); zold = DevBuf(b); p = DevBuf(b); Ap = DevBuf(b);
+    scal = DevBuf(S_COUNT * sizeof(double));
+    partial = DevBuf(kRedBlocks * 4 * sizeof(double));
+    counter = DevBuf(sizeof(unsigned));
+    SIPG_CUDA(cudaMemsetAsync(counter.p, 0, sizeof(unsigned), stream));
+    SIPG_CUDA(cudaMemsetAsync(scal.p, 0, S_COUNT * sizeof(double), stream));
+    rw.partial = partial.as<double>();
+    rw.counter = counter.as<unsigned>();
+    if (kind == SIPG_SOLVER_PMULTIGRID && o.precision == SIPG_FP32) {
+      r32 = DevBuf(n * sizeof(float));
+      z32 = DevBuf(n * sizeof(float));
+    }
+  }
+  if (kind == SIPG_SOLVER_JACOBI) {
+    if (!dinv.p) dinv = DevBuf(n * sizeof(double));
+    op_diag(op, dinv.as<double>(), stream);
+    k_recip<<<grid_for(n), 256, 0, stream>>>(dinv.as<double>(), n);
+      note_launch();
+  } else if (kind == SIPG_SOLVER_BLOCK_JACOBI) {
+    if (!blocks.p) blocks = DevBuf(n * op->Np * sizeof(double));
+    SIPG_CUDA(launch_blocks(op->mesh->dim, op->order,
+                            op->block_args(BLOCK_INVERSE, o.ref_volume_block, blocks.as<double>(), true), stream));
+  } else if (kind == SIPG_SOLVER_INV_MASS) {
+    if (!minv.p) {
+      const RefElement& re = op->dref->ref;
+      std::vector<double> mi(re.Minv);
+      minv = DevBuf(mi.size() * sizeof(double));
+      minv.upload(mi.data(), mi.size() * sizeof(double), stream);
+    }
+  } else if (kind == SIPG_SOLVER_PMULTIGRID) {
+    setup_pmg();
+  }
+  SIPG_CUDA(cudaStreamSynchronize(stream));
+  dirty = false;
+}
+
+template <typename T>
+void sipg_solver::chebyshev(Level& L, bool want_res) {
+  const double hi = L.lmax * o.eig_safety, lo = hi / o.eig_ratio;
+  const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
+  double rho_old = 1.0 / sigma;
+  const T* dinv = std::is_same<T, float>::value ? (const T*)L.dinv32.p : (const T*)L.dinv64.p;
+  T* d = L.d.as<T>();
+  T* z = L.z.as<T>();
+  T* res = L.res.as<T>();
+  for (int it = 0; it < o.cheb_order; ++it) {
+    double c1 = 0.0, c2 = 1.0 / theta;
+    if (it > 0) {
+      double rho = 1.0 / (2.0 * sigma - rho_old);
+      c1 = rho * rho_old;
+      c2 = 2.0 * rho / delta;
+      rho_old = rho;
+    }
+    cheb_step<T>(d, z, res, dinv, (T)c1, (T)c2, L.n, stream);
+    if (it < o.cheb_order - 1 || want_res) L.op->apply<T>(d, res, stream, T(-1), T(1));
+  }
+}
+
+template <typename T>
+void sipg_solver::coarse(Level& L) {
+  // Fixed-count Jacobi-PCG from zero on the coarsest order, scalars on device.
+  const T* dinv = std::is_same<T, float>::value ? (const T*)L.dinv32.p : (const T*)L.dinv64.p;
+  T* z = L.z.as<T>();
+  T* res = L.res.as<T>();
+  T* cp = L.cp.as<T>();
+  T* cs = L.cs.as<T>();
+  T* cAp = L.cAp.as<T>();
+  vzero<T>(z, L.n, stream);
+  vcopy<T>(res, L.rhs.as<T>(), L.n, stream);
+  jacobi<T>(cs, res, dinv, L.n, stream);
+  vcopy<T>(cp, cs, L.n, stream);
+  {
+    const T* a[1] = {res};
+    const T* b[1] = {cs};
+    multi_dot<T>(a, b, 1, L.n, S() + S_C_RZ, 1, rw, stream);
+  }
+  for (int it = 0; it < o.coarse_iters; ++it) {
+    L.op->apply<T>(cp, cAp, stream);
+    const T* a[1] = {cp};
+    const T* b[1] = {cAp};
+    multi_dot<T>(a, b, 1, L.n, S() + S_C_PAP, 1, rw, stream);
+    coarse_update<T>(z, res, cs, cp, cAp, dinv, L.n, S(), rw, stream);
+    coarse_update_p<T>(cp, cs, L.n, S(), stream);
+  }
+}
+
+template <typename T>
+void sipg_solver::vcycle(int l) {
+  Level& L = lv[l];
+  const int nl = (int)lv.size();
+  if (l == nl - 1) {
+    coarse<T>(L);
+    return;
+  }
+  Level& Cl = lv[l + 1];
+  const bool f32 = std::is_same<T, float>::value;
+  const T* P = f32 ? (const T*)L.P32.p : (const T*)L.P64.p;
+  const int K = op->mesh->K, nc = op->ncomp;
+  vzero<T>(L.z.as<T>(), L.n, stream);
+  vcopy<T>(L.res.as<T>(), L.rhs.as<T>(), L.n, stream);
+  chebyshev<T>(L, true);
+  restrict_elem<T>(Cl.rhs.as<T>(), L.res.as<T>(), P, K, L.Np, Cl.Np, nc, stream);
+  vcycle<T>(l + 1);
+  prolong_add<T>(L.z.as<T>(), Cl.z.as<T>(), P, K, L.Np, Cl.Np, nc, stream);
+  vcopy<T>(L.res.as<T>(), L.rhs.as<T>(), L.n, stream);
+  L.op->apply<T>(L.z.as<T>(), L.res.as<T>(), stream, T(-1), T(1));
+  chebyshev<T>(L, false);
+}
+
+void sipg_solver::precondition(const double* rin, double* zout) {
+  switch (kind) {
+    case SIPG_SOLVER_INV_MASS: {
+      const int dim = op->mesh->dim;
+      inv_mass<double>(zout, rin, minv.as<double>(), op->mesh->geof64.as<double>(), dim == 3 ? 10 : 5,
+                       dim == 3 ? 9 : 4, op->mesh->K, op->Np, op->ncomp, o.inv_mass_factor, stream);
+      break;
+    }
+    case SIPG_SOLVER_JACOBI:
+      jacobi<double>(zout, rin, dinv.as<double>(), n, stream);
+      break;
+    case SIPG_SOLVER_BLOCK_JACOBI:
+      block_matvec<double>(zout, blocks.as<double>(), rin, (int)(n / op->Np), op->Np, stream);
+      break;
+    case SIPG_SOLVER_PMULTIGRID:
+      if (o.precision == SIPG_FP32) {
+        to_f32(lv[0].rhs.as<float>(), rin, n, stream);
+        vcycle<float>(0);
+        to_f64(zout, lv[0].z.as<float>(), n, stream);
+      } else {
+        vcopy<double>(lv[0].rhs.as<double>(), rin, n, stream);
+        vcycle<double>(0);
+        vcopy<double>(zout, lv[0].z.as<double>(), n, stream);
+      }
+      break;
+    default:
+      vcopy<double>(zout, rin, n, stream);
+  }
+  if (o.nullspace) {
+    vsum<double>(zout, n, S() + S_SUM, rw, stream);
+    sub_mean<double>(zout, n, S(), S_SUM, stream);
+  }
+}
+
+int sipg_solver::solve(const double* b, double* x, sipg_solve_info* info) {
+  auto t0 = std::chrono::steady_clock::now();
+  if (dirty) setup();
+  auto t1 = std::chrono::steady_clock::now();
+  SIPG_CUDA(cudaEventRecord(ev0, stream));
+  double* R = r.as<double>();
+  double* Z = z.as<double>();
+  double* ZO = zold.as<double>();
+  double* Pv = p.as<double>();
+  double* AP = Ap.as<double>();
+  // r = b - A x (calc_res_explicit, viscous_solver.cpp:329-343)
+  vcopy<double>(R, b, n, stream);
+  op->apply<double>(x, R, stream, -1.0, 1.0);
+  if (o.nullspace) {
+    vsum<double>(R, n, S() + S_SUM, rw, stream);
+    sub_mean<double>(R, n, S(), S_SUM, stream);
+  }
+  dot(b, b, S_BB);
+  dot(R, R, S_RR);
+  const double bnorm = std::sqrt(read_scalar(S_BB));
+  double res = std::sqrt(read_scalar(S_RR));
+  const double tol = std::max(o.abs_tol, o.rel_tol * bnorm);
+  int iter = 0, status = SIPG_OK;
+  if (!std::isfinite(bnorm) || !std::isfinite(res)) {
+    status = SIPG_BREAKDOWN;
+    res = NAN;
+  }
+  if (kind == SIPG_SOLVER_CG) {
+    // conjugate_gradient: explicit residual every iteration (viscous_solver.cpp:115-160)
+    vcopy<double>(Pv, R, n, stream);
+    while (status == SIPG_OK && res > tol && iter < o.max_iter) {
+      op->apply<double>(Pv, AP, stream);
+      const double* a[2] = {R, Pv};
+      const double* bb[2] = {R, AP};
+      multi_dot<double>(a, bb, 2, n, S() + S_RZ, 1, rw, stream);  // S_RZ = r.r, S_PAP = p.Ap
+      // x += alpha p; r is recomputed below, the rr output is unused here
+      cg_update_xr(x, Z, Pv, AP, n, S(), S_RZ, S_PAP, S() + S_TMP, rw, stream);
+      vcopy<double>(R, b, n, stream);
+      op->apply<double>(x, R, stream, -1.0, 1.0);
+      if (o.nullspace) {
+        vsum<double>(R, n, S() + S_SUM, rw, stream);
+        sub_mean<double>(R, n, S(), S_SUM, stream);
+      }
+      dot(R, R, S_RR);
+      update_p<double>(Pv, R, n, S(), S_RR, S_RZ, stream);
+      ++iter;
+      double pap = read_scalar(S_PAP);
+      res = std::sqrt(hs.h[S_RR] = read_scalar(S_RR));
+      if (!(pap > 0.0) || !std::isfinite(res)) { status = SIPG_BREAKDOWN; break; }
+    }
+  } else {
+    // flexible PCG (viscous_solver.cpp:177-301)
+    if (status == SIPG_OK) precondition(R, Z);
+    vcopy<double>(Pv, Z, n, stream);
+    while (status == SIPG_OK && res > tol && iter < o.max_iter) {
+      op->apply<double>(Pv, AP, stream);
+      const double* a[2] = {R, Pv};
+      const double* bb[2] = {Z, AP};
+      multi_dot<double>(a, bb, 2, n, S() + S_RZ, 1, rw, stream);  // cg3_alpha_pre
+      cg_update_xr(x, R, Pv, AP, n, S(), S_RZ, S_PAP, S() + S_RR, rw, stream);  // update_ans + update_res
+      if (o.nullspace) {
+        vsum<double>(R, n, S() + S_SUM, rw, stream);
+        sub_mean<double>(R, n, S(), S_SUM, stream);
+        dot(R, R, S_RR);
+      }
+      std::swap(Z, ZO);
+      precondition(R, Z);
+      dot_diff(R, Z, ZO, n, S() + S_BETA, rw, stream);  // cg3_compute_beta_pre_flex
+      update_p<double>(Pv, Z, n, S(), S_BETA, S_RZ, stream);
+      ++iter;
+      double pap = read_scalar(S_PAP);
+      res = std::sqrt(read_scalar(S_RR));
+      if (!(pap > 0.0) || !std::isfinite(res)) { status = SIPG_BREAKDOWN; break; }
+    }
+  }
+  if (status == SIPG_OK && res > tol) status = SIPG_NOT_CONVERGED;
+  SIPG_CUDA(cudaEventRecord(ev1, stream));
+  // final defect with an explicit FP64 apply
+  vcopy<double>(AP, b, n, stream);
+  op->apply<double>(x, AP, stream, -1.0, 1.0);
+  if (o.nullspace) {
+    vsum<double>(AP, n, S() + S_SUM, rw, stream);
+    sub_mean<double>(AP, n, S(), S_SUM, stream);
+  }
+  dot(AP, AP, S_TMP);
+  double true_res = std::sqrt(read_scalar(S_TMP));
+  float ms = 0.f;
+  SIPG_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+  if (info) {
+    info->iters = iter;
+    info->abs_res = res;
+    info->rel_res = bnorm > 0 ? res / bnorm : res;
+    info->true_rel_res = bnorm > 0 ? true_res / bnorm : true_res;
+    info->setup_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    info->solve_ms = ms;
+    info->status = status;
+  }
+  return status;
+}
+
+extern "C" {
+
+int sipg_solver_default_opts(int kind, sipg_solver_opts* o) {
+  return guarded([&] {
+    if (!o) throw Error(SIPG_INVALID_ARG, "null opts");
+    std::memset(o, 0, sizeof(*o));
+    // set_tol_and_iter defaults of the pressure solve (ins_solver_base.cpp:153-160)
+    o->rel_tol = 1e-8;
+    o->abs_tol = 1e-9;
+    o->max_iter = 500;
+    o->precision = SIPG_FP64;
+    o->inv_mass_factor = 1.0;
+    o->n_levels = 3;
+    o->orders[0] = 3; o->orders[1] = 2; o->orders[2] = 1;
+    o->cheb_order = 4;
+    o->eig_safety = 1.1;
+    o->eig_ratio = 30.0;
+    o->eig_iters = 20;
+    o->coarse_iters = 20;
+    o->check_every = 1;
+    (void)kind;
+  });
+}
+
+int sipg_solver_create(sipg_op* op, int kind, const sipg_solver_opts* o, sipg_solver** out) {
+  return guarded([&] {
+    if (!op || !out || kind < 0 || kind > SIPG_SOLVER_PMULTIGRID) throw Error(SIPG_INVALID_ARG, "solver_create");
+    auto s = std::make_unique<sipg_solver>();
+    s->op = op;
+    s->kind = kind;
+    if (o) s->o = *o;
+    else sipg_solver_default_opts(kind, &s->o);
+    if (s->o.precision != SIPG_FP64 && s->o.precision != SIPG_FP32) throw Error(SIPG_INVALID_ARG, "precision");
+    if (kind == SIPG_SOLVER_PMULTIGRID && s->o.n_levels >= 1) s->o.orders[0] = op->order;
+    SIPG_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    SIPG_CUDA(cudaEventCreate(&s->ev0));
+    SIPG_CUDA(cudaEventCreate(&s->ev1));
+    *out = s.release();
+  });
+}
+
+int sipg_solver_setup(sipg_solver* s) {
+  return guarded([&] {
+    if (!s) throw Error(SIPG_INVALID_ARG, "null solver");
+    s->setup();
+  });
+}
+
+int sipg_solver_solve(sipg_solver* s, const double* b, double* x, sipg_solve_info* info) {
+  int st = SIPG_OK;
+  int g = guarded([&] {
+    if (!s || !b || !x) throw Error(SIPG_INVALID_ARG, "solve arguments");
+    st = s->solve(b, x, info);
+  });
+  return g != SIPG_OK ? g : st;
+}
+
+int sipg_solver_solve_host(sipg_solver* s, const double* b, double* x, sipg_solve_info* info) {
+  int st = SIPG_OK;
+  int g = guarded([&] {
+    if (!s || !b || !x) throw Error(SIPG_INVALID_ARG, "solve arguments");
+    size_t bytes = (size_t)s->op->ncomp * s->op->mesh->K * s->op->Np * sizeof(double);
+    if (!s->bw.p) { s->bw = DevBuf(bytes); s->xw = DevBuf(bytes); }
+    SIPG_CUDA(cudaMemcpyAsync(s->bw.p, b, bytes, cudaMemcpyHostToDevice, s->stream));
+    SIPG_CUDA(cudaMemcpyAsync(s->xw.p, x, bytes, cudaMemcpyHostToDevice, s->stream));
+    st = s->solve(s->bw.as<double>(), s->xw.as<double>(), info);
+    SIPG_CUDA(cudaMemcpyAsync(x, s->xw.p, bytes, cudaMemcpyDeviceToHost, s->stream));
+    SIPG_CUDA(cudaStreamSynchronize(s->stream));
+  });
+  return g != SIPG_OK ? g : st;
+}
+
+void sipg_solver_destroy(sipg_solver* s) { delete s; }
+
+int sipg_launch_count(unsigned long long* n) {
+  return guarded([&] {
+    if (!n) throw Error(SIPG_INVALID_ARG, "null pointer");
+    *n = launch_count();
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,387 @@
+// Vector kernels for the solvers. See vecops.cuh.
+#include <algorithm>
+#include <atomic>
+
+#include "vecops.cuh"
+
+namespace sipg {
+
+static std::atomic<unsigned long long> g_launches{0};
+void note_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+namespace {
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-reduce NK values; thread 0 returns the block totals in v[].
+template <int NK>
+__device__ __forceinline__ void block_sum(double (&v)[NK]) {
+  __shared__ double sh[NK][kRedThreads / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < NK; ++k) {
+    double t = warp_sum(v[k]);
+    if (lane == 0) sh[k][wid] = t;
+  }
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int k = 0; k < NK; ++k) {
+      double t = lane < kRedThreads / 32 ? sh[k][lane] : 0.0;
+      v[k] = warp_sum(t);
+    }
+  }
+}
+
+// Second stage: the last block to finish sums the partials in index order.
+template <int NK>
+__device__ __forceinline__ void finish(const double (&v)[NK], double* partial, unsigned* counter,
+                                       double* out, int out_stride) {
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NK; ++k) partial[blockIdx.x * 4 + k] = v[k];
+    __threadfence();
+    unsigned t = atomicAdd(counter, 1u);
+    last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double acc[NK];
+#pragma unroll
+  for (int k = 0; k < NK; ++k) acc[k] = 0.0;
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+#pragma unroll
+    for (int k = 0; k < NK; ++k) acc[k] += ((volatile double*)partial)[b * 4 + k];
+  block_sum<NK>(acc);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NK; ++k) out[k * out_stride] = acc[k];
+    *counter = 0u;
+  }
+}
+
+template <typename T, int NK>
+__global__ void __launch_bounds__(kRedThreads) k_multi_dot(const T* a0, const T* b0, const T* a1,
+                                                           const T* b1, const T* a2, const T* b2,
+                                                           size_t n, double* partial,
+                                                           unsigned* counter, double* out,
+                                                           int out_stride) {
+  double v[NK];
+#pragma unroll
+  for (int k = 0; k < NK; ++k) v[k] = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    v[0] += (double)a0[i] * (double)b0[i];
+    if (NK > 1) v[1 % NK] += (double)a1[i] * (double)b1[i];
+    if (NK > 2) v[2 % NK] += (double)a2[i] * (double)b2[i];
+  }
+  block_sum<NK>(v);
+  finish<NK>(v, partial, counter, out, out_stride);
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_dot_diff(const double* r, const double* z, const double* zo,
+                                                          size_t n, double* partial, unsigned* counter,
+                                                          double* out) {
+  double v[1] = {0.0};
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    v[0] += r[i] * (z[i] - zo[i]);
+  block_sum<1>(v);
+  finish<1>(v, partial, counter, out, 1);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_sum(const T* a, size_t n, double* partial,
+                                                     unsigned* counter, double* out) {
+  double v[1] = {0.0};
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    v[0] += (double)a[i];
+  block_sum<1>(v);
+  finish<1>(v, partial, counter, out, 1);
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_cg_update_xr(double* x, double* r, const double* p,
+                                                              const double* Ap, size_t n,
+                                                              const double* scal, int num, int den,
+                                                              double* partial, unsigned* counter,
+                                                              double* rr_out) {
+  const double alpha = scal[num] / scal[den];
+  double v[1] = {0.0};
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    x[i] += alpha * p[i];
+    double ri = r[i] - alpha * Ap[i];
+    r[i] = ri;
+    v[0] += ri * ri;
+  }
+  block_sum<1>(v);
+  finish<1>(v, partial, counter, rr_out, 1);
+}
+
+template <typename T>
+__global__ void k_update_p(T* p, const T* z, size_t n, const double* scal, int num, int den) {
+  const T beta = (T)(scal[num] / scal[den]);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    p[i] = z[i] + beta * p[i];
+}
+
+template <typename T>
+__global__ void k_sub_mean(T* v, size_t n, const double* scal, int slot) {
+  const T mean = (T)(scal[slot] / (double)n);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    v[i] -= mean;
+}
+
+template <typename T>
+__global__ void k_copy(T* d, const T* s, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) d[i] = s[i];
+}
+template <typename T>
+__global__ void k_zero(T* d, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) d[i] = T(0);
+}
+__global__ void k_to_f32(float* d, const double* s, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) d[i] = (float)s[i];
+}
+__global__ void k_to_f64(double* d, const float* s, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) d[i] = (double)s[i];
+}
+template <typename T>
+__global__ void k_jacobi(T* z, const T* r, const T* dinv, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) z[i] = dinv[i] * r[i];
+}
+template <typename T>
+__global__ void k_cheb(T* d, T* z, const T* res, const T* dinv, T c1, T c2, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    T di = (c1 != T(0) ? c1 * d[i] : T(0)) + c2 * dinv[i] * res[i];
+    d[i] = di;
+    z[i] += di;
+  }
+}
+
+// One warp per block row set: thread handles (block, row).
+template <typename T>
+__global__ void k_block_matvec(T* y, const T* B, const T* x, int nb, int Np) {
+  const size_t total = (size_t)nb * Np;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t b = i / Np;
+    const int r = (int)(i % Np);
+    const T* Bb = B + (b * Np + r) * Np;
+    const T* xb = x + b * Np;
+    double s = 0.0;
+    for (int j = 0; j < Np; ++j) s += (double)Bb[j] * (double)xb[j];
+    y[i] = (T)s;
+  }
+}
+
+template <typename T>
+__global__ void k_inv_mass(T* y, const T* x, const T* Minv, const T* geof, int ngeof, int jidx, int K,
+                           int Np, int ncomp, T scale) {
+  const size_t total = (size_t)ncomp * K * Np;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t be = i / Np;
+    const int r = (int)(i % Np);
+    const int e = (int)(be % K);
+    const T* xb = x + be * Np;
+    T s = T(0);
+    for (int j = 0; j < Np; ++j) s += Minv[r * Np + j] * xb[j];
+    y[i] = scale * s / geof[(size_t)e * ngeof + jidx];
+  }
+}
+
+template <typename T>
+__global__ void k_restrict(T* rc, const T* r, const T* P, int K, int Npf, int Npc, int ncomp) {
+  const size_t total = (size_t)ncomp * K * Npc;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t be = i / Npc;
+    const int j = (int)(i % Npc);
+    const T* rb = r + be * Npf;
+    T s = T(0);
+    for (int k = 0; k < Npf; ++k) s += P[k * Npc + j] * rb[k];
+    rc[i] = s;
+  }
+}
+
+template <typename T>
+__global__ void k_prolong_add(T* z, const T* zc, const T* P, int K, int Npf, int Npc, int ncomp) {
+  const size_t total = (size_t)ncomp * K * Npf;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t be = i / Npf;
+    const int k = (int)(i % Npf);
+    const T* zb = zc + be * Npc;
+    T s = T(0);
+    for (int j = 0; j < Npc; ++j) s += P[k * Npc + j] * zb[j];
+    z[i] += s;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_coarse_update(T* z, T* r, T* sv, const T* p, const T* Ap,
+                                                               const T* dinv, size_t n, double* scal,
+                                                               double* partial, unsigned* counter) {
+  const double pap = scal[S_C_PAP];
+  const bool ok = pap > 0.0 && scal[S_C_RZ] > 0.0;
+  const T alpha = ok ? (T)(scal[S_C_RZ] / pap) : T(0);
+  double v[1] = {0.0};
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    z[i] += alpha * p[i];
+    T ri = r[i] - alpha * Ap[i];
+    r[i] = ri;
+    T si = dinv[i] * ri;
+    sv[i] = si;
+    v[0] += (double)ri * (double)si;
+  }
+  block_sum<1>(v);
+  finish<1>(v, partial, counter, scal + S_C_RZN, 1);
+}
+
+template <typename T>
+__global__ void k_coarse_update_p(T* p, const T* sv, size_t n, double* scal) {
+  const double rz = scal[S_C_RZ];
+  const T beta = rz > 0.0 ? (T)(scal[S_C_RZN] / rz) : T(0);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    p[i] = sv[i] + beta * p[i];
+}
+
+__global__ void k_shift_scalar(double* scal, int from, int to) { scal[to] = scal[from]; }
+
+inline int grid_for(size_t n) {
+  size_t g = (n + 255) / 256;
+  return (int)std::max<size_t>(1, std::min<size_t>(g, 148 * 16));
+}
+
+}  // namespace
+
+template <typename T>
+void multi_dot(const T* const* a, const T* const* b, int nk, size_t n, double* out, int out_stride,
+               const RedWork& w, cudaStream_t s) {
+  if (nk == 1)
+    k_multi_dot<T, 1><<<kRedBlocks, kRedThreads, 0, s>>>(a[0], b[0], nullptr, nullptr, nullptr, nullptr, n,
+                                                         w.partial, w.counter, out, out_stride);
+  else if (nk == 2)
+    k_multi_dot<T, 2><<<kRedBlocks, kRedThreads, 0, s>>>(a[0], b[0], a[1], b[1], nullptr, nullptr, n,
+                                                         w.partial, w.counter, out, out_stride);
+  else
+    k_multi_dot<T, 3><<<kRedBlocks, kRedThreads, 0, s>>>(a[0], b[0], a[1], b[1], a[2], b[2], n,
+                                                         w.partial, w.counter, out, out_stride);
+  note_launch();
+}
+
+void dot_diff(const double* r, const double* z, const double* zo, size_t n, double* out,
+              const RedWork& w, cudaStream_t s) {
+  k_dot_diff<<<kRedBlocks, kRedThreads, 0, s>>>(r, z, zo, n, w.partial, w.counter, out);
+  note_launch();
+}
+
+template <typename T>
+void vsum(const T* a, size_t n, double* out, const RedWork& w, cudaStream_t s) {
+  k_sum<T><<<kRedBlocks, kRedThreads, 0, s>>>(a, n, w.partial, w.counter, out);
+  note_launch();
+}
+
+void cg_update_xr(double* x, double* r, const double* p, const double* Ap, size_t n,
+                  const double* scal, int num, int den, double* rr_out, const RedWork& w,
+                  cudaStream_t s) {
+  k_cg_update_xr<<<kRedBlocks, kRedThreads, 0, s>>>(x, r, p, Ap, n, scal, num, den, w.partial, w.counter, rr_out);
+  note_launch();
+}
+
+template <typename T>
+void update_p(T* p, const T* z, size_t n, const double* scal, int num, int den, cudaStream_t s) {
+  k_update_p<T><<<grid_for(n), 256, 0, s>>>(p, z, n, scal, num, den);
+  note_launch();
+}
+template <typename T>
+void sub_mean(T* v, size_t n, const double* scal, int slot, cudaStream_t s) {
+  k_sub_mean<T><<<grid_for(n), 256, 0, s>>>(v, n, scal, slot);
+  note_launch();
+}
+template <typename T>
+void vcopy(T* dst, const T* src, size_t n, cudaStream_t s) {
+  k_copy<T><<<grid_for(n), 256, 0, s>>>(dst, src, n);
+  note_launch();
+}
+template <typename T>
+void vzero(T* dst, size_t n, cudaStream_t s) {
+  k_zero<T><<<grid_for(n), 256, 0, s>>>(dst, n);
+  note_launch();
+}
+void to_f32(float* dst, const double* src, size_t n, cudaStream_t s) {
+  k_to_f32<<<grid_for(n), 256, 0, s>>>(dst, src, n);
+  note_launch();
+}
+void to_f64(double* dst, const float* src, size_t n, cudaStream_t s) {
+  k_to_f64<<<grid_for(n), 256, 0, s>>>(dst, src, n);
+  note_launch();
+}
+template <typename T>
+void jacobi(T* z, const T* r, const T* dinv, size_t n, cudaStream_t s) {
+  k_jacobi<T><<<grid_for(n), 256, 0, s>>>(z, r, dinv, n);
+  note_launch();
+}
+template <typename T>
+void cheb_step(T* d, T* z, const T* res, const T* dinv, T c1, T c2, size_t n, cudaStream_t s) {
+  k_cheb<T><<<grid_for(n), 256, 0, s>>>(d, z, res, dinv, c1, c2, n);
+  note_launch();
+}
+template <typename T>
+void block_matvec(T* y, const T* B, const T* x, int nb, int Np, cudaStream_t s) {
+  k_block_matvec<T><<<grid_for((size_t)nb * Np), 256, 0, s>>>(y, B, x, nb, Np);
+  note_launch();
+}
+template <typename T>
+void inv_mass(T* y, const T* x, const T* Minv, const T* geof, int ngeof, int jidx, int K, int Np,
+              int ncomp, T scale, cudaStream_t s) {
+  k_inv_mass<T><<<grid_for((size_t)ncomp * K * Np), 256, 0, s>>>(y, x, Minv, geof, ngeof, jidx, K, Np, ncomp, scale);
+  note_launch();
+}
+template <typename T>
+void restrict_elem(T* rc, const T* r, const T* P, int K, int Npf, int Npc, int ncomp, cudaStream_t s) {
+  k_restrict<T><<<grid_for((size_t)ncomp * K * Npc), 256, 0, s>>>(rc, r, P, K, Npf, Npc, ncomp);
+  note_launch();
+}
+template <typename T>
+void prolong_add(T* z, const T* zc, const T* P, int K, int Npf, int Npc, int ncomp, cudaStream_t s) {
+  k_prolong_add<T><<<grid_for((size_t)ncomp * K * Npf), 256, 0, s>>>(z, zc, P, K, Npf, Npc, ncomp);
+  note_launch();
+}
+template <typename T>
+void coarse_update(T* z, T* r, T* sv, const T* p, const T* Ap, const T* dinv, size_t n, double* scal,
+                   const RedWork& w, cudaStream_t s) {
+  k_coarse_update<T><<<kRedBlocks, kRedThreads, 0, s>>>(z, r, sv, p, Ap, dinv, n, scal, w.partial, w.counter);
+  note_launch();
+}
+template <typename T>
+void coarse_update_p(T* p, const T* sv, size_t n, double* scal, cudaStream_t s) {
+  k_coarse_update_p<T><<<grid_for(n), 256, 0, s>>>(p, sv, n, scal);
+  note_launch();
+  k_shift_scalar<<<1, 1, 0, s>>>(scal, S_C_RZN, S_C_RZ);
+  note_launch();
+}
+
+#define SIPG_INST(T)                                                                              \
+  template void multi_dot<T>(const T* const*, const T* const*, int, size_t, double*, int,         \
+                             const RedWork&, cudaStream_t);                                      \
+  template void vsum<T>(const T*, size_t, double*, const RedWork&, cudaStream_t);                \
+  template void update_p<T>(T*, const T*, size_t, const double*, int, int, cudaStream_t);        \
+  template void sub_mean<T>(T*, size_t, const double*, int, cudaStream_t);                       \
+  template void vcopy<T>(T*, const T*, size_t, cudaStream_t);                                    \
+  template void vzero<T>(T*, size_t, cudaStream_t);                                              \
+  template void jacobi<T>(T*, const T*, const T*, size_t, cudaStream_t);                         \
+  template void cheb_step<T>(T*, T*, const T*, const T*, T, T, size_t, cudaStream_t);            \
+  template void block_matvec<T>(T*, const T*, const T*, int, int, cudaStream_t);                 \
+  template void inv_mass<T>(T*, const T*, const T*, const T*, int, int, int, int, int, T,        \
+                            cudaStream_t);                                                       \
+  template void restrict_elem<T>(T*, const T*, const T*, int, int, int, int, cudaStream_t);      \
+  template void prolong_add<T>(T*, const T*, const T*, int, int, int, int, cudaStream_t);        \
+  template void coarse_update<T>(T*, T*, T*, const T*, const T*, const T*, size_t, double*,      \
+                                 const RedWork&, cudaStream_t);                                  \
+  template void coarse_update_p<T>(T*, const T*, size_t, double*, cudaStream_t);
+
+SIPG_INST(double)
+SIPG_INST(float)
+
+}  // namespace sipg

@@ -1,0 +1,104 @@
+// Vector kernels of the Krylov and multigrid loops (cg3_*.h / cg_*.h kernels of
+// the reference, src/kernels/cg3_alpha_pre.h ... cg3_update_p.h), fused so that
+// each CG step reads every vector once. Reductions are FP64 warp-shuffle sums
+// with a fixed two-stage order (block partials, then the last block reduces the
+// partials in index order), so results are bitwise reproducible run to run and
+// the scalars never leave the device.
+#pragma once
+#include <cstddef>
+#include <cuda_runtime.h>
+
+namespace sipg {
+
+// Count of kernel launches issued by this library (diagnostics).
+void note_launch(unsigned n = 1);
+unsigned long long launch_count();
+
+// Device scalar slots used by the solvers.
+enum Scal : int {
+  S_RZ = 0,    // r . z           (alpha numerator, beta denominator)
+  S_PAP = 1,   // p . A p
+  S_RR = 2,    // r . r
+  S_BETA = 3,  // r . (z - z_old)
+  S_BB = 4,    // b . b
+  S_SUM = 5,   // sum (nullspace projection)
+  S_C_RZ = 6,  // coarse CG: r . s
+  S_C_PAP = 7, // coarse CG: p . Ap
+  S_C_RZN = 8, // coarse CG: new r . s
+  S_C_FLAG = 9,
+  S_TMP = 10,
+  S_COUNT = 16
+};
+
+struct RedWork {
+  double* partial = nullptr;   // kRedBlocks x 4
+  unsigned* counter = nullptr; // 1
+};
+constexpr int kRedBlocks = 296;
+constexpr int kRedThreads = 256;
+
+// out[k] = sum_i a_k[i] * b_k[i] for k < nk (nk <= 3); b_k may alias a_k.
+template <typename T>
+void multi_dot(const T* const* a, const T* const* b, int nk, size_t n, double* out, int out_stride,
+               const RedWork& w, cudaStream_t s);
+
+// out = sum_i r[i] * (z[i] - zo[i])   (cg3_compute_beta_pre_flex.h)
+void dot_diff(const double* r, const double* z, const double* zo, size_t n, double* out,
+              const RedWork& w, cudaStream_t s);
+
+// Sum of entries (nullspace projection).
+template <typename T>
+void vsum(const T* a, size_t n, double* out, const RedWork& w, cudaStream_t s);
+
+// x += alpha p ; r -= alpha Ap ; rr = r.r   with alpha = scal[num] / scal[den]
+void cg_update_xr(double* x, double* r, const double* p, const double* Ap, size_t n,
+                  const double* scal, int num, int den, double* rr_out, const RedWork& w,
+                  cudaStream_t s);
+// p = z + beta p   with beta = scal[num] / scal[den]
+template <typename T>
+void update_p(T* p, const T* z, size_t n, const double* scal, int num, int den, cudaStream_t s);
+// y = a (constant copy), y -= mean (scal[S_SUM] / n)
+template <typename T>
+void sub_mean(T* v, size_t n, const double* scal, int slot, cudaStream_t s);
+
+template <typename T>
+void vcopy(T* dst, const T* src, size_t n, cudaStream_t s);
+template <typename T>
+void vzero(T* dst, size_t n, cudaStream_t s);
+void to_f32(float* dst, const double* src, size_t n, cudaStream_t s);
+void to_f64(double* dst, const float* src, size_t n, cudaStream_t s);
+
+// z = dinv * r
+template <typename T>
+void jacobi(T* z, const T* r, const T* dinv, size_t n, cudaStream_t s);
+
+// Chebyshev step: d = c1 * d + c2 * dinv * res ; z += d
+template <typename T>
+void cheb_step(T* d, T* z, const T* res, const T* dinv, T c1, T c2, size_t n, cudaStream_t s);
+
+// Element-block matvec: y_e = B_e x_e (B: nb x Np x Np row-major, nb blocks)
+template <typename T>
+void block_matvec(T* y, const T* B, const T* x, int nb, int Np, cudaStream_t s);
+
+// Inverse mass: y_e = scale * Minv x_e / J_e (pre_inv_mass / pre_factor_inv_mass)
+template <typename T>
+void inv_mass(T* y, const T* x, const T* Minv, const T* geof, int ngeof, int jidx, int K, int Np,
+              int ncomp, T scale, cudaStream_t s);
+
+// Order transfer per element: restrict  rc_e = P^T r_e  (P: Npf x Npc row-major)
+//                             prolong   z_e += P zc_e
+template <typename T>
+void restrict_elem(T* rc, const T* r, const T* P, int K, int Npf, int Npc, int ncomp, cudaStream_t s);
+template <typename T>
+void prolong_add(T* z, const T* zc, const T* P, int K, int Npf, int Npc, int ncomp, cudaStream_t s);
+
+// Fixed-count coarse CG helpers (device scalars):
+//   alpha = scal[S_C_RZ] / scal[S_C_PAP]; z += alpha p; r -= alpha Ap; s = dinv r; scal[S_C_RZN] = r.s
+template <typename T>
+void coarse_update(T* z, T* r, T* sv, const T* p, const T* Ap, const T* dinv, size_t n, double* scal,
+                   const RedWork& w, cudaStream_t s);
+// p = s + (scal[S_C_RZN]/scal[S_C_RZ]) p ; scal[S_C_RZ] = scal[S_C_RZN]
+template <typename T>
+void coarse_update_p(T* p, const T* sv, size_t n, double* scal, cudaStream_t s);
+
+}  // namespace sipg

@@ -1,0 +1,276 @@
+"""Python binding of the C ABI in include/sipg_b200.h (ctypes + numpy).
+
+Host-side mirror used by the tests and the benchmark. It loads the in-tree
+libsipg_b200.so and fails loudly when it is missing: there is no CPU fallback
+for any operation of the solve path.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsipg_b200.so")
+
+SIPG_OK = 0
+SIPG_NOT_CONVERGED = 1
+SIPG_BREAKDOWN = 2
+SIPG_INVALID_ARG = 3
+SIPG_OUT_OF_MEMORY = 4
+SIPG_CANCELLED = 5
+SIPG_CUDA_ERROR = 6
+SIPG_NO_DEVICE = 7
+
+MM_NONE, MM_SCALAR, MM_NODAL = 0, 1, 2
+BC_DIRICHLET, BC_NEUMANN, BC_SLIP = 0, 1, 2
+FP64, FP32 = 64, 32
+SOLVER_CG, SOLVER_INV_MASS, SOLVER_JACOBI, SOLVER_BLOCK_JACOBI, SOLVER_PMULTIGRID = 0, 1, 2, 3, 4
+
+_lib = None
+
+
+class SipgError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"sipg status {status}: {msg}")
+        self.status = status
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [("iters", C.c_int), ("rel_res", C.c_double), ("abs_res", C.c_double),
+                ("true_rel_res", C.c_double), ("setup_ms", C.c_double), ("solve_ms", C.c_double),
+                ("status", C.c_int)]
+
+
+class SolverOpts(C.Structure):
+    _fields_ = [("rel_tol", C.c_double), ("abs_tol", C.c_double), ("max_iter", C.c_int),
+                ("nullspace", C.c_int), ("precision", C.c_int), ("inv_mass_factor", C.c_double),
+                ("ref_volume_block", C.c_int), ("n_levels", C.c_int), ("orders", C.c_int * 4),
+                ("cheb_order", C.c_int), ("eig_safety", C.c_double), ("eig_ratio", C.c_double),
+                ("eig_iters", C.c_int), ("coarse_iters", C.c_int), ("check_every", C.c_int)]
+
+
+def lib():
+    """Load the native library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C ins-solver_b200`")
+        _lib = C.CDLL(LIB_PATH)
+        _lib.sipg_last_error.restype = C.c_char_p
+    return _lib
+
+
+def check(st):
+    if st != SIPG_OK:
+        raise SipgError(st, lib().sipg_last_error().decode())
+    return st
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
+
+
+def _ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int)) if a is not None else None
+
+
+def device_count():
+    n = C.c_int(0)
+    check(lib().sipg_device_count(C.byref(n)))
+    return n.value
+
+
+def ref_sizes(dim, order):
+    Np, Nfp, Nf, Nperm = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    check(lib().sipg_ref_sizes(dim, order, C.byref(Np), C.byref(Nfp), C.byref(Nf), C.byref(Nperm)))
+    return Np.value, Nfp.value, Nf.value, Nperm.value
+
+
+def ref_tables(dim, order):
+    """Reference element tables (row-major numpy arrays)."""
+    Np, Nfp, Nf, Nperm = ref_sizes(dim, order)
+    t = {k: np.zeros(Np) for k in ("r", "s", "t")}
+    for k in ("Dr", "Ds", "Dt", "M"):
+        t[k] = np.zeros((Np, Np))
+    t["MMF"] = np.zeros((Nf, Np, Np))
+    t["EMAT"] = np.zeros((Np, Nf * Nfp))
+    t["fmask"] = np.zeros((Nf, Nfp), dtype=np.int32)
+    t["perm_pos"] = np.zeros((Nperm, Nfp), dtype=np.int32)
+    check(lib().sipg_ref_tables(dim, order, _dp(t["r"]), _dp(t["s"]), _dp(t["t"]), _dp(t["Dr"]),
+                                _dp(t["Ds"]), _dp(t["Dt"]), _dp(t["M"]), _dp(t["MMF"]),
+                                _dp(t["EMAT"]), _ip(t["fmask"]), _ip(t["perm_pos"])))
+    t.update(Np=Np, Nfp=Nfp, Nf=Nf, dim=dim, order=order)
+    return t
+
+
+def interp_matrix(dim, q, p):
+    Npp = ref_sizes(dim, p)[0]
+    Npq = ref_sizes(dim, q)[0]
+    P = np.zeros((Npp, Npq))
+    check(lib().sipg_interp_matrix(dim, q, p, _dp(P)))
+    return P
+
+
+def box_mesh(dim, n, jitter=0.0, seed=0):
+    Nv, K = C.c_int(), C.c_int()
+    check(lib().sipg_box_mesh_sizes(dim, n, C.byref(Nv), C.byref(K)))
+    vx = np.zeros((Nv.value, dim))
+    e2v = np.zeros((K.value, dim + 1), dtype=np.int32)
+    check(lib().sipg_box_mesh(dim, n, C.c_double(jitter), C.c_uint64(seed), _dp(vx), _ip(e2v)))
+    return vx, e2v
+
+
+class Mesh:
+    """Resident mesh (DGMesh3D / DGMesh2D stand-in)."""
+
+    def __init__(self, dim, vx, e2v):
+        self.dim = dim
+        vx = np.ascontiguousarray(vx, dtype=np.float64)
+        e2v = np.ascontiguousarray(e2v, dtype=np.int32)
+        self.h = C.c_void_p()
+        check(lib().sipg_mesh_create(dim, vx.shape[0], _dp(vx), e2v.shape[0], _ip(e2v), C.byref(self.h)))
+        K, F, Kb = C.c_int(), C.c_int(), C.c_int()
+        check(lib().sipg_mesh_sizes(self.h, C.byref(K), C.byref(F), C.byref(Kb)))
+        self.K, self.F, self.Kb = K.value, F.value, Kb.value
+
+    @classmethod
+    def box(cls, dim, n, jitter=0.0, seed=0):
+        vx, e2v = box_mesh(dim, n, jitter, seed)
+        return cls(dim, vx, e2v)
+
+    def export(self, order):
+        """Per-order host data in the reference's form (dict of numpy arrays)."""
+        Np, Nfp, Nf, _ = ref_sizes(self.dim, order)
+        K, F, Kb, dim = self.K, self.F, self.Kb, self.dim
+        d = dict(geof=np.zeros((K, 10 if dim == 3 else 5)))
+        for k in ("nx", "ny", "nz", "sJ", "fscale"):
+            d[k] = np.zeros((K, Nf))
+        d["face2cells"] = np.zeros((F, 2), np.int32)
+        d["faceNum"] = np.zeros((F, 2), np.int32)
+        d["fmaskL"] = np.zeros((F, Nfp), np.int32)
+        d["fmaskR"] = np.zeros((F, Nfp), np.int32)
+        d["bface2cell"] = np.zeros(Kb, np.int32)
+        d["bfaceNum"] = np.zeros(Kb, np.int32)
+        d["bface_centroid"] = np.zeros((Kb, dim))
+        for k in ("x", "y", "z"):
+            d[k] = np.zeros((K, Np))
+        check(lib().sipg_mesh_export(self.h, order, _dp(d["geof"]), _dp(d["nx"]), _dp(d["ny"]),
+                                     _dp(d["nz"]), _dp(d["sJ"]), _dp(d["fscale"]),
+                                     _ip(d["face2cells"]), _ip(d["faceNum"]), _ip(d["fmaskL"]),
+                                     _ip(d["fmaskR"]), _ip(d["bface2cell"]), _ip(d["bfaceNum"]),
+                                     _dp(d["bface_centroid"]), _dp(d["x"]), _dp(d["y"]), _dp(d["z"])))
+        d.update(K=K, F=F, Kb=Kb, Np=Np, Nfp=Nfp, Nf=Nf, dim=dim, order=order)
+        return d
+
+    def device_bytes(self):
+        b = C.c_size_t()
+        check(lib().sipg_mesh_device_bytes(self.h, C.byref(b)))
+        return b.value
+
+    def __del__(self):
+        if getattr(self, "h", None) and self.h:
+            lib().sipg_mesh_destroy(self.h)
+            self.h = None
+
+
+class Operator:
+    """SIPG operator on a resident mesh (Poisson / Helmholtz / viscous)."""
+
+    def __init__(self, mesh, order, ncomp=1):
+        self.mesh = mesh
+        self.order = order
+        self.ncomp = ncomp
+        self.h = C.c_void_p()
+        check(lib().sipg_op_create(mesh.h, order, ncomp, C.byref(self.h)))
+        self.Np, self.Nfp = ref_sizes(mesh.dim, order)[:2]
+        self.K = mesh.K
+
+    def shape(self):
+        return (self.ncomp, self.K, self.Np)
+
+    def set_factor(self, factor):
+        f = None if factor is None else np.ascontiguousarray(factor, dtype=np.float64)
+        check(lib().sipg_op_set_factor(self.h, _dp(f)))
+
+    def set_mm(self, mode, scalar=0.0, mm=None):
+        m = None if mm is None else np.ascontiguousarray(mm, dtype=np.float64)
+        check(lib().sipg_op_set_mm(self.h, mode, C.c_double(scalar), _dp(m)))
+
+    def set_bc_types(self, types):
+        t = np.ascontiguousarray(types, dtype=np.int32).reshape(-1)
+        check(lib().sipg_op_set_bc_types(self.h, _ip(t)))
+
+    def set_pin(self, elem, node=0):
+        check(lib().sipg_op_set_pin(self.h, elem, node))
+
+    def apply_host(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros_like(x)
+        check(lib().sipg_op_apply_host(self.h, _dp(x), _dp(y)))
+        return y
+
+    def apply_device(self, precision, x_ptr, y_ptr, stream=None):
+        check(lib().sipg_op_apply(self.h, precision, C.c_void_p(x_ptr), C.c_void_p(y_ptr),
+                                  C.c_void_p(stream or 0)))
+
+    def apply_bc_host(self, bc, rhs):
+        bc = np.ascontiguousarray(bc, dtype=np.float64)
+        out = np.ascontiguousarray(rhs, dtype=np.float64).copy()
+        check(lib().sipg_op_apply_bc_host(self.h, _dp(bc), _dp(out)))
+        return out
+
+    def diag_host(self):
+        d = np.zeros(self.shape())
+        check(lib().sipg_op_diag_host(self.h, _dp(d)))
+        return d
+
+    def block_diag_host(self, invert=False, ref_volume_block=False):
+        b = np.zeros(self.shape() + (self.Np,))
+        check(lib().sipg_op_block_diag_host(self.h, int(invert), int(ref_volume_block), _dp(b)))
+        return b
+
+    def __del__(self):
+        if getattr(self, "h", None) and self.h:
+            lib().sipg_op_destroy(self.h)
+            self.h = None
+
+
+def default_opts(kind):
+    o = SolverOpts()
+    check(lib().sipg_solver_default_opts(kind, C.byref(o)))
+    return o
+
+
+class Solver:
+    """Linear solver (LinearSolver / ViscousSolver3D stand-in)."""
+
+    def __init__(self, op, kind, opts=None):
+        self.op = op
+        self.kind = kind
+        self.opts = opts if opts is not None else default_opts(kind)
+        self.h = C.c_void_p()
+        check(lib().sipg_solver_create(op.h, kind, C.byref(self.opts), C.byref(self.h)))
+
+    def setup(self):
+        check(lib().sipg_solver_setup(self.h))
+
+    def solve_host(self, b, x0=None):
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros_like(b) if x0 is None else np.ascontiguousarray(x0, dtype=np.float64).copy()
+        info = SolveInfo()
+        st = lib().sipg_solver_solve_host(self.h, _dp(b), _dp(x), C.byref(info))
+        if st not in (SIPG_OK, SIPG_NOT_CONVERGED, SIPG_BREAKDOWN):
+            check(st)
+        return x, info
+
+    def solve_device(self, b_ptr, x_ptr):
+        info = SolveInfo()
+        st = lib().sipg_solver_solve(self.h, C.c_void_p(b_ptr), C.c_void_p(x_ptr), C.byref(info))
+        if st not in (SIPG_OK, SIPG_NOT_CONVERGED, SIPG_BREAKDOWN):
+            check(st)
+        return info
+
+    def __del__(self):
+        if getattr(self, "h", None) and self.h:
+            lib().sipg_solver_destroy(self.h)
+            self.h = None

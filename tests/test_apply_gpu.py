@@ -1,0 +1,100 @@
+"""CUDA SIPG apply, diagonals, blocks and boundary lifting against the oracle
+and the reference-kernel golden vectors."""
+import numpy as np
+import pytest
+
+import oracle_py as O
+import sipg
+from helpers import (GOLDEN, TOL_FP32, TOL_FP64, DevArray, golden_setup, load_golden, make_op,
+                     random_case, rel_err)
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=lambda p: p.split("/")[-1][:-4])
+def test_apply_fp64_matches_reference_golden(path):
+    g = load_golden(path)
+    mesh, t, e, om = golden_setup(g)
+    op = make_op(mesh, g["order"], g["ncomp"], g.get("factor"), g.get("mm"), bct=g["bct"])
+    y = op.apply_host(g["x"])
+    assert rel_err(y, g["y"]) < TOL_FP64
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=lambda p: p.split("/")[-1][:-4])
+def test_apply_fp32_within_tolerance(path):
+    g = load_golden(path)
+    mesh, t, e, om = golden_setup(g)
+    op = make_op(mesh, g["order"], g["ncomp"], g.get("factor"), g.get("mm"), bct=g["bct"])
+    x = DevArray(g["x"].astype(np.float32))
+    y = DevArray(np.zeros_like(g["x"], dtype=np.float32))
+    op.apply_device(sipg.FP32, x.p, y.p)
+    assert rel_err(y.get().astype(np.float64), g["y"]) < TOL_FP32
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=lambda p: p.split("/")[-1][:-4])
+def test_diag_blocks_and_lift_match_reference_golden(path):
+    g = load_golden(path)
+    mesh, t, e, om = golden_setup(g)
+    op = make_op(mesh, g["order"], g["ncomp"], g.get("factor"), g.get("mm"), bct=g["bct"])
+    assert rel_err(op.diag_host(), g["diag"]) < TOL_FP64
+    blk = op.block_diag_host(invert=False, ref_volume_block=True)
+    assert rel_err(blk[0], g["blocks0"]) < TOL_FP64
+    rhs = op.apply_bc_host(g["bc"], np.zeros_like(g["x"]))
+    assert rel_err(rhs, g["rhs"]) < TOL_FP64
+
+
+@pytest.mark.parametrize("dim,n", [(2, 7), (3, 3)])
+@pytest.mark.parametrize("order", [1, 2, 3, 4])
+@pytest.mark.parametrize("variant", ["poisson", "factor", "helmholtz", "vector_slip"])
+def test_apply_random_cases_vs_oracle(dim, n, order, variant):
+    ncomp = dim if variant == "vector_slip" else 1
+    mesh, t, e, om, x, f, m, bct = random_case(dim, n, order, ncomp, seed=31 * order + dim,
+                                               slip=variant == "vector_slip",
+                                               factor=variant in ("factor", "vector_slip"),
+                                               mm=variant == "helmholtz")
+    op = make_op(mesh, order, ncomp, f, m, bct=bct)
+    y_ref = O.mult(om, x, bct, f, m)
+    assert rel_err(op.apply_host(x), y_ref) < TOL_FP64
+    blocks = op.block_diag_host(invert=True)
+    exact = O.block_diag(om, ncomp, bct, f, m, inv=True)
+    assert rel_err(blocks, exact) < 1e-11
+
+
+def test_apply_alpha_beta_epilogue_and_pinned_dof():
+    mesh, t, e, om, x, f, m, bct = random_case(3, 3, 3, 1, seed=9)
+    op = make_op(mesh, 3, 1, f, bct=bct)
+    op.set_pin(0, 0)
+    xd = DevArray(x)
+    y0 = np.random.default_rng(1).uniform(-1, 1, x.shape)
+    yd = DevArray(y0)
+    lib = sipg.lib()
+    # y = -A x + y0 through the internal epilogue is exercised by the solvers;
+    # here the public apply (alpha=1, beta=0) on a pinned operator:
+    op.apply_device(sipg.FP64, xd.p, yd.p)
+    y = yd.get()
+    xs = x.copy()
+    xs[0, 0, 0] = 0.0
+    ref = O.mult(om, xs, bct, f)
+    d = O.diag(om, 1, bct, f)
+    ref[0, 0, 0] = d[0, 0, 0] * x[0, 0, 0]
+    assert rel_err(y, ref) < TOL_FP64
+    assert lib is not None
+
+
+def test_apply_is_symmetric_and_spd_with_dirichlet():
+    mesh, t, e, om, x, f, m, bct = random_case(3, 2, 3, 1, seed=4)
+    bct[:] = 0
+    op = make_op(mesh, 3, 1, f, bct=bct)
+    rng = np.random.default_rng(3)
+    u, v = rng.uniform(-1, 1, x.shape), rng.uniform(-1, 1, x.shape)
+    Au, Av = op.apply_host(u), op.apply_host(v)
+    assert abs((v * Au).sum() - (u * Av).sum()) < 1e-12 * np.abs(v * Au).sum()
+    assert (u * Au).sum() > 0
+
+
+def test_neumann_operator_annihilates_constants():
+    mesh, t, e, om, x, f, m, bct = random_case(3, 3, 2, 1, seed=8)
+    bct[:] = 1
+    op = make_op(mesh, 2, 1, f, bct=bct)
+    y = op.apply_host(np.ones_like(x))
+    assert np.abs(y).max() < 1e-11

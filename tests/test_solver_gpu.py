@@ -1,0 +1,130 @@
+"""CUDA solvers against the oracle: CG / Jacobi / block-Jacobi / inverse-mass
+PCG (reference golden counts), p-multigrid FP64 and mixed precision."""
+import numpy as np
+import pytest
+
+import oracle_py as O
+import sipg
+import workloads as W
+from helpers import GOLDEN, golden_setup, load_golden, make_op, rel_err
+
+pytestmark = pytest.mark.gpu
+
+KIND = {"cg": sipg.SOLVER_CG, "jacobi": sipg.SOLVER_JACOBI, "bjacobi": sipg.SOLVER_BLOCK_JACOBI,
+        "invmass": sipg.SOLVER_INV_MASS}
+
+
+@pytest.mark.parametrize("path", [p for p in GOLDEN if "slip" not in p], ids=lambda p: p.split("/")[-1][:-4])
+@pytest.mark.parametrize("name", ["cg", "jacobi", "invmass", "bjacobi"])
+def test_krylov_matches_reference_golden(path, name):
+    g = load_golden(path)
+    mesh, t, e, om = golden_setup(g)
+    ref_iters = int(g[f"solve_{name}_iters"])
+    if name == "bjacobi" and ref_iters > 500:
+        pytest.skip("reference block-Jacobi stagnates with its 3D volume block")
+    bd = np.zeros_like(g["bct"])
+    op = make_op(mesh, g["order"], 1, g.get("factor"), g.get("mm"), mm_scalar=1.0, bct=bd)
+    if g.get("mm") is None:
+        op.set_mm(sipg.MM_SCALAR, 1.0)
+    o = sipg.default_opts(KIND[name])
+    o.abs_tol, o.rel_tol, o.max_iter, o.ref_volume_block = 1e-10, 0.0, 2000, 1
+    s = sipg.Solver(op, KIND[name], o)
+    x, info = s.solve_host(g["solve_b"])
+    assert abs(info.iters - ref_iters) <= 1
+    assert rel_err(x, g[f"solve_{name}_x"]) < 1e-8
+
+
+def _pmg_oracle_levels(mesh, orders, factor, bct):
+    meshes, facs, prol = [], [], []
+    for l, p in enumerate(orders):
+        t = sipg.ref_tables(3, p)
+        meshes.append(O.OMesh(t, mesh.export(p)))
+        I = sipg.interp_matrix(3, orders[0], p)
+        facs.append(factor @ I.T)
+        if l + 1 < len(orders):
+            prol.append(sipg.interp_matrix(3, orders[l + 1], p))
+    return dict(orders=orders, meshes=meshes, factors=facs, prolong=prol, cheb_order=4,
+                eig_safety=1.1, eig_ratio=30.0, eig_iters=20, coarse_iters=20)
+
+
+@pytest.fixture(scope="module")
+def two_phase():
+    return W.poisson3d_two_phase(4, order=3, n_modes=64)
+
+
+def _pmg_solver(case, precision):
+    op = make_op(case["mesh"], 3, 1, case["factor"], bct=case["bc_types"])
+    op.set_pin(*case["pin"])
+    o = sipg.default_opts(sipg.SOLVER_PMULTIGRID)
+    o.rel_tol, o.abs_tol, o.max_iter, o.precision = 1e-8, 0.0, 200, precision
+    return op, sipg.Solver(op, sipg.SOLVER_PMULTIGRID, o)
+
+
+def test_pmultigrid_fp64_matches_oracle(two_phase):
+    c = two_phase
+    om = O.OMesh(c["tables"], c["export"])
+    pmg = _pmg_oracle_levels(c["mesh"], [3, 2, 1], c["factor"], c["bc_types"])
+    xo, io = O.solve(om, c["rhs"], c["bc_types"], O.PRE_PMG, c["factor"], abs_tol=0.0, rel_tol=1e-8,
+                     max_iter=200, pin_dof=0, pmg=pmg)
+    assert io.converged
+    op, s = _pmg_solver(c, sipg.FP64)
+    x, info = s.solve_host(c["rhs"])
+    assert info.status == sipg.SIPG_OK
+    assert abs(info.iters - io.iters) <= 1
+    assert rel_err(x, xo) < 1e-9
+    assert info.true_rel_res < 1e-8
+
+
+def test_pmultigrid_mixed_precision_reaches_fp64_tolerance(two_phase):
+    c = two_phase
+    _, s64 = _pmg_solver(c, sipg.FP64)
+    x64, i64 = s64.solve_host(c["rhs"])
+    _, s32 = _pmg_solver(c, sipg.FP32)
+    x32, i32 = s32.solve_host(c["rhs"])
+    assert i32.status == sipg.SIPG_OK
+    assert abs(i32.iters - i64.iters) <= 1
+    assert i32.true_rel_res <= 1e-8
+    assert rel_err(x32, x64) < 1e-6
+
+
+def test_poisson2d_manufactured_solution_converges():
+    errs = []
+    for n in (8, 16, 32):
+        c = W.poisson2d_manufactured(n, order=3)
+        op = make_op(c["mesh"], 3, 1, bct=c["bc_types"])
+        o = sipg.default_opts(sipg.SOLVER_BLOCK_JACOBI)
+        o.rel_tol, o.abs_tol, o.max_iter = 1e-10, 0.0, 5000
+        x, info = sipg.Solver(op, sipg.SOLVER_BLOCK_JACOBI, o).solve_host(c["rhs"])
+        assert info.status == sipg.SIPG_OK
+        errs.append(np.abs(x - c["exact"]).max())
+    rates = np.log2(np.array(errs[:-1]) / np.array(errs[1:]))
+    assert rates.min() > 3.0, (errs, rates)
+
+
+def test_nullspace_projection_solves_pure_neumann(two_phase):
+    c = two_phase
+    op = make_op(c["mesh"], 3, 1, c["factor"], bct=c["bc_types"])
+    o = sipg.default_opts(sipg.SOLVER_JACOBI)
+    o.rel_tol, o.abs_tol, o.max_iter, o.nullspace = 1e-8, 0.0, 3000, 1
+    b = c["rhs"].copy()
+    b -= b.mean()
+    x, info = sipg.Solver(op, sipg.SOLVER_JACOBI, o).solve_host(b)
+    assert info.status == sipg.SIPG_OK
+    assert info.true_rel_res < 1e-7
+
+
+def test_not_converged_and_invalid_arguments_report_status(two_phase):
+    c = two_phase
+    op = make_op(c["mesh"], 3, 1, c["factor"], bct=c["bc_types"])
+    op.set_pin(*c["pin"])
+    o = sipg.default_opts(sipg.SOLVER_JACOBI)
+    o.max_iter = 2
+    x, info = sipg.Solver(op, sipg.SOLVER_JACOBI, o).solve_host(c["rhs"])
+    assert info.status == sipg.SIPG_NOT_CONVERGED and info.iters == 2
+    with pytest.raises(sipg.SipgError) as ei:
+        sipg.Operator(c["mesh"], 5, 1)
+    assert ei.value.status == sipg.SIPG_INVALID_ARG
+    b = c["rhs"].copy()
+    b[0, 5, 3] = np.nan
+    x, info = sipg.Solver(op, sipg.SOLVER_JACOBI, o).solve_host(b)
+    assert info.status == sipg.SIPG_BREAKDOWN
