@@ -1,0 +1,367 @@
+#!/usr/bin/env python3
+"""Benchmark of the SIPG pressure-solve hot path on B200.
+
+Headline workload (one "step" = one Poisson solve):
+  3D variable-density Poisson, unit cube 24^3 hexes x 6 tets = 82,944 elements,
+  interior vertices jittered +-0.1h (seed 20261203), p=3 (Np=20), factor 1/rho with
+  rho = 1000 inside a sphere r=0.25 at the centre, 1 outside (tanh over 1.5h), RHS a
+  Gaussian random field (correlation length 0.1) minus its mean, Neumann walls with
+  the constant nullspace projected out (the reference's [pressure-solve]
+  nullspace = 1 path, src/solvers/3d/ins_solver_base.cpp:151-152); p-multigrid 3->2->1 with Chebyshev(4) smoothing, outer flexible CG
+  in FP64 to a 1e-8 relative residual.
+  value   = solves/s of the mixed-precision path (V-cycle in FP32, outer CG FP64),
+            device-timed with CUDA events, inputs resident in HBM;
+  e2e     = the same solve through the public host-buffer entry point
+            (sipg_solver_solve_host: H2D of the RHS and initial guess, D2H of the
+            solution inside the timed region);
+  fp64    = the plain FP64 GPU path (same algorithm, V-cycle in FP64);
+  apply   = SIPG apply GDOF/s of the 3D viscous Helmholtz configuration
+            (48^3 x 6 = 663,552 tets, p=4) in FP64 and FP32;
+  roofline for the dominant kernel (the FP32 p=3 apply of the V-cycle).
+The operator setup (diagonals, eigenvalue estimates, coarse operators) runs once
+before timing; the coefficient does not change between steps and its setup time
+is reported separately.
+
+--impl reference: the reference's own kernels (src/kernels/fvmf_3d_*.h of
+TobyFlynn/INS-Solver, compiled under oracle/_ref with OpenMP on all host cores)
+execute one outer iteration's worth of applies per step on the same mesh; solves/s
+= 1 / (step time x outer iterations of the FP64 path).
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for sub in ("ins-solver_b200", "oracle"):
+    sys.path.insert(0, os.path.join(ROOT, sub))
+
+import sipg  # noqa: E402
+import workloads as W  # noqa: E402
+
+METRIC = "SIPG apply GDOF/s; Poisson solves/s + p50/p99 latency, mixed vs FP64 @1e-8"
+N_HEAD = 24
+ORDER = 3
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device=0):
+        self.device = device
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            for nm, v in zip(names, s[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def launches():
+    n = C.c_ulonglong()
+    sipg.check(sipg.lib().sipg_launch_count(C.byref(n)))
+    return n.value
+
+
+def build_headline():
+    c = W.poisson3d_two_phase(N_HEAD, order=ORDER, n_modes=256, pin=False)
+    op = sipg.Operator(c["mesh"], ORDER, 1)
+    op.set_bc_types(c["bc_types"])
+    op.set_factor(c["factor"])
+    return c, op
+
+
+def pmg_solver(op, precision):
+    o = sipg.default_opts(sipg.SOLVER_PMULTIGRID)
+    o.precision, o.rel_tol, o.abs_tol, o.max_iter = precision, 1e-8, 0.0, 500
+    o.nullspace = 1
+    s = sipg.Solver(op, sipg.SOLVER_PMULTIGRID, o)
+    t0 = time.perf_counter()
+    s.setup()
+    return s, (time.perf_counter() - t0) * 1e3
+
+
+def time_solves(solver, b_dev, x_dev, steps, warmup):
+    """b_dev, x_dev: torch CUDA tensors; x is zeroed before every solve."""
+    import torch
+    for _ in range(warmup):
+        x_dev.zero_()
+        torch.cuda.synchronize()
+        solver.solve_device(b_dev.data_ptr(), x_dev.data_ptr())
+    ms, infos = [], []
+    for _ in range(steps):
+        x_dev.zero_()
+        torch.cuda.synchronize()
+        info = solver.solve_device(b_dev.data_ptr(), x_dev.data_ptr())
+        ms.append(info.solve_ms)
+        infos.append(info)
+    return np.array(ms), infos
+
+
+def time_apply(op, precision, K, Np, iters=30):
+    """Average device duration of the apply kernel, CUDA events on its stream."""
+    import torch
+    dt = torch.float32 if precision == sipg.FP32 else torch.float64
+    x = torch.rand((K * Np,), dtype=dt, device="cuda") * 2 - 1
+    y = torch.empty_like(x)
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            op.apply_device(precision, x.data_ptr(), y.data_ptr(), stream.cuda_stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(iters):
+            op.apply_device(precision, x.data_ptr(), y.data_ptr(), stream.cuda_stream)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / iters
+
+
+def apply_bytes_per_elem(Np, ts, factor, ngeof=10, nf=4):
+    """Algorithmic HBM bytes of one scalar apply per element: read x, write y,
+    factor (if nodal), geometry (geof) and penalty, neighbour ids and codes.
+    Neighbour traces are L2 hits, not HBM."""
+    return ts * (2 * Np + (Np if factor else 0) + ngeof + nf) + 4 * nf + 4
+
+
+def run_ours(args):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
+    c, op = build_headline()
+    K, Np = c["mesh"].K, op.Np
+    n = K * Np
+    b = c["rhs"].reshape(-1)
+    bd = torch.from_numpy(b).cuda()
+    xd = torch.zeros_like(bd)
+    s32, setup32 = pmg_solver(op, sipg.FP32)
+    s64, setup64 = pmg_solver(op, sipg.FP64)
+    # plain FP64 path (fewer steps; it is the slow one)
+    ms64, inf64 = time_solves(s64, bd, xd, max(1, min(3, args.steps)), 1)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    l0 = launches()
+    with ClockSampler(local) as clk:
+        ms32, inf32 = time_solves(s32, bd, xd, args.steps, args.warmup)
+    l1 = launches()
+    n_launch = (l1 - l0) * args.steps // (args.steps + args.warmup)
+    step_ms = float(np.mean(ms32))
+    total_ms = float(np.sum(ms32))
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * args.steps / (total_ms / 1e3)
+    # end to end through the host-buffer entry point
+    e2e_t = []
+    xh = np.zeros_like(c["rhs"])
+    for _ in range(max(2, min(args.steps, 5))):
+        t0 = time.perf_counter()
+        xs, info = s32.solve_host(c["rhs"], xh)
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_val = world / float(np.mean(e2e_t))
+    # dominant kernel: FP32 p=3 apply of the V-cycle (and the FP64 outer apply)
+    a32 = time_apply(op, sipg.FP32, K, Np)
+    a64 = time_apply(op, sipg.FP64, K, Np)
+    hbm, peak_kind = peaks()
+    bpe = apply_bytes_per_elem(Np, 4, True)
+    achieved = bpe * K / (a32 * 1e-3) / 1e9
+    # C3 apply throughput (p=4 Helmholtz, 663,552 tets)
+    apply_c3 = {}
+    if not args.skip_c3:
+        h = W.helmholtz3d(48, order=4)
+        op4 = sipg.Operator(h["mesh"], 4, 1)
+        op4.set_bc_types(h["bc_types"])
+        op4.set_mm(sipg.MM_SCALAR, h["mm"])
+        K4, Np4 = h["mesh"].K, op4.Np
+        t64 = time_apply(op4, sipg.FP64, K4, Np4, 20)
+        t32 = time_apply(op4, sipg.FP32, K4, Np4, 20)
+        b4 = apply_bytes_per_elem(Np4, 4, False)
+        apply_c3 = {"workload": "3D Helmholtz I/(nu dt) - Lap, 48^3x6=663552 tets, p=4",
+                    "fp64_gdofs": K4 * Np4 / (t64 * 1e-3) / 1e9, "fp32_gdofs": K4 * Np4 / (t32 * 1e-3) / 1e9,
+                    "fp64_ms": t64, "fp32_ms": t32,
+                    "fp32_hbm_frac": b4 * K4 / (t32 * 1e-3) / 1e9 / hbm}
+    lat = np.array(ms32)
+    out = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "solves/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": step_ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "fp32 V-cycle / fp64 outer CG",
+        "data": "synthetic (seeded two-phase density and Gaussian random field RHS)",
+        "config": {"workload": "3D two-phase Poisson 24^3x6=82944 tets p=3, Neumann walls + nullspace projection, "
+                               "p-MG 3-2-1 Chebyshev(4), FPCG rel 1e-8",
+                   "K": K, "dofs": n, "parallelism": f"replicas{world}",
+                   "l2_flush": "inputs larger than L2 across a solve (26 MB/vector, ~30 vectors live)"},
+        "iters": int(inf32[-1].iters),
+        "true_rel_res": float(inf32[-1].true_rel_res),
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "fp64_path": {"solves_per_s": 1e3 / float(np.mean(ms64)), "ms_per_solve": float(np.mean(ms64)),
+                      "iters": int(inf64[-1].iters), "true_rel_res": float(inf64[-1].true_rel_res)},
+        "mixed_vs_fp64_speedup": float(np.mean(ms64)) / step_ms,
+        "setup_ms": {"mixed": setup32, "fp64": setup64},
+        "e2e": {"value": e2e_val, "unit": "solves/s", "h2d_bytes_per_step": int(2 * b.nbytes),
+                "d2h_bytes_per_step": int(b.nbytes)},
+        "gpu_launches": int(n_launch),
+        "apply_p3": {"fp32_ms": a32, "fp64_ms": a64, "fp32_gdofs": n / (a32 * 1e-3) / 1e9,
+                     "fp64_gdofs": n / (a64 * 1e-3) / 1e9},
+        "apply_c3": apply_c3,
+        "roofline": {"kernel": "sipg_apply_kernel<float,3,3>", "bound": "hbm", "achieved": achieved,
+                     "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": None, "bytes_per_elem": bpe},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        out["cpu_baseline"] = cpu_reference(c, op, int(inf64[-1].iters), sample_only=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
+def cpu_reference(c, op, outer_iters, sample_only=False, steps=1, warmup=0):
+    """Reference kernels on the host cores: one outer iteration of the p-MG solve =
+    1 FP64 apply at p=3 + 2x4 Chebyshev applies at p=3 and at p=2 + 20 coarse
+    applies at p=1 (the FP64 path's counts), timed with the reference's own
+    kernels (oracle/_ref, OpenMP)."""
+    import oracle_py as O
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    mesh = c["mesh"]
+    counts = {3: 1 + 8, 2: 8, 1: 20}
+    per = {}
+    rng = np.random.default_rng(0)
+    for p, cnt in counts.items():
+        t = sipg.ref_tables(3, p)
+        e = mesh.export(p)
+        om = O.OMesh(t, e)
+        I = sipg.interp_matrix(3, ORDER, p)
+        f = c["factor"] @ I.T
+        x = rng.uniform(-1, 1, (1, mesh.K, t["Np"]))
+        O.mult(om, x, c["bc_types"], f, use_ref=True)  # warm
+        t0 = time.perf_counter()
+        O.mult(om, x, c["bc_types"], f, use_ref=True)
+        per[p] = time.perf_counter() - t0
+    step_s = sum(per[p] * counts[p] for p in counts)
+    return {"value": 1.0 / (step_s * outer_iters), "unit": "solves/s", "cores": cores, "kind": "reference",
+            "sample": (f"one outer p-MG iteration of applies with the reference kernels (oracle/_ref, "
+                       f"OpenMP {cores} threads): per-apply s {{p3: {per[3]:.3f}, p2: {per[2]:.3f}, "
+                       f"p1: {per[1]:.3f}}} x counts {counts} = {step_s:.2f} s, scaled by {outer_iters} "
+                       f"outer iterations; vector updates excluded"),
+            "step_s": step_s}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle_py as O
+    if not O.have_ref():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libsipgref.so was not built"}))
+        return
+    c = W.poisson3d_two_phase(N_HEAD, order=ORDER, n_modes=256, pin=False)
+    outer = 26  # outer iterations of the FP64 p-MG path on this workload (measured on the GPU)
+    step_times = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_reference(c, None, outer)
+        if i >= args.warmup:
+            step_times.append(r["step_s"])
+    step = float(np.mean(step_times))
+    val = 1.0 / (step * outer)
+    out = {"metric": METRIC, "value": val, "unit": "solves/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": step * 1e3, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "fp64", "data": "synthetic",
+           "config": {"workload": "3D two-phase Poisson 24^3x6=82944 tets p=3, Neumann walls + nullspace projection, "
+                                  "p-MG 3-2-1 Chebyshev(4), FPCG rel 1e-8"},
+           "impl": "reference",
+           "cpu_baseline": {"value": val, "unit": "solves/s", "cores": r["cores"], "kind": "reference",
+                            "sample": r["sample"]},
+           "e2e": {"value": val, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--skip-c3", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

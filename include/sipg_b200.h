@@ -35,6 +35,7 @@ typedef struct sipg_mesh sipg_mesh;
 typedef struct sipg_op sipg_op;
 typedef struct sipg_solver sipg_solver;
 typedef struct sipg_server sipg_server;
+typedef struct sipg_amg sipg_amg;
 
 const char *sipg_last_error(void);
 int sipg_version(void);
@@ -151,8 +152,12 @@ typedef struct {
   double eig_safety;         /* eigen_val_saftey_factor */
   double eig_ratio;          /* lambda_min = lambda_max * safety / eig_ratio */
   int eig_iters;
-  int coarse_iters;          /* Jacobi-PCG iterations on the coarsest order */
+  int coarse_iters;          /* Jacobi-PCG iterations on the coarsest order (coarse_kind 0) */
   int check_every;           /* host convergence check period (iterations) */
+  int coarse_kind;           /* 0: Jacobi-PCG on the lowest order; 1: algebraic multigrid on the
+                                continuous piecewise-linear space (coarse_solver = petsc/amg) */
+  int amg_coarse_max;        /* unknowns of the densely inverted coarsest level */
+  double amg_strength;       /* aggregation strength threshold */
 } sipg_solver_opts;
 
 int sipg_solver_default_opts(int kind, sipg_solver_opts *o);
@@ -165,6 +170,32 @@ int sipg_solver_solve(sipg_solver *s, const double *b, double *x, sipg_solve_inf
 /* Same with host buffers, copies inside the call (end-to-end path). */
 int sipg_solver_solve_host(sipg_solver *s, const double *b, double *x, sipg_solve_info *info);
 void sipg_solver_destroy(sipg_solver *s);
+
+/* ---- algebraic coarse hierarchy below p=0: the B200 stand-in for the PETSc
+ * algebraic multigrid the reference uses as its p-multigrid coarse solver
+ * (coarse_solver = petsc, [petsc-amg], examples/3d/oscillating_droplet/config.ini:24-31,52-64).
+ * Host-side build from the p=0 Galerkin operator (graph Laplacian with face
+ * weights sJ*tau); the solver builds and uploads it itself, these entry points
+ * expose it for inspection. sJ, tau, nbr: K x Nf; bc_dirichlet: Kb flags. */
+int sipg_amg_build(int K, int Nf, const double *sJ, const double *tau, const int *nbr, int Kb,
+                   const int *bc_dirichlet, int coarse_max, double strength, int singular,
+                   sipg_amg **out);
+/* Continuous piecewise-linear coarse space (the default of the p-multigrid):
+ * Galerkin operator of the p=1 SIPG operator restricted to continuous functions
+ * (volume and Dirichlet-boundary terms), host-side from the mesh; factor1 and
+ * tau1 are the p=1 level's nodal factor (K x (dim+1), NULL = 1) and penalty
+ * (K x (dim+1)); mm1: nodal mass factor or NULL. */
+int sipg_amg_build_p1(sipg_mesh *m, const double *factor1, const double *tau1, const int *bc_dirichlet,
+                      int mm_mode, double mm_scalar, const double *mm1, int coarse_max, double strength,
+                      int singular, sipg_amg **out);
+int sipg_amg_sizes(const sipg_amg *a, int *nlevels, int *coarse_n);
+/* which: 0 operator A, 1 prolongation P (to level+1's unknowns), 2 restriction R = P^T;
+ * level -1 is the transfer between the p=1 DG unknowns and level 0 (P, R only).
+ * Call with NULL arrays to get rows/cols/nnz, then with arrays of those sizes. */
+int sipg_amg_level(const sipg_amg *a, int level, int which, int *rows, int *cols, int *nnz, int *ptr,
+                   int *idx, double *val);
+int sipg_amg_coarse_inverse(const sipg_amg *a, double *inv);
+void sipg_amg_destroy(sipg_amg *a);
 
 /* Number of kernels this library has launched so far in the process
  * (diagnostics for benchmarks; no reference counterpart). */

@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "../../include/sipg_b200.h"
+#include "amg.hpp"
 #include "capi_util.hpp"
 #include "runtime.hpp"
 #include "sipg_blocks.cuh"
@@ -80,6 +81,44 @@ __global__ void k_mul(double* v, const double* w, size_t n) {
     v[i] *= w[i];
 }
 
+struct DevCsr {
+  int rows = 0, cols = 0;
+  DevBuf ptr, idx, v64, v32;
+  void upload(const Csr& c) {
+    rows = c.rows;
+    cols = c.cols;
+    ptr = DevBuf((c.ptr.size()) * sizeof(int));
+    ptr.upload(c.ptr.data(), c.ptr.size() * sizeof(int));
+    size_t nz = std::max<size_t>(1, c.nnz());
+    idx = DevBuf(nz * sizeof(int));
+    v64 = DevBuf(nz * sizeof(double));
+    v32 = DevBuf(nz * sizeof(float));
+    if (c.nnz()) {
+      idx.upload(c.idx.data(), c.nnz() * sizeof(int));
+      v64.upload(c.val.data(), c.nnz() * sizeof(double));
+      std::vector<float> f(c.val.begin(), c.val.end());
+      v32.upload(f.data(), f.size() * sizeof(float));
+    }
+  }
+  template <typename T>
+  void mv(const T* x, T* y, T alpha, T beta, cudaStream_t s) const {
+    const T* v = std::is_same<T, float>::value ? (const T*)v32.p : (const T*)v64.p;
+    csr_spmv<T>(rows, ptr.as<int>(), idx.as<int>(), v, x, y, alpha, beta, s);
+  }
+};
+
+struct AmgDevLevel {
+  int n = 0;
+  DevCsr A, P, R;
+  DevBuf dinv64, dinv32;
+  double lmax = 0.0;
+  DevBuf rhs, z, res, d;
+};
+
+// Power iteration on D^-1 A for a host CSR matrix, same start vector and steps as
+// the order levels (splitmix64 seed 0x5eed, U(-1,1)).
+double host_csr_lmax(const Csr& A, const std::vector<double>& dinv, int iters);
+
 int grid_for(size_t n) { return (int)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, 148 * 16)); }
 
 uint64_t smix(uint64_t* s) {
@@ -87,6 +126,30 @@ uint64_t smix(uint64_t* s) {
   z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
   z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
   return z ^ (z >> 31);
+}
+
+double host_csr_lmax(const Csr& A, const std::vector<double>& dinv, int iters) {
+  const size_t n = (size_t)A.rows;
+  std::vector<double> v(n), w(n);
+  uint64_t st = 0x5eedull;
+  for (size_t i = 0; i < n; ++i) v[i] = 2.0 * ((smix(&st) >> 11) * (1.0 / 9007199254740992.0)) - 1.0;
+  double lam = 0.0;
+  for (int it = 0; it < iters; ++it) {
+    double nv = 0.0;
+    for (size_t i = 0; i < n; ++i) nv += v[i] * v[i];
+    nv = std::sqrt(nv);
+    for (size_t i = 0; i < n; ++i) v[i] /= nv;
+    for (size_t i = 0; i < n; ++i) {
+      double s = 0.0;
+      for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) s += A.val[k] * v[A.idx[k]];
+      w[i] = s * dinv[i];
+    }
+    double ww = 0.0;
+    for (size_t i = 0; i < n; ++i) ww += w[i] * w[i];
+    lam = std::sqrt(ww);
+    std::swap(v, w);
+  }
+  return lam;
 }
 
 }  // namespace
@@ -103,6 +166,11 @@ struct sipg_solver {
   PinnedScalars hs;
   DevBuf dinv, blocks, minv;
   std::vector<Level> lv;
+  std::vector<AmgDevLevel> al;
+  DevCsr Pdg, Rdg;
+  DevBuf cinv64, cinv32;
+  int cinv_n = 0;
+  bool use_amg = false;
   bool dirty = true;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
@@ -130,6 +198,10 @@ struct sipg_solver {
   template <typename T> void vcycle(int l);
   template <typename T> void chebyshev(Level& L, bool want_res);
   template <typename T> void coarse(Level& L);
+  template <typename T> void amg_vcycle(int l);
+  template <typename T> void last_level_amg(Level& L);
+  template <typename T> void csr_chebyshev(AmgDevLevel& A, bool want_res);
+  void setup_amg();
   void precondition(const double* rin, double* zout);
   int solve(const double* b, double* x, sipg_solve_info* info);
   double power_lmax(sipg_op* lop, const double* dinv64, size_t nl);
@@ -252,6 +324,76 @@ void sipg_solver::setup_pmg() {
     if (f32) to_f32(L.dinv32.as<float>(), L.dinv64.as<double>(), L.n, stream);
     L.lmax = power_lmax(L.op, L.dinv64.as<double>(), L.n);
   }
+  use_amg = o.coarse_kind == 1 && nc == 1 && lv.back().order == 1;
+  if (use_amg) setup_amg();
+}
+
+void sipg_solver::setup_amg() {
+  Level& L = lv.back();
+  sipg_op* lop = L.op;
+  sipg_mesh* m = op->mesh;
+  const int K = m->K, Np1 = L.Np, Nf = m->dim + 1;
+  std::vector<double> tau1((size_t)K * Nf), fac1;
+  SIPG_CUDA(cudaMemcpyAsync(tau1.data(), lop->tau64.p, tau1.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  if (lop->has_factor) {
+    fac1.resize((size_t)K * Np1);
+    SIPG_CUDA(cudaMemcpyAsync(fac1.data(), lop->factor64.p, fac1.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  }
+  std::vector<double> mm1;
+  if (lop->mm_mode == SIPG_MM_NODAL) {
+    mm1.resize((size_t)K * Np1);
+    SIPG_CUDA(cudaMemcpyAsync(mm1.data(), lop->mm64.p, mm1.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  }
+  SIPG_CUDA(cudaStreamSynchronize(stream));
+  const Mesh& h = m->host_order(1);
+  std::vector<uint8_t> bd(m->Kb);
+  bool any_dirichlet = false;
+  for (int b = 0; b < m->Kb; ++b) {
+    bd[b] = op->bct_host[b] == SIPG_BC_DIRICHLET;
+    any_dirichlet |= bd[b] != 0;
+  }
+  Csr A0, Pd;
+  p1c_operator(dev_ref(m->dim, 1).ref, K, m->Nv, h.geof.data(), h.e2v.data(), fac1.empty() ? nullptr : fac1.data(),
+               tau1.data(), h.sJ.data(), h.nx.data(), h.ny.data(), h.nz.data(), h.nbr.data(), bd, lop->mm_mode,
+               lop->mm_scalar, mm1.empty() ? nullptr : mm1.data(), &A0, &Pd);
+  const bool singular = !any_dirichlet && lop->mm_mode == SIPG_MM_NONE;
+  AmgHierarchy H = build_amg(A0, Pd, std::max(2, o.amg_coarse_max), o.amg_strength, singular);
+  const bool f32 = o.precision == SIPG_FP32;
+  const size_t ts = f32 ? sizeof(float) : sizeof(double);
+  Pdg.upload(H.Pdg);
+  Rdg.upload(H.Rdg);
+  al.clear();
+  al.resize(H.levels.size());
+  for (size_t l = 0; l < H.levels.size(); ++l) {
+    AmgDevLevel& D = al[l];
+    const AmgLevel& HL = H.levels[l];
+    D.n = HL.A.rows;
+    D.A.upload(HL.A);
+    if (l + 1 < H.levels.size()) {
+      D.P.upload(HL.P);
+      D.R.upload(HL.R);
+      std::vector<double> dinv(D.n, 0.0);
+      for (int i = 0; i < D.n; ++i)
+        for (int k = HL.A.ptr[i]; k < HL.A.ptr[i + 1]; ++k)
+          if (HL.A.idx[k] == i) dinv[i] = 1.0 / HL.A.val[k];
+      D.lmax = host_csr_lmax(HL.A, dinv, o.eig_iters);
+      D.dinv64 = DevBuf(D.n * sizeof(double));
+      D.dinv64.upload(dinv.data(), D.n * sizeof(double));
+      std::vector<float> d32(dinv.begin(), dinv.end());
+      D.dinv32 = DevBuf(D.n * sizeof(float));
+      D.dinv32.upload(d32.data(), D.n * sizeof(float));
+    }
+    D.rhs = DevBuf(D.n * ts);
+    D.z = DevBuf(D.n * ts);
+    D.res = DevBuf(D.n * ts);
+    D.d = DevBuf(D.n * ts);
+  }
+  cinv_n = H.coarse_n;
+  cinv64 = DevBuf(H.coarse_inv.size() * sizeof(double));
+  cinv64.upload(H.coarse_inv.data(), H.coarse_inv.size() * sizeof(double));
+  std::vector<float> c32(H.coarse_inv.begin(), H.coarse_inv.end());
+  cinv32 = DevBuf(c32.size() * sizeof(float));
+  cinv32.upload(c32.data(), c32.size() * sizeof(float));
 }
 
 void sipg_solver::setup() {
@@ -345,11 +487,66 @@ void sipg_solver::coarse(Level& L) {
 }
 
 template <typename T>
+void sipg_solver::csr_chebyshev(AmgDevLevel& A, bool want_res) {
+  const double hi = A.lmax * o.eig_safety, lo = hi / o.eig_ratio;
+  const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
+  double rho_old = 1.0 / sigma;
+  const T* dinv = std::is_same<T, float>::value ? (const T*)A.dinv32.p : (const T*)A.dinv64.p;
+  for (int it = 0; it < o.cheb_order; ++it) {
+    double c1 = 0.0, c2 = 1.0 / theta;
+    if (it > 0) {
+      double rho = 1.0 / (2.0 * sigma - rho_old);
+      c1 = rho * rho_old;
+      c2 = 2.0 * rho / delta;
+      rho_old = rho;
+    }
+    cheb_step<T>(A.d.as<T>(), A.z.as<T>(), A.res.as<T>(), dinv, (T)c1, (T)c2, A.n, stream);
+    if (it < o.cheb_order - 1 || want_res) A.A.mv<T>(A.d.as<T>(), A.res.as<T>(), T(-1), T(1), stream);
+  }
+}
+
+template <typename T>
+void sipg_solver::amg_vcycle(int l) {
+  AmgDevLevel& A = al[l];
+  if (l == (int)al.size() - 1) {
+    const T* inv = std::is_same<T, float>::value ? (const T*)cinv32.p : (const T*)cinv64.p;
+    dense_mv<T>(cinv_n, inv, A.rhs.as<T>(), A.z.as<T>(), stream);
+    return;
+  }
+  AmgDevLevel& Cn = al[l + 1];
+  vzero<T>(A.z.as<T>(), A.n, stream);
+  vcopy<T>(A.res.as<T>(), A.rhs.as<T>(), A.n, stream);
+  csr_chebyshev<T>(A, true);
+  A.R.mv<T>(A.res.as<T>(), Cn.rhs.as<T>(), T(1), T(0), stream);
+  amg_vcycle<T>(l + 1);
+  A.P.mv<T>(Cn.z.as<T>(), A.z.as<T>(), T(1), T(1), stream);
+  vcopy<T>(A.res.as<T>(), A.rhs.as<T>(), A.n, stream);
+  A.A.mv<T>(A.z.as<T>(), A.res.as<T>(), T(-1), T(1), stream);
+  csr_chebyshev<T>(A, false);
+}
+
+// Lowest order with the algebraic coarse space: Chebyshev, R_dg, AMG V-cycle,
+// P_dg, Chebyshev.
+template <typename T>
+void sipg_solver::last_level_amg(Level& L) {
+  vzero<T>(L.z.as<T>(), L.n, stream);
+  vcopy<T>(L.res.as<T>(), L.rhs.as<T>(), L.n, stream);
+  chebyshev<T>(L, true);
+  Rdg.mv<T>(L.res.as<T>(), al[0].rhs.as<T>(), T(1), T(0), stream);
+  amg_vcycle<T>(0);
+  Pdg.mv<T>(al[0].z.as<T>(), L.z.as<T>(), T(1), T(1), stream);
+  vcopy<T>(L.res.as<T>(), L.rhs.as<T>(), L.n, stream);
+  L.op->apply<T>(L.z.as<T>(), L.res.as<T>(), stream, T(-1), T(1));
+  chebyshev<T>(L, false);
+}
+
+template <typename T>
 void sipg_solver::vcycle(int l) {
   Level& L = lv[l];
   const int nl = (int)lv.size();
   if (l == nl - 1) {
-    coarse<T>(L);
+    if (use_amg) last_level_amg<T>(L);
+    else coarse<T>(L);
     return;
   }
   Level& Cl = lv[l + 1];
@@ -521,6 +718,9 @@ int sipg_solver_default_opts(int kind, sipg_solver_opts* o) {
     o->eig_iters = 20;
     o->coarse_iters = 20;
     o->check_every = 1;
+    o->coarse_kind = 1;
+    o->amg_coarse_max = 1000;
+    o->amg_strength = 0.08;
     (void)kind;
   });
 }

@@ -248,6 +248,33 @@ __global__ void k_coarse_update_p(T* p, const T* sv, size_t n, double* scal) {
 
 __global__ void k_shift_scalar(double* scal, int from, int to) { scal[to] = scal[from]; }
 
+template <typename T>
+__global__ void k_csr_spmv(int rows, const int* __restrict__ ptr, const int* __restrict__ idx,
+                           const T* __restrict__ val, const T* __restrict__ x, T* y, T alpha, T beta) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+    T s = T(0);
+    for (int k = ptr[r]; k < ptr[r + 1]; ++k) s += val[k] * x[idx[k]];
+    y[r] = beta != T(0) ? alpha * s + beta * y[r] : alpha * s;
+  }
+}
+
+// One warp per row of a dense matrix.
+template <typename T>
+__global__ void k_dense_mv(int n, const T* __restrict__ M, const T* __restrict__ x, T* y) {
+  const int lane = threadIdx.x & 31;
+  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += (gridDim.x * blockDim.x) >> 5) {
+    double s = 0.0;
+    for (int j = lane; j < n; j += 32) s += (double)M[(size_t)r * n + j] * (double)x[j];
+    s = warp_sum(s);
+    if (lane == 0) y[r] = (T)s;
+  }
+}
+
+template <typename T>
+__global__ void k_vadd(T* y, const T* x, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) y[i] += x[i];
+}
+
 inline int grid_for(size_t n) {
   size_t g = (n + 255) / 256;
   return (int)std::max<size_t>(1, std::min<size_t>(g, 148 * 16));
@@ -362,6 +389,24 @@ void coarse_update_p(T* p, const T* sv, size_t n, double* scal, cudaStream_t s) 
   note_launch();
 }
 
+template <typename T>
+void csr_spmv(int rows, const int* ptr, const int* idx, const T* val, const T* x, T* y, T alpha, T beta,
+              cudaStream_t s) {
+  k_csr_spmv<T><<<grid_for((size_t)rows), 256, 0, s>>>(rows, ptr, idx, val, x, y, alpha, beta);
+  note_launch();
+}
+template <typename T>
+void dense_mv(int n, const T* M, const T* x, T* y, cudaStream_t s) {
+  int blocks = std::max(1, std::min((n * 32 + 255) / 256, 148 * 8));
+  k_dense_mv<T><<<blocks, 256, 0, s>>>(n, M, x, y);
+  note_launch();
+}
+template <typename T>
+void vadd(T* y, const T* x, size_t n, cudaStream_t s) {
+  k_vadd<T><<<grid_for(n), 256, 0, s>>>(y, x, n);
+  note_launch();
+}
+
 #define SIPG_INST(T)                                                                              \
   template void multi_dot<T>(const T* const*, const T* const*, int, size_t, double*, int,         \
                              const RedWork&, cudaStream_t);                                      \
@@ -379,7 +424,10 @@ void coarse_update_p(T* p, const T* sv, size_t n, double* scal, cudaStream_t s) 
   template void prolong_add<T>(T*, const T*, const T*, int, int, int, int, cudaStream_t);        \
   template void coarse_update<T>(T*, T*, T*, const T*, const T*, const T*, size_t, double*,      \
                                  const RedWork&, cudaStream_t);                                  \
-  template void coarse_update_p<T>(T*, const T*, size_t, double*, cudaStream_t);
+  template void coarse_update_p<T>(T*, const T*, size_t, double*, cudaStream_t);                 \
+  template void csr_spmv<T>(int, const int*, const int*, const T*, const T*, T*, T, T, cudaStream_t); \
+  template void dense_mv<T>(int, const T*, const T*, T*, cudaStream_t);                          \
+  template void vadd<T>(T*, const T*, size_t, cudaStream_t);
 
 SIPG_INST(double)
 SIPG_INST(float)

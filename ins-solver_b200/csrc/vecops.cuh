@@ -101,4 +101,15 @@ void coarse_update(T* z, T* r, T* sv, const T* p, const T* Ap, const T* dinv, si
 template <typename T>
 void coarse_update_p(T* p, const T* sv, size_t n, double* scal, cudaStream_t s);
 
+// y = alpha * A x + beta * y for a CSR matrix (beta == 0: y is not read)
+template <typename T>
+void csr_spmv(int rows, const int* ptr, const int* idx, const T* val, const T* x, T* y, T alpha, T beta,
+              cudaStream_t s);
+// y = M x for a dense row-major n x n matrix
+template <typename T>
+void dense_mv(int n, const T* M, const T* x, T* y, cudaStream_t s);
+// y += x
+template <typename T>
+void vadd(T* y, const T* x, size_t n, cudaStream_t s);
+
 }  // namespace sipg

@@ -46,7 +46,8 @@ class SolverOpts(C.Structure):
                 ("nullspace", C.c_int), ("precision", C.c_int), ("inv_mass_factor", C.c_double),
                 ("ref_volume_block", C.c_int), ("n_levels", C.c_int), ("orders", C.c_int * 4),
                 ("cheb_order", C.c_int), ("eig_safety", C.c_double), ("eig_ratio", C.c_double),
-                ("eig_iters", C.c_int), ("coarse_iters", C.c_int), ("check_every", C.c_int)]
+                ("eig_iters", C.c_int), ("coarse_iters", C.c_int), ("check_every", C.c_int),
+                ("coarse_kind", C.c_int), ("amg_coarse_max", C.c_int), ("amg_strength", C.c_double)]
 
 
 def lib():
@@ -232,6 +233,61 @@ class Operator:
     def __del__(self):
         if getattr(self, "h", None) and self.h:
             lib().sipg_op_destroy(self.h)
+            self.h = None
+
+
+class Amg:
+    """Algebraic coarse hierarchy (host build) below the p=1 level."""
+
+    def __init__(self, h):
+        self.h = h
+        nl, cn = C.c_int(), C.c_int()
+        check(lib().sipg_amg_sizes(self.h, C.byref(nl), C.byref(cn)))
+        self.nlevels, self.coarse_n = nl.value, cn.value
+
+    @classmethod
+    def p0(cls, K, Nf, sJ, tau, nbr, bc_dirichlet, coarse_max=1000, strength=0.08, singular=False):
+        """Element-wise constant coarse space (penalty graph Laplacian)."""
+        sJ = np.ascontiguousarray(sJ, dtype=np.float64)
+        tau = np.ascontiguousarray(tau, dtype=np.float64)
+        nbr = np.ascontiguousarray(nbr, dtype=np.int32)
+        bd = np.ascontiguousarray(bc_dirichlet, dtype=np.int32)
+        h = C.c_void_p()
+        check(lib().sipg_amg_build(K, Nf, _dp(sJ), _dp(tau), _ip(nbr), len(bd), _ip(bd), coarse_max,
+                                   C.c_double(strength), int(singular), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def p1(cls, mesh, factor1, tau1, bc_dirichlet, mm_mode=0, mm_scalar=0.0, mm1=None, coarse_max=1000,
+           strength=0.08, singular=False):
+        """Continuous piecewise-linear coarse space (Galerkin of the p=1 operator)."""
+        f = None if factor1 is None else np.ascontiguousarray(factor1, dtype=np.float64)
+        t = np.ascontiguousarray(tau1, dtype=np.float64)
+        bd = np.ascontiguousarray(bc_dirichlet, dtype=np.int32)
+        m = None if mm1 is None else np.ascontiguousarray(mm1, dtype=np.float64)
+        h = C.c_void_p()
+        check(lib().sipg_amg_build_p1(mesh.h, _dp(f), _dp(t), _ip(bd), mm_mode, C.c_double(mm_scalar), _dp(m),
+                                      coarse_max, C.c_double(strength), int(singular), C.byref(h)))
+        return cls(h)
+
+    def csr(self, level, which):
+        """(rows, cols, ptr, idx, val) of A (0), P (1) or R (2) at a level."""
+        r, c, z = C.c_int(), C.c_int(), C.c_int()
+        check(lib().sipg_amg_level(self.h, level, which, C.byref(r), C.byref(c), C.byref(z), None, None, None))
+        ptr = np.zeros(r.value + 1, np.int32)
+        idx = np.zeros(z.value, np.int32)
+        val = np.zeros(z.value)
+        check(lib().sipg_amg_level(self.h, level, which, None, None, None, _ip(ptr), _ip(idx), _dp(val)))
+        return r.value, c.value, ptr, idx, val
+
+    def coarse_inverse(self):
+        inv = np.zeros((self.coarse_n, self.coarse_n))
+        check(lib().sipg_amg_coarse_inverse(self.h, _dp(inv)))
+        return inv
+
+    def __del__(self):
+        if getattr(self, "h", None) and self.h:
+            lib().sipg_amg_destroy(self.h)
             self.h = None
 
 

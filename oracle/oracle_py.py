@@ -36,6 +36,10 @@ class SolveInfo(C.Structure):
                 ("converged", C.c_int)]
 
 
+class OracleCsr(C.Structure):
+    _fields_ = [("rows", C.c_int), ("cols", C.c_int), ("ptr", IP), ("idx", IP), ("val", DP)]
+
+
 class SolverOpts(C.Structure):
     _fields_ = [("ncomp", C.c_int), ("bc_types", IP), ("factor", DP), ("mm_factor", DP),
                 ("mm_scalar", C.c_double), ("flags", C.c_int), ("precond", C.c_int),
@@ -44,7 +48,10 @@ class SolverOpts(C.Structure):
                 ("pmg_nlevels", C.c_int), ("pmg_orders", IP), ("pmg_meshes", C.c_void_p),
                 ("pmg_factors", C.POINTER(DP)), ("pmg_prolong", C.POINTER(DP)),
                 ("cheb_order", C.c_int), ("eig_safety", C.c_double), ("eig_ratio", C.c_double),
-                ("eig_iters", C.c_int), ("coarse_iters", C.c_int)]
+                ("eig_iters", C.c_int), ("coarse_iters", C.c_int), ("coarse_kind", C.c_int),
+                ("amg_nlevels", C.c_int), ("amg_A", C.POINTER(OracleCsr)), ("amg_P", C.POINTER(OracleCsr)),
+                ("amg_R", C.POINTER(OracleCsr)), ("amg_Pdg", C.POINTER(OracleCsr)),
+                ("amg_Rdg", C.POINTER(OracleCsr)), ("amg_coarse_inv", DP), ("amg_coarse_n", C.c_int)]
 
 
 _libs = {}
@@ -215,6 +222,29 @@ def solve(om, b, bc_types, precond=PRE_NONE, factor=None, mm=None, mm_scalar=0.0
         o.eig_ratio = pmg.get("eig_ratio", 30.0)
         o.eig_iters = pmg.get("eig_iters", 20)
         o.coarse_iters = pmg.get("coarse_iters", 20)
+        amg = pmg.get("amg")
+        if amg is not None:
+            nl = amg.nlevels
+            mats = {w: [amg.csr(l, w) for l in range(nl)] for w in (0, 1, 2)}
+            arrs = []
+
+            def mk(t):
+                rows, cols, ptr, idx, val = t
+                arrs.extend([ptr, idx, val])
+                return OracleCsr(rows, cols, _i(ptr), _i(idx), _d(val))
+            A = (OracleCsr * nl)(*[mk(t) for t in mats[0]])
+            P = (OracleCsr * nl)(*[mk(t) for t in mats[1]])
+            R = (OracleCsr * nl)(*[mk(t) for t in mats[2]])
+            inv = np.ascontiguousarray(amg.coarse_inverse())
+            Pdg = (OracleCsr * 1)(mk(amg.csr(-1, 1)))
+            Rdg = (OracleCsr * 1)(mk(amg.csr(-1, 2)))
+            keep += [arrs, A, P, R, inv, Pdg, Rdg]
+            o.amg_Pdg, o.amg_Rdg = Pdg, Rdg
+            o.coarse_kind = 1
+            o.amg_nlevels = nl
+            o.amg_A, o.amg_P, o.amg_R = A, P, R
+            o.amg_coarse_inv = _d(inv)
+            o.amg_coarse_n = amg.coarse_n
     info = SolveInfo()
     if use_ref:
         assert ref_lib().ref_solve(C.byref(om.s), C.byref(o), _d(b), _d(x), C.byref(info)) == 0

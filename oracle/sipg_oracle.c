@@ -644,12 +644,123 @@ static void coarse_cg(const pmg_level *L, int iters, const double *r, double *z)
   free(res); free(p); free(s); free(Ap);
 }
 
+/* ---- algebraic levels below p=0 (element-wise constants) */
+static void csr_mv(const oracle_csr *A, const double *x, double *y) {
+  for (int i = 0; i < A->rows; ++i) {
+    double s = 0.0;
+    for (int k = A->ptr[i]; k < A->ptr[i + 1]; ++k) s += A->val[k] * x[A->idx[k]];
+    y[i] = s;
+  }
+}
+
+typedef struct {
+  double *dinv;
+  double lmax;
+} amg_level;
+
+static double csr_power_lmax(const oracle_csr *A, const double *dinv, int iters) {
+  size_t n = (size_t)A->rows;
+  double *v = (double *)malloc(sizeof(double) * n), *w = (double *)malloc(sizeof(double) * n);
+  uint64_t s = 0x5eedull;
+  for (size_t i = 0; i < n; ++i) v[i] = 2.0 * ((smix(&s) >> 11) * (1.0 / 9007199254740992.0)) - 1.0;
+  double lam = 0.0;
+  for (int it = 0; it < iters; ++it) {
+    double nv = sqrt(dot(v, v, n));
+    for (size_t i = 0; i < n; ++i) v[i] /= nv;
+    csr_mv(A, v, w);
+    for (size_t i = 0; i < n; ++i) w[i] *= dinv[i];
+    lam = sqrt(dot(w, w, n));
+    double *t = v; v = w; w = t;
+  }
+  free(v);
+  free(w);
+  return lam;
+}
+
+/* Chebyshev smoothing on a CSR level; same recurrence as chebyshev() above. */
+static void csr_chebyshev(const oracle_csr *A, const amg_level *L, int k, double safety, double ratio,
+                          double *z, double *res, int want_res) {
+  size_t n = (size_t)A->rows;
+  double hi = L->lmax * safety, lo = hi / ratio;
+  double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
+  double *d = (double *)malloc(sizeof(double) * n), *Ad = (double *)malloc(sizeof(double) * n);
+  double rho_old = 1.0 / sigma;
+  for (size_t i = 0; i < n; ++i) d[i] = L->dinv[i] * res[i] / theta;
+  for (int it = 0; it < k; ++it) {
+    if (it > 0) {
+      double rho = 1.0 / (2.0 * sigma - rho_old);
+      for (size_t i = 0; i < n; ++i) d[i] = rho * rho_old * d[i] + (2.0 * rho / delta) * L->dinv[i] * res[i];
+      rho_old = rho;
+    }
+    for (size_t i = 0; i < n; ++i) z[i] += d[i];
+    if (it < k - 1 || want_res) {
+      csr_mv(A, d, Ad);
+      for (size_t i = 0; i < n; ++i) res[i] -= Ad[i];
+    }
+  }
+  free(d);
+  free(Ad);
+}
+
+static void amg_vcycle(const oracle_solver_opts *o, const amg_level *al, int l, const double *r,
+                       double *z) {
+  const oracle_csr *A = &o->amg_A[l];
+  size_t n = (size_t)A->rows;
+  if (l == o->amg_nlevels - 1) {
+    for (size_t i = 0; i < n; ++i) {
+      double s = 0.0;
+      for (size_t j = 0; j < n; ++j) s += o->amg_coarse_inv[i * n + j] * r[j];
+      z[i] = s;
+    }
+    return;
+  }
+  size_t nc = (size_t)o->amg_A[l + 1].rows;
+  double *res = (double *)malloc(sizeof(double) * n), *tmp = (double *)malloc(sizeof(double) * n);
+  double *rc = (double *)malloc(sizeof(double) * nc), *zc = (double *)malloc(sizeof(double) * nc);
+  memset(z, 0, sizeof(double) * n);
+  memcpy(res, r, sizeof(double) * n);
+  csr_chebyshev(A, &al[l], o->cheb_order, o->eig_safety, o->eig_ratio, z, res, 1);
+  csr_mv(&o->amg_R[l], res, rc);
+  amg_vcycle(o, al, l + 1, rc, zc);
+  csr_mv(&o->amg_P[l], zc, tmp);
+  for (size_t i = 0; i < n; ++i) z[i] += tmp[i];
+  csr_mv(A, z, tmp);
+  for (size_t i = 0; i < n; ++i) res[i] = r[i] - tmp[i];
+  csr_chebyshev(A, &al[l], o->cheb_order, o->eig_safety, o->eig_ratio, z, res, 0);
+  free(res); free(tmp); free(rc); free(zc);
+}
+
 static void vcycle(const pmg_level *lv, int nl, int l, const oracle_solver_opts *o,
-                   const double *r, double *z) {
+                   const double *r, double *z, const amg_level *al);
+
+/* Last order level with an algebraic coarse solve: Chebyshev, restriction to
+ * the algebraic level 0 (R_dg), AMG V-cycle, prolongation (P_dg), Chebyshev. */
+static void last_level_amg(const pmg_level *L, const oracle_solver_opts *o, const double *r,
+                           double *z, const amg_level *al) {
+  size_t n = vec_len(&L->op);
+  size_t n0 = (size_t)o->amg_A[0].rows;
+  double *res = (double *)malloc(sizeof(double) * n), *tmp = (double *)malloc(sizeof(double) * n);
+  double *r0 = (double *)malloc(sizeof(double) * n0), *z0 = (double *)malloc(sizeof(double) * n0);
+  memset(z, 0, sizeof(double) * n);
+  memcpy(res, r, sizeof(double) * n);
+  chebyshev(L, o->cheb_order, o->eig_safety, o->eig_ratio, z, res, 1);
+  csr_mv(o->amg_Rdg, res, r0);
+  amg_vcycle(o, al, 0, r0, z0);
+  csr_mv(o->amg_Pdg, z0, tmp);
+  for (size_t i = 0; i < n; ++i) z[i] += tmp[i];
+  op_apply(&L->op, z, tmp);
+  for (size_t i = 0; i < n; ++i) res[i] = r[i] - tmp[i];
+  chebyshev(L, o->cheb_order, o->eig_safety, o->eig_ratio, z, res, 0);
+  free(res); free(tmp); free(r0); free(z0);
+}
+
+static void vcycle(const pmg_level *lv, int nl, int l, const oracle_solver_opts *o,
+                   const double *r, double *z, const amg_level *al) {
   const pmg_level *L = &lv[l];
   size_t n = vec_len(&L->op);
   if (l == nl - 1) {
-    coarse_cg(L, o->coarse_iters, r, z);
+    if (o->coarse_kind == 1) last_level_amg(L, o, r, z, al);
+    else coarse_cg(L, o->coarse_iters, r, z);
     return;
   }
   const pmg_level *C = &lv[l + 1];
@@ -668,7 +779,7 @@ static void vcycle(const pmg_level *lv, int nl, int l, const oracle_solver_opts 
         for (int i = 0; i < Np; ++i) s += L->P[i * Npc + j] * res[((size_t)c * K + e) * Np + i];
         rc[((size_t)c * K + e) * Npc + j] = s;
       }
-  vcycle(lv, nl, l + 1, o, rc, zc);
+  vcycle(lv, nl, l + 1, o, rc, zc, al);
   for (int c = 0; c < L->op.ncomp; ++c)
     for (int e = 0; e < K; ++e)
       for (int i = 0; i < Np; ++i) {
@@ -700,6 +811,7 @@ void oracle_solve(const oracle_mesh *m, const oracle_solver_opts *o, const doubl
   const int Np = m->Np, K = m->K;
   double *dinv = NULL, *blocks = NULL;
   pmg_level *lv = NULL;
+  amg_level *al = NULL;
   int nl = 0;
   if (o->pin_dof >= 0 || o->precond == ORACLE_PRE_JACOBI) {
     dinv = (double *)malloc(sizeof(double) * n);
@@ -723,6 +835,20 @@ void oracle_solve(const oracle_mesh *m, const oracle_solver_opts *o, const doubl
       if (ol.pin_dof >= 0) lv[l].op.pin_scale = 1.0 / lv[l].dinv[ol.pin_dof];
       lv[l].lmax = power_lmax(&lv[l].op, lv[l].dinv, o->eig_iters);
       lv[l].P = l < nl - 1 ? o->pmg_prolong[l] : NULL;
+    }
+    if (o->coarse_kind == 1) {
+      al = (amg_level *)calloc(o->amg_nlevels, sizeof(amg_level));
+      for (int l = 0; l + 1 < o->amg_nlevels; ++l) {
+        const oracle_csr *A = &o->amg_A[l];
+        al[l].dinv = (double *)malloc(sizeof(double) * A->rows);
+        for (int i = 0; i < A->rows; ++i) {
+          double d = 0.0;
+          for (int k = A->ptr[i]; k < A->ptr[i + 1]; ++k)
+            if (A->idx[k] == i) d = A->val[k];
+          al[l].dinv[i] = 1.0 / d;
+        }
+        al[l].lmax = csr_power_lmax(A, al[l].dinv, o->eig_iters);
+      }
     }
   }
   double *r = (double *)malloc(sizeof(double) * n), *z = (double *)malloc(sizeof(double) * n);
@@ -766,7 +892,7 @@ void oracle_solve(const oracle_mesh *m, const oracle_solver_opts *o, const doubl
             out[b_ * Np + i_] = s_;                                                        \
           }                                                                                \
         break;                                                                             \
-      case ORACLE_PRE_PMG: vcycle(lv, nl, 0, o, in, out); break;                           \
+      case ORACLE_PRE_PMG: vcycle(lv, nl, 0, o, in, out, al); break;                       \
     }                                                                                      \
     if (o->nullspace) project_mean(out, n);                                                \
   } while (0)
@@ -825,5 +951,9 @@ void oracle_solve(const oracle_mesh *m, const oracle_solver_opts *o, const doubl
   if (lv) {
     for (int l = 0; l < nl; ++l) free(lv[l].dinv);
     free(lv);
+  }
+  if (al) {
+    for (int l = 0; l + 1 < o->amg_nlevels; ++l) free(al[l].dinv);
+    free(al);
   }
 }

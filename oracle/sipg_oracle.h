@@ -68,6 +68,13 @@ void oracle_block_diag(const oracle_mesh *m, int ncomp, const int *bc_types,
                        const double *factor, const double *mm_factor, double mm_scalar,
                        int flags, int inv, double *blocks);
 
+/* CSR matrix (algebraic levels of the coarse solve). */
+typedef struct {
+  int rows, cols;
+  const int *ptr, *idx;
+  const double *val;
+} oracle_csr;
+
 /* Solvers. Preconditioner kinds follow ViscousSolver3D::Preconditioners. */
 enum {
   ORACLE_PRE_NONE = 0,
@@ -108,7 +115,15 @@ typedef struct {
   double eig_safety;         /* eigenvalue safety factor (eigen_val_saftey_factor) */
   double eig_ratio;          /* lambda_min = lambda_max / eig_ratio */
   int eig_iters;             /* power iterations for lambda_max */
-  int coarse_iters;          /* Jacobi-PCG iterations on the coarsest level */
+  int coarse_iters;          /* Jacobi-PCG iterations on the coarsest level (coarse_kind 0) */
+  /* coarse_kind 1: below the last order, restrict to element-wise constants and
+   * run a V-cycle over an algebraic hierarchy of CSR operators */
+  int coarse_kind;
+  int amg_nlevels;
+  const oracle_csr *amg_A, *amg_P, *amg_R; /* per level (P, R: level l <-> l+1) */
+  const oracle_csr *amg_Pdg, *amg_Rdg;     /* last-order DG unknowns <-> algebraic level 0 */
+  const double *amg_coarse_inv;            /* dense inverse of the coarsest operator */
+  int amg_coarse_n;
 } oracle_solver_opts;
 
 /* Solve A x = b (x holds the initial guess on entry). ncomp components are

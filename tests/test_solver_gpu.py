@@ -34,7 +34,8 @@ def test_krylov_matches_reference_golden(path, name):
     assert rel_err(x, g[f"solve_{name}_x"]) < 1e-8
 
 
-def _pmg_oracle_levels(mesh, orders, factor, bct):
+def _pmg_oracle_levels(mesh, orders, factor, bct, amg=True):
+    import ctypes as C
     meshes, facs, prol = [], [], []
     for l, p in enumerate(orders):
         t = sipg.ref_tables(3, p)
@@ -43,8 +44,15 @@ def _pmg_oracle_levels(mesh, orders, factor, bct):
         facs.append(factor @ I.T)
         if l + 1 < len(orders):
             prol.append(sipg.interp_matrix(3, orders[l + 1], p))
-    return dict(orders=orders, meshes=meshes, factors=facs, prolong=prol, cheb_order=4,
-                eig_safety=1.1, eig_ratio=30.0, eig_iters=20, coarse_iters=20)
+    out = dict(orders=orders, meshes=meshes, factors=facs, prolong=prol, cheb_order=4,
+               eig_safety=1.1, eig_ratio=30.0, eig_iters=20, coarse_iters=20)
+    if amg:
+        tau1 = np.zeros((mesh.K, 4))
+        f1 = np.ascontiguousarray(facs[-1])
+        O.oracle_lib().oracle_tau(C.byref(meshes[-1].s), O._d(f1), O._d(tau1))
+        bd = (np.asarray(bct)[0] == sipg.BC_DIRICHLET).astype(np.int32)
+        out["amg"] = sipg.Amg.p1(mesh, f1, tau1, bd, coarse_max=1000, strength=0.08, singular=not bd.any())
+    return out
 
 
 @pytest.fixture(scope="module")
@@ -52,22 +60,26 @@ def two_phase():
     return W.poisson3d_two_phase(4, order=3, n_modes=64)
 
 
-def _pmg_solver(case, precision):
+def _pmg_solver(case, precision, coarse_kind=1, pin=True):
     op = make_op(case["mesh"], 3, 1, case["factor"], bct=case["bc_types"])
-    op.set_pin(*case["pin"])
+    if pin:
+        op.set_pin(*case["pin"])
     o = sipg.default_opts(sipg.SOLVER_PMULTIGRID)
     o.rel_tol, o.abs_tol, o.max_iter, o.precision = 1e-8, 0.0, 200, precision
+    o.coarse_kind = coarse_kind
+    o.nullspace = 0 if pin else 1
     return op, sipg.Solver(op, sipg.SOLVER_PMULTIGRID, o)
 
 
-def test_pmultigrid_fp64_matches_oracle(two_phase):
+@pytest.mark.parametrize("coarse_kind", [0, 1], ids=["coarse_cg", "coarse_amg"])
+def test_pmultigrid_fp64_matches_oracle(two_phase, coarse_kind):
     c = two_phase
     om = O.OMesh(c["tables"], c["export"])
-    pmg = _pmg_oracle_levels(c["mesh"], [3, 2, 1], c["factor"], c["bc_types"])
+    pmg = _pmg_oracle_levels(c["mesh"], [3, 2, 1], c["factor"], c["bc_types"], amg=coarse_kind == 1)
     xo, io = O.solve(om, c["rhs"], c["bc_types"], O.PRE_PMG, c["factor"], abs_tol=0.0, rel_tol=1e-8,
                      max_iter=200, pin_dof=0, pmg=pmg)
     assert io.converged
-    op, s = _pmg_solver(c, sipg.FP64)
+    op, s = _pmg_solver(c, sipg.FP64, coarse_kind)
     x, info = s.solve_host(c["rhs"])
     assert info.status == sipg.SIPG_OK
     assert abs(info.iters - io.iters) <= 1
@@ -75,11 +87,24 @@ def test_pmultigrid_fp64_matches_oracle(two_phase):
     assert info.true_rel_res < 1e-8
 
 
+def test_pmultigrid_nullspace_fp64_matches_oracle(two_phase):
+    c = W.poisson3d_two_phase(4, order=3, n_modes=64, pin=False)
+    om = O.OMesh(c["tables"], c["export"])
+    pmg = _pmg_oracle_levels(c["mesh"], [3, 2, 1], c["factor"], c["bc_types"])
+    xo, io = O.solve(om, c["rhs"], c["bc_types"], O.PRE_PMG, c["factor"], abs_tol=0.0, rel_tol=1e-8,
+                     max_iter=200, nullspace=1, pmg=pmg)
+    op, s = _pmg_solver(c, sipg.FP64, 1, pin=False)
+    x, info = s.solve_host(c["rhs"])
+    assert info.status == sipg.SIPG_OK
+    assert abs(info.iters - io.iters) <= 1
+    assert rel_err(x, xo) < 1e-9
+
+
 def test_pmultigrid_mixed_precision_reaches_fp64_tolerance(two_phase):
-    c = two_phase
-    _, s64 = _pmg_solver(c, sipg.FP64)
+    c = W.poisson3d_two_phase(6, order=3, n_modes=64, pin=False)
+    _, s64 = _pmg_solver(c, sipg.FP64, pin=False)
     x64, i64 = s64.solve_host(c["rhs"])
-    _, s32 = _pmg_solver(c, sipg.FP32)
+    _, s32 = _pmg_solver(c, sipg.FP32, pin=False)
     x32, i32 = s32.solve_host(c["rhs"])
     assert i32.status == sipg.SIPG_OK
     assert abs(i32.iters - i64.iters) <= 1
