@@ -107,6 +107,10 @@ int sipg_op_set_pin(sipg_op *op, int elem, int node);
 int sipg_op_apply(sipg_op *op, int precision, const void *x, void *y, void *stream);
 /* Same with host FP64 buffers (copies in and out inside the call). */
 int sipg_op_apply_host(sipg_op *op, const double *x, double *y);
+/* Kernel selection of apply(): 0 tensor cores where the operator allows it
+ * (scalar operators: TF32 MMAs for SIPG_FP32, FP64 MMAs for SIPG_FP64), 1 the
+ * CUDA-core kernel. No reference counterpart (the reference has one OP2 path). */
+int sipg_op_set_kernel(sipg_op *op, int kind);
 /* apply_bc (factor_viscous_matrix.cpp:47-68): rhs += lifted bc data; host buffers,
  * bc: ncomp x Kb x Nfp, rhs: ncomp x K x Np (updated in place). */
 int sipg_op_apply_bc_host(sipg_op *op, const double *bc, double *rhs);

@@ -321,8 +321,25 @@ AmgHierarchy build_amg(const Csr& A0, const Csr& Pdg, int coarse_max, double str
       if (C.idx[k] == i) dmax = std::max(dmax, std::fabs(C.val[k]));
     }
   if (singular)
-    for (int i = 0; i < n; ++i) dense[(size_t)i * n + i] += 1e-10 * dmax;
-  H.coarse_inv = dense_inverse(std::move(dense), n);
+    for (int i = 0; i < n; ++i) dense[(size_t)i * n + i] += 1e-8 * dmax;
+  std::vector<double> inv = dense_inverse(std::move(dense), n);
+  if (singular) {
+    // pseudo-inverse on the complement of the constants: Q inv Q with Q = I - 11^T/n,
+    // so the coarsest correction neither sees nor produces the nullspace
+    std::vector<double> rm(n, 0.0), cm(n, 0.0);
+    double all = 0.0;
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j) {
+        double v = inv[(size_t)i * n + j];
+        rm[i] += v;
+        cm[j] += v;
+        all += v;
+      }
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j)
+        inv[(size_t)i * n + j] += -rm[i] / n - cm[j] / n + all / ((double)n * n);
+  }
+  H.coarse_inv = std::move(inv);
   H.coarse_n = n;
   return H;
 }

@@ -108,6 +108,26 @@ const DevRef& dev_ref(int dim, int order) {
   d->itab.upload(itab.data(), itab.size());
   d->mf = DevBuf(d->ref.MF.size() * sizeof(double));
   d->mf.upload(d->ref.MF.data(), d->ref.MF.size() * sizeof(double));
+  {
+    // tensor-core blobs: FP64 as is, FP32 rounded to nearest TF32
+    std::vector<double> t64, t32d;
+    build_tc_consts<double>(dim, order, d->ref, t64);
+    build_tc_consts<float>(dim, order, d->ref, t32d);
+    std::vector<float> t32(t32d.size());
+    for (size_t i = 0; i < t32d.size(); ++i) {
+      float f = (float)t32d[i];
+      uint32_t b;
+      std::memcpy(&b, &f, 4);
+      b = (b + 0x1000u) & ~0x1FFFu;
+      std::memcpy(&t32[i], &b, 4);
+    }
+    d->tc64 = DevBuf(t64.size() * sizeof(double));
+    d->tc64.upload(t64.data(), t64.size() * sizeof(double));
+    d->tc32 = DevBuf(t32.size() * sizeof(float));
+    d->tc32.upload(t32.data(), t32.size() * sizeof(float));
+    d->tc_ok64 = tc_warps_for<double>(dim, order) >= 2;
+    d->tc_ok32 = tc_warps_for<float>(dim, order) >= 2;
+  }
   auto* raw = d.get();
   slot[0] = std::move(d);
   return *raw;
@@ -183,6 +203,14 @@ void sipg_op::apply(const T* x, T* y, cudaStream_t s, T alpha, T beta) const {
   a.eb = f64 ? eb64 : eb32;
   a.alpha = alpha;
   a.beta = beta;
+  const bool tc = kernel == 0 && ncomp == 1 && (f64 ? dref->tc_ok64 : dref->tc_ok32);
+  if (tc) {
+    const T* tcc = f64 ? (const T*)dref->tc64.p : (const T*)dref->tc32.p;
+    DevBuf& tr = f64 ? trace64 : trace32;
+    if (!tr.p) tr = DevBuf(tc_trace_values(mesh->dim, order, mesh->K) * sizeof(T));
+    SIPG_CUDA(launch_apply_tc<T>(mesh->dim, order, a, tcc, tr.as<T>(), num_sms(), s));
+    return;
+  }
   SIPG_CUDA(launch_apply<T>(mesh->dim, order, a, num_sms(), s));
 }
 template void sipg_op::apply<double>(const double*, double*, cudaStream_t, double, double) const;
@@ -512,6 +540,13 @@ int sipg_op_apply(sipg_op* op, int precision, const void* x, void* y, void* stre
     if (precision == SIPG_FP64) op->apply<double>((const double*)x, (double*)y, s);
     else if (precision == SIPG_FP32) op->apply<float>((const float*)x, (float*)y, s);
     else throw Error(SIPG_INVALID_ARG, "precision must be 64 or 32");
+  });
+}
+
+int sipg_op_set_kernel(sipg_op* op, int kind) {
+  return guarded([&] {
+    if (!op || kind < 0 || kind > 1) throw Error(SIPG_INVALID_ARG, "set_kernel");
+    op->kernel = kind;
   });
 }
 

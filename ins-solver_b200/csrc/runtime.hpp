@@ -12,6 +12,7 @@
 #include "mesh.hpp"
 #include "refelem.hpp"
 #include "sipg_apply.cuh"
+#include "sipg_apply_tc.cuh"
 #include "sipg_blocks.cuh"
 
 namespace sipg {
@@ -44,6 +45,8 @@ struct DevBuf {
 struct DevRef {
   RefElement ref;
   DevBuf c64, c32, itab, mf;
+  DevBuf tc64, tc32;   // tensor-core constant blobs (A1 | A2)
+  bool tc_ok64 = false, tc_ok32 = false;
   int Np = 0, Nfp = 0;
 };
 const DevRef& dev_ref(int dim, int order);  // cached per device
@@ -80,6 +83,8 @@ struct sipg_op {
   int pin_elem = -1, pin_node = -1;
   double pin_scale = 1.0;
   int eb64 = 0, eb32 = 0;
+  int kernel = 0;  // 0: tensor cores where available, 1: CUDA cores
+  mutable sipg::DevBuf trace64, trace32;  // face traces of the two-pass tensor-core apply
   // Apply on device buffers in precision T.
   template <typename T>
   void apply(const T* x, T* y, cudaStream_t s, T alpha = T(1), T beta = T(0)) const;

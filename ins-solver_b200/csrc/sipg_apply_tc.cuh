@@ -1,0 +1,27 @@
+// Tensor-core SIPG apply launchers (sipg_apply_tc.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "refelem.hpp"
+#include "sipg_apply.cuh"
+
+namespace sipg {
+
+// Scalar operator (ncomp == 1) on the tensor cores: T = float runs TF32 MMAs
+// with FP32 accumulation, T = double runs FP64 MMAs. tc_consts: device blob of
+// build_tc_consts<T> converted to T.
+// trace: scratch of tc_trace_values(dim, order, K) values (face traces between
+// the two passes); applies sharing one trace buffer must be stream-ordered.
+template <typename T>
+cudaError_t launch_apply_tc(int dim, int order, const ApplyArgs<T>& a, const T* tc_consts, T* trace,
+                            int num_sms, cudaStream_t s);
+size_t tc_trace_values(int dim, int order, int K);
+template <typename T>
+void build_tc_consts(int dim, int order, const RefElement& r, std::vector<double>& out);
+// Warps per CTA of the apply pass (below 2: use the CUDA-core kernel).
+template <typename T>
+int tc_warps_for(int dim, int order);
+
+}  // namespace sipg

@@ -201,6 +201,10 @@ class Operator:
         t = np.ascontiguousarray(types, dtype=np.int32).reshape(-1)
         check(lib().sipg_op_set_bc_types(self.h, _ip(t)))
 
+    def set_kernel(self, kind):
+        """0: tensor cores where available (default), 1: CUDA cores."""
+        check(lib().sipg_op_set_kernel(self.h, int(kind)))
+
     def set_pin(self, elem, node=0):
         check(lib().sipg_op_set_pin(self.h, elem, node))
 

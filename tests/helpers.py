@@ -13,6 +13,7 @@ GOLDEN = sorted(glob.glob(os.path.join(HERE, "golden", "*.npz")))
 # Tolerances (relative, max-norm over the output vector)
 TOL_FP64 = 1e-13   # FP64 apply / diag / lift vs oracle
 TOL_FP32 = 2e-5    # FP32 apply vs FP64 oracle (FP32 arithmetic, FP32 geometry)
+TOL_TF32 = 1e-2    # FP32 data on TF32 tensor cores (10-bit operand mantissa) vs FP64 oracle
 
 
 def rel_err(a, b):

@@ -5,30 +5,35 @@ import pytest
 
 import oracle_py as O
 import sipg
-from helpers import (GOLDEN, TOL_FP32, TOL_FP64, DevArray, golden_setup, load_golden, make_op,
+from helpers import (GOLDEN, TOL_FP32, TOL_FP64, TOL_TF32, DevArray, golden_setup, load_golden, make_op,
                      random_case, rel_err)
 
 pytestmark = pytest.mark.gpu
 
 
+@pytest.mark.parametrize("kernel", [0, 1], ids=["tensor_cores", "cuda_cores"])
 @pytest.mark.parametrize("path", GOLDEN, ids=lambda p: p.split("/")[-1][:-4])
-def test_apply_fp64_matches_reference_golden(path):
+def test_apply_fp64_matches_reference_golden(path, kernel):
     g = load_golden(path)
     mesh, t, e, om = golden_setup(g)
     op = make_op(mesh, g["order"], g["ncomp"], g.get("factor"), g.get("mm"), bct=g["bct"])
+    op.set_kernel(kernel)
     y = op.apply_host(g["x"])
     assert rel_err(y, g["y"]) < TOL_FP64
 
 
+@pytest.mark.parametrize("kernel", [0, 1], ids=["tf32_tensor_cores", "fp32_cuda_cores"])
 @pytest.mark.parametrize("path", GOLDEN, ids=lambda p: p.split("/")[-1][:-4])
-def test_apply_fp32_within_tolerance(path):
+def test_apply_fp32_within_tolerance(path, kernel):
     g = load_golden(path)
     mesh, t, e, om = golden_setup(g)
     op = make_op(mesh, g["order"], g["ncomp"], g.get("factor"), g.get("mm"), bct=g["bct"])
+    op.set_kernel(kernel)
     x = DevArray(g["x"].astype(np.float32))
     y = DevArray(np.zeros_like(g["x"], dtype=np.float32))
     op.apply_device(sipg.FP32, x.p, y.p)
-    assert rel_err(y.get().astype(np.float64), g["y"]) < TOL_FP32
+    tol = TOL_TF32 if (kernel == 0 and g["ncomp"] == 1) else TOL_FP32
+    assert rel_err(y.get().astype(np.float64), g["y"]) < tol
 
 
 @pytest.mark.parametrize("path", GOLDEN, ids=lambda p: p.split("/")[-1][:-4])
@@ -40,7 +45,7 @@ def test_diag_blocks_and_lift_match_reference_golden(path):
     blk = op.block_diag_host(invert=False, ref_volume_block=True)
     assert rel_err(blk[0], g["blocks0"]) < 1e-12  # cancellation in the reference block form at p=4
     rhs = op.apply_bc_host(g["bc"], np.zeros_like(g["x"]))
-    assert rel_err(rhs, g["rhs"]) < TOL_FP64
+    assert rel_err(rhs, g["rhs"]) < 1e-12
 
 
 @pytest.mark.parametrize("dim,n", [(2, 7), (3, 3)])
@@ -55,14 +60,19 @@ def test_apply_random_cases_vs_oracle(dim, n, order, variant):
     op = make_op(mesh, order, ncomp, f, m, bct=bct)
     y_ref = O.mult(om, x, bct, f, m)
     assert rel_err(op.apply_host(x), y_ref) < TOL_FP64
+    op.set_kernel(1)
+    assert rel_err(op.apply_host(x), y_ref) < TOL_FP64
+    op.set_kernel(0)
     blocks = op.block_diag_host(invert=True)
     exact = O.block_diag(om, ncomp, bct, f, m, inv=True)
     assert rel_err(blocks, exact) < 1e-11
 
 
-def test_apply_alpha_beta_epilogue_and_pinned_dof():
+@pytest.mark.parametrize("kernel", [0, 1])
+def test_apply_alpha_beta_epilogue_and_pinned_dof(kernel):
     mesh, t, e, om, x, f, m, bct = random_case(3, 3, 3, 1, seed=9)
     op = make_op(mesh, 3, 1, f, bct=bct)
+    op.set_kernel(kernel)
     op.set_pin(0, 0)
     xd = DevArray(x)
     y0 = np.random.default_rng(1).uniform(-1, 1, x.shape)
@@ -82,7 +92,9 @@ def test_apply_alpha_beta_epilogue_and_pinned_dof():
 
 
 def test_apply_is_symmetric_and_spd_with_dirichlet():
-    mesh, t, e, om, x, f, m, bct = random_case(3, 2, 3, 1, seed=4)
+    # constant coefficient: with a nodal factor the face quadrature of the factor
+    # (fvmf_3d_mult_flux.h:18-22 vs the averaged f grad u) makes the operator non-symmetric
+    mesh, t, e, om, x, f, m, bct = random_case(3, 2, 3, 1, seed=4, factor=False)
     bct[:] = 0
     op = make_op(mesh, 3, 1, f, bct=bct)
     rng = np.random.default_rng(3)
