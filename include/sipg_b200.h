@@ -107,6 +107,21 @@ int sipg_op_set_pin(sipg_op *op, int elem, int node);
 int sipg_op_apply(sipg_op *op, int precision, const void *x, void *y, void *stream);
 /* Same with host FP64 buffers (copies in and out inside the call). */
 int sipg_op_apply_host(sipg_op *op, const double *x, double *y);
+/* Allocation-free apply. No counterpart in the reference (its mult has no
+ * scratch of its own; OP2 leases temporaries from a dat pool). Same arguments,
+ * kernels and results as sipg_op_apply, but the face-trace scratch of the
+ * two-pass tensor-core apply comes from a fixed array of
+ * SIPG_STATIC_SCRATCH_BYTES compiled into the library, not from cudaMalloc,
+ * for callers that cannot allocate device memory at apply time. The first call
+ * on each device (current device) does a one-time set-up, a symbol-address
+ * lookup; make it before any stream capture. Operators whose scratch would
+ * exceed the limit (K * (dim+1) * 2 * Nfp values; at p = 3 in 3D: 209,715
+ * elements FP32, 104,857 FP64) get SIPG_INVALID_ARG. There is one scratch per
+ * device: calls that overlap in time on one device race on it, so order them
+ * on one stream or synchronise between them. Nothing in it needs to start at
+ * zero. */
+#define SIPG_STATIC_SCRATCH_BYTES (64u << 20)
+int sipg_op_apply_static_scratch(sipg_op *op, int precision, const void *x, void *y, void *stream);
 /* Kernel selection of apply(): 0 tensor cores where the operator allows it
  * (scalar operators: TF32 MMAs for SIPG_FP32, FP64 MMAs for SIPG_FP64), 1 the
  * CUDA-core kernel. No reference counterpart (the reference has one OP2 path). */
