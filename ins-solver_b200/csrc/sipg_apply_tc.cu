@@ -5,23 +5,28 @@
 // src/solvers/3d/slip_matrix/factor_viscous_matrix.cpp:96-310, one component).
 // The reference exchanges face data through 12 face buffers per component
 // (mesh->jump / mesh->avg into K x Nf*Nfp op_dats); here each element publishes
-// one trace record per face, and the matrix products are batched over elements:
-//   pass 1 (traces): grad_ref = [D_r] x (G1, 3Np x Np), then per face node
-//           u = x(m) and g = f(m) n.grad x(m) with the element's own outward
-//           normal -> trace[e][f] = (u[0..Nfp), g[0..Nfp)) in the element's
-//           face-node order. 2 Nf Nfp values per element, L2-resident between
-//           the passes.
-//   pass 2 (apply): G1 again for the own gradient; the neighbour's trace gives
-//           u+ and n-.q+ = -g+ (n+ = -n-), so no neighbour volume data is read;
-//           fluxes Fu = sJ (tau [u]/2 - n.{q}), Fq = -n sJ f [u]/2
-//           (fvmf_3d_mult_flux.h:13-22), boundary traces as
-//           vmf_3d_mult_avg_jump.h:43-80; then one product
-//             y_e = A2 b_e,  A2 = [D_r^T M | D_r^T EMAT | EMAT | M]  (Np x K2)
-//           with b_e = [q~_r | F~_r | Fu | J mm x], q~_r = J sum_d G[r][d] q_d,
-//           F~_r = sum_d G[r][d] Fq_d (geometry folded into the data; D_r^T M
-//           and D_r^T EMAT precomputed).
-// Each warp owns a tile of 8 elements (the MMA N dimension) and synchronises at
-// warp level only; the constant operands live in shared memory per CTA.
+// one trace record per face and every matrix product is batched over elements.
+//
+// Elements are the M dimension of mma.sync (16 per warp tile for TF32
+// m16n8k8, 8 for FP64 m8n8k4); the reference-element matrices are the B
+// operands, packed on the host in fragment order. An accumulator block is laid
+// out exactly like an A block once the dummy summation index k is permuted
+// (slot t <-> logical column 2t, slot t+4 <-> 2t+1, folded into the packing of
+// B), so a product's result feeds the next product from registers and the
+// elementwise steps (metric terms, fluxes) run on fragment registers.
+//
+//   pass 1 (traces): per face node k = (f, j) with volume node m = fmask(f, j):
+//           g = f(m) sum_r c_r(f) (D_r x)(m), c_r = n_f . grad r, computed as
+//           x (TE x Np) . BF_r (Np x Nf*Nfp), BF_r[n][k] = D_r[m(k)][n];
+//           trace[e][f] = (x(m(f, j)) for j < Nfp, g(f, j) for j < Nfp).
+//   pass 2 (apply): gr_r = x . B1_r (gradient in the reference directions),
+//           w_r = J f sum_s K_rs gr_s (K = G G^T, the metric of the element),
+//           fluxes from the own and the neighbour's traces
+//             [u] = u- - u+, n.{q} = (g- - g+)/2 (n+ = -n-), boundary faces as
+//             vmf_3d_mult_avg_jump.h:43-80,
+//             Fu = sJ (tau [u]/2 - n.{q}), S = -sJ f [u]/2 (fvmf_3d_mult_flux.h:13-22),
+//           Z_r = w_r . M^T + (c_r S) . EMAT^T,
+//           y = sum_r Z_r . D_r + Fu . EMAT^T + (J mm x) . M^T.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -35,230 +40,155 @@
 namespace sipg {
 namespace {
 
-constexpr int kEl = 8;  // elements per warp tile (MMA N)
-
 __host__ __device__ constexpr int rup(int x, int m) { return (x + m - 1) / m * m; }
-// Leading dimensions congruent to 4 (mod 32) 32-bit words: fragment loads of a
-// warp touch 32 distinct banks.
-__host__ __device__ constexpr int ld32(int x) { return rup(x - 4, 32) + 4 >= x ? rup(x - 4, 32) + 4 : rup(x - 4, 32) + 36; }
-__host__ __device__ constexpr int ld64(int x) { return rup(x - 4, 16) + 4 >= x ? rup(x - 4, 16) + 4 : rup(x - 4, 16) + 20; }
 
+// MMA on logical blocks of 8R element rows x 8 columns. Lane (g = lane/4,
+// t = lane%4) holds rows g + 8 ri (ri < R) and logical columns 2t + ci (ci < 2)
+// of an A block and of an accumulator block, and rows 2t + ci, column g of a
+// B block (one V2 per lane in the packed blobs).
 template <typename T>
-struct Mma;
+struct Frag;
 
-// m16n8k8 TF32 inputs, FP32 accumulate.
 template <>
-struct Mma<float> {
-  static constexpr int MT = 16, KT = 8, NC = 4;
-  using A = uint32_t[4];
-  using B = uint32_t[2];
-  __device__ static __forceinline__ float to_op(float x) {
+struct Frag<float> {
+  static constexpr int R = 2;
+  using V2 = float2;
+  __device__ static __forceinline__ float op(float x) {
     uint32_t r;
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
     return __uint_as_float(r);
   }
-  __device__ static __forceinline__ void load_a(A& a, const float* M, int lda, int m0, int k0, int lane) {
-    const int g = lane >> 2, t = lane & 3;
-    a[0] = __float_as_uint(M[(m0 + g) * lda + k0 + t]);
-    a[1] = __float_as_uint(M[(m0 + g + 8) * lda + k0 + t]);
-    a[2] = __float_as_uint(M[(m0 + g) * lda + k0 + t + 4]);
-    a[3] = __float_as_uint(M[(m0 + g + 8) * lda + k0 + t + 4]);
-  }
-  __device__ static __forceinline__ void load_b(B& b, const float* S, int ldb, int k0, int lane) {
-    const int g = lane >> 2, t = lane & 3;
-    b[0] = __float_as_uint(S[g * ldb + k0 + t]);
-    b[1] = __float_as_uint(S[g * ldb + k0 + t + 4]);
-  }
-  __device__ static __forceinline__ void mma(float* c, const A& a, const B& b) {
+  // m16n8k8: a0 (g, t) a1 (g+8, t) a2 (g, t+4) a3 (g+8, t+4); b0 (t, g) b1 (t+4, g);
+  // c0 (g, 2t) c1 (g, 2t+1) c2 (g+8, 2t) c3 (g+8, 2t+1).
+  __device__ static __forceinline__ void mma(float (&c)[2][2], const float (&a)[2][2], V2 b) {
     asm volatile(
         "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
         "{%0,%1,%2,%3};\n"
-        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-  }
-  // accumulator C[m][n] -> S[n][m]
-  __device__ static __forceinline__ void store_c(const float* c, float* S, int lds, int m0, int lane) {
-    const int g = lane >> 2, t = lane & 3;
-    S[(2 * t) * lds + m0 + g] = c[0];
-    S[(2 * t + 1) * lds + m0 + g] = c[1];
-    S[(2 * t) * lds + m0 + g + 8] = c[2];
-    S[(2 * t + 1) * lds + m0 + g + 8] = c[3];
+        : "+f"(c[0][0]), "+f"(c[0][1]), "+f"(c[1][0]), "+f"(c[1][1])
+        : "r"(__float_as_uint(a[0][0])), "r"(__float_as_uint(a[1][0])), "r"(__float_as_uint(a[0][1])),
+          "r"(__float_as_uint(a[1][1])), "r"(__float_as_uint(b.x)), "r"(__float_as_uint(b.y)));
   }
 };
 
-// m8n8k4 FP64.
 template <>
-struct Mma<double> {
-  static constexpr int MT = 8, KT = 4, NC = 2;
-  using A = double[1];
-  using B = double[1];
-  __device__ static __forceinline__ double to_op(double x) { return x; }
-  __device__ static __forceinline__ void load_a(A& a, const double* M, int lda, int m0, int k0, int lane) {
-    a[0] = M[(m0 + (lane >> 2)) * lda + k0 + (lane & 3)];
-  }
-  __device__ static __forceinline__ void load_b(B& b, const double* S, int ldb, int k0, int lane) {
-    b[0] = S[(lane >> 2) * ldb + k0 + (lane & 3)];
-  }
-  __device__ static __forceinline__ void mma(double* c, const A& a, const B& b) {
+struct Frag<double> {
+  static constexpr int R = 1;
+  using V2 = double2;
+  __device__ static __forceinline__ double op(double x) { return x; }
+  // two m8n8k4 steps: a0 (g, t), b0 (t, g), c0 (g, 2t) c1 (g, 2t+1); the first
+  // binds slot t to logical column 2t, the second to 2t+1.
+  __device__ static __forceinline__ void mma(double (&c)[1][2], const double (&a)[1][2], V2 b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-                 : "+d"(c[0]), "+d"(c[1])
-                 : "d"(a[0]), "d"(b[0]));
-  }
-  __device__ static __forceinline__ void store_c(const double* c, double* S, int lds, int m0, int lane) {
-    const int g = lane >> 2, t = lane & 3;
-    S[(2 * t) * lds + m0 + g] = c[0];
-    S[(2 * t + 1) * lds + m0 + g] = c[1];
+                 : "+d"(c[0][0]), "+d"(c[0][1])
+                 : "d"(a[0][0]), "d"(b.x));
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(c[0][0]), "+d"(c[0][1])
+                 : "d"(a[0][1]), "d"(b.y));
   }
 };
 
-// Asynchronous global -> shared copies (cp.async), zero-filled when !valid.
+template <typename T, int DIM, int P>
+struct Tc {
+  using C = Cfg<DIM, P>;
+  static constexpr int NP = C::NP, NFP = C::NFP, NF = C::NF, NG = C::NG;
+  static constexpr int R = Frag<T>::R, TE = 8 * R;   // elements per warp tile
+  static constexpr int NT = rup(NP, 8) / 8;          // node blocks
+  static constexpr int KF = NF * NFP;                // face nodes of an element
+  static constexpr int FT = rup(KF, 8) / 8;          // face-node blocks
+  static constexpr int TRP = rup(NFP, 2);            // g part of a trace record starts here
+  static constexpr int TR = rup(2 * TRP, 4);         // record length: a 16-byte multiple
+  static constexpr int BLK = 64;                     // values per packed 8 x 8 block
+  // pass-2 blob: B1_r (NT x NT blocks), BM, BE (FT x NT), B3_r; then the pass-1 blob BF_r (NT x FT)
+  static constexpr int B1 = 0;
+  static constexpr int BM = B1 + DIM * NT * NT * BLK;
+  static constexpr int BE = BM + NT * NT * BLK;
+  static constexpr int B3 = BE + FT * NT * BLK;
+  static constexpr int N2 = B3 + DIM * NT * NT * BLK;
+  static constexpr int BF = N2;
+  static constexpr int N1 = DIM * NT * FT * BLK;
+  static constexpr int NALL = N2 + N1;
+  // element stage (T units; every part is a multiple of 64 bytes)
+  static constexpr int SX = 0, SF = TE * NP, SG = 2 * TE * NP, STAU = SG + TE * NG;
+  static constexpr int SOWN = STAU + TE * NF, SNB = SOWN + TE * NF * TR, ST2 = SNB + TE * NF * TR;
+  static constexpr int ST1 = STAU;                   // pass 1: x, factor, geometry
+  static constexpr int FG = 8;                       // per element face: n (3), sJ, c_r (3)
+  static constexpr int SFG = TE * NF * FG;
+  static constexpr int SI = TE * NF + TE;            // int slot: nbr, face codes
+  static constexpr int W1_T = 2 * ST1 + SFG + TE * NF * TR;
+  static constexpr int W2_T = 2 * ST2 + SFG;
+  static constexpr int W2_I = 3 * SI;
+  static constexpr int CH = TR * (int)sizeof(T) / 16;  // 16-byte chunks per trace record
+};
+
 template <typename T>
-__device__ __forceinline__ void cp_async(T* sdst, const T* gsrc, bool valid) {
+__device__ __forceinline__ typename Frag<T>::V2 ldb(const T* blob, int blk, int lane) {
+  return reinterpret_cast<const typename Frag<T>::V2*>(blob)[blk * 32 + lane];
+}
+
+// 16-byte asynchronous copy, zero-filled past `bytes` (0..16).
+__device__ __forceinline__ void cp16(void* sdst, const void* gsrc, int bytes) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
-  const int n = valid ? (int)sizeof(T) : 0;
-  if (sizeof(T) == 8)
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gsrc), "r"(n));
-  else
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gsrc), "r"(n));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gsrc), "r"(bytes));
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
 
-template <typename T, int DIM, int P>
-struct TcCfg {
-  using C = Cfg<DIM, P>;
-  using M = Mma<T>;
-  static constexpr bool F32 = std::is_same<T, float>::value;
-  static constexpr int NP = C::NP, NFP = C::NFP, NF = C::NF, NFNFP = C::NFNFP, NG = C::NG;
-  static constexpr int TR = 2 * NFP;                       // trace record per face: u, g
-  static constexpr int M1 = rup(DIM * NP, M::MT);
-  static constexpr int K1 = rup(NP, M::KT);
-  static constexpr int M2 = rup(NP, M::MT);
-  // G2 in two K-chunks: A = [q~_r | Fu | J mm x], B = [F~_r]
-  static constexpr int KA = rup(DIM * NP + NFNFP + NP, M::KT);
-  static constexpr int KB = rup(DIM * NFNFP, M::KT);
-  static constexpr int OFU = DIM * NP, OMM = DIM * NP + NFNFP;
-  static constexpr int LDA1 = F32 ? ld32(K1) : ld64(K1);
-  static constexpr int LDA2A = F32 ? ld32(KA) : ld64(KA);
-  static constexpr int LDA2B = F32 ? ld32(KB) : ld64(KB);
-  static constexpr int LDB = F32 ? ld32(KA > KB ? KA : KB) : ld64(KA > KB ? KA : KB);
-  static constexpr int LDC = F32 ? ld32(M1 > M2 ? M1 : M2) : ld64(M1 > M2 ? M1 : M2);
-  static constexpr int CONST1 = M1 * LDA1;
-  static constexpr int CONST_T = M1 * LDA1 + M2 * LDA2A + M2 * LDA2B;
-  static constexpr int FG = 8;  // per (element, face): n (3), sJ, c_r = n.grad r (3)
-  // element-data stage (T units): x, factor, geof, tau; ints: nbr, fcode word.
-  // x is read past its end by the G1 operand (K1 > NP columns meet zero A1
-  // columns), so factor follows x directly and stays finite.
-  static constexpr int ST_T = kEl * NP * 2 + kEl * NG + kEl * NF;
-  static constexpr int ST_I = kEl * NF + kEl;
-  static constexpr int TRB = kEl * NF * TR;  // neighbour traces of one tile
-  // pass 1: 2 stages + G1 output + face geometry
-  static constexpr int W1_T = 2 * ST_T + kEl * LDC + kEl * NF * FG;
-  static constexpr int W1_I = 2 * ST_I;
-  // pass 2: 3 stages, 2 trace buffers, operand, G1/G2 output, face geometry, flux scalars
-  static constexpr int W2_T = 3 * ST_T + 2 * TRB + kEl * LDB + kEl * LDC + kEl * NF * FG + kEl * NFNFP;
-  static constexpr int W2_I = 3 * ST_I;
-};
-
-template <typename T, int DIM, int P>
-struct Stage {
-  using TC = TcCfg<T, DIM, P>;
-  T* x; T* fac; T* geo; T* tau; int* nbr; int* code;
-  __device__ Stage(T* tb, int* ib) {
-    x = tb; fac = x + kEl * TC::NP; geo = fac + kEl * TC::NP; tau = geo + kEl * TC::NG;
-    nbr = ib; code = nbr + kEl * TC::NF;
-  }
-};
-
-// Issue the element data of a tile (zero-filled past the last element).
-template <typename T, int DIM, int P>
-__device__ __forceinline__ void issue_own(const ApplyArgs<T>& a, const Stage<T, DIM, P>& st, int tile, int lane) {
-  using TC = TcCfg<T, DIM, P>;
-  constexpr int NP = TC::NP, NG = TC::NG, NF = TC::NF;
-  const int e0 = tile * kEl;
-  const int ne = max(0, min(kEl, a.K - e0));
-  const T* fsrc = a.factor ? a.factor : a.x;
-  for (int i = lane; i < kEl * NP; i += 32) {
-    const bool v = i < ne * NP;
-    cp_async(st.x + i, v ? a.x + (size_t)e0 * NP + i : a.x, v);
-    cp_async(st.fac + i, (v && a.factor) ? fsrc + (size_t)e0 * NP + i : a.x, v && a.factor);
-  }
-  for (int i = lane; i < kEl * NG; i += 32) {
-    const bool v = i < ne * NG;
-    cp_async(st.geo + i, v ? a.geof + (size_t)e0 * NG + i : a.geof, v);
-  }
-  for (int i = lane; i < kEl * NF; i += 32) {
-    const bool v = i < ne * NF;
-    cp_async(st.tau + i, v ? a.tau + (size_t)e0 * NF + i : a.tau, v);
-    cp_async(st.nbr + i, v ? a.nbr + (size_t)e0 * NF + i : a.nbr, v);
-  }
-  if (lane < kEl) {
-    const bool v = lane < ne;
-    cp_async(st.code + lane, v ? (const int*)a.fcode + e0 + lane : (const int*)a.fcode, v);
+// Copy `total` bytes (a multiple of 16) to shared memory: the first `valid`
+// come from base + off (16-byte aligned), the rest is zero.
+__device__ __forceinline__ void copy_block(void* s, const void* base, size_t off, int total, int valid, int lane) {
+  const char* b = static_cast<const char*>(base);
+  for (int c = lane * 16; c < total; c += 32 * 16) {
+    const int n = min(16, max(0, valid - c));
+    cp16(static_cast<char*>(s) + c, n > 0 ? b + off + c : b, n);
   }
 }
 
-// Issue the neighbour trace records of a tile whose element data has arrived.
 template <typename T, int DIM, int P>
-__device__ __forceinline__ void issue_traces(const ApplyArgs<T>& a, const Stage<T, DIM, P>& st, const T* trace,
-                                             T* dst, int tile, int lane) {
-  using TC = TcCfg<T, DIM, P>;
-  constexpr int NF = TC::NF, TR = TC::TR;
-  const int ne = max(0, min(kEl, a.K - tile * kEl));
-  for (int i = lane; i < kEl * NF * TR; i += 32) {
-    const int lf = i / TR, k = i % TR;
-    const int el = lf / NF;
-    const int nb = st.nbr[lf];
+__device__ __forceinline__ void issue_elem(const ApplyArgs<T>& a, const T* trace, T* st, int tile, int lane,
+                                           bool pass2) {
+  using X = Tc<T, DIM, P>;
+  constexpr int NP = X::NP, NG = X::NG, NF = X::NF, TE = X::TE, S = sizeof(T);
+  const int e0 = tile * TE;
+  const int ne = max(0, min(TE, a.K - e0));
+  copy_block(st + X::SX, a.x, (size_t)e0 * NP * S, TE * NP * S, ne * NP * S, lane);
+  if (a.factor) copy_block(st + X::SF, a.factor, (size_t)e0 * NP * S, TE * NP * S, ne * NP * S, lane);
+  copy_block(st + X::SG, a.geof, (size_t)e0 * NG * S, TE * NG * S, ne * NG * S, lane);
+  if (pass2) {
+    copy_block(st + X::STAU, a.tau, (size_t)e0 * NF * S, TE * NF * S, ne * NF * S, lane);
+    copy_block(st + X::SOWN, trace, (size_t)e0 * NF * X::TR * S, TE * NF * X::TR * S, ne * NF * X::TR * S, lane);
+  }
+}
+
+template <typename T, int DIM, int P>
+__device__ __forceinline__ void issue_ints(const ApplyArgs<T>& a, int* slot, int tile, int lane) {
+  using X = Tc<T, DIM, P>;
+  constexpr int NF = X::NF, TE = X::TE;
+  const int e0 = tile * TE;
+  const int ne = max(0, min(TE, a.K - e0));
+  copy_block(slot, a.nbr, (size_t)e0 * NF * 4, TE * NF * 4, ne * NF * 4, lane);
+  copy_block(slot + TE * NF, a.fcode, (size_t)e0 * 4, TE * 4, ne * 4, lane);
+}
+
+// Neighbour trace records of a tile whose connectivity has arrived.
+template <typename T, int DIM, int P>
+__device__ __forceinline__ void issue_nb(const ApplyArgs<T>& a, const T* trace, T* st, const int* slot, int tile,
+                                         int lane) {
+  using X = Tc<T, DIM, P>;
+  constexpr int NF = X::NF, TE = X::TE, CH = X::CH, TR = X::TR, VPC = 16 / sizeof(T);
+  const int ne = max(0, min(TE, a.K - tile * TE));
+  const int* nbr = slot;
+  const int* code = slot + TE * NF;
+  for (int i = lane; i < TE * NF * CH; i += 32) {
+    const int lf = i / CH, c = i % CH;
+    const int el = lf / NF, f = lf % NF;
+    const int nb = nbr[lf];
     const bool v = el < ne && nb >= 0;
-    const int fr = (st.code[el] >> (8 * (lf % NF))) & 3;
-    cp_async(dst + i, v ? trace + ((size_t)nb * NF + fr) * TR + k : trace, v);
+    const int fr = (code[el] >> (8 * f)) & 3;
+    cp16(st + X::SNB + lf * TR + c * VPC, v ? trace + ((size_t)nb * NF + fr) * TR + c * VPC : trace, v ? 16 : 0);
   }
 }
 
-// grad_ref (M1 rows, 8 columns) = A1 x B(8 x K1): all M-tiles in one k-loop.
-template <typename T, int DIM, int P>
-__device__ __forceinline__ void gemm1(const T* A1, const T* Bs, int ldb, T* Cs, int lane) {
-  using TC = TcCfg<T, DIM, P>;
-  using M = Mma<T>;
-  constexpr int NMT = TC::M1 / M::MT;
-  T c[NMT][M::NC];
-#pragma unroll
-  for (int m = 0; m < NMT; ++m)
-#pragma unroll
-    for (int i = 0; i < M::NC; ++i) c[m][i] = T(0);
-#pragma unroll
-  for (int k0 = 0; k0 < TC::K1; k0 += M::KT) {
-    typename M::B b;
-    M::load_b(b, Bs, ldb, k0, lane);
-#pragma unroll
-    for (int m = 0; m < NMT; ++m) {
-      typename M::A a;
-      M::load_a(a, A1, TC::LDA1, m * M::MT, k0, lane);
-      M::mma(c[m], a, b);
-    }
-  }
-#pragma unroll
-  for (int m = 0; m < NMT; ++m) M::store_c(c[m], Cs, TC::LDC, m * M::MT, lane);
-}
-
-// acc += A (M2 x K) * B(8 x K)
-template <typename T, int NMT, int K, int LDA, int LDB>
-__device__ __forceinline__ void gemm_acc(T (&c)[NMT][Mma<T>::NC], const T* A, const T* Bs, int lane) {
-  using M = Mma<T>;
-#pragma unroll 4
-  for (int k0 = 0; k0 < K; k0 += M::KT) {
-    typename M::B b;
-    M::load_b(b, Bs, LDB, k0, lane);
-#pragma unroll
-    for (int m = 0; m < NMT; ++m) {
-      typename M::A af;
-      M::load_a(af, A, LDA, m * M::MT, k0, lane);
-      M::mma(c[m], af, b);
-    }
-  }
-}
-
+// Outward unit normal, sJ and c_r = n . grad r of face f from the geometric factors g.
 template <typename T, int DIM>
 __device__ __forceinline__ void face_geom(const T* g, int f, T* out) {
   T n[3];
@@ -272,7 +202,7 @@ __device__ __forceinline__ void face_geom(const T* g, int f, T* out) {
       else v = -g[d];
       n[d] = v;
     }
-    T len = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+    const T len = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
     n[0] /= len; n[1] /= len; n[2] /= len;
     out[3] = len * g[9];
   } else {
@@ -285,7 +215,7 @@ __device__ __forceinline__ void face_geom(const T* g, int f, T* out) {
       n[d] = v;
     }
     n[2] = T(0);
-    T len = sqrt(n[0] * n[0] + n[1] * n[1]);
+    const T len = sqrt(n[0] * n[0] + n[1] * n[1]);
     n[0] /= len; n[1] /= len;
     out[3] = len * g[4];
   }
@@ -300,318 +230,454 @@ __device__ __forceinline__ void face_geom(const T* g, int f, T* out) {
   }
 }
 
-// Element geometry of padded tile slots is the identity map (finite normals).
-template <typename T, int DIM>
-__device__ __forceinline__ void pad_geometry(T* geo, int ne, int lane) {
-  constexpr int NG = DIM == 3 ? 10 : 5;
-  for (int i = lane + ne * NG; i < kEl * NG; i += 32) {
-    const int k = i % NG;
-    T v = T(0);
-    if (DIM == 3) v = (k == 0 || k == 4 || k == 8 || k == 9) ? T(1) : T(0);
-    else v = (k == 0 || k == 3 || k == 4) ? T(1) : T(0);
-    geo[i] = v;
+// Face geometry of a tile into sfg (zeros for padded element slots).
+template <typename T, int DIM, int P>
+__device__ __forceinline__ void tile_face_geom(const T* sg, T* sfg, int ne, int lane) {
+  using X = Tc<T, DIM, P>;
+  for (int i = lane; i < X::TE * X::NF; i += 32) {
+    const int el = i / X::NF, f = i % X::NF;
+    if (el < ne) {
+      face_geom<T, DIM>(sg + el * X::NG, f, sfg + i * X::FG);
+    } else {
+#pragma unroll
+      for (int q = 0; q < X::FG; ++q) sfg[i * X::FG + q] = T(0);
+    }
   }
+}
+
+// A blocks of x (TF32-rounded on the FP32 path): u[kb][ri][ci] = x[g + 8 ri][8 kb + 2t + ci].
+template <typename T, int DIM, int P>
+__device__ __forceinline__ void load_x_frags(const T* sx, T (&u)[Tc<T, DIM, P>::NT][Frag<T>::R][2], int g, int t) {
+  using X = Tc<T, DIM, P>;
+#pragma unroll
+  for (int kb = 0; kb < X::NT; ++kb)
+#pragma unroll
+    for (int ri = 0; ri < X::R; ++ri)
+#pragma unroll
+      for (int ci = 0; ci < 2; ++ci) {
+        const int k = 8 * kb + 2 * t + ci;
+        const T v = k < X::NP ? sx[(g + 8 * ri) * X::NP + k] : T(0);
+        u[kb][ri][ci] = Frag<T>::op(v);
+      }
 }
 
 // ---------------------------------------------------------------- pass 1
 template <typename T, int DIM, int P, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) sipg_trace_kernel(ApplyArgs<T> a, const T* __restrict__ tc_consts,
+__global__ void __launch_bounds__(WARPS * 32) sipg_trace_kernel(ApplyArgs<T> a, const T* __restrict__ blob,
                                                               T* __restrict__ trace) {
-  using TC = TcCfg<T, DIM, P>;
-  constexpr int NP = TC::NP, NFP = TC::NFP, NF = TC::NF, NG = TC::NG, FG = TC::FG;
+  using X = Tc<T, DIM, P>;
+  using F = Frag<T>;
+  constexpr int NP = X::NP, NFP = X::NFP, NF = X::NF, NT = X::NT, FT = X::FT, R = X::R, TE = X::TE, TR = X::TR,
+                KF = X::KF;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* A1 = reinterpret_cast<T*>(smem_raw);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  T* W = A1 + TC::CONST1 + warp * TC::W1_T;
-  int* I = reinterpret_cast<int*>(A1 + TC::CONST1 + WARPS * TC::W1_T) + warp * TC::W1_I;
-  int8_t* fmask = reinterpret_cast<int8_t*>(reinterpret_cast<int*>(A1 + TC::CONST1 + WARPS * TC::W1_T) +
-                                            WARPS * TC::W1_I);
-  T* sC = W + 2 * TC::ST_T;
-  T* sFG = sC + kEl * TC::LDC;
-  for (int i = threadIdx.x; i < TC::CONST1; i += blockDim.x) A1[i] = tc_consts[i];
-  for (int i = threadIdx.x; i < NF * NFP; i += blockDim.x) fmask[i] = a.itab[i];
-  const int ntiles = (a.K + kEl - 1) / kEl;
+  T* BFs = reinterpret_cast<T*>(smem_raw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  T* W = BFs + X::N1 + warp * X::W1_T;
+  int8_t* fmask = reinterpret_cast<int8_t*>(BFs + X::N1 + WARPS * X::W1_T);
+  T* sfg = W + 2 * X::ST1;
+  T* sout = sfg + X::SFG;
+  const int ntiles = (a.K + TE - 1) / TE;
   const int stride = gridDim.x * WARPS;
   int tile = blockIdx.x * WARPS + warp;
-  issue_own<T, DIM, P>(a, Stage<T, DIM, P>(W, I), tile, lane);
+  issue_elem<T, DIM, P>(a, trace, W, tile, lane, false);
   cp_commit();
+  for (int i = threadIdx.x; i < X::N1; i += blockDim.x) BFs[i] = blob[X::BF + i];
+  for (int i = threadIdx.x; i < NF * NFP; i += blockDim.x) fmask[i] = a.itab[i];
+  for (int i = lane; i < TE * NF * TR; i += 32) sout[i] = T(0);  // record padding stays zero
   __syncthreads();
   for (int it = 0; tile < ntiles; ++it, tile += stride) {
-    const int b = it & 1;
-    const Stage<T, DIM, P> S(W + b * TC::ST_T, I + b * TC::ST_I);
-    issue_own<T, DIM, P>(a, Stage<T, DIM, P>(W + (b ^ 1) * TC::ST_T, I + (b ^ 1) * TC::ST_I), tile + stride, lane);
+    T* st = W + (it & 1) * X::ST1;
+    cp_wait_all();
+    __syncwarp();
+    issue_elem<T, DIM, P>(a, trace, W + ((it & 1) ^ 1) * X::ST1, tile + stride, lane, false);
     cp_commit();
-    cp_wait<1>();
+    const int e0 = tile * TE;
+    const int ne = min(TE, a.K - e0);
+    T* sx = st + X::SX;
+    const T* sf = st + X::SF;
+    if (lane == 0 && a.pin_elem >= e0 && a.pin_elem < e0 + ne) sx[(a.pin_elem - e0) * NP + a.pin_node] = T(0);
+    tile_face_geom<T, DIM, P>(st + X::SG, sfg, ne, lane);
     __syncwarp();
-    const int e0 = tile * kEl;
-    const int ne = min(kEl, a.K - e0);
-    if (a.pin_elem >= e0 && a.pin_elem < e0 + ne && lane == 0) S.x[(a.pin_elem - e0) * NP + a.pin_node] = T(0);
-    pad_geometry<T, DIM>(S.geo, ne, lane);
-    __syncwarp();
-    if (lane < kEl * NF) face_geom<T, DIM>(S.geo + (lane / NF) * NG, lane % NF, sFG + lane * FG);
-    gemm1<T, DIM, P>(A1, S.x, NP, sC, lane);
-    __syncwarp();
-    // trace[e][f] = (x at the face nodes, f n.grad x at the face nodes)
-    for (int i = lane; i < ne * NF * NFP; i += 32) {
-      const int el = i / (NF * NFP), k = i % (NF * NFP);
-      const int f = k / NFP, j = k % NFP;
-      const int m = fmask[f * NFP + j];
-      const T* fg = sFG + (el * NF + f) * FG;
-      T s = T(0);
+    T u[NT][R][2];
+    load_x_frags<T, DIM, P>(sx, u, g, t);
 #pragma unroll
-      for (int r = 0; r < DIM; ++r) s += fg[4 + r] * sC[el * TC::LDC + r * NP + m];
-      const T fm = a.factor ? S.fac[el * NP + m] : T(1);
-      T* tr = trace + ((size_t)(e0 + el) * NF + f) * TC::TR;
-      tr[j] = S.x[el * NP + m];
-      tr[NFP + j] = fm * s;
+    for (int fb = 0; fb < FT; ++fb) {
+      T acc[DIM][R][2];
+#pragma unroll
+      for (int r = 0; r < DIM; ++r)
+#pragma unroll
+        for (int ri = 0; ri < R; ++ri) acc[r][ri][0] = acc[r][ri][1] = T(0);
+#pragma unroll
+      for (int kb = 0; kb < NT; ++kb)
+#pragma unroll
+        for (int r = 0; r < DIM; ++r) F::mma(acc[r], u[kb], ldb(BFs, (r * NT + kb) * FT + fb, lane));
+#pragma unroll
+      for (int ri = 0; ri < R; ++ri)
+#pragma unroll
+        for (int ci = 0; ci < 2; ++ci) {
+          const int k = 8 * fb + 2 * t + ci;
+          if (k < KF) {
+            const int el = g + 8 * ri;
+            const int f = k / NFP, j = k % NFP;
+            const int m = fmask[k];
+            const T* fg = sfg + (el * NF + f) * X::FG;
+            T s = T(0);
+#pragma unroll
+            for (int r = 0; r < DIM; ++r) s += fg[4 + r] * acc[r][ri][ci];
+            const T fm = a.factor ? sf[el * NP + m] : T(1);
+            T* rec = sout + (el * NF + f) * TR;
+            rec[j] = sx[el * NP + m];
+            rec[X::TRP + j] = fm * s;
+          }
+        }
+    }
+    __syncwarp();
+    // coalesced write-out of the tile's records
+    {
+      using V4 = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+      const V4* src = reinterpret_cast<const V4*>(sout);
+      V4* dst = reinterpret_cast<V4*>(trace + (size_t)e0 * NF * TR);
+      const int n = ne * NF * X::CH;
+      for (int i = lane; i < n; i += 32) dst[i] = src[i];
     }
     __syncwarp();
   }
-  cp_wait<0>();
+  cp_wait_all();
 }
 
 // ---------------------------------------------------------------- pass 2
 template <typename T, int DIM, int P, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) sipg_apply_tc_kernel(ApplyArgs<T> a, const T* __restrict__ tc_consts,
+__global__ void __launch_bounds__(WARPS * 32) sipg_apply_tc_kernel(ApplyArgs<T> a, const T* __restrict__ blob,
                                                                  const T* __restrict__ trace) {
-  using TC = TcCfg<T, DIM, P>;
-  using M = Mma<T>;
-  constexpr int NP = TC::NP, NFP = TC::NFP, NF = TC::NF, NFNFP = TC::NFNFP, NG = TC::NG, FG = TC::FG,
-                TR = TC::TR;
-  constexpr int NMT = TC::M2 / M::MT;
+  using X = Tc<T, DIM, P>;
+  using F = Frag<T>;
+  constexpr int NP = X::NP, NFP = X::NFP, NF = X::NF, NT = X::NT, FT = X::FT, R = X::R, TE = X::TE, TR = X::TR,
+                KF = X::KF, TRP = X::TRP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* A1 = reinterpret_cast<T*>(smem_raw);
-  T* A2a = A1 + TC::CONST1;
-  T* A2b = A2a + TC::M2 * TC::LDA2A;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  T* W = A1 + TC::CONST_T + warp * TC::W2_T;
-  int* ibase = reinterpret_cast<int*>(A1 + TC::CONST_T + WARPS * TC::W2_T);
-  int* I = ibase + warp * TC::W2_I;
-  int8_t* itab = reinterpret_cast<int8_t*>(ibase + WARPS * TC::W2_I);
+  T* B = reinterpret_cast<T*>(smem_raw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  T* W = B + X::N2 + warp * X::W2_T;
+  int* ibase = reinterpret_cast<int*>(B + X::N2 + WARPS * X::W2_T);
+  int* I = ibase + warp * X::W2_I;
+  int8_t* itab = reinterpret_cast<int8_t*>(ibase + WARPS * X::W2_I);
   const int8_t* fmask = itab;
   const int8_t* perm = itab + NF * NFP;
-  T* trb0 = W + 3 * TC::ST_T;
-  T* sB = W + 3 * TC::ST_T + 2 * TC::TRB;
-  T* sC = sB + kEl * TC::LDB;
-  T* sFG = sC + kEl * TC::LDC;
-  T* sS = sFG + kEl * NF * FG;
-  for (int i = threadIdx.x; i < TC::CONST_T; i += blockDim.x) A1[i] = tc_consts[i];
-  for (int i = threadIdx.x; i < Cfg<DIM, P>::ITAB; i += blockDim.x) itab[i] = a.itab[i];
-  const int ntiles = (a.K + kEl - 1) / kEl;
+  T* sfg = W + 2 * X::ST2;
+  const int ntiles = (a.K + TE - 1) / TE;
   const int stride = gridDim.x * WARPS;
   int tile = blockIdx.x * WARPS + warp;
-  // prologue: element data of tiles 0 and 1 in flight, traces of tile 0 behind them
-  issue_own<T, DIM, P>(a, Stage<T, DIM, P>(W, I), tile, lane);
+  // prologue: connectivity of the first two tiles, then the first tile's data and traces
+  issue_ints<T, DIM, P>(a, I, tile, lane);
+  issue_ints<T, DIM, P>(a, I + X::SI, tile + stride, lane);
   cp_commit();
-  issue_own<T, DIM, P>(a, Stage<T, DIM, P>(W + TC::ST_T, I + TC::ST_I), tile + stride, lane);
-  cp_commit();
-  cp_wait<1>();
+  for (int i = threadIdx.x; i < X::N2; i += blockDim.x) B[i] = blob[i];
+  for (int i = threadIdx.x; i < Cfg<DIM, P>::ITAB; i += blockDim.x) itab[i] = a.itab[i];
+  cp_wait_all();
   __syncwarp();
-  issue_traces<T, DIM, P>(a, Stage<T, DIM, P>(W, I), trace, trb0, tile, lane);
+  issue_elem<T, DIM, P>(a, trace, W, tile, lane, true);
+  issue_nb<T, DIM, P>(a, trace, W, I, tile, lane);
   cp_commit();
   __syncthreads();
-  int s0 = 0;  // stage of this tile; tile+1 in (s0+1)%3, tile+2 in (s0+2)%3
   for (int it = 0; tile < ntiles; ++it, tile += stride) {
-    const int s1 = s0 == 2 ? 0 : s0 + 1, s2 = s1 == 2 ? 0 : s1 + 1;
-    const Stage<T, DIM, P> S(W + s0 * TC::ST_T, I + s0 * TC::ST_I);
-    T* TRc = trb0 + (it & 1) * TC::TRB;
-    // element data of tile+1 and traces of tile have arrived
-    cp_wait<0>();
+    const int sb = it & 1, slot = it % 3;
+    T* st = W + sb * X::ST2;
+    const int* ints = I + slot * X::SI;
+    cp_wait_all();
     __syncwarp();
-    issue_traces<T, DIM, P>(a, Stage<T, DIM, P>(W + s1 * TC::ST_T, I + s1 * TC::ST_I), trace,
-                            trb0 + ((it + 1) & 1) * TC::TRB, tile + stride, lane);
-    issue_own<T, DIM, P>(a, Stage<T, DIM, P>(W + s2 * TC::ST_T, I + s2 * TC::ST_I), tile + 2 * stride, lane);
+    issue_ints<T, DIM, P>(a, I + ((it + 2) % 3) * X::SI, tile + 2 * stride, lane);
+    issue_elem<T, DIM, P>(a, trace, W + (sb ^ 1) * X::ST2, tile + stride, lane, true);
+    issue_nb<T, DIM, P>(a, trace, W + (sb ^ 1) * X::ST2, I + ((it + 1) % 3) * X::SI, tile + stride, lane);
     cp_commit();
-    s0 = s1;
-    const int e0 = tile * kEl;
-    const int ne = min(kEl, a.K - e0);
-    if (a.pin_elem >= e0 && a.pin_elem < e0 + ne && lane == 0) S.x[(a.pin_elem - e0) * NP + a.pin_node] = T(0);
-    pad_geometry<T, DIM>(S.geo, ne, lane);
+
+    const int e0 = tile * TE;
+    const int ne = min(TE, a.K - e0);
+    T* sx = st + X::SX;
+    const T* sf = st + X::SF;
+    const T* sg = st + X::SG;
+    const T* stau = st + X::STAU;
+    const T* sown = st + X::SOWN;
+    const T* snb = st + X::SNB;
+    const int* snbr = ints;
+    const int* scode = ints + TE * NF;
+    if (lane == 0 && a.pin_elem >= e0 && a.pin_elem < e0 + ne) sx[(a.pin_elem - e0) * NP + a.pin_node] = T(0);
+    tile_face_geom<T, DIM, P>(sg, sfg, ne, lane);
     __syncwarp();
-    if (lane < kEl * NF) face_geom<T, DIM>(S.geo + (lane / NF) * NG, lane % NF, sFG + lane * FG);
-    // ---- G1: own gradient in the reference directions
-    gemm1<T, DIM, P>(A1, S.x, NP, sC, lane);
-    __syncwarp();
-    // ---- chunk A: q~_r, Fu, J mm x
-    for (int i = lane; i < kEl * NP; i += 32) {
-      const int el = i / NP, m = i % NP;
-      const T* g = S.geo + el * NG;
-      const T J = g[DIM == 3 ? 9 : 4], f = a.factor ? S.fac[i] : T(1);
-      T gr[3], q[3];
+
+    // metric of the lane's elements: J and K = G G^T
+    T Jm[R], Km[R][DIM][DIM];
 #pragma unroll
-      for (int r = 0; r < DIM; ++r) gr[r] = sC[el * TC::LDC + r * NP + m];
+    for (int ri = 0; ri < R; ++ri) {
+      const T* ge = sg + (g + 8 * ri) * X::NG;
+      Jm[ri] = ge[DIM * DIM];
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) {
-        T sum = T(0);
+      for (int r = 0; r < DIM; ++r)
 #pragma unroll
-        for (int r = 0; r < DIM; ++r) sum += g[r * DIM + d] * gr[r];
-        q[d] = f * sum;
-      }
+        for (int s = r; s < DIM; ++s) {
+          T v = T(0);
 #pragma unroll
-      for (int r = 0; r < DIM; ++r) {
-        T sum = T(0);
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) sum += g[r * DIM + d] * q[d];
-        sB[el * TC::LDB + r * NP + m] = M::to_op(J * sum);
-      }
-      T mv = T(0);
-      if (a.mm_mode != MM_NONE && el < ne)
-        mv = J * (a.mm_mode == MM_SCALAR ? a.mm_scalar : a.mm[(size_t)e0 * NP + i]) * S.x[i];
-      sB[el * TC::LDB + TC::OMM + m] = M::to_op(mv);
+          for (int d = 0; d < DIM; ++d) v += ge[r * DIM + d] * ge[s * DIM + d];
+          Km[ri][r][s] = v;
+          Km[ri][s][r] = v;
+        }
     }
-    constexpr int PADA = TC::KA - TC::OMM - NP;
-    if (PADA > 0)
-      for (int i = lane; i < kEl * PADA; i += 32) {
-        const int el = i / (PADA > 0 ? PADA : 1), n = i % (PADA > 0 ? PADA : 1);
-        sB[el * TC::LDB + TC::OMM + NP + n] = T(0);
-      }
-    for (int i = lane; i < kEl * NFNFP; i += 32) {
-      const int el = i / NFNFP, k = i % NFNFP;
-      const int f = k / NFP, j = k % NFP;
-      const int lf = el * NF + f;
-      const T* fg = sFG + lf * FG;
-      const int m = fmask[f * NFP + j];
-      const T fm = a.factor ? S.fac[el * NP + m] : T(1);
-      T nq = T(0);
+
+    // gr_r = x . B1_r
+    T w[DIM][NT][R][2];
+    {
+      T u[NT][R][2];
+      load_x_frags<T, DIM, P>(sx, u, g, t);
 #pragma unroll
-      for (int r = 0; r < DIM; ++r) nq += fg[4 + r] * sC[el * TC::LDC + r * NP + m];
-      nq *= fm;
-      const int nb = S.nbr[lf];
-      const T um = S.x[el * NP + m];
-      T jump = T(0), navg = T(0);
-      if (el < ne) {
-        if (nb >= 0) {
-          const int kk = perm[((S.code[el] >> (8 * f + 2)) & 7) * NFP + j];
-          jump = um - TRc[lf * TR + kk];
-          navg = T(0.5) * (nq - TRc[lf * TR + NFP + kk]);
-        } else if (a.bct[-nb - 1] == BC_DIRICHLET) {
-          jump = T(2) * um;
-          navg = nq;
+      for (int r = 0; r < DIM; ++r)
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+          for (int ri = 0; ri < R; ++ri) w[r][nt][ri][0] = w[r][nt][ri][1] = T(0);
+#pragma unroll
+      for (int kb = 0; kb < NT; ++kb)
+#pragma unroll
+        for (int r = 0; r < DIM; ++r)
+#pragma unroll
+          for (int nt = 0; nt < NT; ++nt) F::mma(w[r][nt], u[kb], ldb(B + X::B1, (r * NT + kb) * NT + nt, lane));
+    }
+    // w_r = J f sum_s K_rs gr_s (A blocks of the next product)
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+      for (int ri = 0; ri < R; ++ri)
+#pragma unroll
+        for (int ci = 0; ci < 2; ++ci) {
+          const int m = 8 * nt + 2 * t + ci;
+          const int el = g + 8 * ri;
+          T fJ = Jm[ri];
+          if (a.factor) fJ *= m < NP ? sf[el * NP + m] : T(0);
+          T gr[DIM];
+#pragma unroll
+          for (int s = 0; s < DIM; ++s) gr[s] = w[s][nt][ri][ci];
+#pragma unroll
+          for (int r = 0; r < DIM; ++r) {
+            T v = T(0);
+#pragma unroll
+            for (int s = 0; s < DIM; ++s) v += Km[ri][r][s] * gr[s];
+            w[r][nt][ri][ci] = F::op(fJ * v);
+          }
+        }
+    // Z_r = w_r . M^T ; y = (J mm x) . M^T
+    T z[DIM][NT][R][2], y[NT][R][2];
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+      for (int ri = 0; ri < R; ++ri) {
+        y[nt][ri][0] = y[nt][ri][1] = T(0);
+#pragma unroll
+        for (int r = 0; r < DIM; ++r) z[r][nt][ri][0] = z[r][nt][ri][1] = T(0);
+      }
+    const bool has_mm = a.mm_mode != MM_NONE;
+#pragma unroll
+    for (int kb = 0; kb < NT; ++kb) {
+      T mx[R][2];
+      if (has_mm) {
+#pragma unroll
+        for (int ri = 0; ri < R; ++ri)
+#pragma unroll
+          for (int ci = 0; ci < 2; ++ci) {
+            const int el = g + 8 * ri, m = 8 * kb + 2 * t + ci;
+            T v = T(0);
+            if (m < NP && el < ne) {
+              const T mmv = a.mm_mode == MM_SCALAR ? a.mm_scalar : a.mm[(size_t)(e0 + el) * NP + m];
+              v = Jm[ri] * mmv * sx[el * NP + m];
+            }
+            mx[ri][ci] = F::op(v);
+          }
+      }
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt) {
+        const auto b = ldb(B + X::BM, kb * NT + nt, lane);
+#pragma unroll
+        for (int r = 0; r < DIM; ++r) F::mma(z[r][nt], w[r][kb], b);
+        if (has_mm) F::mma(y[nt], mx, b);
+      }
+    }
+    // face fluxes: y += Fu . EMAT^T ; Z_r += (c_r S) . EMAT^T
+#pragma unroll
+    for (int fb = 0; fb < FT; ++fb) {
+      T fu[R][2], sv[DIM][R][2];
+#pragma unroll
+      for (int ri = 0; ri < R; ++ri)
+#pragma unroll
+        for (int ci = 0; ci < 2; ++ci) {
+          const int el = g + 8 * ri, k = 8 * fb + 2 * t + ci;
+          T vfu = T(0), vs = T(0);
+          T cr[DIM];
+#pragma unroll
+          for (int r = 0; r < DIM; ++r) cr[r] = T(0);
+          if (k < KF && el < ne) {
+            const int f = k / NFP, j = k % NFP;
+            const int lf = el * NF + f;
+            const T* own = sown + lf * TR;
+            const T um = own[j], gm = own[TRP + j];
+            const int nb = snbr[lf];
+            T jump = T(0), navg = T(0);
+            if (nb >= 0) {
+              const int kk = perm[((scode[el] >> (8 * f + 2)) & 7) * NFP + j];
+              const T* rec = snb + lf * TR;
+              jump = um - rec[kk];
+              navg = T(0.5) * (gm - rec[TRP + kk]);
+            } else if (a.bct[-nb - 1] == BC_DIRICHLET) {
+              jump = T(2) * um;
+              navg = gm;
+            }
+            const T hj = T(0.5) * jump;
+            const T* fg = sfg + lf * X::FG;
+            const T sJ = fg[3];
+            const T fm = a.factor ? sf[el * NP + fmask[k]] : T(1);
+            vfu = sJ * (stau[lf] * hj - navg);
+            vs = -sJ * fm * hj;
+#pragma unroll
+            for (int r = 0; r < DIM; ++r) cr[r] = fg[4 + r];
+          }
+          fu[ri][ci] = F::op(vfu);
+#pragma unroll
+          for (int r = 0; r < DIM; ++r) sv[r][ri][ci] = F::op(cr[r] * vs);
+        }
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt) {
+        const auto b = ldb(B + X::BE, fb * NT + nt, lane);
+        F::mma(y[nt], fu, b);
+#pragma unroll
+        for (int r = 0; r < DIM; ++r) F::mma(z[r][nt], sv[r], b);
+      }
+    }
+    // y += sum_r Z_r . D_r
+#pragma unroll
+    for (int r = 0; r < DIM; ++r)
+#pragma unroll
+      for (int kb = 0; kb < NT; ++kb) {
+        T zr[R][2];
+#pragma unroll
+        for (int ri = 0; ri < R; ++ri) {
+          zr[ri][0] = F::op(z[r][kb][ri][0]);
+          zr[ri][1] = F::op(z[r][kb][ri][1]);
+        }
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt) F::mma(y[nt], zr, ldb(B + X::B3, (r * NT + kb) * NT + nt, lane));
+      }
+    // epilogue: pinned row, alpha / beta, store
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+      for (int ri = 0; ri < R; ++ri) {
+        const int el = g + 8 * ri;
+        if (el >= ne) continue;
+        const size_t row = (size_t)(e0 + el) * NP;
+#pragma unroll
+        for (int ci = 0; ci < 2; ++ci) {
+          const int n = 8 * nt + 2 * t + ci;
+          if (n >= NP) continue;
+          T acc = y[nt][ri][ci];
+          if (e0 + el == a.pin_elem && n == a.pin_node) acc = a.pin_scale * a.x[row + n];
+          acc *= a.alpha;
+          if (a.beta != T(0)) acc += a.beta * a.y[row + n];
+          a.y[row + n] = acc;
         }
       }
-      const T hj = T(0.5) * jump, sJ = fg[3];
-      sS[i] = sJ * fm * -hj;
-      sB[el * TC::LDB + TC::OFU + k] = M::to_op(sJ * (S.tau[lf] * hj - navg));
-    }
-    __syncwarp();
-    T c[NMT][M::NC];
-#pragma unroll
-    for (int m = 0; m < NMT; ++m)
-#pragma unroll
-      for (int q = 0; q < M::NC; ++q) c[m][q] = T(0);
-    gemm_acc<T, NMT, TC::KA, TC::LDA2A, TC::LDB>(c, A2a, sB, lane);
-    __syncwarp();
-    // ---- chunk B: F~_r = c_r(f) * sJ f (-[x]/2)
-    for (int i = lane; i < kEl * TC::KB; i += 32) {
-      const int el = i / TC::KB, col = i % TC::KB;
-      T v = T(0);
-      if (col < DIM * NFNFP) {
-        const int r = col / NFNFP, k = col % NFNFP;
-        v = sFG[(el * NF + k / NFP) * FG + 4 + r] * sS[el * NFNFP + k];
-      }
-      sB[el * TC::LDB + col] = M::to_op(v);
-    }
-    __syncwarp();
-    gemm_acc<T, NMT, TC::KB, TC::LDA2B, TC::LDB>(c, A2b, sB, lane);
-#pragma unroll
-    for (int m = 0; m < NMT; ++m) M::store_c(c[m], sC, TC::LDC, m * M::MT, lane);
-    __syncwarp();
-    for (int i = lane; i < ne * NP; i += 32) {
-      const int el = i / NP, m = i % NP;
-      const int e = e0 + el;
-      T acc = sC[el * TC::LDC + m];
-      const size_t yi = (size_t)e0 * NP + i;
-      if (e == a.pin_elem && m == a.pin_node) acc = a.pin_scale * a.x[yi];
-      acc *= a.alpha;
-      if (a.beta != T(0)) acc += a.beta * a.y[yi];
-      a.y[yi] = acc;
-    }
     __syncwarp();
   }
-  cp_wait<0>();
+  cp_wait_all();
 }
 
-constexpr int kSmemBudget = 220 * 1024;
+constexpr int kSmemBudget = 227 * 1024;
 
+template <typename T, int DIM, int P>
+constexpr size_t smem1(int w) {
+  using X = Tc<T, DIM, P>;
+  return (size_t)(X::N1 + w * X::W1_T) * sizeof(T) + X::NF * X::NFP;
+}
+template <typename T, int DIM, int P>
+constexpr size_t smem2(int w) {
+  using X = Tc<T, DIM, P>;
+  return (size_t)(X::N2 + w * X::W2_T) * sizeof(T) + (size_t)w * X::W2_I * 4 + Cfg<DIM, P>::ITAB;
+}
 template <typename T, int DIM, int P>
 constexpr int warps1() {
-  using TC = TcCfg<T, DIM, P>;
-  return std::max(1, std::min(16, (int)((kSmemBudget - TC::CONST1 * (int)sizeof(T) - 64) /
-                                        (TC::W1_T * (int)sizeof(T) + TC::W1_I * 4))));
+  int w = 16;
+  while (w > 1 && smem1<T, DIM, P>(w) > (size_t)kSmemBudget) --w;
+  return w;
 }
-// 0 when the constants leave no room for a warp tile
+// 0 when not even one warp tile fits next to the constants
 template <typename T, int DIM, int P>
 constexpr int warps2() {
-  using TC = TcCfg<T, DIM, P>;
-  return std::min(16, (int)((kSmemBudget - TC::CONST_T * (int)sizeof(T) - 256) /
-                            (TC::W2_T * (int)sizeof(T) + TC::W2_I * 4)));
+  int w = 16;
+  while (w > 0 && smem2<T, DIM, P>(w) > (size_t)kSmemBudget) --w;
+  return w;
 }
 
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
 template <typename T, int DIM, int P>
-cudaError_t launch_tc_t(const ApplyArgs<T>& a, const T* tc_consts, T* trace, int num_sms, cudaStream_t s) {
-  using TC = TcCfg<T, DIM, P>;
-  constexpr int WA = warps1<T, DIM, P>(), WB = warps2<T, DIM, P>() < 1 ? 1 : warps2<T, DIM, P>();
-  if (warps2<T, DIM, P>() < 1) return cudaErrorInvalidConfiguration;
-  const int ntiles = (a.K + kEl - 1) / kEl;
+cudaError_t launch_tc_t(const ApplyArgs<T>& a, const T* blob, T* trace, int num_sms, cudaStream_t s) {
+  constexpr int WA = warps1<T, DIM, P>(), W2 = warps2<T, DIM, P>(), WB = W2 < 1 ? 1 : W2;
+  if (W2 < 1) return cudaErrorInvalidConfiguration;
+  using X = Tc<T, DIM, P>;
+  // the kernels copy caller vectors in 16-byte pieces: other alignments take the CUDA-core kernel
+  if (!aligned16(a.x) || !aligned16(a.y) || !aligned16(trace) || (a.factor && !aligned16(a.factor)))
+    return launch_apply<T>(DIM, P, a, num_sms, s);
+  const int ntiles = (a.K + X::TE - 1) / X::TE;
   {
     auto k = sipg_trace_kernel<T, DIM, P, WA>;
-    size_t bytes = (size_t)(TC::CONST1 + WA * TC::W1_T) * sizeof(T) + (size_t)WA * TC::W1_I * 4 + TC::NF * TC::NFP;
+    const size_t bytes = smem1<T, DIM, P>(WA);
     cudaError_t err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (err != cudaSuccess) return err;
     int per_sm = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, WA * 32, bytes);
-    int grid = std::min((ntiles + WA - 1) / WA, num_sms * std::max(per_sm, 1));
+    const int grid = std::min((ntiles + WA - 1) / WA, num_sms * std::max(per_sm, 1));
     if (grid > 0) {
-      k<<<grid, WA * 32, bytes, s>>>(a, tc_consts, trace);
+      k<<<grid, WA * 32, bytes, s>>>(a, blob, trace);
       note_launch();
     }
   }
   {
     auto k = sipg_apply_tc_kernel<T, DIM, P, WB>;
-    size_t bytes = (size_t)(TC::CONST_T + WB * TC::W2_T) * sizeof(T) + (size_t)WB * TC::W2_I * 4 +
-                   Cfg<DIM, P>::ITAB;
+    const size_t bytes = smem2<T, DIM, P>(WB);
     cudaError_t err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (err != cudaSuccess) return err;
     int per_sm = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, WB * 32, bytes);
-    int grid = std::min((ntiles + WB - 1) / WB, num_sms * std::max(per_sm, 1));
+    const int grid = std::min((ntiles + WB - 1) / WB, num_sms * std::max(per_sm, 1));
     if (grid > 0) {
-      k<<<grid, WB * 32, bytes, s>>>(a, tc_consts, trace);
+      k<<<grid, WB * 32, bytes, s>>>(a, blob, trace);
       note_launch();
     }
   }
   return cudaGetLastError();
 }
 
-// Host construction of the constant blob (A1 | A2a | A2b) in FP64.
+// Host construction of the constant blob in fragment order (FP64 values).
 template <typename T, int DIM, int P>
 void build_tc_consts_t(const RefElement& r, std::vector<double>& out) {
-  using TC = TcCfg<T, DIM, P>;
-  constexpr int NP = TC::NP, NFNFP = TC::NFNFP;
-  out.assign(TC::CONST_T, 0.0);
+  using X = Tc<T, DIM, P>;
+  constexpr int NP = X::NP, NT = X::NT, FT = X::FT, KF = X::KF;
+  out.assign(X::NALL, 0.0);
+  // entry (row, col) of a logical matrix stored as 8 x 8 blocks, nblk_n blocks per block row
+  auto put = [&](int base, int nblk_n, int row, int col, double v) {
+    const int kb = row / 8, kr = row % 8, nt = col / 8, gg = col % 8;
+    const int lane = gg * 4 + kr / 2;
+    out[(size_t)base + ((size_t)(kb * nblk_n + nt) * 32 + lane) * 2 + (kr % 2)] = v;
+  };
   const double* D[3] = {r.Dr.data(), r.Ds.data(), r.Dt.data()};
-  double* A1 = out.data();
-  double* A2a = A1 + TC::CONST1;
-  double* A2b = A2a + TC::M2 * TC::LDA2A;
   for (int rr = 0; rr < DIM; ++rr)
     for (int m = 0; m < NP; ++m)
-      for (int n = 0; n < NP; ++n) A1[(rr * NP + m) * TC::LDA1 + n] = D[rr][m * NP + n];
-  for (int n = 0; n < NP; ++n) {
-    for (int rr = 0; rr < DIM; ++rr) {
-      for (int m = 0; m < NP; ++m) {
-        double s = 0.0;
-        for (int i = 0; i < NP; ++i) s += D[rr][i * NP + n] * r.M[i * NP + m];
-        A2a[n * TC::LDA2A + rr * NP + m] = s;
+      for (int n = 0; n < NP; ++n) {
+        put(X::B1 + rr * NT * NT * X::BLK, NT, n, m, D[rr][m * NP + n]);  // B1_r[n][m] = D_r[m][n]
+        put(X::B3 + rr * NT * NT * X::BLK, NT, m, n, D[rr][m * NP + n]);  // B3_r[m][n] = D_r[m][n]
       }
-      for (int c = 0; c < NFNFP; ++c) {
-        double s = 0.0;
-        for (int i = 0; i < NP; ++i) s += D[rr][i * NP + n] * r.EMAT[i * NFNFP + c];
-        A2b[n * TC::LDA2B + rr * NFNFP + c] = s;
-      }
-    }
-    for (int c = 0; c < NFNFP; ++c) A2a[n * TC::LDA2A + TC::OFU + c] = r.EMAT[n * NFNFP + c];
-    for (int m = 0; m < NP; ++m) A2a[n * TC::LDA2A + TC::OMM + m] = r.M[n * NP + m];
-  }
+  for (int m = 0; m < NP; ++m)
+    for (int n = 0; n < NP; ++n) put(X::BM, NT, m, n, r.M[n * NP + m]);     // BM[m][n] = M[n][m]
+  for (int k = 0; k < KF; ++k)
+    for (int n = 0; n < NP; ++n) put(X::BE, NT, k, n, r.EMAT[n * KF + k]);  // BE[k][n] = EMAT[n][k]
+  for (int rr = 0; rr < DIM; ++rr)
+    for (int n = 0; n < NP; ++n)
+      for (int k = 0; k < KF; ++k)
+        put(X::BF + rr * NT * FT * X::BLK, FT, n, k, D[rr][r.fmask[k] * NP + n]);  // BF_r[n][k] = D_r[m(k)][n]
 }
 
 }  // namespace
@@ -648,7 +714,8 @@ int tc_warps_for(int dim, int order) {
 }
 
 size_t tc_trace_values(int dim, int order, int K) {
-  return (size_t)K * (dim + 1) * 2 * nfp_of(dim, order);
+  const int trp = rup(nfp_of(dim, order), 2);
+  return (size_t)K * (dim + 1) * rup(2 * trp, 4);
 }
 
 template cudaError_t launch_apply_tc<float>(int, int, const ApplyArgs<float>&, const float*, float*, int,
