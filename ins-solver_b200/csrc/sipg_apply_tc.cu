@@ -87,6 +87,11 @@ struct Frag<double> {
   }
 };
 
+// Smallest m >= n with m = 8 (mod 16): row stride of staged element data for
+// which the pair loads of a fragment (two adjacent columns per lane, element
+// rows g) fall in distinct banks.
+__host__ __device__ constexpr int pad816(int n) { return n <= 8 ? 8 : rup(n - 8, 16) + 8; }
+
 template <typename T, int DIM, int P>
 struct Tc {
   using C = Cfg<DIM, P>;
@@ -107,15 +112,20 @@ struct Tc {
   static constexpr int BF = N2;
   static constexpr int N1 = DIM * NT * FT * BLK;
   static constexpr int NALL = N2 + N1;
-  // element stage (T units; every part is a multiple of 64 bytes)
-  static constexpr int SX = 0, SF = TE * NP, SG = 2 * TE * NP, STAU = SG + TE * NG;
-  static constexpr int SOWN = STAU + TE * NF, SNB = SOWN + TE * NF * TR, ST2 = SNB + TE * NF * TR;
+  static constexpr int XS = pad816(NP);              // staged row stride of x and factor
+  static constexpr int TS = pad816(NF * TR);         // staged row stride of an element's trace records
+  // copy piece of an x / factor row (rows start on multiples of Np values)
+  static constexpr int XCB = (NP * (int)sizeof(T)) % 16 == 0 ? 16 : (NP * (int)sizeof(T)) % 8 == 0 ? 8 : 4;
+  // element stage (double-buffered; T units, every part a multiple of 64 bytes)
+  static constexpr int SX = 0, SF = TE * XS, SG = 2 * TE * XS, STAU = SG + TE * NG, ST2 = STAU + TE * NF;
   static constexpr int ST1 = STAU;                   // pass 1: x, factor, geometry
-  static constexpr int FG = 8;                       // per element face: n (3), sJ, c_r (3)
-  static constexpr int SFG = TE * NF * FG;
+  static constexpr int NFG = 4;                      // per element face: sJ, c_r (3), stored [q][f][el]
+  static constexpr int SFG = NFG * NF * TE;
   static constexpr int SI = TE * NF + TE;            // int slot: nbr, face codes
-  static constexpr int W1_T = 2 * ST1 + SFG + TE * NF * TR;
-  static constexpr int W2_T = 2 * ST2 + SFG;
+  // pass 1 warp: 2 stages, face geometry, output records
+  static constexpr int W1_T = 2 * ST1 + SFG + TE * TS;
+  // pass 2 warp: 2 stages, own and neighbour trace records (one buffer each), face geometry
+  static constexpr int STR = 2 * ST2, SNB = STR + TE * TS, SFGO = SNB + TE * TS, W2_T = SFGO + SFG;
   static constexpr int W2_I = 3 * SI;
   static constexpr int CH = TR * (int)sizeof(T) / 16;  // 16-byte chunks per trace record
 };
@@ -124,14 +134,25 @@ template <typename T>
 __device__ __forceinline__ typename Frag<T>::V2 ldb(const T* blob, int blk, int lane) {
   return reinterpret_cast<const typename Frag<T>::V2*>(blob)[blk * 32 + lane];
 }
+template <typename T>
+__device__ __forceinline__ typename Frag<T>::V2 ld2(const T* p) {
+  return *reinterpret_cast<const typename Frag<T>::V2*>(p);
+}
 
-// 16-byte asynchronous copy, zero-filled past `bytes` (0..16).
-__device__ __forceinline__ void cp16(void* sdst, const void* gsrc, int bytes) {
+// CB-byte asynchronous copy (4, 8 or 16), zero-filled past `bytes`.
+template <int CB>
+__device__ __forceinline__ void cp_async_n(void* sdst, const void* gsrc, int bytes) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gsrc), "r"(bytes));
+  if (CB == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gsrc), "r"(bytes));
+  else if (CB == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gsrc), "r"(bytes));
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gsrc), "r"(bytes));
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
+__device__ __forceinline__ void cp_wait_but_one() { asm volatile("cp.async.wait_group 1;\n" ::); }
 
 // Copy `total` bytes (a multiple of 16) to shared memory: the first `valid`
 // come from base + off (16-byte aligned), the rest is zero.
@@ -139,24 +160,34 @@ __device__ __forceinline__ void copy_block(void* s, const void* base, size_t off
   const char* b = static_cast<const char*>(base);
   for (int c = lane * 16; c < total; c += 32 * 16) {
     const int n = min(16, max(0, valid - c));
-    cp16(static_cast<char*>(s) + c, n > 0 ? b + off + c : b, n);
+    cp_async_n<16>(static_cast<char*>(s) + c, n > 0 ? b + off + c : b, n);
+  }
+}
+
+// Rows r < nrows of LEN values (global rows contiguous from row0) into shared
+// rows of stride DS; rows at or past nvalid are zero-filled (zero) or skipped.
+template <typename T, int CB, int LEN, int DS>
+__device__ __forceinline__ void copy_rows(T* dst, const T* base, size_t row0, int nrows, int nvalid, int lane,
+                                          bool zero) {
+  constexpr int V = CB / (int)sizeof(T), CPR = LEN / V;
+  static_assert(LEN % V == 0, "row length must be a multiple of the copy piece");
+  for (int i = lane; i < nrows * CPR; i += 32) {
+    const int r = i / CPR, c = i % CPR;
+    const bool v = r < nvalid;
+    if (v || zero) cp_async_n<CB>(dst + r * DS + c * V, v ? base + (row0 + r) * LEN + c * V : base, v ? CB : 0);
   }
 }
 
 template <typename T, int DIM, int P>
-__device__ __forceinline__ void issue_elem(const ApplyArgs<T>& a, const T* trace, T* st, int tile, int lane,
-                                           bool pass2) {
+__device__ __forceinline__ void issue_elem(const ApplyArgs<T>& a, T* st, int tile, int lane, bool pass2) {
   using X = Tc<T, DIM, P>;
   constexpr int NP = X::NP, NG = X::NG, NF = X::NF, TE = X::TE, S = sizeof(T);
   const int e0 = tile * TE;
   const int ne = max(0, min(TE, a.K - e0));
-  copy_block(st + X::SX, a.x, (size_t)e0 * NP * S, TE * NP * S, ne * NP * S, lane);
-  if (a.factor) copy_block(st + X::SF, a.factor, (size_t)e0 * NP * S, TE * NP * S, ne * NP * S, lane);
+  copy_rows<T, X::XCB, NP, X::XS>(st + X::SX, a.x, (size_t)e0, TE, ne, lane, true);
+  if (a.factor) copy_rows<T, X::XCB, NP, X::XS>(st + X::SF, a.factor, (size_t)e0, TE, ne, lane, true);
   copy_block(st + X::SG, a.geof, (size_t)e0 * NG * S, TE * NG * S, ne * NG * S, lane);
-  if (pass2) {
-    copy_block(st + X::STAU, a.tau, (size_t)e0 * NF * S, TE * NF * S, ne * NF * S, lane);
-    copy_block(st + X::SOWN, trace, (size_t)e0 * NF * X::TR * S, TE * NF * X::TR * S, ne * NF * X::TR * S, lane);
-  }
+  if (pass2) copy_block(st + X::STAU, a.tau, (size_t)e0 * NF * S, TE * NF * S, ne * NF * S, lane);
 }
 
 template <typename T, int DIM, int P>
@@ -169,28 +200,32 @@ __device__ __forceinline__ void issue_ints(const ApplyArgs<T>& a, int* slot, int
   copy_block(slot + TE * NF, a.fcode, (size_t)e0 * 4, TE * 4, ne * 4, lane);
 }
 
-// Neighbour trace records of a tile whose connectivity has arrived.
+// Own and neighbour trace records of a tile whose connectivity has arrived
+// (records that are never read are not copied).
 template <typename T, int DIM, int P>
-__device__ __forceinline__ void issue_nb(const ApplyArgs<T>& a, const T* trace, T* st, const int* slot, int tile,
-                                         int lane) {
+__device__ __forceinline__ void issue_traces(const ApplyArgs<T>& a, const T* trace, T* w, const int* slot, int tile,
+                                             int lane) {
   using X = Tc<T, DIM, P>;
-  constexpr int NF = X::NF, TE = X::TE, CH = X::CH, TR = X::TR, VPC = 16 / sizeof(T);
-  const int ne = max(0, min(TE, a.K - tile * TE));
+  constexpr int NF = X::NF, TE = X::TE, CH = X::CH, TR = X::TR, TS = X::TS, VPC = 16 / sizeof(T);
+  const int e0 = tile * TE;
+  const int ne = max(0, min(TE, a.K - e0));
+  copy_rows<T, 16, NF * TR, TS>(w + X::STR, trace, (size_t)e0, TE, ne, lane, false);
   const int* nbr = slot;
   const int* code = slot + TE * NF;
   for (int i = lane; i < TE * NF * CH; i += 32) {
     const int lf = i / CH, c = i % CH;
     const int el = lf / NF, f = lf % NF;
     const int nb = nbr[lf];
-    const bool v = el < ne && nb >= 0;
-    const int fr = (code[el] >> (8 * f)) & 3;
-    cp16(st + X::SNB + lf * TR + c * VPC, v ? trace + ((size_t)nb * NF + fr) * TR + c * VPC : trace, v ? 16 : 0);
+    if (el < ne && nb >= 0) {
+      const int fr = (code[el] >> (8 * f)) & 3;
+      cp_async_n<16>(w + X::SNB + el * TS + f * TR + c * VPC, trace + ((size_t)nb * NF + fr) * TR + c * VPC, 16);
+    }
   }
 }
 
-// Outward unit normal, sJ and c_r = n . grad r of face f from the geometric factors g.
+// sJ and c_r = n . grad r of face f (n the outward unit normal) from the geometric factors g.
 template <typename T, int DIM>
-__device__ __forceinline__ void face_geom(const T* g, int f, T* out) {
+__device__ __forceinline__ void face_geom(const T* g, int f, T& sJ, T (&c)[3]) {
   T n[3];
   if (DIM == 3) {
 #pragma unroll
@@ -204,7 +239,7 @@ __device__ __forceinline__ void face_geom(const T* g, int f, T* out) {
     }
     const T len = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
     n[0] /= len; n[1] /= len; n[2] /= len;
-    out[3] = len * g[9];
+    sJ = len * g[9];
   } else {
 #pragma unroll
     for (int d = 0; d < 2; ++d) {
@@ -217,58 +252,62 @@ __device__ __forceinline__ void face_geom(const T* g, int f, T* out) {
     n[2] = T(0);
     const T len = sqrt(n[0] * n[0] + n[1] * n[1]);
     n[0] /= len; n[1] /= len;
-    out[3] = len * g[4];
+    sJ = len * g[4];
   }
-  out[0] = n[0]; out[1] = n[1]; out[2] = n[2];
 #pragma unroll
   for (int r = 0; r < 3; ++r) {
     T cr = T(0);
     if (r < DIM)
 #pragma unroll
       for (int d = 0; d < DIM; ++d) cr += n[d] * g[r * DIM + d];
-    out[4 + r] = cr;
+    c[r] = cr;
   }
 }
 
-// Face geometry of a tile into sfg (zeros for padded element slots).
+// Face geometry of a tile into sfg[q][f][el] (q: sJ, c_0, c_1, c_2; zeros for padded slots).
 template <typename T, int DIM, int P>
 __device__ __forceinline__ void tile_face_geom(const T* sg, T* sfg, int ne, int lane) {
   using X = Tc<T, DIM, P>;
-  for (int i = lane; i < X::TE * X::NF; i += 32) {
-    const int el = i / X::NF, f = i % X::NF;
-    if (el < ne) {
-      face_geom<T, DIM>(sg + el * X::NG, f, sfg + i * X::FG);
-    } else {
+  constexpr int NF = X::NF, TE = X::TE;
+  for (int i = lane; i < TE * NF; i += 32) {
+    const int el = i / NF, f = i % NF;
+    T sJ = T(0), c[3] = {T(0), T(0), T(0)};
+    if (el < ne) face_geom<T, DIM>(sg + el * X::NG, f, sJ, c);
+    sfg[f * TE + el] = sJ;
 #pragma unroll
-      for (int q = 0; q < X::FG; ++q) sfg[i * X::FG + q] = T(0);
-    }
+    for (int r = 0; r < 3; ++r) sfg[((1 + r) * NF + f) * TE + el] = c[r];
   }
 }
+template <typename T, int DIM, int P>
+__device__ __forceinline__ T fgeo(const T* sfg, int q, int f, int el) {
+  using X = Tc<T, DIM, P>;
+  return sfg[(q * X::NF + f) * X::TE + el];
+}
 
-// A blocks of x (TF32-rounded on the FP32 path): u[kb][ri][ci] = x[g + 8 ri][8 kb + 2t + ci].
+// A blocks of x (TF32-rounded on the FP32 path): u[kb][ri][ci] = x[g + 8 ri][8 kb + 2t + ci]
+// (staged rows are zero past Np).
 template <typename T, int DIM, int P>
 __device__ __forceinline__ void load_x_frags(const T* sx, T (&u)[Tc<T, DIM, P>::NT][Frag<T>::R][2], int g, int t) {
   using X = Tc<T, DIM, P>;
 #pragma unroll
   for (int kb = 0; kb < X::NT; ++kb)
 #pragma unroll
-    for (int ri = 0; ri < X::R; ++ri)
-#pragma unroll
-      for (int ci = 0; ci < 2; ++ci) {
-        const int k = 8 * kb + 2 * t + ci;
-        const T v = k < X::NP ? sx[(g + 8 * ri) * X::NP + k] : T(0);
-        u[kb][ri][ci] = Frag<T>::op(v);
-      }
+    for (int ri = 0; ri < X::R; ++ri) {
+      const auto v = ld2(sx + (g + 8 * ri) * X::XS + 8 * kb + 2 * t);
+      u[kb][ri][0] = Frag<T>::op(v.x);
+      u[kb][ri][1] = Frag<T>::op(v.y);
+    }
 }
 
 // ---------------------------------------------------------------- pass 1
 template <typename T, int DIM, int P, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) sipg_trace_kernel(ApplyArgs<T> a, const T* __restrict__ blob,
-                                                              T* __restrict__ trace) {
+__global__ void __launch_bounds__(WARPS * 32, 1) sipg_trace_kernel(ApplyArgs<T> a, const T* __restrict__ blob,
+                                                                 T* __restrict__ trace) {
   using X = Tc<T, DIM, P>;
   using F = Frag<T>;
-  constexpr int NP = X::NP, NFP = X::NFP, NF = X::NF, NT = X::NT, FT = X::FT, R = X::R, TE = X::TE, TR = X::TR,
-                KF = X::KF;
+  using V2 = typename F::V2;
+  constexpr int NFP = X::NFP, NF = X::NF, NT = X::NT, FT = X::FT, R = X::R, TE = X::TE, TR = X::TR, KF = X::KF,
+                XS = X::XS, TS = X::TS, TRP = X::TRP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* BFs = reinterpret_cast<T*>(smem_raw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
@@ -279,23 +318,24 @@ __global__ void __launch_bounds__(WARPS * 32) sipg_trace_kernel(ApplyArgs<T> a, 
   const int ntiles = (a.K + TE - 1) / TE;
   const int stride = gridDim.x * WARPS;
   int tile = blockIdx.x * WARPS + warp;
-  issue_elem<T, DIM, P>(a, trace, W, tile, lane, false);
+  for (int i = lane; i < X::W1_T; i += 32) W[i] = T(0);  // row and record padding stays zero
+  __syncwarp();
+  issue_elem<T, DIM, P>(a, W, tile, lane, false);
   cp_commit();
   for (int i = threadIdx.x; i < X::N1; i += blockDim.x) BFs[i] = blob[X::BF + i];
   for (int i = threadIdx.x; i < NF * NFP; i += blockDim.x) fmask[i] = a.itab[i];
-  for (int i = lane; i < TE * NF * TR; i += 32) sout[i] = T(0);  // record padding stays zero
   __syncthreads();
   for (int it = 0; tile < ntiles; ++it, tile += stride) {
     T* st = W + (it & 1) * X::ST1;
     cp_wait_all();
     __syncwarp();
-    issue_elem<T, DIM, P>(a, trace, W + ((it & 1) ^ 1) * X::ST1, tile + stride, lane, false);
+    issue_elem<T, DIM, P>(a, W + ((it & 1) ^ 1) * X::ST1, tile + stride, lane, false);
     cp_commit();
     const int e0 = tile * TE;
     const int ne = min(TE, a.K - e0);
     T* sx = st + X::SX;
     const T* sf = st + X::SF;
-    if (lane == 0 && a.pin_elem >= e0 && a.pin_elem < e0 + ne) sx[(a.pin_elem - e0) * NP + a.pin_node] = T(0);
+    if (lane == 0 && a.pin_elem >= e0 && a.pin_elem < e0 + ne) sx[(a.pin_elem - e0) * XS + a.pin_node] = T(0);
     tile_face_geom<T, DIM, P>(st + X::SG, sfg, ne, lane);
     __syncwarp();
     T u[NT][R][2];
@@ -311,34 +351,61 @@ __global__ void __launch_bounds__(WARPS * 32) sipg_trace_kernel(ApplyArgs<T> a, 
       for (int kb = 0; kb < NT; ++kb)
 #pragma unroll
         for (int r = 0; r < DIM; ++r) F::mma(acc[r], u[kb], ldb(BFs, (r * NT + kb) * FT + fb, lane));
+      if constexpr (NFP % 2 == 0) {
+        // the two columns of a lane lie on one face
+        const int k0 = 8 * fb + 2 * t;
+        if (k0 < KF) {
+          const int f = k0 / NFP, j0 = k0 % NFP;
+          const int m0 = fmask[k0], m1 = fmask[k0 + 1];
 #pragma unroll
-      for (int ri = 0; ri < R; ++ri)
-#pragma unroll
-        for (int ci = 0; ci < 2; ++ci) {
-          const int k = 8 * fb + 2 * t + ci;
-          if (k < KF) {
+          for (int ri = 0; ri < R; ++ri) {
             const int el = g + 8 * ri;
-            const int f = k / NFP, j = k % NFP;
-            const int m = fmask[k];
-            const T* fg = sfg + (el * NF + f) * X::FG;
-            T s = T(0);
+            T s0 = T(0), s1 = T(0);
 #pragma unroll
-            for (int r = 0; r < DIM; ++r) s += fg[4 + r] * acc[r][ri][ci];
-            const T fm = a.factor ? sf[el * NP + m] : T(1);
-            T* rec = sout + (el * NF + f) * TR;
-            rec[j] = sx[el * NP + m];
-            rec[X::TRP + j] = fm * s;
+            for (int r = 0; r < DIM; ++r) {
+              const T c = fgeo<T, DIM, P>(sfg, 1 + r, f, el);
+              s0 += c * acc[r][ri][0];
+              s1 += c * acc[r][ri][1];
+            }
+            const T* xr = sx + el * XS;
+            const T fm0 = a.factor ? sf[el * XS + m0] : T(1), fm1 = a.factor ? sf[el * XS + m1] : T(1);
+            T* rec = sout + el * TS + f * TR;
+            *reinterpret_cast<V2*>(rec + j0) = V2{xr[m0], xr[m1]};
+            *reinterpret_cast<V2*>(rec + TRP + j0) = V2{fm0 * s0, fm1 * s1};
           }
         }
+      } else {
+#pragma unroll
+        for (int ri = 0; ri < R; ++ri)
+#pragma unroll
+          for (int ci = 0; ci < 2; ++ci) {
+            const int k = 8 * fb + 2 * t + ci;
+            if (k < KF) {
+              const int el = g + 8 * ri;
+              const int f = k / NFP, j = k % NFP;
+              const int m = fmask[k];
+              T s = T(0);
+#pragma unroll
+              for (int r = 0; r < DIM; ++r) s += fgeo<T, DIM, P>(sfg, 1 + r, f, el) * acc[r][ri][ci];
+              const T fm = a.factor ? sf[el * XS + m] : T(1);
+              T* rec = sout + el * TS + f * TR;
+              rec[j] = sx[el * XS + m];
+              rec[TRP + j] = fm * s;
+            }
+          }
+      }
     }
     __syncwarp();
     // coalesced write-out of the tile's records
     {
       using V4 = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
-      const V4* src = reinterpret_cast<const V4*>(sout);
-      V4* dst = reinterpret_cast<V4*>(trace + (size_t)e0 * NF * TR);
-      const int n = ne * NF * X::CH;
-      for (int i = lane; i < n; i += 32) dst[i] = src[i];
+      constexpr int VPC = 16 / sizeof(T), CPE = NF * X::CH;
+      const int n = ne * CPE;
+      for (int i = lane; i < n; i += 32) {
+        const int el = i / CPE, c = i % CPE;
+        *reinterpret_cast<V4*>(trace + (size_t)(e0 + el) * NF * TR + c * VPC) =
+            *reinterpret_cast<const V4*>(sout + el * TS + c * VPC);
+      }
     }
     __syncwarp();
   }
@@ -347,12 +414,12 @@ __global__ void __launch_bounds__(WARPS * 32) sipg_trace_kernel(ApplyArgs<T> a, 
 
 // ---------------------------------------------------------------- pass 2
 template <typename T, int DIM, int P, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) sipg_apply_tc_kernel(ApplyArgs<T> a, const T* __restrict__ blob,
-                                                                 const T* __restrict__ trace) {
+__global__ void __launch_bounds__(WARPS * 32, 1) sipg_apply_tc_kernel(ApplyArgs<T> a, const T* __restrict__ blob,
+                                                                    const T* __restrict__ trace) {
   using X = Tc<T, DIM, P>;
   using F = Frag<T>;
   constexpr int NP = X::NP, NFP = X::NFP, NF = X::NF, NT = X::NT, FT = X::FT, R = X::R, TE = X::TE, TR = X::TR,
-                KF = X::KF, TRP = X::TRP;
+                KF = X::KF, TRP = X::TRP, XS = X::XS, TS = X::TS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* B = reinterpret_cast<T*>(smem_raw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
@@ -362,31 +429,33 @@ __global__ void __launch_bounds__(WARPS * 32) sipg_apply_tc_kernel(ApplyArgs<T> 
   int8_t* itab = reinterpret_cast<int8_t*>(ibase + WARPS * X::W2_I);
   const int8_t* fmask = itab;
   const int8_t* perm = itab + NF * NFP;
-  T* sfg = W + 2 * X::ST2;
+  const T* str = W + X::STR;
+  const T* snb = W + X::SNB;
+  T* sfg = W + X::SFGO;
   const int ntiles = (a.K + TE - 1) / TE;
   const int stride = gridDim.x * WARPS;
   int tile = blockIdx.x * WARPS + warp;
-  // prologue: connectivity of the first two tiles, then the first tile's data and traces
+  for (int i = lane; i < X::W2_T; i += 32) W[i] = T(0);  // row padding stays zero
+  __syncwarp();
+  // prologue: connectivity of the first two tiles and the first tile's element data
   issue_ints<T, DIM, P>(a, I, tile, lane);
   issue_ints<T, DIM, P>(a, I + X::SI, tile + stride, lane);
+  issue_elem<T, DIM, P>(a, W, tile, lane, true);
   cp_commit();
   for (int i = threadIdx.x; i < X::N2; i += blockDim.x) B[i] = blob[i];
   for (int i = threadIdx.x; i < Cfg<DIM, P>::ITAB; i += blockDim.x) itab[i] = a.itab[i];
-  cp_wait_all();
-  __syncwarp();
-  issue_elem<T, DIM, P>(a, trace, W, tile, lane, true);
-  issue_nb<T, DIM, P>(a, trace, W, I, tile, lane);
-  cp_commit();
   __syncthreads();
   for (int it = 0; tile < ntiles; ++it, tile += stride) {
     const int sb = it & 1, slot = it % 3;
     T* st = W + sb * X::ST2;
     const int* ints = I + slot * X::SI;
+    // element data of this tile and connectivity of the next one have arrived
     cp_wait_all();
     __syncwarp();
+    issue_traces<T, DIM, P>(a, trace, W, ints, tile, lane);
+    cp_commit();
     issue_ints<T, DIM, P>(a, I + ((it + 2) % 3) * X::SI, tile + 2 * stride, lane);
-    issue_elem<T, DIM, P>(a, trace, W + (sb ^ 1) * X::ST2, tile + stride, lane, true);
-    issue_nb<T, DIM, P>(a, trace, W + (sb ^ 1) * X::ST2, I + ((it + 1) % 3) * X::SI, tile + stride, lane);
+    issue_elem<T, DIM, P>(a, W + (sb ^ 1) * X::ST2, tile + stride, lane, true);
     cp_commit();
 
     const int e0 = tile * TE;
@@ -395,11 +464,9 @@ __global__ void __launch_bounds__(WARPS * 32) sipg_apply_tc_kernel(ApplyArgs<T> 
     const T* sf = st + X::SF;
     const T* sg = st + X::SG;
     const T* stau = st + X::STAU;
-    const T* sown = st + X::SOWN;
-    const T* snb = st + X::SNB;
     const int* snbr = ints;
     const int* scode = ints + TE * NF;
-    if (lane == 0 && a.pin_elem >= e0 && a.pin_elem < e0 + ne) sx[(a.pin_elem - e0) * NP + a.pin_node] = T(0);
+    if (lane == 0 && a.pin_elem >= e0 && a.pin_elem < e0 + ne) sx[(a.pin_elem - e0) * XS + a.pin_node] = T(0);
     tile_face_geom<T, DIM, P>(sg, sfg, ne, lane);
     __syncwarp();
 
@@ -443,13 +510,16 @@ __global__ void __launch_bounds__(WARPS * 32) sipg_apply_tc_kernel(ApplyArgs<T> 
 #pragma unroll
     for (int nt = 0; nt < NT; ++nt)
 #pragma unroll
-      for (int ri = 0; ri < R; ++ri)
+      for (int ri = 0; ri < R; ++ri) {
+        const int el = g + 8 * ri;
+        T fJ[2] = {Jm[ri], Jm[ri]};
+        if (a.factor) {
+          const auto fv = ld2(sf + el * XS + 8 * nt + 2 * t);
+          fJ[0] *= fv.x;
+          fJ[1] *= fv.y;
+        }
 #pragma unroll
         for (int ci = 0; ci < 2; ++ci) {
-          const int m = 8 * nt + 2 * t + ci;
-          const int el = g + 8 * ri;
-          T fJ = Jm[ri];
-          if (a.factor) fJ *= m < NP ? sf[el * NP + m] : T(0);
           T gr[DIM];
 #pragma unroll
           for (int s = 0; s < DIM; ++s) gr[s] = w[s][nt][ri][ci];
@@ -458,9 +528,10 @@ __global__ void __launch_bounds__(WARPS * 32) sipg_apply_tc_kernel(ApplyArgs<T> 
             T v = T(0);
 #pragma unroll
             for (int s = 0; s < DIM; ++s) v += Km[ri][r][s] * gr[s];
-            w[r][nt][ri][ci] = F::op(fJ * v);
+            w[r][nt][ri][ci] = F::op(fJ[ci] * v);
           }
         }
+      }
     // Z_r = w_r . M^T ; y = (J mm x) . M^T
     T z[DIM][NT][R][2], y[NT][R][2];
 #pragma unroll
@@ -484,7 +555,7 @@ __global__ void __launch_bounds__(WARPS * 32) sipg_apply_tc_kernel(ApplyArgs<T> 
             T v = T(0);
             if (m < NP && el < ne) {
               const T mmv = a.mm_mode == MM_SCALAR ? a.mm_scalar : a.mm[(size_t)(e0 + el) * NP + m];
-              v = Jm[ri] * mmv * sx[el * NP + m];
+              v = Jm[ri] * mmv * sx[el * XS + m];
             }
             mx[ri][ci] = F::op(v);
           }
@@ -497,48 +568,101 @@ __global__ void __launch_bounds__(WARPS * 32) sipg_apply_tc_kernel(ApplyArgs<T> 
         if (has_mm) F::mma(y[nt], mx, b);
       }
     }
+    // the tile's trace records have arrived
+    cp_wait_but_one();
+    __syncwarp();
     // face fluxes: y += Fu . EMAT^T ; Z_r += (c_r S) . EMAT^T
 #pragma unroll
     for (int fb = 0; fb < FT; ++fb) {
       T fu[R][2], sv[DIM][R][2];
+      if constexpr (NFP % 2 == 0) {
+        // the two columns of a lane lie on one face
+        const int k0 = 8 * fb + 2 * t;
 #pragma unroll
-      for (int ri = 0; ri < R; ++ri)
-#pragma unroll
-        for (int ci = 0; ci < 2; ++ci) {
-          const int el = g + 8 * ri, k = 8 * fb + 2 * t + ci;
-          T vfu = T(0), vs = T(0);
-          T cr[DIM];
+        for (int ri = 0; ri < R; ++ri) {
+          const int el = g + 8 * ri;
+          T vfu[2] = {T(0), T(0)}, vs[2] = {T(0), T(0)}, cr[DIM];
 #pragma unroll
           for (int r = 0; r < DIM; ++r) cr[r] = T(0);
-          if (k < KF && el < ne) {
-            const int f = k / NFP, j = k % NFP;
+          if (k0 < KF && el < ne) {
+            const int f = k0 / NFP, j0 = k0 % NFP;
             const int lf = el * NF + f;
-            const T* own = sown + lf * TR;
-            const T um = own[j], gm = own[TRP + j];
+            const T* own = str + el * TS + f * TR;
+            const auto um = ld2(own + j0);
+            const auto gm = ld2(own + TRP + j0);
             const int nb = snbr[lf];
-            T jump = T(0), navg = T(0);
+            T jump[2] = {T(0), T(0)}, navg[2] = {T(0), T(0)};
             if (nb >= 0) {
-              const int kk = perm[((scode[el] >> (8 * f + 2)) & 7) * NFP + j];
-              const T* rec = snb + lf * TR;
-              jump = um - rec[kk];
-              navg = T(0.5) * (gm - rec[TRP + kk]);
+              const int8_t* pr = perm + ((scode[el] >> (8 * f + 2)) & 7) * NFP + j0;
+              const T* rec = snb + el * TS + f * TR;
+              const int kk0 = pr[0], kk1 = pr[1];
+              jump[0] = um.x - rec[kk0];
+              jump[1] = um.y - rec[kk1];
+              navg[0] = T(0.5) * (gm.x - rec[TRP + kk0]);
+              navg[1] = T(0.5) * (gm.y - rec[TRP + kk1]);
             } else if (a.bct[-nb - 1] == BC_DIRICHLET) {
-              jump = T(2) * um;
-              navg = gm;
+              jump[0] = T(2) * um.x;
+              jump[1] = T(2) * um.y;
+              navg[0] = gm.x;
+              navg[1] = gm.y;
             }
-            const T hj = T(0.5) * jump;
-            const T* fg = sfg + lf * X::FG;
-            const T sJ = fg[3];
-            const T fm = a.factor ? sf[el * NP + fmask[k]] : T(1);
-            vfu = sJ * (stau[lf] * hj - navg);
-            vs = -sJ * fm * hj;
+            const T sJ = fgeo<T, DIM, P>(sfg, 0, f, el);
 #pragma unroll
-            for (int r = 0; r < DIM; ++r) cr[r] = fg[4 + r];
+            for (int r = 0; r < DIM; ++r) cr[r] = fgeo<T, DIM, P>(sfg, 1 + r, f, el);
+            const T tau = stau[lf];
+            const T fm0 = a.factor ? sf[el * XS + fmask[k0]] : T(1);
+            const T fm1 = a.factor ? sf[el * XS + fmask[k0 + 1]] : T(1);
+            const T h0 = T(0.5) * jump[0], h1 = T(0.5) * jump[1];
+            vfu[0] = sJ * (tau * h0 - navg[0]);
+            vfu[1] = sJ * (tau * h1 - navg[1]);
+            vs[0] = -sJ * fm0 * h0;
+            vs[1] = -sJ * fm1 * h1;
           }
-          fu[ri][ci] = F::op(vfu);
 #pragma unroll
-          for (int r = 0; r < DIM; ++r) sv[r][ri][ci] = F::op(cr[r] * vs);
+          for (int ci = 0; ci < 2; ++ci) {
+            fu[ri][ci] = F::op(vfu[ci]);
+#pragma unroll
+            for (int r = 0; r < DIM; ++r) sv[r][ri][ci] = F::op(cr[r] * vs[ci]);
+          }
         }
+      } else {
+#pragma unroll
+        for (int ri = 0; ri < R; ++ri)
+#pragma unroll
+          for (int ci = 0; ci < 2; ++ci) {
+            const int el = g + 8 * ri, k = 8 * fb + 2 * t + ci;
+            T vfu = T(0), vs = T(0), cr[DIM];
+#pragma unroll
+            for (int r = 0; r < DIM; ++r) cr[r] = T(0);
+            if (k < KF && el < ne) {
+              const int f = k / NFP, j = k % NFP;
+              const int lf = el * NF + f;
+              const T* own = str + el * TS + f * TR;
+              const T um = own[j], gm = own[TRP + j];
+              const int nb = snbr[lf];
+              T jump = T(0), navg = T(0);
+              if (nb >= 0) {
+                const int kk = perm[((scode[el] >> (8 * f + 2)) & 7) * NFP + j];
+                const T* rec = snb + el * TS + f * TR;
+                jump = um - rec[kk];
+                navg = T(0.5) * (gm - rec[TRP + kk]);
+              } else if (a.bct[-nb - 1] == BC_DIRICHLET) {
+                jump = T(2) * um;
+                navg = gm;
+              }
+              const T hj = T(0.5) * jump;
+              const T sJ = fgeo<T, DIM, P>(sfg, 0, f, el);
+              const T fm = a.factor ? sf[el * XS + fmask[k]] : T(1);
+              vfu = sJ * (stau[lf] * hj - navg);
+              vs = -sJ * fm * hj;
+#pragma unroll
+              for (int r = 0; r < DIM; ++r) cr[r] = fgeo<T, DIM, P>(sfg, 1 + r, f, el);
+            }
+            fu[ri][ci] = F::op(vfu);
+#pragma unroll
+            for (int r = 0; r < DIM; ++r) sv[r][ri][ci] = F::op(cr[r] * vs);
+          }
+      }
 #pragma unroll
       for (int nt = 0; nt < NT; ++nt) {
         const auto b = ldb(B + X::BE, fb * NT + nt, lane);
