@@ -115,8 +115,8 @@ int sipg_op_apply_host(sipg_op *op, const double *x, double *y);
  * for callers that cannot allocate device memory at apply time. The first call
  * on each device (current device) does a one-time set-up, a symbol-address
  * lookup; make it before any stream capture. Operators whose scratch would
- * exceed the limit (K * (dim+1) * 2 * Nfp values; at p = 3 in 3D: 209,715
- * elements FP32, 104,857 FP64) get SIPG_INVALID_ARG. There is one scratch per
+ * exceed the limit (K * (dim+1) face records of 2 * Nfp values, padded to
+ * 16-byte multiples; at p = 3 in 3D: 209,715 elements FP32, 104,857 FP64) get SIPG_INVALID_ARG. There is one scratch per
  * device: calls that overlap in time on one device race on it, so order them
  * on one stream or synchronise between them. Nothing in it needs to start at
  * zero. */
@@ -177,6 +177,8 @@ typedef struct {
                                 continuous piecewise-linear space (coarse_solver = petsc/amg) */
   int amg_coarse_max;        /* unknowns of the densely inverted coarsest level */
   double amg_strength;       /* aggregation strength threshold */
+  int graphs;                /* 1: each outer iteration after the first is replayed from a captured
+                                CUDA graph; 0: kernels are launched one by one (same arithmetic) */
 } sipg_solver_opts;
 
 int sipg_solver_default_opts(int kind, sipg_solver_opts *o);

@@ -469,6 +469,7 @@ int sipg_op_create(sipg_mesh* m, int order, int ncomp, sipg_op** out) {
 int sipg_op_set_factor(sipg_op* op, const double* factor) {
   return guarded([&] {
     if (!op) throw Error(SIPG_INVALID_ARG, "null op");
+    ++op->version;
     size_t n = (size_t)op->mesh->K * op->Np;
     if (!factor) {
       op->has_factor = false;
@@ -491,6 +492,7 @@ int sipg_op_set_factor(sipg_op* op, const double* factor) {
 int sipg_op_set_mm(sipg_op* op, int mode, double scalar, const double* mm) {
   return guarded([&] {
     if (!op || mode < 0 || mode > 2 || (mode == SIPG_MM_NODAL && !mm)) throw Error(SIPG_INVALID_ARG, "set_mm");
+    ++op->version;
     op->mm_mode = mode;
     op->mm_scalar = scalar;
     if (mode == SIPG_MM_NODAL) {
@@ -510,6 +512,7 @@ int sipg_op_set_mm(sipg_op* op, int mode, double scalar, const double* mm) {
 int sipg_op_set_bc_types(sipg_op* op, const int* types) {
   return guarded([&] {
     if (!op || (!types && op->mesh->Kb)) throw Error(SIPG_INVALID_ARG, "set_bc_types");
+    ++op->version;
     size_t n = (size_t)op->ncomp * op->mesh->Kb;
     std::vector<uint8_t> b(n);
     for (size_t i = 0; i < n; ++i) {
@@ -525,6 +528,7 @@ int sipg_op_set_bc_types(sipg_op* op, const int* types) {
 int sipg_op_set_pin(sipg_op* op, int elem, int node) {
   return guarded([&] {
     if (!op) throw Error(SIPG_INVALID_ARG, "null op");
+    ++op->version;
     if (elem < 0) { op->pin_elem = -1; op->pin_node = -1; return; }
     if (elem >= op->mesh->K || node < 0 || node >= op->Np) throw Error(SIPG_INVALID_ARG, "pin out of range");
     op->pin_elem = elem;
@@ -546,6 +550,7 @@ int sipg_op_apply(sipg_op* op, int precision, const void* x, void* y, void* stre
 int sipg_op_set_kernel(sipg_op* op, int kind) {
   return guarded([&] {
     if (!op || kind < 0 || kind > 1) throw Error(SIPG_INVALID_ARG, "set_kernel");
+    ++op->version;
     op->kernel = kind;
   });
 }

@@ -84,6 +84,7 @@ struct sipg_op {
   double pin_scale = 1.0;
   int eb64 = 0, eb32 = 0;
   int kernel = 0;  // 0: tensor cores where available, 1: CUDA cores
+  unsigned version = 0;  // bumped by every setter: solvers re-capture their graphs
   mutable sipg::DevBuf trace64, trace32;  // face traces of the two-pass tensor-core apply
   // Apply on device buffers in precision T.
   template <typename T>

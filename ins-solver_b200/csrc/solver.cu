@@ -173,9 +173,24 @@ struct sipg_solver {
   bool use_amg = false;
   bool dirty = true;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // Graph replay of the outer iteration: one graph per parity of the roles of
+  // z and z_old; the solution is iterated in xi so that no caller pointer is baked in.
+  DevBuf xi;
+  cudaGraphExec_t gx[2] = {nullptr, nullptr};
+  unsigned long long gnodes[2] = {0, 0};
+  unsigned gver = 0;
+  bool graph_broken = false;
 
   double* S() const { return scal.as<double>(); }
+  void drop_graphs() {
+    for (auto& g : gx)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
+  }
   ~sipg_solver() {
+    drop_graphs();
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
@@ -186,6 +201,13 @@ struct sipg_solver {
     SIPG_CUDA(cudaStreamSynchronize(stream));
     return hs.h[slot];
   }
+  // all device scalars to the host with one synchronisation
+  void read_scalars() {
+    SIPG_CUDA(cudaMemcpyAsync(hs.h, S(), S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    SIPG_CUDA(cudaStreamSynchronize(stream));
+  }
+  template <typename F>
+  void capture_iteration(int par, F&& body);
 
   void dot(const double* a, const double* b, int slot) {
     const double* aa[1] = {a};
@@ -397,6 +419,8 @@ void sipg_solver::setup_amg() {
 }
 
 void sipg_solver::setup() {
+  drop_graphs();
+  graph_broken = false;
   n = (size_t)op->ncomp * op->mesh->K * op->Np;
   if (!r.p) {
     size_t b = n * sizeof(double);
@@ -598,11 +622,56 @@ void sipg_solver::precondition(const double* rin, double* zout) {
   }
 }
 
-int sipg_solver::solve(const double* b, double* x, sipg_solve_info* info) {
+// Capture one outer iteration into gx[par]; on any failure the solver keeps
+// launching kernels one by one.
+template <typename F>
+void sipg_solver::capture_iteration(int par, F&& body) {
+  const unsigned long long c0 = launch_count();
+  cudaGraph_t g = nullptr;
+  if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+    cudaGetLastError();
+    graph_broken = true;
+    return;
+  }
+  bool ok = true;
+  try {
+    body();
+  } catch (...) {
+    ok = false;
+  }
+  cudaError_t e = cudaStreamEndCapture(stream, &g);
+  const unsigned long long c1 = launch_count();
+  unnote_launch(c1 - c0);  // recorded, not launched
+  if (!ok || e != cudaSuccess || !g) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    graph_broken = true;
+    return;
+  }
+  e = cudaGraphInstantiate(&gx[par], g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    gx[par] = nullptr;
+    cudaGetLastError();
+    graph_broken = true;
+    return;
+  }
+  gnodes[par] = c1 - c0;
+}
+
+int sipg_solver::solve(const double* b, double* x_user, sipg_solve_info* info) {
   auto t0 = std::chrono::steady_clock::now();
   if (dirty) setup();
   auto t1 = std::chrono::steady_clock::now();
+  const bool graphs = o.graphs != 0 && kind != SIPG_SOLVER_CG;
+  if (graphs && gver != op->version) {
+    drop_graphs();
+    gver = op->version;
+  }
+  if (graphs && !xi.p) xi = DevBuf(n * sizeof(double));
   SIPG_CUDA(cudaEventRecord(ev0, stream));
+  double* x = graphs ? xi.as<double>() : x_user;
+  if (graphs) vcopy<double>(x, x_user, n, stream);
   double* R = r.as<double>();
   double* Z = z.as<double>();
   double* ZO = zold.as<double>();
@@ -617,8 +686,9 @@ int sipg_solver::solve(const double* b, double* x, sipg_solve_info* info) {
   }
   dot(b, b, S_BB);
   dot(R, R, S_RR);
-  const double bnorm = std::sqrt(read_scalar(S_BB));
-  double res = std::sqrt(read_scalar(S_RR));
+  read_scalars();
+  const double bnorm = std::sqrt(hs.h[S_BB]);
+  double res = std::sqrt(hs.h[S_RR]);
   const double tol = std::max(o.abs_tol, o.rel_tol * bnorm);
   int iter = 0, status = SIPG_OK;
   if (!std::isfinite(bnorm) || !std::isfinite(res)) {
@@ -644,18 +714,20 @@ int sipg_solver::solve(const double* b, double* x, sipg_solve_info* info) {
       dot(R, R, S_RR);
       update_p<double>(Pv, R, n, S(), S_RR, S_RZ, stream);
       ++iter;
-      double pap = read_scalar(S_PAP);
-      res = std::sqrt(hs.h[S_RR] = read_scalar(S_RR));
+      read_scalars();
+      const double pap = hs.h[S_PAP];
+      res = std::sqrt(hs.h[S_RR]);
       if (!(pap > 0.0) || !std::isfinite(res)) { status = SIPG_BREAKDOWN; break; }
     }
   } else {
     // flexible PCG (viscous_solver.cpp:177-301)
     if (status == SIPG_OK) precondition(R, Z);
     vcopy<double>(Pv, Z, n, stream);
-    while (status == SIPG_OK && res > tol && iter < o.max_iter) {
+    // one iteration; zn receives the new preconditioned residual, zo holds the previous one
+    auto iteration = [&](double* zn, double* zo) {
       op->apply<double>(Pv, AP, stream);
       const double* a[2] = {R, Pv};
-      const double* bb[2] = {Z, AP};
+      const double* bb[2] = {zo, AP};
       multi_dot<double>(a, bb, 2, n, S() + S_RZ, 1, rw, stream);  // cg3_alpha_pre
       cg_update_xr(x, R, Pv, AP, n, S(), S_RZ, S_PAP, S() + S_RR, rw, stream);  // update_ans + update_res
       if (o.nullspace) {
@@ -663,13 +735,27 @@ int sipg_solver::solve(const double* b, double* x, sipg_solve_info* info) {
         sub_mean<double>(R, n, S(), S_SUM, stream);
         dot(R, R, S_RR);
       }
+      precondition(R, zn);
+      dot_diff(R, zn, zo, n, S() + S_BETA, rw, stream);  // cg3_compute_beta_pre_flex
+      update_p<double>(Pv, zn, n, S(), S_BETA, S_RZ, stream);
+    };
+    while (status == SIPG_OK && res > tol && iter < o.max_iter) {
+      double* zn = ZO;
+      double* zo = Z;
+      const int par = iter & 1;  // Z = z, ZO = z_old at iteration 0
+      // the first iteration runs eagerly (lazy buffers are allocated there), the rest replay
+      if (graphs && iter >= 1 && !graph_broken && !gx[par]) capture_iteration(par, [&] { iteration(zn, zo); });
+      if (graphs && iter >= 1 && gx[par]) {
+        SIPG_CUDA(cudaGraphLaunch(gx[par], stream));
+        note_launch((unsigned)gnodes[par]);
+      } else {
+        iteration(zn, zo);
+      }
       std::swap(Z, ZO);
-      precondition(R, Z);
-      dot_diff(R, Z, ZO, n, S() + S_BETA, rw, stream);  // cg3_compute_beta_pre_flex
-      update_p<double>(Pv, Z, n, S(), S_BETA, S_RZ, stream);
       ++iter;
-      double pap = read_scalar(S_PAP);
-      res = std::sqrt(read_scalar(S_RR));
+      read_scalars();
+      const double pap = hs.h[S_PAP];
+      res = std::sqrt(hs.h[S_RR]);
       if (!(pap > 0.0) || !std::isfinite(res)) { status = SIPG_BREAKDOWN; break; }
     }
   }
@@ -683,6 +769,7 @@ int sipg_solver::solve(const double* b, double* x, sipg_solve_info* info) {
     sub_mean<double>(AP, n, S(), S_SUM, stream);
   }
   dot(AP, AP, S_TMP);
+  if (graphs) vcopy<double>(x_user, x, n, stream);
   double true_res = std::sqrt(read_scalar(S_TMP));
   float ms = 0.f;
   SIPG_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
@@ -721,6 +808,7 @@ int sipg_solver_default_opts(int kind, sipg_solver_opts* o) {
     o->coarse_kind = 1;
     o->amg_coarse_max = 1000;
     o->amg_strength = 0.08;
+    o->graphs = 1;
     (void)kind;
   });
 }

@@ -8,6 +8,7 @@ namespace sipg {
 
 static std::atomic<unsigned long long> g_launches{0};
 void note_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+void unnote_launch(unsigned long long n) { g_launches.fetch_sub(n, std::memory_order_relaxed); }
 unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 namespace {
 

@@ -12,6 +12,7 @@ namespace sipg {
 
 // Count of kernel launches issued by this library (diagnostics).
 void note_launch(unsigned n = 1);
+void unnote_launch(unsigned long long n);  // launches recorded during a graph capture
 unsigned long long launch_count();
 
 // Device scalar slots used by the solvers.

@@ -47,7 +47,8 @@ class SolverOpts(C.Structure):
                 ("ref_volume_block", C.c_int), ("n_levels", C.c_int), ("orders", C.c_int * 4),
                 ("cheb_order", C.c_int), ("eig_safety", C.c_double), ("eig_ratio", C.c_double),
                 ("eig_iters", C.c_int), ("coarse_iters", C.c_int), ("check_every", C.c_int),
-                ("coarse_kind", C.c_int), ("amg_coarse_max", C.c_int), ("amg_strength", C.c_double)]
+                ("coarse_kind", C.c_int), ("amg_coarse_max", C.c_int), ("amg_strength", C.c_double),
+                ("graphs", C.c_int)]
 
 
 def lib():
