@@ -17,7 +17,7 @@ Headline workload (one "step" = one Poisson solve):
   fp64    = the plain FP64 GPU path (same algorithm, V-cycle in FP64);
   apply   = SIPG apply GDOF/s of the 3D viscous Helmholtz configuration
             (48^3 x 6 = 663,552 tets, p=4) in FP64 and FP32;
-  roofline for the dominant kernel (the FP32 p=3 apply of the V-cycle).
+  roofline for the dominant kernel pair (the FP32 p=3 two-pass apply of the V-cycle).
 The operator setup (diagonals, eigenvalue estimates, coarse operators) runs once
 before timing; the coefficient does not change between steps and its setup time
 is reported separately.
@@ -172,11 +172,19 @@ def time_apply(op, precision, K, Np, iters=30):
     return e0.elapsed_time(e1) / iters
 
 
-def apply_bytes_per_elem(Np, ts, factor, ngeof=10, nf=4):
+def apply_bytes_per_elem(Np, ts, factor, ngeof=10, nf=4, gface=5):
     """Algorithmic HBM bytes of one scalar apply per element: read x, write y,
-    factor (if nodal), geometry (geof) and penalty, neighbour ids and codes.
-    Neighbour traces are L2 hits, not HBM."""
-    return ts * (2 * Np + (Np if factor else 0) + ngeof + nf) + 4 * nf + 4
+    the nodal factor (if any), the volume geometric factors and nf faces of
+    face geometry (normal, sJ, fscale), and an int32 neighbour id plus face code
+    per face. Neighbour traces count as L2 hits, not HBM. (The kernels derive
+    the face geometry from the volume factors, so they read less than this.)"""
+    return ts * (2 * Np + (Np if factor else 0) + ngeof + nf * gface) + 4 * 2 * nf
+
+
+# DRAM traffic of one FP32 p=3 apply (trace + apply kernels) at the headline
+# size, ncu capture with flushed caches (dram__bytes_read.sum + dram__bytes_write.sum
+# of both launches): profiles/apply_tc_fp32_p3_24cube.txt
+APPLY_P3_FP32_TRAFFIC = 16.629e6 + 0.0018e6 + 46.211e6 + 0.203e6
 
 
 def run_ours(args):
@@ -273,9 +281,11 @@ def run_ours(args):
         "apply_p3": {"fp32_ms": a32, "fp64_ms": a64, "fp32_gdofs": n / (a32 * 1e-3) / 1e9,
                      "fp64_gdofs": n / (a64 * 1e-3) / 1e9},
         "apply_c3": apply_c3,
-        "roofline": {"kernel": "sipg_apply_kernel<float,3,3>", "bound": "hbm", "achieved": achieved,
-                     "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": None, "bytes_per_elem": bpe},
+        "roofline": {"kernel": "sipg_trace_kernel<float,3,3> + sipg_apply_tc_kernel<float,3,3> "
+                               "(one FP32 p=3 apply = 2 launches)",
+                     "bound": "hbm", "achieved": achieved, "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": APPLY_P3_FP32_TRAFFIC, "bytes_per_elem": bpe,
+                     "apply_ms": a32, "elements": K},
         "clocks": clk.summary(),
     }
     if rank == 0 and world == 1 and not args.skip_cpu:
@@ -289,14 +299,15 @@ def run_ours(args):
 
 def cpu_reference(c, op, outer_iters, sample_only=False, steps=1, warmup=0):
     """Reference kernels on the host cores: one outer iteration of the p-MG solve =
-    1 FP64 apply at p=3 + 2x4 Chebyshev applies at p=3 and at p=2 + 20 coarse
-    applies at p=1 (the FP64 path's counts), timed with the reference's own
+    1 FP64 apply at p=3 + 8 V-cycle applies (Chebyshev(4) before and after,
+    one residual) at each of p=3, 2, 1 (the algebraic coarse levels below p=1
+    are excluded), timed with the reference's own
     kernels (oracle/_ref, OpenMP)."""
     import oracle_py as O
     cores = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
     mesh = c["mesh"]
-    counts = {3: 1 + 8, 2: 8, 1: 20}
+    counts = {3: 1 + 8, 2: 8, 1: 8}
     per = {}
     rng = np.random.default_rng(0)
     for p, cnt in counts.items():
@@ -328,7 +339,7 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libsipgref.so was not built"}))
         return
     c = W.poisson3d_two_phase(N_HEAD, order=ORDER, n_modes=256, pin=False)
-    outer = 26  # outer iterations of the FP64 p-MG path on this workload (measured on the GPU)
+    outer = 31  # outer iterations of the FP64 p-MG path on this workload (measured on the GPU)
     step_times = []
     for i in range(args.warmup + args.steps):
         r = cpu_reference(c, None, outer)
