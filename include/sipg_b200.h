@@ -179,6 +179,9 @@ typedef struct {
   double amg_strength;       /* aggregation strength threshold */
   int graphs;                /* 1: each outer iteration after the first is replayed from a captured
                                 CUDA graph; 0: kernels are launched one by one (same arithmetic) */
+  int assembled_max_order;   /* p-multigrid levels below the finest with this order or lower apply
+                                their operator as stored element blocks (assembled once from the
+                                matrix-free apply, scalar operators, orders <= 2); 0: all matrix-free */
 } sipg_solver_opts;
 
 int sipg_solver_default_opts(int kind, sipg_solver_opts *o);

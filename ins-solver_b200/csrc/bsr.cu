@@ -1,0 +1,166 @@
+// Element-block form of low-order SIPG operators: probing assembly and apply.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "../../include/sipg_b200.h"
+#include "bsr.cuh"
+#include "vecops.cuh"
+
+namespace sipg {
+namespace {
+
+int grid_of(size_t n) { return (int)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, 148 * 16)); }
+
+__global__ void k_probe_set(double* x, const int* list, int n, int node, int Np) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    x[(size_t)list[j] * Np + node] = 1.0;
+}
+
+// Column (e, node) of the blocks of every row element k adjacent to a probed element e.
+__global__ void k_probe_extract(const double* y, const int* list, int n, int node, const int* nbr,
+                                const uint32_t* fcode, int K, int Np, int NF, double* v) {
+  const int per = (NF + 1) * Np;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n * per; t += gridDim.x * blockDim.x) {
+    const int j = t / per, q = t % per;
+    const int s = q / Np, r = q % Np;
+    const int e = list[j];
+    int k = e, slot = 0;
+    if (s > 0) {
+      k = nbr[(size_t)e * NF + s - 1];
+      if (k < 0) continue;
+      slot = 1 + (int)((fcode[e] >> (8 * (s - 1))) & 3u);
+    }
+    v[((size_t)(slot * Np + r) * Np + node) * K + k] = y[(size_t)k * Np + r];
+  }
+}
+
+__global__ void k_d2f(float* dst, const double* src, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = (float)src[i];
+}
+
+template <typename T, int NP, int NF>
+__global__ void __launch_bounds__(256) k_bsr(int K, const T* __restrict__ v, const int* __restrict__ nbr,
+                                             const T* __restrict__ x, T* __restrict__ y, T alpha, T beta) {
+  const size_t K_ = (size_t)K;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < K; e += gridDim.x * blockDim.x) {
+    T acc[NP];
+#pragma unroll
+    for (int r = 0; r < NP; ++r) acc[r] = T(0);
+#pragma unroll
+    for (int s = 0; s <= NF; ++s) {
+      const int k = s == 0 ? e : nbr[(size_t)e * NF + s - 1];
+      if (k < 0) continue;
+      T xv[NP];
+#pragma unroll
+      for (int c = 0; c < NP; ++c) xv[c] = x[(size_t)k * NP + c];
+      const T* vs = v + (size_t)s * NP * NP * K_ + e;
+#pragma unroll
+      for (int r = 0; r < NP; ++r)
+#pragma unroll
+        for (int c = 0; c < NP; ++c) acc[r] += vs[(size_t)(r * NP + c) * K_] * xv[c];
+    }
+#pragma unroll
+    for (int r = 0; r < NP; ++r) {
+      T o = alpha * acc[r];
+      if (beta != T(0)) o += beta * y[(size_t)e * NP + r];
+      y[(size_t)e * NP + r] = o;
+    }
+  }
+}
+
+}  // namespace
+
+std::vector<int> distance2_colours(int K, int NF, const int* nbr, int* ncolours) {
+  std::vector<int> col(K, -1);
+  std::vector<int> stamp(64 * 4 + 64, -1);
+  int nc = 0;
+  for (int e = 0; e < K; ++e) {
+    // colours used within distance 2 of e
+    auto mark = [&](int k) {
+      if (k >= 0 && col[k] >= 0) {
+        if (col[k] >= (int)stamp.size()) stamp.resize(col[k] + 1, -1);
+        stamp[col[k]] = e;
+      }
+    };
+    for (int f = 0; f < NF; ++f) {
+      const int k = nbr[(size_t)e * NF + f];
+      if (k < 0) continue;
+      mark(k);
+      for (int g = 0; g < NF; ++g) mark(nbr[(size_t)k * NF + g]);
+    }
+    int c = 0;
+    while (c < (int)stamp.size() && stamp[c] == e) ++c;
+    col[e] = c;
+    nc = std::max(nc, c + 1);
+  }
+  *ncolours = nc;
+  return col;
+}
+
+void bsr_assemble(sipg_op* op, BsrOp& B, bool want32, cudaStream_t s) {
+  if (op->ncomp != 1) throw Error(SIPG_INVALID_ARG, "assembled blocks need a scalar operator");
+  sipg_mesh* m = op->mesh;
+  const int K = m->K, Np = op->Np, NF = m->dim + 1;
+  const Mesh& h = m->host_order(1);
+  int nc = 0;
+  std::vector<int> col = distance2_colours(K, NF, h.nbr.data(), &nc);
+  std::vector<int> off(nc + 1, 0), list(K);
+  for (int e = 0; e < K; ++e) ++off[col[e] + 1];
+  for (int c = 0; c < nc; ++c) off[c + 1] += off[c];
+  {
+    std::vector<int> fill(off.begin(), off.end() - 1);
+    for (int e = 0; e < K; ++e) list[fill[col[e]]++] = e;
+  }
+  B.K = K;
+  B.Np = Np;
+  B.NF = NF;
+  B.dim = m->dim;
+  B.nbr = m->nbr.as<int>();
+  const size_t nv = (size_t)(NF + 1) * Np * Np * K;
+  B.v64 = DevBuf(nv * sizeof(double));
+  SIPG_CUDA(cudaMemsetAsync(B.v64.p, 0, nv * sizeof(double), s));
+  DevBuf dl((size_t)K * sizeof(int)), x((size_t)K * Np * sizeof(double)), y((size_t)K * Np * sizeof(double));
+  SIPG_CUDA(cudaMemcpyAsync(dl.p, list.data(), (size_t)K * sizeof(int), cudaMemcpyHostToDevice, s));
+  for (int c = 0; c < nc; ++c) {
+    const int n = off[c + 1] - off[c];
+    const int* lc = dl.as<int>() + off[c];
+    for (int i = 0; i < Np; ++i) {
+      SIPG_CUDA(cudaMemsetAsync(x.p, 0, (size_t)K * Np * sizeof(double), s));
+      k_probe_set<<<grid_of(n), 256, 0, s>>>(x.as<double>(), lc, n, i, Np);
+      note_launch();
+      op->apply<double>(x.as<double>(), y.as<double>(), s);
+      k_probe_extract<<<grid_of((size_t)n * (NF + 1) * Np), 256, 0, s>>>(
+          y.as<double>(), lc, n, i, m->nbr.as<int>(), m->fcode.as<uint32_t>(), K, Np, NF, B.v64.as<double>());
+      note_launch();
+    }
+  }
+  if (want32) {
+    B.v32 = DevBuf(nv * sizeof(float));
+    k_d2f<<<grid_of(nv), 256, 0, s>>>(B.v32.as<float>(), B.v64.as<double>(), nv);
+    note_launch();
+  }
+  SIPG_CUDA(cudaGetLastError());
+  SIPG_CUDA(cudaStreamSynchronize(s));  // the probe buffers are freed on return
+}
+
+template <typename T>
+void bsr_apply(const BsrOp& B, const T* x, T* y, T alpha, T beta, cudaStream_t s) {
+  const T* v = std::is_same<T, double>::value ? (const T*)B.v64.p : (const T*)B.v32.p;
+  if (!v) throw Error(SIPG_INVALID_ARG, "assembled blocks missing for this precision");
+  const int g = grid_of(B.K);
+  if (B.dim == 3 && B.Np == 4) k_bsr<T, 4, 4><<<g, 256, 0, s>>>(B.K, v, B.nbr, x, y, alpha, beta);
+  else if (B.dim == 3 && B.Np == 10) k_bsr<T, 10, 4><<<g, 256, 0, s>>>(B.K, v, B.nbr, x, y, alpha, beta);
+  else if (B.dim == 2 && B.Np == 3) k_bsr<T, 3, 3><<<g, 256, 0, s>>>(B.K, v, B.nbr, x, y, alpha, beta);
+  else if (B.dim == 2 && B.Np == 6) k_bsr<T, 6, 3><<<g, 256, 0, s>>>(B.K, v, B.nbr, x, y, alpha, beta);
+  else throw Error(SIPG_INVALID_ARG, "no assembled apply for this element");
+  note_launch();
+  SIPG_CUDA(cudaGetLastError());
+}
+
+template void bsr_apply<double>(const BsrOp&, const double*, double*, double, double, cudaStream_t);
+template void bsr_apply<float>(const BsrOp&, const float*, float*, float, float, cudaStream_t);
+
+}  // namespace sipg

@@ -1,0 +1,46 @@
+// Element-block (block-sparse) form of a low-order SIPG operator.
+//
+// At p = 1 the matrix-free apply spends most of its time on per-element
+// overheads (face geometry, traces, two launches) while the operator itself is
+// small: an element row couples to itself and to its face neighbours only, in
+// Np x Np blocks (4 x 4 for tetrahedra at p = 1). The p-multigrid applies such
+// a level's operator eight times per V-cycle, so the levels at or below a
+// chosen order store these blocks once and apply them as a block-sparse
+// product (one thread per element row, coalesced block reads).
+//
+// The blocks are assembled by probing the matrix-free apply in FP64: elements
+// are coloured so that no two elements of one colour share a face neighbour
+// (distance-2 colouring of the face graph); for every colour c and local node i
+// the apply of the indicator vector sum_{e in c} e_(e,i) gives column (e, i) of
+// the blocks of every row element adjacent to e, without overlap.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "runtime.hpp"
+
+namespace sipg {
+
+struct BsrOp {
+  int K = 0, Np = 0, NF = 0, dim = 0;
+  // values[((s * Np + r) * Np + c) * K + e]: block s of element row e, s = 0 the
+  // element itself, s = 1 + f the neighbour across face f (zero at boundary faces)
+  DevBuf v64, v32;
+  const int* nbr = nullptr;  // mesh K x NF (device)
+};
+
+// Orders whose element blocks have an assembled apply (Np x Np registers per thread).
+inline bool bsr_supported(int dim, int order, int ncomp) { return ncomp == 1 && order >= 1 && order <= 2 && dim >= 2; }
+
+// Assemble from the operator's FP64 apply (and an FP32 copy when want32).
+void bsr_assemble(sipg_op* op, BsrOp& B, bool want32, cudaStream_t s);
+
+// y = alpha * B x + beta * y (beta == 0: y is not read).
+template <typename T>
+void bsr_apply(const BsrOp& B, const T* x, T* y, T alpha, T beta, cudaStream_t s);
+
+// Greedy distance-2 colouring of the face graph (nbr: K x NF, negative = boundary).
+std::vector<int> distance2_colours(int K, int NF, const int* nbr, int* ncolours);
+
+}  // namespace sipg

@@ -26,6 +26,7 @@
 #include "../../include/sipg_b200.h"
 #include "amg.hpp"
 #include "capi_util.hpp"
+#include "bsr.cuh"
 #include "runtime.hpp"
 #include "sipg_blocks.cuh"
 #include "vecops.cuh"
@@ -51,6 +52,12 @@ struct Level {
   // work vectors in the V-cycle precision
   DevBuf rhs, z, res, d;
   DevBuf cp, cs, cAp;            // coarse CG
+  std::unique_ptr<BsrOp> bsr;    // assembled element blocks (low orders), else matrix-free
+  template <typename T>
+  void apply(const T* x, T* y, cudaStream_t s, T alpha = T(1), T beta = T(0)) const {
+    if (bsr) bsr_apply<T>(*bsr, x, y, alpha, beta, s);
+    else op->apply<T>(x, y, s, alpha, beta);
+  }
 };
 
 // Per-element interpolation kernel: out_e = I in_e (I: Npo x Npi row-major)
@@ -345,6 +352,11 @@ void sipg_solver::setup_pmg() {
       note_launch();
     if (f32) to_f32(L.dinv32.as<float>(), L.dinv64.as<double>(), L.n, stream);
     L.lmax = power_lmax(L.op, L.dinv64.as<double>(), L.n);
+    L.bsr.reset();
+    if (l > 0 && L.order <= o.assembled_max_order && bsr_supported(dim, L.order, nc)) {
+      L.bsr = std::make_unique<BsrOp>();
+      bsr_assemble(L.op, *L.bsr, f32, stream);
+    }
   }
   use_amg = o.coarse_kind == 1 && nc == 1 && lv.back().order == 1;
   if (use_amg) setup_amg();
@@ -478,7 +490,7 @@ void sipg_solver::chebyshev(Level& L, bool want_res) {
       rho_old = rho;
     }
     cheb_step<T>(d, z, res, dinv, (T)c1, (T)c2, L.n, stream);
-    if (it < o.cheb_order - 1 || want_res) L.op->apply<T>(d, res, stream, T(-1), T(1));
+    if (it < o.cheb_order - 1 || want_res) L.apply<T>(d, res, stream, T(-1), T(1));
   }
 }
 
@@ -501,7 +513,7 @@ void sipg_solver::coarse(Level& L) {
     multi_dot<T>(a, b, 1, L.n, S() + S_C_RZ, 1, rw, stream);
   }
   for (int it = 0; it < o.coarse_iters; ++it) {
-    L.op->apply<T>(cp, cAp, stream);
+    L.apply<T>(cp, cAp, stream);
     const T* a[1] = {cp};
     const T* b[1] = {cAp};
     multi_dot<T>(a, b, 1, L.n, S() + S_C_PAP, 1, rw, stream);
@@ -560,7 +572,7 @@ void sipg_solver::last_level_amg(Level& L) {
   amg_vcycle<T>(0);
   Pdg.mv<T>(al[0].z.as<T>(), L.z.as<T>(), T(1), T(1), stream);
   vcopy<T>(L.res.as<T>(), L.rhs.as<T>(), L.n, stream);
-  L.op->apply<T>(L.z.as<T>(), L.res.as<T>(), stream, T(-1), T(1));
+  L.apply<T>(L.z.as<T>(), L.res.as<T>(), stream, T(-1), T(1));
   chebyshev<T>(L, false);
 }
 
@@ -584,7 +596,7 @@ void sipg_solver::vcycle(int l) {
   vcycle<T>(l + 1);
   prolong_add<T>(L.z.as<T>(), Cl.z.as<T>(), P, K, L.Np, Cl.Np, nc, stream);
   vcopy<T>(L.res.as<T>(), L.rhs.as<T>(), L.n, stream);
-  L.op->apply<T>(L.z.as<T>(), L.res.as<T>(), stream, T(-1), T(1));
+  L.apply<T>(L.z.as<T>(), L.res.as<T>(), stream, T(-1), T(1));
   chebyshev<T>(L, false);
 }
 
@@ -809,6 +821,7 @@ int sipg_solver_default_opts(int kind, sipg_solver_opts* o) {
     o->amg_coarse_max = 1000;
     o->amg_strength = 0.08;
     o->graphs = 1;
+    o->assembled_max_order = 1;
     (void)kind;
   });
 }

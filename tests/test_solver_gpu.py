@@ -181,3 +181,22 @@ def test_graph_replayed_iterations_match_eager_launches(precision):
     for k in (0, 2, 4):
         assert e[k + 1].iters == g[k + 1].iters
         assert np.array_equal(e[k], g[k])
+
+
+@pytest.mark.parametrize("precision", [sipg.FP64, sipg.FP32], ids=["fp64", "mixed"])
+def test_assembled_low_order_levels_match_matrix_free(precision):
+    """The p=1 (and p=2) levels applied from stored element blocks, assembled by
+    probing the matrix-free apply, give the matrix-free solver's iterates."""
+    c = W.poisson3d_two_phase(5, order=3, n_modes=64, pin=False)
+    res = {}
+    for amo in (0, 1, 2):
+        op = make_op(c["mesh"], 3, 1, c["factor"], bct=c["bc_types"])
+        o = sipg.default_opts(sipg.SOLVER_PMULTIGRID)
+        o.rel_tol, o.abs_tol, o.max_iter, o.precision, o.nullspace = 1e-8, 0.0, 200, precision, 1
+        o.assembled_max_order = amo
+        x, info = sipg.Solver(op, sipg.SOLVER_PMULTIGRID, o).solve_host(c["rhs"])
+        assert info.status == sipg.SIPG_OK
+        res[amo] = (x, info)
+    for amo in (1, 2):
+        assert abs(res[amo][1].iters - res[0][1].iters) <= (0 if precision == sipg.FP64 else 1)
+        assert rel_err(res[amo][0], res[0][0]) < (1e-10 if precision == sipg.FP64 else 1e-6)
