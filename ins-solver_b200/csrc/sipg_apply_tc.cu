@@ -223,6 +223,10 @@ __device__ __forceinline__ void issue_traces(const ApplyArgs<T>& a, const T* tra
   }
 }
 
+// 1/sqrt: the hardware approximation in FP32 (the TF32 path tolerates its ulps), exact in FP64.
+__device__ __forceinline__ float inv_sqrt(float v) { return rsqrtf(v); }
+__device__ __forceinline__ double inv_sqrt(double v) { return 1.0 / sqrt(v); }
+
 // sJ and c_r = n . grad r of face f (n the outward unit normal) from the geometric factors g.
 template <typename T, int DIM>
 __device__ __forceinline__ void face_geom(const T* g, int f, T& sJ, T (&c)[3]) {
@@ -237,9 +241,10 @@ __device__ __forceinline__ void face_geom(const T* g, int f, T& sJ, T (&c)[3]) {
       else v = -g[d];
       n[d] = v;
     }
-    const T len = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
-    n[0] /= len; n[1] /= len; n[2] /= len;
-    sJ = len * g[9];
+    const T len2 = n[0] * n[0] + n[1] * n[1] + n[2] * n[2];
+    const T inv = inv_sqrt(len2);
+    n[0] *= inv; n[1] *= inv; n[2] *= inv;
+    sJ = len2 * inv * g[9];
   } else {
 #pragma unroll
     for (int d = 0; d < 2; ++d) {
@@ -250,9 +255,10 @@ __device__ __forceinline__ void face_geom(const T* g, int f, T& sJ, T (&c)[3]) {
       n[d] = v;
     }
     n[2] = T(0);
-    const T len = sqrt(n[0] * n[0] + n[1] * n[1]);
-    n[0] /= len; n[1] /= len;
-    sJ = len * g[4];
+    const T len2 = n[0] * n[0] + n[1] * n[1];
+    const T inv = inv_sqrt(len2);
+    n[0] *= inv; n[1] *= inv;
+    sJ = len2 * inv * g[4];
   }
 #pragma unroll
   for (int r = 0; r < 3; ++r) {
