@@ -473,6 +473,20 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_apply_tc_kernel(ApplyArgs<
     const int* snbr = ints;
     const int* scode = ints + TE * NF;
     if (lane == 0 && a.pin_elem >= e0 && a.pin_elem < e0 + ne) sx[(a.pin_elem - e0) * XS + a.pin_node] = T(0);
+    // y values read by the epilogue (beta != 0), loaded now so that their latency
+    // hides behind the tile's products
+    T yold[NT][R][2];
+    if (a.beta != T(0)) {
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+        for (int ri = 0; ri < R; ++ri)
+#pragma unroll
+          for (int ci = 0; ci < 2; ++ci) {
+            const int el = g + 8 * ri, n = 8 * nt + 2 * t + ci;
+            yold[nt][ri][ci] = (el < ne && n < NP) ? a.y[(size_t)(e0 + el) * NP + n] : T(0);
+          }
+    }
     tile_face_geom<T, DIM, P>(sg, sfg, ne, lane);
     __syncwarp();
 
@@ -706,7 +720,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_apply_tc_kernel(ApplyArgs<
           T acc = y[nt][ri][ci];
           if (e0 + el == a.pin_elem && n == a.pin_node) acc = a.pin_scale * a.x[row + n];
           acc *= a.alpha;
-          if (a.beta != T(0)) acc += a.beta * a.y[row + n];
+          if (a.beta != T(0)) acc += a.beta * yold[nt][ri][ci];
           a.y[row + n] = acc;
         }
       }
