@@ -6,6 +6,7 @@
 
 #include "../../include/sipg_b200.h"
 #include "bsr.cuh"
+#include "pdl.cuh"
 #include "vecops.cuh"
 
 namespace sipg {
@@ -44,6 +45,7 @@ __global__ void k_d2f(float* dst, const double* src, size_t n) {
 template <typename T, int NP, int NF>
 __global__ void __launch_bounds__(256) k_bsr(int K, const T* __restrict__ v, const int* __restrict__ nbr,
                                              const T* __restrict__ x, T* __restrict__ y, T alpha, T beta) {
+  pdl_enter();
   const size_t K_ = (size_t)K;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < K; e += gridDim.x * blockDim.x) {
     T acc[NP];
@@ -151,10 +153,10 @@ void bsr_apply(const BsrOp& B, const T* x, T* y, T alpha, T beta, cudaStream_t s
   const T* v = std::is_same<T, double>::value ? (const T*)B.v64.p : (const T*)B.v32.p;
   if (!v) throw Error(SIPG_INVALID_ARG, "assembled blocks missing for this precision");
   const int g = grid_of(B.K);
-  if (B.dim == 3 && B.Np == 4) k_bsr<T, 4, 4><<<g, 256, 0, s>>>(B.K, v, B.nbr, x, y, alpha, beta);
-  else if (B.dim == 3 && B.Np == 10) k_bsr<T, 10, 4><<<g, 256, 0, s>>>(B.K, v, B.nbr, x, y, alpha, beta);
-  else if (B.dim == 2 && B.Np == 3) k_bsr<T, 3, 3><<<g, 256, 0, s>>>(B.K, v, B.nbr, x, y, alpha, beta);
-  else if (B.dim == 2 && B.Np == 6) k_bsr<T, 6, 3><<<g, 256, 0, s>>>(B.K, v, B.nbr, x, y, alpha, beta);
+  if (B.dim == 3 && B.Np == 4) pdl_launch(k_bsr<T, 4, 4>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta);
+  else if (B.dim == 3 && B.Np == 10) pdl_launch(k_bsr<T, 10, 4>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta);
+  else if (B.dim == 2 && B.Np == 3) pdl_launch(k_bsr<T, 3, 3>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta);
+  else if (B.dim == 2 && B.Np == 6) pdl_launch(k_bsr<T, 6, 3>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta);
   else throw Error(SIPG_INVALID_ARG, "no assembled apply for this element");
   note_launch();
   SIPG_CUDA(cudaGetLastError());

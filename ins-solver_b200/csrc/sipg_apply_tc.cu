@@ -33,6 +33,7 @@
 #include <cstdint>
 #include <type_traits>
 
+#include "pdl.cuh"
 #include "sipg_apply.cuh"
 #include "sipg_apply_tc.cuh"
 #include "vecops.cuh"
@@ -324,12 +325,14 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_trace_kernel(ApplyArgs<T> 
   const int ntiles = (a.K + TE - 1) / TE;
   const int stride = gridDim.x * WARPS;
   int tile = blockIdx.x * WARPS + warp;
+  pdl_trigger();
   for (int i = lane; i < X::W1_T; i += 32) W[i] = T(0);  // row and record padding stays zero
+  for (int i = threadIdx.x; i < X::N1; i += blockDim.x) BFs[i] = blob[X::BF + i];
+  for (int i = threadIdx.x; i < NF * NFP; i += blockDim.x) fmask[i] = a.itab[i];
+  pdl_wait();  // x, factor and the trace buffer belong to the preceding kernels
   __syncwarp();
   issue_elem<T, DIM, P>(a, W, tile, lane, false);
   cp_commit();
-  for (int i = threadIdx.x; i < X::N1; i += blockDim.x) BFs[i] = blob[X::BF + i];
-  for (int i = threadIdx.x; i < NF * NFP; i += blockDim.x) fmask[i] = a.itab[i];
   __syncthreads();
   for (int it = 0; tile < ntiles; ++it, tile += stride) {
     T* st = W + (it & 1) * X::ST1;
@@ -441,15 +444,18 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_apply_tc_kernel(ApplyArgs<
   const int ntiles = (a.K + TE - 1) / TE;
   const int stride = gridDim.x * WARPS;
   int tile = blockIdx.x * WARPS + warp;
+  pdl_trigger();
   for (int i = lane; i < X::W2_T; i += 32) W[i] = T(0);  // row padding stays zero
   __syncwarp();
-  // prologue: connectivity of the first two tiles and the first tile's element data
+  // prologue: constants and the connectivity of the first two tiles (set-up data),
+  // then, once the preceding kernels are done, the first tile's element data
   issue_ints<T, DIM, P>(a, I, tile, lane);
   issue_ints<T, DIM, P>(a, I + X::SI, tile + stride, lane);
-  issue_elem<T, DIM, P>(a, W, tile, lane, true);
-  cp_commit();
   for (int i = threadIdx.x; i < X::N2; i += blockDim.x) B[i] = blob[i];
   for (int i = threadIdx.x; i < Cfg<DIM, P>::ITAB; i += blockDim.x) itab[i] = a.itab[i];
+  pdl_wait();
+  issue_elem<T, DIM, P>(a, W, tile, lane, true);
+  cp_commit();
   __syncthreads();
   for (int it = 0; tile < ntiles; ++it, tile += stride) {
     const int sb = it & 1, slot = it % 3;
@@ -775,7 +781,7 @@ cudaError_t launch_tc_t(const ApplyArgs<T>& a, const T* blob, T* trace, int num_
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, WA * 32, bytes);
     const int grid = std::min((ntiles + WA - 1) / WA, num_sms * std::max(per_sm, 1));
     if (grid > 0) {
-      k<<<grid, WA * 32, bytes, s>>>(a, blob, trace);
+      pdl_launch(k, dim3(grid), dim3(WA * 32), bytes, s, a, blob, (T*)trace);
       note_launch();
     }
   }
@@ -788,7 +794,7 @@ cudaError_t launch_tc_t(const ApplyArgs<T>& a, const T* blob, T* trace, int num_
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, WB * 32, bytes);
     const int grid = std::min((ntiles + WB - 1) / WB, num_sms * std::max(per_sm, 1));
     if (grid > 0) {
-      k<<<grid, WB * 32, bytes, s>>>(a, blob, trace);
+      pdl_launch(k, dim3(grid), dim3(WB * 32), bytes, s, a, blob, (const T*)trace);
       note_launch();
     }
   }

@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <atomic>
 
+#include "pdl.cuh"
 #include "vecops.cuh"
 
 namespace sipg {
@@ -73,6 +74,7 @@ __global__ void __launch_bounds__(kRedThreads) k_multi_dot(const T* a0, const T*
                                                            size_t n, double* partial,
                                                            unsigned* counter, double* out,
                                                            int out_stride) {
+  pdl_enter();
   double v[NK];
 #pragma unroll
   for (int k = 0; k < NK; ++k) v[k] = 0.0;
@@ -88,6 +90,7 @@ __global__ void __launch_bounds__(kRedThreads) k_multi_dot(const T* a0, const T*
 __global__ void __launch_bounds__(kRedThreads) k_dot_diff(const double* r, const double* z, const double* zo,
                                                           size_t n, double* partial, unsigned* counter,
                                                           double* out) {
+  pdl_enter();
   double v[1] = {0.0};
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     v[0] += r[i] * (z[i] - zo[i]);
@@ -98,6 +101,7 @@ __global__ void __launch_bounds__(kRedThreads) k_dot_diff(const double* r, const
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_sum(const T* a, size_t n, double* partial,
                                                      unsigned* counter, double* out) {
+  pdl_enter();
   double v[1] = {0.0};
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     v[0] += (double)a[i];
@@ -110,6 +114,7 @@ __global__ void __launch_bounds__(kRedThreads) k_cg_update_xr(double* x, double*
                                                               const double* scal, int num, int den,
                                                               double* partial, unsigned* counter,
                                                               double* rr_out) {
+  pdl_enter();
   const double alpha = scal[num] / scal[den];
   double v[1] = {0.0};
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -124,6 +129,7 @@ __global__ void __launch_bounds__(kRedThreads) k_cg_update_xr(double* x, double*
 
 template <typename T>
 __global__ void k_update_p(T* p, const T* z, size_t n, const double* scal, int num, int den) {
+  pdl_enter();
   const T beta = (T)(scal[num] / scal[den]);
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     p[i] = z[i] + beta * p[i];
@@ -131,6 +137,7 @@ __global__ void k_update_p(T* p, const T* z, size_t n, const double* scal, int n
 
 template <typename T>
 __global__ void k_sub_mean(T* v, size_t n, const double* scal, int slot) {
+  pdl_enter();
   const T mean = (T)(scal[slot] / (double)n);
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     v[i] -= mean;
@@ -138,24 +145,30 @@ __global__ void k_sub_mean(T* v, size_t n, const double* scal, int slot) {
 
 template <typename T>
 __global__ void k_copy(T* d, const T* s, size_t n) {
+  pdl_enter();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) d[i] = s[i];
 }
 template <typename T>
 __global__ void k_zero(T* d, size_t n) {
+  pdl_enter();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) d[i] = T(0);
 }
 __global__ void k_to_f32(float* d, const double* s, size_t n) {
+  pdl_enter();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) d[i] = (float)s[i];
 }
 __global__ void k_to_f64(double* d, const float* s, size_t n) {
+  pdl_enter();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) d[i] = (double)s[i];
 }
 template <typename T>
 __global__ void k_jacobi(T* z, const T* r, const T* dinv, size_t n) {
+  pdl_enter();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) z[i] = dinv[i] * r[i];
 }
 template <typename T>
 __global__ void k_cheb(T* d, T* z, const T* res, const T* dinv, T c1, T c2, size_t n) {
+  pdl_enter();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     T di = (c1 != T(0) ? c1 * d[i] : T(0)) + c2 * dinv[i] * res[i];
     d[i] = di;
@@ -166,6 +179,7 @@ __global__ void k_cheb(T* d, T* z, const T* res, const T* dinv, T c1, T c2, size
 // One warp per block row set: thread handles (block, row).
 template <typename T>
 __global__ void k_block_matvec(T* y, const T* B, const T* x, int nb, int Np) {
+  pdl_enter();
   const size_t total = (size_t)nb * Np;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
     const size_t b = i / Np;
@@ -181,6 +195,7 @@ __global__ void k_block_matvec(T* y, const T* B, const T* x, int nb, int Np) {
 template <typename T>
 __global__ void k_inv_mass(T* y, const T* x, const T* Minv, const T* geof, int ngeof, int jidx, int K,
                            int Np, int ncomp, T scale) {
+  pdl_enter();
   const size_t total = (size_t)ncomp * K * Np;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
     const size_t be = i / Np;
@@ -195,6 +210,7 @@ __global__ void k_inv_mass(T* y, const T* x, const T* Minv, const T* geof, int n
 
 template <typename T>
 __global__ void k_restrict(T* rc, const T* r, const T* P, int K, int Npf, int Npc, int ncomp) {
+  pdl_enter();
   const size_t total = (size_t)ncomp * K * Npc;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
     const size_t be = i / Npc;
@@ -208,6 +224,7 @@ __global__ void k_restrict(T* rc, const T* r, const T* P, int K, int Npf, int Np
 
 template <typename T>
 __global__ void k_prolong_add(T* z, const T* zc, const T* P, int K, int Npf, int Npc, int ncomp) {
+  pdl_enter();
   const size_t total = (size_t)ncomp * K * Npf;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
     const size_t be = i / Npf;
@@ -223,6 +240,7 @@ template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_coarse_update(T* z, T* r, T* sv, const T* p, const T* Ap,
                                                                const T* dinv, size_t n, double* scal,
                                                                double* partial, unsigned* counter) {
+  pdl_enter();
   const double pap = scal[S_C_PAP];
   const bool ok = pap > 0.0 && scal[S_C_RZ] > 0.0;
   const T alpha = ok ? (T)(scal[S_C_RZ] / pap) : T(0);
@@ -241,17 +259,20 @@ __global__ void __launch_bounds__(kRedThreads) k_coarse_update(T* z, T* r, T* sv
 
 template <typename T>
 __global__ void k_coarse_update_p(T* p, const T* sv, size_t n, double* scal) {
+  pdl_enter();
   const double rz = scal[S_C_RZ];
   const T beta = rz > 0.0 ? (T)(scal[S_C_RZN] / rz) : T(0);
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     p[i] = sv[i] + beta * p[i];
 }
 
-__global__ void k_shift_scalar(double* scal, int from, int to) { scal[to] = scal[from]; }
+__global__ void k_shift_scalar(double* scal, int from, int to) {
+  pdl_enter(); scal[to] = scal[from]; }
 
 template <typename T>
 __global__ void k_csr_spmv(int rows, const int* __restrict__ ptr, const int* __restrict__ idx,
                            const T* __restrict__ val, const T* __restrict__ x, T* y, T alpha, T beta) {
+  pdl_enter();
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
     T s = T(0);
     for (int k = ptr[r]; k < ptr[r + 1]; ++k) s += val[k] * x[idx[k]];
@@ -262,6 +283,7 @@ __global__ void k_csr_spmv(int rows, const int* __restrict__ ptr, const int* __r
 // One warp per row of a dense matrix.
 template <typename T>
 __global__ void k_dense_mv(int n, const T* __restrict__ M, const T* __restrict__ x, T* y) {
+  pdl_enter();
   const int lane = threadIdx.x & 31;
   for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += (gridDim.x * blockDim.x) >> 5) {
     double s = 0.0;
@@ -273,6 +295,7 @@ __global__ void k_dense_mv(int n, const T* __restrict__ M, const T* __restrict__
 
 template <typename T>
 __global__ void k_vadd(T* y, const T* x, size_t n) {
+  pdl_enter();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) y[i] += x[i];
 }
 
@@ -287,124 +310,124 @@ template <typename T>
 void multi_dot(const T* const* a, const T* const* b, int nk, size_t n, double* out, int out_stride,
                const RedWork& w, cudaStream_t s) {
   if (nk == 1)
-    k_multi_dot<T, 1><<<kRedBlocks, kRedThreads, 0, s>>>(a[0], b[0], nullptr, nullptr, nullptr, nullptr, n,
+    pdl_launch(k_multi_dot<T, 1>, dim3(kRedBlocks), dim3(kRedThreads), 0, s, a[0], b[0], nullptr, nullptr, nullptr, nullptr, n,
                                                          w.partial, w.counter, out, out_stride);
   else if (nk == 2)
-    k_multi_dot<T, 2><<<kRedBlocks, kRedThreads, 0, s>>>(a[0], b[0], a[1], b[1], nullptr, nullptr, n,
+    pdl_launch(k_multi_dot<T, 2>, dim3(kRedBlocks), dim3(kRedThreads), 0, s, a[0], b[0], a[1], b[1], nullptr, nullptr, n,
                                                          w.partial, w.counter, out, out_stride);
   else
-    k_multi_dot<T, 3><<<kRedBlocks, kRedThreads, 0, s>>>(a[0], b[0], a[1], b[1], a[2], b[2], n,
+    pdl_launch(k_multi_dot<T, 3>, dim3(kRedBlocks), dim3(kRedThreads), 0, s, a[0], b[0], a[1], b[1], a[2], b[2], n,
                                                          w.partial, w.counter, out, out_stride);
   note_launch();
 }
 
 void dot_diff(const double* r, const double* z, const double* zo, size_t n, double* out,
               const RedWork& w, cudaStream_t s) {
-  k_dot_diff<<<kRedBlocks, kRedThreads, 0, s>>>(r, z, zo, n, w.partial, w.counter, out);
+  pdl_launch(k_dot_diff, dim3(kRedBlocks), dim3(kRedThreads), 0, s, r, z, zo, n, w.partial, w.counter, out);
   note_launch();
 }
 
 template <typename T>
 void vsum(const T* a, size_t n, double* out, const RedWork& w, cudaStream_t s) {
-  k_sum<T><<<kRedBlocks, kRedThreads, 0, s>>>(a, n, w.partial, w.counter, out);
+  pdl_launch(k_sum<T>, dim3(kRedBlocks), dim3(kRedThreads), 0, s, a, n, w.partial, w.counter, out);
   note_launch();
 }
 
 void cg_update_xr(double* x, double* r, const double* p, const double* Ap, size_t n,
                   const double* scal, int num, int den, double* rr_out, const RedWork& w,
                   cudaStream_t s) {
-  k_cg_update_xr<<<kRedBlocks, kRedThreads, 0, s>>>(x, r, p, Ap, n, scal, num, den, w.partial, w.counter, rr_out);
+  pdl_launch(k_cg_update_xr, dim3(kRedBlocks), dim3(kRedThreads), 0, s, x, r, p, Ap, n, scal, num, den, w.partial, w.counter, rr_out);
   note_launch();
 }
 
 template <typename T>
 void update_p(T* p, const T* z, size_t n, const double* scal, int num, int den, cudaStream_t s) {
-  k_update_p<T><<<grid_for(n), 256, 0, s>>>(p, z, n, scal, num, den);
+  pdl_launch(k_update_p<T>, dim3(grid_for(n)), dim3(256), 0, s, p, z, n, scal, num, den);
   note_launch();
 }
 template <typename T>
 void sub_mean(T* v, size_t n, const double* scal, int slot, cudaStream_t s) {
-  k_sub_mean<T><<<grid_for(n), 256, 0, s>>>(v, n, scal, slot);
+  pdl_launch(k_sub_mean<T>, dim3(grid_for(n)), dim3(256), 0, s, v, n, scal, slot);
   note_launch();
 }
 template <typename T>
 void vcopy(T* dst, const T* src, size_t n, cudaStream_t s) {
-  k_copy<T><<<grid_for(n), 256, 0, s>>>(dst, src, n);
+  pdl_launch(k_copy<T>, dim3(grid_for(n)), dim3(256), 0, s, dst, src, n);
   note_launch();
 }
 template <typename T>
 void vzero(T* dst, size_t n, cudaStream_t s) {
-  k_zero<T><<<grid_for(n), 256, 0, s>>>(dst, n);
+  pdl_launch(k_zero<T>, dim3(grid_for(n)), dim3(256), 0, s, dst, n);
   note_launch();
 }
 void to_f32(float* dst, const double* src, size_t n, cudaStream_t s) {
-  k_to_f32<<<grid_for(n), 256, 0, s>>>(dst, src, n);
+  pdl_launch(k_to_f32, dim3(grid_for(n)), dim3(256), 0, s, dst, src, n);
   note_launch();
 }
 void to_f64(double* dst, const float* src, size_t n, cudaStream_t s) {
-  k_to_f64<<<grid_for(n), 256, 0, s>>>(dst, src, n);
+  pdl_launch(k_to_f64, dim3(grid_for(n)), dim3(256), 0, s, dst, src, n);
   note_launch();
 }
 template <typename T>
 void jacobi(T* z, const T* r, const T* dinv, size_t n, cudaStream_t s) {
-  k_jacobi<T><<<grid_for(n), 256, 0, s>>>(z, r, dinv, n);
+  pdl_launch(k_jacobi<T>, dim3(grid_for(n)), dim3(256), 0, s, z, r, dinv, n);
   note_launch();
 }
 template <typename T>
 void cheb_step(T* d, T* z, const T* res, const T* dinv, T c1, T c2, size_t n, cudaStream_t s) {
-  k_cheb<T><<<grid_for(n), 256, 0, s>>>(d, z, res, dinv, c1, c2, n);
+  pdl_launch(k_cheb<T>, dim3(grid_for(n)), dim3(256), 0, s, d, z, res, dinv, c1, c2, n);
   note_launch();
 }
 template <typename T>
 void block_matvec(T* y, const T* B, const T* x, int nb, int Np, cudaStream_t s) {
-  k_block_matvec<T><<<grid_for((size_t)nb * Np), 256, 0, s>>>(y, B, x, nb, Np);
+  pdl_launch(k_block_matvec<T>, dim3(grid_for((size_t)nb * Np)), dim3(256), 0, s, y, B, x, nb, Np);
   note_launch();
 }
 template <typename T>
 void inv_mass(T* y, const T* x, const T* Minv, const T* geof, int ngeof, int jidx, int K, int Np,
               int ncomp, T scale, cudaStream_t s) {
-  k_inv_mass<T><<<grid_for((size_t)ncomp * K * Np), 256, 0, s>>>(y, x, Minv, geof, ngeof, jidx, K, Np, ncomp, scale);
+  pdl_launch(k_inv_mass<T>, dim3(grid_for((size_t)ncomp * K * Np)), dim3(256), 0, s, y, x, Minv, geof, ngeof, jidx, K, Np, ncomp, scale);
   note_launch();
 }
 template <typename T>
 void restrict_elem(T* rc, const T* r, const T* P, int K, int Npf, int Npc, int ncomp, cudaStream_t s) {
-  k_restrict<T><<<grid_for((size_t)ncomp * K * Npc), 256, 0, s>>>(rc, r, P, K, Npf, Npc, ncomp);
+  pdl_launch(k_restrict<T>, dim3(grid_for((size_t)ncomp * K * Npc)), dim3(256), 0, s, rc, r, P, K, Npf, Npc, ncomp);
   note_launch();
 }
 template <typename T>
 void prolong_add(T* z, const T* zc, const T* P, int K, int Npf, int Npc, int ncomp, cudaStream_t s) {
-  k_prolong_add<T><<<grid_for((size_t)ncomp * K * Npf), 256, 0, s>>>(z, zc, P, K, Npf, Npc, ncomp);
+  pdl_launch(k_prolong_add<T>, dim3(grid_for((size_t)ncomp * K * Npf)), dim3(256), 0, s, z, zc, P, K, Npf, Npc, ncomp);
   note_launch();
 }
 template <typename T>
 void coarse_update(T* z, T* r, T* sv, const T* p, const T* Ap, const T* dinv, size_t n, double* scal,
                    const RedWork& w, cudaStream_t s) {
-  k_coarse_update<T><<<kRedBlocks, kRedThreads, 0, s>>>(z, r, sv, p, Ap, dinv, n, scal, w.partial, w.counter);
+  pdl_launch(k_coarse_update<T>, dim3(kRedBlocks), dim3(kRedThreads), 0, s, z, r, sv, p, Ap, dinv, n, scal, w.partial, w.counter);
   note_launch();
 }
 template <typename T>
 void coarse_update_p(T* p, const T* sv, size_t n, double* scal, cudaStream_t s) {
-  k_coarse_update_p<T><<<grid_for(n), 256, 0, s>>>(p, sv, n, scal);
+  pdl_launch(k_coarse_update_p<T>, dim3(grid_for(n)), dim3(256), 0, s, p, sv, n, scal);
   note_launch();
-  k_shift_scalar<<<1, 1, 0, s>>>(scal, S_C_RZN, S_C_RZ);
+  pdl_launch(k_shift_scalar, dim3(1), dim3(1), 0, s, scal, S_C_RZN, S_C_RZ);
   note_launch();
 }
 
 template <typename T>
 void csr_spmv(int rows, const int* ptr, const int* idx, const T* val, const T* x, T* y, T alpha, T beta,
               cudaStream_t s) {
-  k_csr_spmv<T><<<grid_for((size_t)rows), 256, 0, s>>>(rows, ptr, idx, val, x, y, alpha, beta);
+  pdl_launch(k_csr_spmv<T>, dim3(grid_for((size_t)rows)), dim3(256), 0, s, rows, ptr, idx, val, x, y, alpha, beta);
   note_launch();
 }
 template <typename T>
 void dense_mv(int n, const T* M, const T* x, T* y, cudaStream_t s) {
   int blocks = std::max(1, std::min((n * 32 + 255) / 256, 148 * 8));
-  k_dense_mv<T><<<blocks, 256, 0, s>>>(n, M, x, y);
+  pdl_launch(k_dense_mv<T>, dim3(blocks), dim3(256), 0, s, n, M, x, y);
   note_launch();
 }
 template <typename T>
 void vadd(T* y, const T* x, size_t n, cudaStream_t s) {
-  k_vadd<T><<<grid_for(n), 256, 0, s>>>(y, x, n);
+  pdl_launch(k_vadd<T>, dim3(grid_for(n)), dim3(256), 0, s, y, x, n);
   note_launch();
 }
 
