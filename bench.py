@@ -359,8 +359,54 @@ def run_reference(args):
     print(json.dumps(out))
 
 
+def run_profile(args):
+    """Small fixed workloads for ncu captures (no timing is reported from them).
+
+    apply: the headline operator at --n (order --order, precision --precision),
+           3 applies after set-up; with -k regex:"sipg_(trace|apply_tc)" -s 2 -c 2
+           ncu captures the second apply's two kernels.
+    solve: the headline mixed solve: one warm-up solve, then the captured solve;
+           prints the number of kernels launched before it (ncu -s) and in it (-c).
+    """
+    c = W.poisson3d_two_phase(args.n, order=ORDER, n_modes=256, pin=False)
+    if args.profile == "apply":
+        op = sipg.Operator(c["mesh"], args.order, 1)
+        op.set_bc_types(c["bc_types"])
+        if args.order == ORDER:
+            op.set_factor(c["factor"])
+        t = np.float32 if args.precision == 32 else np.float64
+        K, Np = c["mesh"].K, op.Np
+        x = sipg.DeviceVector(np.random.default_rng(1).uniform(-1, 1, K * Np).astype(t))
+        y = sipg.DeviceVector(np.zeros(K * Np, t))
+        for _ in range(3):
+            op.apply_device(args.precision, x.ptr, y.ptr)
+        sipg.check(sipg.lib().sipg_device_synchronize())
+        print("done", K)
+        return
+    c2, op = build_headline() if args.n == N_HEAD else (c, None)
+    if op is None:
+        op = sipg.Operator(c["mesh"], ORDER, 1)
+        op.set_bc_types(c["bc_types"])
+        op.set_factor(c["factor"])
+    s, _ = pmg_solver(op, args.precision)
+    b = sipg.DeviceVector(c2["rhs"].reshape(-1))
+    x = sipg.DeviceVector(np.zeros(c2["rhs"].size))
+    s.solve_device(b.ptr, x.ptr)
+    x = sipg.DeviceVector(np.zeros(c2["rhs"].size))
+    sipg.check(sipg.lib().sipg_device_synchronize())
+    n1 = launches()
+    info = s.solve_device(b.ptr, x.ptr)
+    sipg.check(sipg.lib().sipg_device_synchronize())
+    print("skip", n1, "count", launches() - n1, "iters", info.iters)
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--profile", choices=["apply", "solve"], default=None,
+                    help="run a small fixed workload for an ncu capture instead of the benchmark")
+    ap.add_argument("--n", type=int, default=N_HEAD)
+    ap.add_argument("--order", type=int, default=ORDER)
+    ap.add_argument("--precision", type=int, default=32, choices=[32, 64])
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
@@ -368,7 +414,9 @@ def main():
     ap.add_argument("--skip-c3", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.profile:
+        run_profile(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

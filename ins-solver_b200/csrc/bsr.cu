@@ -42,34 +42,34 @@ __global__ void k_d2f(float* dst, const double* src, size_t n) {
     dst[i] = (float)src[i];
 }
 
+// One thread per (row r, element e), e fastest: block reads are coalesced and
+// there are Np threads per element row to hide the gather latency.
 template <typename T, int NP, int NF>
 __global__ void __launch_bounds__(256) k_bsr(int K, const T* __restrict__ v, const int* __restrict__ nbr,
                                              const T* __restrict__ x, T* __restrict__ y, T alpha, T beta) {
   pdl_enter();
   const size_t K_ = (size_t)K;
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < K; e += gridDim.x * blockDim.x) {
-    T acc[NP];
+  const size_t total = K_ * NP;
+  for (size_t tid = blockIdx.x * (size_t)blockDim.x + threadIdx.x; tid < total; tid += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(tid / K_);
+    const int e = (int)(tid - (size_t)r * K_);
+    int ks[NF + 1];
+    ks[0] = e;
 #pragma unroll
-    for (int r = 0; r < NP; ++r) acc[r] = T(0);
+    for (int f = 0; f < NF; ++f) ks[f + 1] = nbr[(size_t)e * NF + f];
+    T acc = T(0);
 #pragma unroll
     for (int s = 0; s <= NF; ++s) {
-      const int k = s == 0 ? e : nbr[(size_t)e * NF + s - 1];
+      const int k = ks[s];
       if (k < 0) continue;
-      T xv[NP];
+      const T* vs = v + ((size_t)(s * NP + r) * NP) * K_ + e;
+      const T* xk = x + (size_t)k * NP;
 #pragma unroll
-      for (int c = 0; c < NP; ++c) xv[c] = x[(size_t)k * NP + c];
-      const T* vs = v + (size_t)s * NP * NP * K_ + e;
-#pragma unroll
-      for (int r = 0; r < NP; ++r)
-#pragma unroll
-        for (int c = 0; c < NP; ++c) acc[r] += vs[(size_t)(r * NP + c) * K_] * xv[c];
+      for (int c = 0; c < NP; ++c) acc += vs[(size_t)c * K_] * xk[c];
     }
-#pragma unroll
-    for (int r = 0; r < NP; ++r) {
-      T o = alpha * acc[r];
-      if (beta != T(0)) o += beta * y[(size_t)e * NP + r];
-      y[(size_t)e * NP + r] = o;
-    }
+    T o = alpha * acc;
+    if (beta != T(0)) o += beta * y[(size_t)e * NP + r];
+    y[(size_t)e * NP + r] = o;
   }
 }
 
@@ -152,7 +152,7 @@ template <typename T>
 void bsr_apply(const BsrOp& B, const T* x, T* y, T alpha, T beta, cudaStream_t s) {
   const T* v = std::is_same<T, double>::value ? (const T*)B.v64.p : (const T*)B.v32.p;
   if (!v) throw Error(SIPG_INVALID_ARG, "assembled blocks missing for this precision");
-  const int g = grid_of(B.K);
+  const int g = (int)std::max<size_t>(1, std::min<size_t>(((size_t)B.K * B.Np + 255) / 256, 148 * 32));
   if (B.dim == 3 && B.Np == 4) pdl_launch(k_bsr<T, 4, 4>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta);
   else if (B.dim == 3 && B.Np == 10) pdl_launch(k_bsr<T, 10, 4>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta);
   else if (B.dim == 2 && B.Np == 3) pdl_launch(k_bsr<T, 3, 3>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta);

@@ -76,6 +76,33 @@ def _ip(a):
     return a.ctypes.data_as(C.POINTER(C.c_int)) if a is not None else None
 
 
+class DeviceVector:
+    """A device copy of a host array, allocated through the library's own helpers
+    (no torch or CUDA toolkit needed by the caller)."""
+
+    def __init__(self, host):
+        self.host = np.ascontiguousarray(host)
+        self.nbytes = self.host.nbytes
+        self._p = C.c_void_p()
+        check(lib().sipg_dev_alloc(C.c_size_t(self.nbytes), C.byref(self._p)))
+        check(lib().sipg_memcpy_h2d(self._p, self.host.ctypes.data_as(C.c_void_p), C.c_size_t(self.nbytes)))
+
+    @property
+    def ptr(self):
+        return self._p.value
+
+    def get(self):
+        out = np.empty_like(self.host)
+        check(lib().sipg_device_synchronize())
+        check(lib().sipg_memcpy_d2h(out.ctypes.data_as(C.c_void_p), self._p, C.c_size_t(self.nbytes)))
+        return out
+
+    def __del__(self):
+        if getattr(self, "_p", None) is not None and self._p.value:
+            lib().sipg_dev_free(self._p)
+            self._p = None
+
+
 def device_count():
     n = C.c_int(0)
     check(lib().sipg_device_count(C.byref(n)))
