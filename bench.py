@@ -184,7 +184,7 @@ def apply_bytes_per_elem(Np, ts, factor, ngeof=10, nf=4, gface=5):
 # DRAM traffic of one FP32 p=3 apply (trace + apply kernels) at the headline
 # size, ncu capture with flushed caches (dram__bytes_read.sum + dram__bytes_write.sum
 # of both launches): profiles/apply_tc_fp32_p3_24cube.txt
-APPLY_P3_FP32_TRAFFIC = 16.629e6 + 0.0018e6 + 46.211e6 + 0.203e6
+APPLY_P3_FP32_TRAFFIC = 16.628e6 + 0.030e6 + 46.211e6 + 0.205e6
 
 
 def run_ours(args):
