@@ -221,6 +221,17 @@ int sipg_amg_level(const sipg_amg *a, int level, int which, int *rows, int *cols
 int sipg_amg_coarse_inverse(const sipg_amg *a, double *inv);
 void sipg_amg_destroy(sipg_amg *a);
 
+/* ---- initial guess: replaces initial_guess_extrapolation(mesh, pr_history, pr,
+ * time + dt) (src/solvers/3d/ins_solver.cpp:342-343, mp_ins_solver.cpp:629-630;
+ * history kept by add_to_pr_history, ins_solver_base.cpp:1374-1388). out = the
+ * polynomial through the n_hist (1..8) points (times[i], hist[i]) evaluated at
+ * t_new (Lagrange form; one point copies it). n values per vector; device
+ * pointers (stream: cudaStream_t or NULL) or, in the _host variant, host pointers. */
+int sipg_extrapolate_initial_guess(int n_hist, const double *times, const double *const *hist, double t_new,
+                                   size_t n, double *out, void *stream);
+int sipg_extrapolate_initial_guess_host(int n_hist, const double *times, const double *const *hist,
+                                        double t_new, size_t n, double *out);
+
 /* Number of kernels this library has launched so far in the process
  * (diagnostics for benchmarks; no reference counterpart). */
 int sipg_launch_count(unsigned long long *n);

@@ -103,6 +103,26 @@ class DeviceVector:
             self._p = None
 
 
+def extrapolate_initial_guess(times, history, t_new):
+    """Initial guess at t_new from previous solutions (host arrays), the polynomial
+    through (times[i], history[i]) -- initial_guess_extrapolation of the reference."""
+    hs = [np.ascontiguousarray(h, dtype=np.float64) for h in history]
+    t = np.ascontiguousarray(times, dtype=np.float64)
+    out = np.empty_like(hs[0])
+    ptrs = (C.c_void_p * len(hs))(*[h.ctypes.data for h in hs])
+    check(lib().sipg_extrapolate_initial_guess_host(len(hs), _dp(t), ptrs, C.c_double(t_new),
+                                                    C.c_size_t(out.size), _dp(out)))
+    return out
+
+
+def extrapolate_initial_guess_device(times, history_ptrs, t_new, n, out_ptr, stream=None):
+    """Device variant: history_ptrs and out_ptr are device pointers of n FP64 values."""
+    t = np.ascontiguousarray(times, dtype=np.float64)
+    ptrs = (C.c_void_p * len(history_ptrs))(*history_ptrs)
+    check(lib().sipg_extrapolate_initial_guess(len(history_ptrs), _dp(t), ptrs, C.c_double(t_new),
+                                               C.c_size_t(n), C.c_void_p(out_ptr), C.c_void_p(stream or 0)))
+
+
 def device_count():
     n = C.c_int(0)
     check(lib().sipg_device_count(C.byref(n)))

@@ -1,0 +1,131 @@
+// Drives the C++ classes of include/ins_solver_b200/solvers.hpp the way the
+// reference's time-step code drives its solvers (set_matrix, set_bc_types,
+// set_factor, set_tol_and_iter, solve -> bool) on a small jittered tetrahedral box.
+// Right-hand sides are b = A x_true, so every solve can be checked against x_true.
+#include <cmath>
+#include <cstdio>
+#include <random>
+#include <vector>
+
+#include "ins_solver_b200/solvers.hpp"
+
+using namespace ins_solver_b200;
+
+static double rel_diff(const std::vector<double>& a, const std::vector<double>& b, bool remove_mean) {
+  double ma = 0, mb = 0;
+  if (remove_mean) {
+    for (size_t i = 0; i < a.size(); ++i) { ma += a[i]; mb += b[i]; }
+    ma /= a.size(); mb /= b.size();
+  }
+  double num = 0, den = 0;
+  for (size_t i = 0; i < a.size(); ++i) {
+    num = std::max(num, std::fabs((a[i] - ma) - (b[i] - mb)));
+    den = std::max(den, std::fabs(b[i] - mb));
+  }
+  return num / den;
+}
+
+int main() {
+  const int n = 4, order = 3, Np = 20;
+  int nv = 0, k = 0;
+  check(sipg_box_mesh_sizes(3, n, &nv, &k), "box sizes");
+  std::vector<double> vx(3 * (size_t)nv);
+  std::vector<int> e2v(4 * (size_t)k);
+  check(sipg_box_mesh(3, n, 0.1, 7, vx.data(), e2v.data()), "box");
+  DGMesh3D mesh(nv, vx.data(), k, e2v.data());
+  const int kb = mesh.num_bfaces();
+  std::mt19937_64 rng(11);
+  std::uniform_real_distribution<double> U(-1.0, 1.0), F(0.2, 3.0);
+  const size_t N = (size_t)k * Np;
+  int failures = 0;
+
+  {  // pressure: variable coefficient, Neumann walls + nullspace, p-multigrid (mixed precision)
+    FactorPoissonMatrixFreeDiag3D A(&mesh, order);
+    FactorPoissonCoarseMatrix3D coarse(&mesh);
+    std::vector<int> bct(kb, 1);
+    std::vector<double> f(N), xt(N), b(N), x(N, 0.0);
+    for (auto& v : f) v = F(rng);
+    for (auto& v : xt) v = U(rng);
+    A.set_bc_types(IntDat{bct.data(), kb, 1});
+    A.set_factor(Dat{f.data(), k, Np});
+    A.mult(Dat{xt.data(), k, Np}, Dat{b.data(), k, Np});
+    PETScPMultigrid solver(&mesh);
+    solver.set_coarse_matrix(&coarse);
+    solver.set_matrix(&A);
+    solver.set_nullspace(true);
+    solver.set_tol_and_iter(1e-10, 0.0, 200);
+    solver.set_precision(SIPG_FP32);
+    solver.init();
+    const bool ok = solver.solve(Dat{b.data(), k, Np}, Dat{x.data(), k, Np});
+    const double err = rel_diff(x, xt, true);
+    std::printf("pressure pmultigrid converged=%d iters=%d err=%.3e\n", ok, solver.last_info().iters, err);
+    failures += !(ok && err < 1e-6);
+    // a new coefficient: the solver re-runs its set-up on the next solve
+    for (auto& v : f) v *= 2.0;
+    A.set_factor(Dat{f.data(), k, Np});
+    std::vector<double> x2(N, 0.0);
+    const bool ok2 = solver.solve(Dat{b.data(), k, Np}, Dat{x2.data(), k, Np});
+    std::vector<double> half(xt);
+    for (auto& v : half) v *= 0.5;
+    const double err2 = rel_diff(x2, half, true);
+    std::printf("pressure after set_factor converged=%d err=%.3e\n", ok2, err2);
+    failures += !(ok2 && err2 < 1e-6);
+  }
+  {  // viscous: Helmholtz c M + K, Dirichlet walls, inverse-mass PCG
+    MMPoissonMatrixFree3D A(&mesh, order);
+    std::vector<int> bct(kb, 0);
+    std::vector<double> xt(N), b(N), x(N, 0.0);
+    for (auto& v : xt) v = U(rng);
+    A.set_bc_types(IntDat{bct.data(), kb, 1});
+    A.set_factor(100.0);
+    A.mult(Dat{xt.data(), k, Np}, Dat{b.data(), k, Np});
+    PETScInvMassSolver solver(&mesh);
+    solver.set_matrix(&A);
+    solver.setFactor(1.0 / 100.0);
+    solver.set_tol_and_iter(1e-10, 0.0, 2000);
+    const bool ok = solver.solve(Dat{b.data(), k, Np}, Dat{x.data(), k, Np});
+    const double err = rel_diff(x, xt, false);
+    std::printf("viscous inv-mass converged=%d iters=%d err=%.3e\n", ok, solver.last_info().iters, err);
+    failures += !(ok && err < 1e-6);
+  }
+  {  // slip viscous solve on (u, v, w)
+    ViscousMatrix3D A(&mesh, order);
+    std::vector<int> bu(kb, 0), bv(kb, 0), bw(kb, 0);
+    for (int i = 0; i < kb; i += 3) bu[i] = bv[i] = bw[i] = 2;
+    A.set_bc_types(IntDat{bu.data(), kb, 1}, IntDat{bv.data(), kb, 1}, IntDat{bw.data(), kb, 1});
+    A.set_factor(50.0);
+    std::vector<double> xt[3], b[3], x[3];
+    for (int c = 0; c < 3; ++c) {
+      xt[c].resize(N); b[c].resize(N); x[c].assign(N, 0.0);
+      for (auto& v : xt[c]) v = U(rng);
+    }
+    auto D = [&](std::vector<double>& v) { return Dat{v.data(), k, Np}; };
+    A.mult(D(xt[0]), D(xt[1]), D(xt[2]), D(b[0]), D(b[1]), D(b[2]));
+    ViscousSolver3D solver(&mesh);
+    solver.set_matrix(&A);
+    solver.set_preconditioner(ViscousSolver3D::FACTOR_INV_MASS);
+    solver.set_inv_mass_factor(1.0 / 50.0);
+    solver.set_tol_and_iter(1e-8, 1e-11, 5000);
+    const bool ok = solver.solve(D(b[0]), D(b[1]), D(b[2]), D(x[0]), D(x[1]), D(x[2]));
+    double err = 0;
+    for (int c = 0; c < 3; ++c) err = std::max(err, rel_diff(x[c], xt[c], false));
+    std::printf("slip viscous converged=%d iters=%d err=%.3e\n", ok, solver.last_info().iters, err);
+    failures += !(ok && err < 1e-5);  // absolute stopping test of the reference (viscous_solver.cpp:117)
+  }
+  {  // initial guess from the pressure history: exact for data quadratic in time
+    PressureHistory hist(3);
+    std::vector<double> p(N), q(N);
+    auto value = [](size_t i, double t) { return (double)(i % 7) + 0.5 * t - 0.25 * t * t; };
+    for (double t : {0.1, 0.2, 0.3}) {
+      for (size_t i = 0; i < N; ++i) p[i] = value(i, t);
+      hist.add(t, Dat{p.data(), k, Np});
+    }
+    hist.initial_guess_extrapolation(Dat{q.data(), k, Np}, 0.4);
+    double err = 0;
+    for (size_t i = 0; i < N; ++i) err = std::max(err, std::fabs(q[i] - value(i, 0.4)));
+    std::printf("initial_guess_extrapolation err=%.3e\n", err);
+    failures += !(err < 1e-12);
+  }
+  std::printf("%s\n", failures ? "FAILED" : "OK");
+  return failures ? 1 : 0;
+}
