@@ -221,6 +221,41 @@ int sipg_amg_level(const sipg_amg *a, int level, int which, int *rows, int *cols
 int sipg_amg_coarse_inverse(const sipg_amg *a, double *inv);
 void sipg_amg_destroy(sipg_amg *a);
 
+/* ---- serving loop: no reference counterpart (the reference solves one system at
+ * a time inside its time step). Requests (an operator on a resident mesh, solver
+ * kind and options, a right-hand side) arrive at any time; up to `slots` solves
+ * run concurrently, each on its own CUDA stream, so their kernels overlap on the
+ * device. A queued request is admitted as soon as a slot is free, its operator is
+ * not busy with another request, and its solver state fits the HBM budget
+ * (solver states stay resident between requests for the same operator and
+ * options, least recently used first out when the budget needs room). */
+typedef struct {
+  int slots;                  /* concurrent solves (worker threads), >= 1 */
+  size_t hbm_budget_bytes;    /* device bytes for resident solver state; 0: 90% of the free memory */
+} sipg_server_opts;
+
+typedef struct {
+  int status;                 /* SIPG_OK, SIPG_NOT_CONVERGED, SIPG_BREAKDOWN, SIPG_CANCELLED, ... */
+  sipg_solve_info info;
+  double queue_ms;            /* submit -> start */
+  double run_ms;              /* start -> done (includes a solver set-up on first use) */
+  double total_ms;            /* submit -> done */
+} sipg_request_result;
+
+int sipg_server_create(const sipg_server_opts *o, sipg_server **out);
+/* b: host right-hand side, copied at submit; x: host initial guess, read at start,
+ * overwritten with the solution; it must stay valid until the request is done. */
+int sipg_server_submit(sipg_server *s, sipg_op *op, int kind, const sipg_solver_opts *o, const double *b,
+                       double *x, long long *id);
+/* done = 1 and res filled once the request has finished. */
+int sipg_server_poll(sipg_server *s, long long id, int *done, sipg_request_result *res);
+int sipg_server_wait(sipg_server *s, long long id, sipg_request_result *res);
+/* A queued request is dropped; a running one stops after its current iteration. */
+int sipg_server_cancel(sipg_server *s, long long id);
+/* Resident solver states and bytes accounted against the budget. */
+int sipg_server_stats(sipg_server *s, int *resident_solvers, size_t *resident_bytes, int *queued, int *running);
+void sipg_server_destroy(sipg_server *s);
+
 /* ---- initial guess: replaces initial_guess_extrapolation(mesh, pr_history, pr,
  * time + dt) (src/solvers/3d/ins_solver.cpp:342-343, mp_ins_solver.cpp:629-630;
  * history kept by add_to_pr_history, ins_solver_base.cpp:1374-1388). out = the

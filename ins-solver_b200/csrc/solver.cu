@@ -15,6 +15,8 @@
 // lengths, and the final defect r = b - A x stay FP64.
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -187,6 +189,7 @@ struct sipg_solver {
   unsigned long long gnodes[2] = {0, 0};
   unsigned gver = 0;
   bool graph_broken = false;
+  const std::atomic<int>* cancel = nullptr;  // set by a serving loop: non-zero ends the solve
 
   double* S() const { return scal.as<double>(); }
   void drop_graphs() {
@@ -730,6 +733,7 @@ int sipg_solver::solve(const double* b, double* x_user, sipg_solve_info* info) {
       const double pap = hs.h[S_PAP];
       res = std::sqrt(hs.h[S_RR]);
       if (!(pap > 0.0) || !std::isfinite(res)) { status = SIPG_BREAKDOWN; break; }
+      if (cancel && cancel->load(std::memory_order_relaxed)) { status = SIPG_CANCELLED; break; }
     }
   } else {
     // flexible PCG (viscous_solver.cpp:177-301)
@@ -769,6 +773,7 @@ int sipg_solver::solve(const double* b, double* x_user, sipg_solve_info* info) {
       const double pap = hs.h[S_PAP];
       res = std::sqrt(hs.h[S_RR]);
       if (!(pap > 0.0) || !std::isfinite(res)) { status = SIPG_BREAKDOWN; break; }
+      if (cancel && cancel->load(std::memory_order_relaxed)) { status = SIPG_CANCELLED; break; }
     }
   }
   if (status == SIPG_OK && res > tol) status = SIPG_NOT_CONVERGED;
@@ -796,6 +801,11 @@ int sipg_solver::solve(const double* b, double* x_user, sipg_solve_info* info) {
   }
   return status;
 }
+
+namespace sipg {
+void solver_set_cancel(sipg_solver* s, const std::atomic<int>* flag) { s->cancel = flag; }
+cudaStream_t solver_stream(sipg_solver* s) { return s->stream; }
+}  // namespace sipg
 
 extern "C" {
 

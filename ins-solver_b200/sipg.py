@@ -343,6 +343,66 @@ class Amg:
             self.h = None
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("slots", C.c_int), ("hbm_budget_bytes", C.c_size_t)]
+
+
+class RequestResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("info", SolveInfo), ("queue_ms", C.c_double), ("run_ms", C.c_double),
+                ("total_ms", C.c_double)]
+
+
+class Server:
+    """Serving loop: concurrent solves of independent requests (sipg_server_*)."""
+
+    def __init__(self, slots=2, hbm_budget_bytes=0):
+        self.h = C.c_void_p()
+        o = ServerOpts(slots, hbm_budget_bytes)
+        check(lib().sipg_server_create(C.byref(o), C.byref(self.h)))
+        self._pending = {}
+
+    def submit(self, op, kind, opts, b, x0=None):
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros_like(b) if x0 is None else np.ascontiguousarray(x0, dtype=np.float64).copy()
+        rid = C.c_longlong()
+        check(lib().sipg_server_submit(self.h, op.h, kind, C.byref(opts) if opts is not None else None,
+                                       _dp(b), _dp(x), C.byref(rid)))
+        self._pending[rid.value] = (op, x)
+        return rid.value
+
+    def wait(self, rid):
+        res = RequestResult()
+        check(lib().sipg_server_wait(self.h, C.c_longlong(rid), C.byref(res)))
+        op, x = self._pending.pop(rid)
+        return x, res
+
+    def poll(self, rid):
+        res = RequestResult()
+        done = C.c_int()
+        check(lib().sipg_server_poll(self.h, C.c_longlong(rid), C.byref(done), C.byref(res)))
+        if not done.value:
+            return None
+        op, x = self._pending.pop(rid)
+        return x, res
+
+    def cancel(self, rid):
+        check(lib().sipg_server_cancel(self.h, C.c_longlong(rid)))
+
+    def stats(self):
+        a, q, r = C.c_int(), C.c_int(), C.c_int()
+        b = C.c_size_t()
+        check(lib().sipg_server_stats(self.h, C.byref(a), C.byref(b), C.byref(q), C.byref(r)))
+        return {"resident": a.value, "resident_bytes": b.value, "queued": q.value, "running": r.value}
+
+    def close(self):
+        if getattr(self, "h", None) and self.h:
+            lib().sipg_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
 def default_opts(kind):
     o = SolverOpts()
     check(lib().sipg_solver_default_opts(kind, C.byref(o)))
