@@ -288,6 +288,8 @@ def run_ours(args):
                      "apply_ms": a32, "elements": K},
         "clocks": clk.summary(),
     }
+    if not args.skip_serving:
+        out["serving"] = run_serving(seed=1234 + rank)
     if rank == 0 and world == 1 and not args.skip_cpu:
         out["cpu_baseline"] = cpu_reference(c, op, int(inf64[-1].iters), sample_only=True)
     if world > 1:
@@ -295,6 +297,84 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
     if rank == 0:
         print(json.dumps(out))
+
+
+def serving_problems(rng):
+    """A pool of resident problems for the served stream: 2D and 3D jittered boxes,
+    orders 2 and 3, constant or two-phase (ratio 1000) coefficient, element counts
+    from 2e3 to 1.1e4 (a scaled-down form of the served-stream configuration)."""
+    probs = []
+    for dim, n, order in ((3, 8, 2), (3, 10, 3), (3, 12, 2), (2, 32, 3), (2, 64, 2), (2, 48, 3)):
+        if dim == 3:
+            c = W.poisson3d_two_phase(n, order=order, n_modes=64, pin=False)
+            factor = c["factor"] if rng.random() < 0.5 else None
+            bct, rhs = c["bc_types"], c["rhs"].reshape(-1)
+        else:
+            c = W.poisson2d_manufactured(n, order=order)
+            factor, bct, rhs = None, c["bc_types"], c["rhs"].reshape(-1)
+        op = sipg.Operator(c["mesh"], order, 1)
+        op.set_bc_types(bct)
+        if factor is not None:
+            op.set_factor(factor)
+        singular = dim == 3
+        probs.append((op, rhs, singular, order))
+    return probs
+
+
+def serving_opts(order, singular, precision):
+    o = sipg.default_opts(sipg.SOLVER_PMULTIGRID)
+    o.precision, o.rel_tol, o.abs_tol, o.max_iter, o.nullspace = precision, 1e-8, 0.0, 500, int(singular)
+    o.n_levels = order
+    for i in range(order):
+        o.orders[i] = order - i
+    return o
+
+
+def run_serving(seed, n_req=96, rate=400.0, slots=4):
+    """Served stream: n_req requests with Poisson arrivals at `rate` per second over
+    the problem pool, mixed-precision p-multigrid to 1e-8, `slots` concurrent solves;
+    against the same requests solved one at a time on the plain FP64 path."""
+    rng = np.random.default_rng(seed)
+    probs = serving_problems(rng)
+    pick = rng.integers(0, len(probs), n_req)
+    gaps = rng.exponential(1.0 / rate, n_req)
+    srv = sipg.Server(slots=slots)
+    # resident solver states: one warm request per problem (set-up is not part of the stream)
+    for op, rhs, sing, order in probs:
+        srv.wait(srv.submit(op, sipg.SOLVER_PMULTIGRID, serving_opts(order, sing, sipg.FP32), rhs))
+    ids = []
+    t0 = time.perf_counter()
+    t_next = t0
+    for i in range(n_req):
+        t_next += gaps[i]
+        while time.perf_counter() < t_next:
+            time.sleep(max(0.0, min(0.001, t_next - time.perf_counter())))
+        op, rhs, sing, order = probs[pick[i]]
+        ids.append(srv.submit(op, sipg.SOLVER_PMULTIGRID, serving_opts(order, sing, sipg.FP32), rhs))
+    lat, bad = [], 0
+    for rid in ids:
+        _, res = srv.wait(rid)
+        lat.append(res.total_ms)
+        bad += res.status != sipg.SIPG_OK
+    served_s = time.perf_counter() - t0
+    srv.close()
+    # sequential plain FP64 solves of the same requests (solvers set up beforehand)
+    seq = [sipg.Solver(op, sipg.SOLVER_PMULTIGRID, serving_opts(order, sing, sipg.FP64)) for op, _, sing, order in probs]
+    for (op, rhs, _, _), s in zip(probs, seq):
+        s.solve_host(rhs)
+    t1 = time.perf_counter()
+    for i in range(n_req):
+        op, rhs, _, _ = probs[pick[i]]
+        seq[pick[i]].solve_host(rhs)
+    seq_s = time.perf_counter() - t1
+    lat = np.array(lat)
+    return {"workload": f"{n_req} requests, Poisson arrivals {rate:g}/s, {len(probs)} resident problems "
+                        "(2D/3D, p=2/3, K 2048..10368, constant or two-phase coefficient), mixed p-MG to 1e-8, "
+                        f"{slots} slots",
+            "solves_per_s": n_req / served_s, "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "failed": int(bad),
+            "sequential_fp64_solves_per_s": n_req / seq_s,
+            "speedup_vs_sequential_fp64": (n_req / served_s) / (n_req / seq_s)}
 
 
 def cpu_reference(c, op, outer_iters, sample_only=False, steps=1, warmup=0):
@@ -413,6 +493,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-c3", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-serving", action="store_true")
     args = ap.parse_args()
     if args.profile:
         run_profile(args)
