@@ -434,7 +434,7 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libsipgref.so was not built"}))
         return
     c = W.poisson3d_two_phase(N_HEAD, order=ORDER, n_modes=256, pin=False)
-    outer = 31  # outer iterations of the FP64 p-MG path on this workload (measured on the GPU)
+    outer = 22  # outer iterations of the FP64 p-MG path on this workload (measured on the GPU)
     step_times = []
     for i in range(args.warmup + args.steps):
         r = cpu_reference(c, None, outer)

@@ -182,6 +182,8 @@ typedef struct {
   int assembled_max_order;   /* p-multigrid levels below the finest with this order or lower apply
                                 their operator as stored element blocks (assembled once from the
                                 matrix-free apply, scalar operators, orders <= 2); 0: all matrix-free */
+  int smoother;              /* p-multigrid smoothing: 0 Chebyshev on the point-Jacobi (diagonal)
+                                preconditioned operator, 1 on the element-block-Jacobi one */
 } sipg_solver_opts;
 
 int sipg_solver_default_opts(int kind, sipg_solver_opts *o);

@@ -13,6 +13,7 @@
 // Mixed precision: the V-cycle (smoother applies, transfers, coarse CG) runs in
 // FP32 while the outer flexible CG, its residual update, inner products and step
 // lengths, and the final defect r = b - A x stay FP64.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -54,6 +55,7 @@ struct Level {
   // work vectors in the V-cycle precision
   DevBuf rhs, z, res, d;
   DevBuf cp, cs, cAp;            // coarse CG
+  DevBuf bc64, bc32;             // inverse diagonal blocks, column-major (block-Jacobi smoothing; bc32 in bf16)
   std::unique_ptr<BsrOp> bsr;    // assembled element blocks (low orders), else matrix-free
   template <typename T>
   void apply(const T* x, T* y, cudaStream_t s, T alpha = T(1), T beta = T(0)) const {
@@ -236,7 +238,7 @@ struct sipg_solver {
   void setup_amg();
   void precondition(const double* rin, double* zout);
   int solve(const double* b, double* x, sipg_solve_info* info);
-  double power_lmax(sipg_op* lop, const double* dinv64, size_t nl);
+  double power_lmax(sipg_op* lop, const double* dinv64, size_t nl, const double* blocks = nullptr, int Np = 0);
 };
 
 // Diagonal of an operator (FP64), with its pinned DOF.
@@ -244,12 +246,13 @@ static void op_diag(sipg_op* op, double* out, cudaStream_t s) {
   SIPG_CUDA(launch_blocks(op->mesh->dim, op->order, op->block_args(BLOCK_DIAG_ONLY, 0, out, true), s));
 }
 
-double sipg_solver::power_lmax(sipg_op* lop, const double* dinv64, size_t nl) {
-  // Power iteration on D^-1 A from v0_i = U(-1,1), splitmix64 seed 0x5eed.
+double sipg_solver::power_lmax(sipg_op* lop, const double* dinv64, size_t nl, const double* blocks, int Np) {
+  // Power iteration on D^-1 A (D the diagonal, or the diagonal blocks when `blocks`
+  // holds their inverses row by row) from v0_i = U(-1,1), splitmix64 seed 0x5eed.
   std::vector<double> h(nl);
   uint64_t st = 0x5eedull;
   for (size_t i = 0; i < nl; ++i) h[i] = 2.0 * ((smix(&st) >> 11) * (1.0 / 9007199254740992.0)) - 1.0;
-  DevBuf v(nl * sizeof(double)), w(nl * sizeof(double));
+  DevBuf v(nl * sizeof(double)), w(nl * sizeof(double)), tb(blocks ? nl * sizeof(double) : 0);
   SIPG_CUDA(cudaMemcpyAsync(v.p, h.data(), nl * sizeof(double), cudaMemcpyHostToDevice, stream));
   double lam = 0.0;
   for (int it = 0; it < o.eig_iters; ++it) {
@@ -257,9 +260,14 @@ double sipg_solver::power_lmax(sipg_op* lop, const double* dinv64, size_t nl) {
     multi_dot<double>(a, a, 1, nl, S() + S_TMP, 1, rw, stream);
     k_scale<<<grid_for(nl), 256, 0, stream>>>(v.as<double>(), nl, S(), S_TMP);
       note_launch();
-    lop->apply<double>(v.as<double>(), w.as<double>(), stream);
-    k_mul<<<grid_for(nl), 256, 0, stream>>>(w.as<double>(), dinv64, nl);
+    if (blocks) {
+      lop->apply<double>(v.as<double>(), tb.as<double>(), stream);
+      block_matvec<double>(w.as<double>(), blocks, tb.as<double>(), (int)(nl / Np), Np, stream);
+    } else {
+      lop->apply<double>(v.as<double>(), w.as<double>(), stream);
+      k_mul<<<grid_for(nl), 256, 0, stream>>>(w.as<double>(), dinv64, nl);
       note_launch();
+    }
     const double* b[1] = {w.as<double>()};
     multi_dot<double>(b, b, 1, nl, S() + S_TMP, 1, rw, stream);
     lam = std::sqrt(read_scalar(S_TMP));
@@ -354,7 +362,24 @@ void sipg_solver::setup_pmg() {
     k_recip<<<grid_for(L.n), 256, 0, stream>>>(L.dinv64.as<double>(), L.n);
       note_launch();
     if (f32) to_f32(L.dinv32.as<float>(), L.dinv64.as<double>(), L.n, stream);
-    L.lmax = power_lmax(L.op, L.dinv64.as<double>(), L.n);
+    L.bc64 = DevBuf();
+    L.bc32 = DevBuf();
+    if (o.smoother == 1) {
+      // element-block Jacobi: inverse diagonal blocks, column-major in the level precision
+      const int nb = (int)(L.n / L.Np);
+      DevBuf rows((size_t)nb * L.Np * L.Np * sizeof(double));
+      SIPG_CUDA(launch_blocks(dim, L.order, L.op->block_args(BLOCK_INVERSE, 0, rows.as<double>(), true), stream));
+      if (f32) {  // bfloat16 blocks: the smoother tolerates 8 mantissa bits, and they stay in L2
+        L.bc32 = DevBuf((size_t)nb * L.Np * L.Np * sizeof(__nv_bfloat16));
+        block_transpose<__nv_bfloat16>(L.bc32.as<__nv_bfloat16>(), rows.as<double>(), nb, L.Np, stream);
+      } else {
+        L.bc64 = DevBuf((size_t)nb * L.Np * L.Np * sizeof(double));
+        block_transpose<double>(L.bc64.as<double>(), rows.as<double>(), nb, L.Np, stream);
+      }
+      L.lmax = power_lmax(L.op, nullptr, L.n, rows.as<double>(), L.Np);
+    } else {
+      L.lmax = power_lmax(L.op, L.dinv64.as<double>(), L.n);
+    }
     L.bsr.reset();
     if (l > 0 && L.order <= o.assembled_max_order && bsr_supported(dim, L.order, nc)) {
       L.bsr = std::make_unique<BsrOp>();
@@ -492,7 +517,14 @@ void sipg_solver::chebyshev(Level& L, bool want_res) {
       c2 = 2.0 * rho / delta;
       rho_old = rho;
     }
-    cheb_step<T>(d, z, res, dinv, (T)c1, (T)c2, L.n, stream);
+    if (L.bc32.p && std::is_same<T, float>::value) {
+      cheb_step_block<float, __nv_bfloat16>((float*)d, (float*)z, (const float*)res, L.bc32.as<__nv_bfloat16>(),
+                                            (float)c1, (float)c2, (int)(L.n / L.Np), L.Np, stream);
+    } else if (L.bc64.p) {
+      cheb_step_block<T, T>(d, z, res, (const T*)L.bc64.p, (T)c1, (T)c2, (int)(L.n / L.Np), L.Np, stream);
+    } else {
+      cheb_step<T>(d, z, res, dinv, (T)c1, (T)c2, L.n, stream);
+    }
     if (it < o.cheb_order - 1 || want_res) L.apply<T>(d, res, stream, T(-1), T(1));
   }
 }
@@ -832,6 +864,7 @@ int sipg_solver_default_opts(int kind, sipg_solver_opts* o) {
     o->amg_strength = 0.08;
     o->graphs = 1;
     o->assembled_max_order = 1;
+    o->smoother = 1;
     (void)kind;
   });
 }

@@ -2,6 +2,8 @@
 #include <algorithm>
 #include <atomic>
 
+#include <cuda_bf16.h>
+
 #include "pdl.cuh"
 #include "vecops.cuh"
 
@@ -173,6 +175,46 @@ __global__ void k_cheb(T* d, T* z, const T* res, const T* dinv, T c1, T c2, size
     T di = (c1 != T(0) ? c1 * d[i] : T(0)) + c2 * dinv[i] * res[i];
     d[i] = di;
     z[i] += di;
+  }
+}
+
+// Chebyshev step with an element-block Jacobi preconditioner: d <- c1 d + c2 B res,
+// z += d; B holds the inverse diagonal blocks column by column (Bc[b][c][r]) so
+// that the threads of one block read consecutive addresses.
+__device__ __forceinline__ float blk_val(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+__device__ __forceinline__ float blk_val(const float* p) { return *p; }
+__device__ __forceinline__ double blk_val(const double* p) { return *p; }
+
+template <typename T, typename TB>
+__global__ void k_cheb_block(T* d, T* z, const T* res, const TB* Bc, T c1, T c2, int nb, int Np) {
+  pdl_enter();
+  const size_t total = (size_t)nb * Np;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t b = i / Np;
+    const int r = (int)(i % Np);
+    const TB* Bb = Bc + b * Np * Np + r;
+    const T* rb = res + b * Np;
+    T s = T(0);
+    for (int c = 0; c < Np; ++c) s += (T)blk_val(Bb + (size_t)c * Np) * rb[c];
+    const T di = (c1 != T(0) ? c1 * d[i] : T(0)) + c2 * s;
+    d[i] = di;
+    z[i] += di;
+  }
+}
+
+// Row-major FP64 blocks -> column-major blocks in T.
+__device__ __forceinline__ void blk_store(__nv_bfloat16* p, double v) { *p = __double2bfloat16(v); }
+__device__ __forceinline__ void blk_store(float* p, double v) { *p = (float)v; }
+__device__ __forceinline__ void blk_store(double* p, double v) { *p = v; }
+template <typename T>
+__global__ void k_block_transpose(T* dst, const double* src, int nb, int Np) {
+  pdl_enter();
+  const size_t total = (size_t)nb * Np * Np;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t b = i / ((size_t)Np * Np);
+    const int q = (int)(i % ((size_t)Np * Np));
+    const int c = q / Np, r = q % Np;
+    blk_store(dst + i, src[(b * Np + r) * Np + c]);
   }
 }
 
@@ -368,6 +410,19 @@ void to_f64(double* dst, const float* src, size_t n, cudaStream_t s) {
   pdl_launch(k_to_f64, dim3(grid_for(n)), dim3(256), 0, s, dst, src, n);
   note_launch();
 }
+template <typename T, typename TB>
+void cheb_step_block(T* d, T* z, const T* res, const TB* Bc, T c1, T c2, int nb, int Np, cudaStream_t s) {
+  pdl_launch(k_cheb_block<T, TB>, dim3(grid_for((size_t)nb * Np)), dim3(256), 0, s, d, z, res, Bc, c1, c2, nb, Np);
+  note_launch();
+}
+template void cheb_step_block<float, __nv_bfloat16>(float*, float*, const float*, const __nv_bfloat16*, float, float,
+                                                    int, int, cudaStream_t);
+template void block_transpose<__nv_bfloat16>(__nv_bfloat16*, const double*, int, int, cudaStream_t);
+template <typename T>
+void block_transpose(T* dst, const double* src, int nb, int Np, cudaStream_t s) {
+  pdl_launch(k_block_transpose<T>, dim3(grid_for((size_t)nb * Np * Np)), dim3(256), 0, s, dst, src, nb, Np);
+  note_launch();
+}
 template <typename T>
 void jacobi(T* z, const T* r, const T* dinv, size_t n, cudaStream_t s) {
   pdl_launch(k_jacobi<T>, dim3(grid_for(n)), dim3(256), 0, s, z, r, dinv, n);
@@ -442,6 +497,8 @@ void vadd(T* y, const T* x, size_t n, cudaStream_t s) {
   template void jacobi<T>(T*, const T*, const T*, size_t, cudaStream_t);                         \
   template void cheb_step<T>(T*, T*, const T*, const T*, T, T, size_t, cudaStream_t);            \
   template void block_matvec<T>(T*, const T*, const T*, int, int, cudaStream_t);                 \
+  template void cheb_step_block<T, T>(T*, T*, const T*, const T*, T, T, int, int, cudaStream_t);  \
+  template void block_transpose<T>(T*, const double*, int, int, cudaStream_t);                     \
   template void inv_mass<T>(T*, const T*, const T*, const T*, int, int, int, int, int, T,        \
                             cudaStream_t);                                                       \
   template void restrict_elem<T>(T*, const T*, const T*, int, int, int, int, cudaStream_t);      \

@@ -6,6 +6,7 @@
 // the scalars never leave the device.
 #pragma once
 #include <cstddef>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 namespace sipg {
@@ -76,6 +77,11 @@ void jacobi(T* z, const T* r, const T* dinv, size_t n, cudaStream_t s);
 // Chebyshev step: d = c1 * d + c2 * dinv * res ; z += d
 template <typename T>
 void cheb_step(T* d, T* z, const T* res, const T* dinv, T c1, T c2, size_t n, cudaStream_t s);
+// d <- c1 d + c2 Bc res, z += d with column-major inverse diagonal blocks Bc (nb blocks of Np x Np)
+template <typename T, typename TB>
+void cheb_step_block(T* d, T* z, const T* res, const TB* Bc, T c1, T c2, int nb, int Np, cudaStream_t s);
+template <typename T>
+void block_transpose(T* dst, const double* src, int nb, int Np, cudaStream_t s);
 
 // Element-block matvec: y_e = B_e x_e (B: nb x Np x Np row-major, nb blocks)
 template <typename T>
