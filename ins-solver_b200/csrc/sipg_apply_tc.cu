@@ -165,17 +165,24 @@ __device__ __forceinline__ void copy_block(void* s, const void* base, size_t off
   }
 }
 
-// Rows r < nrows of LEN values (global rows contiguous from row0) into shared
-// rows of stride DS; rows at or past nvalid are zero-filled (zero) or skipped.
-template <typename T, int CB, int LEN, int DS>
-__device__ __forceinline__ void copy_rows(T* dst, const T* base, size_t row0, int nrows, int nvalid, int lane,
-                                          bool zero) {
-  constexpr int V = CB / (int)sizeof(T), CPR = LEN / V;
+// NR rows of LEN values (global rows contiguous from row0) into shared rows of
+// stride DS; rows at or past nvalid are zero-filled (zero) or skipped. Lane
+// handles row lane % NR and every (32 / NR)-th piece of it, so the row address is
+// computed once.
+template <typename T, int CB, int LEN, int DS, int NR>
+__device__ __forceinline__ void copy_rows(T* dst, const T* base, size_t row0, int nvalid, int lane, bool zero) {
+  constexpr int V = CB / (int)sizeof(T), CPR = LEN / V, LPR = 32 / NR;
   static_assert(LEN % V == 0, "row length must be a multiple of the copy piece");
-  for (int i = lane; i < nrows * CPR; i += 32) {
-    const int r = i / CPR, c = i % CPR;
-    const bool v = r < nvalid;
-    if (v || zero) cp_async_n<CB>(dst + r * DS + c * V, v ? base + (row0 + r) * LEN + c * V : base, v ? CB : 0);
+  static_assert(32 % NR == 0, "rows must divide the warp");
+  const int r = lane % NR, q = lane / NR;
+  const bool v = r < nvalid;
+  if (!v && !zero) return;
+  T* d = dst + r * DS;
+  const T* src = v ? base + (row0 + r) * LEN : base;
+#pragma unroll
+  for (int c0 = 0; c0 < CPR; c0 += LPR) {
+    const int c = c0 + q;
+    if (c < CPR) cp_async_n<CB>(d + c * V, v ? src + c * V : base, v ? CB : 0);
   }
 }
 
@@ -185,8 +192,8 @@ __device__ __forceinline__ void issue_elem(const ApplyArgs<T>& a, T* st, int til
   constexpr int NP = X::NP, NG = X::NG, NF = X::NF, TE = X::TE, S = sizeof(T);
   const int e0 = tile * TE;
   const int ne = max(0, min(TE, a.K - e0));
-  copy_rows<T, X::XCB, NP, X::XS>(st + X::SX, a.x, (size_t)e0, TE, ne, lane, true);
-  if (a.factor) copy_rows<T, X::XCB, NP, X::XS>(st + X::SF, a.factor, (size_t)e0, TE, ne, lane, true);
+  copy_rows<T, X::XCB, NP, X::XS, TE>(st + X::SX, a.x, (size_t)e0, ne, lane, true);
+  if (a.factor) copy_rows<T, X::XCB, NP, X::XS, TE>(st + X::SF, a.factor, (size_t)e0, ne, lane, true);
   copy_block(st + X::SG, a.geof, (size_t)e0 * NG * S, TE * NG * S, ne * NG * S, lane);
   if (pass2) copy_block(st + X::STAU, a.tau, (size_t)e0 * NF * S, TE * NF * S, ne * NF * S, lane);
 }
@@ -210,16 +217,23 @@ __device__ __forceinline__ void issue_traces(const ApplyArgs<T>& a, const T* tra
   constexpr int NF = X::NF, TE = X::TE, CH = X::CH, TR = X::TR, TS = X::TS, VPC = 16 / sizeof(T);
   const int e0 = tile * TE;
   const int ne = max(0, min(TE, a.K - e0));
-  copy_rows<T, 16, NF * TR, TS>(w + X::STR, trace, (size_t)e0, TE, ne, lane, false);
+  copy_rows<T, 16, NF * TR, TS, TE>(w + X::STR, trace, (size_t)e0, ne, lane, false);
   const int* nbr = slot;
   const int* code = slot + TE * NF;
-  for (int i = lane; i < TE * NF * CH; i += 32) {
-    const int lf = i / CH, c = i % CH;
-    const int el = lf / NF, f = lf % NF;
-    const int nb = nbr[lf];
-    if (el < ne && nb >= 0) {
-      const int fr = (code[el] >> (8 * f)) & 3;
-      cp_async_n<16>(w + X::SNB + el * TS + f * TR + c * VPC, trace + ((size_t)nb * NF + fr) * TR + c * VPC, 16);
+  // one neighbour record (CH pieces) per lane and round
+#pragma unroll
+  for (int lf0 = 0; lf0 < TE * NF; lf0 += 32) {
+    const int lf = lf0 + lane;
+    if (lf < TE * NF) {
+      const int el = lf / NF, f = lf % NF;
+      const int nb = nbr[lf];
+      if (el < ne && nb >= 0) {
+        const int fr = (code[el] >> (8 * f)) & 3;
+        T* d = w + X::SNB + el * TS + f * TR;
+        const T* src = trace + ((size_t)nb * NF + fr) * TR;
+#pragma unroll
+        for (int c = 0; c < CH; ++c) cp_async_n<16>(d + c * VPC, src + c * VPC, 16);
+      }
     }
   }
 }
@@ -457,6 +471,14 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_apply_tc_kernel(ApplyArgs<
   issue_elem<T, DIM, P>(a, W, tile, lane, true);
   cp_commit();
   __syncthreads();
+  // this lane's face-node columns per block: face | node in face << 4 | volume nodes << 10, << 18
+  int fbi[FT];
+#pragma unroll
+  for (int fb = 0; fb < FT; ++fb) {
+    const int k0 = 8 * fb + 2 * t;
+    fbi[fb] = -1;
+    if (NFP % 2 == 0 && k0 < KF) fbi[fb] = (k0 / NFP) | ((k0 % NFP) << 4) | (fmask[k0] << 10) | (fmask[k0 + 1] << 18);
+  }
   for (int it = 0; tile < ntiles; ++it, tile += stride) {
     const int sb = it & 1, slot = it % 3;
     T* st = W + sb * X::ST2;
@@ -603,15 +625,15 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_apply_tc_kernel(ApplyArgs<
       T fu[R][2], sv[DIM][R][2];
       if constexpr (NFP % 2 == 0) {
         // the two columns of a lane lie on one face
-        const int k0 = 8 * fb + 2 * t;
+        const int fi = fbi[fb];
+        const int f = fi & 15, j0 = (fi >> 4) & 63, m0 = (fi >> 10) & 255, m1 = (fi >> 18) & 255;
 #pragma unroll
         for (int ri = 0; ri < R; ++ri) {
           const int el = g + 8 * ri;
           T vfu[2] = {T(0), T(0)}, vs[2] = {T(0), T(0)}, cr[DIM];
 #pragma unroll
           for (int r = 0; r < DIM; ++r) cr[r] = T(0);
-          if (k0 < KF && el < ne) {
-            const int f = k0 / NFP, j0 = k0 % NFP;
+          if (fi >= 0 && el < ne) {
             const int lf = el * NF + f;
             const T* own = str + el * TS + f * TR;
             const auto um = ld2(own + j0);
@@ -636,8 +658,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_apply_tc_kernel(ApplyArgs<
 #pragma unroll
             for (int r = 0; r < DIM; ++r) cr[r] = fgeo<T, DIM, P>(sfg, 1 + r, f, el);
             const T tau = stau[lf];
-            const T fm0 = a.factor ? sf[el * XS + fmask[k0]] : T(1);
-            const T fm1 = a.factor ? sf[el * XS + fmask[k0 + 1]] : T(1);
+            const T fm0 = a.factor ? sf[el * XS + m0] : T(1);
+            const T fm1 = a.factor ? sf[el * XS + m1] : T(1);
             const T h0 = T(0.5) * jump[0], h1 = T(0.5) * jump[1];
             vfu[0] = sJ * (tau * h0 - navg[0]);
             vfu[1] = sJ * (tau * h1 - navg[1]);
@@ -711,7 +733,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_apply_tc_kernel(ApplyArgs<
 #pragma unroll
         for (int nt = 0; nt < NT; ++nt) F::mma(y[nt], zr, ldb(B + X::B3, (r * NT + kb) * NT + nt, lane));
       }
-    // epilogue: pinned row, alpha / beta, store
+    // epilogue: pinned row, alpha / beta, store (pairs of nodes when Np is even)
+    const bool pin_here = a.pin_elem >= e0 && a.pin_elem < e0 + ne;
 #pragma unroll
     for (int nt = 0; nt < NT; ++nt)
 #pragma unroll
@@ -719,15 +742,21 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_apply_tc_kernel(ApplyArgs<
         const int el = g + 8 * ri;
         if (el >= ne) continue;
         const size_t row = (size_t)(e0 + el) * NP;
+        T acc[2];
 #pragma unroll
         for (int ci = 0; ci < 2; ++ci) {
           const int n = 8 * nt + 2 * t + ci;
-          if (n >= NP) continue;
-          T acc = y[nt][ri][ci];
-          if (e0 + el == a.pin_elem && n == a.pin_node) acc = a.pin_scale * a.x[row + n];
-          acc *= a.alpha;
-          if (a.beta != T(0)) acc += a.beta * yold[nt][ri][ci];
-          a.y[row + n] = acc;
+          acc[ci] = y[nt][ri][ci];
+          if (pin_here && e0 + el == a.pin_elem && n == a.pin_node) acc[ci] = a.pin_scale * a.x[row + n];
+          acc[ci] *= a.alpha;
+          if (a.beta != T(0)) acc[ci] += a.beta * yold[nt][ri][ci];
+        }
+        const int n0 = 8 * nt + 2 * t;
+        if (NP % 2 == 0) {
+          if (n0 < NP) *reinterpret_cast<typename F::V2*>(a.y + row + n0) = typename F::V2{acc[0], acc[1]};
+        } else {
+          if (n0 < NP) a.y[row + n0] = acc[0];
+          if (n0 + 1 < NP) a.y[row + n0 + 1] = acc[1];
         }
       }
     __syncwarp();

@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <mutex>
 
 #include <algorithm>
 #include <chrono>
@@ -671,8 +672,13 @@ void sipg_solver::precondition(const double* rin, double* zout) {
 
 // Capture one outer iteration into gx[par]; on any failure the solver keeps
 // launching kernels one by one.
+// One capture at a time in the process (solvers of a serving loop capture from
+// several threads).
+static std::mutex g_capture_mu;
+
 template <typename F>
 void sipg_solver::capture_iteration(int par, F&& body) {
+  std::lock_guard<std::mutex> capture_lock(g_capture_mu);
   const unsigned long long c0 = launch_count();
   cudaGraph_t g = nullptr;
   if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
