@@ -202,6 +202,52 @@ __global__ void k_cheb_block(T* d, T* z, const T* res, const TB* Bc, T c1, T c2,
   }
 }
 
+template <typename TB> struct Pair;
+template <> struct Pair<__nv_bfloat16> {
+  static __device__ __forceinline__ float2 ld(const __nv_bfloat16* p) {
+    return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p));
+  }
+};
+template <> struct Pair<float> {
+  static __device__ __forceinline__ float2 ld(const float* p) { return *reinterpret_cast<const float2*>(p); }
+};
+template <> struct Pair<double> {
+  static __device__ __forceinline__ double2 ld(const double* p) { return *reinterpret_cast<const double2*>(p); }
+};
+template <typename T> struct Vec2;
+template <> struct Vec2<float> { using t = float2; };
+template <> struct Vec2<double> { using t = double2; };
+
+// Same step, two rows per thread with paired loads (even Np).
+template <typename T, typename TB>
+__global__ void k_cheb_block2(T* d, T* z, const T* res, const TB* Bc, T c1, T c2, int nb, int Np) {
+  pdl_enter();
+  using V = typename Vec2<T>::t;
+  const int hp = Np / 2;
+  const size_t total = (size_t)nb * hp;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t b = i / hp;
+    const int r = 2 * (int)(i % hp);
+    const TB* Bb = Bc + b * Np * Np + r;
+    const T* rb = res + b * Np;
+    T s0 = T(0), s1 = T(0);
+    for (int c = 0; c < Np; ++c) {
+      const auto v = Pair<TB>::ld(Bb + (size_t)c * Np);
+      const T rc = rb[c];
+      s0 += (T)v.x * rc;
+      s1 += (T)v.y * rc;
+    }
+    const size_t o = b * Np + r;
+    V dv = *reinterpret_cast<const V*>(d + o), zv = *reinterpret_cast<const V*>(z + o);
+    dv.x = (c1 != T(0) ? c1 * dv.x : T(0)) + c2 * s0;
+    dv.y = (c1 != T(0) ? c1 * dv.y : T(0)) + c2 * s1;
+    zv.x += dv.x;
+    zv.y += dv.y;
+    *reinterpret_cast<V*>(d + o) = dv;
+    *reinterpret_cast<V*>(z + o) = zv;
+  }
+}
+
 // Row-major FP64 blocks -> column-major blocks in T.
 __device__ __forceinline__ void blk_store(__nv_bfloat16* p, double v) { *p = __double2bfloat16(v); }
 __device__ __forceinline__ void blk_store(float* p, double v) { *p = (float)v; }
@@ -311,14 +357,21 @@ __global__ void k_coarse_update_p(T* p, const T* sv, size_t n, double* scal) {
 __global__ void k_shift_scalar(double* scal, int from, int to) {
   pdl_enter(); scal[to] = scal[from]; }
 
+// Eight lanes per row (the algebraic levels are small: parallelism, not bytes, limits them).
 template <typename T>
 __global__ void k_csr_spmv(int rows, const int* __restrict__ ptr, const int* __restrict__ idx,
                            const T* __restrict__ val, const T* __restrict__ x, T* y, T alpha, T beta) {
   pdl_enter();
-  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31, sub = lane & 7;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; 4 * w < rows; w += warps) {
+    const int r = 4 * w + (lane >> 3);
     T s = T(0);
-    for (int k = ptr[r]; k < ptr[r + 1]; ++k) s += val[k] * x[idx[k]];
-    y[r] = beta != T(0) ? alpha * s + beta * y[r] : alpha * s;
+    if (r < rows)
+      for (int k = ptr[r] + sub; k < ptr[r + 1]; k += 8) s += val[k] * x[idx[k]];
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, 8);
+    if (r < rows && sub == 0) y[r] = beta != T(0) ? alpha * s + beta * y[r] : alpha * s;
   }
 }
 
@@ -412,7 +465,11 @@ void to_f64(double* dst, const float* src, size_t n, cudaStream_t s) {
 }
 template <typename T, typename TB>
 void cheb_step_block(T* d, T* z, const T* res, const TB* Bc, T c1, T c2, int nb, int Np, cudaStream_t s) {
-  pdl_launch(k_cheb_block<T, TB>, dim3(grid_for((size_t)nb * Np)), dim3(256), 0, s, d, z, res, Bc, c1, c2, nb, Np);
+  if (Np % 2 == 0)
+    pdl_launch(k_cheb_block2<T, TB>, dim3(grid_for((size_t)nb * Np / 2)), dim3(256), 0, s, d, z, res, Bc, c1, c2,
+               nb, Np);
+  else
+    pdl_launch(k_cheb_block<T, TB>, dim3(grid_for((size_t)nb * Np)), dim3(256), 0, s, d, z, res, Bc, c1, c2, nb, Np);
   note_launch();
 }
 template void cheb_step_block<float, __nv_bfloat16>(float*, float*, const float*, const __nv_bfloat16*, float, float,
@@ -471,7 +528,8 @@ void coarse_update_p(T* p, const T* sv, size_t n, double* scal, cudaStream_t s) 
 template <typename T>
 void csr_spmv(int rows, const int* ptr, const int* idx, const T* val, const T* x, T* y, T alpha, T beta,
               cudaStream_t s) {
-  pdl_launch(k_csr_spmv<T>, dim3(grid_for((size_t)rows)), dim3(256), 0, s, rows, ptr, idx, val, x, y, alpha, beta);
+  const int blocks = std::max(1, std::min((rows + 31) / 32, 148 * 16));
+  pdl_launch(k_csr_spmv<T>, dim3(blocks), dim3(256), 0, s, rows, ptr, idx, val, x, y, alpha, beta);
   note_launch();
 }
 template <typename T>
