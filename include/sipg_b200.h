@@ -184,6 +184,12 @@ typedef struct {
                                 matrix-free apply, scalar operators, orders <= 2); 0: all matrix-free */
   int smoother;              /* p-multigrid smoothing: 0 Chebyshev on the point-Jacobi (diagonal)
                                 preconditioned operator, 1 on the element-block-Jacobi one */
+  /* per p-multigrid level (the [p-multigrid] keys cheb_orders, pre_it, post_it of
+   * examples/3d/oscillating_droplet/config.ini:24-31): Chebyshev degree (0: cheb_order)
+   * and Chebyshev sweeps before and after the coarse-level correction */
+  int cheb_orders[4];
+  int pre_it[4];
+  int post_it[4];
 } sipg_solver_opts;
 
 int sipg_solver_default_opts(int kind, sipg_solver_opts *o);

@@ -58,6 +58,7 @@ struct Level {
   DevBuf cp, cs, cAp;            // coarse CG
   DevBuf bc64, bc32;             // inverse diagonal blocks, column-major (block-Jacobi smoothing; bc32 in bf16)
   std::unique_ptr<BsrOp> bsr;    // assembled element blocks (low orders), else matrix-free
+  int cheb = 4, pre = 1, post = 1;  // Chebyshev degree, smoothing sweeps before / after the coarse correction
   template <typename T>
   void apply(const T* x, T* y, cudaStream_t s, T alpha = T(1), T beta = T(0)) const {
     if (bsr) bsr_apply<T>(*bsr, x, y, alpha, beta, s);
@@ -232,6 +233,7 @@ struct sipg_solver {
   void setup_pmg();
   template <typename T> void vcycle(int l);
   template <typename T> void chebyshev(Level& L, bool want_res);
+  template <typename T> void smooth(Level& L, int sweeps, bool want_res);
   template <typename T> void coarse(Level& L);
   template <typename T> void amg_vcycle(int l);
   template <typename T> void last_level_amg(Level& L);
@@ -359,6 +361,9 @@ void sipg_solver::setup_pmg() {
   }
   for (int l = 0; l < nl; ++l) {
     Level& L = lv[l];
+    L.cheb = o.cheb_orders[l] > 0 ? o.cheb_orders[l] : o.cheb_order;
+    L.pre = std::max(0, o.pre_it[l]);
+    L.post = std::max(0, o.post_it[l]);
     op_diag(L.op, L.dinv64.as<double>(), stream);
     k_recip<<<grid_for(L.n), 256, 0, stream>>>(L.dinv64.as<double>(), L.n);
       note_launch();
@@ -510,7 +515,7 @@ void sipg_solver::chebyshev(Level& L, bool want_res) {
   T* d = L.d.as<T>();
   T* z = L.z.as<T>();
   T* res = L.res.as<T>();
-  for (int it = 0; it < o.cheb_order; ++it) {
+  for (int it = 0; it < L.cheb; ++it) {
     double c1 = 0.0, c2 = 1.0 / theta;
     if (it > 0) {
       double rho = 1.0 / (2.0 * sigma - rho_old);
@@ -526,8 +531,15 @@ void sipg_solver::chebyshev(Level& L, bool want_res) {
     } else {
       cheb_step<T>(d, z, res, dinv, (T)c1, (T)c2, L.n, stream);
     }
-    if (it < o.cheb_order - 1 || want_res) L.apply<T>(d, res, stream, T(-1), T(1));
+    if (it < L.cheb - 1 || want_res) L.apply<T>(d, res, stream, T(-1), T(1));
   }
+}
+
+// `sweeps` Chebyshev sweeps on z with residual res; the residual is kept current
+// except, when !want_res, after the last sweep.
+template <typename T>
+void sipg_solver::smooth(Level& L, int sweeps, bool want_res) {
+  for (int k = 0; k < sweeps; ++k) chebyshev<T>(L, k < sweeps - 1 || want_res);
 }
 
 template <typename T>
@@ -603,13 +615,15 @@ template <typename T>
 void sipg_solver::last_level_amg(Level& L) {
   vzero<T>(L.z.as<T>(), L.n, stream);
   vcopy<T>(L.res.as<T>(), L.rhs.as<T>(), L.n, stream);
-  chebyshev<T>(L, true);
+  smooth<T>(L, L.pre, true);
   Rdg.mv<T>(L.res.as<T>(), al[0].rhs.as<T>(), T(1), T(0), stream);
   amg_vcycle<T>(0);
   Pdg.mv<T>(al[0].z.as<T>(), L.z.as<T>(), T(1), T(1), stream);
-  vcopy<T>(L.res.as<T>(), L.rhs.as<T>(), L.n, stream);
-  L.apply<T>(L.z.as<T>(), L.res.as<T>(), stream, T(-1), T(1));
-  chebyshev<T>(L, false);
+  if (L.post > 0) {
+    vcopy<T>(L.res.as<T>(), L.rhs.as<T>(), L.n, stream);
+    L.apply<T>(L.z.as<T>(), L.res.as<T>(), stream, T(-1), T(1));
+    smooth<T>(L, L.post, false);
+  }
 }
 
 template <typename T>
@@ -627,13 +641,15 @@ void sipg_solver::vcycle(int l) {
   const int K = op->mesh->K, nc = op->ncomp;
   vzero<T>(L.z.as<T>(), L.n, stream);
   vcopy<T>(L.res.as<T>(), L.rhs.as<T>(), L.n, stream);
-  chebyshev<T>(L, true);
+  smooth<T>(L, L.pre, true);
   restrict_elem<T>(Cl.rhs.as<T>(), L.res.as<T>(), P, K, L.Np, Cl.Np, nc, stream);
   vcycle<T>(l + 1);
   prolong_add<T>(L.z.as<T>(), Cl.z.as<T>(), P, K, L.Np, Cl.Np, nc, stream);
-  vcopy<T>(L.res.as<T>(), L.rhs.as<T>(), L.n, stream);
-  L.apply<T>(L.z.as<T>(), L.res.as<T>(), stream, T(-1), T(1));
-  chebyshev<T>(L, false);
+  if (L.post > 0) {
+    vcopy<T>(L.res.as<T>(), L.rhs.as<T>(), L.n, stream);
+    L.apply<T>(L.z.as<T>(), L.res.as<T>(), stream, T(-1), T(1));
+    smooth<T>(L, L.post, false);
+  }
 }
 
 void sipg_solver::precondition(const double* rin, double* zout) {
@@ -871,6 +887,11 @@ int sipg_solver_default_opts(int kind, sipg_solver_opts* o) {
     o->graphs = 1;
     o->assembled_max_order = 1;
     o->smoother = 1;
+    for (int l = 0; l < 4; ++l) {
+      o->cheb_orders[l] = 0;
+      o->pre_it[l] = 1;
+      o->post_it[l] = 1;
+    }
     (void)kind;
   });
 }

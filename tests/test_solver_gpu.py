@@ -221,3 +221,22 @@ def test_block_jacobi_smoothing_converges_faster_to_the_same_solution(precision)
     assert i1.iters < i0.iters
     assert i1.true_rel_res < 1e-9
     assert rel_err(x1, x0) < 1e-6
+
+
+def test_per_level_chebyshev_degrees_and_sweeps():
+    """The [p-multigrid] per-level keys: cheb_orders, pre_it, post_it."""
+    c = W.poisson3d_two_phase(5, order=3, n_modes=64, pin=False)
+    base = None
+    for ch, pre, post in (((4, 4, 4), (1, 1, 1), (1, 1, 1)), ((3, 2, 4), (2, 1, 1), (1, 0, 1)),
+                          ((4, 2, 2), (1, 1, 2), (0, 1, 2))):
+        op = make_op(c["mesh"], 3, 1, c["factor"], bct=c["bc_types"])
+        o = sipg.default_opts(sipg.SOLVER_PMULTIGRID)
+        o.rel_tol, o.abs_tol, o.max_iter, o.nullspace = 1e-9, 0.0, 300, 1
+        for i in range(3):
+            o.cheb_orders[i], o.pre_it[i], o.post_it[i] = ch[i], pre[i], post[i]
+        x, info = sipg.Solver(op, sipg.SOLVER_PMULTIGRID, o).solve_host(c["rhs"])
+        assert info.status == sipg.SIPG_OK and info.true_rel_res < 1e-9
+        if base is None:
+            base = x
+        else:
+            assert rel_err(x, base) < 1e-6
