@@ -471,6 +471,10 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_apply_tc_kernel(ApplyArgs<
   issue_elem<T, DIM, P>(a, W, tile, lane, true);
   cp_commit();
   __syncthreads();
+  cp_wait_all();
+  __syncwarp();
+  issue_traces<T, DIM, P>(a, trace, W, I, tile, lane);
+  cp_commit();
   // this lane's face-node columns per block: face | node in face << 4 | volume nodes << 10, << 18
   int fbi[FT];
 #pragma unroll
@@ -483,11 +487,10 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_apply_tc_kernel(ApplyArgs<
     const int sb = it & 1, slot = it % 3;
     T* st = W + sb * X::ST2;
     const int* ints = I + slot * X::SI;
-    // element data of this tile and connectivity of the next one have arrived
-    cp_wait_all();
+    // element data of this tile and connectivity of the next one have arrived (the
+    // tile's trace records, issued after the previous tile's fluxes, may still be in flight)
+    cp_wait_but_one();
     __syncwarp();
-    issue_traces<T, DIM, P>(a, trace, W, ints, tile, lane);
-    cp_commit();
     issue_ints<T, DIM, P>(a, I + ((it + 2) % 3) * X::SI, tile + 2 * stride, lane);
     issue_elem<T, DIM, P>(a, W + (sb ^ 1) * X::ST2, tile + stride, lane, true);
     cp_commit();
@@ -719,6 +722,11 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_apply_tc_kernel(ApplyArgs<
         for (int r = 0; r < DIM; ++r) F::mma(z[r][nt], sv[r], b);
       }
     }
+    // the trace buffer is free: the next tile's records land during the rest of this
+    // tile and the next tile's volume products
+    __syncwarp();
+    issue_traces<T, DIM, P>(a, trace, W, I + ((it + 1) % 3) * X::SI, tile + stride, lane);
+    cp_commit();
     // y += sum_r Z_r . D_r
 #pragma unroll
     for (int r = 0; r < DIM; ++r)
