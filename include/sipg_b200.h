@@ -177,8 +177,12 @@ typedef struct {
                                 continuous piecewise-linear space (coarse_solver = petsc/amg) */
   int amg_coarse_max;        /* unknowns of the densely inverted coarsest level */
   double amg_strength;       /* aggregation strength threshold */
-  int graphs;                /* 1: each outer iteration after the first is replayed from a captured
-                                CUDA graph; 0: kernels are launched one by one (same arithmetic) */
+  int graphs;                /* 2: the outer iterations after the first run inside one CUDA graph
+                                whose conditional while-node repeats an iteration until the
+                                stopping test on the device ends it (host reads once per 64
+                                iterations; falls back to 1 where unsupported); 1: each outer
+                                iteration after the first is replayed from a captured CUDA graph;
+                                0: kernels are launched one by one (same arithmetic as 1) */
   int assembled_max_order;   /* p-multigrid levels below the finest with this order or lower apply
                                 their operator as stored element blocks (assembled once from the
                                 matrix-free apply, scalar operators, orders <= 2); 0: all matrix-free */

@@ -167,6 +167,30 @@ double host_csr_lmax(const Csr& A, const std::vector<double>& dinv, int iters) {
 
 }  // namespace
 
+// Device-resident outer loop: beta numerator of the flexible CG from two dots
+// (r.z_new - r.z_old) and the per-iteration stopping test, which ends the
+// conditional while-node of the loop graph.
+__global__ void k_beta_flex(double* scal) {
+  scal[S_BETA] = scal[S_RZN] - scal[S_RZO];
+  scal[S_RZP] = scal[S_RZ];
+  scal[S_RZ] = scal[S_RZN];
+}
+
+__global__ void k_loop_check(double* scal, cudaGraphConditionalHandle h, int max_iter) {
+  const double it = scal[S_ITER] + 1.0;
+  scal[S_ITER] = it;
+  const double pap = scal[S_PAP], rr = scal[S_RR];
+  double st = 0.0;
+  if (!(pap > 0.0) || !isfinite(rr)) st = 2.0;
+  else if (sqrt(rr) <= scal[S_TOL]) st = 1.0;
+  else if (it >= (double)max_iter) st = 3.0;
+  else if ((scal[S_CHUNK] -= 1.0) <= 0.0) st = 4.0;
+  if (st != 0.0) {
+    scal[S_STATUS] = st;
+    cudaGraphSetConditional(h, 0);
+  }
+}
+
 struct sipg_solver {
   sipg_op* op = nullptr;
   int kind = 0;
@@ -194,6 +218,11 @@ struct sipg_solver {
   unsigned gver = 0;
   bool graph_broken = false;
   const std::atomic<int>* cancel = nullptr;  // set by a serving loop: non-zero ends the solve
+  // device-resident loop (conditional while-node around one iteration on fixed buffers)
+  cudaGraphExec_t gloop = nullptr;
+  unsigned long long gloop_nodes = 0;
+  bool gloop_broken = false;
+  PinnedScalars hw;  // host staging of scalars written before a loop launch
 
   double* S() const { return scal.as<double>(); }
   void drop_graphs() {
@@ -202,7 +231,13 @@ struct sipg_solver {
         cudaGraphExecDestroy(g);
         g = nullptr;
       }
+    if (gloop) {
+      cudaGraphExecDestroy(gloop);
+      gloop = nullptr;
+    }
   }
+  template <typename F>
+  void capture_loop(F&& body);
   ~sipg_solver() {
     drop_graphs();
     if (ev0) cudaEventDestroy(ev0);
@@ -467,6 +502,7 @@ void sipg_solver::setup_amg() {
 void sipg_solver::setup() {
   drop_graphs();
   graph_broken = false;
+  gloop_broken = false;
   n = (size_t)op->ncomp * op->mesh->K * op->Np;
   if (!r.p) {
     size_t b = n * sizeof(double);
@@ -728,6 +764,53 @@ void sipg_solver::capture_iteration(int par, F&& body) {
   gnodes[par] = c1 - c0;
 }
 
+// Build gloop: a conditional while-node whose body is one iteration followed by
+// the stopping test. On any failure the solver falls back to per-iteration graphs.
+template <typename F>
+void sipg_solver::capture_loop(F&& body) {
+  std::lock_guard<std::mutex> capture_lock(g_capture_mu);
+  const unsigned long long c0 = launch_count();
+  cudaGraph_t g = nullptr;
+  bool ok = cudaGraphCreate(&g, 0) == cudaSuccess;
+  cudaGraphConditionalHandle h{};
+  cudaGraphNodeParams cp{};
+  cudaGraphNode_t node = nullptr;
+  if (ok) ok = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+  if (ok) {
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    ok = cudaGraphAddNode(&node, g, nullptr, 0, &cp) == cudaSuccess;
+  }
+  if (ok) ok = cudaStreamBeginCaptureToGraph(stream, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                             cudaStreamCaptureModeRelaxed) == cudaSuccess;
+  if (ok) {
+    bool body_ok = true;
+    try {
+      body();
+      k_loop_check<<<1, 1, 0, stream>>>(S(), h, o.max_iter);
+      note_launch();
+    } catch (...) {
+      body_ok = false;
+    }
+    cudaGraph_t out = nullptr;
+    ok = cudaStreamEndCapture(stream, &out) == cudaSuccess && body_ok;
+  }
+  const unsigned long long c1 = launch_count();
+  unnote_launch(c1 - c0);
+  if (ok) ok = cudaGraphInstantiate(&gloop, g, 0) == cudaSuccess;
+  if (g) cudaGraphDestroy(g);
+  if (!ok) {
+    if (gloop) cudaGraphExecDestroy(gloop);
+    gloop = nullptr;
+    cudaGetLastError();
+    gloop_broken = true;
+    return;
+  }
+  gloop_nodes = c1 - c0;
+}
+
 int sipg_solver::solve(const double* b, double* x_user, sipg_solve_info* info) {
   auto t0 = std::chrono::steady_clock::now();
   if (dirty) setup();
@@ -793,41 +876,93 @@ int sipg_solver::solve(const double* b, double* x_user, sipg_solve_info* info) {
     // flexible PCG (viscous_solver.cpp:177-301)
     if (status == SIPG_OK) precondition(R, Z);
     vcopy<double>(Pv, Z, n, stream);
-    // one iteration; zn receives the new preconditioned residual, zo holds the previous one
-    auto iteration = [&](double* zn, double* zo) {
-      op->apply<double>(Pv, AP, stream);
-      const double* a[2] = {R, Pv};
-      const double* bb[2] = {zo, AP};
-      multi_dot<double>(a, bb, 2, n, S() + S_RZ, 1, rw, stream);  // cg3_alpha_pre
-      cg_update_xr(x, R, Pv, AP, n, S(), S_RZ, S_PAP, S() + S_RR, rw, stream);  // update_ans + update_res
-      if (o.nullspace) {
-        vsum<double>(R, n, S() + S_SUM, rw, stream);
-        sub_mean<double>(R, n, S(), S_SUM, stream);
-        dot(R, R, S_RR);
+    if (graphs && o.graphs >= 2 && !gloop_broken) {
+      // Device-resident loop: one iteration on fixed buffers (z overwritten in place,
+      // beta = r.z_new - r.z_old from two dots), replayed by a conditional while-node
+      // until the stopping test in k_loop_check ends it; the host reads the scalars
+      // once per launch of at most kLoopChunk iterations.
+      constexpr int kLoopChunk = 64;
+      dot(R, Z, S_RZ);
+      auto body = [&] {
+        op->apply<double>(Pv, AP, stream);
+        dot(Pv, AP, S_PAP);                                              // cg3_alpha_pre
+        cg_update_xr(x, R, Pv, AP, n, S(), S_RZ, S_PAP, S() + S_RR, rw, stream);  // update_ans + update_res
+        if (o.nullspace) {
+          vsum<double>(R, n, S() + S_SUM, rw, stream);
+          sub_mean<double>(R, n, S(), S_SUM, stream);
+          dot(R, R, S_RR);
+        }
+        dot(R, Z, S_RZO);
+        precondition(R, Z);
+        dot(R, Z, S_RZN);
+        k_beta_flex<<<1, 1, 0, stream>>>(S());  // cg3_compute_beta_pre_flex
+        note_launch();
+        update_p<double>(Pv, Z, n, S(), S_BETA, S_RZP, stream);
+      };
+      auto after = [&](int it_now) {
+        iter = it_now;
+        const double pap = hs.h[S_PAP];
+        res = std::sqrt(hs.h[S_RR]);
+        if (!(pap > 0.0) || !std::isfinite(res)) status = SIPG_BREAKDOWN;
+        else if (cancel && cancel->load(std::memory_order_relaxed)) status = SIPG_CANCELLED;
+      };
+      while (status == SIPG_OK && res > tol && iter < o.max_iter) {
+        // the first iteration runs eagerly (lazy buffers are allocated there)
+        if (iter >= 1 && !gloop && !gloop_broken) capture_loop(body);
+        if (iter == 0 || !gloop) {
+          body();
+          read_scalars();
+          after(iter + 1);
+          continue;
+        }
+        hw.h[S_ITER] = (double)iter;
+        hw.h[S_STATUS] = 0.0;
+        hw.h[S_TOL] = tol;
+        hw.h[S_CHUNK] = (double)kLoopChunk;
+        SIPG_CUDA(cudaMemcpyAsync(S() + S_ITER, hw.h + S_ITER, 4 * sizeof(double), cudaMemcpyHostToDevice, stream));
+        SIPG_CUDA(cudaGraphLaunch(gloop, stream));
+        read_scalars();
+        const int done = (int)hs.h[S_ITER];
+        note_launch((unsigned)((done - iter) * gloop_nodes));
+        after(done);
       }
-      precondition(R, zn);
-      dot_diff(R, zn, zo, n, S() + S_BETA, rw, stream);  // cg3_compute_beta_pre_flex
-      update_p<double>(Pv, zn, n, S(), S_BETA, S_RZ, stream);
-    };
-    while (status == SIPG_OK && res > tol && iter < o.max_iter) {
-      double* zn = ZO;
-      double* zo = Z;
-      const int par = iter & 1;  // Z = z, ZO = z_old at iteration 0
-      // the first iteration runs eagerly (lazy buffers are allocated there), the rest replay
-      if (graphs && iter >= 1 && !graph_broken && !gx[par]) capture_iteration(par, [&] { iteration(zn, zo); });
-      if (graphs && iter >= 1 && gx[par]) {
-        SIPG_CUDA(cudaGraphLaunch(gx[par], stream));
-        note_launch((unsigned)gnodes[par]);
-      } else {
-        iteration(zn, zo);
+    } else {
+      // one iteration; zn receives the new preconditioned residual, zo holds the previous one
+      auto iteration = [&](double* zn, double* zo) {
+        op->apply<double>(Pv, AP, stream);
+        const double* a[2] = {R, Pv};
+        const double* bb[2] = {zo, AP};
+        multi_dot<double>(a, bb, 2, n, S() + S_RZ, 1, rw, stream);  // cg3_alpha_pre
+        cg_update_xr(x, R, Pv, AP, n, S(), S_RZ, S_PAP, S() + S_RR, rw, stream);  // update_ans + update_res
+        if (o.nullspace) {
+          vsum<double>(R, n, S() + S_SUM, rw, stream);
+          sub_mean<double>(R, n, S(), S_SUM, stream);
+          dot(R, R, S_RR);
+        }
+        precondition(R, zn);
+        dot_diff(R, zn, zo, n, S() + S_BETA, rw, stream);  // cg3_compute_beta_pre_flex
+        update_p<double>(Pv, zn, n, S(), S_BETA, S_RZ, stream);
+      };
+      while (status == SIPG_OK && res > tol && iter < o.max_iter) {
+        double* zn = ZO;
+        double* zo = Z;
+        const int par = iter & 1;  // Z = z, ZO = z_old at iteration 0
+        // the first iteration runs eagerly (lazy buffers are allocated there), the rest replay
+        if (graphs && iter >= 1 && !graph_broken && !gx[par]) capture_iteration(par, [&] { iteration(zn, zo); });
+        if (graphs && iter >= 1 && gx[par]) {
+          SIPG_CUDA(cudaGraphLaunch(gx[par], stream));
+          note_launch((unsigned)gnodes[par]);
+        } else {
+          iteration(zn, zo);
+        }
+        std::swap(Z, ZO);
+        ++iter;
+        read_scalars();
+        const double pap = hs.h[S_PAP];
+        res = std::sqrt(hs.h[S_RR]);
+        if (!(pap > 0.0) || !std::isfinite(res)) { status = SIPG_BREAKDOWN; break; }
+        if (cancel && cancel->load(std::memory_order_relaxed)) { status = SIPG_CANCELLED; break; }
       }
-      std::swap(Z, ZO);
-      ++iter;
-      read_scalars();
-      const double pap = hs.h[S_PAP];
-      res = std::sqrt(hs.h[S_RR]);
-      if (!(pap > 0.0) || !std::isfinite(res)) { status = SIPG_BREAKDOWN; break; }
-      if (cancel && cancel->load(std::memory_order_relaxed)) { status = SIPG_CANCELLED; break; }
     }
   }
   if (status == SIPG_OK && res > tol) status = SIPG_NOT_CONVERGED;
@@ -884,7 +1019,7 @@ int sipg_solver_default_opts(int kind, sipg_solver_opts* o) {
     o->coarse_kind = 1;
     o->amg_coarse_max = 1000;
     o->amg_strength = 0.08;
-    o->graphs = 1;
+    o->graphs = 2;
     o->assembled_max_order = 1;
     o->smoother = 1;
     for (int l = 0; l < 4; ++l) {

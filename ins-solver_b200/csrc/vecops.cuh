@@ -29,7 +29,14 @@ enum Scal : int {
   S_C_RZN = 8, // coarse CG: new r . s
   S_C_FLAG = 9,
   S_TMP = 10,
-  S_COUNT = 16
+  S_RZO = 11,    // r_(k+1) . z_k   (device-resident loop: beta without swapping z buffers)
+  S_RZN = 12,    // r_(k+1) . z_(k+1)
+  S_ITER = 13,   // iterations done
+  S_STATUS = 14, // 0 running, 1 converged, 2 breakdown, 3 iteration limit, 4 chunk done
+  S_TOL = 15,    // absolute tolerance on ||r||
+  S_CHUNK = 16,  // iterations left in this launch
+  S_RZP = 17,    // r_k . z_k of the previous iteration (beta denominator)
+  S_COUNT = 24
 };
 
 struct RedWork {

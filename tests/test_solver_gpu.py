@@ -185,6 +185,56 @@ def test_graph_replayed_iterations_match_eager_launches(precision):
 
 
 @pytest.mark.parametrize("precision", [sipg.FP64, sipg.FP32], ids=["fp64", "mixed"])
+def test_device_resident_loop_matches_host_loop(precision):
+    """The outer loop run on the device (conditional while-node, stopping test on
+    the device) converges like the host-driven loop: same iteration count within
+    one, the same solution to the solve tolerance, reproducible run to run, and a
+    coefficient change after the capture is picked up."""
+    c = W.poisson3d_two_phase(5, order=3, n_modes=64, pin=False)
+    out = {}
+    for graphs in (1, 2):
+        op = make_op(c["mesh"], 3, 1, c["factor"], bct=c["bc_types"])
+        o = sipg.default_opts(sipg.SOLVER_PMULTIGRID)
+        o.rel_tol, o.abs_tol, o.max_iter, o.precision, o.nullspace = 1e-10, 0.0, 200, precision, 1
+        o.graphs = graphs
+        s = sipg.Solver(op, sipg.SOLVER_PMULTIGRID, o)
+        x1, i1 = s.solve_host(c["rhs"])
+        x2, i2 = s.solve_host(c["rhs"])
+        op.set_factor(2.0 * c["factor"])
+        s.setup()
+        x3, i3 = s.solve_host(c["rhs"])
+        out[graphs] = (x1, i1, x3, i3)
+        assert i1.status == i2.status == i3.status == sipg.SIPG_OK
+        assert np.array_equal(x1, x2) and i1.iters == i2.iters
+        assert rel_err(x3, 0.5 * x1) < 1e-8
+        assert i1.true_rel_res < 1e-9
+    h, d = out[1], out[2]
+    assert abs(h[1].iters - d[1].iters) <= 1 and abs(h[3].iters - d[3].iters) <= 1
+    assert rel_err(d[0], h[0]) < 1e-8 and rel_err(d[2], h[2]) < 1e-8
+
+
+def test_device_resident_loop_chunks_and_iteration_limit():
+    """A solve longer than one device launch (64 iterations) continues across
+    launches with the host loop's iteration count, and the iteration limit stops
+    the device loop exactly."""
+    c = W.poisson3d_two_phase(5, order=3, n_modes=64, pin=False)
+    op = make_op(c["mesh"], 3, 1, c["factor"], bct=c["bc_types"])
+    res = {}
+    for graphs in (1, 2):
+        o = sipg.default_opts(sipg.SOLVER_JACOBI)
+        o.rel_tol, o.abs_tol, o.max_iter, o.nullspace = 1e-9, 0.0, 2000, 1
+        o.graphs = graphs
+        x, info = sipg.Solver(op, sipg.SOLVER_JACOBI, o).solve_host(c["rhs"])
+        assert info.status == sipg.SIPG_OK and info.iters > 130
+        res[graphs] = (x, info)
+        o.max_iter = 77
+        _, lim = sipg.Solver(op, sipg.SOLVER_JACOBI, o).solve_host(c["rhs"])
+        assert lim.status == sipg.SIPG_NOT_CONVERGED and lim.iters == 77
+    assert abs(res[1][1].iters - res[2][1].iters) <= 2
+    assert rel_err(res[2][0], res[1][0]) < 1e-6
+
+
+@pytest.mark.parametrize("precision", [sipg.FP64, sipg.FP32], ids=["fp64", "mixed"])
 def test_assembled_low_order_levels_match_matrix_free(precision):
     """The p=1 (and p=2) levels applied from stored element blocks, assembled by
     probing the matrix-free apply, give the matrix-free solver's iterates."""
