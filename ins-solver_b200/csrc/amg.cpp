@@ -262,6 +262,11 @@ std::vector<double> dense_inverse(std::vector<double> a, int n) {
 
 }  // namespace
 
+// A level must keep at most this fraction of its rows; the densely inverted
+// coarsest level holds at most kMaxDenseCoarse rows.
+constexpr double kMinCoarsening = 0.6;
+constexpr int kMaxDenseCoarse = 8192;
+
 AmgHierarchy build_amg(const Csr& A0, const Csr& Pdg, int coarse_max, double strength, bool singular) {
   AmgHierarchy H;
   H.Pdg = Pdg;
@@ -269,9 +274,16 @@ AmgHierarchy build_amg(const Csr& A0, const Csr& Pdg, int coarse_max, double str
   H.levels.push_back({A0, {}, {}});
   while (H.levels.back().A.rows > coarse_max && H.levels.size() < 16) {
     const Csr& A = H.levels.back().A;
+    // A threshold that leaves most connections weak coarsens little and makes the
+    // Galerkin products dense; such a level is aggregated again with a lower threshold.
     int na = 0;
-    std::vector<int> agg = aggregate(A, strength, &na);
-    if (na >= A.rows || na < 1) break;
+    double theta = strength;
+    std::vector<int> agg = aggregate(A, theta, &na);
+    for (int retry = 0; retry < 3 && na > kMinCoarsening * A.rows; ++retry) {
+      theta *= 0.25;
+      agg = aggregate(A, theta, &na);
+    }
+    if (na > kMinCoarsening * A.rows || na < 1) break;
     // tentative prolongator: piecewise constant on aggregates
     Csr T;
     T.rows = A.rows;
@@ -313,6 +325,8 @@ AmgHierarchy build_amg(const Csr& A0, const Csr& Pdg, int coarse_max, double str
   }
   const Csr& C = H.levels.back().A;
   const int n = C.rows;
+  if (n > kMaxDenseCoarse)
+    throw std::runtime_error("algebraic coarsening stalled: coarsest level too large for a dense inverse");
   std::vector<double> dense((size_t)n * n, 0.0);
   double dmax = 0.0;
   for (int i = 0; i < n; ++i)

@@ -64,3 +64,20 @@ def test_aggregation_levels_are_galerkin_products():
     inv = amg.coarse_inverse()
     Ac = csr_dense(amg.csr(amg.nlevels - 1, 0))
     assert np.abs(inv @ Ac - np.eye(Ac.shape[0])).max() < 1e-8
+
+
+def test_weak_threshold_still_coarsens():
+    """A strength threshold that leaves most connections weak (0.25 on a P1
+    Laplacian) is lowered level by level, so every level keeps at most 60 % of
+    the rows above it and the set-up stays fast."""
+    import time
+    mesh, t, e, om, x, f, m, bct = random_case(3, 10, 1, 1, seed=5)
+    tau = np.zeros((mesh.K, 4))
+    O.oracle_lib().oracle_tau(C.byref(om.s), O._d(np.ascontiguousarray(f)), O._d(tau))
+    t0 = time.perf_counter()
+    amg = sipg.Amg.p1(mesh, f, tau, np.zeros(mesh.Kb, np.int32), coarse_max=50, strength=0.25, singular=True)
+    assert time.perf_counter() - t0 < 20.0
+    rows = [amg.csr(l, 0)[0] for l in range(amg.nlevels)]
+    assert len(rows) >= 2 and rows[-1] == amg.coarse_n
+    for a, b in zip(rows, rows[1:]):
+        assert b <= 0.6 * a
