@@ -87,6 +87,7 @@ ApplyArgs<T> args_of(const sipg_op* op, const T* x, T* y) {
   a.eb = f64 ? op->eb64 : op->eb32;
   a.alpha = T(1);
   a.beta = T(0);
+  a.c = y;
   return a;
 }
 

@@ -46,7 +46,7 @@ __global__ void k_d2f(float* dst, const double* src, size_t n) {
 // there are Np threads per element row to hide the gather latency.
 template <typename T, int NP, int NF>
 __global__ void __launch_bounds__(256) k_bsr(int K, const T* __restrict__ v, const int* __restrict__ nbr,
-                                             const T* __restrict__ x, T* __restrict__ y, T alpha, T beta) {
+                                             const T* __restrict__ x, T* y, T alpha, T beta, const T* c) {
   pdl_enter();
   const size_t K_ = (size_t)K;
   const size_t total = K_ * NP;
@@ -68,7 +68,7 @@ __global__ void __launch_bounds__(256) k_bsr(int K, const T* __restrict__ v, con
       for (int c = 0; c < NP; ++c) acc += vs[(size_t)c * K_] * xk[c];
     }
     T o = alpha * acc;
-    if (beta != T(0)) o += beta * y[(size_t)e * NP + r];
+    if (beta != T(0)) o += beta * c[(size_t)e * NP + r];
     y[(size_t)e * NP + r] = o;
   }
 }
@@ -149,20 +149,21 @@ void bsr_assemble(sipg_op* op, BsrOp& B, bool want32, cudaStream_t s) {
 }
 
 template <typename T>
-void bsr_apply(const BsrOp& B, const T* x, T* y, T alpha, T beta, cudaStream_t s) {
+void bsr_apply(const BsrOp& B, const T* x, T* y, T alpha, T beta, cudaStream_t s, const T* c) {
+  if (!c) c = y;
   const T* v = std::is_same<T, double>::value ? (const T*)B.v64.p : (const T*)B.v32.p;
   if (!v) throw Error(SIPG_INVALID_ARG, "assembled blocks missing for this precision");
   const int g = (int)std::max<size_t>(1, std::min<size_t>(((size_t)B.K * B.Np + 255) / 256, 148 * 32));
-  if (B.dim == 3 && B.Np == 4) pdl_launch(k_bsr<T, 4, 4>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta);
-  else if (B.dim == 3 && B.Np == 10) pdl_launch(k_bsr<T, 10, 4>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta);
-  else if (B.dim == 2 && B.Np == 3) pdl_launch(k_bsr<T, 3, 3>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta);
-  else if (B.dim == 2 && B.Np == 6) pdl_launch(k_bsr<T, 6, 3>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta);
+  if (B.dim == 3 && B.Np == 4) pdl_launch(k_bsr<T, 4, 4>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta, c);
+  else if (B.dim == 3 && B.Np == 10) pdl_launch(k_bsr<T, 10, 4>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta, c);
+  else if (B.dim == 2 && B.Np == 3) pdl_launch(k_bsr<T, 3, 3>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta, c);
+  else if (B.dim == 2 && B.Np == 6) pdl_launch(k_bsr<T, 6, 3>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta, c);
   else throw Error(SIPG_INVALID_ARG, "no assembled apply for this element");
   note_launch();
   SIPG_CUDA(cudaGetLastError());
 }
 
-template void bsr_apply<double>(const BsrOp&, const double*, double*, double, double, cudaStream_t);
-template void bsr_apply<float>(const BsrOp&, const float*, float*, float, float, cudaStream_t);
+template void bsr_apply<double>(const BsrOp&, const double*, double*, double, double, cudaStream_t, const double*);
+template void bsr_apply<float>(const BsrOp&, const float*, float*, float, float, cudaStream_t, const float*);
 
 }  // namespace sipg

@@ -36,9 +36,9 @@ inline bool bsr_supported(int dim, int order, int ncomp) { return ncomp == 1 && 
 // Assemble from the operator's FP64 apply (and an FP32 copy when want32).
 void bsr_assemble(sipg_op* op, BsrOp& B, bool want32, cudaStream_t s);
 
-// y = alpha * B x + beta * y (beta == 0: y is not read).
+// y = alpha * B x + beta * c, c = y when null (beta == 0: c is not read).
 template <typename T>
-void bsr_apply(const BsrOp& B, const T* x, T* y, T alpha, T beta, cudaStream_t s);
+void bsr_apply(const BsrOp& B, const T* x, T* y, T alpha, T beta, cudaStream_t s, const T* c = nullptr);
 
 // Greedy distance-2 colouring of the face graph (nbr: K x NF, negative = boundary).
 std::vector<int> distance2_colours(int K, int NF, const int* nbr, int* ncolours);

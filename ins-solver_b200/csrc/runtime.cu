@@ -178,7 +178,7 @@ void sipg_mesh::ensure_device() {
 }
 
 template <typename T>
-void sipg_op::apply(const T* x, T* y, cudaStream_t s, T alpha, T beta) const {
+void sipg_op::apply(const T* x, T* y, cudaStream_t s, T alpha, T beta, const T* c) const {
   constexpr bool f64 = std::is_same<T, double>::value;
   ApplyArgs<T> a;
   a.consts = f64 ? (const T*)dref->c64.p : (const T*)dref->c32.p;
@@ -203,6 +203,7 @@ void sipg_op::apply(const T* x, T* y, cudaStream_t s, T alpha, T beta) const {
   a.eb = f64 ? eb64 : eb32;
   a.alpha = alpha;
   a.beta = beta;
+  a.c = c ? c : y;
   const bool tc = kernel == 0 && ncomp == 1 && (f64 ? dref->tc_ok64 : dref->tc_ok32);
   if (tc) {
     const T* tcc = f64 ? (const T*)dref->tc64.p : (const T*)dref->tc32.p;
@@ -213,8 +214,8 @@ void sipg_op::apply(const T* x, T* y, cudaStream_t s, T alpha, T beta) const {
   }
   SIPG_CUDA(launch_apply<T>(mesh->dim, order, a, num_sms(), s));
 }
-template void sipg_op::apply<double>(const double*, double*, cudaStream_t, double, double) const;
-template void sipg_op::apply<float>(const float*, float*, cudaStream_t, float, float) const;
+template void sipg_op::apply<double>(const double*, double*, cudaStream_t, double, double, const double*) const;
+template void sipg_op::apply<float>(const float*, float*, cudaStream_t, float, float, const float*) const;
 
 void sipg_op::refresh_tau(cudaStream_t s) {
   const double* f = has_factor ? factor64.as<double>() : nullptr;

@@ -88,7 +88,8 @@ struct sipg_op {
   mutable sipg::DevBuf trace64, trace32;  // face traces of the two-pass tensor-core apply
   // Apply on device buffers in precision T.
   template <typename T>
-  void apply(const T* x, T* y, cudaStream_t s, T alpha = T(1), T beta = T(0)) const;
+  // y = alpha A x + beta c, c = y when null (beta == 0: c is not read)
+  void apply(const T* x, T* y, cudaStream_t s, T alpha = T(1), T beta = T(0), const T* c = nullptr) const;
   void refresh_tau(cudaStream_t s);
   sipg::BlockArgs block_args(int mode, int ref_volume, double* out, bool with_pin) const;
   void apply_bc_device(const double* bc, double* rhs, cudaStream_t s) const;

@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(256) sipg_apply_kernel(ApplyArgs<T> a) {
       if (e == a.pin_elem && m == a.pin_node) acc = a.pin_scale * a.x[((size_t)c * a.K + e) * NP + m];
       const size_t yi = ((size_t)c * a.K + e) * NP + m;
       acc *= a.alpha;
-      if (a.beta != T(0)) acc += a.beta * a.y[yi];
+      if (a.beta != T(0)) acc += a.beta * a.c[yi];
       a.y[yi] = acc;
     }
   }

@@ -74,7 +74,8 @@ struct ApplyArgs {
   int pin_elem, pin_node; // pinned DOF (row/column replaced by pin_scale * I), -1: none
   T pin_scale;
   int eb;                 // elements per CTA batch
-  T alpha, beta;          // y = alpha * A x + beta * y (beta == 0: y is not read)
+  T alpha, beta;          // y = alpha * A x + beta * c (beta == 0: c is not read)
+  const T* c;             // ncomp x K x NP; y unless the caller gives another vector
 };
 
 // Host-side launchers (sipg_apply.cu).

@@ -504,7 +504,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_apply_tc_kernel(ApplyArgs<
     const int* snbr = ints;
     const int* scode = ints + TE * NF;
     if (lane == 0 && a.pin_elem >= e0 && a.pin_elem < e0 + ne) sx[(a.pin_elem - e0) * XS + a.pin_node] = T(0);
-    // y values read by the epilogue (beta != 0), loaded now so that their latency
+    // c values read by the epilogue (beta != 0), loaded now so that their latency
     // hides behind the tile's products
     T yold[NT][R][2];
     if (a.beta != T(0)) {
@@ -515,7 +515,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_apply_tc_kernel(ApplyArgs<
 #pragma unroll
           for (int ci = 0; ci < 2; ++ci) {
             const int el = g + 8 * ri, n = 8 * nt + 2 * t + ci;
-            yold[nt][ri][ci] = (el < ne && n < NP) ? a.y[(size_t)(e0 + el) * NP + n] : T(0);
+            yold[nt][ri][ci] = (el < ne && n < NP) ? a.c[(size_t)(e0 + el) * NP + n] : T(0);
           }
     }
     tile_face_geom<T, DIM, P>(sg, sfg, ne, lane);

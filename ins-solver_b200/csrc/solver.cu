@@ -59,10 +59,11 @@ struct Level {
   DevBuf bc64, bc32;             // inverse diagonal blocks, column-major (block-Jacobi smoothing; bc32 in bf16)
   std::unique_ptr<BsrOp> bsr;    // assembled element blocks (low orders), else matrix-free
   int cheb = 4, pre = 1, post = 1;  // Chebyshev degree, smoothing sweeps before / after the coarse correction
+  // y = alpha A x + beta c (c = y when null)
   template <typename T>
-  void apply(const T* x, T* y, cudaStream_t s, T alpha = T(1), T beta = T(0)) const {
-    if (bsr) bsr_apply<T>(*bsr, x, y, alpha, beta, s);
-    else op->apply<T>(x, y, s, alpha, beta);
+  void apply(const T* x, T* y, cudaStream_t s, T alpha = T(1), T beta = T(0), const T* c = nullptr) const {
+    if (bsr) bsr_apply<T>(*bsr, x, y, alpha, beta, s, c);
+    else op->apply<T>(x, y, s, alpha, beta, c);
   }
 };
 
@@ -114,9 +115,13 @@ struct DevCsr {
     }
   }
   template <typename T>
-  void mv(const T* x, T* y, T alpha, T beta, cudaStream_t s) const {
-    const T* v = std::is_same<T, float>::value ? (const T*)v32.p : (const T*)v64.p;
-    csr_spmv<T>(rows, ptr.as<int>(), idx.as<int>(), v, x, y, alpha, beta, s);
+  const T* vals() const {
+    return std::is_same<T, float>::value ? (const T*)v32.p : (const T*)v64.p;
+  }
+  // y = alpha A x + beta c (c = y when null)
+  template <typename T>
+  void mv(const T* x, T* y, T alpha, T beta, cudaStream_t s, const T* c = nullptr) const {
+    csr_spmv<T>(rows, ptr.as<int>(), idx.as<int>(), vals<T>(), x, y, alpha, beta, s, c);
   }
 };
 
@@ -126,6 +131,7 @@ struct AmgDevLevel {
   DevBuf dinv64, dinv32;
   double lmax = 0.0;
   DevBuf rhs, z, res, d;
+  DevBuf res2, d2;  // the fused Chebyshev steps alternate between (d, res) and (d2, res2)
 };
 
 // Power iteration on D^-1 A for a host CSR matrix, same start vector and steps as
@@ -267,12 +273,12 @@ struct sipg_solver {
   void setup();
   void setup_pmg();
   template <typename T> void vcycle(int l);
-  template <typename T> void chebyshev(Level& L, bool want_res);
-  template <typename T> void smooth(Level& L, int sweeps, bool want_res);
+  template <typename T> void chebyshev(Level& L, bool want_res, bool first);
+  template <typename T> void smooth(Level& L, int sweeps, bool want_res, bool first);
   template <typename T> void coarse(Level& L);
   template <typename T> void amg_vcycle(int l);
   template <typename T> void last_level_amg(Level& L);
-  template <typename T> void csr_chebyshev(AmgDevLevel& A, bool want_res);
+  template <typename T> const T* csr_chebyshev(AmgDevLevel& A, const T* rin, bool first, bool want_res);
   void setup_amg();
   void precondition(const double* rin, double* zout);
   int solve(const double* b, double* x, sipg_solve_info* info);
@@ -490,6 +496,8 @@ void sipg_solver::setup_amg() {
     D.z = DevBuf(D.n * ts);
     D.res = DevBuf(D.n * ts);
     D.d = DevBuf(D.n * ts);
+    D.res2 = DevBuf(D.n * ts);
+    D.d2 = DevBuf(D.n * ts);
   }
   cinv_n = H.coarse_n;
   cinv64 = DevBuf(H.coarse_inv.size() * sizeof(double));
@@ -542,8 +550,11 @@ void sipg_solver::setup() {
   dirty = false;
 }
 
+// One Chebyshev sweep on z with the residual res kept current (except, when
+// !want_res, after the last step). `first`: z = 0 and res = rhs before the sweep,
+// which the first step reads from rhs directly (no zeroing or copy).
 template <typename T>
-void sipg_solver::chebyshev(Level& L, bool want_res) {
+void sipg_solver::chebyshev(Level& L, bool want_res, bool first) {
   const double hi = L.lmax * o.eig_safety, lo = hi / o.eig_ratio;
   const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
   double rho_old = 1.0 / sigma;
@@ -559,23 +570,25 @@ void sipg_solver::chebyshev(Level& L, bool want_res) {
       c2 = 2.0 * rho / delta;
       rho_old = rho;
     }
+    const bool from_rhs = first && it == 0;
+    const T* rin = from_rhs ? L.rhs.as<T>() : res;
     if (L.bc32.p && std::is_same<T, float>::value) {
-      cheb_step_block<float, __nv_bfloat16>((float*)d, (float*)z, (const float*)res, L.bc32.as<__nv_bfloat16>(),
-                                            (float)c1, (float)c2, (int)(L.n / L.Np), L.Np, stream);
+      cheb_step_block<float, __nv_bfloat16>((float*)d, (float*)z, (const float*)rin, L.bc32.as<__nv_bfloat16>(),
+                                            (float)c1, (float)c2, (int)(L.n / L.Np), L.Np, stream, from_rhs);
     } else if (L.bc64.p) {
-      cheb_step_block<T, T>(d, z, res, (const T*)L.bc64.p, (T)c1, (T)c2, (int)(L.n / L.Np), L.Np, stream);
+      cheb_step_block<T, T>(d, z, rin, (const T*)L.bc64.p, (T)c1, (T)c2, (int)(L.n / L.Np), L.Np, stream, from_rhs);
     } else {
-      cheb_step<T>(d, z, res, dinv, (T)c1, (T)c2, L.n, stream);
+      cheb_step<T>(d, z, rin, dinv, (T)c1, (T)c2, L.n, stream, from_rhs);
     }
-    if (it < L.cheb - 1 || want_res) L.apply<T>(d, res, stream, T(-1), T(1));
+    if (it < L.cheb - 1 || want_res) L.apply<T>(d, res, stream, T(-1), T(1), rin);
   }
 }
 
 // `sweeps` Chebyshev sweeps on z with residual res; the residual is kept current
-// except, when !want_res, after the last sweep.
+// except, when !want_res, after the last sweep. `first`: from z = 0, res = rhs.
 template <typename T>
-void sipg_solver::smooth(Level& L, int sweeps, bool want_res) {
-  for (int k = 0; k < sweeps; ++k) chebyshev<T>(L, k < sweeps - 1 || want_res);
+void sipg_solver::smooth(Level& L, int sweeps, bool want_res, bool first) {
+  for (int k = 0; k < sweeps; ++k) chebyshev<T>(L, k < sweeps - 1 || want_res, first && k == 0);
 }
 
 template <typename T>
@@ -606,12 +619,20 @@ void sipg_solver::coarse(Level& L) {
   }
 }
 
+// Chebyshev sweep on an algebraic level from the residual rin (z = 0 before it when
+// `first`), one fused kernel per step; returns the final residual (null when
+// !want_res).
 template <typename T>
-void sipg_solver::csr_chebyshev(AmgDevLevel& A, bool want_res) {
+const T* sipg_solver::csr_chebyshev(AmgDevLevel& A, const T* rin, bool first, bool want_res) {
   const double hi = A.lmax * o.eig_safety, lo = hi / o.eig_ratio;
   const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
   double rho_old = 1.0 / sigma;
   const T* dinv = std::is_same<T, float>::value ? (const T*)A.dinv32.p : (const T*)A.dinv64.p;
+  T* dbuf[2] = {A.d.as<T>(), A.d2.as<T>()};
+  T* rbuf[2] = {A.res.as<T>(), A.res2.as<T>()};
+  const T* dcur = nullptr;  // not read by the first step (c1 = 0)
+  const T* rcur = rin;
+  int ob = rin == rbuf[0] ? 1 : 0;
   for (int it = 0; it < o.cheb_order; ++it) {
     double c1 = 0.0, c2 = 1.0 / theta;
     if (it > 0) {
@@ -620,9 +641,15 @@ void sipg_solver::csr_chebyshev(AmgDevLevel& A, bool want_res) {
       c2 = 2.0 * rho / delta;
       rho_old = rho;
     }
-    cheb_step<T>(A.d.as<T>(), A.z.as<T>(), A.res.as<T>(), dinv, (T)c1, (T)c2, A.n, stream);
-    if (it < o.cheb_order - 1 || want_res) A.A.mv<T>(A.d.as<T>(), A.res.as<T>(), T(-1), T(1), stream);
+    T* dn = dbuf[ob];
+    T* rn = (it < o.cheb_order - 1 || want_res) ? rbuf[ob] : nullptr;
+    csr_cheb<T>(A.n, A.A.ptr.as<int>(), A.A.idx.as<int>(), A.A.vals<T>(), dcur ? dcur : dn, rcur, dinv, dn, rn,
+                A.z.as<T>(), (T)c1, (T)c2, first && it == 0, stream);
+    dcur = dn;
+    rcur = rn;
+    ob ^= 1;
   }
+  return rcur;
 }
 
 template <typename T>
@@ -634,31 +661,30 @@ void sipg_solver::amg_vcycle(int l) {
     return;
   }
   AmgDevLevel& Cn = al[l + 1];
-  vzero<T>(A.z.as<T>(), A.n, stream);
-  vcopy<T>(A.res.as<T>(), A.rhs.as<T>(), A.n, stream);
-  csr_chebyshev<T>(A, true);
-  A.R.mv<T>(A.res.as<T>(), Cn.rhs.as<T>(), T(1), T(0), stream);
+  const T* r = csr_chebyshev<T>(A, A.rhs.as<T>(), true, true);
+  A.R.mv<T>(r, Cn.rhs.as<T>(), T(1), T(0), stream);
   amg_vcycle<T>(l + 1);
   A.P.mv<T>(Cn.z.as<T>(), A.z.as<T>(), T(1), T(1), stream);
-  vcopy<T>(A.res.as<T>(), A.rhs.as<T>(), A.n, stream);
-  A.A.mv<T>(A.z.as<T>(), A.res.as<T>(), T(-1), T(1), stream);
-  csr_chebyshev<T>(A, false);
+  A.A.mv<T>(A.z.as<T>(), A.res2.as<T>(), T(-1), T(1), stream, A.rhs.as<T>());
+  csr_chebyshev<T>(A, A.res2.as<T>(), false, false);
 }
 
 // Lowest order with the algebraic coarse space: Chebyshev, R_dg, AMG V-cycle,
 // P_dg, Chebyshev.
 template <typename T>
 void sipg_solver::last_level_amg(Level& L) {
-  vzero<T>(L.z.as<T>(), L.n, stream);
-  vcopy<T>(L.res.as<T>(), L.rhs.as<T>(), L.n, stream);
-  smooth<T>(L, L.pre, true);
-  Rdg.mv<T>(L.res.as<T>(), al[0].rhs.as<T>(), T(1), T(0), stream);
+  if (L.pre > 0) {
+    smooth<T>(L, L.pre, true, true);
+    Rdg.mv<T>(L.res.as<T>(), al[0].rhs.as<T>(), T(1), T(0), stream);
+  } else {
+    vzero<T>(L.z.as<T>(), L.n, stream);
+    Rdg.mv<T>(L.rhs.as<T>(), al[0].rhs.as<T>(), T(1), T(0), stream);
+  }
   amg_vcycle<T>(0);
   Pdg.mv<T>(al[0].z.as<T>(), L.z.as<T>(), T(1), T(1), stream);
   if (L.post > 0) {
-    vcopy<T>(L.res.as<T>(), L.rhs.as<T>(), L.n, stream);
-    L.apply<T>(L.z.as<T>(), L.res.as<T>(), stream, T(-1), T(1));
-    smooth<T>(L, L.post, false);
+    L.apply<T>(L.z.as<T>(), L.res.as<T>(), stream, T(-1), T(1), L.rhs.as<T>());
+    smooth<T>(L, L.post, false, false);
   }
 }
 
@@ -675,16 +701,18 @@ void sipg_solver::vcycle(int l) {
   const bool f32 = std::is_same<T, float>::value;
   const T* P = f32 ? (const T*)L.P32.p : (const T*)L.P64.p;
   const int K = op->mesh->K, nc = op->ncomp;
-  vzero<T>(L.z.as<T>(), L.n, stream);
-  vcopy<T>(L.res.as<T>(), L.rhs.as<T>(), L.n, stream);
-  smooth<T>(L, L.pre, true);
-  restrict_elem<T>(Cl.rhs.as<T>(), L.res.as<T>(), P, K, L.Np, Cl.Np, nc, stream);
+  if (L.pre > 0) {
+    smooth<T>(L, L.pre, true, true);
+    restrict_elem<T>(Cl.rhs.as<T>(), L.res.as<T>(), P, K, L.Np, Cl.Np, nc, stream);
+  } else {
+    vzero<T>(L.z.as<T>(), L.n, stream);
+    restrict_elem<T>(Cl.rhs.as<T>(), L.rhs.as<T>(), P, K, L.Np, Cl.Np, nc, stream);
+  }
   vcycle<T>(l + 1);
   prolong_add<T>(L.z.as<T>(), Cl.z.as<T>(), P, K, L.Np, Cl.Np, nc, stream);
   if (L.post > 0) {
-    vcopy<T>(L.res.as<T>(), L.rhs.as<T>(), L.n, stream);
-    L.apply<T>(L.z.as<T>(), L.res.as<T>(), stream, T(-1), T(1));
-    smooth<T>(L, L.post, false);
+    L.apply<T>(L.z.as<T>(), L.res.as<T>(), stream, T(-1), T(1), L.rhs.as<T>());
+    smooth<T>(L, L.post, false, false);
   }
 }
 
@@ -883,18 +911,33 @@ int sipg_solver::solve(const double* b, double* x_user, sipg_solve_info* info) {
       // once per launch of at most kLoopChunk iterations.
       constexpr int kLoopChunk = 64;
       dot(R, Z, S_RZ);
+      // mixed p-multigrid: the nullspace projections, the FP32 / FP64 conversions and
+      // the dots ride on the vector passes next to them
+      const bool fused = kind == SIPG_SOLVER_PMULTIGRID && o.precision == SIPG_FP32;
+      const int mean_slot = o.nullspace ? (int)S_SUM : -1;
       auto body = [&] {
         op->apply<double>(Pv, AP, stream);
-        dot(Pv, AP, S_PAP);                                              // cg3_alpha_pre
-        cg_update_xr(x, R, Pv, AP, n, S(), S_RZ, S_PAP, S() + S_RR, rw, stream);  // update_ans + update_res
-        if (o.nullspace) {
-          vsum<double>(R, n, S() + S_SUM, rw, stream);
-          sub_mean<double>(R, n, S(), S_SUM, stream);
-          dot(R, R, S_RR);
+        dot(Pv, AP, S_PAP);  // cg3_alpha_pre
+        if (fused) {
+          // update_ans + update_res, projection, r . r, r . z_old, r to FP32
+          if (o.nullspace) cg_update_xr_sum(x, R, Pv, AP, n, S(), S_RZ, S_PAP, S() + S_SUM, S_TMP - S_SUM, rw, stream);
+          else cg_update_xr(x, R, Pv, AP, n, S(), S_RZ, S_PAP, S() + S_TMP, rw, stream);
+          resid_prep(R, lv[0].rhs.as<float>(), Z, n, S(), mean_slot, S() + S_RR, S_RZO - S_RR, rw, stream);
+          vcycle<float>(0);
+          // z to FP64, projection, r . z_new
+          if (o.nullspace) to_f64_sum(Z, lv[0].z.as<float>(), n, S() + S_SUM, rw, stream);
+          finish_z_dot(Z, o.nullspace ? nullptr : lv[0].z.as<float>(), R, n, S(), mean_slot, S() + S_RZN, rw, stream);
+        } else {
+          cg_update_xr(x, R, Pv, AP, n, S(), S_RZ, S_PAP, S() + S_RR, rw, stream);  // update_ans + update_res
+          if (o.nullspace) {
+            vsum<double>(R, n, S() + S_SUM, rw, stream);
+            sub_mean<double>(R, n, S(), S_SUM, stream);
+            dot(R, R, S_RR);
+          }
+          dot(R, Z, S_RZO);
+          precondition(R, Z);
+          dot(R, Z, S_RZN);
         }
-        dot(R, Z, S_RZO);
-        precondition(R, Z);
-        dot(R, Z, S_RZN);
         k_beta_flex<<<1, 1, 0, stream>>>(S());  // cg3_compute_beta_pre_flex
         note_launch();
         update_p<double>(Pv, Z, n, S(), S_BETA, S_RZP, stream);

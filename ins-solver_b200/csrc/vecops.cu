@@ -129,6 +129,78 @@ __global__ void __launch_bounds__(kRedThreads) k_cg_update_xr(double* x, double*
   finish<1>(v, partial, counter, rr_out, 1);
 }
 
+// x += alpha p ; r -= alpha Ap ; out[0] = sum r, out[stride] = r . r
+__global__ void __launch_bounds__(kRedThreads) k_cg_update_xr_sum(double* x, double* r, const double* p,
+                                                                  const double* Ap, size_t n, const double* scal,
+                                                                  int num, int den, double* partial,
+                                                                  unsigned* counter, double* out, int stride) {
+  pdl_enter();
+  const double alpha = scal[num] / scal[den];
+  double v[2] = {0.0, 0.0};
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    x[i] += alpha * p[i];
+    double ri = r[i] - alpha * Ap[i];
+    r[i] = ri;
+    v[0] += ri;
+    v[1] += ri * ri;
+  }
+  block_sum<2>(v);
+  finish<2>(v, partial, counter, out, stride);
+}
+
+// r -= mean (scal[mean_slot] / n; none when mean_slot < 0); r32 = (float) r;
+// out[0] = r . r, out[stride] = r . zo
+__global__ void __launch_bounds__(kRedThreads) k_resid_prep(double* r, float* r32, const double* zo, size_t n,
+                                                            const double* scal, int mean_slot, double* partial,
+                                                            unsigned* counter, double* out, int stride) {
+  pdl_enter();
+  const double m = mean_slot >= 0 ? scal[mean_slot] / (double)n : 0.0;
+  double v[2] = {0.0, 0.0};
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    double ri = r[i];
+    if (mean_slot >= 0) {
+      ri -= m;
+      r[i] = ri;
+    }
+    r32[i] = (float)ri;
+    v[0] += ri * ri;
+    v[1] += ri * zo[i];
+  }
+  block_sum<2>(v);
+  finish<2>(v, partial, counter, out, stride);
+}
+
+// z = (double) z32 ; out = sum z
+__global__ void __launch_bounds__(kRedThreads) k_to_f64_sum(double* z, const float* z32, size_t n, double* partial,
+                                                            unsigned* counter, double* out) {
+  pdl_enter();
+  double v[1] = {0.0};
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double zi = (double)z32[i];
+    z[i] = zi;
+    v[0] += zi;
+  }
+  block_sum<1>(v);
+  finish<1>(v, partial, counter, out, 1);
+}
+
+// z = (z32 ? (double) z32 : z) - mean (scal[mean_slot] / n; none when mean_slot < 0); out = r . z
+__global__ void __launch_bounds__(kRedThreads) k_finish_z_dot(double* z, const float* z32, const double* r,
+                                                              size_t n, const double* scal, int mean_slot,
+                                                              double* partial, unsigned* counter, double* out) {
+  pdl_enter();
+  const double m = mean_slot >= 0 ? scal[mean_slot] / (double)n : 0.0;
+  double v[1] = {0.0};
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    double zi = z32 ? (double)z32[i] : z[i];
+    if (mean_slot >= 0) zi -= m;
+    z[i] = zi;
+    v[0] += r[i] * zi;
+  }
+  block_sum<1>(v);
+  finish<1>(v, partial, counter, out, 1);
+}
+
 template <typename T>
 __global__ void k_update_p(T* p, const T* z, size_t n, const double* scal, int num, int den) {
   pdl_enter();
@@ -169,12 +241,12 @@ __global__ void k_jacobi(T* z, const T* r, const T* dinv, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) z[i] = dinv[i] * r[i];
 }
 template <typename T>
-__global__ void k_cheb(T* d, T* z, const T* res, const T* dinv, T c1, T c2, size_t n) {
+__global__ void k_cheb(T* d, T* z, const T* res, const T* dinv, T c1, T c2, size_t n, int first) {
   pdl_enter();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     T di = (c1 != T(0) ? c1 * d[i] : T(0)) + c2 * dinv[i] * res[i];
     d[i] = di;
-    z[i] += di;
+    z[i] = first ? di : z[i] + di;
   }
 }
 
@@ -186,7 +258,7 @@ __device__ __forceinline__ float blk_val(const float* p) { return *p; }
 __device__ __forceinline__ double blk_val(const double* p) { return *p; }
 
 template <typename T, typename TB>
-__global__ void k_cheb_block(T* d, T* z, const T* res, const TB* Bc, T c1, T c2, int nb, int Np) {
+__global__ void k_cheb_block(T* d, T* z, const T* res, const TB* Bc, T c1, T c2, int nb, int Np, int first) {
   pdl_enter();
   const size_t total = (size_t)nb * Np;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
@@ -198,7 +270,7 @@ __global__ void k_cheb_block(T* d, T* z, const T* res, const TB* Bc, T c1, T c2,
     for (int c = 0; c < Np; ++c) s += (T)blk_val(Bb + (size_t)c * Np) * rb[c];
     const T di = (c1 != T(0) ? c1 * d[i] : T(0)) + c2 * s;
     d[i] = di;
-    z[i] += di;
+    z[i] = first ? di : z[i] + di;
   }
 }
 
@@ -220,7 +292,7 @@ template <> struct Vec2<double> { using t = double2; };
 
 // Same step, two rows per thread with paired loads (even Np).
 template <typename T, typename TB>
-__global__ void k_cheb_block2(T* d, T* z, const T* res, const TB* Bc, T c1, T c2, int nb, int Np) {
+__global__ void k_cheb_block2(T* d, T* z, const T* res, const TB* Bc, T c1, T c2, int nb, int Np, int first) {
   pdl_enter();
   using V = typename Vec2<T>::t;
   const int hp = Np / 2;
@@ -238,9 +310,11 @@ __global__ void k_cheb_block2(T* d, T* z, const T* res, const TB* Bc, T c1, T c2
       s1 += (T)v.y * rc;
     }
     const size_t o = b * Np + r;
-    V dv = *reinterpret_cast<const V*>(d + o), zv = *reinterpret_cast<const V*>(z + o);
-    dv.x = (c1 != T(0) ? c1 * dv.x : T(0)) + c2 * s0;
-    dv.y = (c1 != T(0) ? c1 * dv.y : T(0)) + c2 * s1;
+    V dv{T(0), T(0)}, zv{T(0), T(0)};
+    if (c1 != T(0)) dv = *reinterpret_cast<const V*>(d + o);
+    if (!first) zv = *reinterpret_cast<const V*>(z + o);
+    dv.x = c1 * dv.x + c2 * s0;
+    dv.y = c1 * dv.y + c2 * s1;
     zv.x += dv.x;
     zv.y += dv.y;
     *reinterpret_cast<V*>(d + o) = dv;
@@ -360,7 +434,7 @@ __global__ void k_shift_scalar(double* scal, int from, int to) {
 // Eight lanes per row (the algebraic levels are small: parallelism, not bytes, limits them).
 template <typename T>
 __global__ void k_csr_spmv(int rows, const int* __restrict__ ptr, const int* __restrict__ idx,
-                           const T* __restrict__ val, const T* __restrict__ x, T* y, T alpha, T beta) {
+                           const T* __restrict__ val, const T* __restrict__ x, T* y, T alpha, T beta, const T* c) {
   pdl_enter();
   const int lane = threadIdx.x & 31, sub = lane & 7;
   const int warps = (gridDim.x * blockDim.x) >> 5;
@@ -371,7 +445,39 @@ __global__ void k_csr_spmv(int rows, const int* __restrict__ ptr, const int* __r
       for (int k = ptr[r] + sub; k < ptr[r + 1]; k += 8) s += val[k] * x[idx[k]];
 #pragma unroll
     for (int o = 4; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, 8);
-    if (r < rows && sub == 0) y[r] = beta != T(0) ? alpha * s + beta * y[r] : alpha * s;
+    if (r < rows && sub == 0) y[r] = beta != T(0) ? alpha * s + beta * c[r] : alpha * s;
+  }
+}
+
+// One Chebyshev step of an algebraic level fused with its residual update, eight
+// lanes per row:  dn = c1 d + c2 dinv r ; z = (first ? 0 : z) + dn ; rn = r - A dn
+// (rn skipped when null). d and r are only read (rows read their neighbours'
+// entries), dn and rn are other buffers; c1 == 0 reads no d.
+template <typename T>
+__device__ __forceinline__ T cheb_dir(const T* d, const T* r, const T* dinv, int j, T c1, T c2) {
+  return (c1 != T(0) ? c1 * d[j] : T(0)) + c2 * dinv[j] * r[j];
+}
+template <typename T>
+__global__ void k_csr_cheb(int rows, const int* __restrict__ ptr, const int* __restrict__ idx,
+                           const T* __restrict__ val, const T* __restrict__ d, const T* __restrict__ r,
+                           const T* __restrict__ dinv, T* __restrict__ dn, T* __restrict__ rn, T* z, T c1, T c2,
+                           int first) {
+  pdl_enter();
+  const int lane = threadIdx.x & 31, sub = lane & 7;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; 4 * w < rows; w += warps) {
+    const int i = 4 * w + (lane >> 3);
+    T s = T(0);
+    if (i < rows && rn)
+      for (int k = ptr[i] + sub; k < ptr[i + 1]; k += 8) s += val[k] * cheb_dir(d, r, dinv, idx[k], c1, c2);
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, 8);
+    if (i < rows && sub == 0) {
+      const T di = cheb_dir(d, r, dinv, i, c1, c2);
+      dn[i] = di;
+      z[i] = first ? di : z[i] + di;
+      if (rn) rn[i] = r[i] - s;
+    }
   }
 }
 
@@ -435,6 +541,29 @@ void cg_update_xr(double* x, double* r, const double* p, const double* Ap, size_
   note_launch();
 }
 
+void cg_update_xr_sum(double* x, double* r, const double* p, const double* Ap, size_t n, const double* scal, int num,
+                      int den, double* out, int stride, const RedWork& w, cudaStream_t s) {
+  pdl_launch(k_cg_update_xr_sum, dim3(kRedBlocks), dim3(kRedThreads), 0, s, x, r, p, Ap, n, scal, num, den, w.partial,
+             w.counter, out, stride);
+  note_launch();
+}
+void resid_prep(double* r, float* r32, const double* zo, size_t n, const double* scal, int mean_slot, double* out,
+                int stride, const RedWork& w, cudaStream_t s) {
+  pdl_launch(k_resid_prep, dim3(kRedBlocks), dim3(kRedThreads), 0, s, r, r32, zo, n, scal, mean_slot, w.partial,
+             w.counter, out, stride);
+  note_launch();
+}
+void to_f64_sum(double* z, const float* z32, size_t n, double* out, const RedWork& w, cudaStream_t s) {
+  pdl_launch(k_to_f64_sum, dim3(kRedBlocks), dim3(kRedThreads), 0, s, z, z32, n, w.partial, w.counter, out);
+  note_launch();
+}
+void finish_z_dot(double* z, const float* z32, const double* r, size_t n, const double* scal, int mean_slot,
+                  double* out, const RedWork& w, cudaStream_t s) {
+  pdl_launch(k_finish_z_dot, dim3(kRedBlocks), dim3(kRedThreads), 0, s, z, z32, r, n, scal, mean_slot, w.partial,
+             w.counter, out);
+  note_launch();
+}
+
 template <typename T>
 void update_p(T* p, const T* z, size_t n, const double* scal, int num, int den, cudaStream_t s) {
   pdl_launch(k_update_p<T>, dim3(grid_for(n)), dim3(256), 0, s, p, z, n, scal, num, den);
@@ -464,16 +593,18 @@ void to_f64(double* dst, const float* src, size_t n, cudaStream_t s) {
   note_launch();
 }
 template <typename T, typename TB>
-void cheb_step_block(T* d, T* z, const T* res, const TB* Bc, T c1, T c2, int nb, int Np, cudaStream_t s) {
+void cheb_step_block(T* d, T* z, const T* res, const TB* Bc, T c1, T c2, int nb, int Np, cudaStream_t s,
+                     bool first) {
   if (Np % 2 == 0)
     pdl_launch(k_cheb_block2<T, TB>, dim3(grid_for((size_t)nb * Np / 2)), dim3(256), 0, s, d, z, res, Bc, c1, c2,
-               nb, Np);
+               nb, Np, (int)first);
   else
-    pdl_launch(k_cheb_block<T, TB>, dim3(grid_for((size_t)nb * Np)), dim3(256), 0, s, d, z, res, Bc, c1, c2, nb, Np);
+    pdl_launch(k_cheb_block<T, TB>, dim3(grid_for((size_t)nb * Np)), dim3(256), 0, s, d, z, res, Bc, c1, c2, nb, Np,
+               (int)first);
   note_launch();
 }
 template void cheb_step_block<float, __nv_bfloat16>(float*, float*, const float*, const __nv_bfloat16*, float, float,
-                                                    int, int, cudaStream_t);
+                                                    int, int, cudaStream_t, bool);
 template void block_transpose<__nv_bfloat16>(__nv_bfloat16*, const double*, int, int, cudaStream_t);
 template <typename T>
 void block_transpose(T* dst, const double* src, int nb, int Np, cudaStream_t s) {
@@ -486,8 +617,8 @@ void jacobi(T* z, const T* r, const T* dinv, size_t n, cudaStream_t s) {
   note_launch();
 }
 template <typename T>
-void cheb_step(T* d, T* z, const T* res, const T* dinv, T c1, T c2, size_t n, cudaStream_t s) {
-  pdl_launch(k_cheb<T>, dim3(grid_for(n)), dim3(256), 0, s, d, z, res, dinv, c1, c2, n);
+void cheb_step(T* d, T* z, const T* res, const T* dinv, T c1, T c2, size_t n, cudaStream_t s, bool first) {
+  pdl_launch(k_cheb<T>, dim3(grid_for(n)), dim3(256), 0, s, d, z, res, dinv, c1, c2, n, (int)first);
   note_launch();
 }
 template <typename T>
@@ -527,9 +658,17 @@ void coarse_update_p(T* p, const T* sv, size_t n, double* scal, cudaStream_t s) 
 
 template <typename T>
 void csr_spmv(int rows, const int* ptr, const int* idx, const T* val, const T* x, T* y, T alpha, T beta,
-              cudaStream_t s) {
+              cudaStream_t s, const T* c) {
   const int blocks = std::max(1, std::min((rows + 31) / 32, 148 * 16));
-  pdl_launch(k_csr_spmv<T>, dim3(blocks), dim3(256), 0, s, rows, ptr, idx, val, x, y, alpha, beta);
+  pdl_launch(k_csr_spmv<T>, dim3(blocks), dim3(256), 0, s, rows, ptr, idx, val, x, y, alpha, beta, c ? c : y);
+  note_launch();
+}
+template <typename T>
+void csr_cheb(int rows, const int* ptr, const int* idx, const T* val, const T* d, const T* r, const T* dinv, T* dn,
+              T* rn, T* z, T c1, T c2, bool first, cudaStream_t s) {
+  const int blocks = std::max(1, std::min((rows + 31) / 32, 148 * 16));
+  pdl_launch(k_csr_cheb<T>, dim3(blocks), dim3(256), 0, s, rows, ptr, idx, val, d, r, dinv, dn, rn, z, c1, c2,
+             (int)first);
   note_launch();
 }
 template <typename T>
@@ -553,9 +692,9 @@ void vadd(T* y, const T* x, size_t n, cudaStream_t s) {
   template void vcopy<T>(T*, const T*, size_t, cudaStream_t);                                    \
   template void vzero<T>(T*, size_t, cudaStream_t);                                              \
   template void jacobi<T>(T*, const T*, const T*, size_t, cudaStream_t);                         \
-  template void cheb_step<T>(T*, T*, const T*, const T*, T, T, size_t, cudaStream_t);            \
+  template void cheb_step<T>(T*, T*, const T*, const T*, T, T, size_t, cudaStream_t, bool);      \
   template void block_matvec<T>(T*, const T*, const T*, int, int, cudaStream_t);                 \
-  template void cheb_step_block<T, T>(T*, T*, const T*, const T*, T, T, int, int, cudaStream_t);  \
+  template void cheb_step_block<T, T>(T*, T*, const T*, const T*, T, T, int, int, cudaStream_t, bool); \
   template void block_transpose<T>(T*, const double*, int, int, cudaStream_t);                     \
   template void inv_mass<T>(T*, const T*, const T*, const T*, int, int, int, int, int, T,        \
                             cudaStream_t);                                                       \
@@ -564,7 +703,9 @@ void vadd(T* y, const T* x, size_t n, cudaStream_t s) {
   template void coarse_update<T>(T*, T*, T*, const T*, const T*, const T*, size_t, double*,      \
                                  const RedWork&, cudaStream_t);                                  \
   template void coarse_update_p<T>(T*, const T*, size_t, double*, cudaStream_t);                 \
-  template void csr_spmv<T>(int, const int*, const int*, const T*, const T*, T*, T, T, cudaStream_t); \
+  template void csr_spmv<T>(int, const int*, const int*, const T*, const T*, T*, T, T, cudaStream_t, const T*); \
+  template void csr_cheb<T>(int, const int*, const int*, const T*, const T*, const T*, const T*, T*, T*, T*, T, T, \
+                            bool, cudaStream_t);                                                   \
   template void dense_mv<T>(int, const T*, const T*, T*, cudaStream_t);                          \
   template void vadd<T>(T*, const T*, size_t, cudaStream_t);
 

@@ -63,6 +63,19 @@ void vsum(const T* a, size_t n, double* out, const RedWork& w, cudaStream_t s);
 void cg_update_xr(double* x, double* r, const double* p, const double* Ap, size_t n,
                   const double* scal, int num, int den, double* rr_out, const RedWork& w,
                   cudaStream_t s);
+// Fused steps of the mixed-precision outer iteration (two-output reductions write
+// out[0] and out[stride]):
+//   x += alpha p ; r -= alpha Ap ; out = (sum r, r . r)
+void cg_update_xr_sum(double* x, double* r, const double* p, const double* Ap, size_t n, const double* scal, int num,
+                      int den, double* out, int stride, const RedWork& w, cudaStream_t s);
+//   r -= mean (scal[mean_slot] / n, none when mean_slot < 0) ; r32 = r ; out = (r . r, r . zo)
+void resid_prep(double* r, float* r32, const double* zo, size_t n, const double* scal, int mean_slot, double* out,
+                int stride, const RedWork& w, cudaStream_t s);
+//   z = z32 ; out = sum z
+void to_f64_sum(double* z, const float* z32, size_t n, double* out, const RedWork& w, cudaStream_t s);
+//   z = (z32 ? z32 : z) - mean (as above) ; out = r . z
+void finish_z_dot(double* z, const float* z32, const double* r, size_t n, const double* scal, int mean_slot,
+                  double* out, const RedWork& w, cudaStream_t s);
 // p = z + beta p   with beta = scal[num] / scal[den]
 template <typename T>
 void update_p(T* p, const T* z, size_t n, const double* scal, int num, int den, cudaStream_t s);
@@ -81,12 +94,13 @@ void to_f64(double* dst, const float* src, size_t n, cudaStream_t s);
 template <typename T>
 void jacobi(T* z, const T* r, const T* dinv, size_t n, cudaStream_t s);
 
-// Chebyshev step: d = c1 * d + c2 * dinv * res ; z += d
+// Chebyshev step: d = c1 * d + c2 * dinv * res ; z += d  (first: z = d; c1 == 0 reads no d)
 template <typename T>
-void cheb_step(T* d, T* z, const T* res, const T* dinv, T c1, T c2, size_t n, cudaStream_t s);
+void cheb_step(T* d, T* z, const T* res, const T* dinv, T c1, T c2, size_t n, cudaStream_t s, bool first = false);
 // d <- c1 d + c2 Bc res, z += d with column-major inverse diagonal blocks Bc (nb blocks of Np x Np)
 template <typename T, typename TB>
-void cheb_step_block(T* d, T* z, const T* res, const TB* Bc, T c1, T c2, int nb, int Np, cudaStream_t s);
+void cheb_step_block(T* d, T* z, const T* res, const TB* Bc, T c1, T c2, int nb, int Np, cudaStream_t s,
+                     bool first = false);
 template <typename T>
 void block_transpose(T* dst, const double* src, int nb, int Np, cudaStream_t s);
 
@@ -115,10 +129,16 @@ void coarse_update(T* z, T* r, T* sv, const T* p, const T* Ap, const T* dinv, si
 template <typename T>
 void coarse_update_p(T* p, const T* sv, size_t n, double* scal, cudaStream_t s);
 
-// y = alpha * A x + beta * y for a CSR matrix (beta == 0: y is not read)
+// y = alpha * A x + beta * c for a CSR matrix (c = y when null; beta == 0: c is not read)
 template <typename T>
 void csr_spmv(int rows, const int* ptr, const int* idx, const T* val, const T* x, T* y, T alpha, T beta,
-              cudaStream_t s);
+              cudaStream_t s, const T* c = nullptr);
+// Chebyshev step fused with the residual update on a CSR level:
+//   dn = c1 d + c2 dinv r ; z = (first ? 0 : z) + dn ; rn = r - A dn (rn may be null)
+// dn, rn must not alias d, r; c1 == 0 reads no d.
+template <typename T>
+void csr_cheb(int rows, const int* ptr, const int* idx, const T* val, const T* d, const T* r, const T* dinv, T* dn,
+              T* rn, T* z, T c1, T c2, bool first, cudaStream_t s);
 // y = M x for a dense row-major n x n matrix
 template <typename T>
 void dense_mv(int n, const T* M, const T* x, T* y, cudaStream_t s);
