@@ -307,7 +307,7 @@ def run_ours(args):
     }
     out["config_2d"] = run_config_2d()
     if not args.skip_serving:
-        out["serving"] = run_serving(seed=1234 + rank)
+        out["serving"] = serving_sweep(seed=1234 + rank)
     if rank == 0 and world == 1 and not args.skip_cpu:
         out["cpu_baseline"] = cpu_reference(c, op, int(inf64[-1].iters), sample_only=True)
     if world > 1:
@@ -368,6 +368,17 @@ def serving_opts(order, singular, precision):
     for i in range(order):
         o.orders[i] = order - i
     return o
+
+
+def serving_sweep(seed):
+    """The served stream below capacity (400 arrivals/s: latency) and above it
+    (2000/s: the throughput the server sustains); the headline fields are the
+    saturated run's."""
+    low = run_serving(seed, n_req=96, rate=400.0)
+    high = run_serving(seed, n_req=192, rate=2000.0)
+    keys = ("solves_per_s", "p50_ms", "p99_ms", "failed")
+    return {**high, "sweep": [{"rate_per_s": 400.0, **{k: low[k] for k in keys}},
+                              {"rate_per_s": 2000.0, **{k: high[k] for k in keys}}]}
 
 
 def run_serving(seed, n_req=96, rate=400.0, slots=4):

@@ -125,10 +125,17 @@ struct Tc {
   static constexpr int SI = TE * NF + TE;            // int slot: nbr, face codes
   // pass 1 warp: 2 stages, face geometry, output records
   static constexpr int W1_T = 2 * ST1 + SFG + TE * TS;
-  // pass 2 warp: 2 stages, own and neighbour trace records (one buffer each), face geometry
-  static constexpr int STR = 2 * ST2, SNB = STR + TE * TS, SFGO = SNB + TE * TS, W2_T = SFGO + SFG;
   static constexpr int W2_I = 3 * SI;
   static constexpr int CH = TR * (int)sizeof(T) / 16;  // 16-byte chunks per trace record
+};
+
+// Pass-2 warp area: NS element stages, own and neighbour trace records (one
+// buffer each), face geometry.
+template <typename T, int DIM, int P, int NS>
+struct W2 {
+  using X = Tc<T, DIM, P>;
+  static constexpr int STR = NS * X::ST2, SNB = STR + X::TE * X::TS, SFGO = SNB + X::TE * X::TS,
+                       T_ = SFGO + X::SFG;
 };
 
 template <typename T>
@@ -210,14 +217,15 @@ __device__ __forceinline__ void issue_ints(const ApplyArgs<T>& a, int* slot, int
 
 // Own and neighbour trace records of a tile whose connectivity has arrived
 // (records that are never read are not copied).
-template <typename T, int DIM, int P>
+template <typename T, int DIM, int P, int NS>
 __device__ __forceinline__ void issue_traces(const ApplyArgs<T>& a, const T* trace, T* w, const int* slot, int tile,
                                              int lane) {
   using X = Tc<T, DIM, P>;
+  using L = W2<T, DIM, P, NS>;
   constexpr int NF = X::NF, TE = X::TE, CH = X::CH, TR = X::TR, TS = X::TS, VPC = 16 / sizeof(T);
   const int e0 = tile * TE;
   const int ne = max(0, min(TE, a.K - e0));
-  copy_rows<T, 16, NF * TR, TS, TE>(w + X::STR, trace, (size_t)e0, ne, lane, false);
+  copy_rows<T, 16, NF * TR, TS, TE>(w + L::STR, trace, (size_t)e0, ne, lane, false);
   const int* nbr = slot;
   const int* code = slot + TE * NF;
   // one neighbour record (CH pieces) per lane and round
@@ -229,7 +237,7 @@ __device__ __forceinline__ void issue_traces(const ApplyArgs<T>& a, const T* tra
       const int nb = nbr[lf];
       if (el < ne && nb >= 0) {
         const int fr = (code[el] >> (8 * f)) & 3;
-        T* d = w + X::SNB + el * TS + f * TR;
+        T* d = w + L::SNB + el * TS + f * TR;
         const T* src = trace + ((size_t)nb * NF + fr) * TR;
 #pragma unroll
         for (int c = 0; c < CH; ++c) cp_async_n<16>(d + c * VPC, src + c * VPC, 16);
@@ -436,30 +444,34 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_trace_kernel(ApplyArgs<T> 
 }
 
 // ---------------------------------------------------------------- pass 2
-template <typename T, int DIM, int P, int WARPS>
+// NS = 2: the next tile's element data is fetched during the whole current tile
+// (double-buffered stage); NS = 1: after the current tile's fluxes, which frees
+// shared memory for more warps per SM.
+template <typename T, int DIM, int P, int WARPS, int NS>
 __global__ void __launch_bounds__(WARPS * 32, 1) sipg_apply_tc_kernel(ApplyArgs<T> a, const T* __restrict__ blob,
                                                                     const T* __restrict__ trace) {
   using X = Tc<T, DIM, P>;
+  using L = W2<T, DIM, P, NS>;
   using F = Frag<T>;
   constexpr int NP = X::NP, NFP = X::NFP, NF = X::NF, NT = X::NT, FT = X::FT, R = X::R, TE = X::TE, TR = X::TR,
                 KF = X::KF, TRP = X::TRP, XS = X::XS, TS = X::TS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* B = reinterpret_cast<T*>(smem_raw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  T* W = B + X::N2 + warp * X::W2_T;
-  int* ibase = reinterpret_cast<int*>(B + X::N2 + WARPS * X::W2_T);
+  T* W = B + X::N2 + warp * L::T_;
+  int* ibase = reinterpret_cast<int*>(B + X::N2 + WARPS * L::T_);
   int* I = ibase + warp * X::W2_I;
   int8_t* itab = reinterpret_cast<int8_t*>(ibase + WARPS * X::W2_I);
   const int8_t* fmask = itab;
   const int8_t* perm = itab + NF * NFP;
-  const T* str = W + X::STR;
-  const T* snb = W + X::SNB;
-  T* sfg = W + X::SFGO;
+  const T* str = W + L::STR;
+  const T* snb = W + L::SNB;
+  T* sfg = W + L::SFGO;
   const int ntiles = (a.K + TE - 1) / TE;
   const int stride = gridDim.x * WARPS;
   int tile = blockIdx.x * WARPS + warp;
   pdl_trigger();
-  for (int i = lane; i < X::W2_T; i += 32) W[i] = T(0);  // row padding stays zero
+  for (int i = lane; i < L::T_; i += 32) W[i] = T(0);  // row padding stays zero
   __syncwarp();
   // prologue: constants and the connectivity of the first two tiles (set-up data),
   // then, once the preceding kernels are done, the first tile's element data
@@ -473,7 +485,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_apply_tc_kernel(ApplyArgs<
   __syncthreads();
   cp_wait_all();
   __syncwarp();
-  issue_traces<T, DIM, P>(a, trace, W, I, tile, lane);
+  issue_traces<T, DIM, P, NS>(a, trace, W, I, tile, lane);
   cp_commit();
   // this lane's face-node columns per block: face | node in face << 4 | volume nodes << 10, << 18
   int fbi[FT];
@@ -484,16 +496,18 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_apply_tc_kernel(ApplyArgs<
     if (NFP % 2 == 0 && k0 < KF) fbi[fb] = (k0 / NFP) | ((k0 % NFP) << 4) | (fmask[k0] << 10) | (fmask[k0 + 1] << 18);
   }
   for (int it = 0; tile < ntiles; ++it, tile += stride) {
-    const int sb = it & 1, slot = it % 3;
+    const int sb = NS == 2 ? (it & 1) : 0, slot = it % 3;
     T* st = W + sb * X::ST2;
     const int* ints = I + slot * X::SI;
     // element data of this tile and connectivity of the next one have arrived (the
     // tile's trace records, issued after the previous tile's fluxes, may still be in flight)
     cp_wait_but_one();
     __syncwarp();
-    issue_ints<T, DIM, P>(a, I + ((it + 2) % 3) * X::SI, tile + 2 * stride, lane);
-    issue_elem<T, DIM, P>(a, W + (sb ^ 1) * X::ST2, tile + stride, lane, true);
-    cp_commit();
+    if (NS == 2) {
+      issue_ints<T, DIM, P>(a, I + ((it + 2) % 3) * X::SI, tile + 2 * stride, lane);
+      issue_elem<T, DIM, P>(a, W + (sb ^ 1) * X::ST2, tile + stride, lane, true);
+      cp_commit();
+    }
 
     const int e0 = tile * TE;
     const int ne = min(TE, a.K - e0);
@@ -620,7 +634,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_apply_tc_kernel(ApplyArgs<
       }
     }
     // the tile's trace records have arrived
-    cp_wait_but_one();
+    if (NS == 2) cp_wait_but_one();
+    else cp_wait_all();
     __syncwarp();
     // face fluxes: y += Fu . EMAT^T ; Z_r += (c_r S) . EMAT^T
 #pragma unroll
@@ -722,10 +737,15 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_apply_tc_kernel(ApplyArgs<
         for (int r = 0; r < DIM; ++r) F::mma(z[r][nt], sv[r], b);
       }
     }
-    // the trace buffer is free: the next tile's records land during the rest of this
-    // tile and the next tile's volume products
+    // the trace buffer (and with NS = 1 the element stage) is free: the next tile's
+    // data lands during the rest of this tile and the next tile's volume products
     __syncwarp();
-    issue_traces<T, DIM, P>(a, trace, W, I + ((it + 1) % 3) * X::SI, tile + stride, lane);
+    if (NS == 1) {
+      issue_ints<T, DIM, P>(a, I + ((it + 2) % 3) * X::SI, tile + 2 * stride, lane);
+      issue_elem<T, DIM, P>(a, W, tile + stride, lane, true);
+      cp_commit();
+    }
+    issue_traces<T, DIM, P, NS>(a, trace, W, I + ((it + 1) % 3) * X::SI, tile + stride, lane);
     cp_commit();
     // y += sum_r Z_r . D_r
 #pragma unroll
@@ -779,10 +799,10 @@ constexpr size_t smem1(int w) {
   using X = Tc<T, DIM, P>;
   return (size_t)(X::N1 + w * X::W1_T) * sizeof(T) + X::NF * X::NFP;
 }
-template <typename T, int DIM, int P>
+template <typename T, int DIM, int P, int NS>
 constexpr size_t smem2(int w) {
   using X = Tc<T, DIM, P>;
-  return (size_t)(X::N2 + w * X::W2_T) * sizeof(T) + (size_t)w * X::W2_I * 4 + Cfg<DIM, P>::ITAB;
+  return (size_t)(X::N2 + w * W2<T, DIM, P, NS>::T_) * sizeof(T) + (size_t)w * X::W2_I * 4 + Cfg<DIM, P>::ITAB;
 }
 template <typename T, int DIM, int P>
 constexpr int warps1() {
@@ -791,50 +811,76 @@ constexpr int warps1() {
   return w;
 }
 // 0 when not even one warp tile fits next to the constants
-template <typename T, int DIM, int P>
+template <typename T, int DIM, int P, int NS>
 constexpr int warps2() {
   int w = 16;
-  while (w > 0 && smem2<T, DIM, P>(w) > (size_t)kSmemBudget) --w;
+  while (w > 0 && smem2<T, DIM, P, NS>(w) > (size_t)kSmemBudget) --w;
   return w;
 }
 
 inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
+template <typename T, int DIM, int P, int WARPS>
+cudaError_t launch_pass1(const ApplyArgs<T>& a, const T* blob, T* trace, int ntiles, int num_sms, cudaStream_t s) {
+  static_assert(WARPS >= 1 && smem1<T, DIM, P>(WARPS) <= (size_t)kSmemBudget, "pass-1 warps do not fit");
+  auto k = sipg_trace_kernel<T, DIM, P, WARPS>;
+  const size_t bytes = smem1<T, DIM, P>(WARPS);
+  cudaError_t err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (err != cudaSuccess) return err;
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, WARPS * 32, bytes);
+  const int grid = std::min((ntiles + WARPS - 1) / WARPS, num_sms * std::max(per_sm, 1));
+  if (grid > 0) {
+    pdl_launch(k, dim3(grid), dim3(WARPS * 32), bytes, s, a, blob, trace);
+    note_launch();
+  }
+  return cudaSuccess;
+}
+
+template <typename T, int DIM, int P, int NS, int WARPS>
+cudaError_t launch_pass2(const ApplyArgs<T>& a, const T* blob, const T* trace, int ntiles, int num_sms,
+                         cudaStream_t s) {
+  static_assert(WARPS >= 1 && smem2<T, DIM, P, NS>(WARPS) <= (size_t)kSmemBudget, "pass-2 warps do not fit");
+  auto k = sipg_apply_tc_kernel<T, DIM, P, WARPS, NS>;
+  const size_t bytes = smem2<T, DIM, P, NS>(WARPS);
+  cudaError_t err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (err != cudaSuccess) return err;
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, WARPS * 32, bytes);
+  const int grid = std::min((ntiles + WARPS - 1) / WARPS, num_sms * std::max(per_sm, 1));
+  if (grid > 0) {
+    pdl_launch(k, dim3(grid), dim3(WARPS * 32), bytes, s, a, blob, trace);
+    note_launch();
+  }
+  return cudaSuccess;
+}
+
+constexpr int cmin(int a, int b) { return a < b ? a : b; }
+
+// Launch shapes by the number of warp tiles: large meshes run as many warps per SM
+// as shared memory allows (pass 2 single-buffered once every warp has at least two
+// tiles); meshes with fewer tiles than a full-width wave over the SMs use narrow
+// CTAs (4 or 2 warps), so that every SM gets work.
 template <typename T, int DIM, int P>
 cudaError_t launch_tc_t(const ApplyArgs<T>& a, const T* blob, T* trace, int num_sms, cudaStream_t s) {
-  constexpr int WA = warps1<T, DIM, P>(), W2 = warps2<T, DIM, P>(), WB = W2 < 1 ? 1 : W2;
-  if (W2 < 1) return cudaErrorInvalidConfiguration;
+  constexpr int WA = warps1<T, DIM, P>(), W2D = warps2<T, DIM, P, 2>(), W2S = warps2<T, DIM, P, 1>();
+  if (W2D < 1) return cudaErrorInvalidConfiguration;
   using X = Tc<T, DIM, P>;
   // the kernels copy caller vectors in 16-byte pieces: other alignments take the CUDA-core kernel
   if (!aligned16(a.x) || !aligned16(a.y) || !aligned16(trace) || (a.factor && !aligned16(a.factor)))
     return launch_apply<T>(DIM, P, a, num_sms, s);
   const int ntiles = (a.K + X::TE - 1) / X::TE;
-  {
-    auto k = sipg_trace_kernel<T, DIM, P, WA>;
-    const size_t bytes = smem1<T, DIM, P>(WA);
-    cudaError_t err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    if (err != cudaSuccess) return err;
-    int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, WA * 32, bytes);
-    const int grid = std::min((ntiles + WA - 1) / WA, num_sms * std::max(per_sm, 1));
-    if (grid > 0) {
-      pdl_launch(k, dim3(grid), dim3(WA * 32), bytes, s, a, blob, (T*)trace);
-      note_launch();
-    }
-  }
-  {
-    auto k = sipg_apply_tc_kernel<T, DIM, P, WB>;
-    const size_t bytes = smem2<T, DIM, P>(WB);
-    cudaError_t err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    if (err != cudaSuccess) return err;
-    int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, WB * 32, bytes);
-    const int grid = std::min((ntiles + WB - 1) / WB, num_sms * std::max(per_sm, 1));
-    if (grid > 0) {
-      pdl_launch(k, dim3(grid), dim3(WB * 32), bytes, s, a, blob, (const T*)trace);
-      note_launch();
-    }
-  }
+  const long long wave = (long long)num_sms;
+  cudaError_t err;
+  if (ntiles >= wave * WA) err = launch_pass1<T, DIM, P, WA>(a, blob, trace, ntiles, num_sms, s);
+  else if (ntiles >= wave * 4) err = launch_pass1<T, DIM, P, cmin(4, WA)>(a, blob, trace, ntiles, num_sms, s);
+  else err = launch_pass1<T, DIM, P, cmin(2, WA)>(a, blob, trace, ntiles, num_sms, s);
+  if (err != cudaSuccess) return err;
+  if (W2S > W2D && ntiles >= 2 * wave * W2S) err = launch_pass2<T, DIM, P, 1, (W2S > W2D ? W2S : W2D)>(a, blob, trace, ntiles, num_sms, s);
+  else if (ntiles >= wave * W2D) err = launch_pass2<T, DIM, P, 2, W2D>(a, blob, trace, ntiles, num_sms, s);
+  else if (ntiles >= wave * 4) err = launch_pass2<T, DIM, P, 2, cmin(4, W2D)>(a, blob, trace, ntiles, num_sms, s);
+  else err = launch_pass2<T, DIM, P, 2, cmin(2, W2D)>(a, blob, trace, ntiles, num_sms, s);
+  if (err != cudaSuccess) return err;
   return cudaGetLastError();
 }
 
@@ -896,7 +942,7 @@ void build_tc_consts(int dim, int order, const RefElement& r, std::vector<double
 
 template <typename T>
 int tc_warps_for(int dim, int order) {
-  SIPG_DISPATCH_TC(dim, order, return warps2<T, D, P>());
+  SIPG_DISPATCH_TC(dim, order, return warps2<T, D, P, 2>());
   return 0;
 }
 
