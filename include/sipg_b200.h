@@ -182,7 +182,8 @@ typedef struct {
                                 stopping test on the device ends it (host reads once per 64
                                 iterations; falls back to 1 where unsupported); 1: each outer
                                 iteration after the first is replayed from a captured CUDA graph;
-                                0: kernels are launched one by one (same arithmetic as 1) */
+                                0: kernels are launched one by one. The three run the same
+                                kernels: identical iterates. */
   int assembled_max_order;   /* p-multigrid levels below the finest with this order or lower apply
                                 their operator as stored element blocks (assembled once from the
                                 matrix-free apply, scalar operators, orders <= 2); 0: all matrix-free */
@@ -252,6 +253,8 @@ typedef struct {
   double queue_ms;            /* submit -> start */
   double run_ms;              /* start -> done (includes a solver set-up on first use) */
   double total_ms;            /* submit -> done */
+  char error[160];            /* why the request failed (status other than OK, NOT_CONVERGED,
+                                 BREAKDOWN, CANCELLED); empty otherwise */
 } sipg_request_result;
 
 int sipg_server_create(const sipg_server_opts *o, sipg_server **out);

@@ -14,6 +14,7 @@
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -177,13 +178,17 @@ struct sipg_server {
         st = sipg_solver_solve_host(slot->solver, req->b.data(), req->x, &info);
         solver_set_cancel(slot->solver, nullptr);
       }
+      const bool hard = st != SIPG_OK && st != SIPG_NOT_CONVERGED && st != SIPG_BREAKDOWN && st != SIPG_CANCELLED;
+      if (hard) std::snprintf(req->res.error, sizeof(req->res.error), "%s", sipg_last_error());
       lk.lock();
       --running;
       req->res.info = info;
       finish(*req, st);
       slot->busy = false;
       slot->last_use = ++tick;
-      if (!slot->solver) evict(slot);
+      // a solver that failed with an error may hold inconsistent state: the next
+      // request of its kind gets a new one
+      if (!slot->solver || hard) evict(slot);
       busy_ops.erase(req->op);
       cv_done.notify_all();
       cv_work.notify_all();

@@ -173,6 +173,12 @@ double host_csr_lmax(const Csr& A, const std::vector<double>& dinv, int iters) {
 
 }  // namespace
 
+// One capture at a time in the process (solvers of a serving loop capture from
+// several threads), and no capture while another thread runs a solver's first
+// solve or set-up: those launch kernels for the first time, and loading a kernel
+// module while another thread captures a stream can fail or invalidate the capture.
+static std::recursive_mutex g_graph_mu;
+
 // Device-resident outer loop: beta numerator of the flexible CG from two dots
 // (r.z_new - r.z_old) and the per-iteration stopping test, which ends the
 // conditional while-node of the loop graph.
@@ -203,7 +209,7 @@ struct sipg_solver {
   sipg_solver_opts o{};
   size_t n = 0;
   cudaStream_t stream = nullptr;
-  DevBuf r, z, zold, p, Ap, bw, xw, r32, z32;
+  DevBuf r, z, p, Ap, bw, xw, r32, z32;
   DevBuf scal, partial, counter;
   RedWork rw;
   PinnedScalars hs;
@@ -228,6 +234,7 @@ struct sipg_solver {
   cudaGraphExec_t gloop = nullptr;
   unsigned long long gloop_nodes = 0;
   bool gloop_broken = false;
+  bool warm = false;  // a solve has run since the last set-up: its kernels are loaded
   PinnedScalars hw;  // host staging of scalars written before a loop launch
 
   double* S() const { return scal.as<double>(); }
@@ -271,6 +278,7 @@ struct sipg_solver {
   }
 
   void setup();
+  void setup_body();
   void setup_pmg();
   template <typename T> void vcycle(int l);
   template <typename T> void chebyshev(Level& L, bool want_res, bool first);
@@ -507,14 +515,30 @@ void sipg_solver::setup_amg() {
   cinv32.upload(c32.data(), c32.size() * sizeof(float));
 }
 
+// A set-up that fails part-way leaves no half-built levels behind: the next
+// solve builds them again from the start.
 void sipg_solver::setup() {
+  std::lock_guard<std::recursive_mutex> first_use(g_graph_mu);
+  warm = false;
+  try {
+    setup_body();
+  } catch (...) {
+    lv.clear();
+    al.clear();
+    use_amg = false;
+    dirty = true;
+    throw;
+  }
+}
+
+void sipg_solver::setup_body() {
   drop_graphs();
   graph_broken = false;
   gloop_broken = false;
   n = (size_t)op->ncomp * op->mesh->K * op->Np;
   if (!r.p) {
     size_t b = n * sizeof(double);
-    r = DevBuf(b); z = DevBuf(b); zold = DevBuf(b); p = DevBuf(b); Ap = DevBuf(b);
+    r = DevBuf(b); z = DevBuf(b); p = DevBuf(b); Ap = DevBuf(b);
     scal = DevBuf(S_COUNT * sizeof(double));
     partial = DevBuf(kRedBlocks * 4 * sizeof(double));
     counter = DevBuf(sizeof(unsigned));
@@ -752,14 +776,10 @@ void sipg_solver::precondition(const double* rin, double* zout) {
 
 // Capture one outer iteration into gx[par]; on any failure the solver keeps
 // launching kernels one by one.
-// One capture at a time in the process (solvers of a serving loop capture from
-// several threads).
-static std::mutex g_capture_mu;
-
 template <typename F>
 void sipg_solver::capture_iteration(int par, F&& body) {
-  std::lock_guard<std::mutex> capture_lock(g_capture_mu);
-  const unsigned long long c0 = launch_count();
+  std::lock_guard<std::recursive_mutex> capture_lock(g_graph_mu);
+  unsigned long long nodes = 0;
   cudaGraph_t g = nullptr;
   if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
     cudaGetLastError();
@@ -767,14 +787,14 @@ void sipg_solver::capture_iteration(int par, F&& body) {
     return;
   }
   bool ok = true;
+  record_launches(&nodes);  // recorded, not launched
   try {
     body();
   } catch (...) {
     ok = false;
   }
+  record_launches(nullptr);
   cudaError_t e = cudaStreamEndCapture(stream, &g);
-  const unsigned long long c1 = launch_count();
-  unnote_launch(c1 - c0);  // recorded, not launched
   if (!ok || e != cudaSuccess || !g) {
     if (g) cudaGraphDestroy(g);
     cudaGetLastError();
@@ -789,15 +809,15 @@ void sipg_solver::capture_iteration(int par, F&& body) {
     graph_broken = true;
     return;
   }
-  gnodes[par] = c1 - c0;
+  gnodes[par] = nodes;
 }
 
 // Build gloop: a conditional while-node whose body is one iteration followed by
 // the stopping test. On any failure the solver falls back to per-iteration graphs.
 template <typename F>
 void sipg_solver::capture_loop(F&& body) {
-  std::lock_guard<std::mutex> capture_lock(g_capture_mu);
-  const unsigned long long c0 = launch_count();
+  std::lock_guard<std::recursive_mutex> capture_lock(g_graph_mu);
+  unsigned long long nodes = 0;
   cudaGraph_t g = nullptr;
   bool ok = cudaGraphCreate(&g, 0) == cudaSuccess;
   cudaGraphConditionalHandle h{};
@@ -815,6 +835,7 @@ void sipg_solver::capture_loop(F&& body) {
                                              cudaStreamCaptureModeRelaxed) == cudaSuccess;
   if (ok) {
     bool body_ok = true;
+    record_launches(&nodes);  // recorded, not launched
     try {
       body();
       k_loop_check<<<1, 1, 0, stream>>>(S(), h, o.max_iter);
@@ -822,11 +843,10 @@ void sipg_solver::capture_loop(F&& body) {
     } catch (...) {
       body_ok = false;
     }
+    record_launches(nullptr);
     cudaGraph_t out = nullptr;
     ok = cudaStreamEndCapture(stream, &out) == cudaSuccess && body_ok;
   }
-  const unsigned long long c1 = launch_count();
-  unnote_launch(c1 - c0);
   if (ok) ok = cudaGraphInstantiate(&gloop, g, 0) == cudaSuccess;
   if (g) cudaGraphDestroy(g);
   if (!ok) {
@@ -836,10 +856,12 @@ void sipg_solver::capture_loop(F&& body) {
     gloop_broken = true;
     return;
   }
-  gloop_nodes = c1 - c0;
+  gloop_nodes = nodes;
 }
 
 int sipg_solver::solve(const double* b, double* x_user, sipg_solve_info* info) {
+  std::unique_lock<std::recursive_mutex> first_use(g_graph_mu, std::defer_lock);
+  if (!warm || dirty) first_use.lock();
   auto t0 = std::chrono::steady_clock::now();
   if (dirty) setup();
   auto t1 = std::chrono::steady_clock::now();
@@ -854,7 +876,6 @@ int sipg_solver::solve(const double* b, double* x_user, sipg_solve_info* info) {
   if (graphs) vcopy<double>(x, x_user, n, stream);
   double* R = r.as<double>();
   double* Z = z.as<double>();
-  double* ZO = zold.as<double>();
   double* Pv = p.as<double>();
   double* AP = Ap.as<double>();
   // r = b - A x (calc_res_explicit, viscous_solver.cpp:329-343)
@@ -901,63 +922,57 @@ int sipg_solver::solve(const double* b, double* x_user, sipg_solve_info* info) {
       if (cancel && cancel->load(std::memory_order_relaxed)) { status = SIPG_CANCELLED; break; }
     }
   } else {
-    // flexible PCG (viscous_solver.cpp:177-301)
+    // flexible PCG (viscous_solver.cpp:177-301). One iteration on fixed buffers: z is
+    // overwritten in place and beta = r.z_new - r.z_old comes from two dots.
     if (status == SIPG_OK) precondition(R, Z);
     vcopy<double>(Pv, Z, n, stream);
-    if (graphs && o.graphs >= 2 && !gloop_broken) {
-      // Device-resident loop: one iteration on fixed buffers (z overwritten in place,
-      // beta = r.z_new - r.z_old from two dots), replayed by a conditional while-node
-      // until the stopping test in k_loop_check ends it; the host reads the scalars
-      // once per launch of at most kLoopChunk iterations.
-      constexpr int kLoopChunk = 64;
-      dot(R, Z, S_RZ);
-      // mixed p-multigrid: the nullspace projections, the FP32 / FP64 conversions and
-      // the dots ride on the vector passes next to them
-      const bool fused = kind == SIPG_SOLVER_PMULTIGRID && o.precision == SIPG_FP32;
-      const int mean_slot = o.nullspace ? (int)S_SUM : -1;
-      auto body = [&] {
-        op->apply<double>(Pv, AP, stream);
-        dot(Pv, AP, S_PAP);  // cg3_alpha_pre
-        if (fused) {
-          // update_ans + update_res, projection, r . r, r . z_old, r to FP32
-          if (o.nullspace) cg_update_xr_sum(x, R, Pv, AP, n, S(), S_RZ, S_PAP, S() + S_SUM, S_TMP - S_SUM, rw, stream);
-          else cg_update_xr(x, R, Pv, AP, n, S(), S_RZ, S_PAP, S() + S_TMP, rw, stream);
-          resid_prep(R, lv[0].rhs.as<float>(), Z, n, S(), mean_slot, S() + S_RR, S_RZO - S_RR, rw, stream);
-          vcycle<float>(0);
-          // z to FP64, projection, r . z_new
-          if (o.nullspace) to_f64_sum(Z, lv[0].z.as<float>(), n, S() + S_SUM, rw, stream);
-          finish_z_dot(Z, o.nullspace ? nullptr : lv[0].z.as<float>(), R, n, S(), mean_slot, S() + S_RZN, rw, stream);
-        } else {
-          cg_update_xr(x, R, Pv, AP, n, S(), S_RZ, S_PAP, S() + S_RR, rw, stream);  // update_ans + update_res
-          if (o.nullspace) {
-            vsum<double>(R, n, S() + S_SUM, rw, stream);
-            sub_mean<double>(R, n, S(), S_SUM, stream);
-            dot(R, R, S_RR);
-          }
-          dot(R, Z, S_RZO);
-          precondition(R, Z);
-          dot(R, Z, S_RZN);
+    dot(R, Z, S_RZ);
+    // mixed p-multigrid: the nullspace projections, the FP32 / FP64 conversions and
+    // the dots ride on the vector passes next to them
+    const bool fused = kind == SIPG_SOLVER_PMULTIGRID && o.precision == SIPG_FP32;
+    const int mean_slot = o.nullspace ? (int)S_SUM : -1;
+    auto body = [&] {
+      op->apply<double>(Pv, AP, stream);
+      dot(Pv, AP, S_PAP);  // cg3_alpha_pre
+      if (fused) {
+        // update_ans + update_res, projection, r . r, r . z_old, r to FP32
+        if (o.nullspace) cg_update_xr_sum(x, R, Pv, AP, n, S(), S_RZ, S_PAP, S() + S_SUM, S_TMP - S_SUM, rw, stream);
+        else cg_update_xr(x, R, Pv, AP, n, S(), S_RZ, S_PAP, S() + S_TMP, rw, stream);
+        resid_prep(R, lv[0].rhs.as<float>(), Z, n, S(), mean_slot, S() + S_RR, S_RZO - S_RR, rw, stream);
+        vcycle<float>(0);
+        // z to FP64, projection, r . z_new
+        if (o.nullspace) to_f64_sum(Z, lv[0].z.as<float>(), n, S() + S_SUM, rw, stream);
+        finish_z_dot(Z, o.nullspace ? nullptr : lv[0].z.as<float>(), R, n, S(), mean_slot, S() + S_RZN, rw, stream);
+      } else {
+        cg_update_xr(x, R, Pv, AP, n, S(), S_RZ, S_PAP, S() + S_RR, rw, stream);  // update_ans + update_res
+        if (o.nullspace) {
+          vsum<double>(R, n, S() + S_SUM, rw, stream);
+          sub_mean<double>(R, n, S(), S_SUM, stream);
+          dot(R, R, S_RR);
         }
-        k_beta_flex<<<1, 1, 0, stream>>>(S());  // cg3_compute_beta_pre_flex
-        note_launch();
-        update_p<double>(Pv, Z, n, S(), S_BETA, S_RZP, stream);
-      };
-      auto after = [&](int it_now) {
-        iter = it_now;
-        const double pap = hs.h[S_PAP];
-        res = std::sqrt(hs.h[S_RR]);
-        if (!(pap > 0.0) || !std::isfinite(res)) status = SIPG_BREAKDOWN;
-        else if (cancel && cancel->load(std::memory_order_relaxed)) status = SIPG_CANCELLED;
-      };
-      while (status == SIPG_OK && res > tol && iter < o.max_iter) {
-        // the first iteration runs eagerly (lazy buffers are allocated there)
-        if (iter >= 1 && !gloop && !gloop_broken) capture_loop(body);
-        if (iter == 0 || !gloop) {
-          body();
-          read_scalars();
-          after(iter + 1);
-          continue;
-        }
+        dot(R, Z, S_RZO);
+        precondition(R, Z);
+        dot(R, Z, S_RZN);
+      }
+      k_beta_flex<<<1, 1, 0, stream>>>(S());  // cg3_compute_beta_pre_flex
+      note_launch();
+      update_p<double>(Pv, Z, n, S(), S_BETA, S_RZP, stream);
+    };
+    auto after = [&](int it_now) {
+      iter = it_now;
+      const double pap = hs.h[S_PAP];
+      res = std::sqrt(hs.h[S_RR]);
+      if (!(pap > 0.0) || !std::isfinite(res)) status = SIPG_BREAKDOWN;
+      else if (cancel && cancel->load(std::memory_order_relaxed)) status = SIPG_CANCELLED;
+    };
+    // graphs = 2: the iterations after the first run inside gloop, whose while-node
+    // repeats the body until k_loop_check ends it; the host reads the scalars once
+    // per launch of at most kLoopChunk iterations. graphs = 1: one graph launch per
+    // iteration. The first iteration runs eagerly (lazy buffers are allocated there).
+    constexpr int kLoopChunk = 64;
+    while (status == SIPG_OK && res > tol && iter < o.max_iter) {
+      if (graphs && iter >= 1 && o.graphs >= 2 && !gloop && !gloop_broken) capture_loop(body);
+      if (graphs && iter >= 1 && gloop) {
         hw.h[S_ITER] = (double)iter;
         hw.h[S_STATUS] = 0.0;
         hw.h[S_TOL] = tol;
@@ -968,44 +983,17 @@ int sipg_solver::solve(const double* b, double* x_user, sipg_solve_info* info) {
         const int done = (int)hs.h[S_ITER];
         note_launch((unsigned)((done - iter) * gloop_nodes));
         after(done);
+        continue;
       }
-    } else {
-      // one iteration; zn receives the new preconditioned residual, zo holds the previous one
-      auto iteration = [&](double* zn, double* zo) {
-        op->apply<double>(Pv, AP, stream);
-        const double* a[2] = {R, Pv};
-        const double* bb[2] = {zo, AP};
-        multi_dot<double>(a, bb, 2, n, S() + S_RZ, 1, rw, stream);  // cg3_alpha_pre
-        cg_update_xr(x, R, Pv, AP, n, S(), S_RZ, S_PAP, S() + S_RR, rw, stream);  // update_ans + update_res
-        if (o.nullspace) {
-          vsum<double>(R, n, S() + S_SUM, rw, stream);
-          sub_mean<double>(R, n, S(), S_SUM, stream);
-          dot(R, R, S_RR);
-        }
-        precondition(R, zn);
-        dot_diff(R, zn, zo, n, S() + S_BETA, rw, stream);  // cg3_compute_beta_pre_flex
-        update_p<double>(Pv, zn, n, S(), S_BETA, S_RZ, stream);
-      };
-      while (status == SIPG_OK && res > tol && iter < o.max_iter) {
-        double* zn = ZO;
-        double* zo = Z;
-        const int par = iter & 1;  // Z = z, ZO = z_old at iteration 0
-        // the first iteration runs eagerly (lazy buffers are allocated there), the rest replay
-        if (graphs && iter >= 1 && !graph_broken && !gx[par]) capture_iteration(par, [&] { iteration(zn, zo); });
-        if (graphs && iter >= 1 && gx[par]) {
-          SIPG_CUDA(cudaGraphLaunch(gx[par], stream));
-          note_launch((unsigned)gnodes[par]);
-        } else {
-          iteration(zn, zo);
-        }
-        std::swap(Z, ZO);
-        ++iter;
-        read_scalars();
-        const double pap = hs.h[S_PAP];
-        res = std::sqrt(hs.h[S_RR]);
-        if (!(pap > 0.0) || !std::isfinite(res)) { status = SIPG_BREAKDOWN; break; }
-        if (cancel && cancel->load(std::memory_order_relaxed)) { status = SIPG_CANCELLED; break; }
+      if (graphs && iter >= 1 && !gx[0] && !graph_broken) capture_iteration(0, body);
+      if (graphs && iter >= 1 && gx[0]) {
+        SIPG_CUDA(cudaGraphLaunch(gx[0], stream));
+        note_launch((unsigned)gnodes[0]);
+      } else {
+        body();
       }
+      read_scalars();
+      after(iter + 1);
     }
   }
   if (status == SIPG_OK && res > tol) status = SIPG_NOT_CONVERGED;
@@ -1031,6 +1019,7 @@ int sipg_solver::solve(const double* b, double* x_user, sipg_solve_info* info) {
     info->solve_ms = ms;
     info->status = status;
   }
+  warm = true;
   return status;
 }
 

@@ -10,8 +10,12 @@
 namespace sipg {
 
 static std::atomic<unsigned long long> g_launches{0};
-void note_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
-void unnote_launch(unsigned long long n) { g_launches.fetch_sub(n, std::memory_order_relaxed); }
+static thread_local unsigned long long* t_recorded = nullptr;
+void note_launch(unsigned n) {
+  if (t_recorded) *t_recorded += n;
+  else g_launches.fetch_add(n, std::memory_order_relaxed);
+}
+void record_launches(unsigned long long* counter) { t_recorded = counter; }
 unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 namespace {
 

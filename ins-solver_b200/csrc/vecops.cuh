@@ -13,7 +13,9 @@ namespace sipg {
 
 // Count of kernel launches issued by this library (diagnostics).
 void note_launch(unsigned n = 1);
-void unnote_launch(unsigned long long n);  // launches recorded during a graph capture
+// While counter is set, this thread's note_launch calls add to it instead (kernels
+// recorded into a graph during a capture, not launched); null restores counting.
+void record_launches(unsigned long long* counter);
 unsigned long long launch_count();
 
 // Device scalar slots used by the solvers.

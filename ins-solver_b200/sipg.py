@@ -350,7 +350,7 @@ class ServerOpts(C.Structure):
 
 class RequestResult(C.Structure):
     _fields_ = [("status", C.c_int), ("info", SolveInfo), ("queue_ms", C.c_double), ("run_ms", C.c_double),
-                ("total_ms", C.c_double)]
+                ("total_ms", C.c_double), ("error", C.c_char * 160)]
 
 
 class Server:

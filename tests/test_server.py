@@ -62,7 +62,7 @@ def test_results_are_the_same_alone_and_in_the_mix():
             ids.append((i, srv.submit(op, kind, o, b)))
     for i, rid in ids:
         x, res = srv.wait(rid)
-        assert res.status == sipg.SIPG_OK
+        assert res.status == sipg.SIPG_OK, (res.status, res.error)
         assert res.total_ms >= res.run_ms >= 0.0
         assert np.array_equal(x, alone[i]), (i, np.abs(x - alone[i]).max())
     st = srv.stats()

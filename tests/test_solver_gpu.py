@@ -187,9 +187,9 @@ def test_graph_replayed_iterations_match_eager_launches(precision):
 @pytest.mark.parametrize("precision", [sipg.FP64, sipg.FP32], ids=["fp64", "mixed"])
 def test_device_resident_loop_matches_host_loop(precision):
     """The outer loop run on the device (conditional while-node, stopping test on
-    the device) converges like the host-driven loop: same iteration count within
-    one, the same solution to the solve tolerance, reproducible run to run, and a
-    coefficient change after the capture is picked up."""
+    the device) runs the host-driven loop's kernels: the same iterations and the
+    same iterates, reproducible run to run, and a coefficient change after the
+    capture is picked up."""
     c = W.poisson3d_two_phase(5, order=3, n_modes=64, pin=False)
     out = {}
     for graphs in (1, 2):
@@ -209,8 +209,8 @@ def test_device_resident_loop_matches_host_loop(precision):
         assert rel_err(x3, 0.5 * x1) < 1e-8
         assert i1.true_rel_res < 1e-9
     h, d = out[1], out[2]
-    assert abs(h[1].iters - d[1].iters) <= 1 and abs(h[3].iters - d[3].iters) <= 1
-    assert rel_err(d[0], h[0]) < 1e-8 and rel_err(d[2], h[2]) < 1e-8
+    assert h[1].iters == d[1].iters and h[3].iters == d[3].iters
+    assert np.array_equal(d[0], h[0]) and np.array_equal(d[2], h[2])
 
 
 def test_device_resident_loop_chunks_and_iteration_limit():
@@ -230,8 +230,8 @@ def test_device_resident_loop_chunks_and_iteration_limit():
         o.max_iter = 77
         _, lim = sipg.Solver(op, sipg.SOLVER_JACOBI, o).solve_host(c["rhs"])
         assert lim.status == sipg.SIPG_NOT_CONVERGED and lim.iters == 77
-    assert abs(res[1][1].iters - res[2][1].iters) <= 2
-    assert rel_err(res[2][0], res[1][0]) < 1e-6
+    assert res[1][1].iters == res[2][1].iters
+    assert np.array_equal(res[2][0], res[1][0])
 
 
 @pytest.mark.parametrize("precision", [sipg.FP64, sipg.FP32], ids=["fp64", "mixed"])
