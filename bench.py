@@ -186,7 +186,7 @@ def apply_bytes_per_elem(Np, ts, factor, ngeof=10, nf=4, gface=5):
 # DRAM traffic of one FP32 p=3 apply (trace + apply kernels) at the headline
 # size, ncu capture with flushed caches (dram__bytes_read.sum + dram__bytes_write.sum
 # of both launches): profiles/apply_tc_fp32_p3_24cube.txt
-APPLY_P3_FP32_TRAFFIC = 16.628e6 + 0.030e6 + 46.211e6 + 0.205e6
+APPLY_P3_FP32_TRAFFIC = 16.627e6 + 0.006e6 + 46.210e6 + 0.449e6
 
 
 def max_over_ranks(x, world, device):
