@@ -2,6 +2,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/sipg_b200.h"
@@ -44,7 +46,8 @@ __global__ void k_d2f(float* dst, const double* src, size_t n) {
 
 // One thread per (row r, element e), e fastest: block reads are coalesced and
 // there are Np threads per element row to hide the gather latency.
-template <typename T, int NP, int NF>
+// V4: x rows read as one 16-byte load (FP32, Np = 4, x 16-byte aligned).
+template <typename T, int NP, int NF, bool V4 = false>
 __global__ void __launch_bounds__(256) k_bsr(int K, const T* __restrict__ v, const int* __restrict__ nbr,
                                              const T* __restrict__ x, T* y, T alpha, T beta, const T* c) {
   pdl_enter();
@@ -64,8 +67,16 @@ __global__ void __launch_bounds__(256) k_bsr(int K, const T* __restrict__ v, con
       if (k < 0) continue;
       const T* vs = v + ((size_t)(s * NP + r) * NP) * K_ + e;
       const T* xk = x + (size_t)k * NP;
+      T xv[NP];
+      if constexpr (V4 && std::is_same<T, float>::value && NP == 4) {
+        const float4 q = *reinterpret_cast<const float4*>(xk);
+        xv[0] = q.x; xv[1] = q.y; xv[2] = q.z; xv[3] = q.w;
+      } else {
 #pragma unroll
-      for (int c = 0; c < NP; ++c) acc += vs[(size_t)c * K_] * xk[c];
+        for (int c = 0; c < NP; ++c) xv[c] = xk[c];
+      }
+#pragma unroll
+      for (int c = 0; c < NP; ++c) acc += vs[(size_t)c * K_] * xv[c];
     }
     T o = alpha * acc;
     if (beta != T(0)) o += beta * c[(size_t)e * NP + r];
@@ -154,7 +165,10 @@ void bsr_apply(const BsrOp& B, const T* x, T* y, T alpha, T beta, cudaStream_t s
   const T* v = std::is_same<T, double>::value ? (const T*)B.v64.p : (const T*)B.v32.p;
   if (!v) throw Error(SIPG_INVALID_ARG, "assembled blocks missing for this precision");
   const int g = (int)std::max<size_t>(1, std::min<size_t>(((size_t)B.K * B.Np + 255) / 256, 148 * 32));
-  if (B.dim == 3 && B.Np == 4) pdl_launch(k_bsr<T, 4, 4>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta, c);
+  const bool v4 = std::is_same<T, float>::value && (reinterpret_cast<uintptr_t>(x) & 15) == 0;
+  if (B.dim == 3 && B.Np == 4 && v4)
+    pdl_launch(k_bsr<T, 4, 4, true>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta, c);
+  else if (B.dim == 3 && B.Np == 4) pdl_launch(k_bsr<T, 4, 4>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta, c);
   else if (B.dim == 3 && B.Np == 10) pdl_launch(k_bsr<T, 10, 4>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta, c);
   else if (B.dim == 2 && B.Np == 3) pdl_launch(k_bsr<T, 3, 3>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta, c);
   else if (B.dim == 2 && B.Np == 6) pdl_launch(k_bsr<T, 6, 3>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta, c);

@@ -56,7 +56,8 @@ struct Level {
   // work vectors in the V-cycle precision
   DevBuf rhs, z, res, d;
   DevBuf cp, cs, cAp;            // coarse CG
-  DevBuf bc64, bc32;             // inverse diagonal blocks, column-major (block-Jacobi smoothing; bc32 in bf16)
+  DevBuf bc64, bc32;             // inverse diagonal blocks (block-Jacobi smoothing; bc32 in bf16)
+  bool bsym = false;             // bc* packed symmetric (large meshes) or full column-major blocks
   std::unique_ptr<BsrOp> bsr;    // assembled element blocks (low orders), else matrix-free
   int cheb = 4, pre = 1, post = 1;  // Chebyshev degree, smoothing sweeps before / after the coarse correction
   // y = alpha A x + beta c (c = y when null)
@@ -178,6 +179,10 @@ double host_csr_lmax(const Csr& A, const std::vector<double>& dinv, int iters) {
 // solve or set-up: those launch kernels for the first time, and loading a kernel
 // module while another thread captures a stream can fail or invalidate the capture.
 static std::recursive_mutex g_graph_mu;
+
+// Levels with at least this many element blocks store them packed symmetric
+// (one thread per block fills the GPU from here on).
+constexpr int kSymMinBlocks = 148 * 128;
 
 // Device-resident outer loop: beta numerator of the flexible CG from two dots
 // (r.z_new - r.z_old) and the per-iteration stopping test, which ends the
@@ -420,13 +425,23 @@ void sipg_solver::setup_pmg() {
     L.bc64 = DevBuf();
     L.bc32 = DevBuf();
     if (o.smoother == 1) {
-      // element-block Jacobi: inverse diagonal blocks, column-major in the level precision
+      // element-block Jacobi: inverse diagonal blocks in the level precision (BF16 for
+      // the FP32 V-cycle: the smoother tolerates 8 mantissa bits). Large meshes store
+      // them as packed symmetric triangles (one thread per block, half the bytes);
+      // small ones as full column-major blocks (ten threads per block at p = 3).
       const int nb = (int)(L.n / L.Np);
+      L.bsym = block_sym_supported(L.Np) && nb >= kSymMinBlocks;
       DevBuf rows((size_t)nb * L.Np * L.Np * sizeof(double));
       SIPG_CUDA(launch_blocks(dim, L.order, L.op->block_args(BLOCK_INVERSE, 0, rows.as<double>(), true), stream));
-      if (f32) {  // bfloat16 blocks: the smoother tolerates 8 mantissa bits, and they stay in L2
+      if (f32 && L.bsym) {
+        L.bc32 = DevBuf(block_sym_values<__nv_bfloat16>(nb, L.Np) * sizeof(__nv_bfloat16));
+        block_pack_sym<__nv_bfloat16>(L.bc32.as<__nv_bfloat16>(), rows.as<double>(), nb, L.Np, stream);
+      } else if (f32) {
         L.bc32 = DevBuf((size_t)nb * L.Np * L.Np * sizeof(__nv_bfloat16));
         block_transpose<__nv_bfloat16>(L.bc32.as<__nv_bfloat16>(), rows.as<double>(), nb, L.Np, stream);
+      } else if (L.bsym) {
+        L.bc64 = DevBuf(block_sym_values<double>(nb, L.Np) * sizeof(double));
+        block_pack_sym<double>(L.bc64.as<double>(), rows.as<double>(), nb, L.Np, stream);
       } else {
         L.bc64 = DevBuf((size_t)nb * L.Np * L.Np * sizeof(double));
         block_transpose<double>(L.bc64.as<double>(), rows.as<double>(), nb, L.Np, stream);
@@ -596,11 +611,18 @@ void sipg_solver::chebyshev(Level& L, bool want_res, bool first) {
     }
     const bool from_rhs = first && it == 0;
     const T* rin = from_rhs ? L.rhs.as<T>() : res;
-    if (L.bc32.p && std::is_same<T, float>::value) {
+    const int nb = (int)(L.n / L.Np);
+    if (L.bc32.p && std::is_same<T, float>::value && L.bsym) {
+      cheb_step_sym<float, __nv_bfloat16>((float*)d, (float*)z, (const float*)rin, L.bc32.as<__nv_bfloat16>(),
+                                          (float)c1, (float)c2, nb, L.Np, stream, from_rhs);
+    } else if (L.bc32.p && std::is_same<T, float>::value) {
       cheb_step_block<float, __nv_bfloat16>((float*)d, (float*)z, (const float*)rin, L.bc32.as<__nv_bfloat16>(),
-                                            (float)c1, (float)c2, (int)(L.n / L.Np), L.Np, stream, from_rhs);
+                                            (float)c1, (float)c2, nb, L.Np, stream, from_rhs);
+    } else if (L.bc64.p && std::is_same<T, double>::value && L.bsym) {
+      cheb_step_sym<double, double>((double*)d, (double*)z, (const double*)rin, L.bc64.as<double>(), (double)c1,
+                                    (double)c2, nb, L.Np, stream, from_rhs);
     } else if (L.bc64.p) {
-      cheb_step_block<T, T>(d, z, rin, (const T*)L.bc64.p, (T)c1, (T)c2, (int)(L.n / L.Np), L.Np, stream, from_rhs);
+      cheb_step_block<T, T>(d, z, rin, (const T*)L.bc64.p, (T)c1, (T)c2, nb, L.Np, stream, from_rhs);
     } else {
       cheb_step<T>(d, z, rin, dinv, (T)c1, (T)c2, L.n, stream, from_rhs);
     }

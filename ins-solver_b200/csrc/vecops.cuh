@@ -99,12 +99,27 @@ void jacobi(T* z, const T* r, const T* dinv, size_t n, cudaStream_t s);
 // Chebyshev step: d = c1 * d + c2 * dinv * res ; z += d  (first: z = d; c1 == 0 reads no d)
 template <typename T>
 void cheb_step(T* d, T* z, const T* res, const T* dinv, T c1, T c2, size_t n, cudaStream_t s, bool first = false);
-// d <- c1 d + c2 Bc res, z += d with column-major inverse diagonal blocks Bc (nb blocks of Np x Np)
+// Same step with full column-major blocks Bc (nb blocks of Np x Np): ten threads per
+// block at p = 3, for meshes too small to fill the GPU with one thread per block.
 template <typename T, typename TB>
 void cheb_step_block(T* d, T* z, const T* res, const TB* Bc, T c1, T c2, int nb, int Np, cudaStream_t s,
                      bool first = false);
 template <typename T>
 void block_transpose(T* dst, const double* src, int nb, int Np, cudaStream_t s);
+// Element-block Jacobi Chebyshev step: d <- c1 d + c2 B res, z += d (first: z = d;
+// c1 == 0 reads no d), with the inverse diagonal blocks B stored as packed symmetric
+// triangles (block_pack_sym) for Np in {3, 4, 6, 10, 15, 20, 35}.
+bool block_sym_supported(int Np);
+template <typename T, typename TB>
+void cheb_step_sym(T* d, T* z, const T* res, const TB* P, T c1, T c2, int nb, int Np, cudaStream_t s,
+                   bool first = false);
+// Row-major FP64 blocks (nb x Np x Np) -> packed symmetric triangles (mean of the two),
+// in 16-byte chunks of 16 / sizeof(TB) values: chunk k of block b at P[(k * nb + b) * CH].
+template <typename TB>
+void block_pack_sym(TB* P, const double* B, int nb, int Np, cudaStream_t s);
+// Values (padding included) that block_pack_sym writes.
+template <typename TB>
+size_t block_sym_values(int nb, int Np);
 
 // Element-block matvec: y_e = B_e x_e (B: nb x Np x Np row-major, nb blocks)
 template <typename T>
