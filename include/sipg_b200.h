@@ -195,6 +195,9 @@ typedef struct {
   int cheb_orders[4];
   int pre_it[4];
   int post_it[4];
+  int amg_cheb_order;        /* Chebyshev degree on the algebraic coarse levels (0: cheb_order);
+                                default 2 (the coarse correction needs no more at C2: same
+                                iteration count as degree 4) */
 } sipg_solver_opts;
 
 int sipg_solver_default_opts(int kind, sipg_solver_opts *o);

@@ -679,7 +679,8 @@ const T* sipg_solver::csr_chebyshev(AmgDevLevel& A, const T* rin, bool first, bo
   const T* dcur = nullptr;  // not read by the first step (c1 = 0)
   const T* rcur = rin;
   int ob = rin == rbuf[0] ? 1 : 0;
-  for (int it = 0; it < o.cheb_order; ++it) {
+  const int deg = o.amg_cheb_order > 0 ? o.amg_cheb_order : o.cheb_order;
+  for (int it = 0; it < deg; ++it) {
     double c1 = 0.0, c2 = 1.0 / theta;
     if (it > 0) {
       double rho = 1.0 / (2.0 * sigma - rho_old);
@@ -688,7 +689,7 @@ const T* sipg_solver::csr_chebyshev(AmgDevLevel& A, const T* rin, bool first, bo
       rho_old = rho;
     }
     T* dn = dbuf[ob];
-    T* rn = (it < o.cheb_order - 1 || want_res) ? rbuf[ob] : nullptr;
+    T* rn = (it < deg - 1 || want_res) ? rbuf[ob] : nullptr;
     csr_cheb<T>(A.n, A.A.ptr.as<int>(), A.A.idx.as<int>(), A.A.vals<T>(), dcur ? dcur : dn, rcur, dinv, dn, rn,
                 A.z.as<T>(), (T)c1, (T)c2, first && it == 0, stream);
     dcur = dn;
@@ -1076,6 +1077,7 @@ int sipg_solver_default_opts(int kind, sipg_solver_opts* o) {
     o->graphs = 2;
     o->assembled_max_order = 1;
     o->smoother = 1;
+    o->amg_cheb_order = 2;
     for (int l = 0; l < 4; ++l) {
       o->cheb_orders[l] = 0;
       o->pre_it[l] = 1;

@@ -49,7 +49,8 @@ class SolverOpts(C.Structure):
                 ("eig_iters", C.c_int), ("coarse_iters", C.c_int), ("check_every", C.c_int),
                 ("coarse_kind", C.c_int), ("amg_coarse_max", C.c_int), ("amg_strength", C.c_double),
                 ("graphs", C.c_int), ("assembled_max_order", C.c_int), ("smoother", C.c_int),
-                ("cheb_orders", C.c_int * 4), ("pre_it", C.c_int * 4), ("post_it", C.c_int * 4)]
+                ("cheb_orders", C.c_int * 4), ("pre_it", C.c_int * 4), ("post_it", C.c_int * 4),
+                ("amg_cheb_order", C.c_int)]
 
 
 def lib():

@@ -69,6 +69,7 @@ def _pmg_solver(case, precision, coarse_kind=1, pin=True):
     o.coarse_kind = coarse_kind
     o.nullspace = 0 if pin else 1
     o.smoother = 0  # the oracle's p-multigrid smooths with point Jacobi
+    o.amg_cheb_order = 0  # and uses the order levels' Chebyshev degree on the algebraic levels
     return op, sipg.Solver(op, sipg.SOLVER_PMULTIGRID, o)
 
 
