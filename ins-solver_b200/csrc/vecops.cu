@@ -299,11 +299,21 @@ __global__ void __launch_bounds__(BT) k_cheb_sym(T* d, T* z, const T* __restrict
   for (size_t e0 = (size_t)blockIdx.x * BT; e0 < (size_t)nb; e0 += (size_t)gridDim.x * BT) {
     const int ne = (size_t)nb - e0 < (size_t)BT ? (int)((size_t)nb - e0) : BT;
     const size_t g0 = e0 * NP;
-    for (int i = tid; i < ne * NP; i += BT) {
-      const int s = (i / NP) * LD + i % NP;
-      sr[s] = res[g0 + i];
-      if (use_d) sd[s] = d[g0 + i];
-      if (!first) sz[s] = z[g0 + i];
+    if (ne == BT) {  // full group: every load issued back to back
+#pragma unroll
+      for (int k = 0; k < NP; ++k) {
+        const int i = tid + k * BT, s = (i / NP) * LD + i % NP;
+        sr[s] = res[g0 + i];
+        if (use_d) sd[s] = d[g0 + i];
+        if (!first) sz[s] = z[g0 + i];
+      }
+    } else {
+      for (int i = tid; i < ne * NP; i += BT) {
+        const int s = (i / NP) * LD + i % NP;
+        sr[s] = res[g0 + i];
+        if (use_d) sd[s] = d[g0 + i];
+        if (!first) sz[s] = z[g0 + i];
+      }
     }
     __syncthreads();
     if (tid < ne) {
@@ -336,10 +346,19 @@ __global__ void __launch_bounds__(BT) k_cheb_sym(T* d, T* z, const T* __restrict
       }
     }
     __syncthreads();
-    for (int i = tid; i < ne * NP; i += BT) {
-      const int s = (i / NP) * LD + i % NP;
-      d[g0 + i] = sd[s];
-      z[g0 + i] = sz[s];
+    if (ne == BT) {
+#pragma unroll
+      for (int k = 0; k < NP; ++k) {
+        const int i = tid + k * BT, s = (i / NP) * LD + i % NP;
+        d[g0 + i] = sd[s];
+        z[g0 + i] = sz[s];
+      }
+    } else {
+      for (int i = tid; i < ne * NP; i += BT) {
+        const int s = (i / NP) * LD + i % NP;
+        d[g0 + i] = sd[s];
+        z[g0 + i] = sz[s];
+      }
     }
     __syncthreads();
   }
