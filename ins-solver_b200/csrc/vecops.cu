@@ -84,6 +84,7 @@ __global__ void __launch_bounds__(kRedThreads) k_multi_dot(const T* a0, const T*
   double v[NK];
 #pragma unroll
   for (int k = 0; k < NK; ++k) v[k] = 0.0;
+  #pragma unroll 4
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     v[0] += (double)a0[i] * (double)b0[i];
     if (NK > 1) v[1 % NK] += (double)a1[i] * (double)b1[i];
@@ -98,6 +99,7 @@ __global__ void __launch_bounds__(kRedThreads) k_dot_diff(const double* r, const
                                                           double* out) {
   pdl_enter();
   double v[1] = {0.0};
+  #pragma unroll 4
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     v[0] += r[i] * (z[i] - zo[i]);
   block_sum<1>(v);
@@ -109,6 +111,7 @@ __global__ void __launch_bounds__(kRedThreads) k_sum(const T* a, size_t n, doubl
                                                      unsigned* counter, double* out) {
   pdl_enter();
   double v[1] = {0.0};
+  #pragma unroll 4
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     v[0] += (double)a[i];
   block_sum<1>(v);
@@ -123,6 +126,7 @@ __global__ void __launch_bounds__(kRedThreads) k_cg_update_xr(double* x, double*
   pdl_enter();
   const double alpha = scal[num] / scal[den];
   double v[1] = {0.0};
+  #pragma unroll 4
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     x[i] += alpha * p[i];
     double ri = r[i] - alpha * Ap[i];
@@ -141,6 +145,7 @@ __global__ void __launch_bounds__(kRedThreads) k_cg_update_xr_sum(double* x, dou
   pdl_enter();
   const double alpha = scal[num] / scal[den];
   double v[2] = {0.0, 0.0};
+  #pragma unroll 4
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     x[i] += alpha * p[i];
     double ri = r[i] - alpha * Ap[i];
@@ -160,6 +165,7 @@ __global__ void __launch_bounds__(kRedThreads) k_resid_prep(double* r, float* r3
   pdl_enter();
   const double m = mean_slot >= 0 ? scal[mean_slot] / (double)n : 0.0;
   double v[2] = {0.0, 0.0};
+  #pragma unroll 4
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     double ri = r[i];
     if (mean_slot >= 0) {
@@ -179,6 +185,7 @@ __global__ void __launch_bounds__(kRedThreads) k_to_f64_sum(double* z, const flo
                                                             unsigned* counter, double* out) {
   pdl_enter();
   double v[1] = {0.0};
+  #pragma unroll 4
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const double zi = (double)z32[i];
     z[i] = zi;
@@ -195,6 +202,7 @@ __global__ void __launch_bounds__(kRedThreads) k_finish_z_dot(double* z, const f
   pdl_enter();
   const double m = mean_slot >= 0 ? scal[mean_slot] / (double)n : 0.0;
   double v[1] = {0.0};
+  #pragma unroll 4
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     double zi = z32 ? (double)z32[i] : z[i];
     if (mean_slot >= 0) zi -= m;
@@ -548,6 +556,7 @@ __global__ void __launch_bounds__(kRedThreads) k_coarse_update(T* z, T* r, T* sv
   const bool ok = pap > 0.0 && scal[S_C_RZ] > 0.0;
   const T alpha = ok ? (T)(scal[S_C_RZ] / pap) : T(0);
   double v[1] = {0.0};
+  #pragma unroll 4
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     z[i] += alpha * p[i];
     T ri = r[i] - alpha * Ap[i];
@@ -641,6 +650,14 @@ __global__ void k_vadd(T* y, const T* x, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) y[i] += x[i];
 }
 
+// Reduction grid: one element per thread for short vectors (up to 296 CTAs),
+// about eight per thread for long ones, at most kRedBlocks CTAs (the partial sums
+// depend on n only, so results stay reproducible).
+inline int red_grid(size_t n) {
+  const size_t short_grid = std::min<size_t>((n + kRedThreads - 1) / kRedThreads, 296);
+  const size_t long_grid = (n + 8 * kRedThreads - 1) / (8 * kRedThreads);
+  return (int)std::max<size_t>(1, std::min<size_t>(kRedBlocks, std::max(short_grid, long_grid)));
+}
 inline int grid_for(size_t n) {
   size_t g = (n + 255) / 256;
   return (int)std::max<size_t>(1, std::min<size_t>(g, 148 * 16));
@@ -652,55 +669,55 @@ template <typename T>
 void multi_dot(const T* const* a, const T* const* b, int nk, size_t n, double* out, int out_stride,
                const RedWork& w, cudaStream_t s) {
   if (nk == 1)
-    pdl_launch(k_multi_dot<T, 1>, dim3(kRedBlocks), dim3(kRedThreads), 0, s, a[0], b[0], nullptr, nullptr, nullptr, nullptr, n,
+    pdl_launch(k_multi_dot<T, 1>, dim3(red_grid(n)), dim3(kRedThreads), 0, s, a[0], b[0], nullptr, nullptr, nullptr, nullptr, n,
                                                          w.partial, w.counter, out, out_stride);
   else if (nk == 2)
-    pdl_launch(k_multi_dot<T, 2>, dim3(kRedBlocks), dim3(kRedThreads), 0, s, a[0], b[0], a[1], b[1], nullptr, nullptr, n,
+    pdl_launch(k_multi_dot<T, 2>, dim3(red_grid(n)), dim3(kRedThreads), 0, s, a[0], b[0], a[1], b[1], nullptr, nullptr, n,
                                                          w.partial, w.counter, out, out_stride);
   else
-    pdl_launch(k_multi_dot<T, 3>, dim3(kRedBlocks), dim3(kRedThreads), 0, s, a[0], b[0], a[1], b[1], a[2], b[2], n,
+    pdl_launch(k_multi_dot<T, 3>, dim3(red_grid(n)), dim3(kRedThreads), 0, s, a[0], b[0], a[1], b[1], a[2], b[2], n,
                                                          w.partial, w.counter, out, out_stride);
   note_launch();
 }
 
 void dot_diff(const double* r, const double* z, const double* zo, size_t n, double* out,
               const RedWork& w, cudaStream_t s) {
-  pdl_launch(k_dot_diff, dim3(kRedBlocks), dim3(kRedThreads), 0, s, r, z, zo, n, w.partial, w.counter, out);
+  pdl_launch(k_dot_diff, dim3(red_grid(n)), dim3(kRedThreads), 0, s, r, z, zo, n, w.partial, w.counter, out);
   note_launch();
 }
 
 template <typename T>
 void vsum(const T* a, size_t n, double* out, const RedWork& w, cudaStream_t s) {
-  pdl_launch(k_sum<T>, dim3(kRedBlocks), dim3(kRedThreads), 0, s, a, n, w.partial, w.counter, out);
+  pdl_launch(k_sum<T>, dim3(red_grid(n)), dim3(kRedThreads), 0, s, a, n, w.partial, w.counter, out);
   note_launch();
 }
 
 void cg_update_xr(double* x, double* r, const double* p, const double* Ap, size_t n,
                   const double* scal, int num, int den, double* rr_out, const RedWork& w,
                   cudaStream_t s) {
-  pdl_launch(k_cg_update_xr, dim3(kRedBlocks), dim3(kRedThreads), 0, s, x, r, p, Ap, n, scal, num, den, w.partial, w.counter, rr_out);
+  pdl_launch(k_cg_update_xr, dim3(red_grid(n)), dim3(kRedThreads), 0, s, x, r, p, Ap, n, scal, num, den, w.partial, w.counter, rr_out);
   note_launch();
 }
 
 void cg_update_xr_sum(double* x, double* r, const double* p, const double* Ap, size_t n, const double* scal, int num,
                       int den, double* out, int stride, const RedWork& w, cudaStream_t s) {
-  pdl_launch(k_cg_update_xr_sum, dim3(kRedBlocks), dim3(kRedThreads), 0, s, x, r, p, Ap, n, scal, num, den, w.partial,
+  pdl_launch(k_cg_update_xr_sum, dim3(red_grid(n)), dim3(kRedThreads), 0, s, x, r, p, Ap, n, scal, num, den, w.partial,
              w.counter, out, stride);
   note_launch();
 }
 void resid_prep(double* r, float* r32, const double* zo, size_t n, const double* scal, int mean_slot, double* out,
                 int stride, const RedWork& w, cudaStream_t s) {
-  pdl_launch(k_resid_prep, dim3(kRedBlocks), dim3(kRedThreads), 0, s, r, r32, zo, n, scal, mean_slot, w.partial,
+  pdl_launch(k_resid_prep, dim3(red_grid(n)), dim3(kRedThreads), 0, s, r, r32, zo, n, scal, mean_slot, w.partial,
              w.counter, out, stride);
   note_launch();
 }
 void to_f64_sum(double* z, const float* z32, size_t n, double* out, const RedWork& w, cudaStream_t s) {
-  pdl_launch(k_to_f64_sum, dim3(kRedBlocks), dim3(kRedThreads), 0, s, z, z32, n, w.partial, w.counter, out);
+  pdl_launch(k_to_f64_sum, dim3(red_grid(n)), dim3(kRedThreads), 0, s, z, z32, n, w.partial, w.counter, out);
   note_launch();
 }
 void finish_z_dot(double* z, const float* z32, const double* r, size_t n, const double* scal, int mean_slot,
                   double* out, const RedWork& w, cudaStream_t s) {
-  pdl_launch(k_finish_z_dot, dim3(kRedBlocks), dim3(kRedThreads), 0, s, z, z32, r, n, scal, mean_slot, w.partial,
+  pdl_launch(k_finish_z_dot, dim3(red_grid(n)), dim3(kRedThreads), 0, s, z, z32, r, n, scal, mean_slot, w.partial,
              w.counter, out);
   note_launch();
 }
@@ -834,7 +851,7 @@ void prolong_add(T* z, const T* zc, const T* P, int K, int Npf, int Npc, int nco
 template <typename T>
 void coarse_update(T* z, T* r, T* sv, const T* p, const T* Ap, const T* dinv, size_t n, double* scal,
                    const RedWork& w, cudaStream_t s) {
-  pdl_launch(k_coarse_update<T>, dim3(kRedBlocks), dim3(kRedThreads), 0, s, z, r, sv, p, Ap, dinv, n, scal, w.partial, w.counter);
+  pdl_launch(k_coarse_update<T>, dim3(red_grid(n)), dim3(kRedThreads), 0, s, z, r, sv, p, Ap, dinv, n, scal, w.partial, w.counter);
   note_launch();
 }
 template <typename T>

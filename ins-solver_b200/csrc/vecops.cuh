@@ -45,7 +45,7 @@ struct RedWork {
   double* partial = nullptr;   // kRedBlocks x 4
   unsigned* counter = nullptr; // 1
 };
-constexpr int kRedBlocks = 296;
+constexpr int kRedBlocks = 148 * 8;
 constexpr int kRedThreads = 256;
 
 // out[k] = sum_i a_k[i] * b_k[i] for k < nk (nk <= 3); b_k may alias a_k.
