@@ -1,0 +1,727 @@
+// Per-element forms of the reference's OP2 user kernels on the solve path.
+//
+// Each function has the name and the argument list of a kernel under the
+// reference's src/kernels/ (for example fvmf_3d_mult_flux.h:1-5,
+// cg3_update_res.h:1-3) and computes the same values for one cell (or one face,
+// for the face loops), so that a caller that drives those kernels through
+// op_par_loop can call these instead, and so that each kernel can be checked on
+// its own against the reference. The fused tensor-core kernels of libsipg_b200
+// are the performance path; these are the per-kernel drop-ins.
+//
+// Compile-time sizes replace the reference build's macros: the polynomial order
+// is the template argument ORDER (DG_ORDER), the dimension is part of the name
+// (fvmf_3d_* / vmf_3d_* / cg3_* in 3D, fvmf_2d_* / vmf_2d_* / cg_* in 2D; the
+// kernels the two builds share take DIM as well), and DG_FP is double.
+// The reference-element tables that the reference's kernels read by name
+// (dg_Dr_kernel, dg_Ds_kernel, dg_Dt_kernel, dg_Mass_kernel, dg_MM_F0..3_kernel,
+// FMASK) come from ref_tables<DIM, ORDER>(), which the program defines for every
+// (DIM, ORDER) it uses, as the reference's build generates those constants.
+//
+// SIPG_OP2_REF_QUIRKS (default 1) keeps the reference's statements where they
+// differ from the SIPG formula they implement (vmf_3d_mult_flux.h:10-11 drops
+// the n_z term of n . {grad u}; fvmf_3d_op1.h:17-18 multiplies without the
+// transpose); 0 gives the corrected forms.
+#pragma once
+
+#include <cmath>
+
+#if defined(__CUDACC__)
+#define SIPG_OP2_HD __host__ __device__ inline
+#else
+#define SIPG_OP2_HD inline
+#endif
+
+#ifndef SIPG_OP2_REF_QUIRKS
+#define SIPG_OP2_REF_QUIRKS 1
+#endif
+
+namespace ins_solver_b200 {
+namespace op2 {
+
+// Sizes of one (DIM, ORDER) and the positions in geof (3D: rx ry rz sx sy sz tx
+// ty tz J; 2D: rx ry sx sy J).
+template <int DIM, int ORDER>
+struct Dg {
+  static constexpr int NP = DIM == 3 ? (ORDER + 1) * (ORDER + 2) * (ORDER + 3) / 6 : (ORDER + 1) * (ORDER + 2) / 2;
+  static constexpr int NPF = DIM == 3 ? (ORDER + 1) * (ORDER + 2) / 2 : ORDER + 1;
+  static constexpr int NUM_FACES = DIM + 1;
+  static constexpr int RX = 0, RY = 1, RZ = 2;
+  static constexpr int SX = DIM == 3 ? 3 : 2, SY = DIM == 3 ? 4 : 3, SZ = 5;
+  static constexpr int TX = 6, TY = 7, TZ = 8;
+  static constexpr int J = DIM == 3 ? 9 : 4;
+  // penalty constant of fvmf_*_calc_tau_*: 2 (p + 1) (p + 2)
+  static constexpr double TAU_ORDER = 2.0 * (ORDER + 1) * (ORDER + 2);
+};
+
+// Reference-element tables of one (DIM, ORDER): NP x NP matrices column-major
+// (entry (i, j) at i + j * NP, as the dg_*_kernel constants), MM_F[f] the face
+// mass of face f embedded in the volume, fmask the volume node of each face node
+// (NUM_FACES x NPF, as FMASK).
+struct RefTables {
+  const double *Dr, *Ds, *Dt, *Mass;
+  const double *MM_F[4];
+  const int *fmask;
+};
+
+template <int DIM, int ORDER>
+SIPG_OP2_HD const RefTables &ref_tables();
+
+namespace detail {
+
+SIPG_OP2_HD double dmax(double a, double b) { return a > b ? a : b; }
+
+// y = A x for a column-major NP x NP matrix (op2_in_kernel_gemv, no transpose)
+template <int NP>
+SIPG_OP2_HD void matvec(const double *A, const double *x, double *y) {
+  for (int i = 0; i < NP; ++i) {
+    double s = 0.0;
+    for (int j = 0; j < NP; ++j) s += A[i + j * NP] * x[j];
+    y[i] = s;
+  }
+}
+
+// Physical derivative matrix of direction d (0 x, 1 y, 2 z), column-major:
+// Dd = r_d Dr + s_d Ds (+ t_d Dt)
+template <int DIM, int ORDER>
+SIPG_OP2_HD double dphys(const RefTables &t, const double *geof, int d, int ind) {
+  using G = Dg<DIM, ORDER>;
+  const int r = d == 0 ? G::RX : d == 1 ? G::RY : G::RZ;
+  const int s = d == 0 ? G::SX : d == 1 ? G::SY : G::SZ;
+  double v = geof[r] * t.Dr[ind] + geof[s] * t.Ds[ind];
+  if (DIM == 3) v += geof[d == 0 ? G::TX : d == 1 ? G::TY : G::TZ] * t.Dt[ind];
+  return v;
+}
+
+}  // namespace detail
+
+// ---------------------------------------------------------------- CG (cg3_*.h: 3 components, cg_*.h: 2)
+
+template <int ORDER>
+SIPG_OP2_HD void cg3_alpha(double *tmp_alpha_0, double *tmp_alpha_1, const double *r0, const double *r1,
+                           const double *r2, const double *p0, const double *p1, const double *p2, const double *Ax0,
+                           const double *Ax1, const double *Ax2) {
+  double rr = 0.0, pap = 0.0;
+  for (int i = 0; i < Dg<3, ORDER>::NP; ++i) {
+    rr += r0[i] * r0[i] + r1[i] * r1[i] + r2[i] * r2[i];
+    pap += p0[i] * Ax0[i] + p1[i] * Ax1[i] + p2[i] * Ax2[i];
+  }
+  *tmp_alpha_0 += rr;
+  *tmp_alpha_1 += pap;
+}
+
+template <int ORDER>
+SIPG_OP2_HD void cg3_alpha_pre(double *tmp_alpha_0, double *tmp_alpha_1, const double *r0, const double *r1,
+                               const double *r2, const double *z0, const double *z1, const double *z2,
+                               const double *p0, const double *p1, const double *p2, const double *Ax0,
+                               const double *Ax1, const double *Ax2) {
+  double rz = 0.0, pap = 0.0;
+  for (int i = 0; i < Dg<3, ORDER>::NP; ++i) {
+    rz += r0[i] * z0[i] + r1[i] * z1[i] + r2[i] * z2[i];
+    pap += p0[i] * Ax0[i] + p1[i] * Ax1[i] + p2[i] * Ax2[i];
+  }
+  *tmp_alpha_0 += rz;
+  *tmp_alpha_1 += pap;
+}
+
+template <int ORDER>
+SIPG_OP2_HD void cg3_block_jacobi(const double *u_pre_mat, const double *v_pre_mat, const double *w_pre_mat,
+                                  const double *u_in, const double *v_in, const double *w_in, double *u_out,
+                                  double *v_out, double *w_out) {
+  constexpr int NP = Dg<3, ORDER>::NP;
+  detail::matvec<NP>(u_pre_mat, u_in, u_out);
+  detail::matvec<NP>(v_pre_mat, v_in, v_out);
+  detail::matvec<NP>(w_pre_mat, w_in, w_out);
+}
+
+template <int ORDER>
+SIPG_OP2_HD void cg3_compute_beta(double *beta, const double *r0, const double *r1, const double *r2) {
+  double s = 0.0;
+  for (int i = 0; i < Dg<3, ORDER>::NP; ++i) s += r0[i] * r0[i] + r1[i] * r1[i] + r2[i] * r2[i];
+  *beta += s;
+}
+
+template <int ORDER>
+SIPG_OP2_HD void cg3_compute_beta_pre(double *beta, const double *r0, const double *r1, const double *r2,
+                                      const double *z0, const double *z1, const double *z2) {
+  double s = 0.0;
+  for (int i = 0; i < Dg<3, ORDER>::NP; ++i) s += r0[i] * z0[i] + r1[i] * z1[i] + r2[i] * z2[i];
+  *beta += s;
+}
+
+template <int ORDER>
+SIPG_OP2_HD void cg3_compute_beta_pre_flex(double *beta, const double *r0, const double *r1, const double *r2,
+                                           const double *z0, const double *z1, const double *z2, const double *z0_1,
+                                           const double *z1_1, const double *z2_1) {
+  double s = 0.0;
+  for (int i = 0; i < Dg<3, ORDER>::NP; ++i)
+    s += r0[i] * (z0[i] - z0_1[i]) + r1[i] * (z1[i] - z1_1[i]) + r2[i] * (z2[i] - z2_1[i]);
+  *beta += s;
+}
+
+template <int ORDER>
+SIPG_OP2_HD void cg3_jacobi(const double *u_diag, const double *v_diag, const double *w_diag, const double *u_in,
+                            const double *v_in, const double *w_in, double *u, double *v, double *w) {
+  for (int i = 0; i < Dg<3, ORDER>::NP; ++i) {
+    u[i] = u_in[i] / u_diag[i];
+    v[i] = v_in[i] / v_diag[i];
+    w[i] = w_in[i] / w_diag[i];
+  }
+}
+
+template <int ORDER>
+SIPG_OP2_HD void cg3_recp_factor_inv_mass(const double *factor, double *u, double *v, double *w) {
+  for (int i = 0; i < Dg<3, ORDER>::NP; ++i) {
+    u[i] /= factor[i];
+    v[i] /= factor[i];
+    w[i] /= factor[i];
+  }
+}
+
+template <int ORDER>
+SIPG_OP2_HD void cg3_residual(double *residual, const double *rhs0, const double *rhs1, const double *rhs2,
+                              double *r0, double *r1, double *r2) {
+  double s = 0.0;
+  for (int i = 0; i < Dg<3, ORDER>::NP; ++i) {
+    r0[i] = rhs0[i] - r0[i];
+    r1[i] = rhs1[i] - r1[i];
+    r2[i] = rhs2[i] - r2[i];
+    s += r0[i] * r0[i] + r1[i] * r1[i] + r2[i] * r2[i];
+  }
+  *residual += s;
+}
+
+template <int ORDER>
+SIPG_OP2_HD void cg3_update_ans(const double *alpha, const double *p0, const double *p1, const double *p2, double *u,
+                                double *v, double *w) {
+  for (int i = 0; i < Dg<3, ORDER>::NP; ++i) {
+    u[i] += *alpha * p0[i];
+    v[i] += *alpha * p1[i];
+    w[i] += *alpha * p2[i];
+  }
+}
+
+template <int ORDER>
+SIPG_OP2_HD void cg3_update_p(const double *beta, const double *r0, const double *r1, const double *r2, double *p0,
+                              double *p1, double *p2) {
+  for (int i = 0; i < Dg<3, ORDER>::NP; ++i) {
+    p0[i] = r0[i] + *beta * p0[i];
+    p1[i] = r1[i] + *beta * p1[i];
+    p2[i] = r2[i] + *beta * p2[i];
+  }
+}
+
+template <int ORDER>
+SIPG_OP2_HD void cg3_update_res(const double *alpha, double *residual, const double *Ap0, const double *Ap1,
+                                const double *Ap2, double *r0, double *r1, double *r2) {
+  double s = 0.0;
+  for (int i = 0; i < Dg<3, ORDER>::NP; ++i) {
+    r0[i] -= *alpha * Ap0[i];
+    r1[i] -= *alpha * Ap1[i];
+    r2[i] -= *alpha * Ap2[i];
+    s += r0[i] * r0[i] + r1[i] * r1[i] + r2[i] * r2[i];
+  }
+  *residual += s;
+}
+
+template <int ORDER>
+SIPG_OP2_HD void cg_alpha(double *tmp_alpha_0, double *tmp_alpha_1, const double *r0, const double *r1,
+                          const double *p0, const double *p1, const double *Ax0, const double *Ax1) {
+  double rr = 0.0, pap = 0.0;
+  for (int i = 0; i < Dg<2, ORDER>::NP; ++i) {
+    rr += r0[i] * r0[i] + r1[i] * r1[i];
+    pap += p0[i] * Ax0[i] + p1[i] * Ax1[i];
+  }
+  *tmp_alpha_0 += rr;
+  *tmp_alpha_1 += pap;
+}
+
+template <int ORDER>
+SIPG_OP2_HD void cg_alpha_pre(double *tmp_alpha_0, double *tmp_alpha_1, const double *r0, const double *r1,
+                              const double *z0, const double *z1, const double *p0, const double *p1,
+                              const double *Ax0, const double *Ax1) {
+  double rz = 0.0, pap = 0.0;
+  for (int i = 0; i < Dg<2, ORDER>::NP; ++i) {
+    rz += r0[i] * z0[i] + r1[i] * z1[i];
+    pap += p0[i] * Ax0[i] + p1[i] * Ax1[i];
+  }
+  *tmp_alpha_0 += rz;
+  *tmp_alpha_1 += pap;
+}
+
+template <int ORDER>
+SIPG_OP2_HD void cg_block_jacobi(const double *u_pre_mat, const double *v_pre_mat, const double *u_in,
+                                 const double *v_in, double *u_out, double *v_out) {
+  constexpr int NP = Dg<2, ORDER>::NP;
+  detail::matvec<NP>(u_pre_mat, u_in, u_out);
+  detail::matvec<NP>(v_pre_mat, v_in, v_out);
+}
+
+template <int ORDER>
+SIPG_OP2_HD void cg_compute_beta(double *beta, const double *r0, const double *r1) {
+  double s = 0.0;
+  for (int i = 0; i < Dg<2, ORDER>::NP; ++i) s += r0[i] * r0[i] + r1[i] * r1[i];
+  *beta += s;
+}
+
+template <int ORDER>
+SIPG_OP2_HD void cg_compute_beta_pre(double *beta, const double *r0, const double *r1, const double *z0,
+                                     const double *z1) {
+  double s = 0.0;
+  for (int i = 0; i < Dg<2, ORDER>::NP; ++i) s += r0[i] * z0[i] + r1[i] * z1[i];
+  *beta += s;
+}
+
+template <int ORDER>
+SIPG_OP2_HD void cg_compute_beta_pre_flex(double *beta, const double *r0, const double *r1, const double *z0,
+                                          const double *z1, const double *z0_1, const double *z1_1) {
+  double s = 0.0;
+  for (int i = 0; i < Dg<2, ORDER>::NP; ++i) s += r0[i] * (z0[i] - z0_1[i]) + r1[i] * (z1[i] - z1_1[i]);
+  *beta += s;
+}
+
+template <int ORDER>
+SIPG_OP2_HD void cg_jacobi(const double *u_diag, const double *v_diag, const double *u_in, const double *v_in,
+                           double *u, double *v) {
+  for (int i = 0; i < Dg<2, ORDER>::NP; ++i) {
+    u[i] = u_in[i] / u_diag[i];
+    v[i] = v_in[i] / v_diag[i];
+  }
+}
+
+template <int ORDER>
+SIPG_OP2_HD void cg_recp_factor_inv_mass(const double *factor, double *u, double *v) {
+  for (int i = 0; i < Dg<2, ORDER>::NP; ++i) {
+    u[i] /= factor[i];
+    v[i] /= factor[i];
+  }
+}
+
+template <int ORDER>
+SIPG_OP2_HD void cg_residual(double *residual, const double *rhs0, const double *rhs1, double *r0, double *r1) {
+  double s = 0.0;
+  for (int i = 0; i < Dg<2, ORDER>::NP; ++i) {
+    r0[i] = rhs0[i] - r0[i];
+    r1[i] = rhs1[i] - r1[i];
+    s += r0[i] * r0[i] + r1[i] * r1[i];
+  }
+  *residual += s;
+}
+
+template <int ORDER>
+SIPG_OP2_HD void cg_update_ans(const double *alpha, const double *p0, const double *p1, double *u, double *v) {
+  for (int i = 0; i < Dg<2, ORDER>::NP; ++i) {
+    u[i] += *alpha * p0[i];
+    v[i] += *alpha * p1[i];
+  }
+}
+
+template <int ORDER>
+SIPG_OP2_HD void cg_update_p(const double *beta, const double *r0, const double *r1, double *p0, double *p1) {
+  for (int i = 0; i < Dg<2, ORDER>::NP; ++i) {
+    p0[i] = r0[i] + *beta * p0[i];
+    p1[i] = r1[i] + *beta * p1[i];
+  }
+}
+
+template <int ORDER>
+SIPG_OP2_HD void cg_update_res(const double *alpha, double *residual, const double *Ap0, const double *Ap1,
+                               double *r0, double *r1) {
+  double s = 0.0;
+  for (int i = 0; i < Dg<2, ORDER>::NP; ++i) {
+    r0[i] -= *alpha * Ap0[i];
+    r1[i] -= *alpha * Ap1[i];
+    s += r0[i] * r0[i] + r1[i] * r1[i];
+  }
+  *residual += s;
+}
+
+// ---------------------------------------------------------------- small cell kernels (both builds)
+
+template <int DIM, int ORDER>
+SIPG_OP2_HD void constant_mult(const double *constant, double *val) {
+  for (int i = 0; i < Dg<DIM, ORDER>::NP; ++i) val[i] *= *constant;
+}
+
+template <int DIM, int ORDER>
+SIPG_OP2_HD void copy_dg_np(const double *in, double *out) {
+  for (int i = 0; i < Dg<DIM, ORDER>::NP; ++i) out[i] = in[i];
+}
+
+template <int DIM, int ORDER>
+SIPG_OP2_HD void copy_dg_np_mat(const double *in, double *out) {
+  constexpr int NP = Dg<DIM, ORDER>::NP;
+  for (int i = 0; i < NP * NP; ++i) out[i] = in[i];
+}
+
+template <int DIM, int ORDER>
+SIPG_OP2_HD void reciprocal(const double *in, double *out) {
+  for (int i = 0; i < Dg<DIM, ORDER>::NP; ++i) out[i] = 1.0 / in[i];
+}
+
+template <int DIM, int ORDER>
+SIPG_OP2_HD void zero_npf_3(double *x, double *y, double *z) {
+  using G = Dg<DIM, ORDER>;
+  for (int i = 0; i < G::NUM_FACES * G::NPF; ++i) x[i] = y[i] = z[i] = 0.0;
+}
+
+// factor = 1 / rho (the pressure Poisson coefficient)
+template <int DIM, int ORDER>
+SIPG_OP2_HD void poisson_pr_fact(const double *rho, double *factor) {
+  for (int i = 0; i < Dg<DIM, ORDER>::NP; ++i) factor[i] = 1.0 / rho[i];
+}
+
+// viscous Helmholtz coefficients: factor = mu, mmFactor = mmConst rho
+template <int DIM, int ORDER>
+SIPG_OP2_HD void poisson_vis_fact(const double *mmConst, const double *mu, const double *rho, double *factor,
+                                  double *mmFactor) {
+  for (int i = 0; i < Dg<DIM, ORDER>::NP; ++i) {
+    factor[i] = mu[i];
+    mmFactor[i] = *mmConst * rho[i];
+  }
+}
+
+// ---------------------------------------------------------------- penalty (fvmf_*_calc_tau_*, vmf_calc_tau_*)
+
+namespace detail {
+// interior face: tau of both sides = 2 (p + 1) (p + 2) max over the face nodes of
+// max(fscale_L f_L, fscale_R f_R)
+template <int DIM, int ORDER>
+SIPG_OP2_HD void tau_faces(const int *faceNum, const int *fmaskR_corrected, const double *fscale,
+                           const double **factor, double **tau) {
+  using G = Dg<DIM, ORDER>;
+  const int *fm = ref_tables<DIM, ORDER>().fmask + faceNum[0] * G::NPF;
+  double m = 0.0;
+  for (int j = 0; j < G::NPF; ++j)
+    m = dmax(m, G::TAU_ORDER * dmax(fscale[0] * factor[0][fm[j]], fscale[1] * factor[1][fmaskR_corrected[j]]));
+  tau[0][faceNum[0]] = m;
+  tau[1][faceNum[1]] = m;
+}
+// boundary face: 2 (p + 1) (p + 2) fscale max over the face nodes of f
+template <int DIM, int ORDER>
+SIPG_OP2_HD void tau_bfaces(const int *faceNum, const double *fscale, const double *factor, double *tau) {
+  using G = Dg<DIM, ORDER>;
+  const int *fm = ref_tables<DIM, ORDER>().fmask + faceNum[0] * G::NPF;
+  double m = factor[fm[0]];
+  for (int j = 1; j < G::NPF; ++j) m = dmax(m, factor[fm[j]]);
+  tau[faceNum[0]] = m * (G::TAU_ORDER * fscale[0]);
+}
+}  // namespace detail
+
+template <int ORDER>
+SIPG_OP2_HD void fvmf_3d_calc_tau_faces(const int *faceNum, const int *fmaskR_corrected, const double *fscale,
+                                        const double **factor, double **tau) {
+  detail::tau_faces<3, ORDER>(faceNum, fmaskR_corrected, fscale, factor, tau);
+}
+// 2D: the neighbour's face nodes are its own face's nodes, in reverse order when *reverse
+template <int ORDER>
+SIPG_OP2_HD void fvmf_2d_calc_tau_faces(const int *faceNum, const bool *reverse, const double *fscale,
+                                        const double **factor, double **tau) {
+  using G = Dg<2, ORDER>;
+  const int *fR = ref_tables<2, ORDER>().fmask + faceNum[1] * G::NPF;
+  int fmaskR[G::NPF];
+  for (int j = 0; j < G::NPF; ++j) fmaskR[j] = fR[*reverse ? G::NPF - 1 - j : j];
+  detail::tau_faces<2, ORDER>(faceNum, fmaskR, fscale, factor, tau);
+}
+template <int ORDER>
+SIPG_OP2_HD void fvmf_3d_calc_tau_bfaces(const int *faceNum, const double *fscale, const double *factor,
+                                         double *tau) {
+  detail::tau_bfaces<3, ORDER>(faceNum, fscale, factor, tau);
+}
+template <int ORDER>
+SIPG_OP2_HD void fvmf_2d_calc_tau_bfaces(const int *faceNum, const double *fscale, const double *factor,
+                                         double *tau) {
+  detail::tau_bfaces<2, ORDER>(faceNum, fscale, factor, tau);
+}
+
+// constant coefficient
+template <int DIM, int ORDER>
+SIPG_OP2_HD void vmf_calc_tau_faces(const int *faceNum, const double *fscale, double **tau) {
+  const double t = Dg<DIM, ORDER>::TAU_ORDER * detail::dmax(fscale[0], fscale[1]);
+  tau[0][faceNum[0]] = t;
+  tau[1][faceNum[1]] = t;
+}
+template <int DIM, int ORDER>
+SIPG_OP2_HD void vmf_calc_tau_bfaces(const int *faceNum, const double *fscale, double *tau) {
+  tau[faceNum[0]] = Dg<DIM, ORDER>::TAU_ORDER * fscale[0];
+}
+
+// ---------------------------------------------------------------- apply: volume terms
+
+// reference derivatives (in place) -> f G^T grad: ux = f (rx ur + sx us + tx ut), ...
+template <int ORDER>
+SIPG_OP2_HD void fvmf_3d_grad(const double *geof, const double *fact, double *ux, double *uy, double *uz, double *vx,
+                              double *vy, double *vz, double *wx, double *wy, double *wz) {
+  using G = Dg<3, ORDER>;
+  double *comp[3][3] = {{ux, uy, uz}, {vx, vy, vz}, {wx, wy, wz}};
+  for (int m = 0; m < G::NP; ++m)
+    for (int c = 0; c < 3; ++c) {
+      const double ur = comp[c][0][m], us = comp[c][1][m], ut = comp[c][2][m];
+      comp[c][0][m] = fact[m] * (geof[G::RX] * ur + geof[G::SX] * us + geof[G::TX] * ut);
+      comp[c][1][m] = fact[m] * (geof[G::RY] * ur + geof[G::SY] * us + geof[G::TY] * ut);
+      comp[c][2][m] = fact[m] * (geof[G::RZ] * ur + geof[G::SZ] * us + geof[G::TZ] * ut);
+    }
+}
+
+template <int ORDER>
+SIPG_OP2_HD void fvmf_2d_grad(const double *geof, const double *factor, double *ux, double *uy, double *vx,
+                              double *vy) {
+  using G = Dg<2, ORDER>;
+  double *comp[2][2] = {{ux, uy}, {vx, vy}};
+  for (int m = 0; m < G::NP; ++m)
+    for (int c = 0; c < 2; ++c) {
+      const double ur = comp[c][0][m], us = comp[c][1][m];
+      comp[c][0][m] = factor[m] * (geof[G::RX] * ur + geof[G::SX] * us);
+      comp[c][1][m] = factor[m] * (geof[G::RY] * ur + geof[G::SY] * us);
+    }
+}
+
+// physical -> reference-direction components for the transposed derivative: (q_r, q_s, q_t) = G q
+template <int ORDER>
+SIPG_OP2_HD void vmf_3d_mult_cells_geof(const double *geof, double *u_x, double *u_y, double *u_z, double *v_x,
+                                        double *v_y, double *v_z, double *w_x, double *w_y, double *w_z) {
+  using G = Dg<3, ORDER>;
+  double *comp[3][3] = {{u_x, u_y, u_z}, {v_x, v_y, v_z}, {w_x, w_y, w_z}};
+  for (int n = 0; n < G::NP; ++n)
+    for (int c = 0; c < 3; ++c) {
+      const double qx = comp[c][0][n], qy = comp[c][1][n], qz = comp[c][2][n];
+      comp[c][0][n] = geof[G::RX] * qx + geof[G::RY] * qy + geof[G::RZ] * qz;
+      comp[c][1][n] = geof[G::SX] * qx + geof[G::SY] * qy + geof[G::SZ] * qz;
+      comp[c][2][n] = geof[G::TX] * qx + geof[G::TY] * qy + geof[G::TZ] * qz;
+    }
+}
+
+template <int ORDER>
+SIPG_OP2_HD void vmf_2d_mult_cells_geof(const double *geof, double *u_x, double *u_y, double *v_x, double *v_y) {
+  using G = Dg<2, ORDER>;
+  double *comp[2][2] = {{u_x, u_y}, {v_x, v_y}};
+  for (int c = 0; c < 2; ++c)
+    for (int n = 0; n < G::NP; ++n) {
+      const double qx = comp[c][0][n], qy = comp[c][1][n];
+      comp[c][0][n] = geof[G::RX] * qx + geof[G::RY] * qy;
+      comp[c][1][n] = geof[G::SX] * qx + geof[G::SY] * qy;
+    }
+}
+
+namespace detail {
+// out_c += J M (mm in_c): nodal mm (per-node factor inside the product) or scalar
+template <int DIM, int ORDER, int NC>
+SIPG_OP2_HD void mass_terms(const double *geof, const double *mm, bool nodal, const double *const *in,
+                            double *const *out) {
+  using G = Dg<DIM, ORDER>;
+  const double *M = ref_tables<DIM, ORDER>().Mass;
+  for (int m = 0; m < G::NP; ++m)
+    for (int c = 0; c < NC; ++c) {
+      double s = 0.0;
+      for (int n = 0; n < G::NP; ++n) s += (nodal ? mm[n] * M[m + n * G::NP] : M[m + n * G::NP]) * in[c][n];
+      out[c][m] += nodal ? s * geof[G::J] : *mm * s * geof[G::J];
+    }
+}
+}  // namespace detail
+
+template <int ORDER>
+SIPG_OP2_HD void fvmf_3d_mult_mm_geof(const double *geof, const double *mm_factor, const double *u_in,
+                                      const double *v_in, const double *w_in, double *u_out, double *v_out,
+                                      double *w_out) {
+  const double *in[3] = {u_in, v_in, w_in};
+  double *out[3] = {u_out, v_out, w_out};
+  detail::mass_terms<3, ORDER, 3>(geof, mm_factor, true, in, out);
+}
+template <int ORDER>
+SIPG_OP2_HD void fvmf_2d_mult_mm_geof(const double *geof, const double *mm_factor, const double *u, const double *v,
+                                      double *u_out, double *v_out) {
+  const double *in[2] = {u, v};
+  double *out[2] = {u_out, v_out};
+  detail::mass_terms<2, ORDER, 2>(geof, mm_factor, true, in, out);
+}
+template <int ORDER>
+SIPG_OP2_HD void vmf_3d_mult_mm_geof(const double *geof, const double *mm_factor, const double *u, const double *v,
+                                     const double *w, double *u_out, double *v_out, double *w_out) {
+  const double *in[3] = {u, v, w};
+  double *out[3] = {u_out, v_out, w_out};
+  detail::mass_terms<3, ORDER, 3>(geof, mm_factor, false, in, out);
+}
+template <int ORDER>
+SIPG_OP2_HD void vmf_2d_mult_mm_geof(const double *geof, const double *mm_factor, const double *u, const double *v,
+                                     double *u_out, double *v_out) {
+  const double *in[2] = {u, v};
+  double *out[2] = {u_out, v_out};
+  detail::mass_terms<2, ORDER, 2>(geof, mm_factor, false, in, out);
+}
+
+// ---------------------------------------------------------------- apply: boundary traces (vmf_*_mult_avg_jump)
+
+namespace detail {
+// Boundary face faceNum[0] of a cell: Dirichlet components add 2 u and grad u at
+// the face nodes to the jump / average buffers, Neumann ones nothing; when every
+// component is slip (type 2) the normal projection n n^T of u and of each
+// derivative component is added instead.
+template <int DIM, int ORDER>
+SIPG_OP2_HD void avg_jump(const int *const *bc, const int *faceNum, const double *const *n,
+                          const double *const *u, const double *const (*du)[3], double *const *jump,
+                          double *const (*avg)[3]) {
+  using G = Dg<DIM, ORDER>;
+  const int *fm = ref_tables<DIM, ORDER>().fmask + faceNum[0] * G::NPF;
+  bool slip = true;
+  for (int c = 0; c < DIM; ++c) slip = slip && *bc[c] == 2;
+  for (int j = 0; j < G::NPF; ++j) {
+    const int m = fm[j], k = faceNum[0] * G::NPF + j;
+    if (slip) {
+      for (int c = 0; c < DIM; ++c) {
+        double pu = 0.0, pd[3] = {0.0, 0.0, 0.0};
+        for (int e = 0; e < DIM; ++e) {
+          const double nn = *n[c] * *n[e];
+          pu += nn * u[e][m];
+          for (int d = 0; d < DIM; ++d) pd[d] += nn * du[e][d][m];
+        }
+        jump[c][k] += 2.0 * pu;
+        for (int d = 0; d < DIM; ++d) avg[c][d][k] += pd[d];
+      }
+    } else {
+      for (int c = 0; c < DIM; ++c)
+        if (*bc[c] == 0) {
+          jump[c][k] += 2.0 * u[c][m];
+          for (int d = 0; d < DIM; ++d) avg[c][d][k] += du[c][d][m];
+        }
+    }
+  }
+}
+}  // namespace detail
+
+template <int ORDER>
+SIPG_OP2_HD void vmf_3d_mult_avg_jump(const int *u_bc_type, const int *v_bc_type, const int *w_bc_type,
+                                      const int *faceNum, const double *nx, const double *ny, const double *nz,
+                                      const double *u, const double *u_x, const double *u_y, const double *u_z,
+                                      const double *v, const double *v_x, const double *v_y, const double *v_z,
+                                      const double *w, const double *w_x, const double *w_y, const double *w_z,
+                                      double *u_jump, double *u_x_avg, double *u_y_avg, double *u_z_avg,
+                                      double *v_jump, double *v_x_avg, double *v_y_avg, double *v_z_avg,
+                                      double *w_jump, double *w_x_avg, double *w_y_avg, double *w_z_avg) {
+  const int *bc[3] = {u_bc_type, v_bc_type, w_bc_type};
+  const double *n[3] = {nx, ny, nz};
+  const double *uu[3] = {u, v, w};
+  const double *du[3][3] = {{u_x, u_y, u_z}, {v_x, v_y, v_z}, {w_x, w_y, w_z}};
+  double *jump[3] = {u_jump, v_jump, w_jump};
+  double *avg[3][3] = {{u_x_avg, u_y_avg, u_z_avg}, {v_x_avg, v_y_avg, v_z_avg}, {w_x_avg, w_y_avg, w_z_avg}};
+  detail::avg_jump<3, ORDER>(bc, faceNum, n, uu, du, jump, avg);
+}
+
+template <int ORDER>
+SIPG_OP2_HD void vmf_2d_mult_avg_jump(const int *u_bc_type, const int *v_bc_type, const int *faceNum,
+                                      const double *nx, const double *ny, const double *u, const double *u_x,
+                                      const double *u_y, const double *v, const double *v_x, const double *v_y,
+                                      double *u_jump, double *u_x_avg, double *u_y_avg, double *v_jump,
+                                      double *v_x_avg, double *v_y_avg) {
+  const int *bc[2] = {u_bc_type, v_bc_type};
+  const double *n[2] = {nx, ny};
+  const double *uu[2] = {u, v};
+  const double *du[2][3] = {{u_x, u_y, nullptr}, {v_x, v_y, nullptr}};
+  double *jump[2] = {u_jump, v_jump};
+  double *avg[2][3] = {{u_x_avg, u_y_avg, nullptr}, {v_x_avg, v_y_avg, nullptr}};
+  detail::avg_jump<2, ORDER>(bc, faceNum, n, uu, du, jump, avg);
+}
+
+// ---------------------------------------------------------------- apply: face fluxes (*_mult_flux)
+
+namespace detail {
+// Per face node of each face i: with h = [u]/2 and s = n . {grad u},
+//   jump <- sJ (tau h - s),  avg_d <- -n_d sJ f h
+// (f the nodal factor at the face node, 1 for the constant-coefficient form;
+// drop_nz: the n_z term of s left out, as vmf_3d_mult_flux.h:10-11).
+template <int DIM, int ORDER, int NC>
+SIPG_OP2_HD void flux(const double *const *n, const double *sJ, const double *tau, const double *factor,
+                      bool drop_nz, double *const *jump, double *const (*avg)[3]) {
+  using G = Dg<DIM, ORDER>;
+  const int *fmask = ref_tables<DIM, ORDER>().fmask;
+  for (int c = 0; c < NC; ++c)
+    for (int i = 0; i < G::NUM_FACES; ++i)
+      for (int j = 0; j < G::NPF; ++j) {
+        const int k = i * G::NPF + j;
+        const double h = 0.5 * jump[c][k];
+        double s = 0.0;
+        for (int d = 0; d < DIM; ++d)
+          if (!(drop_nz && d == 2)) s += n[d][i] * avg[c][d][k];
+        const double f = factor ? factor[fmask[k]] : 1.0;
+        jump[c][k] = sJ[i] * (tau[i] * h - s);
+        for (int d = 0; d < DIM; ++d) avg[c][d][k] = n[d][i] * sJ[i] * f * -h;
+      }
+}
+}  // namespace detail
+
+template <int ORDER>
+SIPG_OP2_HD void fvmf_3d_mult_flux(const double *nx, const double *ny, const double *nz, const double *sJ,
+                                   const double *tau, const double *factor, double *u_jump, double *u_avg_x,
+                                   double *u_avg_y, double *u_avg_z, double *v_jump, double *v_avg_x,
+                                   double *v_avg_y, double *v_avg_z, double *w_jump, double *w_avg_x,
+                                   double *w_avg_y, double *w_avg_z) {
+  const double *n[3] = {nx, ny, nz};
+  double *jump[3] = {u_jump, v_jump, w_jump};
+  double *avg[3][3] = {{u_avg_x, u_avg_y, u_avg_z}, {v_avg_x, v_avg_y, v_avg_z}, {w_avg_x, w_avg_y, w_avg_z}};
+  detail::flux<3, ORDER, 3>(n, sJ, tau, factor, false, jump, avg);
+}
+
+template <int ORDER>
+SIPG_OP2_HD void fvmf_2d_mult_flux(const double *nx, const double *ny, const double *sJ, const double *tau,
+                                   const double *factor, double *u_jump, double *u_x_avg, double *u_y_avg,
+                                   double *v_jump, double *v_x_avg, double *v_y_avg) {
+  const double *n[2] = {nx, ny};
+  double *jump[2] = {u_jump, v_jump};
+  double *avg[2][3] = {{u_x_avg, u_y_avg, nullptr}, {v_x_avg, v_y_avg, nullptr}};
+  detail::flux<2, ORDER, 2>(n, sJ, tau, factor, false, jump, avg);
+}
+
+template <int ORDER>
+SIPG_OP2_HD void vmf_3d_mult_flux(const double *nx, const double *ny, const double *nz, const double *sJ,
+                                  const double *tau, double *u_jump, double *u_x_avg, double *u_y_avg,
+                                  double *u_z_avg, double *v_jump, double *v_x_avg, double *v_y_avg, double *v_z_avg,
+                                  double *w_jump, double *w_x_avg, double *w_y_avg, double *w_z_avg) {
+  const double *n[3] = {nx, ny, nz};
+  double *jump[3] = {u_jump, v_jump, w_jump};
+  double *avg[3][3] = {{u_x_avg, u_y_avg, u_z_avg}, {v_x_avg, v_y_avg, v_z_avg}, {w_x_avg, w_y_avg, w_z_avg}};
+  detail::flux<3, ORDER, 3>(n, sJ, tau, nullptr, SIPG_OP2_REF_QUIRKS != 0, jump, avg);
+}
+
+template <int ORDER>
+SIPG_OP2_HD void vmf_2d_mult_flux(const double *nx, const double *ny, const double *sJ, const double *tau,
+                                  double *u_jump, double *u_x_avg, double *u_y_avg, double *v_jump, double *v_x_avg,
+                                  double *v_y_avg) {
+  const double *n[2] = {nx, ny};
+  double *jump[2] = {u_jump, v_jump};
+  double *avg[2][3] = {{u_x_avg, u_y_avg, nullptr}, {v_x_avg, v_y_avg, nullptr}};
+  detail::flux<2, ORDER, 2>(n, sJ, tau, nullptr, false, jump, avg);
+}
+
+// ---------------------------------------------------------------- diagonal / block-diagonal mass terms
+
+template <int DIM, int ORDER>
+SIPG_OP2_HD void mm_diag(const double *factor, const double *geof, double *diag) {
+  using G = Dg<DIM, ORDER>;
+  const double *M = ref_tables<DIM, ORDER>().Mass;
+  for (int i = 0; i < G::NP; ++i) diag[i] += factor[i] * geof[G::J] * M[i + i * G::NP];
+}
+template <int DIM, int ORDER>
+SIPG_OP2_HD void mm_block_diag(const double *factor, const double *geof, double *op1) {
+  using G = Dg<DIM, ORDER>;
+  const double *M = ref_tables<DIM, ORDER>().Mass;
+  for (int j = 0; j < G::NP; ++j)
+    for (int i = 0; i < G::NP; ++i) op1[i + j * G::NP] += factor[i] * geof[G::J] * M[i + j * G::NP];
+}
+
+template <int ORDER>
+SIPG_OP2_HD void fvmf_3d_mm_diag(const double *factor, const double *geof, double *diag) {
+  mm_diag<3, ORDER>(factor, geof, diag);
+}
+template <int ORDER>
+SIPG_OP2_HD void fvmf_2d_mm_diag(const double *factor, const double *geof, double *diag) {
+  mm_diag<2, ORDER>(factor, geof, diag);
+}
+template <int ORDER>
+SIPG_OP2_HD void fvmf_3d_mm_block_diag(const double *factor, const double *geof, double *op1) {
+  mm_block_diag<3, ORDER>(factor, geof, op1);
+}
+template <int ORDER>
+SIPG_OP2_HD void fvmf_2d_mm_block_diag(const double *factor, const double *geof, double *op1) {
+  mm_block_diag<2, ORDER>(factor, geof, op1);
+}
+
+}  // namespace op2
+}  // namespace ins_solver_b200

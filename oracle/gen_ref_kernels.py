@@ -26,6 +26,8 @@ KERNELS_3D = [
     "cg3_alpha", "cg3_alpha_pre", "cg3_compute_beta", "cg3_compute_beta_pre",
     "cg3_compute_beta_pre_flex", "cg3_update_ans", "cg3_update_res", "cg3_update_p",
     "cg3_residual", "cg3_jacobi", "cg3_block_jacobi", "zero_npf_3", "copy_dg_np",
+    "cg3_recp_factor_inv_mass", "vmf_3d_mult_mm_geof", "vmf_3d_apply_bc",
+    "constant_mult", "reciprocal", "copy_dg_np_mat", "poisson_pr_fact", "poisson_vis_fact",
 ]
 KERNELS_2D = [
     "fvmf_2d_grad", "fvmf_2d_calc_tau_faces", "fvmf_2d_calc_tau_bfaces", "vmf_2d_mult_avg_jump",
@@ -36,6 +38,8 @@ KERNELS_2D = [
     "cg_alpha", "cg_alpha_pre", "cg_compute_beta", "cg_compute_beta_pre",
     "cg_compute_beta_pre_flex", "cg_update_ans", "cg_update_res", "cg_update_p",
     "cg_residual", "cg_jacobi", "cg_block_jacobi", "zero_npf_3", "copy_dg_np",
+    "cg_recp_factor_inv_mass", "vmf_2d_mult_flux", "vmf_2d_mult_mm_geof", "vmf_2d_apply_bc",
+    "constant_mult", "reciprocal", "copy_dg_np_mat", "poisson_pr_fact", "poisson_vis_fact",
 ]
 
 
@@ -130,6 +134,35 @@ def specialise(text, dim, p):
     return text
 
 
+def signature(text):
+    """(name, [arg type, ...]) of the first `inline void name(...)` in text."""
+    i = text.index("inline void ")
+    j = text.index("(", i)
+    name = text[i + len("inline void "):j].strip()
+    depth, k = 1, j + 1
+    while depth:
+        depth += {"(": 1, ")": -1}.get(text[k], 0)
+        k += 1
+    types = []
+    for a in text[j + 1:k - 1].split(","):
+        a = " ".join(a.split())
+        cut = len(a)
+        while cut > 0 and (a[cut - 1].isalnum() or a[cut - 1] == "_"):
+            cut -= 1
+        types.append(a[:cut].strip())
+    return name, types
+
+
+def dispatch(sigs):
+    """Body of call_kernel(name, args): one branch per kernel, arguments cast from void*."""
+    lines = ["static int call_kernel(const char *name, void **a) {"]
+    for name, types in sigs:
+        args = ", ".join(f"({t})a[{i}]" for i, t in enumerate(types))
+        lines.append(f'  if (!std::strcmp(name, "{name}")) {{ {name}({args}); return 0; }}')
+    lines.append("  return -1;\n}")
+    return "\n".join(lines) + "\n"
+
+
 def main():
     ref_root, out_dir = sys.argv[1], sys.argv[2]
     kdir = os.path.join(ref_root, "src", "kernels")
@@ -137,13 +170,18 @@ def main():
         for p in range(1, 5):
             d = os.path.join(out_dir, f"d{dim}p{p}")
             os.makedirs(d, exist_ok=True)
+            sigs = []
             for n in names:
                 with open(os.path.join(kdir, n + ".h")) as f:
                     text = f.read()
+                spec = specialise(text, dim, p)
+                sigs.append(signature(spec))
                 with open(os.path.join(d, n + ".h"), "w") as f:
-                    f.write(specialise(text, dim, p) + "\n")
+                    f.write(spec + "\n")
             with open(os.path.join(d, "all.h"), "w") as f:
                 f.write("".join(f'#include "{n}.h"\n' for n in names))
+            with open(os.path.join(d, "dispatch.inc"), "w") as f:
+                f.write(dispatch(sigs))
 
 
 if __name__ == "__main__":

@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstddef>
+#include <cstring>
 #include <vector>
 
 #include "sipg_oracle.h"
@@ -26,21 +27,25 @@ using std::fmax;
 namespace d2p1 { constexpr int ORDER = 1, NP = 3, NPF = 2, NF = 3;
 #include "ref_harness_pre.inc"
 #include "_ref/gen/d2p1/all.h"
+#include "_ref/gen/d2p1/dispatch.inc"
 #include "ref_harness_body.inc"
 }
 namespace d2p2 { constexpr int ORDER = 2, NP = 6, NPF = 3, NF = 3;
 #include "ref_harness_pre.inc"
 #include "_ref/gen/d2p2/all.h"
+#include "_ref/gen/d2p2/dispatch.inc"
 #include "ref_harness_body.inc"
 }
 namespace d2p3 { constexpr int ORDER = 3, NP = 10, NPF = 4, NF = 3;
 #include "ref_harness_pre.inc"
 #include "_ref/gen/d2p3/all.h"
+#include "_ref/gen/d2p3/dispatch.inc"
 #include "ref_harness_body.inc"
 }
 namespace d2p4 { constexpr int ORDER = 4, NP = 15, NPF = 5, NF = 3;
 #include "ref_harness_pre.inc"
 #include "_ref/gen/d2p4/all.h"
+#include "_ref/gen/d2p4/dispatch.inc"
 #include "ref_harness_body.inc"
 }
 #undef DIM
@@ -60,21 +65,25 @@ namespace d2p4 { constexpr int ORDER = 4, NP = 15, NPF = 5, NF = 3;
 namespace d3p1 { constexpr int ORDER = 1, NP = 4, NPF = 3, NF = 4;
 #include "ref_harness_pre.inc"
 #include "_ref/gen/d3p1/all.h"
+#include "_ref/gen/d3p1/dispatch.inc"
 #include "ref_harness_body.inc"
 }
 namespace d3p2 { constexpr int ORDER = 2, NP = 10, NPF = 6, NF = 4;
 #include "ref_harness_pre.inc"
 #include "_ref/gen/d3p2/all.h"
+#include "_ref/gen/d3p2/dispatch.inc"
 #include "ref_harness_body.inc"
 }
 namespace d3p3 { constexpr int ORDER = 3, NP = 20, NPF = 10, NF = 4;
 #include "ref_harness_pre.inc"
 #include "_ref/gen/d3p3/all.h"
+#include "_ref/gen/d3p3/dispatch.inc"
 #include "ref_harness_body.inc"
 }
 namespace d3p4 { constexpr int ORDER = 4, NP = 35, NPF = 15, NF = 4;
 #include "ref_harness_pre.inc"
 #include "_ref/gen/d3p4/all.h"
+#include "_ref/gen/d3p4/dispatch.inc"
 #include "ref_harness_body.inc"
 }
 
@@ -112,5 +121,20 @@ int ref_block_diag(const oracle_mesh *m, int ncomp, const int *bc_types, const d
 int ref_solve(const oracle_mesh *m, const oracle_solver_opts *o, const double *b, double *x,
               oracle_solve_info *info) {
   DISPATCH(solve_api(m, o, b, x, info))
+}
+// One reference kernel by name on caller buffers (args: its arguments in order),
+// with the reference-element tables of m; -1 for an unknown name or element.
+int ref_kernel(const oracle_mesh *m, const char *name, void **args) {
+  switch (m->dim * 10 + m->order) {
+    case 21: d2p1::load_constants(m); return d2p1::call_kernel(name, args);
+    case 22: d2p2::load_constants(m); return d2p2::call_kernel(name, args);
+    case 23: d2p3::load_constants(m); return d2p3::call_kernel(name, args);
+    case 24: d2p4::load_constants(m); return d2p4::call_kernel(name, args);
+    case 31: d3p1::load_constants(m); return d3p1::call_kernel(name, args);
+    case 32: d3p2::load_constants(m); return d3p2::call_kernel(name, args);
+    case 33: d3p3::load_constants(m); return d3p3::call_kernel(name, args);
+    case 34: d3p4::load_constants(m); return d3p4::call_kernel(name, args);
+    default: return -1;
+  }
 }
 }
