@@ -20,7 +20,8 @@
 // SIPG_OP2_REF_QUIRKS (default 1) keeps the reference's statements where they
 // differ from the SIPG formula they implement (vmf_3d_mult_flux.h:10-11 drops
 // the n_z term of n . {grad u}; fvmf_3d_op1.h:17-18 multiplies without the
-// transpose); 0 gives the corrected forms.
+// transpose; fvmf_2d_op1.h:20-37 applies the factor between the transposed
+// derivative and the mass matrix); 0 gives the corrected forms.
 #pragma once
 
 #include <cmath>
@@ -721,6 +722,412 @@ SIPG_OP2_HD void fvmf_3d_mm_block_diag(const double *factor, const double *geof,
 template <int ORDER>
 SIPG_OP2_HD void fvmf_2d_mm_block_diag(const double *factor, const double *geof, double *op1) {
   mm_block_diag<2, ORDER>(factor, geof, op1);
+}
+
+
+// ---------------------------------------------------------------- diagonal and block diagonal (calc_diag, calc_inv_block_diag)
+
+namespace detail {
+
+// n . grad in reference coordinates with its rows scaled by f (none when f is null):
+// D[i + j NP] = f_i sum_r (n . g_r) D_r[i + j NP], g_r the rows of geof
+template <int DIM, int ORDER>
+SIPG_OP2_HD void normal_deriv(const double *n, const double *geof, const double *f, double *D) {
+  using G = Dg<DIM, ORDER>;
+  constexpr int NP = G::NP;
+  const RefTables &t = ref_tables<DIM, ORDER>();
+  double c[3];
+  c[0] = n[0] * geof[G::RX] + n[1] * geof[G::RY];
+  c[1] = n[0] * geof[G::SX] + n[1] * geof[G::SY];
+  c[2] = 0.0;
+  if (DIM == 3) {
+    c[0] += n[2] * geof[G::RZ];
+    c[1] += n[2] * geof[G::SZ];
+    c[2] = n[0] * geof[G::TX] + n[1] * geof[G::TY] + n[2] * geof[G::TZ];
+  }
+  for (int j = 0; j < NP; ++j)
+    for (int i = 0; i < NP; ++i) {
+      const int ind = i + j * NP;
+      double v = c[0] * t.Dr[ind] + c[1] * t.Ds[ind];
+      if (DIM == 3) v += c[2] * t.Dt[ind];
+      D[ind] = f ? v * f[i] : v;
+    }
+}
+
+// (MF D + D^T MF)_ij, the consistency and symmetry terms of a face
+template <int NP>
+SIPG_OP2_HD double face_sym(const double *MF, const double *D, int i, int j) {
+  double s = 0.0;
+  for (int k = 0; k < NP; ++k) s += MF[i + k * NP] * D[k + j * NP] + D[k + i * NP] * MF[k + j * NP];
+  return s;
+}
+
+// interior-face penalty from the two sides' nodal factors at the matched face nodes
+template <int DIM, int ORDER>
+SIPG_OP2_HD double pair_gtau(const int *fmaskL, const int *fmaskR, const double *fscale, const double *const *factor) {
+  using G = Dg<DIM, ORDER>;
+  double g = 0.0;
+  for (int j = 0; j < G::NPF; ++j)
+    g = dmax(g, G::TAU_ORDER * dmax(fscale[0] * factor[0][fmaskL[j]], fscale[1] * factor[1][fmaskR[j]]));
+  return g;
+}
+
+// boundary-face penalty: max over the face nodes of 2 (p + 1) (p + 2) fscale f
+template <int DIM, int ORDER>
+SIPG_OP2_HD double bface_gtau(const int *fmaskB, double fscale, const double *factor) {
+  using G = Dg<DIM, ORDER>;
+  double g = 0.0;
+  for (int j = 0; j < G::NPF; ++j) g = dmax(g, G::TAU_ORDER * fscale * factor[fmaskB[j]]);
+  return g;
+}
+
+// Volume block J sum_d D_d^T M F D_d (F the nodal factor), or the reference's
+// forms: 3D sum_d D_d (J M F D_d); 2D J sum_d D_d^T F (M D_d).
+template <int DIM, int ORDER>
+SIPG_OP2_HD void volume_block(const double *geof, const double *factor, double *op1) {
+  using G = Dg<DIM, ORDER>;
+  constexpr int NP = G::NP;
+  const RefTables &t = ref_tables<DIM, ORDER>();
+  const double J = geof[G::J];
+  double D[NP * NP], T[NP * NP];
+  const bool ref2d = SIPG_OP2_REF_QUIRKS && DIM == 2, ref3d = SIPG_OP2_REF_QUIRKS && DIM == 3;
+  if (ref2d) {
+    // D: x derivative, T = M D; Dy: y derivative, Ty = M Dy
+    double Dy[NP * NP], Ty[NP * NP];
+    for (int j = 0; j < NP; ++j)
+      for (int i = 0; i < NP; ++i) {
+        D[i + j * NP] = dphys<DIM, ORDER>(t, geof, 0, i + j * NP);
+        Dy[i + j * NP] = dphys<DIM, ORDER>(t, geof, 1, i + j * NP);
+      }
+    for (int j = 0; j < NP; ++j)
+      for (int i = 0; i < NP; ++i) {
+        double a = 0.0, b = 0.0;
+        for (int k = 0; k < NP; ++k) {
+          a += t.Mass[i + k * NP] * D[k + j * NP];
+          b += t.Mass[i + k * NP] * Dy[k + j * NP];
+        }
+        T[i + j * NP] = a;
+        Ty[i + j * NP] = b;
+      }
+    for (int j = 0; j < NP; ++j)
+      for (int i = 0; i < NP; ++i) {
+        double s = 0.0;
+        for (int k = 0; k < NP; ++k)
+          s += factor[k] * (D[k + i * NP] * T[k + j * NP] + Dy[k + i * NP] * Ty[k + j * NP]);
+        op1[i + j * NP] = s * J;
+      }
+    return;
+  }
+  for (int d = 0; d < DIM; ++d) {
+    for (int j = 0; j < NP; ++j)
+      for (int i = 0; i < NP; ++i) D[i + j * NP] = dphys<DIM, ORDER>(t, geof, d, i + j * NP);
+    for (int j = 0; j < NP; ++j)
+      for (int i = 0; i < NP; ++i) {
+        double s = 0.0;
+        for (int k = 0; k < NP; ++k) s += t.Mass[i + k * NP] * (D[k + j * NP] * factor[k]);
+        T[i + j * NP] = J * s;
+      }
+    for (int j = 0; j < NP; ++j)
+      for (int i = 0; i < NP; ++i) {
+        double s = 0.0;
+        for (int k = 0; k < NP; ++k) s += (ref3d ? D[i + k * NP] : D[k + i * NP]) * T[k + j * NP];
+        op1[i + j * NP] = (d == 0 ? 0.0 : op1[i + j * NP]) + s;
+      }
+  }
+}
+
+// Its diagonal, J sum_d (D_d^T M F D_d)_ii.
+template <int DIM, int ORDER>
+SIPG_OP2_HD void volume_diag(const double *geof, const double *factor, double *diag) {
+  using G = Dg<DIM, ORDER>;
+  constexpr int NP = G::NP;
+  const RefTables &t = ref_tables<DIM, ORDER>();
+  double D[NP * NP], T[NP * NP];
+  for (int i = 0; i < NP; ++i) diag[i] = 0.0;
+  for (int d = 0; d < DIM; ++d) {
+    for (int j = 0; j < NP; ++j)
+      for (int i = 0; i < NP; ++i) D[i + j * NP] = dphys<DIM, ORDER>(t, geof, d, i + j * NP) * factor[i];
+    for (int j = 0; j < NP; ++j)
+      for (int i = 0; i < NP; ++i) {
+        double s = 0.0;
+        for (int k = 0; k < NP; ++k) s += t.Mass[i + k * NP] * D[k + j * NP];
+        T[i + j * NP] = s;
+      }
+    for (int i = 0; i < NP; ++i)
+      for (int k = 0; k < NP; ++k) diag[i] += dphys<DIM, ORDER>(t, geof, d, k + i * NP) * T[k + i * NP];
+  }
+  for (int i = 0; i < NP; ++i) diag[i] *= geof[G::J];
+}
+
+// Interior face (fvmf_*_op2_diag / _block_diag): for each side s,
+//   block_s += sJ_s / 2 (gtau MF_s - (MF_s D_s + D_s^T MF_s)), D_s = n_s . grad with rows f_s
+template <int DIM, int ORDER>
+SIPG_OP2_HD void face_pair(const int *faceNum, const int *fmaskR, const double *const *n, const double *fscale,
+                           const double *sJ, const double *const *geof, const double *const *factor, double *outL,
+                           double *outR, bool block) {
+  using G = Dg<DIM, ORDER>;
+  constexpr int NP = G::NP;
+  const RefTables &t = ref_tables<DIM, ORDER>();
+  const double gtau = pair_gtau<DIM, ORDER>(t.fmask + faceNum[0] * G::NPF, fmaskR, fscale, factor);
+  double D[NP * NP];
+  for (int s = 0; s < 2; ++s) {
+    double ns[3] = {n[0][s], n[1][s], DIM == 3 ? n[2][s] : 0.0};
+    normal_deriv<DIM, ORDER>(ns, geof[s], factor[s], D);
+    const double *MF = t.MM_F[faceNum[s]];
+    double *out = s == 0 ? outL : outR;
+    if (block) {
+      for (int j = 0; j < NP; ++j)
+        for (int i = 0; i < NP; ++i) {
+          double a = 0.0;
+          for (int k = 0; k < NP; ++k) a += MF[i + k * NP] * D[k + j * NP];
+          out[i + j * NP] = out[i + j * NP] + (-0.5 * sJ[s]) * a;
+        }
+      for (int j = 0; j < NP; ++j)
+        for (int i = 0; i < NP; ++i) {
+          double a = 0.0;
+          for (int k = 0; k < NP; ++k) a += D[k + i * NP] * MF[k + j * NP];
+          out[i + j * NP] = out[i + j * NP] + (-0.5 * sJ[s]) * a;
+        }
+      const double c = 0.5 * sJ[s] * gtau;
+      for (int j = 0; j < NP; ++j)
+        for (int i = 0; i < NP; ++i) out[i + j * NP] += c * MF[i + j * NP];
+    } else {
+      for (int i = 0; i < NP; ++i)
+        out[i] += 0.5 * sJ[s] * (gtau * MF[i + i * NP] - face_sym<NP>(MF, D, i, i));
+    }
+  }
+}
+
+// Boundary face (fvmf_*_bop_diag / _block_diag): Dirichlet components add
+// sJ (gtau MF - (MF D + D^T MF)), Neumann ones nothing; when every component is
+// slip, each adds sJ n_c^2 (gtau MF - (MF D + D^T MF)).
+template <int DIM, int ORDER>
+SIPG_OP2_HD void face_bnd(const int *faceNum, const int *const *bc, const double *const *n, const double *fscale,
+                          const double *sJ, const double *geof, const double *factor, double *const *out,
+                          bool block) {
+  using G = Dg<DIM, ORDER>;
+  constexpr int NP = G::NP;
+  const RefTables &t = ref_tables<DIM, ORDER>();
+  bool slip = true, any = false;
+  for (int c = 0; c < DIM; ++c) {
+    slip = slip && *bc[c] == 2;
+    any = any || *bc[c] == 0;
+  }
+  if (!slip && !any) return;
+  double D[NP * NP];
+  const double ns[3] = {*n[0], *n[1], DIM == 3 ? *n[2] : 0.0};
+  normal_deriv<DIM, ORDER>(ns, geof, factor, D);
+  const double gtau = bface_gtau<DIM, ORDER>(t.fmask + faceNum[0] * G::NPF, *fscale, factor);
+  const double *MF = t.MM_F[faceNum[0]];
+  for (int c = 0; c < DIM; ++c) {
+    if (!slip && *bc[c] != 0) continue;
+    const double w = slip ? *sJ * ns[c] * ns[c] : *sJ;
+    if (block) {
+      for (int j = 0; j < NP; ++j)
+        for (int i = 0; i < NP; ++i)
+          out[c][i + j * NP] += w * (gtau * MF[i + j * NP] - face_sym<NP>(MF, D, i, j));
+    } else {
+      for (int i = 0; i < NP; ++i) out[c][i] += w * (gtau * MF[i + i * NP] - face_sym<NP>(MF, D, i, i));
+    }
+  }
+}
+
+// Boundary lifting of one boundary face (fvmf_*_apply_bc with the nodal factor,
+// vmf_*_apply_bc without): Dirichlet data g adds gtau sJ MF g - D^T (sJ MF g),
+// Neumann data adds sJ MF g, slip nothing.
+template <int DIM, int ORDER>
+SIPG_OP2_HD void lift_bc(const int *faceNum, const int *const *bc, const double *const *n, const double *fscale,
+                         const double *sJ, const double *geof, const double *fact, const double *const *g,
+                         double *const *rhs) {
+  using G = Dg<DIM, ORDER>;
+  constexpr int NP = G::NP;
+  const RefTables &t = ref_tables<DIM, ORDER>();
+  const int *fm = t.fmask + faceNum[0] * G::NPF;
+  const double *MF = t.MM_F[faceNum[0]];
+  for (int c = 0; c < DIM; ++c) {
+    if (*bc[c] == 1) {
+      for (int i = 0; i < NP; ++i)
+        for (int j = 0; j < G::NPF; ++j) rhs[c][i] += *sJ * MF[i + fm[j] * NP] * g[c][j];
+      continue;
+    }
+    if (*bc[c] != 0) continue;
+    double D[NP * NP], tmp[NP];
+    for (int j = 0; j < NP; ++j)
+      for (int i = 0; i < NP; ++i) {
+        const int ind = i + j * NP;
+        double v = 0.0;
+        for (int d = 0; d < DIM; ++d) v += *n[d] * dphys<DIM, ORDER>(t, geof, d, ind);
+        D[ind] = fact ? v * fact[i] : v;
+      }
+    double gtau = G::TAU_ORDER * *fscale;
+    if (fact) {
+      double m = fact[fm[0]];
+      for (int j = 1; j < G::NPF; ++j) m = dmax(m, fact[fm[j]]);
+      gtau = m * gtau;
+    }
+    for (int i = 0; i < NP; ++i) {
+      tmp[i] = 0.0;
+      for (int j = 0; j < G::NPF; ++j) {
+        rhs[c][i] += gtau * *sJ * MF[i + fm[j] * NP] * g[c][j];
+        tmp[i] += *sJ * MF[i + fm[j] * NP] * g[c][j];
+      }
+    }
+    for (int i = 0; i < NP; ++i)
+      for (int j = 0; j < NP; ++j) rhs[c][i] += -D[j + i * NP] * tmp[j];
+  }
+}
+
+}  // namespace detail
+
+template <int ORDER>
+SIPG_OP2_HD void fvmf_3d_op1(const double *geof, const double *factor, double *op1) {
+  detail::volume_block<3, ORDER>(geof, factor, op1);
+}
+template <int ORDER>
+SIPG_OP2_HD void fvmf_2d_op1(const double *geof, const double *factor, double *op1) {
+  detail::volume_block<2, ORDER>(geof, factor, op1);
+}
+template <int ORDER>
+SIPG_OP2_HD void fvmf_3d_op1_diag(const double *geof, const double *factor, double *diag) {
+  detail::volume_diag<3, ORDER>(geof, factor, diag);
+}
+template <int ORDER>
+SIPG_OP2_HD void fvmf_2d_op1_diag(const double *geof, const double *factor, double *diag) {
+  detail::volume_diag<2, ORDER>(geof, factor, diag);
+}
+
+template <int ORDER>
+SIPG_OP2_HD void fvmf_3d_op2_diag(const int *faceNum, const int *fmaskL_corrected, const int *fmaskR_corrected,
+                                  const double *nx, const double *ny, const double *nz, const double *fscale,
+                                  const double *sJ, const double **geof, const double **factor, double *diagL,
+                                  double *diagR) {
+  (void)fmaskL_corrected;  // the reference takes the left side's nodes from FMASK
+  const double *n[3] = {nx, ny, nz};
+  detail::face_pair<3, ORDER>(faceNum, fmaskR_corrected, n, fscale, sJ, geof, factor, diagL, diagR, false);
+}
+template <int ORDER>
+SIPG_OP2_HD void fvmf_3d_op2_block_diag(const int *faceNum, const int *fmaskL_corrected, const int *fmaskR_corrected,
+                                        const double *nx, const double *ny, const double *nz, const double *fscale,
+                                        const double *sJ, const double **geof, const double **factor, double *op1L,
+                                        double *op1R) {
+  (void)fmaskL_corrected;
+  const double *n[3] = {nx, ny, nz};
+  detail::face_pair<3, ORDER>(faceNum, fmaskR_corrected, n, fscale, sJ, geof, factor, op1L, op1R, true);
+}
+
+namespace detail {
+// 2D: the right side's nodes are its face's nodes, reversed when *reverse
+template <int ORDER>
+SIPG_OP2_HD void fmask_2d_right(const int *faceNum, const bool *reverse, int *fmaskR) {
+  using G = Dg<2, ORDER>;
+  const int *fR = ref_tables<2, ORDER>().fmask + faceNum[1] * G::NPF;
+  for (int j = 0; j < G::NPF; ++j) fmaskR[j] = fR[*reverse ? G::NPF - 1 - j : j];
+}
+}  // namespace detail
+
+template <int ORDER>
+SIPG_OP2_HD void fvmf_2d_op2_diag(const int *faceNum, const bool *reverse, const double *nx, const double *ny,
+                                  const double *fscale, const double *sJ, const double **geof, const double **factor,
+                                  double *diagL, double *diagR) {
+  int fmaskR[Dg<2, ORDER>::NPF];
+  detail::fmask_2d_right<ORDER>(faceNum, reverse, fmaskR);
+  const double *n[3] = {nx, ny, nullptr};
+  detail::face_pair<2, ORDER>(faceNum, fmaskR, n, fscale, sJ, geof, factor, diagL, diagR, false);
+}
+template <int ORDER>
+SIPG_OP2_HD void fvmf_2d_op2_block_diag(const int *faceNum, const bool *reverse, const double *nx, const double *ny,
+                                        const double *fscale, const double *sJ, const double **geof,
+                                        const double **factor, double *op1L, double *op1R) {
+  int fmaskR[Dg<2, ORDER>::NPF];
+  detail::fmask_2d_right<ORDER>(faceNum, reverse, fmaskR);
+  const double *n[3] = {nx, ny, nullptr};
+  detail::face_pair<2, ORDER>(faceNum, fmaskR, n, fscale, sJ, geof, factor, op1L, op1R, true);
+}
+
+template <int ORDER>
+SIPG_OP2_HD void fvmf_3d_bop_diag(const int *faceNum, const int *u_bc_type, const int *v_bc_type,
+                                  const int *w_bc_type, const double *nx, const double *ny, const double *nz,
+                                  const double *fscale, const double *sJ, const double *geof, const double *factor,
+                                  double *u_diag, double *v_diag, double *w_diag) {
+  const int *bc[3] = {u_bc_type, v_bc_type, w_bc_type};
+  const double *n[3] = {nx, ny, nz};
+  double *out[3] = {u_diag, v_diag, w_diag};
+  detail::face_bnd<3, ORDER>(faceNum, bc, n, fscale, sJ, geof, factor, out, false);
+}
+template <int ORDER>
+SIPG_OP2_HD void fvmf_3d_bop_block_diag(const int *faceNum, const int *u_bc_type, const int *v_bc_type,
+                                        const int *w_bc_type, const double *nx, const double *ny, const double *nz,
+                                        const double *fscale, const double *sJ, const double *geof,
+                                        const double *factor, double *u_op1, double *v_op1, double *w_op1) {
+  const int *bc[3] = {u_bc_type, v_bc_type, w_bc_type};
+  const double *n[3] = {nx, ny, nz};
+  double *out[3] = {u_op1, v_op1, w_op1};
+  detail::face_bnd<3, ORDER>(faceNum, bc, n, fscale, sJ, geof, factor, out, true);
+}
+template <int ORDER>
+SIPG_OP2_HD void fvmf_2d_bop_diag(const int *faceNum, const int *u_bc_type, const int *v_bc_type, const double *nx,
+                                  const double *ny, const double *fscale, const double *sJ, const double *geof,
+                                  const double *factor, double *u_diag, double *v_diag) {
+  const int *bc[2] = {u_bc_type, v_bc_type};
+  const double *n[2] = {nx, ny};
+  double *out[2] = {u_diag, v_diag};
+  detail::face_bnd<2, ORDER>(faceNum, bc, n, fscale, sJ, geof, factor, out, false);
+}
+template <int ORDER>
+SIPG_OP2_HD void fvmf_2d_bop_block_diag(const int *faceNum, const int *u_bc_type, const int *v_bc_type,
+                                        const double *nx, const double *ny, const double *fscale, const double *sJ,
+                                        const double *geof, const double *factor, double *u_op1, double *v_op1) {
+  const int *bc[2] = {u_bc_type, v_bc_type};
+  const double *n[2] = {nx, ny};
+  double *out[2] = {u_op1, v_op1};
+  detail::face_bnd<2, ORDER>(faceNum, bc, n, fscale, sJ, geof, factor, out, true);
+}
+
+// ---------------------------------------------------------------- boundary lifting of the right-hand side (apply_bc)
+
+template <int ORDER>
+SIPG_OP2_HD void fvmf_3d_apply_bc(const int *faceNum, const int *u_bc_type, const int *v_bc_type,
+                                  const int *w_bc_type, const double *nx, const double *ny, const double *nz,
+                                  const double *fscale, const double *sJ, const double *geof, const double *fact,
+                                  const double *u_bc, const double *v_bc, const double *w_bc, double *u_rhs,
+                                  double *v_rhs, double *w_rhs) {
+  const int *bc[3] = {u_bc_type, v_bc_type, w_bc_type};
+  const double *n[3] = {nx, ny, nz};
+  const double *g[3] = {u_bc, v_bc, w_bc};
+  double *rhs[3] = {u_rhs, v_rhs, w_rhs};
+  detail::lift_bc<3, ORDER>(faceNum, bc, n, fscale, sJ, geof, fact, g, rhs);
+}
+template <int ORDER>
+SIPG_OP2_HD void vmf_3d_apply_bc(const int *faceNum, const int *u_bc_type, const int *v_bc_type, const int *w_bc_type,
+                                 const double *nx, const double *ny, const double *nz, const double *fscale,
+                                 const double *sJ, const double *geof, const double *u_bc, const double *v_bc,
+                                 const double *w_bc, double *u_rhs, double *v_rhs, double *w_rhs) {
+  const int *bc[3] = {u_bc_type, v_bc_type, w_bc_type};
+  const double *n[3] = {nx, ny, nz};
+  const double *g[3] = {u_bc, v_bc, w_bc};
+  double *rhs[3] = {u_rhs, v_rhs, w_rhs};
+  detail::lift_bc<3, ORDER>(faceNum, bc, n, fscale, sJ, geof, nullptr, g, rhs);
+}
+template <int ORDER>
+SIPG_OP2_HD void fvmf_2d_apply_bc(const int *faceNum, const int *u_bc_type, const int *v_bc_type, const double *nx,
+                                  const double *ny, const double *fscale, const double *sJ, const double *geof,
+                                  const double *factor, const double *u_bc, const double *v_bc, double *u_rhs,
+                                  double *v_rhs) {
+  const int *bc[2] = {u_bc_type, v_bc_type};
+  const double *n[2] = {nx, ny};
+  const double *g[2] = {u_bc, v_bc};
+  double *rhs[2] = {u_rhs, v_rhs};
+  detail::lift_bc<2, ORDER>(faceNum, bc, n, fscale, sJ, geof, factor, g, rhs);
+}
+template <int ORDER>
+SIPG_OP2_HD void vmf_2d_apply_bc(const int *faceNum, const int *u_bc_type, const int *v_bc_type, const double *nx,
+                                 const double *ny, const double *fscale, const double *sJ, const double *geof,
+                                 const double *u_bc, const double *v_bc, double *u_rhs, double *v_rhs) {
+  const int *bc[2] = {u_bc_type, v_bc_type};
+  const double *n[2] = {nx, ny};
+  const double *g[2] = {u_bc, v_bc};
+  double *rhs[2] = {u_rhs, v_rhs};
+  detail::lift_bc<2, ORDER>(faceNum, bc, n, fscale, sJ, geof, nullptr, g, rhs);
 }
 
 }  // namespace op2

@@ -82,12 +82,7 @@ def ref_names(dim):
         return [l.split('"')[1][:-2] for l in f if l.startswith("#include")]
 
 
-@pytest.fixture(scope="module")
-def libs(tmp_path_factory):
-    if not O.have_ref():
-        pytest.skip("oracle/_ref not built (the reference tree is not available)")
-    ours = header_kernels()
-    d = tmp_path_factory.mktemp("op2")
+def build_lib(d, ours, defines=()):
     lines = []
     for dim in (2, 3):
         for p in (1, 2, 3, 4):
@@ -101,9 +96,19 @@ def libs(tmp_path_factory):
             lines.append("  return -1;\n}")
     (d / "op2_dispatch.inc").write_text("\n".join(lines) + "\n")
     so = d / "libop2k.so"
-    subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", f"-I{d}", LIB_SRC, "-o", str(so)], check=True)
-    mine = C.CDLL(str(so))
-    mine.op2_kernel.restype = C.c_int
+    subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", f"-I{d}", *defines, LIB_SRC, "-o", str(so)],
+                   check=True)
+    lib = C.CDLL(str(so))
+    lib.op2_kernel.restype = C.c_int
+    return lib
+
+
+@pytest.fixture(scope="module")
+def libs(tmp_path_factory):
+    if not O.have_ref():
+        pytest.skip("oracle/_ref not built (the reference tree is not available)")
+    ours = header_kernels()
+    mine = build_lib(tmp_path_factory.mktemp("op2"), ours)
     ref = O.ref_lib()
     ref.ref_kernel.restype = C.c_int
     return ours, mine, ref
@@ -119,8 +124,9 @@ def table_mesh(dim, order):
     return t, O.OMesh(t, e)
 
 
-def make_args(name, args, t, rng):
-    """One random set of arguments; returns (list of numpy objects or lists, outputs to compare)."""
+def make_args(name, args, t, rng, bc_mode=None):
+    """One random set of arguments: (kind, values, const) per argument. bc_mode
+    0 / 1 / 2 gives every component that boundary type, None random types."""
     dim, Np, Nfp, Nf = t["dim"], t["Np"], t["Nfp"], t["Nf"]
     ng = 10 if dim == 3 else 5
     fL, fR = int(rng.integers(Nf)), int(rng.integers(Nf))
@@ -134,7 +140,7 @@ def make_args(name, args, t, rng):
             if an == "faceNum":
                 v = [fL, fR] if name in PAIR else [fL]
             elif an.endswith("bc_type"):
-                v = [int(rng.integers(3))]
+                v = [int(rng.integers(3)) if bc_mode is None else bc_mode]
             elif an in ("fmaskR_corrected", "fmaskL_corrected"):
                 v = list(t["fmask"][fR if an == "fmaskR_corrected" else fL])
                 if rng.integers(2):
@@ -155,7 +161,9 @@ def make_args(name, args, t, rng):
                 n = Nf
             elif "jump" in an or "avg" in an or (name == "zero_npf_3"):
                 n = Nf * Nfp
-            elif an in MATS or name == "copy_dg_np_mat":
+            elif an.endswith("_bc"):
+                n = Nfp
+            elif an in MATS or an.endswith("_op1") or name == "copy_dg_np_mat":
                 n = Np * Np
             else:
                 n = Np
@@ -188,7 +196,7 @@ def test_every_provided_kernel_has_the_reference_argument_list(libs):
                 continue
             assert ours[name][1] == ref_signature(dim, 3, name), name
             checked += 1
-    assert checked >= 60
+    assert checked == 80  # 40 kernels of each build, the shared ones counted in both
 
 
 @pytest.mark.parametrize("dim,order", [(2, 1), (2, 2), (2, 3), (2, 4), (3, 1), (3, 2), (3, 3), (3, 4)])
@@ -197,10 +205,11 @@ def test_kernels_match_the_reference_kernels(libs, dim, order):
     t, om = table_mesh(dim, order)
     rng = np.random.default_rng(100 * dim + order)
     names = [n for n in ref_names(dim) if n in ours]
-    assert len(names) >= 30
+    assert len(names) == 40
     for name in names:
         for trial in range(6):
-            vals = make_args(name, ours[name][1], t, rng)
+            # Dirichlet, Neumann and slip on every component, then random mixes
+            vals = make_args(name, ours[name][1], t, rng, bc_mode=trial if trial < 3 else None)
             ka, pa = pointers(vals)
             kb, pb = pointers(vals)
             assert mine.op2_kernel(C.byref(om.s), name.encode(), pa) == 0, name
@@ -213,3 +222,77 @@ def test_kernels_match_the_reference_kernels(libs, dim, order):
                 for u, v in zip(xa, xb):
                     scale = max(1.0, float(np.abs(v).max()))
                     assert np.abs(u - v).max() <= 1e-13 * scale, (name, trial)
+
+
+def test_corrected_forms_without_the_reference_quirks(tmp_path):
+    """SIPG_OP2_REF_QUIRKS=0: the volume block is J sum_d D_d^T M F D_d and the
+    constant-coefficient flux keeps the n_z term of n . {grad u}."""
+    ours = header_kernels()
+    lib = build_lib(tmp_path, ours, ("-DSIPG_OP2_REF_QUIRKS=0",))
+    rng = np.random.default_rng(5)
+    for dim, order in ((2, 3), (3, 2)):
+        t, om = table_mesh(dim, order)
+        Np, Nfp, Nf = t["Np"], t["Nfp"], t["Nf"]
+        geof = rng.uniform(0.5, 1.5, 10 if dim == 3 else 5)
+        f = rng.uniform(0.5, 1.5, Np)
+        op1 = np.zeros(Np * Np)
+        keep, args = pointers([("d", geof, True), ("d", f, True), ("d", op1, False)])
+        assert lib.op2_kernel(C.byref(om.s), f"fvmf_{dim}d_op1".encode(), args) == 0
+        G = geof[:dim * dim].reshape(dim, dim)
+        Dref = [t["Dr"], t["Ds"], t["Dt"]][:dim]
+        want = np.zeros((Np, Np))
+        for d in range(dim):
+            Dd = sum(G[r, d] * Dref[r] for r in range(dim))
+            want += Dd.T @ t["M"] @ np.diag(f) @ Dd
+        want *= geof[dim * dim]
+        got = keep[2].reshape(Np, Np).T  # column-major
+        assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
+    t, om = table_mesh(3, 2)
+    Nf, Nfp = t["Nf"], t["Nfp"]
+    n = [rng.uniform(-1, 1, Nf) for _ in range(3)]
+    sJ, tau = rng.uniform(0.5, 1.5, Nf), rng.uniform(0.5, 1.5, Nf)
+    jump = rng.uniform(-1, 1, Nf * Nfp)
+    avg = [rng.uniform(-1, 1, Nf * Nfp) for _ in range(3)]
+    bufs = [("d", n[0], True), ("d", n[1], True), ("d", n[2], True), ("d", sJ, True), ("d", tau, True)]
+    for c in range(3):
+        bufs += [("d", jump.copy(), False)] + [("d", a.copy(), False) for a in avg]
+    keep, args = pointers(bufs)
+    assert lib.op2_kernel(C.byref(om.s), b"vmf_3d_mult_flux", args) == 0
+    fi = np.repeat(np.arange(Nf), Nfp)
+    s_full = n[0][fi] * avg[0] + n[1][fi] * avg[1] + n[2][fi] * avg[2]
+    want = sJ[fi] * (tau[fi] * 0.5 * jump - s_full)
+    assert np.abs(keep[5] - want).max() <= 1e-13
+
+
+def test_kernels_compile_into_a_device_kernel(tmp_path):
+    """The header's kernels are __host__ __device__: a CUDA kernel that calls them
+    (per element, tables in device memory) compiles for sm_100a."""
+    src = tmp_path / "op2_device.cu"
+    src.write_text(f"""
+#include "{HEADER}"
+namespace op2 = ins_solver_b200::op2;
+__device__ op2::RefTables g_tables;
+namespace ins_solver_b200 {{ namespace op2 {{
+template <> __host__ __device__ const RefTables& ref_tables<3, 3>() {{
+#ifdef __CUDA_ARCH__
+  return g_tables;
+#else
+  static RefTables h{{}};
+  return h;
+#endif
+}}
+}} }}
+__global__ void cells(const double* geof, const double* f, double* op1, double* diag, double* r, const double* Ap,
+                      double* res) {{
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  op2::fvmf_3d_op1<3>(geof + 10 * e, f + 20 * e, op1 + 400 * e);
+  op2::fvmf_3d_op1_diag<3>(geof + 10 * e, f + 20 * e, diag + 20 * e);
+  const double alpha = 0.5;
+  op2::cg3_update_res<3>(&alpha, res + e, Ap + 60 * e, Ap + 60 * e + 20, Ap + 60 * e + 40, r + 60 * e,
+                         r + 60 * e + 20, r + 60 * e + 40);
+}}
+""")
+    out = tmp_path / "op2_device.o"
+    subprocess.run(["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-std=c++17", "-c", str(src), "-o",
+                    str(out)], check=True)
+    assert out.stat().st_size > 0
