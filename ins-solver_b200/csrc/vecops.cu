@@ -533,6 +533,40 @@ __global__ void k_restrict(T* rc, const T* r, const T* P, int K, int Npf, int Np
   }
 }
 
+// Fixed-size transfers: P (Npf x Npc) in shared memory, loops unrolled.
+template <typename T, int NPF, int NPC>
+__global__ void k_restrict_n(T* rc, const T* __restrict__ r, const T* __restrict__ P, size_t total) {
+  __shared__ T sP[NPF * NPC];
+  for (int i = threadIdx.x; i < NPF * NPC; i += blockDim.x) sP[i] = P[i];  // set-up data
+  __syncthreads();
+  pdl_enter();
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t be = i / NPC;
+    const int j = (int)(i - be * NPC);
+    const T* rb = r + be * NPF;
+    T s = T(0);
+#pragma unroll
+    for (int k = 0; k < NPF; ++k) s += sP[k * NPC + j] * rb[k];
+    rc[i] = s;
+  }
+}
+template <typename T, int NPF, int NPC>
+__global__ void k_prolong_add_n(T* z, const T* __restrict__ zc, const T* __restrict__ P, size_t total) {
+  __shared__ T sP[NPF * NPC];
+  for (int i = threadIdx.x; i < NPF * NPC; i += blockDim.x) sP[i] = P[i];  // set-up data
+  __syncthreads();
+  pdl_enter();
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t be = i / NPF;
+    const int k = (int)(i - be * NPF);
+    const T* zb = zc + be * NPC;
+    T s = T(0);
+#pragma unroll
+    for (int j = 0; j < NPC; ++j) s += sP[k * NPC + j] * zb[j];
+    z[i] += s;
+  }
+}
+
 template <typename T>
 __global__ void k_prolong_add(T* z, const T* zc, const T* P, int K, int Npf, int Npc, int ncomp) {
   pdl_enter();
@@ -840,12 +874,26 @@ void inv_mass(T* y, const T* x, const T* Minv, const T* geof, int ngeof, int jid
 }
 template <typename T>
 void restrict_elem(T* rc, const T* r, const T* P, int K, int Npf, int Npc, int ncomp, cudaStream_t s) {
-  pdl_launch(k_restrict<T>, dim3(grid_for((size_t)ncomp * K * Npc)), dim3(256), 0, s, rc, r, P, K, Npf, Npc, ncomp);
+  const size_t total = (size_t)ncomp * K * Npc;
+  const dim3 g(grid_for(total)), b(256);
+  if (Npf == 20 && Npc == 10) pdl_launch(k_restrict_n<T, 20, 10>, g, b, 0, s, rc, r, P, total);
+  else if (Npf == 10 && Npc == 4) pdl_launch(k_restrict_n<T, 10, 4>, g, b, 0, s, rc, r, P, total);
+  else if (Npf == 20 && Npc == 4) pdl_launch(k_restrict_n<T, 20, 4>, g, b, 0, s, rc, r, P, total);
+  else if (Npf == 10 && Npc == 6) pdl_launch(k_restrict_n<T, 10, 6>, g, b, 0, s, rc, r, P, total);
+  else if (Npf == 6 && Npc == 3) pdl_launch(k_restrict_n<T, 6, 3>, g, b, 0, s, rc, r, P, total);
+  else pdl_launch(k_restrict<T>, g, b, 0, s, rc, r, P, K, Npf, Npc, ncomp);
   note_launch();
 }
 template <typename T>
 void prolong_add(T* z, const T* zc, const T* P, int K, int Npf, int Npc, int ncomp, cudaStream_t s) {
-  pdl_launch(k_prolong_add<T>, dim3(grid_for((size_t)ncomp * K * Npf)), dim3(256), 0, s, z, zc, P, K, Npf, Npc, ncomp);
+  const size_t total = (size_t)ncomp * K * Npf;
+  const dim3 g(grid_for(total)), b(256);
+  if (Npf == 20 && Npc == 10) pdl_launch(k_prolong_add_n<T, 20, 10>, g, b, 0, s, z, zc, P, total);
+  else if (Npf == 10 && Npc == 4) pdl_launch(k_prolong_add_n<T, 10, 4>, g, b, 0, s, z, zc, P, total);
+  else if (Npf == 20 && Npc == 4) pdl_launch(k_prolong_add_n<T, 20, 4>, g, b, 0, s, z, zc, P, total);
+  else if (Npf == 10 && Npc == 6) pdl_launch(k_prolong_add_n<T, 10, 6>, g, b, 0, s, z, zc, P, total);
+  else if (Npf == 6 && Npc == 3) pdl_launch(k_prolong_add_n<T, 6, 3>, g, b, 0, s, z, zc, P, total);
+  else pdl_launch(k_prolong_add<T>, g, b, 0, s, z, zc, P, K, Npf, Npc, ncomp);
   note_launch();
 }
 template <typename T>
