@@ -966,6 +966,11 @@ int sipg_solver::solve(const double* b, double* x_user, sipg_solve_info* info) {
         // z to FP64, projection, r . z_new
         if (o.nullspace) to_f64_sum(Z, lv[0].z.as<float>(), n, S() + S_SUM, rw, stream);
         finish_z_dot(Z, o.nullspace ? nullptr : lv[0].z.as<float>(), R, n, S(), mean_slot, S() + S_RZN, rw, stream);
+      } else if (!o.nullspace && (kind == SIPG_SOLVER_JACOBI || kind == SIPG_SOLVER_BLOCK_JACOBI)) {
+        // update_ans + update_res with r . r and r . z_old; z = M^-1 r with r . z_new
+        cg_update_xr_rzo(x, R, Pv, AP, Z, n, S(), S_RZ, S_PAP, S() + S_RR, S_RZO - S_RR, rw, stream);
+        if (kind == SIPG_SOLVER_JACOBI) precond_dot(Z, R, dinv.as<double>(), 0, n, S() + S_RZN, rw, stream);
+        else precond_dot(Z, R, blocks.as<double>(), op->Np, n, S() + S_RZN, rw, stream);
       } else {
         cg_update_xr(x, R, Pv, AP, n, S(), S_RZ, S_PAP, S() + S_RR, rw, stream);  // update_ans + update_res
         if (o.nullspace) {

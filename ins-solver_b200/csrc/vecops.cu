@@ -213,6 +213,52 @@ __global__ void __launch_bounds__(kRedThreads) k_finish_z_dot(double* z, const f
   finish<1>(v, partial, counter, out, 1);
 }
 
+// x += alpha p ; r -= alpha Ap ; out[0] = r . r, out[stride] = r . zo
+__global__ void __launch_bounds__(kRedThreads) k_cg_update_xr_rzo(double* x, double* r, const double* p,
+                                                                  const double* Ap, const double* zo, size_t n,
+                                                                  const double* scal, int num, int den,
+                                                                  double* partial, unsigned* counter, double* out,
+                                                                  int stride) {
+  pdl_enter();
+  const double alpha = scal[num] / scal[den];
+  double v[2] = {0.0, 0.0};
+#pragma unroll 4
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    x[i] += alpha * p[i];
+    double ri = r[i] - alpha * Ap[i];
+    r[i] = ri;
+    v[0] += ri * ri;
+    v[1] += ri * zo[i];
+  }
+  block_sum<2>(v);
+  finish<2>(v, partial, counter, out, stride);
+}
+
+// z = B r (row-major blocks; point Jacobi z = dinv r when Np == 0) ; out = r . z
+__global__ void __launch_bounds__(kRedThreads) k_precond_dot(double* z, const double* r, const double* B, int Np,
+                                                             size_t n, double* partial, unsigned* counter,
+                                                             double* out) {
+  pdl_enter();
+  double v[1] = {0.0};
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    double zi;
+    if (Np > 0) {
+      const size_t b = i / Np;
+      const int row = (int)(i - b * Np);
+      const double* Bb = B + (b * Np + row) * Np;
+      const double* rb = r + b * Np;
+      zi = 0.0;
+      for (int j = 0; j < Np; ++j) zi += Bb[j] * rb[j];
+    } else {
+      zi = B[i] * r[i];
+    }
+    z[i] = zi;
+    v[0] += r[i] * zi;
+  }
+  block_sum<1>(v);
+  finish<1>(v, partial, counter, out, 1);
+}
+
 template <typename T>
 __global__ void k_update_p(T* p, const T* z, size_t n, const double* scal, int num, int den) {
   pdl_enter();
@@ -737,6 +783,18 @@ void cg_update_xr_sum(double* x, double* r, const double* p, const double* Ap, s
                       int den, double* out, int stride, const RedWork& w, cudaStream_t s) {
   pdl_launch(k_cg_update_xr_sum, dim3(red_grid(n)), dim3(kRedThreads), 0, s, x, r, p, Ap, n, scal, num, den, w.partial,
              w.counter, out, stride);
+  note_launch();
+}
+void cg_update_xr_rzo(double* x, double* r, const double* p, const double* Ap, const double* zo, size_t n,
+                      const double* scal, int num, int den, double* out, int stride, const RedWork& w,
+                      cudaStream_t s) {
+  pdl_launch(k_cg_update_xr_rzo, dim3(red_grid(n)), dim3(kRedThreads), 0, s, x, r, p, Ap, zo, n, scal, num, den,
+             w.partial, w.counter, out, stride);
+  note_launch();
+}
+void precond_dot(double* z, const double* r, const double* B, int Np, size_t n, double* out, const RedWork& w,
+                 cudaStream_t s) {
+  pdl_launch(k_precond_dot, dim3(red_grid(n)), dim3(kRedThreads), 0, s, z, r, B, Np, n, w.partial, w.counter, out);
   note_launch();
 }
 void resid_prep(double* r, float* r32, const double* zo, size_t n, const double* scal, int mean_slot, double* out,

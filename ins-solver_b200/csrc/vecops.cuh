@@ -73,6 +73,13 @@ void cg_update_xr_sum(double* x, double* r, const double* p, const double* Ap, s
 //   r -= mean (scal[mean_slot] / n, none when mean_slot < 0) ; r32 = r ; out = (r . r, r . zo)
 void resid_prep(double* r, float* r32, const double* zo, size_t n, const double* scal, int mean_slot, double* out,
                 int stride, const RedWork& w, cudaStream_t s);
+//   x += alpha p ; r -= alpha Ap ; out = (r . r, r . zo)
+void cg_update_xr_rzo(double* x, double* r, const double* p, const double* Ap, const double* zo, size_t n,
+                      const double* scal, int num, int den, double* out, int stride, const RedWork& w,
+                      cudaStream_t s);
+//   z = B r (row-major Np x Np blocks; Np == 0: z = B r elementwise, point Jacobi) ; out = r . z
+void precond_dot(double* z, const double* r, const double* B, int Np, size_t n, double* out, const RedWork& w,
+                 cudaStream_t s);
 //   z = z32 ; out = sum z
 void to_f64_sum(double* z, const float* z32, size_t n, double* out, const RedWork& w, cudaStream_t s);
 //   z = (z32 ? z32 : z) - mean (as above) ; out = r . z
