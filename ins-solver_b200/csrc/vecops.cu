@@ -347,12 +347,22 @@ __global__ void __launch_bounds__(BT) k_cheb_sym(T* d, T* z, const T* __restrict
   pdl_enter();
   using C = Chunk<TB>;
   constexpr int LD = SymCfg<T, NP>::LD;
+  constexpr int NK = (NP * (NP + 1) / 2 + C::CH - 1) / C::CH;  // 16-byte chunks per block
+  // the first PF chunks (at most 56 registers) are requested before the staging
+  // loads, so that their latency overlaps; the rest are read during the products
+  constexpr int PF = NK < 14 ? NK : 14;
   __shared__ T sr[BT * LD], sd[BT * LD], sz[BT * LD];
   const int tid = threadIdx.x;
   const bool use_d = c1 != T(0);
   for (size_t e0 = (size_t)blockIdx.x * BT; e0 < (size_t)nb; e0 += (size_t)gridDim.x * BT) {
     const int ne = (size_t)nb - e0 < (size_t)BT ? (int)((size_t)nb - e0) : BT;
     const size_t g0 = e0 * NP;
+    const uint4* pb = reinterpret_cast<const uint4*>(P) + e0 + tid;
+    uint4 qa[PF];
+    if (tid < ne) {
+#pragma unroll
+      for (int k = 0; k < PF; ++k) qa[k] = pb[(size_t)k * nb];
+    }
     if (ne == BT) {  // full group: every load issued back to back
 #pragma unroll
       for (int k = 0; k < NP; ++k) {
@@ -371,12 +381,10 @@ __global__ void __launch_bounds__(BT) k_cheb_sym(T* d, T* z, const T* __restrict
     }
     __syncthreads();
     if (tid < ne) {
-      const size_t b = e0 + tid;
       const T* rr = sr + tid * LD;
       T y[NP];
 #pragma unroll
       for (int i = 0; i < NP; ++i) y[i] = T(0);
-      const uint4* pb = reinterpret_cast<const uint4*>(P) + b;
       uint4 q = make_uint4(0u, 0u, 0u, 0u);
 #pragma unroll
       for (int c = 0; c < NP; ++c) {
@@ -384,7 +392,8 @@ __global__ void __launch_bounds__(BT) k_cheb_sym(T* d, T* z, const T* __restrict
 #pragma unroll
         for (int k = 0; k <= c; ++k) {
           const int t = c * (c + 1) / 2 + k;
-          if (t % C::CH == 0) q = pb[(size_t)(t / C::CH) * nb];
+          if (t / C::CH < PF) q = qa[t / C::CH < PF ? t / C::CH : 0];
+          else if (t % C::CH == 0) q = pb[(size_t)(t / C::CH) * nb];
           const T v = (T)C::at(q, t % C::CH);
           y[k] += v * rc;
           if (k != c) y[c] += v * rr[k];
