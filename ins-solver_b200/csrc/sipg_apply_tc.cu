@@ -346,7 +346,9 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_trace_kernel(ApplyArgs<T> 
   T* sout = sfg + X::SFG;
   const int ntiles = (a.K + TE - 1) / TE;
   const int stride = gridDim.x * WARPS;
-  int tile = blockIdx.x * WARPS + warp;
+  // warp-major tile order: the last, partial round of tiles is spread over all
+  // CTAs (SMs) instead of filling the first ones
+  int tile = warp * gridDim.x + blockIdx.x;
   pdl_trigger();
   for (int i = lane; i < X::W1_T; i += 32) W[i] = T(0);  // row and record padding stays zero
   for (int i = threadIdx.x; i < X::N1; i += blockDim.x) BFs[i] = blob[X::BF + i];
@@ -469,7 +471,9 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_apply_tc_kernel(ApplyArgs<
   T* sfg = W + L::SFGO;
   const int ntiles = (a.K + TE - 1) / TE;
   const int stride = gridDim.x * WARPS;
-  int tile = blockIdx.x * WARPS + warp;
+  // warp-major tile order: the last, partial round of tiles is spread over all
+  // CTAs (SMs) instead of filling the first ones
+  int tile = warp * gridDim.x + blockIdx.x;
   pdl_trigger();
   for (int i = lane; i < L::T_; i += 32) W[i] = T(0);  // row padding stays zero
   __syncwarp();
