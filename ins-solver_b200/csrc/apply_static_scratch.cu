@@ -88,6 +88,7 @@ ApplyArgs<T> args_of(const sipg_op* op, const T* x, T* y) {
   a.alpha = T(1);
   a.beta = T(0);
   a.c = y;
+  a.tcg = f64 ? (const T*)op->mesh->tcg64.p : (const T*)op->mesh->tcg32.p;
   return a;
 }
 

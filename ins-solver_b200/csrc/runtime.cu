@@ -174,6 +174,11 @@ void sipg_mesh::ensure_device() {
   n_belem = (int)be.size();
   belems = DevBuf(std::max<size_t>(1, be.size()) * sizeof(int));
   if (!be.empty()) belems.upload(be.data(), be.size() * sizeof(int));
+  tcg64 = DevBuf(tc_geom_values<double>(dim, K) * sizeof(double));
+  tcg32 = DevBuf(tc_geom_values<float>(dim, K) * sizeof(float));
+  SIPG_CUDA(launch_tc_geom<double>(dim, geof64.as<double>(), K, tcg64.as<double>(), 0));
+  SIPG_CUDA(launch_tc_geom<float>(dim, geof32.as<float>(), K, tcg32.as<float>(), 0));
+  SIPG_CUDA(cudaDeviceSynchronize());
   device_ready = true;
 }
 
@@ -204,6 +209,7 @@ void sipg_op::apply(const T* x, T* y, cudaStream_t s, T alpha, T beta, const T* 
   a.alpha = alpha;
   a.beta = beta;
   a.c = c ? c : y;
+  a.tcg = f64 ? (const T*)mesh->tcg64.p : (const T*)mesh->tcg32.p;
   const bool tc = kernel == 0 && ncomp == 1 && (f64 ? dref->tc_ok64 : dref->tc_ok32);
   if (tc) {
     const T* tcc = f64 ? (const T*)dref->tc64.p : (const T*)dref->tc32.p;
@@ -454,7 +460,8 @@ int sipg_mesh_export(const sipg_mesh* mc, int order, double* geof, double* nx, d
 
 int sipg_mesh_device_bytes(const sipg_mesh* m, size_t* bytes) {
   return guarded([&] {
-    *bytes = m->geof64.bytes + m->geof32.bytes + m->nbr.bytes + m->fcode.bytes + m->belems.bytes;
+    *bytes = m->geof64.bytes + m->geof32.bytes + m->nbr.bytes + m->fcode.bytes + m->belems.bytes +
+             m->tcg64.bytes + m->tcg32.bytes;
   });
 }
 

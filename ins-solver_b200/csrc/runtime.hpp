@@ -62,6 +62,7 @@ struct sipg_mesh {
   std::map<int, sipg::Mesh> host;  // per-order host tables (lazily built)
   std::mutex host_mu;
   sipg::DevBuf geof64, geof32, nbr, fcode, belems;
+  sipg::DevBuf tcg64, tcg32;  // geometry blocks of the tensor-core apply (launch_tc_geom)
   int n_belem = 0;
   bool device_ready = false;
   std::mutex dev_mu;

@@ -76,6 +76,7 @@ struct ApplyArgs {
   int eb;                 // elements per CTA batch
   T alpha, beta;          // y = alpha * A x + beta * c (beta == 0: c is not read)
   const T* c;             // ncomp x K x NP; y unless the caller gives another vector
+  const T* tcg;           // tensor-core path: tile-major element and face geometry (launch_tc_geom)
 };
 
 // Host-side launchers (sipg_apply.cu).

@@ -96,7 +96,7 @@ __host__ __device__ constexpr int pad816(int n) { return n <= 8 ? 8 : rup(n - 8,
 template <typename T, int DIM, int P>
 struct Tc {
   using C = Cfg<DIM, P>;
-  static constexpr int NP = C::NP, NFP = C::NFP, NF = C::NF, NG = C::NG;
+  static constexpr int NP = C::NP, NFP = C::NFP, NF = C::NF;
   static constexpr int R = Frag<T>::R, TE = 8 * R;   // elements per warp tile
   static constexpr int NT = rup(NP, 8) / 8;          // node blocks
   static constexpr int KF = NF * NFP;                // face nodes of an element
@@ -117,26 +117,33 @@ struct Tc {
   static constexpr int TS = pad816(NF * TR);         // staged row stride of an element's trace records
   // copy piece of an x / factor row (rows start on multiples of Np values)
   static constexpr int XCB = (NP * (int)sizeof(T)) % 16 == 0 ? 16 : (NP * (int)sizeof(T)) % 8 == 0 ? 8 : 4;
-  // element stage (double-buffered; T units, every part a multiple of 64 bytes)
-  static constexpr int SX = 0, SF = TE * XS, SG = 2 * TE * XS, STAU = SG + TE * NG, ST2 = STAU + TE * NF;
-  static constexpr int ST1 = STAU;                   // pass 1: x, factor, geometry
-  static constexpr int NFG = 4;                      // per element face: sJ, c_r (3), stored [q][f][el]
+  // geometry block of a warp tile (launch_tc_geom), rows of TE values: NV volume
+  // rows (J, then the metric K = G G^T by rows of its upper triangle, zero rows),
+  // then NFG x NF face rows [q][f] (q: sJ, c_0, c_1, c_2)
+  static constexpr int NV = 8, NFG = 4, GROWS = NV + NFG * NF;
   static constexpr int SFG = NFG * NF * TE;
+  // element stage (T units, every part a multiple of 64 bytes): x, factor, then
+  // the face rows of the geometry block (pass 1) or the whole block and tau (pass 2)
+  static constexpr int SX = 0, SF = TE * XS, SG = 2 * TE * XS;
+  static constexpr int ST1 = SG + SFG;
+  static constexpr int STAU = SG + GROWS * TE, ST2 = STAU + TE * NF;
   static constexpr int SI = TE * NF + TE;            // int slot: nbr, face codes
-  // pass 1 warp: 2 stages, face geometry, output records
-  static constexpr int W1_T = 2 * ST1 + SFG + TE * TS;
+  // pass 1 warp: 2 stages, output records
+  static constexpr int W1_T = 2 * ST1 + TE * TS;
   static constexpr int W2_I = 3 * SI;
   static constexpr int CH = TR * (int)sizeof(T) / 16;  // 16-byte chunks per trace record
 };
 
 // Pass-2 warp area: NS element stages, own and neighbour trace records (one
-// buffer each), face geometry.
+// buffer each).
 template <typename T, int DIM, int P, int NS>
 struct W2 {
   using X = Tc<T, DIM, P>;
-  static constexpr int STR = NS * X::ST2, SNB = STR + X::TE * X::TS, SFGO = SNB + X::TE * X::TS,
-                       T_ = SFGO + X::SFG;
+  static constexpr int STR = NS * X::ST2, SNB = STR + X::TE * X::TS, T_ = SNB + X::TE * X::TS;
 };
+
+// Row of the metric entry K_rs (r <= s) in the geometry block.
+__host__ __device__ constexpr int kidx(int dim, int r, int s) { return 1 + r * dim - r * (r - 1) / 2 + (s - r); }
 
 template <typename T>
 __device__ __forceinline__ typename Frag<T>::V2 ldb(const T* blob, int blk, int lane) {
@@ -196,13 +203,19 @@ __device__ __forceinline__ void copy_rows(T* dst, const T* base, size_t row0, in
 template <typename T, int DIM, int P>
 __device__ __forceinline__ void issue_elem(const ApplyArgs<T>& a, T* st, int tile, int lane, bool pass2) {
   using X = Tc<T, DIM, P>;
-  constexpr int NP = X::NP, NG = X::NG, NF = X::NF, TE = X::TE, S = sizeof(T);
+  constexpr int NP = X::NP, NF = X::NF, TE = X::TE, S = sizeof(T);
   const int e0 = tile * TE;
   const int ne = max(0, min(TE, a.K - e0));
   copy_rows<T, X::XCB, NP, X::XS, TE>(st + X::SX, a.x, (size_t)e0, ne, lane, true);
   if (a.factor) copy_rows<T, X::XCB, NP, X::XS, TE>(st + X::SF, a.factor, (size_t)e0, ne, lane, true);
-  copy_block(st + X::SG, a.geof, (size_t)e0 * NG * S, TE * NG * S, ne * NG * S, lane);
-  if (pass2) copy_block(st + X::STAU, a.tau, (size_t)e0 * NF * S, TE * NF * S, ne * NF * S, lane);
+  // the geometry block is zero past K, so a started tile copies it whole
+  const size_t gb = (size_t)tile * X::GROWS * TE * S;
+  if (pass2) {
+    copy_block(st + X::SG, a.tcg, gb, X::GROWS * TE * S, ne > 0 ? X::GROWS * TE * S : 0, lane);
+    copy_block(st + X::STAU, a.tau, (size_t)e0 * NF * S, TE * NF * S, ne * NF * S, lane);
+  } else {
+    copy_block(st + X::SG, a.tcg, gb + (size_t)X::NV * TE * S, X::SFG * S, ne > 0 ? X::SFG * S : 0, lane);
+  }
 }
 
 template <typename T, int DIM, int P>
@@ -293,20 +306,6 @@ __device__ __forceinline__ void face_geom(const T* g, int f, T& sJ, T (&c)[3]) {
   }
 }
 
-// Face geometry of a tile into sfg[q][f][el] (q: sJ, c_0, c_1, c_2; zeros for padded slots).
-template <typename T, int DIM, int P>
-__device__ __forceinline__ void tile_face_geom(const T* sg, T* sfg, int ne, int lane) {
-  using X = Tc<T, DIM, P>;
-  constexpr int NF = X::NF, TE = X::TE;
-  for (int i = lane; i < TE * NF; i += 32) {
-    const int el = i / NF, f = i % NF;
-    T sJ = T(0), c[3] = {T(0), T(0), T(0)};
-    if (el < ne) face_geom<T, DIM>(sg + el * X::NG, f, sJ, c);
-    sfg[f * TE + el] = sJ;
-#pragma unroll
-    for (int r = 0; r < 3; ++r) sfg[((1 + r) * NF + f) * TE + el] = c[r];
-  }
-}
 template <typename T, int DIM, int P>
 __device__ __forceinline__ T fgeo(const T* sfg, int q, int f, int el) {
   using X = Tc<T, DIM, P>;
@@ -342,8 +341,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_trace_kernel(ApplyArgs<T> 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
   T* W = BFs + X::N1 + warp * X::W1_T;
   int8_t* fmask = reinterpret_cast<int8_t*>(BFs + X::N1 + WARPS * X::W1_T);
-  T* sfg = W + 2 * X::ST1;
-  T* sout = sfg + X::SFG;
+  T* sout = W + 2 * X::ST1;
   const int ntiles = (a.K + TE - 1) / TE;
   const int stride = gridDim.x * WARPS;
   // warp-major tile order: the last, partial round of tiles is spread over all
@@ -368,8 +366,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_trace_kernel(ApplyArgs<T> 
     const int ne = min(TE, a.K - e0);
     T* sx = st + X::SX;
     const T* sf = st + X::SF;
+    const T* sfg = st + X::SG;  // face rows of the geometry block
     if (lane == 0 && a.pin_elem >= e0 && a.pin_elem < e0 + ne) sx[(a.pin_elem - e0) * XS + a.pin_node] = T(0);
-    tile_face_geom<T, DIM, P>(st + X::SG, sfg, ne, lane);
     __syncwarp();
     T u[NT][R][2];
     load_x_frags<T, DIM, P>(sx, u, g, t);
@@ -468,7 +466,6 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_apply_tc_kernel(ApplyArgs<
   const int8_t* perm = itab + NF * NFP;
   const T* str = W + L::STR;
   const T* snb = W + L::SNB;
-  T* sfg = W + L::SFGO;
   const int ntiles = (a.K + TE - 1) / TE;
   const int stride = gridDim.x * WARPS;
   // warp-major tile order: the last, partial round of tiles is spread over all
@@ -536,22 +533,20 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_apply_tc_kernel(ApplyArgs<
             yold[nt][ri][ci] = (el < ne && n < NP) ? a.c[(size_t)(e0 + el) * NP + n] : T(0);
           }
     }
-    tile_face_geom<T, DIM, P>(sg, sfg, ne, lane);
+    const T* sfg = sg + X::NV * TE;  // face rows of the geometry block
     __syncwarp();
 
     // metric of the lane's elements: J and K = G G^T
     T Jm[R], Km[R][DIM][DIM];
 #pragma unroll
     for (int ri = 0; ri < R; ++ri) {
-      const T* ge = sg + (g + 8 * ri) * X::NG;
-      Jm[ri] = ge[DIM * DIM];
+      const int el = g + 8 * ri;
+      Jm[ri] = sg[el];
 #pragma unroll
       for (int r = 0; r < DIM; ++r)
 #pragma unroll
         for (int s = r; s < DIM; ++s) {
-          T v = T(0);
-#pragma unroll
-          for (int d = 0; d < DIM; ++d) v += ge[r * DIM + d] * ge[s * DIM + d];
+          const T v = sg[kidx(DIM, r, s) * TE + el];
           Km[ri][r][s] = v;
           Km[ri][s][r] = v;
         }
@@ -796,6 +791,44 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_apply_tc_kernel(ApplyArgs<
   cp_wait_all();
 }
 
+// Geometry blocks of the tensor-core apply, one thread per element slot of a
+// warp tile: J, the metric K = G G^T and per face sJ and c_r = n . grad r (the
+// same arithmetic for every apply, so it is done once per mesh).
+template <typename T, int DIM, int TE>
+__global__ void k_tc_geom(const T* __restrict__ geof, int K, T* __restrict__ out) {
+  constexpr int NF = DIM + 1, NG = DIM == 3 ? 10 : 5, NV = 8, NFG = 4, GROWS = NV + NFG * NF;
+  const int ntiles = (K + TE - 1) / TE;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ntiles * TE; e += gridDim.x * blockDim.x) {
+    T v[GROWS];
+#pragma unroll
+    for (int i = 0; i < GROWS; ++i) v[i] = T(0);
+    if (e < K) {
+      const T* g = geof + (size_t)e * NG;
+      v[0] = g[DIM * DIM];
+#pragma unroll
+      for (int r = 0; r < DIM; ++r)
+#pragma unroll
+        for (int s = r; s < DIM; ++s) {
+          T k = T(0);
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) k += g[r * DIM + d] * g[s * DIM + d];
+          v[kidx(DIM, r, s)] = k;
+        }
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        T sJ, c[3];
+        face_geom<T, DIM>(g, f, sJ, c);
+        v[NV + f] = sJ;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) v[NV + (1 + r) * NF + f] = c[r];
+      }
+    }
+    T* o = out + (size_t)(e / TE) * GROWS * TE + e % TE;
+#pragma unroll
+    for (int i = 0; i < GROWS; ++i) o[(size_t)i * TE] = v[i];
+  }
+}
+
 constexpr int kSmemBudget = 227 * 1024;
 
 template <typename T, int DIM, int P>
@@ -950,6 +983,25 @@ int tc_warps_for(int dim, int order) {
   return 0;
 }
 
+template <typename T>
+size_t tc_geom_values(int dim, int K) {
+  constexpr int TE = 8 * Frag<T>::R;
+  const size_t ntiles = ((size_t)K + TE - 1) / TE;
+  return ntiles * TE * (8 + 4 * (dim + 1));
+}
+
+template <typename T>
+cudaError_t launch_tc_geom(int dim, const T* geof, int K, T* out, cudaStream_t s) {
+  constexpr int TE = 8 * Frag<T>::R;
+  const size_t n = ((size_t)K + TE - 1) / TE * TE;
+  const int grid = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
+  if (grid == 0) return cudaSuccess;
+  if (dim == 3) k_tc_geom<T, 3, TE><<<grid, 256, 0, s>>>(geof, K, out);
+  else if (dim == 2) k_tc_geom<T, 2, TE><<<grid, 256, 0, s>>>(geof, K, out);
+  else return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
 size_t tc_trace_values(int dim, int order, int K) {
   const int trp = rup(nfp_of(dim, order), 2);
   return (size_t)K * (dim + 1) * rup(2 * trp, 4);
@@ -963,5 +1015,9 @@ template void build_tc_consts<float>(int, int, const RefElement&, std::vector<do
 template void build_tc_consts<double>(int, int, const RefElement&, std::vector<double>&);
 template int tc_warps_for<float>(int, int);
 template int tc_warps_for<double>(int, int);
+template size_t tc_geom_values<float>(int, int);
+template size_t tc_geom_values<double>(int, int);
+template cudaError_t launch_tc_geom<float>(int, const float*, int, float*, cudaStream_t);
+template cudaError_t launch_tc_geom<double>(int, const double*, int, double*, cudaStream_t);
 
 }  // namespace sipg

@@ -23,5 +23,12 @@ void build_tc_consts(int dim, int order, const RefElement& r, std::vector<double
 // Warps per CTA of the apply pass (below 2: use the CUDA-core kernel).
 template <typename T>
 int tc_warps_for(int dim, int order);
+// Element and face geometry of the tensor-core apply (ApplyArgs::tcg), computed
+// once per mesh from the K x NG geometric factors: tc_geom_values<T>(dim, K)
+// values, one block per warp tile of elements (zero past K).
+template <typename T>
+size_t tc_geom_values(int dim, int K);
+template <typename T>
+cudaError_t launch_tc_geom(int dim, const T* geof, int K, T* out, cudaStream_t s);
 
 }  // namespace sipg
