@@ -54,11 +54,12 @@ template <>
 struct Frag<float> {
   static constexpr int R = 2;
   using V2 = float2;
-  __device__ static __forceinline__ float op(float x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return __uint_as_float(r);
-  }
+  // FP32 values go to the TF32 MMA as they are: the tensor core uses the sign,
+  // exponent and top 10 mantissa bits (truncation, relative error below 2^-10
+  // per operand instead of 2^-11 after a round-to-nearest conversion). Dropping
+  // the conversion instruction (about 160 per warp tile and lane at p = 3) left
+  // the iteration counts of the mixed-precision solves unchanged.
+  __device__ static __forceinline__ float op(float x) { return x; }
   // m16n8k8: a0 (g, t) a1 (g+8, t) a2 (g, t+4) a3 (g+8, t+4); b0 (t, g) b1 (t+4, g);
   // c0 (g, 2t) c1 (g, 2t+1) c2 (g+8, 2t) c3 (g+8, 2t+1).
   __device__ static __forceinline__ void mma(float (&c)[2][2], const float (&a)[2][2], V2 b) {
@@ -312,7 +313,21 @@ __device__ __forceinline__ T fgeo(const T* sfg, int q, int f, int el) {
   return sfg[(q * X::NF + f) * X::TE + el];
 }
 
-// A blocks of x (TF32-rounded on the FP32 path): u[kb][ri][ci] = x[g + 8 ri][8 kb + 2t + ci]
+// Zero the padding columns (Np .. XS-1) of the x and factor rows of `nst` element
+// stages `stride` values apart: the fragment loads read them and the copies never
+// write them. Nothing else in a warp area is read before it is written.
+template <typename T, int DIM, int P>
+__device__ __forceinline__ void zero_row_padding(T* W, int nst, int stride, int lane) {
+  using X = Tc<T, DIM, P>;
+  constexpr int PAD = X::XS - X::NP, TE = X::TE;
+  if (PAD == 0) return;
+  for (int i = lane; i < nst * 2 * TE * PAD; i += 32) {
+    const int row = i / PAD, c = i % PAD;  // row over (stage, x rows then factor rows)
+    W[(row / (2 * TE)) * stride + (row % (2 * TE)) * X::XS + X::NP + c] = T(0);
+  }
+}
+
+// A blocks of x: u[kb][ri][ci] = x[g + 8 ri][8 kb + 2t + ci]
 // (staged rows are zero past Np).
 template <typename T, int DIM, int P>
 __device__ __forceinline__ void load_x_frags(const T* sx, T (&u)[Tc<T, DIM, P>::NT][Frag<T>::R][2], int g, int t) {
@@ -348,7 +363,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_trace_kernel(ApplyArgs<T> 
   // CTAs (SMs) instead of filling the first ones
   int tile = warp * gridDim.x + blockIdx.x;
   pdl_trigger();
-  for (int i = lane; i < X::W1_T; i += 32) W[i] = T(0);  // row and record padding stays zero
+  zero_row_padding<T, DIM, P>(W, 2, X::ST1, lane);
   for (int i = threadIdx.x; i < X::N1; i += blockDim.x) BFs[i] = blob[X::BF + i];
   for (int i = threadIdx.x; i < NF * NFP; i += blockDim.x) fmask[i] = a.itab[i];
   pdl_wait();  // x, factor and the trace buffer belong to the preceding kernels
@@ -472,7 +487,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_apply_tc_kernel(ApplyArgs<
   // CTAs (SMs) instead of filling the first ones
   int tile = warp * gridDim.x + blockIdx.x;
   pdl_trigger();
-  for (int i = lane; i < L::T_; i += 32) W[i] = T(0);  // row padding stays zero
+  zero_row_padding<T, DIM, P>(W, NS, X::ST2, lane);
   __syncwarp();
   // prologue: constants and the connectivity of the first two tiles (set-up data),
   // then, once the preceding kernels are done, the first tile's element data
@@ -526,12 +541,19 @@ __global__ void __launch_bounds__(WARPS * 32, 1) sipg_apply_tc_kernel(ApplyArgs<
 #pragma unroll
       for (int nt = 0; nt < NT; ++nt)
 #pragma unroll
-        for (int ri = 0; ri < R; ++ri)
+        for (int ri = 0; ri < R; ++ri) {
+          const int el = g + 8 * ri, n0 = 8 * nt + 2 * t;
+          const T* crow = a.c + (size_t)(e0 + el) * NP;
+          if (NP % 2 == 0) {  // node pairs (n0, n0 + 1) are aligned
+            typename F::V2 v{T(0), T(0)};
+            if (el < ne && n0 < NP) v = ld2(crow + n0);
+            yold[nt][ri][0] = v.x;
+            yold[nt][ri][1] = v.y;
+          } else {
 #pragma unroll
-          for (int ci = 0; ci < 2; ++ci) {
-            const int el = g + 8 * ri, n = 8 * nt + 2 * t + ci;
-            yold[nt][ri][ci] = (el < ne && n < NP) ? a.c[(size_t)(e0 + el) * NP + n] : T(0);
+            for (int ci = 0; ci < 2; ++ci) yold[nt][ri][ci] = (el < ne && n0 + ci < NP) ? crow[n0 + ci] : T(0);
           }
+        }
     }
     const T* sfg = sg + X::NV * TE;  // face rows of the geometry block
     __syncwarp();
@@ -904,12 +926,16 @@ cudaError_t launch_tc_t(const ApplyArgs<T>& a, const T* blob, T* trace, int num_
   if (W2D < 1) return cudaErrorInvalidConfiguration;
   using X = Tc<T, DIM, P>;
   // the kernels copy caller vectors in 16-byte pieces: other alignments take the CUDA-core kernel
-  if (!aligned16(a.x) || !aligned16(a.y) || !aligned16(trace) || (a.factor && !aligned16(a.factor)))
+  if (!aligned16(a.x) || !aligned16(a.y) || !aligned16(trace) || (a.factor && !aligned16(a.factor)) ||
+      (a.beta != T(0) && !aligned16(a.c)))
     return launch_apply<T>(DIM, P, a, num_sms, s);
   const int ntiles = (a.K + X::TE - 1) / X::TE;
   const long long wave = (long long)num_sms;
   cudaError_t err;
-  if (ntiles >= wave * WA) err = launch_pass1<T, DIM, P, WA>(a, blob, trace, ntiles, num_sms, s);
+  // pass 1 on large meshes: at most 12 warps per SM. It is latency-bound, so the
+  // time goes with the number of tile rounds; at 24^3 x 6 tets (35 tiles per SM in
+  // FP32, 70 in FP64) 12 warps give full rounds where 15 or 16 leave a partial one
+  if (ntiles >= wave * WA) err = launch_pass1<T, DIM, P, cmin(12, WA)>(a, blob, trace, ntiles, num_sms, s);
   else if (ntiles >= wave * 4) err = launch_pass1<T, DIM, P, cmin(4, WA)>(a, blob, trace, ntiles, num_sms, s);
   else err = launch_pass1<T, DIM, P, cmin(2, WA)>(a, blob, trace, ntiles, num_sms, s);
   if (err != cudaSuccess) return err;
@@ -999,6 +1025,7 @@ cudaError_t launch_tc_geom(int dim, const T* geof, int K, T* out, cudaStream_t s
   if (dim == 3) k_tc_geom<T, 3, TE><<<grid, 256, 0, s>>>(geof, K, out);
   else if (dim == 2) k_tc_geom<T, 2, TE><<<grid, 256, 0, s>>>(geof, K, out);
   else return cudaErrorInvalidValue;
+  note_launch();
   return cudaGetLastError();
 }
 
