@@ -186,7 +186,10 @@ typedef struct {
                                 kernels: identical iterates. */
   int assembled_max_order;   /* p-multigrid levels below the finest with this order or lower apply
                                 their operator as stored element blocks (assembled once from the
-                                matrix-free apply, scalar operators, orders <= 2); 0: all matrix-free */
+                                matrix-free apply, scalar operators, orders <= 2; in the FP32
+                                V-cycle p = 1 blocks are FP32 and p = 2 blocks FP16 scaled per
+                                element); 0: all matrix-free; -1 (default): 2 in the FP32 V-cycle,
+                                1 in the FP64 V-cycle */
   int smoother;              /* p-multigrid smoothing: 0 Chebyshev on the point-Jacobi (diagonal)
                                 preconditioned operator, 1 on the element-block-Jacobi one */
   /* per p-multigrid level (the [p-multigrid] keys cheb_orders, pre_it, post_it of

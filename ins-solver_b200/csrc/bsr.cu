@@ -1,4 +1,5 @@
 // Element-block form of low-order SIPG operators: probing assembly and apply.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -84,6 +85,80 @@ __global__ void __launch_bounds__(256) k_bsr(int K, const T* __restrict__ v, con
   }
 }
 
+// Scaled FP16 copy of the blocks: per element the largest magnitude over its
+// (NF + 1) Np^2 values is the scale, and v16 holds values / scale in the
+// row-fastest layout of k_bsr16.
+__global__ void k_bsr16_pack(const double* __restrict__ v64, int K, int Np, int NS, __half* __restrict__ v16,
+                             float* __restrict__ scale) {
+  const size_t K_ = (size_t)K;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < K; e += gridDim.x * blockDim.x) {
+    double m = 0.0;
+    for (int q = 0; q < NS * Np * Np; ++q) m = fmax(m, fabs(v64[(size_t)q * K_ + e]));
+    const float sc = m > 0.0 ? (float)m : 1.0f;
+    scale[e] = sc;
+    for (int s = 0; s < NS; ++s)
+      for (int r = 0; r < Np; ++r)
+        for (int c = 0; c < Np; ++c)
+          v16[(((size_t)s * Np + c) * K_ + e) * Np + r] =
+              __double2half(v64[(((size_t)s * Np + r) * Np + c) * K_ + e] / (double)sc);
+  }
+}
+
+// Two rows per thread: t2 = e Np/2 + r/2 (Np even), so the Np/2 threads of an
+// element read consecutive FP16 pairs and the same x values (broadcast). The
+// neighbour list is read first and every block value is loaded without a branch
+// (boundary slots hold zero blocks and read the element's own x row), so all
+// loads of a thread are independent. y = alpha scale[e] acc + beta c, FP32
+// accumulation.
+template <int NP, int NF>
+__global__ void __launch_bounds__(256, 2) k_bsr16(int K, const __half* __restrict__ v, const float* __restrict__ scale,
+                                               const int* __restrict__ nbr, const float* __restrict__ x, float* y,
+                                               float alpha, float beta, const float* c) {
+  static_assert(NP % 2 == 0, "two rows per thread");
+  pdl_enter();
+  constexpr int H = NP / 2;
+  const size_t KH = (size_t)K * H;
+  const __half2* v2 = reinterpret_cast<const __half2*>(v);
+  for (size_t t2 = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t2 < KH; t2 += (size_t)gridDim.x * blockDim.x) {
+    const int e = (int)(t2 / H);
+    int ks[NF + 1];
+    ks[0] = e;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      const int k = nbr[(size_t)e * NF + f];
+      ks[f + 1] = k < 0 ? e : k;
+    }
+    // all loads first (about 100 in flight per thread), then the products
+    __half2 w[NF + 1][NP];
+    float xv[NF + 1][NP];
+#pragma unroll
+    for (int s = 0; s <= NF; ++s)
+#pragma unroll
+      for (int cc = 0; cc < NP; ++cc) w[s][cc] = v2[(size_t)(s * NP + cc) * KH + t2];
+#pragma unroll
+    for (int s = 0; s <= NF; ++s)
+#pragma unroll
+      for (int cc = 0; cc < NP; ++cc) xv[s][cc] = x[(size_t)ks[s] * NP + cc];
+    float a0 = 0.0f, a1 = 0.0f;
+#pragma unroll
+    for (int s = 0; s <= NF; ++s)
+#pragma unroll
+      for (int cc = 0; cc < NP; ++cc) {
+        const float2 wf = __half22float2(w[s][cc]);
+        a0 += wf.x * xv[s][cc];
+        a1 += wf.y * xv[s][cc];
+      }
+    const float sc = scale[e];
+    float2 o = make_float2(alpha * (sc * a0), alpha * (sc * a1));
+    if (beta != 0.0f) {
+      const float2 cv = *reinterpret_cast<const float2*>(c + 2 * t2);
+      o.x += beta * cv.x;
+      o.y += beta * cv.y;
+    }
+    *reinterpret_cast<float2*>(y + 2 * t2) = o;
+  }
+}
+
 }  // namespace
 
 std::vector<int> distance2_colours(int K, int NF, const int* nbr, int* ncolours) {
@@ -150,18 +225,44 @@ void bsr_assemble(sipg_op* op, BsrOp& B, bool want32, cudaStream_t s) {
       note_launch();
     }
   }
-  if (want32) {
+  const bool half = want32 && Np > m->dim + 1;  // above p = 1
+  if (half) {
+    B.v16 = DevBuf(nv * sizeof(__half));
+    B.scale16 = DevBuf((size_t)K * sizeof(float));
+    k_bsr16_pack<<<grid_of(K), 256, 0, s>>>(B.v64.as<double>(), K, Np, NF + 1, B.v16.as<__half>(),
+                                            B.scale16.as<float>());
+    note_launch();
+  } else if (want32) {
     B.v32 = DevBuf(nv * sizeof(float));
     k_d2f<<<grid_of(nv), 256, 0, s>>>(B.v32.as<float>(), B.v64.as<double>(), nv);
     note_launch();
   }
   SIPG_CUDA(cudaGetLastError());
   SIPG_CUDA(cudaStreamSynchronize(s));  // the probe buffers are freed on return
+  if (half) B.v64 = DevBuf();            // the FP32 V-cycle reads the FP16 copy only
 }
 
 template <typename T>
 void bsr_apply(const BsrOp& B, const T* x, T* y, T alpha, T beta, cudaStream_t s, const T* c) {
   if (!c) c = y;
+  if constexpr (std::is_same<T, float>::value) {
+    if (B.v16.p) {
+      if (((reinterpret_cast<uintptr_t>(y) | reinterpret_cast<uintptr_t>(c)) & 7) != 0)
+        throw Error(SIPG_INVALID_ARG, "the FP16 assembled apply needs 8-byte aligned vectors");
+      const int g = (int)std::max<size_t>(1, std::min<size_t>(((size_t)B.K * B.Np / 2 + 255) / 256, 148 * 32));
+      const __half* v = B.v16.as<__half>();
+      const float* sc = B.scale16.as<float>();
+      if (B.dim == 3 && B.Np == 10)
+        pdl_launch(k_bsr16<10, 4>, dim3(g), dim3(256), 0, s, B.K, v, sc, B.nbr, x, y, alpha, beta, c);
+      else if (B.dim == 2 && B.Np == 6)
+        pdl_launch(k_bsr16<6, 3>, dim3(g), dim3(256), 0, s, B.K, v, sc, B.nbr, x, y, alpha, beta, c);
+      else
+        throw Error(SIPG_INVALID_ARG, "no FP16 assembled apply for this element");
+      note_launch();
+      SIPG_CUDA(cudaGetLastError());
+      return;
+    }
+  }
   const T* v = std::is_same<T, double>::value ? (const T*)B.v64.p : (const T*)B.v32.p;
   if (!v) throw Error(SIPG_INVALID_ARG, "assembled blocks missing for this precision");
   const int g = (int)std::max<size_t>(1, std::min<size_t>(((size_t)B.K * B.Np + 255) / 256, 148 * 32));

@@ -451,7 +451,11 @@ void sipg_solver::setup_pmg() {
       L.lmax = power_lmax(L.op, L.dinv64.as<double>(), L.n);
     }
     L.bsr.reset();
-    if (l > 0 && L.order <= o.assembled_max_order && bsr_supported(dim, L.order, nc)) {
+    // -1: p = 2 and below in the FP32 V-cycle (p = 2 as scaled FP16 blocks: half the
+    // bytes of the matrix-free apply's per-element work, same iteration counts), p = 1
+    // in the FP64 V-cycle (FP64 blocks at p = 2 move more bytes than the matrix-free apply)
+    const int amo = o.assembled_max_order >= 0 ? o.assembled_max_order : (f32 ? 2 : 1);
+    if (l > 0 && L.order <= amo && bsr_supported(dim, L.order, nc)) {
       L.bsr = std::make_unique<BsrOp>();
       bsr_assemble(L.op, *L.bsr, f32, stream);
     }
@@ -1080,7 +1084,7 @@ int sipg_solver_default_opts(int kind, sipg_solver_opts* o) {
     o->amg_coarse_max = 1000;
     o->amg_strength = 0.08;
     o->graphs = 2;
-    o->assembled_max_order = 1;
+    o->assembled_max_order = -1;
     o->smoother = 1;
     o->amg_cheb_order = 2;
     for (int l = 0; l < 4; ++l) {
