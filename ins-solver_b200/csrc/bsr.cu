@@ -225,7 +225,7 @@ void bsr_assemble(sipg_op* op, BsrOp& B, bool want32, cudaStream_t s) {
       note_launch();
     }
   }
-  const bool half = want32 && Np > m->dim + 1;  // above p = 1
+  const bool half = want32 && Np % 2 == 0;  // two rows per thread in k_bsr16
   if (half) {
     B.v16 = DevBuf(nv * sizeof(__half));
     B.scale16 = DevBuf((size_t)K * sizeof(float));
@@ -254,6 +254,8 @@ void bsr_apply(const BsrOp& B, const T* x, T* y, T alpha, T beta, cudaStream_t s
       const float* sc = B.scale16.as<float>();
       if (B.dim == 3 && B.Np == 10)
         pdl_launch(k_bsr16<10, 4>, dim3(g), dim3(256), 0, s, B.K, v, sc, B.nbr, x, y, alpha, beta, c);
+      else if (B.dim == 3 && B.Np == 4)
+        pdl_launch(k_bsr16<4, 4>, dim3(g), dim3(256), 0, s, B.K, v, sc, B.nbr, x, y, alpha, beta, c);
       else if (B.dim == 2 && B.Np == 6)
         pdl_launch(k_bsr16<6, 3>, dim3(g), dim3(256), 0, s, B.K, v, sc, B.nbr, x, y, alpha, beta, c);
       else

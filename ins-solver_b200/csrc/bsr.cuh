@@ -27,7 +27,7 @@ struct BsrOp {
   // values[((s * Np + r) * Np + c) * K + e]: block s of element row e, s = 0 the
   // element itself, s = 1 + f the neighbour across face f (zero at boundary faces)
   DevBuf v64, v32;
-  // FP32 V-cycle above p = 1: FP16 values scaled per element (10-bit mantissa like
+  // FP32 V-cycle, even Np: FP16 values scaled per element (10-bit mantissa like
   // the TF32 matrix-free apply, half the bytes of FP32) in the layout
   // v16[((s * Np + c) * K + e) * Np + r] = values / scale16[e], so that the Np
   // threads of an element row block read consecutive values
@@ -39,7 +39,7 @@ struct BsrOp {
 inline bool bsr_supported(int dim, int order, int ncomp) { return ncomp == 1 && order >= 1 && order <= 2 && dim >= 2; }
 
 // Assemble from the operator's FP64 apply; want32: also the FP32 V-cycle's copy
-// (FP32 at p = 1, scaled FP16 above, the FP64 values then released).
+// (scaled FP16 for even Np, the FP64 values then released; FP32 otherwise).
 void bsr_assemble(sipg_op* op, BsrOp& B, bool want32, cudaStream_t s);
 
 // y = alpha * B x + beta * c, c = y when null (beta == 0: c is not read).
