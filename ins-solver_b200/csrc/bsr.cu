@@ -159,6 +159,79 @@ __global__ void __launch_bounds__(256, 2) k_bsr16(int K, const __half* __restric
   }
 }
 
+// C = Bs A per element row block (FP64), Bs the symmetric part of the inverse
+// diagonal block (the smoother stores that part too, k_block_pack_sym):
+// C[s][r][c][e] = sum_m Bs_e[r][m] A[s][m][c][e], one thread per (block entry,
+// element), element fastest.
+__global__ void k_bsr_precond(const double* __restrict__ A, const double* __restrict__ binv, int K, int Np, int NS,
+                              double* __restrict__ C) {
+  const size_t K_ = (size_t)K, total = (size_t)NS * Np * Np * K_;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t e = i % K_, q = i / K_;
+    const int c = (int)(q % Np), r = (int)((q / Np) % Np), s = (int)(q / ((size_t)Np * Np));
+    const double* be = binv + e * Np * Np;
+    double acc = 0.0;
+    for (int m = 0; m < Np; ++m)
+      acc += 0.5 * (be[(size_t)r * Np + m] + be[(size_t)m * Np + r]) * A[(((size_t)s * Np + m) * Np + c) * K_ + e];
+    C[i] = acc;
+  }
+}
+
+// One fused Chebyshev step (bsr_cheb_step), same thread layout and loads as k_bsr16.
+template <int NP, int NF>
+__global__ void __launch_bounds__(256, 2) k_bsr16_cheb(int K, const __half* __restrict__ v,
+                                                       const float* __restrict__ scale, const int* __restrict__ nbr,
+                                                       const float* __restrict__ din, float* __restrict__ dout,
+                                                       float* sres, float* z, float c1, float c2, float s0_scale) {
+  static_assert(NP % 2 == 0, "two rows per thread");
+  pdl_enter();
+  constexpr int H = NP / 2;
+  const size_t KH = (size_t)K * H;
+  const __half2* v2 = reinterpret_cast<const __half2*>(v);
+  for (size_t t2 = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t2 < KH; t2 += (size_t)gridDim.x * blockDim.x) {
+    const int e = (int)(t2 / H);
+    int ks[NF + 1];
+    ks[0] = e;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      const int k = nbr[(size_t)e * NF + f];
+      ks[f + 1] = k < 0 ? e : k;
+    }
+    __half2 w[NF + 1][NP];
+    float xv[NF + 1][NP];
+#pragma unroll
+    for (int s = 0; s <= NF; ++s)
+#pragma unroll
+      for (int cc = 0; cc < NP; ++cc) w[s][cc] = v2[(size_t)(s * NP + cc) * KH + t2];
+#pragma unroll
+    for (int s = 0; s <= NF; ++s)
+#pragma unroll
+      for (int cc = 0; cc < NP; ++cc) xv[s][cc] = din[(size_t)ks[s] * NP + cc];
+    float a0 = 0.0f, a1 = 0.0f;
+#pragma unroll
+    for (int s = 0; s <= NF; ++s)
+#pragma unroll
+      for (int cc = 0; cc < NP; ++cc) {
+        const float2 wf = __half22float2(w[s][cc]);
+        a0 += wf.x * xv[s][cc];
+        a1 += wf.y * xv[s][cc];
+      }
+    const float sc = scale[e];
+    const float2 d0 = *reinterpret_cast<const float2*>(din + 2 * t2);
+    float2 sr = s0_scale != 0.0f ? make_float2(s0_scale * d0.x, s0_scale * d0.y)
+                                 : *reinterpret_cast<const float2*>(sres + 2 * t2);
+    sr.x -= sc * a0;
+    sr.y -= sc * a1;
+    const float2 dn = make_float2(c1 * d0.x + c2 * sr.x, c1 * d0.y + c2 * sr.y);
+    float2 zz = *reinterpret_cast<const float2*>(z + 2 * t2);
+    zz.x += dn.x;
+    zz.y += dn.y;
+    *reinterpret_cast<float2*>(sres + 2 * t2) = sr;
+    *reinterpret_cast<float2*>(dout + 2 * t2) = dn;
+    *reinterpret_cast<float2*>(z + 2 * t2) = zz;
+  }
+}
+
 }  // namespace
 
 std::vector<int> distance2_colours(int K, int NF, const int* nbr, int* ncolours) {
@@ -188,7 +261,7 @@ std::vector<int> distance2_colours(int K, int NF, const int* nbr, int* ncolours)
   return col;
 }
 
-void bsr_assemble(sipg_op* op, BsrOp& B, bool want32, cudaStream_t s) {
+void bsr_assemble(sipg_op* op, BsrOp& B, bool want32, cudaStream_t s, const double* binv_rows) {
   if (op->ncomp != 1) throw Error(SIPG_INVALID_ARG, "assembled blocks need a scalar operator");
   sipg_mesh* m = op->mesh;
   const int K = m->K, Np = op->Np, NF = m->dim + 1;
@@ -232,6 +305,17 @@ void bsr_assemble(sipg_op* op, BsrOp& B, bool want32, cudaStream_t s) {
     k_bsr16_pack<<<grid_of(K), 256, 0, s>>>(B.v64.as<double>(), K, Np, NF + 1, B.v16.as<__half>(),
                                             B.scale16.as<float>());
     note_launch();
+    if (binv_rows) {
+      DevBuf c64(nv * sizeof(double));
+      k_bsr_precond<<<grid_of(nv), 256, 0, s>>>(B.v64.as<double>(), binv_rows, K, Np, NF + 1, c64.as<double>());
+      note_launch();
+      B.c16 = DevBuf(nv * sizeof(__half));
+      B.cscale16 = DevBuf((size_t)K * sizeof(float));
+      k_bsr16_pack<<<grid_of(K), 256, 0, s>>>(c64.as<double>(), K, Np, NF + 1, B.c16.as<__half>(),
+                                              B.cscale16.as<float>());
+      note_launch();
+      SIPG_CUDA(cudaStreamSynchronize(s));  // c64 is freed on scope exit
+    }
   } else if (want32) {
     B.v32 = DevBuf(nv * sizeof(float));
     k_d2f<<<grid_of(nv), 256, 0, s>>>(B.v32.as<float>(), B.v64.as<double>(), nv);
@@ -276,6 +360,27 @@ void bsr_apply(const BsrOp& B, const T* x, T* y, T alpha, T beta, cudaStream_t s
   else if (B.dim == 2 && B.Np == 3) pdl_launch(k_bsr<T, 3, 3>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta, c);
   else if (B.dim == 2 && B.Np == 6) pdl_launch(k_bsr<T, 6, 3>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta, c);
   else throw Error(SIPG_INVALID_ARG, "no assembled apply for this element");
+  note_launch();
+  SIPG_CUDA(cudaGetLastError());
+}
+
+void bsr_cheb_step(const BsrOp& B, const float* din, float* dout, float* sres, float* z, float c1, float c2,
+                   float s0_scale, cudaStream_t s) {
+  if (!B.c16.p) throw Error(SIPG_INVALID_ARG, "preconditioned FP16 blocks missing");
+  if (((reinterpret_cast<uintptr_t>(din) | reinterpret_cast<uintptr_t>(dout) | reinterpret_cast<uintptr_t>(sres) |
+        reinterpret_cast<uintptr_t>(z)) & 7) != 0)
+    throw Error(SIPG_INVALID_ARG, "the fused Chebyshev step needs 8-byte aligned vectors");
+  const int g = (int)std::max<size_t>(1, std::min<size_t>(((size_t)B.K * B.Np / 2 + 255) / 256, 148 * 32));
+  const __half* v = B.c16.as<__half>();
+  const float* sc = B.cscale16.as<float>();
+  if (B.dim == 3 && B.Np == 10)
+    pdl_launch(k_bsr16_cheb<10, 4>, dim3(g), dim3(256), 0, s, B.K, v, sc, B.nbr, din, dout, sres, z, c1, c2, s0_scale);
+  else if (B.dim == 3 && B.Np == 4)
+    pdl_launch(k_bsr16_cheb<4, 4>, dim3(g), dim3(256), 0, s, B.K, v, sc, B.nbr, din, dout, sres, z, c1, c2, s0_scale);
+  else if (B.dim == 2 && B.Np == 6)
+    pdl_launch(k_bsr16_cheb<6, 3>, dim3(g), dim3(256), 0, s, B.K, v, sc, B.nbr, din, dout, sres, z, c1, c2, s0_scale);
+  else
+    throw Error(SIPG_INVALID_ARG, "no fused Chebyshev step for this element");
   note_launch();
   SIPG_CUDA(cudaGetLastError());
 }

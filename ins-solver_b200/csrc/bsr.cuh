@@ -32,6 +32,10 @@ struct BsrOp {
   // v16[((s * Np + c) * K + e) * Np + r] = values / scale16[e], so that the Np
   // threads of an element row block read consecutive values
   DevBuf v16, scale16;
+  // Block-Jacobi preconditioned blocks C = Bd^-1 A (Bd the diagonal block of the
+  // element row), same layout and scaling as v16: one kernel per Chebyshev step
+  // (k_bsr16_cheb) then updates the preconditioned residual directly
+  DevBuf c16, cscale16;
   const int* nbr = nullptr;  // mesh K x NF (device)
 };
 
@@ -40,11 +44,21 @@ inline bool bsr_supported(int dim, int order, int ncomp) { return ncomp == 1 && 
 
 // Assemble from the operator's FP64 apply; want32: also the FP32 V-cycle's copy
 // (scaled FP16 for even Np, the FP64 values then released; FP32 otherwise).
-void bsr_assemble(sipg_op* op, BsrOp& B, bool want32, cudaStream_t s);
+// binv_rows (FP32 V-cycle, even Np): the inverse diagonal blocks, row-major per
+// element, for the preconditioned copy C.
+void bsr_assemble(sipg_op* op, BsrOp& B, bool want32, cudaStream_t s, const double* binv_rows = nullptr);
 
 // y = alpha * B x + beta * c, c = y when null (beta == 0: c is not read).
 template <typename T>
 void bsr_apply(const BsrOp& B, const T* x, T* y, T alpha, T beta, cudaStream_t s, const T* c = nullptr);
+
+// One Chebyshev step on the block-Jacobi preconditioned operator of an assembled
+// FP32 level (B.c16 present), with the preconditioned residual sres = Bd^-1 r kept
+// current: sres -= C din, dout = c1 din + c2 sres, z += dout. din and dout are
+// distinct buffers (neighbours read din). s0_scale != 0: sres is first set to
+// s0_scale * din (the step after a first step din = c2 Bd^-1 r, s0_scale = 1 / c2).
+void bsr_cheb_step(const BsrOp& B, const float* din, float* dout, float* sres, float* z, float c1, float c2,
+                   float s0_scale, cudaStream_t s);
 
 // Greedy distance-2 colouring of the face graph (nbr: K x NF, negative = boundary).
 std::vector<int> distance2_colours(int K, int NF, const int* nbr, int* ncolours);

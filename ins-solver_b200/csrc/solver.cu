@@ -55,6 +55,7 @@ struct Level {
   DevBuf P64, P32;               // prolongation from the next level: Np x Np_next
   // work vectors in the V-cycle precision
   DevBuf rhs, z, res, d;
+  DevBuf d2, sres;               // fused Chebyshev steps (bsr->c16): second d buffer, Bd^-1 r
   DevBuf cp, cs, cAp;            // coarse CG
   DevBuf bc64, bc32;             // inverse diagonal blocks (block-Jacobi smoothing; bc32 in bf16)
   bool bsym = false;             // bc* packed symmetric (large meshes) or full column-major blocks
@@ -424,6 +425,7 @@ void sipg_solver::setup_pmg() {
     if (f32) to_f32(L.dinv32.as<float>(), L.dinv64.as<double>(), L.n, stream);
     L.bc64 = DevBuf();
     L.bc32 = DevBuf();
+    DevBuf rows;  // FP64 inverse diagonal blocks, row-major per element (block-Jacobi smoothing)
     if (o.smoother == 1) {
       // element-block Jacobi: inverse diagonal blocks in the level precision (BF16 for
       // the FP32 V-cycle: the smoother tolerates 8 mantissa bits). Large meshes store
@@ -431,7 +433,7 @@ void sipg_solver::setup_pmg() {
       // small ones as full column-major blocks (ten threads per block at p = 3).
       const int nb = (int)(L.n / L.Np);
       L.bsym = block_sym_supported(L.Np) && nb >= kSymMinBlocks;
-      DevBuf rows((size_t)nb * L.Np * L.Np * sizeof(double));
+      rows = DevBuf((size_t)nb * L.Np * L.Np * sizeof(double));
       SIPG_CUDA(launch_blocks(dim, L.order, L.op->block_args(BLOCK_INVERSE, 0, rows.as<double>(), true), stream));
       if (f32 && L.bsym) {
         L.bc32 = DevBuf(block_sym_values<__nv_bfloat16>(nb, L.Np) * sizeof(__nv_bfloat16));
@@ -455,9 +457,18 @@ void sipg_solver::setup_pmg() {
     // bytes of the matrix-free apply's per-element work, same iteration counts), p = 1
     // in the FP64 V-cycle (FP64 blocks at p = 2 move more bytes than the matrix-free apply)
     const int amo = o.assembled_max_order >= 0 ? o.assembled_max_order : (f32 ? 2 : 1);
+    L.d2 = DevBuf();
+    L.sres = DevBuf();
     if (l > 0 && L.order <= amo && bsr_supported(dim, L.order, nc)) {
       L.bsr = std::make_unique<BsrOp>();
-      bsr_assemble(L.op, *L.bsr, f32, stream);
+      // FP32 V-cycle with packed symmetric block-Jacobi smoothing: also C = Bd^-1 A, so
+      // that one kernel per Chebyshev step after the first updates Bd^-1 r directly
+      const bool fused = f32 && o.smoother == 1 && L.bsym && L.Np % 2 == 0;
+      bsr_assemble(L.op, *L.bsr, f32, stream, fused ? rows.as<double>() : nullptr);
+      if (L.bsr->c16.p) {
+        L.d2 = DevBuf(L.n * sizeof(float));
+        L.sres = DevBuf(L.n * sizeof(float));
+      }
     }
   }
   use_amg = o.coarse_kind == 1 && nc == 1 && lv.back().order == 1;
@@ -605,6 +616,27 @@ void sipg_solver::chebyshev(Level& L, bool want_res, bool first) {
   T* d = L.d.as<T>();
   T* z = L.z.as<T>();
   T* res = L.res.as<T>();
+  if (std::is_same<T, float>::value && L.bsr && L.bsr->c16.p && L.bc32.p && L.bsym) {
+    // first step from Bd^-1 r (block smoother kernel), then one fused kernel per step
+    // on C = Bd^-1 A with s = Bd^-1 r kept current; the residual, where wanted, from rhs
+    const bool from_rhs = first;
+    const T* rin = from_rhs ? L.rhs.as<T>() : res;
+    const int nb = (int)(L.n / L.Np);
+    cheb_step_sym<float, __nv_bfloat16>((float*)d, (float*)z, (const float*)rin, L.bc32.as<__nv_bfloat16>(), 0.0f,
+                                        (float)(1.0 / theta), nb, L.Np, stream, from_rhs);
+    float* dc = (float*)d;
+    float* dn = L.d2.as<float>();
+    for (int it = 1; it < L.cheb; ++it) {
+      const double rho = 1.0 / (2.0 * sigma - rho_old);
+      const double c1 = rho * rho_old, c2 = 2.0 * rho / delta;
+      rho_old = rho;
+      bsr_cheb_step(*L.bsr, dc, dn, L.sres.as<float>(), (float*)z, (float)c1, (float)c2,
+                    it == 1 ? (float)theta : 0.0f, stream);
+      std::swap(dc, dn);
+    }
+    if (want_res) L.apply<T>(z, res, stream, T(-1), T(1), L.rhs.as<T>());
+    return;
+  }
   for (int it = 0; it < L.cheb; ++it) {
     double c1 = 0.0, c2 = 1.0 / theta;
     if (it > 0) {
