@@ -159,20 +159,22 @@ __global__ void __launch_bounds__(256, 2) k_bsr16(int K, const __half* __restric
   }
 }
 
-// C = Bs A per element row block (FP64), Bs the symmetric part of the inverse
-// diagonal block (the smoother stores that part too, k_block_pack_sym):
-// C[s][r][c][e] = sum_m Bs_e[r][m] A[s][m][c][e], one thread per (block entry,
-// element), element fastest.
+// C = Bi A per element row block (FP64), Bi the inverse diagonal block as the
+// smoother stores it: its symmetric part when sym (packed triangles,
+// k_block_pack_sym), else as is. C[s][r][c][e] = sum_m Bi_e[r][m] A[s][m][c][e],
+// one thread per (block entry, element), element fastest.
 __global__ void k_bsr_precond(const double* __restrict__ A, const double* __restrict__ binv, int K, int Np, int NS,
-                              double* __restrict__ C) {
+                              int sym, double* __restrict__ C) {
   const size_t K_ = (size_t)K, total = (size_t)NS * Np * Np * K_;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
     const size_t e = i % K_, q = i / K_;
     const int c = (int)(q % Np), r = (int)((q / Np) % Np), s = (int)(q / ((size_t)Np * Np));
     const double* be = binv + e * Np * Np;
     double acc = 0.0;
-    for (int m = 0; m < Np; ++m)
-      acc += 0.5 * (be[(size_t)r * Np + m] + be[(size_t)m * Np + r]) * A[(((size_t)s * Np + m) * Np + c) * K_ + e];
+    for (int m = 0; m < Np; ++m) {
+      const double b = sym ? 0.5 * (be[(size_t)r * Np + m] + be[(size_t)m * Np + r]) : be[(size_t)r * Np + m];
+      acc += b * A[(((size_t)s * Np + m) * Np + c) * K_ + e];
+    }
     C[i] = acc;
   }
 }
@@ -261,7 +263,7 @@ std::vector<int> distance2_colours(int K, int NF, const int* nbr, int* ncolours)
   return col;
 }
 
-void bsr_assemble(sipg_op* op, BsrOp& B, bool want32, cudaStream_t s, const double* binv_rows) {
+void bsr_assemble(sipg_op* op, BsrOp& B, bool want32, cudaStream_t s, const double* binv_rows, bool binv_sym) {
   if (op->ncomp != 1) throw Error(SIPG_INVALID_ARG, "assembled blocks need a scalar operator");
   sipg_mesh* m = op->mesh;
   const int K = m->K, Np = op->Np, NF = m->dim + 1;
@@ -307,7 +309,8 @@ void bsr_assemble(sipg_op* op, BsrOp& B, bool want32, cudaStream_t s, const doub
     note_launch();
     if (binv_rows) {
       DevBuf c64(nv * sizeof(double));
-      k_bsr_precond<<<grid_of(nv), 256, 0, s>>>(B.v64.as<double>(), binv_rows, K, Np, NF + 1, c64.as<double>());
+      k_bsr_precond<<<grid_of(nv), 256, 0, s>>>(B.v64.as<double>(), binv_rows, K, Np, NF + 1, binv_sym ? 1 : 0,
+                                                c64.as<double>());
       note_launch();
       B.c16 = DevBuf(nv * sizeof(__half));
       B.cscale16 = DevBuf((size_t)K * sizeof(float));

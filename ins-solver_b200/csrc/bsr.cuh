@@ -45,8 +45,10 @@ inline bool bsr_supported(int dim, int order, int ncomp) { return ncomp == 1 && 
 // Assemble from the operator's FP64 apply; want32: also the FP32 V-cycle's copy
 // (scaled FP16 for even Np, the FP64 values then released; FP32 otherwise).
 // binv_rows (FP32 V-cycle, even Np): the inverse diagonal blocks, row-major per
-// element, for the preconditioned copy C.
-void bsr_assemble(sipg_op* op, BsrOp& B, bool want32, cudaStream_t s, const double* binv_rows = nullptr);
+// element, for the preconditioned copy C (binv_sym: with their symmetric part, as
+// the packed smoother blocks hold them).
+void bsr_assemble(sipg_op* op, BsrOp& B, bool want32, cudaStream_t s, const double* binv_rows = nullptr,
+                  bool binv_sym = false);
 
 // y = alpha * B x + beta * c, c = y when null (beta == 0: c is not read).
 template <typename T>

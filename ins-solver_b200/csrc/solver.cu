@@ -463,8 +463,8 @@ void sipg_solver::setup_pmg() {
       L.bsr = std::make_unique<BsrOp>();
       // FP32 V-cycle with packed symmetric block-Jacobi smoothing: also C = Bd^-1 A, so
       // that one kernel per Chebyshev step after the first updates Bd^-1 r directly
-      const bool fused = f32 && o.smoother == 1 && L.bsym && L.Np % 2 == 0;
-      bsr_assemble(L.op, *L.bsr, f32, stream, fused ? rows.as<double>() : nullptr);
+      const bool fused = f32 && o.smoother == 1 && L.Np % 2 == 0;
+      bsr_assemble(L.op, *L.bsr, f32, stream, fused ? rows.as<double>() : nullptr, L.bsym);
       if (L.bsr->c16.p) {
         L.d2 = DevBuf(L.n * sizeof(float));
         L.sres = DevBuf(L.n * sizeof(float));
@@ -616,14 +616,18 @@ void sipg_solver::chebyshev(Level& L, bool want_res, bool first) {
   T* d = L.d.as<T>();
   T* z = L.z.as<T>();
   T* res = L.res.as<T>();
-  if (std::is_same<T, float>::value && L.bsr && L.bsr->c16.p && L.bc32.p && L.bsym) {
+  if (std::is_same<T, float>::value && L.bsr && L.bsr->c16.p && L.bc32.p) {
     // first step from Bd^-1 r (block smoother kernel), then one fused kernel per step
     // on C = Bd^-1 A with s = Bd^-1 r kept current; the residual, where wanted, from rhs
     const bool from_rhs = first;
     const T* rin = from_rhs ? L.rhs.as<T>() : res;
     const int nb = (int)(L.n / L.Np);
-    cheb_step_sym<float, __nv_bfloat16>((float*)d, (float*)z, (const float*)rin, L.bc32.as<__nv_bfloat16>(), 0.0f,
-                                        (float)(1.0 / theta), nb, L.Np, stream, from_rhs);
+    if (L.bsym)
+      cheb_step_sym<float, __nv_bfloat16>((float*)d, (float*)z, (const float*)rin, L.bc32.as<__nv_bfloat16>(), 0.0f,
+                                          (float)(1.0 / theta), nb, L.Np, stream, from_rhs);
+    else
+      cheb_step_block<float, __nv_bfloat16>((float*)d, (float*)z, (const float*)rin, L.bc32.as<__nv_bfloat16>(),
+                                            0.0f, (float)(1.0 / theta), nb, L.Np, stream, from_rhs);
     float* dc = (float*)d;
     float* dn = L.d2.as<float>();
     for (int it = 1; it < L.cheb; ++it) {
