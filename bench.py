@@ -338,6 +338,7 @@ def run_ours(args):
         "clocks": clk.summary(),
     }
     out["config_2d"] = run_config_2d()
+    out["projection"] = run_projection(cpu=rank == 0 and world == 1 and not args.skip_cpu)
     if not args.skip_serving:
         out["serving"] = serving_sweep(seed=1234 + rank)
     if rank == 0 and world == 1 and not args.skip_cpu:
@@ -347,6 +348,114 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
     if rank == 0:
         print(json.dumps(out))
+
+
+PROJ_N, PROJ_ORDER, PROJ_DT = 32, 3, 1e-3
+
+
+def projection_inputs(n=PROJ_N, order=PROJ_ORDER):
+    """Velocity projection workload: the 3D rising-bubble mesh (32^3 x 6 =
+    196,608 tets, jittered +-0.1h, seed 20261203), p = 3, velT and grad p
+    U(-1, 1) (seed 5). dt = 1e-3 is CFL 0.5 at h = 1/32, p = 3, |u| = 1."""
+    mesh = sipg.Mesh.box(3, n, jitter=0.1, seed=20261203)
+    Np = sipg.ref_sizes(3, order)[0]
+    rng = np.random.default_rng(5)
+    return mesh, rng.uniform(-1, 1, (3, mesh.K, Np)), rng.uniform(-1, 1, (3, mesh.K, Np))
+
+
+def fp64_peak_tflops():
+    """Measured FP64 denominator: cuBLAS DGEMM (torch float64 matmul 8192^3), best of 5."""
+    import torch
+    a = torch.rand((8192, 8192), dtype=torch.float64, device="cuda")
+    b = torch.rand_like(a)
+    best = 1e30
+    for _ in range(6):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+
+
+def run_projection(steps=20, cpu=True):
+    """Element-local velocity projection (INSSolverBase3D::project_velocity,
+    div_div = 1): one fused kernel per call on resident inputs (CUDA events on its
+    stream; inputs 189 MB and output 94 MB, larger than L2), the host-buffer entry
+    point end to end, and the reference's own kernels on all host cores."""
+    import torch
+    mesh, velT, dp = projection_inputs()
+    K, Np = mesh.K, velT.shape[2]
+    d_dp, d_v = torch.from_numpy(dp).cuda(), torch.from_numpy(velT).cuda()
+    d_out = torch.empty_like(d_v)
+    d_st = torch.zeros(2, dtype=torch.int64, device="cuda")
+    stream = torch.cuda.Stream()
+    lib = sipg.lib()
+
+    def call(st_ptr):
+        sipg.check(lib.sipg_project_velocity(mesh.h, PROJ_ORDER, C.c_double(PROJ_DT), C.c_double(PROJ_DT),
+                                             C.c_void_p(d_dp.data_ptr()), C.c_void_p(d_v.data_ptr()),
+                                             C.c_void_p(d_out.data_ptr()), C.c_void_p(st_ptr),
+                                             C.c_void_p(stream.cuda_stream)))
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            call(d_st.data_ptr())
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            call(0)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    conv, iters = (int(v) for v in d_st.cpu())
+    # end to end: sipg_project_velocity_host from pinned host buffers
+    h_dp, h_v = torch.from_numpy(dp).pin_memory(), torch.from_numpy(velT).pin_memory()
+    h_out = torch.empty_like(h_v).pin_memory()
+    st = np.zeros(3)
+    e2e = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        sipg.check(lib.sipg_project_velocity_host(mesh.h, PROJ_ORDER, C.c_double(PROJ_DT), C.c_double(PROJ_DT),
+                                                  C.c_void_p(h_dp.data_ptr()), C.c_void_p(h_v.data_ptr()),
+                                                  C.c_void_p(h_out.data_ptr()), st.ctypes.data_as(C.c_void_p)))
+        e2e.append(time.perf_counter() - t0)
+    npp = Np * Np
+    # FP64 flops: per element one operator application and one preconditioner
+    # application to start, then per CG iteration one of each (20 Np^2 and 6 Np^2
+    # multiply-adds' worth of flops, counted 2 per FMA), plus the breaking iteration's
+    # operator application; iterations as counted by the reference (the breaking one excluded)
+    flops = K * (2 * 20 + 6) * npp + iters * 26 * npp
+    bytes_ = K * (9 * Np * 8 + 11 * 8)
+    pk = fp64_peak_tflops()
+    dofs = 3 * K * Np
+    out = {"workload": "velocity projection (div_div=1), 3D 32^3x6=196608 tets p=3, dt=1e-3, "
+                       "velT and grad p U(-1,1)",
+           "kernel": "k_proj_cg<3,3> (one launch per projection)",
+           "ms": ms, "gdofs": dofs / (ms * 1e-3) / 1e9, "converged": conv, "cells": K,
+           "mean_iters": iters / K,
+           "e2e": {"ms": float(np.mean(e2e)) * 1e3, "gdofs": dofs / float(np.mean(e2e)) / 1e9,
+                   "h2d_bytes": int(dp.nbytes + velT.nbytes), "d2h_bytes": int(velT.nbytes)},
+           "roofline": {"bound": "fp64", "achieved": flops / (ms * 1e-3) / 1e12, "peak": pk,
+                        "peak_kind": "measured (cuBLAS DGEMM 8192^3 in this run)", "unit": "TFLOP/s",
+                        "frac": flops / (ms * 1e-3) / 1e12 / pk, "flops_per_call": flops,
+                        "hbm_gbs": bytes_ / (ms * 1e-3) / 1e9, "bytes_per_elem": 9 * Np * 8 + 11 * 8}}
+    if cpu:
+        import oracle_py as O
+        if O.have_ref():
+            t, e = sipg.ref_tables(3, PROJ_ORDER), mesh.export(PROJ_ORDER)
+            om = O.OMesh(t, e)
+            best = 1e30
+            for _ in range(3):
+                t0 = time.perf_counter()
+                O.project_velocity(om, PROJ_DT, PROJ_DT, dp, velT, use_ref=True)
+                best = min(best, time.perf_counter() - t0)
+            out["cpu_baseline"] = {"ms": best * 1e3, "gdofs": dofs / best / 1e9, "cores": os.cpu_count(),
+                                   "kind": "reference",
+                                   "sample": "the whole workload through the reference's kernels "
+                                             "(oracle/_ref, OpenMP on all host cores), best of 3"}
+    return out
 
 
 def run_config_2d(reps=5):
@@ -528,12 +637,21 @@ def run_profile(args):
     apply: the headline operator at --n (order --order, precision --precision),
            3 applies after set-up; with -k regex:"sipg_(trace|apply_tc)" -s 2 -c 2
            ncu captures the second apply's two kernels.
+    projection: the velocity projection workload at --n (3 launches of k_proj_cg).
     solve: the headline mixed solve: one warm-up solve, then the captured solve;
            prints the number of kernels launched before it (ncu -s) and in it (-c).
            The outer iterations replay one host-launched graph each (graphs = 1):
            the kernels of the device-resident loop, which the profiler then sees
            as ordinary graph launches.
     """
+    if args.profile == "projection":
+        mesh, velT, dp = projection_inputs(args.n)
+        d_dp, d_v, d_o = sipg.DeviceVector(dp), sipg.DeviceVector(velT), sipg.DeviceVector(np.zeros_like(velT))
+        for _ in range(3):
+            sipg.project_velocity_device(mesh, PROJ_ORDER, PROJ_DT, d_dp.ptr, d_v.ptr, d_o.ptr)
+        sipg.check(sipg.lib().sipg_device_synchronize())
+        print("done", mesh.K)
+        return
     c = W.poisson3d_two_phase(args.n, order=ORDER, n_modes=256, pin=False)
     if args.profile == "apply":
         op = sipg.Operator(c["mesh"], args.order, 1)
@@ -568,7 +686,7 @@ def run_profile(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--profile", choices=["apply", "solve"], default=None,
+    ap.add_argument("--profile", choices=["apply", "solve", "projection"], default=None,
                     help="run a small fixed workload for an ncu capture instead of the benchmark")
     ap.add_argument("--n", type=int, default=N_HEAD)
     ap.add_argument("--order", type=int, default=ORDER)

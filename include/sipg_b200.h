@@ -288,6 +288,29 @@ int sipg_extrapolate_initial_guess(int n_hist, const double *times, const double
 int sipg_extrapolate_initial_guess_host(int n_hist, const double *times, const double *const *hist,
                                         double t_new, size_t n, double *out);
 
+/* ---- velocity projection: replaces INSSolverBase3D::project_velocity with
+ * div_div = 1 (pr_projection_method 1, src/solvers/3d/ins_solver_base.cpp:1052-1124;
+ * 2D src/solvers/2d/ins_solver_base.cpp:894-955): the OP2 loops
+ * ins_3d_proj_rhs, mesh->mass, ins_3d_proj_pen and ins_3d_proj_cg_precon
+ * (2D: ins_2d_proj_rhs, ins_2d_proj_pen, ins_proj_cg_2d) as one kernel, with the
+ * penalty length h of ins_proj_setup_0/1 (ins_solver_base.cpp:201-214) cached
+ * on the mesh. Per element: velTT = velT - dt * dp, then the element-local CG
+ * solve of (J M + pen G^T D^T J M D G) velTT = J M velTT_0 from velTT_0,
+ * pen = factor * h / (order + 1); 3D preconditioned by (1/J) M^-1 and stopped
+ * at |r|_2 < 1e-8, 2D unpreconditioned and stopped at |r|_2^2 < 1e-16, both
+ * after at most 100 iterations. The reference passes factor = dt in 3D and
+ * dt * 1e3 in 2D. dp (grad p), velT and velTT hold dim components one after the
+ * other (dim x K x Np); velTT must not alias dp or velT. Device pointers; stats,
+ * if not NULL, is a device array of 2 counters (converged elements, iterations
+ * summed over elements) that the call zeroes and the kernel fills, the
+ * reference's num_converge / num_iter (num_cells is K). The _host variant takes
+ * host arrays, is synchronous, and returns stats = {cells, converged,
+ * iterations} as doubles. */
+int sipg_project_velocity(sipg_mesh *m, int order, double dt, double factor, const double *dp,
+                          const double *velT, double *velTT, unsigned long long *stats, void *stream);
+int sipg_project_velocity_host(sipg_mesh *m, int order, double dt, double factor, const double *dp,
+                               const double *velT, double *velTT, double *stats);
+
 /* Number of kernels this library has launched so far in the process
  * (diagnostics for benchmarks; no reference counterpart). */
 int sipg_launch_count(unsigned long long *n);

@@ -63,6 +63,7 @@ struct sipg_mesh {
   std::mutex host_mu;
   sipg::DevBuf geof64, geof32, nbr, fcode, belems;
   sipg::DevBuf tcg64, tcg32;  // geometry blocks of the tensor-core apply (launch_tc_geom)
+  sipg::DevBuf proj_h;        // velocity projection: 1 / max interior-face fscale per element
   int n_belem = 0;
   bool device_ready = false;
   std::mutex dev_mu;

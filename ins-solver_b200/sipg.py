@@ -224,6 +224,38 @@ class Mesh:
             self.h = None
 
 
+
+def projection_factor(dim, dt):
+    """The penalty factor INSSolverBase{3D,2D}::project_velocity passes to the
+    element-local solve: dt in 3D (src/solvers/3d/ins_solver_base.cpp:1082),
+    dt * 1e3 in 2D (src/solvers/2d/ins_solver_base.cpp:916)."""
+    return dt if dim == 3 else dt * 1e3
+
+
+def project_velocity(mesh, order, dt, dp, velT, factor=None):
+    """Element-local velocity projection (div_div = 1) on host arrays.
+
+    dp (pressure gradient) and velT: (dim, K, Np). Returns (velTT, stats) with
+    stats = (cells, converged cells, iterations summed over cells)."""
+    dp = np.ascontiguousarray(dp, dtype=np.float64)
+    velT = np.ascontiguousarray(velT, dtype=np.float64)
+    out = np.empty_like(velT)
+    st = np.zeros(3)
+    f = projection_factor(mesh.dim, dt) if factor is None else factor
+    check(lib().sipg_project_velocity_host(mesh.h, order, C.c_double(dt), C.c_double(f), _dp(dp), _dp(velT),
+                                           _dp(out), _dp(st)))
+    return out, st
+
+
+def project_velocity_device(mesh, order, dt, dp_ptr, velT_ptr, velTT_ptr, stats_ptr=None, factor=None,
+                            stream=None):
+    """Device variant: FP64 device pointers (dim x K x Np); stats_ptr, if given,
+    points to 2 uint64 counters (converged elements, iterations)."""
+    f = projection_factor(mesh.dim, dt) if factor is None else factor
+    check(lib().sipg_project_velocity(mesh.h, order, C.c_double(dt), C.c_double(f), C.c_void_p(dp_ptr),
+                                      C.c_void_p(velT_ptr), C.c_void_p(velTT_ptr), C.c_void_p(stats_ptr or 0),
+                                      C.c_void_p(stream or 0)))
+
 class Operator:
     """SIPG operator on a resident mesh (Poisson / Helmholtz / viscous)."""
 

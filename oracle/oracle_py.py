@@ -251,3 +251,27 @@ def solve(om, b, bc_types, precond=PRE_NONE, factor=None, mm=None, mm_scalar=0.0
     else:
         oracle_lib().oracle_solve(C.byref(om.s), C.byref(o), _d(b), _d(x), C.byref(info))
     return x, info
+
+
+def proj_h(om):
+    """Per-element penalty length of the velocity projection (K values)."""
+    h = np.zeros(om.K)
+    oracle_lib().oracle_proj_h(C.byref(om.s), _d(h))
+    return h
+
+
+def project_velocity(om, dt, factor, dp, velT, use_ref=False):
+    """Element-local velocity projection (pr_projection_method == 1).
+
+    dp, velT: (dim, K, Np). Returns (velTT, stats) with stats = (cells,
+    converged cells, iterations summed over cells)."""
+    dp = np.ascontiguousarray(dp, dtype=np.float64)
+    velT = np.ascontiguousarray(velT, dtype=np.float64)
+    out = np.zeros_like(velT)
+    st = np.zeros(3)
+    args = (C.byref(om.s), C.c_double(dt), C.c_double(factor), _d(dp), _d(velT), _d(out), _d(st))
+    if use_ref:
+        assert ref_lib().ref_project_velocity(*args) == 0
+    else:
+        oracle_lib().oracle_project_velocity(*args)
+    return out, st

@@ -13,6 +13,7 @@
 
 #define DG_MAT_IND(row, col, num_rows, num_cols) ((row) + (col) * (num_rows))
 using std::fmax;
+using std::isnan;
 
 
 // One namespace per (dim, order); geof index macros follow the shared layout.
@@ -121,6 +122,10 @@ int ref_block_diag(const oracle_mesh *m, int ncomp, const int *bc_types, const d
 int ref_solve(const oracle_mesh *m, const oracle_solver_opts *o, const double *b, double *x,
               oracle_solve_info *info) {
   DISPATCH(solve_api(m, o, b, x, info))
+}
+int ref_project_velocity(const oracle_mesh *m, double dt, double factor, const double *dp,
+                         const double *velT, double *velTT, double *stats) {
+  DISPATCH(project_velocity_api(m, dt, factor, dp, velT, velTT, stats))
 }
 // One reference kernel by name on caller buffers (args: its arguments in order),
 // with the reference-element tables of m; -1 for an unknown name or element.

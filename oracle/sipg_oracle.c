@@ -957,3 +957,182 @@ void oracle_solve(const oracle_mesh *m, const oracle_solver_opts *o, const doubl
     free(al);
   }
 }
+
+/* ------------------------------------------------- velocity projection */
+/* Element length scale of the projection penalty: 1 / max over the element's
+ * interior faces of fscale (ins_proj_setup_0.h:1-6 accumulates fscale into a
+ * zeroed per-face array over interior faces only; ins_proj_setup_1.h:1-7 takes
+ * the reciprocal of the maximum). Set-up at src/solvers/3d/ins_solver_base.cpp:201-214
+ * (2D: src/solvers/2d/ins_solver_base.cpp:204-217). */
+void oracle_proj_h(const oracle_mesh *m, double *h) {
+  const int Nf = m->Nf;
+  double *fs = (double *)calloc((size_t)m->K * Nf, sizeof(double));
+  for (int fc = 0; fc < m->F; ++fc) {
+    int eL = m->face2cells[2 * fc], eR = m->face2cells[2 * fc + 1];
+    int fL = m->faceNum[2 * fc], fR = m->faceNum[2 * fc + 1];
+    fs[IDX(eL, fL, Nf)] += m->fscale[IDX(eL, fL, Nf)];
+    fs[IDX(eR, fR, Nf)] += m->fscale[IDX(eR, fR, Nf)];
+  }
+  for (int e = 0; e < m->K; ++e) {
+    double mx = 0.0;
+    for (int f = 0; f < Nf; ++f) mx = fmax(mx, fs[IDX(e, f, Nf)]);
+    h[e] = 1.0 / mx;
+  }
+  free(fs);
+}
+
+/* One element of the divergence-penalised projection operator
+ *   A v = J M v + pen * G^T D^T (J M (D G v)),
+ * applied component-wise exactly as ins_3d_proj_cg_precon.h:31-51 writes it:
+ * divergence d = Dr (G v)_r + Ds (G v)_s [+ Dt (G v)_t], m = J M d,
+ * w_k = Dk^T m, out_c = sum_k G_kc w_k, then out_c <- pen * out_c + J M v_c. */
+static void proj_op(int dim, int Np, const double *Dk[3], const double *M, const double G[3][3],
+                    double J, double pen, double *const v[3], double *out[3], double *w) {
+  double *dv = w, *mv = w + Np, *gv = w + 2 * Np; /* gv: 3 x Np */
+  for (int i = 0; i < Np; ++i)
+    for (int k = 0; k < dim; ++k) {
+      double s = 0.0;
+      for (int c = 0; c < dim; ++c) s += G[k][c] * v[c][i];
+      gv[k * Np + i] = s;
+    }
+  for (int i = 0; i < Np; ++i) {
+    double d = 0.0;
+    for (int k = 0; k < dim; ++k) {
+      double s = 0.0;
+      for (int j = 0; j < Np; ++j) s += Dk[k][i * Np + j] * gv[k * Np + j];
+      d += s;
+    }
+    dv[i] = d;
+  }
+  for (int i = 0; i < Np; ++i) {
+    double s = 0.0;
+    for (int j = 0; j < Np; ++j) s += M[i * Np + j] * dv[j];
+    mv[i] = J * s;
+  }
+  for (int k = 0; k < dim; ++k)
+    for (int i = 0; i < Np; ++i) {
+      double s = 0.0;
+      for (int j = 0; j < Np; ++j) s += Dk[k][j * Np + i] * mv[j];
+      gv[k * Np + i] = s;
+    }
+  for (int c = 0; c < dim; ++c)
+    for (int i = 0; i < Np; ++i) {
+      double s = 0.0, mm = 0.0;
+      for (int k = 0; k < dim; ++k) s += G[k][c] * gv[k * Np + i];
+      for (int j = 0; j < Np; ++j) mm += M[i * Np + j] * v[c][j];
+      out[c][i] = pen * s + J * mm;
+    }
+}
+
+/* INSSolverBase3D::project_velocity with pr_projection_method == 1
+ * (src/solvers/3d/ins_solver_base.cpp:1052-1124): per element,
+ *   velTT = velT - dt * grad p                     (ins_3d_proj_rhs.h:1-13)
+ *   b     = J M velTT                              (mesh->mass)
+ *   pen   = factor * h / (p + 1)                   (ins_3d_proj_pen.h:24-25)
+ *   solve A velTT = b from velTT by CG with the inverse mass matrix (1/J) M^-1
+ *   as preconditioner, |r|_2 < 1e-8, at most 100 iterations
+ *                                                  (ins_3d_proj_cg_precon.h:1-160).
+ * 2D (src/solvers/2d/ins_solver_base.cpp:894-955, ins_proj_cg_2d.h): plain CG,
+ * stopping on |r|_2^2 < 1e-16. The caller's factor is dt in 3D and dt * 1e3 in
+ * 2D (ins_solver_base.cpp:1082 and 2D :916). stats = {cells, converged cells,
+ * iterations summed over cells}; an element counts as converged when it stopped
+ * before 100 iterations with a residual that is not NaN. dp, velT, velTT hold
+ * dim components one after the other (dim x K x Np). */
+void oracle_project_velocity(const oracle_mesh *m, double dt, double factor, const double *dp,
+                             const double *velT, double *velTT, double *stats) {
+  const int dim = m->dim, Np = m->Np, K = m->K, p = m->order;
+  const size_t n = (size_t)K * Np;
+  const int precond = dim == 3;
+  const double tol = dim == 3 ? 1e-8 : 1e-16;
+  const int max_iter = 100;
+  const double *Dk[3] = {m->Dr, m->Ds, m->Dt};
+  double *minv = (double *)malloc(sizeof(double) * Np * Np);
+  memcpy(minv, m->M, sizeof(double) * Np * Np);
+  invert_inplace(minv, Np);
+  double *h = (double *)malloc(sizeof(double) * K);
+  oracle_proj_h(m, h);
+  double *buf = (double *)malloc(sizeof(double) * Np * 27);
+  double cells = 0.0, conv = 0.0, iters = 0.0;
+  for (int e = 0; e < K; ++e) {
+    double G[3][3], J;
+    geo_unpack(m, e, G, &J);
+    const double pen = factor * (h[e] / ((double)p + 1.0));
+    double *x[3], *r[3], *z[3], *pp[3], *ap[3], *b[3];
+    for (int c = 0; c < 3; ++c) {
+      x[c] = buf + (size_t)(c * 6 + 0) * Np; r[c] = buf + (size_t)(c * 6 + 1) * Np;
+      z[c] = buf + (size_t)(c * 6 + 2) * Np; pp[c] = buf + (size_t)(c * 6 + 3) * Np;
+      ap[c] = buf + (size_t)(c * 6 + 4) * Np; b[c] = buf + (size_t)(c * 6 + 5) * Np;
+    }
+    double *w = buf + (size_t)18 * Np;
+    for (int c = 0; c < dim; ++c)
+      for (int i = 0; i < Np; ++i)
+        x[c][i] = velT[c * n + IDX(e, i, Np)] - dt * dp[c * n + IDX(e, i, Np)];
+    for (int c = 0; c < dim; ++c)
+      for (int i = 0; i < Np; ++i) {
+        double s = 0.0;
+        for (int j = 0; j < Np; ++j) s += m->M[i * Np + j] * x[c][j];
+        b[c][i] = J * s;
+      }
+    proj_op(dim, Np, Dk, m->M, G, J, pen, x, ap, w);
+    double res = 0.0;
+    for (int c = 0; c < dim; ++c)
+      for (int i = 0; i < Np; ++i) {
+        r[c][i] = b[c][i] - ap[c][i];
+        res += r[c][i] * r[c][i];
+      }
+    if (precond) res = sqrt(res);
+    for (int c = 0; c < dim; ++c)
+      for (int i = 0; i < Np; ++i) {
+        double s = 0.0;
+        if (precond) {
+          for (int j = 0; j < Np; ++j) s += minv[i * Np + j] * r[c][j];
+          s *= 1.0 / J;
+        } else {
+          s = r[c][i];
+        }
+        z[c][i] = s;
+        pp[c][i] = s;
+      }
+    int it = 0;
+    while (res > tol && it < max_iter) {
+      proj_op(dim, Np, Dk, m->M, G, J, pen, pp, ap, w);
+      double rz = 0.0, pap = 0.0;
+      for (int c = 0; c < dim; ++c)
+        for (int i = 0; i < Np; ++i) { rz += r[c][i] * z[c][i]; pap += pp[c][i] * ap[c][i]; }
+      const double alpha = rz / pap;
+      res = 0.0;
+      for (int c = 0; c < dim; ++c)
+        for (int i = 0; i < Np; ++i) {
+          x[c][i] += alpha * pp[c][i];
+          r[c][i] -= alpha * ap[c][i];
+          res += r[c][i] * r[c][i];
+        }
+      if (precond) res = sqrt(res);
+      if (res < tol) break;
+      double rz_new = 0.0;
+      for (int c = 0; c < dim; ++c)
+        for (int i = 0; i < Np; ++i) {
+          double s = 0.0;
+          if (precond) {
+            for (int j = 0; j < Np; ++j) s += minv[i * Np + j] * r[c][j];
+            s *= 1.0 / J;
+          } else {
+            s = r[c][i];
+          }
+          z[c][i] = s;
+          rz_new += r[c][i] * s;
+        }
+      const double beta = rz_new / rz;
+      for (int c = 0; c < dim; ++c)
+        for (int i = 0; i < Np; ++i) pp[c][i] = z[c][i] + beta * pp[c][i];
+      ++it;
+    }
+    for (int c = 0; c < dim; ++c)
+      for (int i = 0; i < Np; ++i) velTT[c * n + IDX(e, i, Np)] = x[c][i];
+    cells += 1.0;
+    iters += it;
+    if (it < max_iter && !isnan(res)) conv += 1.0;
+  }
+  stats[0] = cells; stats[1] = conv; stats[2] = iters;
+  free(buf); free(h); free(minv);
+}

@@ -136,6 +136,12 @@ void oracle_solve(const oracle_mesh *m, const oracle_solver_opts *o, const doubl
 double oracle_pmg_lambda_max(const oracle_mesh *m, const int *bc_types, const double *factor,
                              int pin_dof, int iters);
 
+/* Velocity projection (pr_projection_method == 1): per-element penalty length
+ * h (K values) and the element-local projection solve; see sipg_oracle.c. */
+void oracle_proj_h(const oracle_mesh *m, double *h);
+void oracle_project_velocity(const oracle_mesh *m, double dt, double factor, const double *dp,
+                             const double *velT, double *velTT, double *stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,158 @@
+"""Element-local velocity projection (INSSolverBase3D::project_velocity with
+div_div = 1, src/solvers/3d/ins_solver_base.cpp:1052-1124; 2D
+src/solvers/2d/ins_solver_base.cpp:894-955).
+
+CPU: the oracle's restatement against the golden vectors made by the
+reference's own kernels (ins_proj_setup_0/1, ins_3d_proj_rhs, ins_3d_proj_pen,
+ins_3d_proj_cg_precon and the 2D twins) and against those kernels on fresh
+cases. GPU: sipg_project_velocity(_host) against the oracle, the device
+counters, argument errors, and a full-size case (32^3 x 6 tets, p = 3).
+
+Tolerances. 3D: the solve is preconditioned by the inverse mass matrix and
+converges in a few iterations per element, so results agree to round-off
+(TOL_PROJ_3D) with identical iteration counts. 2D: the reference's CG is
+unpreconditioned and stops on the absolute |r|_2^2 < 1e-16 of a system scaled by
+the element Jacobian (J ~ h^2), so the solution is fixed only to about
+|A^-1| * 1e-8 ~ 1e-5 of its size: round-off in a different summation order moves
+the last iterates by that much and the iteration count of an element by one
+(the test allows one iteration per element on the total).
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import oracle_py as O
+import sipg
+from helpers import rel_err
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLDEN_PROJ = sorted(glob.glob(os.path.join(HERE, "golden", "projection", "*.npz")))
+
+TOL_PROJ_3D = 1e-12
+TOL_PROJ_2D = 2e-4
+
+
+def case(dim, n, order, seed, dt, jitter=0.1):
+    mesh = sipg.Mesh.box(dim, n, jitter=jitter, seed=seed)
+    t, e = sipg.ref_tables(dim, order), mesh.export(order)
+    rng = np.random.default_rng(seed)
+    velT = rng.uniform(-1, 1, (dim, e["K"], t["Np"]))
+    dp = rng.uniform(-1, 1, (dim, e["K"], t["Np"]))
+    return mesh, O.OMesh(t, e), velT, dp
+
+
+def check_close(dim, got, gst, want, wst):
+    assert gst[0] == wst[0] and gst[1] == wst[1], (gst, wst)
+    if dim == 3:
+        assert rel_err(got, want) < TOL_PROJ_3D
+        assert gst[2] == wst[2], (gst, wst)
+    else:
+        assert rel_err(got, want) < TOL_PROJ_2D
+        assert abs(gst[2] - wst[2]) <= wst[0], (gst, wst)  # at most one iteration per element
+
+
+@pytest.mark.parametrize("path", GOLDEN_PROJ, ids=[os.path.basename(p)[:-4] for p in GOLDEN_PROJ])
+def test_oracle_matches_reference_golden(path):
+    g = dict(np.load(path))
+    dim, n, order, seed = int(g["dim"]), int(g["n"]), int(g["order"]), int(g["seed"])
+    mesh = sipg.Mesh.box(dim, n, jitter=float(g["jitter"]), seed=seed)
+    t, e = sipg.ref_tables(dim, order), mesh.export(order)
+    assert np.array_equal(e["geof"], g["geof"]), "mesh builder drifted from the golden fixture"
+    got, st = O.project_velocity(O.OMesh(t, e), float(g["dt"]), float(g["factor"]), g["dp"], g["velT"])
+    check_close(dim, got, st, g["velTT"], g["stats"])
+
+
+@pytest.mark.parametrize("dim,n,order,dt", [(3, 3, 2, 1e-2), (3, 2, 4, 5e-2), (2, 5, 1, 1e-3), (2, 4, 4, 1e-3)])
+def test_oracle_matches_reference_kernels(dim, n, order, dt):
+    if not O.have_ref():
+        pytest.skip("oracle/_ref not built (the reference tree is not available)")
+    _, om, velT, dp = case(dim, n, order, 7 + order, dt)
+    f = sipg.projection_factor(dim, dt)
+    a, sa = O.project_velocity(om, dt, f, dp, velT)
+    b, sb = O.project_velocity(om, dt, f, dp, velT, use_ref=True)
+    check_close(dim, a, sa, b, sb)
+
+
+def test_oracle_penalty_length_is_inverse_max_interior_fscale():
+    mesh, om, _, _ = case(3, 3, 2, 1, 1e-2)
+    e = mesh.export(2)
+    h = O.proj_h(om)
+    inner = np.zeros_like(e["fscale"])
+    for (eL, eR), (fL, fR) in zip(e["face2cells"], e["faceNum"]):
+        inner[eL, fL] = e["fscale"][eL, fL]
+        inner[eR, fR] = e["fscale"][eR, fR]
+    assert np.array_equal(h, 1.0 / inner.max(axis=1))
+
+
+def test_projection_factor_follows_the_reference():
+    assert sipg.projection_factor(3, 2e-3) == 2e-3
+    assert sipg.projection_factor(2, 2e-3) == pytest.approx(2.0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", GOLDEN_PROJ, ids=[os.path.basename(p)[:-4] for p in GOLDEN_PROJ])
+def test_gpu_matches_reference_golden(path):
+    g = dict(np.load(path))
+    dim, order = int(g["dim"]), int(g["order"])
+    mesh = sipg.Mesh.box(dim, int(g["n"]), jitter=float(g["jitter"]), seed=int(g["seed"]))
+    got, st = sipg.project_velocity(mesh, order, float(g["dt"]), g["dp"], g["velT"], factor=float(g["factor"]))
+    check_close(dim, got, st, g["velTT"], g["stats"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dim,n,order,dt", [(3, 3, 1, 1e-2), (3, 3, 2, 1e-2), (3, 3, 3, 1e-3), (3, 3, 3, 0.2),
+                                            (3, 2, 4, 1e-2), (2, 6, 1, 1e-3), (2, 6, 2, 1e-3), (2, 6, 3, 1e-4),
+                                            (2, 4, 4, 1e-3)])
+def test_gpu_matches_oracle(dim, n, order, dt):
+    mesh, om, velT, dp = case(dim, n, order, 100 + 10 * dim + order, dt)
+    want, wst = O.project_velocity(om, dt, sipg.projection_factor(dim, dt), dp, velT)
+    got, gst = sipg.project_velocity(mesh, order, dt, dp, velT)
+    check_close(dim, got, gst, want, wst)
+
+
+@pytest.mark.gpu
+def test_gpu_device_entry_point_counters_and_repeatability():
+    dim, order, dt = 3, 3, 0.05
+    mesh, om, velT, dp = case(dim, 3, order, 3, dt)
+    host, hst = sipg.project_velocity(mesh, order, dt, dp, velT)
+    d_dp, d_v = sipg.DeviceVector(dp), sipg.DeviceVector(velT)
+    d_out = sipg.DeviceVector(np.zeros_like(velT))
+    d_st = sipg.DeviceVector(np.full(2, 12345, np.uint64))
+    for _ in range(2):  # the counters are zeroed by every call
+        sipg.project_velocity_device(mesh, order, dt, d_dp.ptr, d_v.ptr, d_out.ptr, d_st.ptr)
+        assert np.array_equal(d_out.get(), host)
+        st = d_st.get()
+        assert st[0] == hst[1] and st[1] == hst[2]
+
+
+@pytest.mark.gpu
+def test_gpu_rejects_aliasing_and_bad_arguments():
+    mesh, _, velT, dp = case(3, 2, 2, 1, 1e-2)
+    d_dp, d_v = sipg.DeviceVector(dp), sipg.DeviceVector(velT)
+    with pytest.raises(sipg.SipgError):
+        sipg.project_velocity_device(mesh, 2, 1e-2, d_dp.ptr, d_v.ptr, d_v.ptr)
+    with pytest.raises(sipg.SipgError):
+        sipg.project_velocity_device(mesh, 5, 1e-2, d_dp.ptr, d_v.ptr, d_dp.ptr)
+    with pytest.raises(sipg.SipgError):
+        sipg.project_velocity(mesh, 2, float("nan"), dp, velT)
+
+
+@pytest.mark.gpu
+def test_gpu_full_size_32cube_p3():
+    """32^3 x 6 = 196,608 tets at p = 3 (the rising-bubble mesh): every element
+    converges, the result equals the oracle's, and a field with zero pressure
+    gradient that is constant per element is returned unchanged (its divergence
+    vanishes to round-off, so the initial residual is below the tolerance and no
+    iteration runs)."""
+    dim, order, dt = 3, 3, 1e-3
+    mesh, om, velT, dp = case(dim, 32, order, 20261203, dt)
+    got, st = sipg.project_velocity(mesh, order, dt, dp, velT)
+    assert st[0] == st[1] == mesh.K
+    want, wst = O.project_velocity(om, dt, dt, dp, velT)
+    check_close(dim, got, st, want, wst)
+    const = np.repeat(velT[:, :, :1], velT.shape[2], axis=2)
+    out, st0 = sipg.project_velocity(mesh, order, dt, np.zeros_like(dp), const)
+    assert st0[2] == 0
+    assert rel_err(out, const) < 1e-13
