@@ -13,15 +13,20 @@
 // unpreconditioned in 2D (ins_proj_cg_2d.h), stopping on the absolute residual
 // (3D |r|_2 < 1e-8, 2D |r|_2^2 < 1e-16) or after 100 iterations.
 //
-// Here the whole sequence is one kernel: a warp owns an element (a lane per
-// node, two nodes per lane at p = 4), reads velT, grad p, its geometric factors
-// and h once, iterates the CG entirely in registers and shared memory, and
-// writes velTT once. The reference-element matrices sit in shared memory in the
-// layouts that make every product conflict-free (lane i reads consecutive
-// doubles; the vector operand is a broadcast), the warp's vectors are exchanged
-// through a per-warp shared buffer, and the dot products are xor-butterfly warp
-// reductions, which leave the same bits in every lane so the stopping test is
-// warp-uniform. The counters the reference accumulates (cells, converged cells,
+// Here the whole sequence is one kernel. A warp owns two elements (one at
+// p = 4 in 3D), a lane per node: it reads velT, grad p, the geometric factors
+// and h once, iterates both elements' CG in registers and shared memory, and
+// writes velTT once. The solve is bound by shared-memory bandwidth (the
+// reference-element matrices are read from shared memory at every product), so
+// the kernel minimises shared traffic per multiply-add: each matrix entry read
+// serves both elements of the warp, matrix entries and vector values are read
+// in 16-byte pairs (column pairs of Np rows; vectors padded to an even length
+// with zeros), and in 3D the mass term J M p of the operator is carried by the
+// recursion J M p_new = r_new + beta J M p (since J M z = r for z = (1/J) M^-1 r)
+// instead of three mass products per iteration. Dot products are xor-butterfly
+// warp reductions, which leave the same bits in every lane, so the stopping
+// tests are warp-uniform; an element that has stopped idles while the other
+// finishes. The counters the reference accumulates (cells, converged cells,
 // iterations) are summed per warp and added once per warp.
 #include <cuda_runtime.h>
 
@@ -39,18 +44,25 @@
 namespace sipg {
 namespace {
 
-constexpr int kProjWarps = 8;   // warps (elements in flight) per CTA
+constexpr int kProjWarps = 4;   // warps per CTA
 constexpr int kProjMaxIter = 100;
 
 __host__ __device__ constexpr int proj_np(int D, int P) {
   return D == 2 ? (P + 1) * (P + 2) / 2 : (P + 1) * (P + 2) * (P + 3) / 6;
 }
-// Matrices in the blob: D_k by columns (D of them), D_k by rows (D), M, and M^-1 in 3D.
+// Np rounded up to even: vectors and matrix columns are read in pairs.
+__host__ __device__ constexpr int proj_npe(int D, int P) { return (proj_np(D, P) + 1) & ~1; }
+// Elements per warp: two while a node per lane covers the element, else one.
+__host__ __device__ constexpr int proj_epw(int D, int P) { return proj_np(D, P) <= 32 ? 2 : 1; }
+// Matrices in the blob: D_k for products (D), D_k^T for products (D), M, and M^-1 in 3D;
+// each stored as Npe/2 column pairs of Np rows: A(i, 2q + t) at (q * Np + i) * 2 + t.
 __host__ __device__ constexpr int proj_nmat(int D) { return 2 * D + 1 + (D == 3 ? 1 : 0); }
 template <int D, int P>
+__host__ __device__ constexpr int proj_mat_doubles() { return proj_np(D, P) * proj_npe(D, P); }
+template <int D, int P>
 __host__ __device__ constexpr int proj_smem_doubles() {
-  // matrices + per warp: A (D x Np), B (D x Np), C (Np)
-  return proj_nmat(D) * proj_np(D, P) * proj_np(D, P) + kProjWarps * (2 * D + 1) * proj_np(D, P);
+  // matrices + per warp and element: A (D x Npe), B (D x Npe), C (Npe)
+  return proj_nmat(D) * proj_mat_doubles<D, P>() + kProjWarps * proj_epw(D, P) * (2 * D + 1) * proj_npe(D, P);
 }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -59,241 +71,324 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// One element, one warp. NPL = nodes per lane.
+// y_e(i) = sum_j A(i, j) v_e(j) for the E vectors v_e (stride vs doubles apart),
+// even and odd j summed separately (two independent FMA chains); A in the pair
+// layout, v padded with zeros to Npe.
+template <int NP, int NPE, int E>
+__device__ __forceinline__ void mat_vec(const double* __restrict__ A, const double* v, int vs, int i,
+                                        double (&y)[E]) {
+  double y1[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) y[e] = y1[e] = 0.0;
+#pragma unroll 5
+  for (int q = 0; q < NPE / 2; ++q) {
+    const double2 a = *reinterpret_cast<const double2*>(A + (q * NP + i) * 2);
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const double2 x = *reinterpret_cast<const double2*>(v + e * vs + 2 * q);
+      y[e] += a.x * x.x;
+      y1[e] += a.y * x.y;
+    }
+  }
+#pragma unroll
+  for (int e = 0; e < E; ++e) y[e] += y1[e];
+}
+
+// E elements per warp (a lane per node, NPL nodes per lane).
 template <int D, int P>
 __global__ void __launch_bounds__(kProjWarps * 32)
 k_proj_cg(int K, const double* __restrict__ geof, const double* __restrict__ hK,
           const double* __restrict__ mats, double dt, double factor, const double* __restrict__ dp,
           const double* __restrict__ velT, double* __restrict__ velTT,
           unsigned long long* __restrict__ stats) {
-  constexpr int NP = proj_np(D, P), NPP = NP * NP, NPL = (NP + 31) / 32, NG = D == 3 ? 10 : 5;
+  constexpr int NP = proj_np(D, P), NPE = proj_npe(D, P), NPL = (NP + 31) / 32, NG = D == 3 ? 10 : 5;
+  constexpr int E = proj_epw(D, P), MAT = proj_mat_doubles<D, P>();
+  constexpr int WB = E * (2 * D + 1) * NPE;  // per-warp buffer
   constexpr bool kPre = D == 3;
   extern __shared__ double sm[];
-  double* sDc = sm;                       // D_k(i, j) at k*NPP + j*NP + i
-  double* sDr = sm + D * NPP;             // D_k(j, i) at k*NPP + j*NP + i
-  double* sM = sm + 2 * D * NPP;          // M(i, j) at j*NP + i
-  double* sMi = sm + (2 * D + 1) * NPP;   // M^-1(i, j) at j*NP + i (3D)
+  const double* sD = sm;                  // D_k, k < D
+  const double* sDt = sm + D * MAT;       // D_k^T
+  const double* sM = sm + 2 * D * MAT;    // M
+  const double* sMi = sm + (2 * D + 1) * MAT;  // M^-1 (3D)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double* sA = sm + proj_nmat(D) * NPP + warp * (2 * D + 1) * NP;
-  double* sB = sA + D * NP;
-  double* sC = sB + D * NP;
-  for (int i = threadIdx.x; i < proj_nmat(D) * NPP; i += blockDim.x) sm[i] = mats[i];
+  double* sA = sm + proj_nmat(D) * MAT + warp * WB;  // [E][D][NPE]
+  double* sB = sA + E * D * NPE;                      // [E][D][NPE]
+  double* sC = sB + E * D * NPE;                      // [E][NPE]
+  for (int i = threadIdx.x; i < proj_nmat(D) * MAT; i += blockDim.x) sm[i] = mats[i];
+  // zero the warp buffers once: their pad entries (Np..Npe-1) stay zero
+  for (int i = lane; i < WB; i += 32) sA[i] = 0.0;
   __syncthreads();
 
   const size_t n = (size_t)K * NP;
   const double tol = kPre ? 1e-8 : 1e-16;
   unsigned long long n_conv = 0, n_iter = 0;
 
-  for (int e = blockIdx.x * kProjWarps + warp; e < K; e += gridDim.x * kProjWarps) {
-    double G[3][3] = {};
-    double J;
-    if (D == 3) {
+  for (int e0 = (blockIdx.x * kProjWarps + warp) * E; e0 < K; e0 += gridDim.x * kProjWarps * E) {
+    double G[E][3][3], J[E], pen[E], inv_J[E];
+    bool valid[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int el = e0 + e;
+      valid[e] = el < K;
+      const int ec = valid[e] ? el : e0;
+      const double* g = geof + (size_t)ec * NG;
 #pragma unroll
       for (int k = 0; k < 3; ++k)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) G[k][c] = __ldg(geof + (size_t)e * NG + k * 3 + c);
-      J = __ldg(geof + (size_t)e * NG + 9);
-    } else {
-      G[0][0] = __ldg(geof + (size_t)e * NG + 0); G[0][1] = __ldg(geof + (size_t)e * NG + 1);
-      G[1][0] = __ldg(geof + (size_t)e * NG + 2); G[1][1] = __ldg(geof + (size_t)e * NG + 3);
-      J = __ldg(geof + (size_t)e * NG + 4);
+        for (int c = 0; c < 3; ++c) G[e][k][c] = 0.0;
+      if (D == 3) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) G[e][k][c] = __ldg(g + k * 3 + c);
+        J[e] = __ldg(g + 9);
+      } else {
+        G[e][0][0] = __ldg(g + 0); G[e][0][1] = __ldg(g + 1);
+        G[e][1][0] = __ldg(g + 2); G[e][1][1] = __ldg(g + 3);
+        J[e] = __ldg(g + 4);
+      }
+      pen[e] = factor * (__ldg(hK + ec) / ((double)P + 1.0));
+      inv_J[e] = 1.0 / J[e];
     }
-    const double pen = factor * (__ldg(hK + e) / ((double)P + 1.0));
-    const double inv_J = 1.0 / J;
 
-    double x[D][NPL], r[D][NPL], z[D][NPL], p[D][NPL], ap[D][NPL], mv[D][NPL];
+    double x[E][D][NPL], r[E][D][NPL], z[E][D][NPL], p[E][D][NPL], ap[E][D][NPL], q[E][D][NPL];
 
-    // out = pen * G^T D^T (J M (D G v)) + J M v; mvo = J M v. v is read from sB.
-    auto apply = [&](double (&out)[D][NPL], double (&mvo)[D][NPL]) {
-      // stage 1: (G v)_k at the lane's nodes -> sA (v already in sB)
+    // ap = pen * G^T D^T (J M (D G v)) + mass, v read from sB; mass = J M v when
+    // explicit_mass (also returned in q), else the q carried by the caller.
+    auto apply = [&](bool explicit_mass) {
 #pragma unroll
-      for (int q = 0; q < NPL; ++q) {
-        const int i = lane + 32 * q;
-        if (i < NP) {
-#pragma unroll
-          for (int k = 0; k < D; ++k) {
-            double s = 0.0;
-#pragma unroll
-            for (int c = 0; c < D; ++c) s += G[k][c] * sB[c * NP + i];
-            sA[k * NP + i] = s;
-          }
-        }
-      }
-      __syncwarp();
-      // stage 2: divergence d = sum_k D_k (G v)_k -> sC
-#pragma unroll
-      for (int q = 0; q < NPL; ++q) {
-        const int i = lane + 32 * q;
-        if (i < NP) {
-          double d = 0.0;
-#pragma unroll
-          for (int k = 0; k < D; ++k) {
-            double s = 0.0;
-#pragma unroll 4
-            for (int j = 0; j < NP; ++j) s += sDc[k * NPP + j * NP + i] * sA[k * NP + j];
-            d += s;
-          }
-          sC[i] = d;
-        }
-      }
-      __syncwarp();
-      // stage 3: m = J M d -> sA[0..NP)
-#pragma unroll
-      for (int q = 0; q < NPL; ++q) {
-        const int i = lane + 32 * q;
-        if (i < NP) {
-          double s = 0.0;
-#pragma unroll 4
-          for (int j = 0; j < NP; ++j) s += sM[j * NP + i] * sC[j];
-          sA[i] = J * s;
-        }
-      }
-      __syncwarp();
-      // stages 4-5: w_k = D_k^T m, out_c = pen * sum_k G_kc w_k + J (M v_c)
-#pragma unroll
-      for (int q = 0; q < NPL; ++q) {
-        const int i = lane + 32 * q;
-        if (i < NP) {
-          double w[D];
-#pragma unroll
-          for (int k = 0; k < D; ++k) {
-            double s = 0.0;
-#pragma unroll 4
-            for (int j = 0; j < NP; ++j) s += sDr[k * NPP + j * NP + i] * sA[j];
-            w[k] = s;
-          }
-#pragma unroll
-          for (int c = 0; c < D; ++c) {
-            double s = 0.0, mm = 0.0;
-#pragma unroll
-            for (int k = 0; k < D; ++k) s += G[k][c] * w[k];
-#pragma unroll 4
-            for (int j = 0; j < NP; ++j) mm += sM[j * NP + i] * sB[c * NP + j];
-            mvo[c][q] = J * mm;
-            out[c][q] = pen * s + mvo[c][q];
-          }
-        } else {
-#pragma unroll
-          for (int c = 0; c < D; ++c) { out[c][q] = 0.0; mvo[c][q] = 0.0; }
-        }
-      }
-    };
-    // z = (1/J) M^-1 r (3D) or r (2D); returns the lane's part of r . z
-    auto precondition = [&]() {
-      double rz = 0.0;
-      if (kPre) {
-        __syncwarp();
-#pragma unroll
-        for (int q = 0; q < NPL; ++q) {
-          const int i = lane + 32 * q;
-          if (i < NP)
-#pragma unroll
-            for (int c = 0; c < D; ++c) sB[c * NP + i] = r[c][q];
-        }
-        __syncwarp();
-      }
-#pragma unroll
-      for (int q = 0; q < NPL; ++q) {
-        const int i = lane + 32 * q;
-#pragma unroll
-        for (int c = 0; c < D; ++c) {
-          double s = 0.0;
-          if (i < NP) {
-            if (kPre) {
-#pragma unroll 4
-              for (int j = 0; j < NP; ++j) s += sMi[j * NP + i] * sB[c * NP + j];
-              s = inv_J * s;
-            } else {
-              s = r[c][q];
-            }
-          }
-          z[c][q] = s;
-          rz += r[c][q] * s;
-        }
-      }
-      return rz;
-    };
-    auto stage_v = [&](const double (&v)[D][NPL]) {
-      __syncwarp();
-#pragma unroll
-      for (int q = 0; q < NPL; ++q) {
-        const int i = lane + 32 * q;
+      for (int u = 0; u < NPL; ++u) {  // (G v)_k -> sA
+        const int i = lane + 32 * u;
         if (i < NP)
 #pragma unroll
-          for (int c = 0; c < D; ++c) sB[c * NP + i] = v[c][q];
+          for (int e = 0; e < E; ++e)
+#pragma unroll
+            for (int k = 0; k < D; ++k) {
+              double s = 0.0;
+#pragma unroll
+              for (int c = 0; c < D; ++c) s += G[e][k][c] * sB[(e * D + c) * NPE + i];
+              sA[(e * D + k) * NPE + i] = s;
+            }
       }
       __syncwarp();
+#pragma unroll
+      for (int u = 0; u < NPL; ++u) {  // divergence d = sum_k D_k (G v)_k -> sC
+        const int i = lane + 32 * u;
+        if (i < NP) {
+          double d[E];
+#pragma unroll
+          for (int e = 0; e < E; ++e) d[e] = 0.0;
+#pragma unroll
+          for (int k = 0; k < D; ++k) {
+            double s[E];
+            mat_vec<NP, NPE, E>(sD + k * MAT, sA + k * NPE, D * NPE, i, s);
+#pragma unroll
+            for (int e = 0; e < E; ++e) d[e] += s[e];
+          }
+#pragma unroll
+          for (int e = 0; e < E; ++e) sC[e * NPE + i] = d[e];
+        }
+      }
+      __syncwarp();
+#pragma unroll
+      for (int u = 0; u < NPL; ++u) {  // m = J M d -> sA[e][0]
+        const int i = lane + 32 * u;
+        if (i < NP) {
+          double s[E];
+          mat_vec<NP, NPE, E>(sM, sC, NPE, i, s);
+#pragma unroll
+          for (int e = 0; e < E; ++e) sA[e * D * NPE + i] = J[e] * s[e];
+        }
+      }
+      __syncwarp();
+#pragma unroll
+      for (int u = 0; u < NPL; ++u) {  // w_k = D_k^T m; ap_c = pen sum_k G_kc w_k + mass_c
+        const int i = lane + 32 * u;
+        if (i < NP) {
+          double w[D][E];
+#pragma unroll
+          for (int k = 0; k < D; ++k) mat_vec<NP, NPE, E>(sDt + k * MAT, sA, D * NPE, i, w[k]);
+          if (explicit_mass)
+#pragma unroll
+            for (int c = 0; c < D; ++c) {
+              double s[E];
+              mat_vec<NP, NPE, E>(sM, sB + c * NPE, D * NPE, i, s);
+#pragma unroll
+              for (int e = 0; e < E; ++e) q[e][c][u] = J[e] * s[e];
+            }
+#pragma unroll
+          for (int e = 0; e < E; ++e)
+#pragma unroll
+            for (int c = 0; c < D; ++c) {
+              double s = 0.0;
+#pragma unroll
+              for (int k = 0; k < D; ++k) s += G[e][k][c] * w[k][e];
+              ap[e][c][u] = pen[e] * s + q[e][c][u];
+            }
+        } else {
+#pragma unroll
+          for (int e = 0; e < E; ++e)
+#pragma unroll
+            for (int c = 0; c < D; ++c) { ap[e][c][u] = 0.0; q[e][c][u] = 0.0; }
+        }
+      }
+    };
+    auto stage = [&](const double (&v)[E][D][NPL]) {
+      __syncwarp();
+#pragma unroll
+      for (int u = 0; u < NPL; ++u) {
+        const int i = lane + 32 * u;
+        if (i < NP)
+#pragma unroll
+          for (int e = 0; e < E; ++e)
+#pragma unroll
+            for (int c = 0; c < D; ++c) sB[(e * D + c) * NPE + i] = v[e][c][u];
+      }
+      __syncwarp();
+    };
+    // z = (1/J) M^-1 r (3D) or r (2D); rz = r . z per element (warp sums)
+    auto precondition = [&](double (&rz)[E]) {
+      if (kPre) stage(r);
+#pragma unroll
+      for (int e = 0; e < E; ++e) rz[e] = 0.0;
+#pragma unroll
+      for (int u = 0; u < NPL; ++u) {
+        const int i = lane + 32 * u;
+#pragma unroll
+        for (int c = 0; c < D; ++c) {
+          double s[E];
+          if (kPre && i < NP) {
+            mat_vec<NP, NPE, E>(sMi, sB + c * NPE, D * NPE, i, s);
+#pragma unroll
+            for (int e = 0; e < E; ++e) s[e] = inv_J[e] * s[e];
+          } else {
+#pragma unroll
+            for (int e = 0; e < E; ++e) s[e] = i < NP ? r[e][c][u] : 0.0;
+          }
+#pragma unroll
+          for (int e = 0; e < E; ++e) {
+            z[e][c][u] = s[e];
+            rz[e] += r[e][c][u] * s[e];
+          }
+        }
+      }
+#pragma unroll
+      for (int e = 0; e < E; ++e) rz[e] = warp_sum(rz[e]);
     };
 
     // velTT = velT - dt grad p: the initial guess and, through J M, the right-hand side
 #pragma unroll
-    for (int q = 0; q < NPL; ++q) {
-      const int i = lane + 32 * q;
+    for (int e = 0; e < E; ++e)
 #pragma unroll
-      for (int c = 0; c < D; ++c) {
-        const size_t g = c * n + (size_t)e * NP + i;
-        x[c][q] = i < NP ? __ldg(velT + g) - dt * __ldg(dp + g) : 0.0;
-      }
-    }
-    stage_v(x);
-    apply(ap, mv);
-    double res = 0.0;
-#pragma unroll
-    for (int q = 0; q < NPL; ++q)
-#pragma unroll
-      for (int c = 0; c < D; ++c) {
-        r[c][q] = mv[c][q] - ap[c][q];
-        res += r[c][q] * r[c][q];
-      }
-    res = warp_sum(res);
-    if (kPre) res = sqrt(res);
-    double rz = warp_sum(precondition());
-#pragma unroll
-    for (int q = 0; q < NPL; ++q)
-#pragma unroll
-      for (int c = 0; c < D; ++c) p[c][q] = z[c][q];
-
-    int it = 0;
-    while (res > tol && it < kProjMaxIter) {
-      stage_v(p);
-      apply(ap, mv);
-      double pap = 0.0;
-#pragma unroll
-      for (int q = 0; q < NPL; ++q)
-#pragma unroll
-        for (int c = 0; c < D; ++c) pap += p[c][q] * ap[c][q];
-      pap = warp_sum(pap);
-      const double alpha = rz / pap;
-      res = 0.0;
-#pragma unroll
-      for (int q = 0; q < NPL; ++q)
+      for (int u = 0; u < NPL; ++u) {
+        const int i = lane + 32 * u;
 #pragma unroll
         for (int c = 0; c < D; ++c) {
-          x[c][q] += alpha * p[c][q];
-          r[c][q] -= alpha * ap[c][q];
-          res += r[c][q] * r[c][q];
+          const size_t g = c * n + (size_t)(e0 + e) * NP + i;
+          x[e][c][u] = (valid[e] && i < NP) ? __ldg(velT + g) - dt * __ldg(dp + g) : 0.0;
         }
-      res = warp_sum(res);
-      if (kPre) res = sqrt(res);
-      if (res < tol) break;
-      const double rz_new = warp_sum(precondition());
-      const double beta = rz_new / rz;
-      rz = rz_new;
+      }
+    stage(x);
+    apply(true);  // q = J M x is the right-hand side, ap = A x
+    double res[E], rz[E];
+    bool active[E];
+    int it[E];
 #pragma unroll
-      for (int q = 0; q < NPL; ++q)
+    for (int e = 0; e < E; ++e) {
+      double s = 0.0;
 #pragma unroll
-        for (int c = 0; c < D; ++c) p[c][q] = z[c][q] + beta * p[c][q];
-      ++it;
+      for (int u = 0; u < NPL; ++u)
+#pragma unroll
+        for (int c = 0; c < D; ++c) {
+          r[e][c][u] = q[e][c][u] - ap[e][c][u];
+          s += r[e][c][u] * r[e][c][u];
+        }
+      s = warp_sum(s);
+      res[e] = kPre ? sqrt(s) : s;
+      it[e] = 0;
+      active[e] = valid[e] && res[e] > tol;
+    }
+    precondition(rz);
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+#pragma unroll
+      for (int u = 0; u < NPL; ++u)
+#pragma unroll
+        for (int c = 0; c < D; ++c) {
+          p[e][c][u] = z[e][c][u];
+          q[e][c][u] = r[e][c][u];  // J M p = J M z = r (3D)
+        }
+
+    bool any = false;
+#pragma unroll
+    for (int e = 0; e < E; ++e) any |= active[e];
+    while (any) {
+      stage(p);
+      apply(!kPre);  // 3D: J M p is carried in q
+      double pap[E];
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        double s = 0.0;
+#pragma unroll
+        for (int u = 0; u < NPL; ++u)
+#pragma unroll
+          for (int c = 0; c < D; ++c) s += p[e][c][u] * ap[e][c][u];
+        pap[e] = warp_sum(s);
+      }
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const double alpha = rz[e] / pap[e];
+        double s = 0.0;
+#pragma unroll
+        for (int u = 0; u < NPL; ++u)
+#pragma unroll
+          for (int c = 0; c < D; ++c) {
+            if (active[e]) {
+              x[e][c][u] += alpha * p[e][c][u];
+              r[e][c][u] -= alpha * ap[e][c][u];
+            }
+            s += r[e][c][u] * r[e][c][u];
+          }
+        s = warp_sum(s);
+        if (active[e]) {
+          res[e] = kPre ? sqrt(s) : s;
+          if (res[e] < tol) active[e] = false;  // the reference's break: not counted
+        }
+      }
+      double rz_new[E];
+      precondition(rz_new);
+      any = false;
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        if (active[e]) {
+          const double beta = rz_new[e] / rz[e];
+          rz[e] = rz_new[e];
+#pragma unroll
+          for (int u = 0; u < NPL; ++u)
+#pragma unroll
+            for (int c = 0; c < D; ++c) {
+              p[e][c][u] = z[e][c][u] + beta * p[e][c][u];
+              if (kPre) q[e][c][u] = r[e][c][u] + beta * q[e][c][u];
+            }
+          ++it[e];
+          active[e] = res[e] > tol && it[e] < kProjMaxIter;
+        }
+        any |= active[e];
+      }
     }
 #pragma unroll
-    for (int q = 0; q < NPL; ++q) {
-      const int i = lane + 32 * q;
-      if (i < NP)
+    for (int e = 0; e < E; ++e) {
+      if (!valid[e]) continue;
 #pragma unroll
-        for (int c = 0; c < D; ++c) velTT[c * n + (size_t)e * NP + i] = x[c][q];
+      for (int u = 0; u < NPL; ++u) {
+        const int i = lane + 32 * u;
+        if (i < NP)
+#pragma unroll
+          for (int c = 0; c < D; ++c) velTT[c * n + (size_t)(e0 + e) * NP + i] = x[e][c][u];
+      }
+      n_iter += (unsigned long long)it[e];
+      n_conv += (it[e] < kProjMaxIter && !isnan(res[e])) ? 1ull : 0ull;
     }
-    n_iter += (unsigned long long)it;
-    n_conv += (it < kProjMaxIter && !isnan(res)) ? 1ull : 0ull;
   }
   if (stats && lane == 0) {
     atomicAdd(stats + 0, n_conv);
@@ -317,20 +412,22 @@ const ProjMats& proj_mats(int dim, int order) {
   if (slot) return *slot;
   const DevRef& dr = dev_ref(dim, order);
   const RefElement& ref = dr.ref;
-  const int Np = ref.Np, NPP = Np * Np;
-  const std::vector<double>* Dk[3] = {&ref.Dr, &ref.Ds, &ref.Dt};
-  std::vector<double> b((size_t)proj_nmat(dim) * NPP);
-  for (int k = 0; k < dim; ++k)
+  const int Np = ref.Np, Npe = (Np + 1) & ~1;
+  const size_t MAT = (size_t)Np * Npe;
+  std::vector<double> b((size_t)proj_nmat(dim) * MAT, 0.0);  // pad columns stay zero
+  // A(i, j) of matrix m at m * MAT + ((j / 2) * Np + i) * 2 + j % 2; rm: row-major source
+  auto put = [&](int m, const std::vector<double>& rm, bool transpose) {
     for (int i = 0; i < Np; ++i)
-      for (int j = 0; j < Np; ++j) {
-        b[(size_t)k * NPP + j * Np + i] = (*Dk[k])[(size_t)i * Np + j];           // by columns
-        b[(size_t)(dim + k) * NPP + j * Np + i] = (*Dk[k])[(size_t)j * Np + i];   // by rows
-      }
-  for (int i = 0; i < Np; ++i)
-    for (int j = 0; j < Np; ++j) {
-      b[(size_t)2 * dim * NPP + j * Np + i] = ref.M[(size_t)i * Np + j];
-      if (dim == 3) b[(size_t)(2 * dim + 1) * NPP + j * Np + i] = ref.Minv[(size_t)i * Np + j];
-    }
+      for (int j = 0; j < Np; ++j)
+        b[m * MAT + ((size_t)(j / 2) * Np + i) * 2 + j % 2] = transpose ? rm[(size_t)j * Np + i] : rm[(size_t)i * Np + j];
+  };
+  const std::vector<double>* Dk[3] = {&ref.Dr, &ref.Ds, &ref.Dt};
+  for (int k = 0; k < dim; ++k) {
+    put(k, *Dk[k], false);
+    put(dim + k, *Dk[k], true);
+  }
+  put(2 * dim, ref.M, false);
+  if (dim == 3) put(2 * dim + 1, ref.Minv, false);
   auto pm = std::make_unique<ProjMats>();
   pm->Np = Np;
   pm->blob = DevBuf(b.size() * sizeof(double));
@@ -421,15 +518,25 @@ extern "C" int sipg_project_velocity_host(sipg_mesh* m, int order, double dt, do
     if (!m || order < 1 || order > 4 || !dp || !velT || !velTT)
       throw Error(SIPG_INVALID_ARG, "project_velocity: null mesh/array or order outside 1..4");
     const size_t n = (size_t)m->dim * m->K * np_of(m->dim, order), bytes = n * sizeof(double);
-    DevBuf d_dp(std::max<size_t>(bytes, 8)), d_v(std::max<size_t>(bytes, 8)), d_out(std::max<size_t>(bytes, 8));
-    DevBuf d_st(2 * sizeof(unsigned long long));
-    SIPG_CUDA(cudaMemcpy(d_dp.p, dp, bytes, cudaMemcpyHostToDevice));
-    SIPG_CUDA(cudaMemcpy(d_v.p, velT, bytes, cudaMemcpyHostToDevice));
-    project_device(m, order, dt, factor, d_dp.as<double>(), d_v.as<double>(), d_out.as<double>(),
-                   d_st.as<unsigned long long>(), 0);
+    // device copies stay on the mesh between calls (grown on demand), so a time
+    // step's projection allocates nothing after the first call
+    std::lock_guard<std::mutex> lk(m->proj_mu);
+    const size_t need = 3 * bytes + 2 * sizeof(unsigned long long);
+    if (m->proj_io.bytes < need) {
+      m->proj_io = DevBuf();
+      m->proj_io = DevBuf(need);
+    }
+    char* base = m->proj_io.as<char>();
+    double* d_dp = reinterpret_cast<double*>(base);
+    double* d_v = reinterpret_cast<double*>(base + bytes);
+    double* d_out = reinterpret_cast<double*>(base + 2 * bytes);
+    auto* d_st = reinterpret_cast<unsigned long long*>(base + 3 * bytes);
+    SIPG_CUDA(cudaMemcpy(d_dp, dp, bytes, cudaMemcpyHostToDevice));
+    SIPG_CUDA(cudaMemcpy(d_v, velT, bytes, cudaMemcpyHostToDevice));
+    project_device(m, order, dt, factor, d_dp, d_v, d_out, d_st, 0);
     unsigned long long st[2] = {0, 0};
-    SIPG_CUDA(cudaMemcpy(velTT, d_out.p, bytes, cudaMemcpyDeviceToHost));
-    SIPG_CUDA(cudaMemcpy(st, d_st.p, sizeof(st), cudaMemcpyDeviceToHost));
+    SIPG_CUDA(cudaMemcpy(velTT, d_out, bytes, cudaMemcpyDeviceToHost));
+    SIPG_CUDA(cudaMemcpy(st, d_st, sizeof(st), cudaMemcpyDeviceToHost));
     if (stats) {
       stats[0] = (double)m->K;
       stats[1] = (double)st[0];

@@ -461,7 +461,7 @@ int sipg_mesh_export(const sipg_mesh* mc, int order, double* geof, double* nx, d
 int sipg_mesh_device_bytes(const sipg_mesh* m, size_t* bytes) {
   return guarded([&] {
     *bytes = m->geof64.bytes + m->geof32.bytes + m->nbr.bytes + m->fcode.bytes + m->belems.bytes +
-             m->tcg64.bytes + m->tcg32.bytes;
+             m->tcg64.bytes + m->tcg32.bytes + m->proj_h.bytes + m->proj_io.bytes;
   });
 }
 

@@ -64,6 +64,8 @@ struct sipg_mesh {
   sipg::DevBuf geof64, geof32, nbr, fcode, belems;
   sipg::DevBuf tcg64, tcg32;  // geometry blocks of the tensor-core apply (launch_tc_geom)
   sipg::DevBuf proj_h;        // velocity projection: 1 / max interior-face fscale per element
+  sipg::DevBuf proj_io;       // velocity projection: device copies for the host-buffer entry point
+  std::mutex proj_mu;         // serialises host-buffer projections on this mesh
   int n_belem = 0;
   bool device_ready = false;
   std::mutex dev_mu;
