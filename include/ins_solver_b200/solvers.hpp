@@ -11,7 +11,9 @@
 //     mp_ins_solver.cpp:85-89);
 //   Matrix3Vec, FactorViscousMatrix3D, ViscousMatrix3D and ViscousSolver3D
 //     (include/slip_matrix/3d/*.h);
-//   initial_guess_extrapolation / add_to_pr_history (ins_solver_base.cpp:1374-1388).
+//   initial_guess_extrapolation / add_to_pr_history (ins_solver_base.cpp:1374-1388);
+//   the element-local velocity projection of INSSolverBase3D/2D::project_velocity
+//     with div_div = 1 (ins_solver_base.cpp:1052-1124, 2D :894-955).
 //
 // The reference passes OP2 op_dats; here an op_dat is represented by a view of
 // its host array (Dat: `dim` values per set element, element-major, which is the
@@ -475,6 +477,45 @@ class PressureHistory {
  private:
   size_t max_;
   std::vector<std::pair<double, std::vector<double>>> hist_;
+};
+
+// Element-local velocity projection of the pressure step: the body of
+// INSSolverBase3D::project_velocity / INSSolverBase2D::project_velocity with
+// div_div = 1 (src/solvers/3d/ins_solver_base.cpp:1052-1124; 2D
+// src/solvers/2d/ins_solver_base.cpp:894-955): velTT = the per-element CG
+// projection of velT - dt * grad p with the penalty factor the reference uses
+// (dt in 3D, dt * 1e3 in 2D). The reference's velocity and gradient components
+// are separate op_dats; they are passed here as dim Dats each. project()
+// returns the number of converged cells (the reference's num_converge; the
+// 2D solver aborts when it is not num_cells, src/solvers/2d/ins_solver_base.cpp:946-949)
+// and, if asked, the mean iteration count (num_iter / num_cells).
+class VelocityProjection {
+ public:
+  VelocityProjection(DGMesh* mesh, int order) : mesh_(mesh), order_(order) {}
+  int project(double dt, const Dat* dpd, const Dat* velT, Dat* velTT, double* mean_iters = nullptr) {
+    const int dim = mesh_->dim();
+    const size_t n = velT[0].size();
+    in_dp_.resize(dim * n);
+    in_v_.resize(dim * n);
+    out_.resize(dim * n);
+    for (int c = 0; c < dim; ++c) {
+      std::copy(dpd[c].data, dpd[c].data + n, in_dp_.begin() + c * n);
+      std::copy(velT[c].data, velT[c].data + n, in_v_.begin() + c * n);
+    }
+    double st[3] = {0, 0, 0};
+    const double factor = dim == 3 ? dt : dt * 1e3;
+    check(sipg_project_velocity_host(mesh_->handle(), order_, dt, factor, in_dp_.data(), in_v_.data(),
+                                     out_.data(), st),
+          "project_velocity");
+    for (int c = 0; c < dim; ++c) std::copy(out_.begin() + c * n, out_.begin() + (c + 1) * n, velTT[c].data);
+    if (mean_iters) *mean_iters = st[0] > 0 ? st[2] / st[0] : 0.0;
+    return (int)st[1];
+  }
+
+ private:
+  DGMesh* mesh_;
+  int order_;
+  std::vector<double> in_dp_, in_v_, out_;
 };
 
 }  // namespace ins_solver_b200

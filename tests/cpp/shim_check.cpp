@@ -126,6 +126,30 @@ int main() {
     std::printf("initial_guess_extrapolation err=%.3e\n", err);
     failures += !(err < 1e-12);
   }
+  {  // velocity projection: a field constant per element with zero pressure
+     // gradient is divergence-free and returned unchanged; a random one converges
+    VelocityProjection proj(&mesh, order);
+    std::vector<double> u[3], g[3], o[3];
+    for (int c = 0; c < 3; ++c) {
+      u[c].resize(N); g[c].assign(N, 0.0); o[c].assign(N, 0.0);
+      for (int e = 0; e < k; ++e) {
+        const double v = U(rng);
+        for (int i = 0; i < Np; ++i) u[c][(size_t)e * Np + i] = v;
+      }
+    }
+    auto D = [&](std::vector<double>& v) { return Dat{v.data(), k, Np}; };
+    Dat gd[3] = {D(g[0]), D(g[1]), D(g[2])}, ud[3] = {D(u[0]), D(u[1]), D(u[2])}, od[3] = {D(o[0]), D(o[1]), D(o[2])};
+    double it = -1;
+    int conv = proj.project(1e-3, gd, ud, od, &it);
+    double err = 0;
+    for (int c = 0; c < 3; ++c) err = std::max(err, rel_diff(o[c], u[c], false));
+    for (int c = 0; c < 3; ++c)
+      for (auto& v : g[c]) v = U(rng);
+    int conv2 = proj.project(1e-2, gd, ud, od, nullptr);
+    std::printf("velocity projection converged=%d/%d iters=%.2f err=%.3e; random gradient converged=%d\n", conv, k,
+                it, err, conv2);
+    failures += !(conv == k && it == 0.0 && err < 1e-13 && conv2 == k);
+  }
   std::printf("%s\n", failures ? "FAILED" : "OK");
   return failures ? 1 : 0;
 }
