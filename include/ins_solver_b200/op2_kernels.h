@@ -14,7 +14,7 @@
 // kernels the two builds share take DIM as well), and DG_FP is double.
 // The reference-element tables that the reference's kernels read by name
 // (dg_Dr_kernel, dg_Ds_kernel, dg_Dt_kernel, dg_Mass_kernel, dg_MM_F0..3_kernel,
-// FMASK) come from ref_tables<DIM, ORDER>(), which the program defines for every
+// dg_InvMass_kernel, FMASK) come from ref_tables<DIM, ORDER>(), which the program defines for every
 // (DIM, ORDER) it uses, as the reference's build generates those constants.
 //
 // SIPG_OP2_REF_QUIRKS (default 1) keeps the reference's statements where they
@@ -62,6 +62,7 @@ struct RefTables {
   const double *Dr, *Ds, *Dt, *Mass;
   const double *MM_F[4];
   const int *fmask;
+  const double *InvMass;  // inverse of Mass (dg_InvMass_kernel), read by the projection solve
 };
 
 template <int DIM, int ORDER>
@@ -1128,6 +1129,207 @@ SIPG_OP2_HD void vmf_2d_apply_bc(const int *faceNum, const int *u_bc_type, const
   const double *g[2] = {u_bc, v_bc};
   double *rhs[2] = {u_rhs, v_rhs};
   detail::lift_bc<2, ORDER>(faceNum, bc, n, fscale, sJ, geof, nullptr, g, rhs);
+}
+
+// ---- velocity projection, div_div = 1: INSSolverBase3D::project_velocity
+// (src/solvers/3d/ins_solver_base.cpp:1052-1124, set-up :201-214) and
+// INSSolverBase2D::project_velocity (src/solvers/2d/ins_solver_base.cpp:894-955).
+// The fused performance path is sipg_project_velocity.
+
+// face loop of the set-up: each side of an interior face writes its fscale into
+// its cell's per-face slots (ins_proj_setup_0.h)
+template <int DIM, int ORDER>
+SIPG_OP2_HD void ins_proj_setup_0(const int *faceNum, const double *fscale, double **f0) {
+  for (int side = 0; side < 2; ++side) f0[side][faceNum[side]] += fscale[side];
+}
+
+// h = 1 / the largest per-face fscale of the cell (ins_proj_setup_1.h)
+template <int DIM, int ORDER>
+SIPG_OP2_HD void ins_proj_setup_1(const double *fscale, double *h) {
+  double m = 0.0;
+  for (int f = 0; f < Dg<DIM, ORDER>::NUM_FACES; ++f) m = std::fmax(m, fscale[f]);
+  *h = 1.0 / m;
+}
+
+// velTT = velT - dt grad p, copied to the projection right-hand side (ins_3d_proj_rhs.h)
+template <int ORDER>
+SIPG_OP2_HD void ins_3d_proj_rhs(const double *dt, const double *dpdx, const double *dpdy, const double *dpdz,
+                                 const double *uT, const double *vT, const double *wT, double *uTT, double *vTT,
+                                 double *wTT, double *proj0, double *proj1, double *proj2) {
+  for (int i = 0; i < Dg<3, ORDER>::NP; ++i) {
+    proj0[i] = uTT[i] = uT[i] - *dt * dpdx[i];
+    proj1[i] = vTT[i] = vT[i] - *dt * dpdy[i];
+    proj2[i] = wTT[i] = wT[i] - *dt * dpdz[i];
+  }
+}
+
+template <int ORDER>
+SIPG_OP2_HD void ins_2d_proj_rhs(const double *dt, const double *dpdx, const double *dpdy, const double *uT,
+                                 const double *vT, double *uTT, double *vTT, double *proj0, double *proj1) {
+  for (int i = 0; i < Dg<2, ORDER>::NP; ++i) {
+    proj0[i] = uTT[i] = uT[i] - *dt * dpdx[i];
+    proj1[i] = vTT[i] = vT[i] - *dt * dpdy[i];
+  }
+}
+
+// penalty of the element solve: pen = factor h / (p + 1), pen_f = factor. The
+// reference also forms the mass-weighted velocity magnitude from (a0 u0 + a1 u1,
+// ...), which does not enter either output (ins_3d_proj_pen.h:24-25).
+template <int ORDER>
+SIPG_OP2_HD void ins_3d_proj_pen(const double *factor, const double *a0, const double *a1, const double *geof,
+                                 const double *u0, const double *v0, const double *w0, const double *u1,
+                                 const double *v1, const double *w1, const double *h, double *pen, double *pen_f) {
+  *pen = *factor * (*h / ((double)ORDER + 1.0));
+  *pen_f = *factor;
+}
+
+template <int ORDER>
+SIPG_OP2_HD void ins_2d_proj_pen(const double *factor, const double *a0, const double *a1, const double *geof,
+                                 const double *u0, const double *v0, const double *u1, const double *v1,
+                                 const double *h, double *pen, double *pen_f) {
+  *pen = *factor * (*h / ((double)ORDER + 1.0));
+  *pen_f = *factor;
+}
+
+namespace detail {
+
+// out_c = pen * (G^T D^T (J M (D G v)))_c + J (M v_c), with every product summed
+// over j in order and the sums combined as op2_in_kernel_gemv combines them.
+template <int DIM, int ORDER>
+SIPG_OP2_HD void proj_operator(const double *geof, double pen, double *const *v, double *const *out) {
+  using G = Dg<DIM, ORDER>;
+  constexpr int NP = G::NP;
+  const RefTables &t = ref_tables<DIM, ORDER>();
+  const double *Dk[3] = {t.Dr, t.Ds, t.Dt};
+  const int gi[3][3] = {{G::RX, G::RY, G::RZ}, {G::SX, G::SY, G::SZ}, {G::TX, G::TY, G::TZ}};
+  const double J = geof[G::J];
+  double gv[3][NP], div[NP], mdiv[NP];
+  for (int i = 0; i < NP; ++i)
+    for (int k = 0; k < DIM; ++k) {
+      double s = geof[gi[k][0]] * v[0][i] + geof[gi[k][1]] * v[1][i];
+      if (DIM == 3) s += geof[gi[k][2]] * v[2][i];
+      gv[k][i] = s;
+    }
+  for (int k = 0; k < DIM; ++k)
+    for (int i = 0; i < NP; ++i) {
+      double s = 0.0;
+      for (int j = 0; j < NP; ++j) s += Dk[k][i + j * NP] * gv[k][j];
+      div[i] = k == 0 ? s : div[i] + s;
+    }
+  for (int i = 0; i < NP; ++i) {
+    double s = 0.0;
+    for (int j = 0; j < NP; ++j) s += t.Mass[i + j * NP] * div[j];
+    mdiv[i] = J * s;
+  }
+  for (int k = 0; k < DIM; ++k)
+    for (int i = 0; i < NP; ++i) {
+      double s = 0.0;
+      for (int j = 0; j < NP; ++j) s += Dk[k][j + i * NP] * mdiv[j];
+      gv[k][i] = s;
+    }
+  for (int i = 0; i < NP; ++i)
+    for (int c = 0; c < DIM; ++c) {
+      double s = geof[gi[0][c]] * gv[0][i] + geof[gi[1][c]] * gv[1][i];
+      if (DIM == 3) s += geof[gi[2][c]] * gv[2][i];
+      out[c][i] = s;
+    }
+  for (int c = 0; c < DIM; ++c)
+    for (int i = 0; i < NP; ++i) {
+      double s = 0.0;
+      for (int j = 0; j < NP; ++j) s += t.Mass[i + j * NP] * v[c][j];
+      out[c][i] = pen * out[c][i] + J * s;
+    }
+}
+
+// sum over the nodes of a[0] b[0] + a[1] b[1] (+ a[2] b[2])
+template <int DIM, int NP>
+SIPG_OP2_HD double proj_dot(double *const *a, double *const *b) {
+  double s = 0.0;
+  for (int i = 0; i < NP; ++i) {
+    double t = a[0][i] * b[0][i] + a[1][i] * b[1][i];
+    if (DIM == 3) t += a[2][i] * b[2][i];
+    s += t;
+  }
+  return s;
+}
+
+// Element-local CG of the projection: 3D preconditioned by (1/J) M^-1 and
+// stopped at |r|_2 < 1e-8 (ins_3d_proj_cg_precon.h), 2D unpreconditioned and
+// stopped at |r|_2^2 < 1e-16 (ins_proj_cg_2d.h); at most 100 iterations. The
+// iteration that meets the tolerance is not counted, as in the reference.
+template <int DIM, int ORDER>
+SIPG_OP2_HD void proj_cg(const double *geof, const double *pen, const double *const *rhs, double *const *x,
+                         int *cell_g, int *conv_g, double *iter_g) {
+  using G = Dg<DIM, ORDER>;
+  constexpr int NP = G::NP;
+  constexpr bool pre = DIM == 3;
+  const double tol = pre ? 1e-8 : 1e-16;
+  const double inv_J = 1.0 / geof[G::J];
+  const double *Mi = ref_tables<DIM, ORDER>().InvMass;
+  double rb[3][NP], zb[3][NP], pb[3][NP], ab[3][NP];
+  double *r[3] = {rb[0], rb[1], rb[2]}, *z[3] = {zb[0], zb[1], zb[2]};
+  double *p[3] = {pb[0], pb[1], pb[2]}, *ap[3] = {ab[0], ab[1], ab[2]};
+  auto precondition = [&]() {
+    for (int c = 0; c < DIM; ++c)
+      for (int i = 0; i < NP; ++i) {
+        if (pre) {
+          double s = 0.0;
+          for (int j = 0; j < NP; ++j) s += Mi[i + j * NP] * r[c][j];
+          z[c][i] = inv_J * s;
+        } else {
+          z[c][i] = r[c][i];
+        }
+      }
+  };
+  proj_operator<DIM, ORDER>(geof, *pen, x, ap);
+  for (int c = 0; c < DIM; ++c)
+    for (int i = 0; i < NP; ++i) r[c][i] = rhs[c][i] - ap[c][i];
+  double res = proj_dot<DIM, NP>(r, r);
+  if (pre) res = std::sqrt(res);
+  precondition();
+  for (int c = 0; c < DIM; ++c)
+    for (int i = 0; i < NP; ++i) p[c][i] = z[c][i];
+  double it = 0.0;
+  while (res > tol && it < 100.0) {
+    proj_operator<DIM, ORDER>(geof, *pen, p, ap);
+    const double alpha = proj_dot<DIM, NP>(r, z) / proj_dot<DIM, NP>(p, ap);
+    // r_old . z_old (3D) or r_old . r_old (2D) for beta, taken before r moves
+    const double rz_old = pre ? proj_dot<DIM, NP>(r, z) : proj_dot<DIM, NP>(r, r);
+    for (int c = 0; c < DIM; ++c)
+      for (int i = 0; i < NP; ++i) x[c][i] = x[c][i] + alpha * p[c][i];
+    for (int c = 0; c < DIM; ++c)
+      for (int i = 0; i < NP; ++i) r[c][i] = r[c][i] - alpha * ap[c][i];
+    res = proj_dot<DIM, NP>(r, r);
+    if (pre) res = std::sqrt(res);
+    if (res < tol) break;
+    precondition();
+    const double beta = (pre ? proj_dot<DIM, NP>(r, z) : proj_dot<DIM, NP>(r, r)) / rz_old;
+    for (int c = 0; c < DIM; ++c)
+      for (int i = 0; i < NP; ++i) p[c][i] = z[c][i] + beta * p[c][i];
+    it += 1.0;
+  }
+  *cell_g += 1;
+  *iter_g += it;
+  if (it < 100.0 && !std::isnan(res)) *conv_g += 1;
+}
+
+}  // namespace detail
+
+template <int ORDER>
+SIPG_OP2_HD void ins_3d_proj_cg_precon(const double *geof, const double *pen, const double *rhs0,
+                                       const double *rhs1, const double *rhs2, double *u, double *v, double *w,
+                                       int *cell_g, int *conv_g, double *iter_g) {
+  const double *rhs[3] = {rhs0, rhs1, rhs2};
+  double *x[3] = {u, v, w};
+  detail::proj_cg<3, ORDER>(geof, pen, rhs, x, cell_g, conv_g, iter_g);
+}
+
+template <int ORDER>
+SIPG_OP2_HD void ins_proj_cg_2d(const double *geof, const double *pen, const double *rhs0, const double *rhs1,
+                                double *u, double *v, int *cell_g, int *conv_g, double *iter_g) {
+  const double *rhs[3] = {rhs0, rhs1, rhs1};
+  double *x[3] = {u, v, v};
+  detail::proj_cg<2, ORDER>(geof, pen, rhs, x, cell_g, conv_g, iter_g);
 }
 
 }  // namespace op2

@@ -21,17 +21,20 @@ LIB_SRC = os.path.join(ROOT, "tests", "cpp", "op2_kernels_lib.cpp")
 REF_GEN = os.path.join(ROOT, "oracle", "_ref", "gen")
 
 # kernels on a pair of cells sharing a face (faceNum = {face in L, face in R})
-PAIR = {"fvmf_3d_calc_tau_faces", "fvmf_2d_calc_tau_faces", "vmf_calc_tau_faces", "fvmf_3d_op2_diag",
+PAIR = {"ins_proj_setup_0", "fvmf_3d_calc_tau_faces", "fvmf_2d_calc_tau_faces", "vmf_calc_tau_faces", "fvmf_3d_op2_diag",
         "fvmf_2d_op2_diag", "fvmf_3d_op2_block_diag", "fvmf_2d_op2_block_diag"}
 # kernels on one boundary face of a cell
 BFACE = {"fvmf_3d_calc_tau_bfaces", "fvmf_2d_calc_tau_bfaces", "vmf_calc_tau_bfaces", "vmf_3d_mult_avg_jump",
          "vmf_2d_mult_avg_jump", "fvmf_3d_apply_bc", "fvmf_2d_apply_bc", "vmf_3d_apply_bc", "vmf_2d_apply_bc",
          "fvmf_3d_bop_diag", "fvmf_2d_bop_diag", "fvmf_3d_bop_block_diag", "fvmf_2d_bop_block_diag"}
-SCALARS = {"alpha", "beta", "residual", "tmp_alpha_0", "tmp_alpha_1", "constant", "mmConst"}
+SCALARS = {"alpha", "beta", "residual", "tmp_alpha_0", "tmp_alpha_1", "constant", "mmConst", "dt", "a0", "a1", "h",
+           "pen", "pen_f", "iter_g"}
+# kernels whose `factor` is a scalar
+SCALAR_FACTOR = {"ins_3d_proj_pen", "ins_2d_proj_pen"}
 MATS = {"u_pre_mat", "v_pre_mat", "w_pre_mat", "op1", "op1L", "op1R"}
 # kernels every (shared) build has; the others belong to the dimension in their name
 SHARED = {"constant_mult", "copy_dg_np", "copy_dg_np_mat", "reciprocal", "zero_npf_3", "poisson_pr_fact",
-          "poisson_vis_fact", "vmf_calc_tau_faces", "vmf_calc_tau_bfaces"}
+          "poisson_vis_fact", "vmf_calc_tau_faces", "vmf_calc_tau_bfaces", "ins_proj_setup_0", "ins_proj_setup_1"}
 
 
 def split_args(s):
@@ -74,7 +77,7 @@ def ref_signature(dim, order, name):
 def kernel_dim(name):
     if name in SHARED:
         return None
-    return 3 if name.startswith(("fvmf_3d", "vmf_3d", "cg3_")) else 2
+    return 3 if name.startswith(("fvmf_3d", "vmf_3d", "cg3_", "ins_3d_")) else 2
 
 
 def ref_names(dim):
@@ -134,13 +137,15 @@ def make_args(name, args, t, rng, bc_mode=None):
     for typ, an in args:
         const = typ.startswith("const")
         if typ.endswith("**"):
-            n = {"factor": Np, "tau": Nf, "geof": ng}[an]
+            n = {"factor": Np, "tau": Nf, "geof": ng, "f0": Nf * Nfp}[an]
             vals.append(("pp", [rng.uniform(0.5, 1.5, n) for _ in range(2)], const))
         elif "int" in typ:
             if an == "faceNum":
                 v = [fL, fR] if name in PAIR else [fL]
             elif an.endswith("bc_type"):
                 v = [int(rng.integers(3)) if bc_mode is None else bc_mode]
+            elif an in ("cell_g", "conv_g"):
+                v = [int(rng.integers(5))]
             elif an in ("fmaskR_corrected", "fmaskL_corrected"):
                 v = list(t["fmask"][fR if an == "fmaskR_corrected" else fL])
                 if rng.integers(2):
@@ -151,7 +156,8 @@ def make_args(name, args, t, rng, bc_mode=None):
         elif "bool" in typ:
             vals.append(("b", np.array([bool(rng.integers(2))]), const))
         else:
-            if an in SCALARS or (an == "mm_factor" and name.startswith("vmf_")):
+            if an in SCALARS or (an == "mm_factor" and name.startswith("vmf_")) or \
+                    (an == "factor" and name in SCALAR_FACTOR):
                 n = 1
             elif an == "geof":
                 n = ng
@@ -196,7 +202,7 @@ def test_every_provided_kernel_has_the_reference_argument_list(libs):
                 continue
             assert ours[name][1] == ref_signature(dim, 3, name), name
             checked += 1
-    assert checked == 80  # 40 kernels of each build, the shared ones counted in both
+    assert checked == 90  # 45 kernels of each build, the shared ones counted in both
 
 
 @pytest.mark.parametrize("dim,order", [(2, 1), (2, 2), (2, 3), (2, 4), (3, 1), (3, 2), (3, 3), (3, 4)])
@@ -205,7 +211,7 @@ def test_kernels_match_the_reference_kernels(libs, dim, order):
     t, om = table_mesh(dim, order)
     rng = np.random.default_rng(100 * dim + order)
     names = [n for n in ref_names(dim) if n in ours]
-    assert len(names) == 40
+    assert len(names) == 45
     for name in names:
         for trial in range(6):
             # Dirichlet, Neumann and slip on every component, then random mixes
@@ -283,13 +289,15 @@ template <> __host__ __device__ const RefTables& ref_tables<3, 3>() {{
 }}
 }} }}
 __global__ void cells(const double* geof, const double* f, double* op1, double* diag, double* r, const double* Ap,
-                      double* res) {{
+                      double* res, int* counts, double* iters) {{
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   op2::fvmf_3d_op1<3>(geof + 10 * e, f + 20 * e, op1 + 400 * e);
   op2::fvmf_3d_op1_diag<3>(geof + 10 * e, f + 20 * e, diag + 20 * e);
   const double alpha = 0.5;
   op2::cg3_update_res<3>(&alpha, res + e, Ap + 60 * e, Ap + 60 * e + 20, Ap + 60 * e + 40, r + 60 * e,
                          r + 60 * e + 20, r + 60 * e + 40);
+  op2::ins_3d_proj_cg_precon<3>(geof + 10 * e, res + e, Ap + 60 * e, Ap + 60 * e + 20, Ap + 60 * e + 40,
+                                r + 60 * e, r + 60 * e + 20, r + 60 * e + 40, counts, counts + 1, iters);
 }}
 """)
     out = tmp_path / "op2_device.o"
