@@ -421,6 +421,27 @@ def run_projection(steps=20, cpu=True):
                                                   C.c_void_p(h_dp.data_ptr()), C.c_void_p(h_v.data_ptr()),
                                                   C.c_void_p(h_out.data_ptr()), st.ctypes.data_as(C.c_void_p)))
         e2e.append(time.perf_counter() - t0)
+    # the pressure step fused: central-flux grad p / rho, then the projection, from
+    # the pressure (K x Np) and a two-phase density instead of a stored gradient
+    pr = torch.from_numpy(np.random.default_rng(6).uniform(-1, 1, (K, Np))).cuda()
+    rho = torch.from_numpy(np.random.default_rng(7).uniform(1.0, 1000.0, (K, Np))).cuda()
+
+    def call_p():
+        sipg.check(lib.sipg_pressure_projection(mesh.h, PROJ_ORDER, C.c_double(PROJ_DT), C.c_double(PROJ_DT),
+                                                C.c_void_p(pr.data_ptr()), C.c_void_p(rho.data_ptr()),
+                                                C.c_void_p(d_v.data_ptr()), C.c_void_p(d_out.data_ptr()),
+                                                C.c_void_p(0), C.c_void_p(stream.cuda_stream)))
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            call_p()
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for _ in range(steps):
+            call_p()
+        p1.record(stream)
+    torch.cuda.synchronize()
+    ms_p = p0.elapsed_time(p1) / steps
     npp = Np * Np
     # FP64 flops: per element one operator application and one preconditioner
     # application to start, then per CG iteration one of each (20 Np^2 and 6 Np^2
@@ -435,6 +456,9 @@ def run_projection(steps=20, cpu=True):
            "kernel": "k_proj_cg<3,3> (one launch per projection)",
            "ms": ms, "gdofs": dofs / (ms * 1e-3) / 1e9, "converged": conv, "cells": K,
            "mean_iters": iters / K,
+           "pressure_step": {"ms": ms_p, "gdofs": dofs / (ms_p * 1e-3) / 1e9,
+                             "what": "sipg_pressure_projection: central-flux grad p / rho (rho U(1,1000)) and the "
+                                     "projection in one kernel, from pr (K x Np) instead of a stored gradient"},
            "e2e": {"ms": float(np.mean(e2e)) * 1e3, "gdofs": dofs / float(np.mean(e2e)) / 1e9,
                    "h2d_bytes": int(dp.nbytes + velT.nbytes), "d2h_bytes": int(velT.nbytes)},
            "roofline": {"bound": "fp64", "achieved": flops / (ms * 1e-3) / 1e12, "peak": pk,

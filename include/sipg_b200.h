@@ -311,6 +311,23 @@ int sipg_project_velocity(sipg_mesh *m, int order, double dt, double factor, con
 int sipg_project_velocity_host(sipg_mesh *m, int order, double dt, double factor, const double *dp,
                                const double *velT, double *velTT, double *stats);
 
+/* ---- pressure projection step: replaces, in MPINSSolver3D::pressure
+ * (src/solvers/3d/mp_ins_solver.cpp:650-661; INSSolver3D::pressure
+ * ins_solver.cpp:358-363), the sequence mesh->grad_with_central_flux(pr, dpdx,
+ * dpdy, dpdz) (OP2-DG-Toolkit, unvendored), update_pressure_gradient (grad p /
+ * rho, mp_ins_3d_pr_2.h, mp_ins_solver.cpp:546-552) and project_velocity, as
+ * one kernel: grad p = G^T (Dr, Ds, Dt) pr + LIFT (fscale n (pr+ - pr-) / 2) over
+ * interior faces (central flux; boundary faces add nothing), divided by rho
+ * when rho is not NULL (the two-phase solver; NULL for INSSolver3D), then the
+ * element-local projection of sipg_project_velocity. pr and rho: K x Np; velT,
+ * velTT: dim x K x Np; stats as there. Device pointers, or host pointers in the
+ * synchronous _host variant. */
+int sipg_pressure_projection(sipg_mesh *m, int order, double dt, double factor, const double *pr,
+                             const double *rho, const double *velT, double *velTT, unsigned long long *stats,
+                             void *stream);
+int sipg_pressure_projection_host(sipg_mesh *m, int order, double dt, double factor, const double *pr,
+                                  const double *rho, const double *velT, double *velTT, double *stats);
+
 /* Number of kernels this library has launched so far in the process
  * (diagnostics for benchmarks; no reference counterpart). */
 int sipg_launch_count(unsigned long long *n);

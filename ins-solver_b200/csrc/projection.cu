@@ -59,11 +59,42 @@ __host__ __device__ constexpr int proj_epw(int D, int P) { return proj_np(D, P) 
 __host__ __device__ constexpr int proj_nmat(int D) { return 2 * D + 1 + (D == 3 ? 1 : 0); }
 template <int D, int P>
 __host__ __device__ constexpr int proj_mat_doubles() { return proj_np(D, P) * proj_npe(D, P); }
+__host__ __device__ constexpr int proj_nfp(int D, int P) { return D == 2 ? P + 1 : (P + 1) * (P + 2) / 2; }
+__host__ __device__ constexpr int proj_nfpe(int D, int P) { return (proj_nfp(D, P) + 1) & ~1; }
+// LIFT = M^-1 EMAT after the matrices, per face f: LIFT(i, f Nfp + k) in the pair
+// layout of an Np x Nfpe block (the fused-gradient variant reads it)
+template <int D, int P>
+__host__ __device__ constexpr int proj_lift_doubles() { return (D + 1) * proj_np(D, P) * proj_nfpe(D, P); }
+template <int D, int P>
+__host__ __device__ constexpr int proj_blob_doubles() {
+  return proj_nmat(D) * proj_mat_doubles<D, P>() + proj_lift_doubles<D, P>();
+}
+template <int D, int P>
+__host__ __device__ constexpr int proj_warp_doubles() {
+  // per element: A (D x Npe), B (D x Npe), C (Npe), face jumps ((D + 1) x Nfpe)
+  return proj_epw(D, P) * ((2 * D + 1) * proj_npe(D, P) + (D + 1) * proj_nfpe(D, P));
+}
 template <int D, int P>
 __host__ __device__ constexpr int proj_smem_doubles() {
-  // matrices + per warp and element: A (D x Npe), B (D x Npe), C (Npe)
-  return proj_nmat(D) * proj_mat_doubles<D, P>() + kProjWarps * proj_epw(D, P) * (2 * D + 1) * proj_npe(D, P);
+  return proj_blob_doubles<D, P>() + kProjWarps * proj_warp_doubles<D, P>();
 }
+
+struct ProjArgs {
+  int K;
+  const double* geof;      // K x ngeof
+  const double* hK;        // K: penalty length
+  const double* mats;      // proj_blob_doubles
+  double dt, factor;
+  const double* dp;        // grad p, dim x K x Np (plain variant)
+  const double* pr;        // pressure, K x Np (fused-gradient variant)
+  const double* rho;       // density K x Np or null (fused-gradient variant: grad p / rho)
+  const int* nbr;          // K x (dim + 1): neighbour or -(bface + 1)
+  const uint32_t* fcode;   // K: byte f = neighbour face | orientation << 2
+  const int8_t* itab;      // fmask ((dim + 1) x Nfp) then neighbour node positions (Nperm x Nfp)
+  const double* velT;
+  double* velTT;
+  unsigned long long* stats;
+};
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -94,27 +125,34 @@ __device__ __forceinline__ void mat_vec(const double* __restrict__ A, const doub
   for (int e = 0; e < E; ++e) y[e] += y1[e];
 }
 
-// E elements per warp (a lane per node, NPL nodes per lane).
-template <int D, int P>
-__global__ void __launch_bounds__(kProjWarps * 32)
-k_proj_cg(int K, const double* __restrict__ geof, const double* __restrict__ hK,
-          const double* __restrict__ mats, double dt, double factor, const double* __restrict__ dp,
-          const double* __restrict__ velT, double* __restrict__ velTT,
-          unsigned long long* __restrict__ stats) {
+// E elements per warp (a lane per node, NPL nodes per lane). GRAD: the pressure
+// gradient is computed here from the pressure (central flux, then / rho) instead
+// of being read.
+template <int D, int P, bool GRAD>
+__global__ void __launch_bounds__(kProjWarps * 32) k_proj_cg(const ProjArgs a) {
   constexpr int NP = proj_np(D, P), NPE = proj_npe(D, P), NPL = (NP + 31) / 32, NG = D == 3 ? 10 : 5;
+  constexpr int NF = D + 1, NFP = proj_nfp(D, P), NFPE = proj_nfpe(D, P);
   constexpr int E = proj_epw(D, P), MAT = proj_mat_doubles<D, P>();
-  constexpr int WB = E * (2 * D + 1) * NPE;  // per-warp buffer
+  constexpr int WB = proj_warp_doubles<D, P>();  // per-warp buffer
   constexpr bool kPre = D == 3;
+  const int K = a.K;
+  const double* __restrict__ geof = a.geof;
+  const double* __restrict__ hK = a.hK;
+  const double dt = a.dt, factor = a.factor;
+  const double* __restrict__ velT = a.velT;
+  double* __restrict__ velTT = a.velTT;
   extern __shared__ double sm[];
   const double* sD = sm;                  // D_k, k < D
   const double* sDt = sm + D * MAT;       // D_k^T
   const double* sM = sm + 2 * D * MAT;    // M
   const double* sMi = sm + (2 * D + 1) * MAT;  // M^-1 (3D)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double* sA = sm + proj_nmat(D) * MAT + warp * WB;  // [E][D][NPE]
-  double* sB = sA + E * D * NPE;                      // [E][D][NPE]
-  double* sC = sB + E * D * NPE;                      // [E][NPE]
-  for (int i = threadIdx.x; i < proj_nmat(D) * MAT; i += blockDim.x) sm[i] = mats[i];
+  const double* sL = sm + proj_nmat(D) * MAT;  // LIFT, per face an Np x Nfpe pair block
+  double* sA = sm + proj_blob_doubles<D, P>() + warp * WB;  // [E][D][NPE]
+  double* sB = sA + E * D * NPE;                             // [E][D][NPE]
+  double* sC = sB + E * D * NPE;                             // [E][NPE]
+  double* sJ = sC + E * NPE;                                 // [E][NF][NFPE] face jumps
+  for (int i = threadIdx.x; i < proj_blob_doubles<D, P>(); i += blockDim.x) sm[i] = a.mats[i];
   // zero the warp buffers once: their pad entries (Np..Npe-1) stay zero
   for (int i = lane; i < WB; i += 32) sA[i] = 0.0;
   __syncthreads();
@@ -276,6 +314,87 @@ k_proj_cg(int K, const double* __restrict__ geof, const double* __restrict__ hK,
       for (int e = 0; e < E; ++e) rz[e] = warp_sum(rz[e]);
     };
 
+    // grad p: read, or (GRAD) computed with the central flux and divided by rho
+    double gp[E][D][NPL];
+    if (GRAD) {
+      const int8_t* fmask = a.itab;
+      const int8_t* npos = a.itab + NF * NFP;
+#pragma unroll
+      for (int e = 0; e < E; ++e)
+#pragma unroll
+        for (int u = 0; u < NPL; ++u) {
+          const int i = lane + 32 * u;
+          if (i < NP) sB[e * D * NPE + i] = valid[e] ? __ldg(a.pr + (size_t)(e0 + e) * NP + i) : 0.0;
+        }
+      __syncwarp();
+      // (p+ - p-) / 2 at every face node; boundary faces add nothing
+#pragma unroll
+      for (int e = 0; e < E; ++e)
+        for (int m = lane; m < NF * NFP; m += 32) {
+          const int f = m / NFP, k = m - f * NFP;
+          double jv = 0.0;
+          if (valid[e]) {
+            const int el = e0 + e;
+            const int nb = __ldg(a.nbr + (size_t)el * NF + f);
+            if (nb >= 0) {
+              const int code = (__ldg(a.fcode + el) >> (8 * f)) & 0xff;
+              const int fr = code & 3, sg = code >> 2;
+              const int nn = fmask[fr * NFP + npos[sg * NFP + k]];
+              jv = 0.5 * (__ldg(a.pr + (size_t)nb * NP + nn) - sB[e * D * NPE + fmask[f * NFP + k]]);
+            }
+          }
+          sJ[(e * NF + f) * NFPE + k] = jv;
+        }
+      __syncwarp();
+#pragma unroll
+      for (int u = 0; u < NPL; ++u) {
+        const int i = lane + 32 * u;
+        if (i < NP) {
+          double dr[D][E], lf[NF][E];
+#pragma unroll
+          for (int k = 0; k < D; ++k) mat_vec<NP, NPE, E>(sD + k * MAT, sB, D * NPE, i, dr[k]);
+#pragma unroll
+          for (int f = 0; f < NF; ++f) mat_vec<NP, NFPE, E>(sL + f * NP * NFPE, sJ + f * NFPE, NF * NFPE, i, lf[f]);
+#pragma unroll
+          for (int e = 0; e < E; ++e) {
+            const double rinv = (valid[e] && a.rho) ? 1.0 / __ldg(a.rho + (size_t)(e0 + e) * NP + i) : 1.0;
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+              double g = 0.0;
+#pragma unroll
+              for (int k = 0; k < D; ++k) g += G[e][k][d] * dr[k][e];
+              // fscale n of each face (the unnormalised outward normal)
+              if (D == 3) {
+                g += -G[e][2][d] * lf[0][e];
+                g += -G[e][1][d] * lf[1][e];
+                g += ((G[e][0][d] + G[e][1][d]) + G[e][2][d]) * lf[2][e];
+                g += -G[e][0][d] * lf[3][e];
+              } else {
+                g += -G[e][1][d] * lf[0][e];
+                g += (G[e][0][d] + G[e][1][d]) * lf[1][e];
+                g += -G[e][0][d] * lf[2][e];
+              }
+              gp[e][d][u] = g * rinv;
+            }
+          }
+        } else {
+#pragma unroll
+          for (int e = 0; e < E; ++e)
+#pragma unroll
+            for (int d = 0; d < D; ++d) gp[e][d][u] = 0.0;
+        }
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < E; ++e)
+#pragma unroll
+        for (int u = 0; u < NPL; ++u) {
+          const int i = lane + 32 * u;
+#pragma unroll
+          for (int c = 0; c < D; ++c)
+            gp[e][c][u] = (valid[e] && i < NP) ? __ldg(a.dp + c * n + (size_t)(e0 + e) * NP + i) : 0.0;
+        }
+    }
     // velTT = velT - dt grad p: the initial guess and, through J M, the right-hand side
 #pragma unroll
     for (int e = 0; e < E; ++e)
@@ -285,7 +404,7 @@ k_proj_cg(int K, const double* __restrict__ geof, const double* __restrict__ hK,
 #pragma unroll
         for (int c = 0; c < D; ++c) {
           const size_t g = c * n + (size_t)(e0 + e) * NP + i;
-          x[e][c][u] = (valid[e] && i < NP) ? __ldg(velT + g) - dt * __ldg(dp + g) : 0.0;
+          x[e][c][u] = (valid[e] && i < NP) ? __ldg(velT + g) - dt * gp[e][c][u] : 0.0;
         }
       }
     stage(x);
@@ -390,9 +509,9 @@ k_proj_cg(int K, const double* __restrict__ geof, const double* __restrict__ hK,
       n_conv += (it[e] < kProjMaxIter && !isnan(res[e])) ? 1ull : 0ull;
     }
   }
-  if (stats && lane == 0) {
-    atomicAdd(stats + 0, n_conv);
-    atomicAdd(stats + 1, n_iter);
+  if (a.stats && lane == 0) {
+    atomicAdd(a.stats + 0, n_conv);
+    atomicAdd(a.stats + 1, n_iter);
   }
 }
 
@@ -414,7 +533,8 @@ const ProjMats& proj_mats(int dim, int order) {
   const RefElement& ref = dr.ref;
   const int Np = ref.Np, Npe = (Np + 1) & ~1;
   const size_t MAT = (size_t)Np * Npe;
-  std::vector<double> b((size_t)proj_nmat(dim) * MAT, 0.0);  // pad columns stay zero
+  const int Nfpe0 = (ref.Nfp + 1) & ~1;
+  std::vector<double> b((size_t)proj_nmat(dim) * MAT + (size_t)(dim + 1) * Np * Nfpe0, 0.0);  // pads stay zero
   // A(i, j) of matrix m at m * MAT + ((j / 2) * Np + i) * 2 + j % 2; rm: row-major source
   auto put = [&](int m, const std::vector<double>& rm, bool transpose) {
     for (int i = 0; i < Np; ++i)
@@ -428,6 +548,12 @@ const ProjMats& proj_mats(int dim, int order) {
   }
   put(2 * dim, ref.M, false);
   if (dim == 3) put(2 * dim + 1, ref.Minv, false);
+  const int Nf = dim + 1, Nfp = ref.Nfp, Nfpe = (Nfp + 1) & ~1;
+  double* lift = b.data() + (size_t)proj_nmat(dim) * MAT;
+  for (int f = 0; f < Nf; ++f)
+    for (int i = 0; i < Np; ++i)
+      for (int k = 0; k < Nfp; ++k)
+        lift[(size_t)f * Np * Nfpe + ((size_t)(k / 2) * Np + i) * 2 + k % 2] = ref.LIFT[(size_t)i * Nf * Nfp + f * Nfp + k];
   auto pm = std::make_unique<ProjMats>();
   pm->Np = Np;
   pm->blob = DevBuf(b.size() * sizeof(double));
@@ -460,44 +586,103 @@ const double* proj_h_device(sipg_mesh* m) {
   return m->proj_h.as<double>();
 }
 
-template <int D, int P>
-void launch_proj(sipg_mesh* m, const double* mats, const double* hK, double dt, double factor, const double* dp,
-                 const double* velT, double* velTT, unsigned long long* stats, cudaStream_t s) {
+template <int D, int P, bool GRAD>
+void launch_proj(const ProjArgs& a, cudaStream_t s) {
   constexpr size_t smem = proj_smem_doubles<D, P>() * sizeof(double);
   static_assert(smem <= 227 * 1024, "projection shared memory");
-  auto kern = k_proj_cg<D, P>;
-  SIPG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int per_sm = 0;
-  SIPG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kProjWarps * 32, smem));
-  per_sm = std::max(per_sm, 1);
-  const int need = (m->K + kProjWarps - 1) / kProjWarps;
+  auto kern = k_proj_cg<D, P, GRAD>;
+  static const int per_sm = [&] {  // once per instantiation
+    SIPG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int n = 0;
+    SIPG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, kProjWarps * 32, smem));
+    return std::max(n, 1);
+  }();
+  const int epc = kProjWarps * proj_epw(D, P);  // elements per CTA round
+  const int need = (a.K + epc - 1) / epc;
   const int grid = std::max(1, std::min(need, per_sm * num_sms()));
-  kern<<<grid, kProjWarps * 32, smem, s>>>(m->K, m->geof64.as<double>(), hK, mats, dt, factor, dp, velT, velTT,
-                                           stats);
+  kern<<<grid, kProjWarps * 32, smem, s>>>(a);
   SIPG_CUDA(cudaGetLastError());
   note_launch();
 }
 
-void project_device(sipg_mesh* m, int order, double dt, double factor, const double* dp, const double* velT,
-                    double* velTT, unsigned long long* stats, cudaStream_t s) {
-  if (!m || order < 1 || order > 4 || !dp || !velT || !velTT)
+// velTT from velT and either grad p (dp) or the pressure (pr, rho: GRAD).
+void project_device(sipg_mesh* m, int order, double dt, double factor, const double* dp, const double* pr,
+                    const double* rho, const double* velT, double* velTT, unsigned long long* stats,
+                    cudaStream_t s) {
+  const bool grad = pr != nullptr;
+  if (!m || order < 1 || order > 4 || (!dp && !pr) || !velT || !velTT)
     throw Error(SIPG_INVALID_ARG, "project_velocity: null mesh/array or order outside 1..4");
   if (!std::isfinite(dt) || !std::isfinite(factor)) throw Error(SIPG_INVALID_ARG, "project_velocity: dt/factor");
-  if (velTT == velT || velTT == dp) throw Error(SIPG_INVALID_ARG, "project_velocity: velTT must not alias its inputs");
-  const double* hK = proj_h_device(m);
-  const double* mats = proj_mats(m->dim, order).blob.as<double>();
+  if (velTT == velT || (dp && velTT == dp) || (pr && velTT == pr) || (rho && velTT == rho))
+    throw Error(SIPG_INVALID_ARG, "project_velocity: velTT must not alias its inputs");
+  ProjArgs a{};
+  a.K = m->K;
+  a.hK = proj_h_device(m);  // also uploads the mesh
+  a.geof = m->geof64.as<double>();
+  a.mats = proj_mats(m->dim, order).blob.as<double>();
+  a.dt = dt;
+  a.factor = factor;
+  a.dp = dp;
+  a.pr = pr;
+  a.rho = rho;
+  a.nbr = m->nbr.as<int>();
+  a.fcode = m->fcode.as<uint32_t>();
+  a.itab = dev_ref(m->dim, order).itab.as<int8_t>();
+  a.velT = velT;
+  a.velTT = velTT;
+  a.stats = stats;
   if (stats) SIPG_CUDA(cudaMemsetAsync(stats, 0, 2 * sizeof(unsigned long long), s));
   if (m->K == 0) return;
+#define SIPG_PROJ(D, P)                        \
+  (grad ? launch_proj<D, P, true>(a, s) : launch_proj<D, P, false>(a, s))
   switch (m->dim * 10 + order) {
-    case 21: launch_proj<2, 1>(m, mats, hK, dt, factor, dp, velT, velTT, stats, s); break;
-    case 22: launch_proj<2, 2>(m, mats, hK, dt, factor, dp, velT, velTT, stats, s); break;
-    case 23: launch_proj<2, 3>(m, mats, hK, dt, factor, dp, velT, velTT, stats, s); break;
-    case 24: launch_proj<2, 4>(m, mats, hK, dt, factor, dp, velT, velTT, stats, s); break;
-    case 31: launch_proj<3, 1>(m, mats, hK, dt, factor, dp, velT, velTT, stats, s); break;
-    case 32: launch_proj<3, 2>(m, mats, hK, dt, factor, dp, velT, velTT, stats, s); break;
-    case 33: launch_proj<3, 3>(m, mats, hK, dt, factor, dp, velT, velTT, stats, s); break;
-    case 34: launch_proj<3, 4>(m, mats, hK, dt, factor, dp, velT, velTT, stats, s); break;
+    case 21: SIPG_PROJ(2, 1); break;
+    case 22: SIPG_PROJ(2, 2); break;
+    case 23: SIPG_PROJ(2, 3); break;
+    case 24: SIPG_PROJ(2, 4); break;
+    case 31: SIPG_PROJ(3, 1); break;
+    case 32: SIPG_PROJ(3, 2); break;
+    case 33: SIPG_PROJ(3, 3); break;
+    case 34: SIPG_PROJ(3, 4); break;
     default: throw Error(SIPG_INVALID_ARG, "project_velocity: dimension");
+  }
+#undef SIPG_PROJ
+}
+
+// The host-buffer variants: inputs and output through device copies kept on the
+// mesh between calls (grown on demand), so a time step allocates nothing after
+// its first call. nin input arrays of in_bytes[i] bytes.
+void project_host(sipg_mesh* m, int order, double dt, double factor, const double* dp, const double* pr,
+                  const double* rho, const double* velT, double* velTT, double* stats) {
+  if (!m || order < 1 || order > 4 || (!dp && !pr) || !velT || !velTT)
+    throw Error(SIPG_INVALID_ARG, "project_velocity: null mesh/array or order outside 1..4");
+  const size_t nv = (size_t)m->K * np_of(m->dim, order);
+  const size_t vb = m->dim * nv * sizeof(double), sb = nv * sizeof(double);
+  const size_t gb = pr ? sb : vb;  // grad p or pressure
+  const size_t rb = rho ? sb : 0;
+  std::lock_guard<std::mutex> lk(m->proj_mu);
+  const size_t need = gb + rb + 2 * vb + 2 * sizeof(unsigned long long);
+  if (m->proj_io.bytes < need) {
+    m->proj_io = DevBuf();
+    m->proj_io = DevBuf(need);
+  }
+  char* base = m->proj_io.as<char>();
+  double* d_g = reinterpret_cast<double*>(base);
+  double* d_r = rho ? reinterpret_cast<double*>(base + gb) : nullptr;
+  double* d_v = reinterpret_cast<double*>(base + gb + rb);
+  double* d_out = reinterpret_cast<double*>(base + gb + rb + vb);
+  auto* d_st = reinterpret_cast<unsigned long long*>(base + gb + rb + 2 * vb);
+  SIPG_CUDA(cudaMemcpy(d_g, pr ? pr : dp, gb, cudaMemcpyHostToDevice));
+  if (rho) SIPG_CUDA(cudaMemcpy(d_r, rho, rb, cudaMemcpyHostToDevice));
+  SIPG_CUDA(cudaMemcpy(d_v, velT, vb, cudaMemcpyHostToDevice));
+  project_device(m, order, dt, factor, pr ? nullptr : d_g, pr ? d_g : nullptr, d_r, d_v, d_out, d_st, 0);
+  unsigned long long st[2] = {0, 0};
+  SIPG_CUDA(cudaMemcpy(velTT, d_out, vb, cudaMemcpyDeviceToHost));
+  SIPG_CUDA(cudaMemcpy(st, d_st, sizeof(st), cudaMemcpyDeviceToHost));
+  if (stats) {
+    stats[0] = (double)m->K;
+    stats[1] = (double)st[0];
+    stats[2] = (double)st[1];
   }
 }
 
@@ -509,38 +694,33 @@ using namespace sipg;
 extern "C" int sipg_project_velocity(sipg_mesh* m, int order, double dt, double factor, const double* dp,
                                      const double* velT, double* velTT, unsigned long long* stats,
                                      void* stream) {
-  return guarded([&] { project_device(m, order, dt, factor, dp, velT, velTT, stats, (cudaStream_t)stream); });
+  return guarded([&] {
+    if (!dp) throw Error(SIPG_INVALID_ARG, "project_velocity: null dp");
+    project_device(m, order, dt, factor, dp, nullptr, nullptr, velT, velTT, stats, (cudaStream_t)stream);
+  });
 }
 
 extern "C" int sipg_project_velocity_host(sipg_mesh* m, int order, double dt, double factor, const double* dp,
                                           const double* velT, double* velTT, double* stats) {
   return guarded([&] {
-    if (!m || order < 1 || order > 4 || !dp || !velT || !velTT)
-      throw Error(SIPG_INVALID_ARG, "project_velocity: null mesh/array or order outside 1..4");
-    const size_t n = (size_t)m->dim * m->K * np_of(m->dim, order), bytes = n * sizeof(double);
-    // device copies stay on the mesh between calls (grown on demand), so a time
-    // step's projection allocates nothing after the first call
-    std::lock_guard<std::mutex> lk(m->proj_mu);
-    const size_t need = 3 * bytes + 2 * sizeof(unsigned long long);
-    if (m->proj_io.bytes < need) {
-      m->proj_io = DevBuf();
-      m->proj_io = DevBuf(need);
-    }
-    char* base = m->proj_io.as<char>();
-    double* d_dp = reinterpret_cast<double*>(base);
-    double* d_v = reinterpret_cast<double*>(base + bytes);
-    double* d_out = reinterpret_cast<double*>(base + 2 * bytes);
-    auto* d_st = reinterpret_cast<unsigned long long*>(base + 3 * bytes);
-    SIPG_CUDA(cudaMemcpy(d_dp, dp, bytes, cudaMemcpyHostToDevice));
-    SIPG_CUDA(cudaMemcpy(d_v, velT, bytes, cudaMemcpyHostToDevice));
-    project_device(m, order, dt, factor, d_dp, d_v, d_out, d_st, 0);
-    unsigned long long st[2] = {0, 0};
-    SIPG_CUDA(cudaMemcpy(velTT, d_out, bytes, cudaMemcpyDeviceToHost));
-    SIPG_CUDA(cudaMemcpy(st, d_st, sizeof(st), cudaMemcpyDeviceToHost));
-    if (stats) {
-      stats[0] = (double)m->K;
-      stats[1] = (double)st[0];
-      stats[2] = (double)st[1];
-    }
+    if (!dp) throw Error(SIPG_INVALID_ARG, "project_velocity: null dp");
+    project_host(m, order, dt, factor, dp, nullptr, nullptr, velT, velTT, stats);
+  });
+}
+
+extern "C" int sipg_pressure_projection(sipg_mesh* m, int order, double dt, double factor, const double* pr,
+                                        const double* rho, const double* velT, double* velTT,
+                                        unsigned long long* stats, void* stream) {
+  return guarded([&] {
+    if (!pr) throw Error(SIPG_INVALID_ARG, "pressure_projection: null pr");
+    project_device(m, order, dt, factor, nullptr, pr, rho, velT, velTT, stats, (cudaStream_t)stream);
+  });
+}
+
+extern "C" int sipg_pressure_projection_host(sipg_mesh* m, int order, double dt, double factor, const double* pr,
+                                             const double* rho, const double* velT, double* velTT, double* stats) {
+  return guarded([&] {
+    if (!pr) throw Error(SIPG_INVALID_ARG, "pressure_projection: null pr");
+    project_host(m, order, dt, factor, nullptr, pr, rho, velT, velTT, stats);
   });
 }

@@ -256,6 +256,21 @@ def project_velocity_device(mesh, order, dt, dp_ptr, velT_ptr, velTT_ptr, stats_
                                       C.c_void_p(velT_ptr), C.c_void_p(velTT_ptr), C.c_void_p(stats_ptr or 0),
                                       C.c_void_p(stream or 0)))
 
+
+def pressure_projection(mesh, order, dt, pr, velT, rho=None, factor=None):
+    """Pressure projection step on host arrays: grad p with the central flux
+    (divided by rho when given), then the element-local velocity projection.
+    pr, rho: (K, Np); velT: (dim, K, Np). Returns (velTT, stats)."""
+    pr = np.ascontiguousarray(pr, dtype=np.float64)
+    velT = np.ascontiguousarray(velT, dtype=np.float64)
+    r = None if rho is None else np.ascontiguousarray(rho, dtype=np.float64)
+    out = np.empty_like(velT)
+    st = np.zeros(3)
+    f = projection_factor(mesh.dim, dt) if factor is None else factor
+    check(lib().sipg_pressure_projection_host(mesh.h, order, C.c_double(dt), C.c_double(f), _dp(pr), _dp(r),
+                                              _dp(velT), _dp(out), _dp(st)))
+    return out, st
+
 class Operator:
     """SIPG operator on a resident mesh (Poisson / Helmholtz / viscous)."""
 

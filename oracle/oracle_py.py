@@ -275,3 +275,11 @@ def project_velocity(om, dt, factor, dp, velT, use_ref=False):
     else:
         oracle_lib().oracle_project_velocity(*args)
     return out, st
+
+
+def grad_central(om, p):
+    """Central-flux DG gradient (dim, K, Np) of the nodal field p (K, Np)."""
+    p = np.ascontiguousarray(p, dtype=np.float64)
+    g = np.zeros((om.dim, om.K, om.Np))
+    oracle_lib().oracle_grad_central(C.byref(om.s), _d(p), _d(g))
+    return g

@@ -1136,3 +1136,62 @@ void oracle_project_velocity(const oracle_mesh *m, double dt, double factor, con
   stats[0] = cells; stats[1] = conv; stats[2] = iters;
   free(buf); free(h); free(minv);
 }
+
+/* DGMesh3D::grad_with_central_flux (unvendored OP2-DG-Toolkit; called at
+ * src/solvers/3d/mp_ins_solver.cpp:653 and ins_solver.cpp:361 before
+ * project_velocity), restated in strong form with the central flux:
+ *   grad_d p = sum_k G[k][d] (D_k p) + LIFT (fscale n_d ({p} - p^-))
+ * over interior faces ({p} - p^- = (p^+ - p^-) / 2); a boundary face takes
+ * p^+ = p^- and adds nothing. LIFT = M^-1 EMAT. grad holds dim components
+ * (dim x K x Np). Parity of this glue with the toolkit is unpinned (the toolkit
+ * is not vendored); it is pinned by its properties (exact for continuous
+ * polynomials of degree <= p). */
+void oracle_grad_central(const oracle_mesh *m, const double *p, double *grad) {
+  const int dim = m->dim, Np = m->Np, Nfp = m->Nfp, Nf = m->Nf, K = m->K, NFN = Nf * Nfp;
+  const size_t n = (size_t)K * Np;
+  const double *Dk[3] = {m->Dr, m->Ds, m->Dt};
+  const double *nrm[3] = {m->nx, m->ny, m->nz};
+  double *minv = (double *)malloc(sizeof(double) * Np * Np);
+  memcpy(minv, m->M, sizeof(double) * Np * Np);
+  invert_inplace(minv, Np);
+  double *lift = (double *)calloc((size_t)Np * NFN, sizeof(double));
+  for (int i = 0; i < Np; ++i)
+    for (int c = 0; c < NFN; ++c) {
+      double s = 0.0;
+      for (int j = 0; j < Np; ++j) s += minv[i * Np + j] * m->EMAT[(size_t)j * NFN + c];
+      lift[(size_t)i * NFN + c] = s;
+    }
+  /* per element face node: (p^+ - p^-) / 2, zero on boundary faces */
+  double *jmp = (double *)calloc((size_t)K * NFN, sizeof(double));
+  for (int fc = 0; fc < m->F; ++fc) {
+    const int eL = m->face2cells[2 * fc], eR = m->face2cells[2 * fc + 1];
+    const int fL = m->faceNum[2 * fc], fR = m->faceNum[2 * fc + 1];
+    for (int j = 0; j < Nfp; ++j) {
+      const int nl = m->fmaskL[fc * Nfp + j], nr = m->fmaskR[fc * Nfp + j];
+      const double pl = p[IDX(eL, nl, Np)], pr = p[IDX(eR, nr, Np)];
+      jmp[IDX(eL, fL * Nfp + face_pos(m, fL, nl), NFN)] = 0.5 * (pr - pl);
+      jmp[IDX(eR, fR * Nfp + face_pos(m, fR, nr), NFN)] = 0.5 * (pl - pr);
+    }
+  }
+  for (int e = 0; e < K; ++e) {
+    double G[3][3], J;
+    geo_unpack(m, e, G, &J);
+    for (int i = 0; i < Np; ++i) {
+      double dr[3] = {0, 0, 0};
+      for (int k = 0; k < dim; ++k)
+        for (int j = 0; j < Np; ++j) dr[k] += Dk[k][i * Np + j] * p[IDX(e, j, Np)];
+      for (int d = 0; d < dim; ++d) {
+        double s = 0.0;
+        for (int k = 0; k < dim; ++k) s += G[k][d] * dr[k];
+        for (int f = 0; f < Nf; ++f) {
+          const double w = m->fscale[IDX(e, f, Nf)] * nrm[d][IDX(e, f, Nf)];
+          double l = 0.0;
+          for (int k = 0; k < Nfp; ++k) l += lift[(size_t)i * NFN + f * Nfp + k] * jmp[IDX(e, f * Nfp + k, NFN)];
+          s += w * l;
+        }
+        grad[d * n + IDX(e, i, Np)] = s;
+      }
+    }
+  }
+  free(jmp); free(lift); free(minv);
+}

@@ -141,6 +141,8 @@ double oracle_pmg_lambda_max(const oracle_mesh *m, const int *bc_types, const do
 void oracle_proj_h(const oracle_mesh *m, double *h);
 void oracle_project_velocity(const oracle_mesh *m, double dt, double factor, const double *dp,
                              const double *velT, double *velTT, double *stats);
+/* Central-flux DG gradient of p (K x Np) into grad (dim x K x Np). */
+void oracle_grad_central(const oracle_mesh *m, const double *p, double *grad);
 
 #ifdef __cplusplus
 }

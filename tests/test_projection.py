@@ -156,3 +156,85 @@ def test_gpu_full_size_32cube_p3():
     out, st0 = sipg.project_velocity(mesh, order, dt, np.zeros_like(dp), const)
     assert st0[2] == 0
     assert rel_err(out, const) < 1e-13
+
+
+# ---- pressure projection step: central-flux gradient (/ rho) fused with the projection
+
+def poly_case(dim, n, order, seed=3):
+    """A continuous polynomial of degree `order` at the nodes, with its gradient."""
+    mesh = sipg.Mesh.box(dim, n, jitter=0.1, seed=seed)
+    t, e = sipg.ref_tables(dim, order), mesh.export(order)
+    x, y = e["x"], e["y"]
+    z = e["z"] if dim == 3 else np.zeros_like(x)
+    s = x + 2 * y - z
+    p = s ** order + 0.5 * x
+    g = [order * s ** (order - 1) + 0.5, 2 * order * s ** (order - 1), -order * s ** (order - 1)]
+    return mesh, O.OMesh(t, e), p, np.stack(g[:dim])
+
+
+@pytest.mark.parametrize("dim,order", [(3, 2), (3, 3), (3, 4), (2, 2), (2, 4)])
+def test_oracle_central_gradient_is_exact_for_continuous_polynomials(dim, order):
+    _, om, p, g = poly_case(dim, 3 if dim == 3 else 5, order)
+    assert np.abs(O.grad_central(om, p) - g).max() < 1e-9 * max(1.0, np.abs(g).max())
+
+
+def test_oracle_central_gradient_is_linear_and_kills_constants():
+    """On a discontinuous field: linear in p, and a constant adds nothing."""
+    mesh, om, _, _ = poly_case(3, 3, 3)
+    rng = np.random.default_rng(4)
+    p = rng.uniform(-1, 1, (om.K, om.Np))
+    g = O.grad_central(om, p)
+    a = O.grad_central(om, 2.0 * p + 1.0)
+    assert np.abs(a - 2.0 * g).max() < 1e-11 * np.abs(g).max()  # linear, constants have zero gradient
+
+
+def pressure_chain_oracle(om, dim, dt, pr, rho, velT):
+    g = O.grad_central(om, pr)
+    if rho is not None:
+        g = g / rho[None]
+    return O.project_velocity(om, dt, sipg.projection_factor(dim, dt), g, velT)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dim,n,order,dt,two_phase", [(3, 3, 3, 1e-2, True), (3, 3, 2, 1e-2, False),
+                                                       (3, 2, 4, 1e-2, True), (3, 3, 1, 1e-2, False),
+                                                       (2, 6, 3, 1e-3, True), (2, 6, 2, 1e-3, False)])
+def test_gpu_pressure_projection_matches_oracle(dim, n, order, dt, two_phase):
+    mesh, om, velT, _ = case(dim, n, order, 200 + 10 * dim + order, dt)
+    rng = np.random.default_rng(order)
+    pr = rng.uniform(-1, 1, (om.K, om.Np))
+    rho = rng.uniform(1.0, 1000.0, (om.K, om.Np)) if two_phase else None
+    want, wst = pressure_chain_oracle(om, dim, dt, pr, rho, velT)
+    got, gst = sipg.pressure_projection(mesh, order, dt, pr, velT, rho=rho)
+    check_close(dim, got, gst, want, wst)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dim,order", [(3, 3), (3, 4), (2, 3)])
+def test_gpu_central_gradient_alone(dim, order):
+    """factor = 0, dt = -1 and velT = 0 leave velTT = grad p / rho (the initial
+    residual is exactly zero): the gradient against the oracle, and exact for a
+    continuous polynomial."""
+    mesh, om, p, g = poly_case(dim, 3 if dim == 3 else 5, order)
+    zero = np.zeros((dim, om.K, om.Np))
+    got, st = sipg.pressure_projection(mesh, order, -1.0, p, zero, factor=0.0)
+    assert st[2] == 0
+    assert np.abs(got - g).max() < 1e-9 * np.abs(g).max()
+    rng = np.random.default_rng(9)
+    q = rng.uniform(-1, 1, p.shape)
+    rho = rng.uniform(1.0, 10.0, p.shape)
+    got, _ = sipg.pressure_projection(mesh, order, -1.0, q, zero, rho=rho, factor=0.0)
+    assert rel_err(got, O.grad_central(om, q) / rho[None]) < 1e-12
+
+
+@pytest.mark.gpu
+def test_gpu_fused_step_equals_gradient_then_projection():
+    dim, order, dt = 3, 3, 0.05
+    mesh, om, velT, _ = case(dim, 3, order, 77, dt)
+    rng = np.random.default_rng(1)
+    pr = rng.uniform(-1, 1, (om.K, om.Np))
+    rho = rng.uniform(1.0, 1000.0, (om.K, om.Np))
+    grad, _ = sipg.pressure_projection(mesh, order, -1.0, pr, np.zeros_like(velT), rho=rho, factor=0.0)
+    two_step, st2 = sipg.project_velocity(mesh, order, dt, grad, velT)
+    fused, st1 = sipg.pressure_projection(mesh, order, dt, pr, velT, rho=rho)
+    assert np.array_equal(fused, two_step) and np.array_equal(st1, st2)
