@@ -511,6 +511,25 @@ class VelocityProjection {
     if (mean_iters) *mean_iters = st[0] > 0 ? st[2] / st[0] : 0.0;
     return (int)st[1];
   }
+  // The pressure step from the pressure itself: grad_with_central_flux(pr),
+  // update_pressure_gradient (/ rho; rho.data == nullptr for the single-phase
+  // solver) and project_velocity (src/solvers/3d/mp_ins_solver.cpp:653-659,
+  // ins_solver.cpp:361-363) in one call.
+  int project_from_pressure(double dt, Dat pr, Dat rho, const Dat* velT, Dat* velTT, double* mean_iters = nullptr) {
+    const int dim = mesh_->dim();
+    const size_t n = velT[0].size();
+    in_v_.resize(dim * n);
+    out_.resize(dim * n);
+    for (int c = 0; c < dim; ++c) std::copy(velT[c].data, velT[c].data + n, in_v_.begin() + c * n);
+    double st[3] = {0, 0, 0};
+    const double factor = dim == 3 ? dt : dt * 1e3;
+    check(sipg_pressure_projection_host(mesh_->handle(), order_, dt, factor, pr.data, rho.data, in_v_.data(),
+                                        out_.data(), st),
+          "pressure_projection");
+    for (int c = 0; c < dim; ++c) std::copy(out_.begin() + c * n, out_.begin() + (c + 1) * n, velTT[c].data);
+    if (mean_iters) *mean_iters = st[0] > 0 ? st[2] / st[0] : 0.0;
+    return (int)st[1];
+  }
 
  private:
   DGMesh* mesh_;

@@ -149,6 +149,20 @@ int main() {
     std::printf("velocity projection converged=%d/%d iters=%.2f err=%.3e; random gradient converged=%d\n", conv, k,
                 it, err, conv2);
     failures += !(conv == k && it == 0.0 && err < 1e-13 && conv2 == k);
+    // from the pressure: a constant pressure has no gradient, so the result is the
+    // projection of velT alone, whatever rho is
+    std::vector<double> pc(N, 3.5), rho(N, 1.0), o2[3];
+    for (int c = 0; c < 3; ++c) o2[c].assign(N, 0.0);
+    for (auto& v : rho) v = 1.0 + 999.0 * (0.5 + 0.5 * U(rng));
+    for (int c = 0; c < 3; ++c)
+      for (auto& v : g[c]) v = 0.0;
+    Dat o2d[3] = {D(o2[0]), D(o2[1]), D(o2[2])};
+    proj.project(1e-2, gd, ud, od, nullptr);
+    int conv3 = proj.project_from_pressure(1e-2, D(pc), D(rho), ud, o2d, nullptr);
+    double err3 = 0;
+    for (int c = 0; c < 3; ++c) err3 = std::max(err3, rel_diff(o2[c], o[c], false));
+    std::printf("pressure projection converged=%d/%d vs zero-gradient projection err=%.3e\n", conv3, k, err3);
+    failures += !(conv3 == k && err3 < 1e-12);
   }
   std::printf("%s\n", failures ? "FAILED" : "OK");
   return failures ? 1 : 0;
