@@ -442,6 +442,30 @@ def run_projection(steps=20, cpu=True):
         p1.record(stream)
     torch.cuda.synchronize()
     ms_p = p0.elapsed_time(p1) / steps
+    # the right-hand side of the same pressure step: central-flux div velT, the
+    # dPdN update and lift, mass (sipg_pressure_rhs), Neumann data U(-1, 1)
+    Nfp = sipg.ref_sizes(3, PROJ_ORDER)[1]
+    dn = torch.from_numpy(np.random.default_rng(8).uniform(-1, 1, (K, 4, Nfp))).cuda()
+    do = torch.zeros_like(dn)
+    rhs = torch.empty((K, Np), dtype=torch.float64, device="cuda")
+
+    def call_r():
+        sipg.check(lib.sipg_pressure_rhs(mesh.h, PROJ_ORDER, C.c_double(PROJ_DT), C.c_double(2.0),
+                                         C.c_double(-1.0), C.c_void_p(d_v.data_ptr()), C.c_void_p(dn.data_ptr()),
+                                         C.c_void_p(do.data_ptr()), C.c_void_p(rhs.data_ptr()),
+                                         C.c_void_p(stream.cuda_stream)))
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            call_r()
+        torch.cuda.synchronize()
+        r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        r0.record(stream)
+        for _ in range(steps):
+            call_r()
+        r1.record(stream)
+    torch.cuda.synchronize()
+    ms_r = r0.elapsed_time(r1) / steps
+    rhs_bytes = K * (3 * Np * 8 + 3 * 4 * Nfp * 8 + Np * 8 + 10 * 8 + 4 * 4 + 4)
     npp = Np * Np
     # FP64 flops: per element one operator application and one preconditioner
     # application to start, then per CG iteration one of each (20 Np^2 and 6 Np^2
@@ -456,6 +480,10 @@ def run_projection(steps=20, cpu=True):
            "kernel": "k_proj_cg<3,3> (one launch per projection)",
            "ms": ms, "gdofs": dofs / (ms * 1e-3) / 1e9, "converged": conv, "cells": K,
            "mean_iters": iters / K,
+           "pressure_rhs": {"ms": ms_r, "hbm_gbs": rhs_bytes / (ms_r * 1e-3) / 1e9,
+                            "bytes_per_elem": rhs_bytes // K,
+                            "what": "sipg_pressure_rhs: J M (-div_c velT / dt + LIFT (b0 dPdN + b1 dPdN_old)), "
+                                    "dPdN_old updated, one kernel"},
            "pressure_step": {"ms": ms_p, "gdofs": dofs / (ms_p * 1e-3) / 1e9,
                              "what": "sipg_pressure_projection: central-flux grad p / rho (rho U(1,1000)) and the "
                                      "projection in one kernel, from pr (K x Np) instead of a stored gradient"},

@@ -328,6 +328,26 @@ int sipg_pressure_projection(sipg_mesh *m, int order, double dt, double factor, 
 int sipg_pressure_projection_host(sipg_mesh *m, int order, double dt, double factor, const double *pr,
                                   const double *rho, const double *velT, double *velTT, double *stats);
 
+/* ---- pressure right-hand side: replaces, in INSSolver3D::pressure
+ * (src/solvers/3d/ins_solver.cpp:313-322; 2D src/solvers/2d/ins_solver.cpp:269,
+ * 309-319; MPINSSolver3D mp_ins_solver.cpp:581-612 with its own dPdN update),
+ * mesh->div_with_central_flux(velT) (OP2-DG-Toolkit, unvendored), ins_3d_pr_1 /
+ * ins_pressure_rhs_2d (divVelT *= -1/dt; dPdN_old = b0 dPdN + b1 dPdN_old), the
+ * LIFT of dPdN_old and mesh->mass, as one kernel:
+ *   rhs = J M ( -div_c(velT) / dt + LIFT (b0 dPdN + b1 dPdN_old) ),
+ * div_c = sum_d d(u_d)/dx_d + LIFT (fscale n . (u+ - u-) / 2) over interior faces
+ * (central flux; boundary faces add nothing). dPdN_old is updated in place. The
+ * Neumann data dPdN (the curl-curl boundary term the caller assembles,
+ * ins_3d_pr_0.h / mp_ins_3d_pr_0.h) and dPdN_old are K x (dim + 1) x Nfp in the
+ * face-node order of the reference's FMASK, or NULL (zero; dPdN_old NULL is not
+ * written). velT: dim x K x Np; rhs: K x Np. The Dirichlet data of
+ * ins_3d_pr_dirichlet enter through sipg_op_apply_bc_host as before. Device
+ * pointers, or host pointers in the synchronous _host variant. */
+int sipg_pressure_rhs(sipg_mesh *m, int order, double dt, double b0, double b1, const double *velT,
+                      const double *dPdN, double *dPdN_old, double *rhs, void *stream);
+int sipg_pressure_rhs_host(sipg_mesh *m, int order, double dt, double b0, double b1, const double *velT,
+                           const double *dPdN, double *dPdN_old, double *rhs);
+
 /* Number of kernels this library has launched so far in the process
  * (diagnostics for benchmarks; no reference counterpart). */
 int sipg_launch_count(unsigned long long *n);

@@ -515,6 +515,142 @@ __global__ void __launch_bounds__(kProjWarps * 32) k_proj_cg(const ProjArgs a) {
   }
 }
 
+
+// Right-hand side of the pressure solve, one warp per element:
+//   rhs = J M ( -(div_c velT) / dt + LIFT dPdN_new ),  dPdN_new = b0 dPdN + b1 dPdN_old,
+// div_c the central-flux divergence (volume sum_k D_k (G u)_k plus LIFT of
+// fscale n . (u+ - u-) / 2 on interior faces); dPdN_old <- dPdN_new.
+struct PrRhsArgs {
+  int K;
+  const double* geof;
+  const double* mats;
+  double dt, b0, b1;
+  const int* nbr;
+  const uint32_t* fcode;
+  const int8_t* itab;
+  const double* velT;      // dim x K x Np
+  const double* dPdN;      // K x (dim + 1) x Nfp or null
+  double* dPdN_old;        // K x (dim + 1) x Nfp or null
+  double* rhs;             // K x Np
+};
+
+template <int D, int P>
+__global__ void __launch_bounds__(kProjWarps * 32) k_pr_rhs(const PrRhsArgs a) {
+  constexpr int NP = proj_np(D, P), NPE = proj_npe(D, P), NPL = (NP + 31) / 32, NG = D == 3 ? 10 : 5;
+  constexpr int NF = D + 1, NFP = proj_nfp(D, P), NFPE = proj_nfpe(D, P), MAT = proj_mat_doubles<D, P>();
+  constexpr int WB = (D + 1) * NPE + 2 * NF * NFPE;
+  extern __shared__ double sm[];
+  const double* sD = sm;
+  const double* sM = sm + 2 * D * MAT;
+  const double* sL = sm + proj_nmat(D) * MAT;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* sGU = sm + proj_blob_doubles<D, P>() + warp * WB;  // [D][NPE]
+  double* sPre = sGU + D * NPE;                              // [NPE]
+  double* sF1 = sPre + NPE;                                  // [NF][NFPE] n . (u+ - u-) / 2 fscale
+  double* sF2 = sF1 + NF * NFPE;                             // [NF][NFPE] dPdN_new
+  for (int i = threadIdx.x; i < proj_blob_doubles<D, P>(); i += blockDim.x) sm[i] = a.mats[i];
+  for (int i = lane; i < WB; i += 32) sGU[i] = 0.0;
+  __syncthreads();
+  const size_t n = (size_t)a.K * NP;
+  const int8_t* fmask = a.itab;
+  const int8_t* npos = a.itab + NF * NFP;
+  const double inv_dt = 1.0 / a.dt;
+  for (int e = blockIdx.x * kProjWarps + warp; e < a.K; e += gridDim.x * kProjWarps) {
+    double G[3][3] = {};
+    const double* g = a.geof + (size_t)e * NG;
+    double J;
+    if (D == 3) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) G[k][c] = __ldg(g + k * 3 + c);
+      J = __ldg(g + 9);
+    } else {
+      G[0][0] = __ldg(g + 0); G[0][1] = __ldg(g + 1);
+      G[1][0] = __ldg(g + 2); G[1][1] = __ldg(g + 3);
+      J = __ldg(g + 4);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int u = 0; u < NPL; ++u) {
+      const int i = lane + 32 * u;
+      if (i < NP) {
+        double uc[D];
+#pragma unroll
+        for (int c = 0; c < D; ++c) uc[c] = __ldg(a.velT + c * n + (size_t)e * NP + i);
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+          double s = 0.0;
+#pragma unroll
+          for (int c = 0; c < D; ++c) s += G[k][c] * uc[c];
+          sGU[k * NPE + i] = s;
+        }
+      }
+    }
+    for (int m = lane; m < NF * NFP; m += 32) {
+      const int f = m / NFP, k = m - f * NFP;
+      double un = 0.0;
+      const int nb = __ldg(a.nbr + (size_t)e * NF + f);
+      if (nb >= 0) {
+        const int code = (__ldg(a.fcode + e) >> (8 * f)) & 0xff;
+        const int fr = code & 3, sg = code >> 2;
+        const int nn = fmask[fr * NFP + npos[sg * NFP + k]], o = fmask[f * NFP + k];
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          double v;  // fscale n_d of face f (the unnormalised outward normal)
+          if (D == 3) v = f == 0 ? -G[2][d] : f == 1 ? -G[1][d] : f == 2 ? (G[0][d] + G[1][d]) + G[2][d] : -G[0][d];
+          else v = f == 0 ? -G[1][d] : f == 1 ? G[0][d] + G[1][d] : -G[0][d];
+          un += v * (0.5 * (__ldg(a.velT + d * n + (size_t)nb * NP + nn) - __ldg(a.velT + d * n + (size_t)e * NP + o)));
+        }
+      }
+      const size_t fi = (size_t)e * NF * NFP + m;
+      const double dn = (a.dPdN ? a.b0 * a.dPdN[fi] : 0.0) + (a.dPdN_old ? a.b1 * a.dPdN_old[fi] : 0.0);
+      if (a.dPdN_old) a.dPdN_old[fi] = dn;
+      sF1[f * NFPE + k] = un;
+      sF2[f * NFPE + k] = dn;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int u = 0; u < NPL; ++u) {
+      const int i = lane + 32 * u;
+      if (i < NP) {
+        double vol = 0.0, l1 = 0.0, l2 = 0.0;
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+          double y[1];
+          mat_vec<NP, NPE, 1>(sD + k * MAT, sGU + k * NPE, 0, i, y);
+          vol += y[0];
+        }
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+          double y[1];
+          mat_vec<NP, NFPE, 1>(sL + f * NP * NFPE, sF1 + f * NFPE, 0, i, y);
+          l1 += y[0];
+          mat_vec<NP, NFPE, 1>(sL + f * NP * NFPE, sF2 + f * NFPE, 0, i, y);
+          l2 += y[0];
+        }
+        sPre[i] = -(vol + l1) * inv_dt + l2;
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int u = 0; u < NPL; ++u) {
+      const int i = lane + 32 * u;
+      if (i < NP) {
+        double y[1];
+        mat_vec<NP, NPE, 1>(sM, sPre, 0, i, y);
+        a.rhs[(size_t)e * NP + i] = J * y[0];
+      }
+    }
+  }
+}
+
+template <int D, int P>
+__host__ __device__ constexpr int pr_rhs_smem_doubles() {
+  return proj_blob_doubles<D, P>() +
+         kProjWarps * ((D + 1) * proj_npe(D, P) + 2 * (D + 1) * proj_nfpe(D, P));
+}
+
 // Reference-element matrices in the kernel's layouts, per (device, dim, order).
 struct ProjMats {
   DevBuf blob;
@@ -686,6 +822,61 @@ void project_host(sipg_mesh* m, int order, double dt, double factor, const doubl
   }
 }
 
+
+template <int D, int P>
+void launch_pr_rhs(const PrRhsArgs& a, cudaStream_t s) {
+  constexpr size_t smem = pr_rhs_smem_doubles<D, P>() * sizeof(double);
+  static_assert(smem <= 227 * 1024, "pressure rhs shared memory");
+  auto kern = k_pr_rhs<D, P>;
+  static const int per_sm = [&] {
+    SIPG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int nb = 0;
+    SIPG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, kProjWarps * 32, smem));
+    return std::max(nb, 1);
+  }();
+  const int need = (a.K + kProjWarps - 1) / kProjWarps;
+  const int grid = std::max(1, std::min(need, per_sm * num_sms()));
+  kern<<<grid, kProjWarps * 32, smem, s>>>(a);
+  SIPG_CUDA(cudaGetLastError());
+  note_launch();
+}
+
+void pressure_rhs_device(sipg_mesh* m, int order, double dt, double b0, double b1, const double* velT,
+                         const double* dPdN, double* dPdN_old, double* rhs, cudaStream_t s) {
+  if (!m || order < 1 || order > 4 || !velT || !rhs)
+    throw Error(SIPG_INVALID_ARG, "pressure_rhs: null mesh/array or order outside 1..4");
+  if (!std::isfinite(dt) || dt == 0.0 || !std::isfinite(b0) || !std::isfinite(b1))
+    throw Error(SIPG_INVALID_ARG, "pressure_rhs: dt/b0/b1");
+  if (rhs == velT || (dPdN_old && dPdN_old == dPdN)) throw Error(SIPG_INVALID_ARG, "pressure_rhs: aliasing");
+  m->ensure_device();
+  PrRhsArgs a{};
+  a.K = m->K;
+  a.geof = m->geof64.as<double>();
+  a.mats = proj_mats(m->dim, order).blob.as<double>();
+  a.dt = dt;
+  a.b0 = b0;
+  a.b1 = b1;
+  a.nbr = m->nbr.as<int>();
+  a.fcode = m->fcode.as<uint32_t>();
+  a.itab = dev_ref(m->dim, order).itab.as<int8_t>();
+  a.velT = velT;
+  a.dPdN = dPdN;
+  a.dPdN_old = dPdN_old;
+  a.rhs = rhs;
+  if (m->K == 0) return;
+  switch (m->dim * 10 + order) {
+    case 21: launch_pr_rhs<2, 1>(a, s); break;
+    case 22: launch_pr_rhs<2, 2>(a, s); break;
+    case 23: launch_pr_rhs<2, 3>(a, s); break;
+    case 24: launch_pr_rhs<2, 4>(a, s); break;
+    case 31: launch_pr_rhs<3, 1>(a, s); break;
+    case 32: launch_pr_rhs<3, 2>(a, s); break;
+    case 33: launch_pr_rhs<3, 3>(a, s); break;
+    case 34: launch_pr_rhs<3, 4>(a, s); break;
+    default: throw Error(SIPG_INVALID_ARG, "pressure_rhs: dimension");
+  }
+}
+
 }  // namespace
 }  // namespace sipg
 
@@ -722,5 +913,38 @@ extern "C" int sipg_pressure_projection_host(sipg_mesh* m, int order, double dt,
   return guarded([&] {
     if (!pr) throw Error(SIPG_INVALID_ARG, "pressure_projection: null pr");
     project_host(m, order, dt, factor, nullptr, pr, rho, velT, velTT, stats);
+  });
+}
+
+extern "C" int sipg_pressure_rhs(sipg_mesh* m, int order, double dt, double b0, double b1, const double* velT,
+                                 const double* dPdN, double* dPdN_old, double* rhs, void* stream) {
+  return guarded([&] { pressure_rhs_device(m, order, dt, b0, b1, velT, dPdN, dPdN_old, rhs, (cudaStream_t)stream); });
+}
+
+extern "C" int sipg_pressure_rhs_host(sipg_mesh* m, int order, double dt, double b0, double b1, const double* velT,
+                                      const double* dPdN, double* dPdN_old, double* rhs) {
+  return guarded([&] {
+    if (!m || order < 1 || order > 4 || !velT || !rhs)
+      throw Error(SIPG_INVALID_ARG, "pressure_rhs: null mesh/array or order outside 1..4");
+    const int Np = np_of(m->dim, order), Nfp = m->dim == 2 ? order + 1 : (order + 1) * (order + 2) / 2;
+    const size_t vb = (size_t)m->dim * m->K * Np * sizeof(double), sb = (size_t)m->K * Np * sizeof(double);
+    const size_t fb = (size_t)m->K * (m->dim + 1) * Nfp * sizeof(double);
+    std::lock_guard<std::mutex> lk(m->proj_mu);
+    const size_t need = vb + sb + 2 * fb;
+    if (m->proj_io.bytes < need) {
+      m->proj_io = DevBuf();
+      m->proj_io = DevBuf(need);
+    }
+    char* base = m->proj_io.as<char>();
+    double* d_v = reinterpret_cast<double*>(base);
+    double* d_rhs = reinterpret_cast<double*>(base + vb);
+    double* d_n = dPdN ? reinterpret_cast<double*>(base + vb + sb) : nullptr;
+    double* d_o = dPdN_old ? reinterpret_cast<double*>(base + vb + sb + fb) : nullptr;
+    SIPG_CUDA(cudaMemcpy(d_v, velT, vb, cudaMemcpyHostToDevice));
+    if (d_n) SIPG_CUDA(cudaMemcpy(d_n, dPdN, fb, cudaMemcpyHostToDevice));
+    if (d_o) SIPG_CUDA(cudaMemcpy(d_o, dPdN_old, fb, cudaMemcpyHostToDevice));
+    pressure_rhs_device(m, order, dt, b0, b1, d_v, d_n, d_o, d_rhs, 0);
+    SIPG_CUDA(cudaMemcpy(rhs, d_rhs, sb, cudaMemcpyDeviceToHost));
+    if (d_o) SIPG_CUDA(cudaMemcpy(dPdN_old, d_o, fb, cudaMemcpyDeviceToHost));
   });
 }

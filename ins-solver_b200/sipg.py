@@ -271,6 +271,19 @@ def pressure_projection(mesh, order, dt, pr, velT, rho=None, factor=None):
                                               _dp(velT), _dp(out), _dp(st)))
     return out, st
 
+
+def pressure_rhs(mesh, order, dt, velT, dPdN=None, dPdN_old=None, b0=1.0, b1=0.0):
+    """Right-hand side of the pressure solve on host arrays: J M (-div_c(velT) / dt
+    + LIFT (b0 dPdN + b1 dPdN_old)). velT: (dim, K, Np); dPdN, dPdN_old:
+    (K, dim + 1, Nfp) or None. Returns (rhs (K, Np), updated dPdN_old or None)."""
+    velT = np.ascontiguousarray(velT, dtype=np.float64)
+    dn = None if dPdN is None else np.ascontiguousarray(dPdN, dtype=np.float64)
+    do = None if dPdN_old is None else np.array(dPdN_old, dtype=np.float64, order="C", copy=True)
+    rhs = np.empty(velT.shape[1:])
+    check(lib().sipg_pressure_rhs_host(mesh.h, order, C.c_double(dt), C.c_double(b0), C.c_double(b1), _dp(velT),
+                                       _dp(dn), _dp(do), _dp(rhs)))
+    return rhs, do
+
 class Operator:
     """SIPG operator on a resident mesh (Poisson / Helmholtz / viscous)."""
 

@@ -283,3 +283,14 @@ def grad_central(om, p):
     g = np.zeros((om.dim, om.K, om.Np))
     oracle_lib().oracle_grad_central(C.byref(om.s), _d(p), _d(g))
     return g
+
+
+def pressure_rhs(om, dt, velT, dPdN=None, dPdN_old=None, b0=1.0, b1=0.0):
+    """J M (-div_c(velT) / dt + LIFT (b0 dPdN + b1 dPdN_old)); returns (rhs, dPdN_old updated)."""
+    velT = np.ascontiguousarray(velT, dtype=np.float64)
+    dn = None if dPdN is None else np.ascontiguousarray(dPdN, dtype=np.float64)
+    do = None if dPdN_old is None else np.array(dPdN_old, dtype=np.float64, order="C", copy=True)
+    rhs = np.zeros((om.K, om.Np))
+    oracle_lib().oracle_pressure_rhs(C.byref(om.s), C.c_double(dt), C.c_double(b0), C.c_double(b1), _d(velT),
+                                     _d(dn), _d(do), _d(rhs))
+    return rhs, do

@@ -1195,3 +1195,58 @@ void oracle_grad_central(const oracle_mesh *m, const double *p, double *grad) {
   }
   free(jmp); free(lift); free(minv);
 }
+
+/* DGMesh3D::div_with_central_flux (unvendored OP2-DG-Toolkit), restated like
+ * the gradient above: div u = sum_d sum_k G[k][d] (D_k u_d) + LIFT (fscale n .
+ * (u+ - u-) / 2) over interior faces. u: dim x K x Np; div: K x Np. */
+static void div_central(const oracle_mesh *m, const double *u, double *div) {
+  const int dim = m->dim, Np = m->Np, K = m->K;
+  const size_t n = (size_t)K * Np;
+  double *g = (double *)malloc(sizeof(double) * dim * n);
+  for (int d = 0; d < dim; ++d) {
+    oracle_grad_central(m, u + d * n, g);
+    for (size_t i = 0; i < n; ++i) div[i] = (d == 0 ? 0.0 : div[i]) + g[d * n + i];
+  }
+  free(g);
+}
+
+/* Right-hand side of the pressure solve: INSSolver3D::pressure
+ * (src/solvers/3d/ins_solver.cpp:313-322): ins_3d_pr_1.h (divVelT *= -1/dt,
+ * dPdN_old = b0 dPdN + b1 dPdN_old), then divVelT += LIFT dPdN_old
+ * (op2_gemv), then mesh->mass; 2D src/solvers/2d/ins_solver.cpp:309-319
+ * (ins_pressure_rhs_2d.h). dPdN, dPdN_old: K x Nf x Nfp or NULL. */
+void oracle_pressure_rhs(const oracle_mesh *m, double dt, double b0, double b1, const double *velT,
+                         const double *dPdN, double *dPdN_old, double *rhs) {
+  const int Np = m->Np, Nf = m->Nf, Nfp = m->Nfp, K = m->K, NFN = Nf * Nfp;
+  double *minv = (double *)malloc(sizeof(double) * Np * Np);
+  memcpy(minv, m->M, sizeof(double) * Np * Np);
+  invert_inplace(minv, Np);
+  double *div = (double *)malloc(sizeof(double) * (size_t)K * Np);
+  double *dn = (double *)calloc(NFN, sizeof(double));
+  div_central(m, velT, div);
+  const double factor = 1.0 / dt;
+  for (int e = 0; e < K; ++e) {
+    double G[3][3], J, pre[64];
+    geo_unpack(m, e, G, &J);
+    for (int c = 0; c < NFN; ++c) {
+      const size_t fi = (size_t)e * NFN + c;
+      dn[c] = (dPdN ? b0 * dPdN[fi] : 0.0) + (dPdN_old ? b1 * dPdN_old[fi] : 0.0);
+      if (dPdN_old) dPdN_old[fi] = dn[c];
+    }
+    for (int i = 0; i < Np; ++i) {
+      double l = 0.0;
+      for (int c = 0; c < NFN; ++c) {
+        double lift = 0.0;
+        for (int j = 0; j < Np; ++j) lift += minv[i * Np + j] * m->EMAT[(size_t)j * NFN + c];
+        l += lift * dn[c];
+      }
+      pre[i] = -div[IDX(e, i, Np)] * factor + l;
+    }
+    for (int i = 0; i < Np; ++i) {
+      double s = 0.0;
+      for (int j = 0; j < Np; ++j) s += m->M[i * Np + j] * pre[j];
+      rhs[IDX(e, i, Np)] = J * s;
+    }
+  }
+  free(dn); free(div); free(minv);
+}

@@ -143,6 +143,9 @@ void oracle_project_velocity(const oracle_mesh *m, double dt, double factor, con
                              const double *velT, double *velTT, double *stats);
 /* Central-flux DG gradient of p (K x Np) into grad (dim x K x Np). */
 void oracle_grad_central(const oracle_mesh *m, const double *p, double *grad);
+/* Pressure right-hand side J M (-div_c(velT)/dt + LIFT (b0 dPdN + b1 dPdN_old)). */
+void oracle_pressure_rhs(const oracle_mesh *m, double dt, double b0, double b1, const double *velT,
+                         const double *dPdN, double *dPdN_old, double *rhs);
 
 #ifdef __cplusplus
 }

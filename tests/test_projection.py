@@ -238,3 +238,67 @@ def test_gpu_fused_step_equals_gradient_then_projection():
     two_step, st2 = sipg.project_velocity(mesh, order, dt, grad, velT)
     fused, st1 = sipg.pressure_projection(mesh, order, dt, pr, velT, rho=rho)
     assert np.array_equal(fused, two_step) and np.array_equal(st1, st2)
+
+
+# ---- pressure right-hand side: central-flux divergence, dPdN update and lift, mass
+
+def vec_poly_case(dim, n, order, seed=5):
+    """A continuous polynomial velocity field of degree `order` and its divergence."""
+    mesh = sipg.Mesh.box(dim, n, jitter=0.1, seed=seed)
+    t, e = sipg.ref_tables(dim, order), mesh.export(order)
+    x, y = e["x"], e["y"]
+    z = e["z"] if dim == 3 else np.zeros_like(x)
+    s = x - y + 2 * z
+    u = [s ** order, x * 0.5 + y ** order, (x + z) ** order]
+    div = order * s ** (order - 1) + order * y ** (order - 1)
+    if dim == 3:
+        div = div + order * (x + z) ** (order - 1)
+    return mesh, t, e, O.OMesh(t, e), np.stack(u[:dim]), div
+
+
+@pytest.mark.parametrize("dim,order", [(3, 2), (3, 3), (2, 3), (2, 4)])
+def test_oracle_pressure_rhs_divergence_is_exact_for_continuous_polynomials(dim, order):
+    mesh, t, e, om, u, div = vec_poly_case(dim, 3 if dim == 3 else 5, order)
+    dt = 0.01
+    rhs, _ = O.pressure_rhs(om, dt, u)
+    J = e["geof"][:, -1]
+    want = J[:, None] * ((-div / dt) @ t["M"].T)
+    assert np.abs(rhs - want).max() < 1e-9 * np.abs(want).max()
+
+
+def test_oracle_pressure_rhs_neumann_term_is_the_face_mass():
+    """LIFT then mass is EMAT: with velT = 0, rhs = J EMAT (b0 dPdN + b1 dPdN_old)."""
+    mesh, t, e, om, u, _ = vec_poly_case(3, 2, 3)
+    rng = np.random.default_rng(2)
+    shp = (om.K, 4, t["Nfp"])
+    dn, do = rng.uniform(-1, 1, shp), rng.uniform(-1, 1, shp)
+    rhs, do2 = O.pressure_rhs(om, 0.01, np.zeros_like(u), dn, do, b0=2.0, b1=-1.0)
+    new = 2.0 * dn - do
+    assert np.array_equal(do2, new)
+    want = e["geof"][:, -1][:, None] * (new.reshape(om.K, -1) @ t["EMAT"].T)
+    assert np.abs(rhs - want).max() < 1e-11 * np.abs(want).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dim,n,order", [(3, 3, 3), (3, 3, 1), (3, 2, 4), (3, 3, 2), (2, 6, 3), (2, 5, 2)])
+def test_gpu_pressure_rhs_matches_oracle(dim, n, order):
+    mesh, om, velT, _ = case(dim, n, order, 300 + 10 * dim + order, 1e-2)
+    rng = np.random.default_rng(order + 10 * dim)
+    shp = (om.K, dim + 1, sipg.ref_sizes(dim, order)[1])
+    dn, do = rng.uniform(-1, 1, shp), rng.uniform(-1, 1, shp)
+    want, wdo = O.pressure_rhs(om, 1e-2, velT, dn, do, b0=2.0, b1=-1.0)
+    got, gdo = sipg.pressure_rhs(mesh, order, 1e-2, velT, dn, do, b0=2.0, b1=-1.0)
+    assert rel_err(got, want) < 1e-12
+    assert rel_err(gdo, wdo) < 1e-15
+    got0, none = sipg.pressure_rhs(mesh, order, 1e-2, velT)  # no Neumann data
+    want0, _ = O.pressure_rhs(om, 1e-2, velT)
+    assert none is None and rel_err(got0, want0) < 1e-12
+
+
+@pytest.mark.gpu
+def test_gpu_pressure_rhs_exact_divergence():
+    dim, order = 3, 3
+    mesh, t, e, om, u, div = vec_poly_case(dim, 3, order)
+    got, _ = sipg.pressure_rhs(mesh, order, 0.01, u)
+    want = e["geof"][:, -1][:, None] * ((-div / 0.01) @ t["M"].T)
+    assert np.abs(got - want).max() < 1e-9 * np.abs(want).max()
