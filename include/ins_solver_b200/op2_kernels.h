@@ -1332,5 +1332,69 @@ SIPG_OP2_HD void ins_proj_cg_2d(const double *geof, const double *pen, const dou
   detail::proj_cg<2, ORDER>(geof, pen, rhs, x, cell_g, conv_g, iter_g);
 }
 
+// ---- pressure step around the solve (src/solvers/3d/ins_solver.cpp:313-322,
+// mp_ins_solver.cpp:581-612, :546-552, :676-692; 2D src/solvers/2d/ins_solver.cpp:309-319).
+// The fused performance path is sipg_pressure_rhs / sipg_pressure_projection.
+
+// divVelT <- -divVelT / dt; dPdN_old <- b0 dPdN + b1 dPdN_old (ins_3d_pr_1.h)
+template <int ORDER>
+SIPG_OP2_HD void ins_3d_pr_1(const double *b0, const double *b1, const double *dt, const double *dPdN,
+                             double *dPdN_old, double *divVelT) {
+  using G = Dg<3, ORDER>;
+  const double inv_dt = 1.0 / *dt;
+  for (int i = 0; i < G::NP; ++i) divVelT[i] = -divVelT[i] * inv_dt;
+  for (int i = 0; i < G::NUM_FACES * G::NPF; ++i) dPdN_old[i] = (*b0) * dPdN[i] + (*b1) * dPdN_old[i];
+}
+
+// the 2D twin (ins_pressure_rhs_2d.h)
+template <int ORDER>
+SIPG_OP2_HD void ins_pressure_rhs_2d(const double *b0, const double *b1, const double *dt, const double *dPdN,
+                                     double *dPdNOld, double *divVelT) {
+  using G = Dg<2, ORDER>;
+  const double inv_dt = 1.0 / *dt;
+  for (int i = 0; i < G::NP; ++i) divVelT[i] = -divVelT[i] * inv_dt;
+  for (int i = 0; i < G::NUM_FACES * G::NPF; ++i) dPdNOld[i] = (*b0) * dPdN[i] + (*b1) * dPdNOld[i];
+}
+
+// dPdNOld <- b0 dPdN + b1 dPdNOld (mp_ins_pr_bc_dpdn_factors.h)
+template <int DIM, int ORDER>
+SIPG_OP2_HD void mp_ins_pr_bc_dpdn_factors(const double *b0, const double *b1, const double *dPdN,
+                                           double *dPdNOld) {
+  using G = Dg<DIM, ORDER>;
+  for (int i = 0; i < G::NUM_FACES * G::NPF; ++i) dPdNOld[i] = (*b0) * dPdN[i] + (*b1) * dPdNOld[i];
+}
+
+// div <- div * factor (mp_ins_pr_div_factor.h; the caller passes -1 / dt)
+template <int DIM, int ORDER>
+SIPG_OP2_HD void mp_ins_pr_div_factor(const double *_div_factor, double *div) {
+  const double f = *_div_factor;
+  for (int i = 0; i < Dg<DIM, ORDER>::NP; ++i) div[i] *= f;
+}
+
+// grad p <- grad p / rho (mp_ins_3d_pr_2.h, update_pressure_gradient)
+template <int ORDER>
+SIPG_OP2_HD void mp_ins_3d_pr_2(const double *rho, double *dpdx, double *dpdy, double *dpdz) {
+  for (int i = 0; i < Dg<3, ORDER>::NP; ++i) {
+    dpdx[i] /= rho[i];
+    dpdy[i] /= rho[i];
+    dpdz[i] /= rho[i];
+  }
+}
+
+// viscous right-hand side rho u Re/dt and the mass factor g0 Re/dt rho of the
+// two-phase Helmholtz solve (mp_ins_3d_vis_0.h; mu and art_vis are not changed:
+// the reference leaves its artificial-viscosity update commented out)
+template <int ORDER>
+SIPG_OP2_HD void mp_ins_3d_vis_0(const double *fact0, const double *fact1, const double *rho, double *mu,
+                                 const double *art_vis, const double *u, const double *v, const double *w,
+                                 double *rhs0, double *rhs1, double *rhs2, double *mm_factor) {
+  for (int i = 0; i < Dg<3, ORDER>::NP; ++i) {
+    rhs0[i] = u[i] * *fact0 * rho[i];
+    rhs1[i] = v[i] * *fact0 * rho[i];
+    rhs2[i] = w[i] * *fact0 * rho[i];
+    mm_factor[i] = *fact1 * rho[i];
+  }
+}
+
 }  // namespace op2
 }  // namespace ins_solver_b200

@@ -29,6 +29,7 @@ KERNELS_3D = [
     "cg3_recp_factor_inv_mass", "vmf_3d_mult_mm_geof", "vmf_3d_apply_bc",
     "constant_mult", "reciprocal", "copy_dg_np_mat", "poisson_pr_fact", "poisson_vis_fact",
     "ins_3d_proj_rhs", "ins_3d_proj_pen", "ins_3d_proj_cg_precon", "ins_proj_setup_0", "ins_proj_setup_1",
+    "ins_3d_pr_1", "mp_ins_3d_pr_2", "mp_ins_pr_bc_dpdn_factors", "mp_ins_pr_div_factor", "mp_ins_3d_vis_0",
 ]
 KERNELS_2D = [
     "fvmf_2d_grad", "fvmf_2d_calc_tau_faces", "fvmf_2d_calc_tau_bfaces", "vmf_2d_mult_avg_jump",
@@ -42,6 +43,7 @@ KERNELS_2D = [
     "cg_recp_factor_inv_mass", "vmf_2d_mult_flux", "vmf_2d_mult_mm_geof", "vmf_2d_apply_bc",
     "constant_mult", "reciprocal", "copy_dg_np_mat", "poisson_pr_fact", "poisson_vis_fact",
     "ins_2d_proj_rhs", "ins_2d_proj_pen", "ins_proj_cg_2d", "ins_proj_setup_0", "ins_proj_setup_1",
+    "ins_pressure_rhs_2d", "mp_ins_pr_bc_dpdn_factors", "mp_ins_pr_div_factor",
 ]
 
 

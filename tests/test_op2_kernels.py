@@ -28,13 +28,18 @@ BFACE = {"fvmf_3d_calc_tau_bfaces", "fvmf_2d_calc_tau_bfaces", "vmf_calc_tau_bfa
          "vmf_2d_mult_avg_jump", "fvmf_3d_apply_bc", "fvmf_2d_apply_bc", "vmf_3d_apply_bc", "vmf_2d_apply_bc",
          "fvmf_3d_bop_diag", "fvmf_2d_bop_diag", "fvmf_3d_bop_block_diag", "fvmf_2d_bop_block_diag"}
 SCALARS = {"alpha", "beta", "residual", "tmp_alpha_0", "tmp_alpha_1", "constant", "mmConst", "dt", "a0", "a1", "h",
-           "pen", "pen_f", "iter_g"}
+           "pen", "pen_f", "iter_g", "b0", "b1", "_div_factor", "fact0", "fact1", "art_vis"}
+# per cell face-node data (DG_NUM_FACES x DG_NPF)
+FACE_DATS = {"dPdN", "dPdN_old", "dPdNOld"}
 # kernels whose `factor` is a scalar
 SCALAR_FACTOR = {"ins_3d_proj_pen", "ins_2d_proj_pen"}
 MATS = {"u_pre_mat", "v_pre_mat", "w_pre_mat", "op1", "op1L", "op1R"}
 # kernels every (shared) build has; the others belong to the dimension in their name
 SHARED = {"constant_mult", "copy_dg_np", "copy_dg_np_mat", "reciprocal", "zero_npf_3", "poisson_pr_fact",
-          "poisson_vis_fact", "vmf_calc_tau_faces", "vmf_calc_tau_bfaces", "ins_proj_setup_0", "ins_proj_setup_1"}
+          "poisson_vis_fact", "vmf_calc_tau_faces", "vmf_calc_tau_bfaces", "ins_proj_setup_0", "ins_proj_setup_1",
+          "mp_ins_pr_bc_dpdn_factors", "mp_ins_pr_div_factor"}
+# kernels provided per build (the shared ones in both)
+PER_BUILD = {2: 48, 3: 50}
 
 
 def split_args(s):
@@ -77,7 +82,7 @@ def ref_signature(dim, order, name):
 def kernel_dim(name):
     if name in SHARED:
         return None
-    return 3 if name.startswith(("fvmf_3d", "vmf_3d", "cg3_", "ins_3d_")) else 2
+    return 3 if name.startswith(("fvmf_3d", "vmf_3d", "cg3_", "ins_3d_", "mp_ins_3d_")) else 2
 
 
 def ref_names(dim):
@@ -165,7 +170,7 @@ def make_args(name, args, t, rng, bc_mode=None):
                 n = 2 if name in PAIR else 1 if name in BFACE else Nf
             elif an == "tau":
                 n = Nf
-            elif "jump" in an or "avg" in an or (name == "zero_npf_3"):
+            elif "jump" in an or "avg" in an or (name == "zero_npf_3") or an in FACE_DATS:
                 n = Nf * Nfp
             elif an.endswith("_bc"):
                 n = Nfp
@@ -202,7 +207,7 @@ def test_every_provided_kernel_has_the_reference_argument_list(libs):
                 continue
             assert ours[name][1] == ref_signature(dim, 3, name), name
             checked += 1
-    assert checked == 90  # 45 kernels of each build, the shared ones counted in both
+    assert checked == PER_BUILD[2] + PER_BUILD[3]  # the shared ones counted in both builds
 
 
 @pytest.mark.parametrize("dim,order", [(2, 1), (2, 2), (2, 3), (2, 4), (3, 1), (3, 2), (3, 3), (3, 4)])
@@ -211,7 +216,7 @@ def test_kernels_match_the_reference_kernels(libs, dim, order):
     t, om = table_mesh(dim, order)
     rng = np.random.default_rng(100 * dim + order)
     names = [n for n in ref_names(dim) if n in ours]
-    assert len(names) == 45
+    assert len(names) == PER_BUILD[dim]
     for name in names:
         for trial in range(6):
             # Dirichlet, Neumann and slip on every component, then random mixes
