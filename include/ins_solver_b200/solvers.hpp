@@ -511,6 +511,19 @@ class VelocityProjection {
     if (mean_iters) *mean_iters = st[0] > 0 ? st[2] / st[0] : 0.0;
     return (int)st[1];
   }
+  // Right-hand side of the pressure solve (INSSolver3D::pressure,
+  // src/solvers/3d/ins_solver.cpp:313-322): rhs = J M (-div_c(velT) / dt +
+  // LIFT (b0 dPdN + b1 dPdN_old)), dPdN_old updated in place; dPdN / dPdN_old
+  // are the cells x (dim + 1) * Nfp face dats (data == nullptr: zero, not written).
+  void pressure_rhs(double dt, double b0, double b1, const Dat* velT, Dat dPdN, Dat dPdN_old, Dat rhs) {
+    const int dim = mesh_->dim();
+    const size_t n = velT[0].size();
+    in_v_.resize(dim * n);
+    for (int c = 0; c < dim; ++c) std::copy(velT[c].data, velT[c].data + n, in_v_.begin() + c * n);
+    check(sipg_pressure_rhs_host(mesh_->handle(), order_, dt, b0, b1, in_v_.data(), dPdN.data, dPdN_old.data,
+                                 rhs.data),
+          "pressure_rhs");
+  }
   // The pressure step from the pressure itself: grad_with_central_flux(pr),
   // update_pressure_gradient (/ rho; rho.data == nullptr for the single-phase
   // solver) and project_velocity (src/solvers/3d/mp_ins_solver.cpp:653-659,

@@ -163,6 +163,22 @@ int main() {
     for (int c = 0; c < 3; ++c) err3 = std::max(err3, rel_diff(o2[c], o[c], false));
     std::printf("pressure projection converged=%d/%d vs zero-gradient projection err=%.3e\n", conv3, k, err3);
     failures += !(conv3 == k && err3 < 1e-12);
+    // pressure right-hand side: a velocity constant over the whole mesh has no
+    // divergence, so with Neumann data only the rhs is J EMAT (b0 dPdN + b1 dPdN_old),
+    // and the data are updated in place
+    const int nfn = 4 * 10;  // faces x face nodes at p = 3
+    std::vector<double> cu[3], dn((size_t)k * nfn), dold((size_t)k * nfn, 0.0), r1(N), r2(N);
+    for (int c = 0; c < 3; ++c) cu[c].assign(N, 0.25 * (c + 1));
+    for (auto& v : dn) v = U(rng);
+    Dat cud[3] = {D(cu[0]), D(cu[1]), D(cu[2])};
+    proj.pressure_rhs(1e-2, 1.0, 0.0, cud, Dat{dn.data(), k, nfn}, Dat{dold.data(), k, nfn}, D(r1));
+    double upd = 0;
+    for (size_t i = 0; i < dn.size(); ++i) upd = std::max(upd, std::fabs(dold[i] - dn[i]));
+    for (int c = 0; c < 3; ++c) std::fill(cu[c].begin(), cu[c].end(), 0.0);
+    proj.pressure_rhs(1e-2, 0.0, 1.0, cud, Dat{nullptr, k, nfn}, Dat{dold.data(), k, nfn}, D(r2));
+    const double err4 = rel_diff(r1, r2, false);
+    std::printf("pressure rhs: dPdN update err=%.3e, constant velocity adds nothing err=%.3e\n", upd, err4);
+    failures += !(upd == 0.0 && err4 < 1e-8);  // round-off of D 1 = 0 in the volume term
   }
   std::printf("%s\n", failures ? "FAILED" : "OK");
   return failures ? 1 : 0;
