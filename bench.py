@@ -690,12 +690,36 @@ def run_profile(args):
            3 applies after set-up; with -k regex:"sipg_(trace|apply_tc)" -s 2 -c 2
            ncu captures the second apply's two kernels.
     projection: the velocity projection workload at --n (3 launches of k_proj_cg).
+    pressure: the pressure step kernels at --n: sipg_pressure_rhs and
+           sipg_pressure_projection alternately, 3 launches each.
     solve: the headline mixed solve: one warm-up solve, then the captured solve;
            prints the number of kernels launched before it (ncu -s) and in it (-c).
            The outer iterations replay one host-launched graph each (graphs = 1):
            the kernels of the device-resident loop, which the profiler then sees
            as ordinary graph launches.
     """
+    if args.profile == "pressure":
+        mesh, velT, dp = projection_inputs(args.n)
+        K, Np = mesh.K, velT.shape[2]
+        Nfp = sipg.ref_sizes(3, PROJ_ORDER)[1]
+        rng = np.random.default_rng(6)
+        d_v, d_o = sipg.DeviceVector(velT), sipg.DeviceVector(np.zeros_like(velT))
+        d_pr = sipg.DeviceVector(rng.uniform(-1, 1, (K, Np)))
+        d_rho = sipg.DeviceVector(rng.uniform(1.0, 1000.0, (K, Np)))
+        d_dn = sipg.DeviceVector(rng.uniform(-1, 1, (K, 4, Nfp)))
+        d_do = sipg.DeviceVector(np.zeros((K, 4, Nfp)))
+        d_rhs = sipg.DeviceVector(np.zeros((K, Np)))
+        lib = sipg.lib()
+        for _ in range(3):  # k_pr_rhs and k_proj_cg<3,3,true> alternate
+            sipg.check(lib.sipg_pressure_rhs(mesh.h, PROJ_ORDER, C.c_double(PROJ_DT), C.c_double(2.0),
+                                             C.c_double(-1.0), C.c_void_p(d_v.ptr), C.c_void_p(d_dn.ptr),
+                                             C.c_void_p(d_do.ptr), C.c_void_p(d_rhs.ptr), C.c_void_p(0)))
+            sipg.check(lib.sipg_pressure_projection(mesh.h, PROJ_ORDER, C.c_double(PROJ_DT), C.c_double(PROJ_DT),
+                                                    C.c_void_p(d_pr.ptr), C.c_void_p(d_rho.ptr), C.c_void_p(d_v.ptr),
+                                                    C.c_void_p(d_o.ptr), C.c_void_p(0), C.c_void_p(0)))
+        sipg.check(lib.sipg_device_synchronize())
+        print("done", K)
+        return
     if args.profile == "projection":
         mesh, velT, dp = projection_inputs(args.n)
         d_dp, d_v, d_o = sipg.DeviceVector(dp), sipg.DeviceVector(velT), sipg.DeviceVector(np.zeros_like(velT))
@@ -738,7 +762,7 @@ def run_profile(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--profile", choices=["apply", "solve", "projection"], default=None,
+    ap.add_argument("--profile", choices=["apply", "solve", "projection", "pressure"], default=None,
                     help="run a small fixed workload for an ncu capture instead of the benchmark")
     ap.add_argument("--n", type=int, default=N_HEAD)
     ap.add_argument("--order", type=int, default=ORDER)
