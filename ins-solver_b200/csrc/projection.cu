@@ -722,17 +722,31 @@ const double* proj_h_device(sipg_mesh* m) {
   return m->proj_h.as<double>();
 }
 
+// Opt the kernel into its dynamic shared memory and return its resident CTAs per
+// SM, once per (kernel, device): the attribute belongs to the current device.
+template <typename Kern>
+int kernel_setup(Kern kern, size_t smem) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, int> per_sm;  // (kernel, device)
+  int dev = 0;
+  SIPG_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  int& n = per_sm[{reinterpret_cast<const void*>(kern), dev}];
+  if (!n) {
+    SIPG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int b = 0;
+    SIPG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, kProjWarps * 32, smem));
+    n = std::max(b, 1);
+  }
+  return n;
+}
+
 template <int D, int P, bool GRAD>
 void launch_proj(const ProjArgs& a, cudaStream_t s) {
   constexpr size_t smem = proj_smem_doubles<D, P>() * sizeof(double);
   static_assert(smem <= 227 * 1024, "projection shared memory");
   auto kern = k_proj_cg<D, P, GRAD>;
-  static const int per_sm = [&] {  // once per instantiation
-    SIPG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int n = 0;
-    SIPG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, kProjWarps * 32, smem));
-    return std::max(n, 1);
-  }();
+  const int per_sm = kernel_setup(kern, smem);
   const int epc = kProjWarps * proj_epw(D, P);  // elements per CTA round
   const int need = (a.K + epc - 1) / epc;
   const int grid = std::max(1, std::min(need, per_sm * num_sms()));
@@ -828,12 +842,7 @@ void launch_pr_rhs(const PrRhsArgs& a, cudaStream_t s) {
   constexpr size_t smem = pr_rhs_smem_doubles<D, P>() * sizeof(double);
   static_assert(smem <= 227 * 1024, "pressure rhs shared memory");
   auto kern = k_pr_rhs<D, P>;
-  static const int per_sm = [&] {
-    SIPG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int nb = 0;
-    SIPG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, kProjWarps * 32, smem));
-    return std::max(nb, 1);
-  }();
+  const int per_sm = kernel_setup(kern, smem);
   const int need = (a.K + kProjWarps - 1) / kProjWarps;
   const int grid = std::max(1, std::min(need, per_sm * num_sms()));
   kern<<<grid, kProjWarps * 32, smem, s>>>(a);
