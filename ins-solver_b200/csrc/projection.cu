@@ -319,6 +319,7 @@ __global__ void __launch_bounds__(kProjWarps * 32) k_proj_cg(const ProjArgs a) {
     if (GRAD) {
       const int8_t* fmask = a.itab;
       const int8_t* npos = a.itab + NF * NFP;
+      __syncwarp();  // the previous element's last reads of sB are done
 #pragma unroll
       for (int e = 0; e < E; ++e)
 #pragma unroll
