@@ -517,7 +517,7 @@ __global__ void __launch_bounds__(kProjWarps * 32) k_proj_cg(const ProjArgs a) {
 }
 
 
-// Right-hand side of the pressure solve, one warp per element:
+// Right-hand side of the pressure solve, two elements per warp (one at p = 4 in 3D):
 //   rhs = J M ( -(div_c velT) / dt + LIFT dPdN_new ),  dPdN_new = b0 dPdN + b1 dPdN_old,
 // div_c the central-flux divergence (volume sum_k D_k (G u)_k plus LIFT of
 // fscale n . (u+ - u-) / 2 on interior faces); dPdN_old <- dPdN_new.
@@ -539,16 +539,17 @@ template <int D, int P>
 __global__ void __launch_bounds__(kProjWarps * 32) k_pr_rhs(const PrRhsArgs a) {
   constexpr int NP = proj_np(D, P), NPE = proj_npe(D, P), NPL = (NP + 31) / 32, NG = D == 3 ? 10 : 5;
   constexpr int NF = D + 1, NFP = proj_nfp(D, P), NFPE = proj_nfpe(D, P), MAT = proj_mat_doubles<D, P>();
-  constexpr int WB = (D + 1) * NPE + 2 * NF * NFPE;
+  constexpr int E = proj_epw(D, P);  // elements per warp: each matrix read serves all of them
+  constexpr int WB = E * ((D + 1) * NPE + 2 * NF * NFPE);
   extern __shared__ double sm[];
   const double* sD = sm;
   const double* sM = sm + 2 * D * MAT;
   const double* sL = sm + proj_nmat(D) * MAT;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double* sGU = sm + proj_blob_doubles<D, P>() + warp * WB;  // [D][NPE]
-  double* sPre = sGU + D * NPE;                              // [NPE]
-  double* sF1 = sPre + NPE;                                  // [NF][NFPE] n . (u+ - u-) / 2 fscale
-  double* sF2 = sF1 + NF * NFPE;                             // [NF][NFPE] dPdN_new
+  double* sGU = sm + proj_blob_doubles<D, P>() + warp * WB;  // [E][D][NPE]
+  double* sPre = sGU + E * D * NPE;                          // [E][NPE]
+  double* sF1 = sPre + E * NPE;                              // [E][NF][NFPE] fscale n . (u+ - u-) / 2
+  double* sF2 = sF1 + E * NF * NFPE;                         // [E][NF][NFPE] dPdN_new
   for (int i = threadIdx.x; i < proj_blob_doubles<D, P>(); i += blockDim.x) sm[i] = a.mats[i];
   for (int i = lane; i < WB; i += 32) sGU[i] = 0.0;
   __syncthreads();
@@ -556,81 +557,104 @@ __global__ void __launch_bounds__(kProjWarps * 32) k_pr_rhs(const PrRhsArgs a) {
   const int8_t* fmask = a.itab;
   const int8_t* npos = a.itab + NF * NFP;
   const double inv_dt = 1.0 / a.dt;
-  for (int e = blockIdx.x * kProjWarps + warp; e < a.K; e += gridDim.x * kProjWarps) {
-    double G[3][3] = {};
-    const double* g = a.geof + (size_t)e * NG;
-    double J;
-    if (D == 3) {
+  for (int e0 = (blockIdx.x * kProjWarps + warp) * E; e0 < a.K; e0 += gridDim.x * kProjWarps * E) {
+    double G[E][3][3], J[E];
+    bool valid[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      valid[e] = e0 + e < a.K;
+      const double* g = a.geof + (size_t)(valid[e] ? e0 + e : e0) * NG;
 #pragma unroll
       for (int k = 0; k < 3; ++k)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) G[k][c] = __ldg(g + k * 3 + c);
-      J = __ldg(g + 9);
-    } else {
-      G[0][0] = __ldg(g + 0); G[0][1] = __ldg(g + 1);
-      G[1][0] = __ldg(g + 2); G[1][1] = __ldg(g + 3);
-      J = __ldg(g + 4);
+        for (int c = 0; c < 3; ++c) G[e][k][c] = 0.0;
+      if (D == 3) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) G[e][k][c] = __ldg(g + k * 3 + c);
+        J[e] = __ldg(g + 9);
+      } else {
+        G[e][0][0] = __ldg(g + 0); G[e][0][1] = __ldg(g + 1);
+        G[e][1][0] = __ldg(g + 2); G[e][1][1] = __ldg(g + 3);
+        J[e] = __ldg(g + 4);
+      }
     }
+    __syncwarp();  // the previous elements' reads of the buffers are done
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+#pragma unroll
+      for (int u = 0; u < NPL; ++u) {
+        const int i = lane + 32 * u;
+        if (i < NP) {
+          double uc[D];
+#pragma unroll
+          for (int c = 0; c < D; ++c) uc[c] = valid[e] ? __ldg(a.velT + c * n + (size_t)(e0 + e) * NP + i) : 0.0;
+#pragma unroll
+          for (int k = 0; k < D; ++k) {
+            double s = 0.0;
+#pragma unroll
+            for (int c = 0; c < D; ++c) s += G[e][k][c] * uc[c];
+            sGU[(e * D + k) * NPE + i] = s;
+          }
+        }
+      }
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+      for (int m = lane; m < NF * NFP; m += 32) {
+        const int f = m / NFP, k = m - f * NFP;
+        double un = 0.0, dn = 0.0;
+        if (valid[e]) {
+          const int el = e0 + e;
+          const int nb = __ldg(a.nbr + (size_t)el * NF + f);
+          if (nb >= 0) {
+            const int code = (__ldg(a.fcode + el) >> (8 * f)) & 0xff;
+            const int fr = code & 3, sg = code >> 2;
+            const int nn = fmask[fr * NFP + npos[sg * NFP + k]], o = fmask[f * NFP + k];
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+              double v;  // fscale n_d of face f (the unnormalised outward normal)
+              if (D == 3)
+                v = f == 0 ? -G[e][2][d] : f == 1 ? -G[e][1][d] : f == 2 ? (G[e][0][d] + G[e][1][d]) + G[e][2][d]
+                                                                           : -G[e][0][d];
+              else
+                v = f == 0 ? -G[e][1][d] : f == 1 ? G[e][0][d] + G[e][1][d] : -G[e][0][d];
+              un += v * (0.5 * (__ldg(a.velT + d * n + (size_t)nb * NP + nn) -
+                                __ldg(a.velT + d * n + (size_t)el * NP + o)));
+            }
+          }
+          const size_t fi = (size_t)el * NF * NFP + m;
+          dn = (a.dPdN ? a.b0 * a.dPdN[fi] : 0.0) + (a.dPdN_old ? a.b1 * a.dPdN_old[fi] : 0.0);
+          if (a.dPdN_old) a.dPdN_old[fi] = dn;
+        }
+        sF1[(e * NF + f) * NFPE + k] = un;
+        sF2[(e * NF + f) * NFPE + k] = dn;
+      }
     __syncwarp();
 #pragma unroll
     for (int u = 0; u < NPL; ++u) {
       const int i = lane + 32 * u;
       if (i < NP) {
-        double uc[D];
+        double vol[E], l1[E], l2[E], y[E];
 #pragma unroll
-        for (int c = 0; c < D; ++c) uc[c] = __ldg(a.velT + c * n + (size_t)e * NP + i);
-#pragma unroll
-        for (int k = 0; k < D; ++k) {
-          double s = 0.0;
-#pragma unroll
-          for (int c = 0; c < D; ++c) s += G[k][c] * uc[c];
-          sGU[k * NPE + i] = s;
-        }
-      }
-    }
-    for (int m = lane; m < NF * NFP; m += 32) {
-      const int f = m / NFP, k = m - f * NFP;
-      double un = 0.0;
-      const int nb = __ldg(a.nbr + (size_t)e * NF + f);
-      if (nb >= 0) {
-        const int code = (__ldg(a.fcode + e) >> (8 * f)) & 0xff;
-        const int fr = code & 3, sg = code >> 2;
-        const int nn = fmask[fr * NFP + npos[sg * NFP + k]], o = fmask[f * NFP + k];
-#pragma unroll
-        for (int d = 0; d < D; ++d) {
-          double v;  // fscale n_d of face f (the unnormalised outward normal)
-          if (D == 3) v = f == 0 ? -G[2][d] : f == 1 ? -G[1][d] : f == 2 ? (G[0][d] + G[1][d]) + G[2][d] : -G[0][d];
-          else v = f == 0 ? -G[1][d] : f == 1 ? G[0][d] + G[1][d] : -G[0][d];
-          un += v * (0.5 * (__ldg(a.velT + d * n + (size_t)nb * NP + nn) - __ldg(a.velT + d * n + (size_t)e * NP + o)));
-        }
-      }
-      const size_t fi = (size_t)e * NF * NFP + m;
-      const double dn = (a.dPdN ? a.b0 * a.dPdN[fi] : 0.0) + (a.dPdN_old ? a.b1 * a.dPdN_old[fi] : 0.0);
-      if (a.dPdN_old) a.dPdN_old[fi] = dn;
-      sF1[f * NFPE + k] = un;
-      sF2[f * NFPE + k] = dn;
-    }
-    __syncwarp();
-#pragma unroll
-    for (int u = 0; u < NPL; ++u) {
-      const int i = lane + 32 * u;
-      if (i < NP) {
-        double vol = 0.0, l1 = 0.0, l2 = 0.0;
+        for (int e = 0; e < E; ++e) vol[e] = l1[e] = l2[e] = 0.0;
 #pragma unroll
         for (int k = 0; k < D; ++k) {
-          double y[1];
-          mat_vec<NP, NPE, 1>(sD + k * MAT, sGU + k * NPE, 0, i, y);
-          vol += y[0];
+          mat_vec<NP, NPE, E>(sD + k * MAT, sGU + k * NPE, D * NPE, i, y);
+#pragma unroll
+          for (int e = 0; e < E; ++e) vol[e] += y[e];
         }
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
-          double y[1];
-          mat_vec<NP, NFPE, 1>(sL + f * NP * NFPE, sF1 + f * NFPE, 0, i, y);
-          l1 += y[0];
-          mat_vec<NP, NFPE, 1>(sL + f * NP * NFPE, sF2 + f * NFPE, 0, i, y);
-          l2 += y[0];
+          mat_vec<NP, NFPE, E>(sL + f * NP * NFPE, sF1 + f * NFPE, NF * NFPE, i, y);
+#pragma unroll
+          for (int e = 0; e < E; ++e) l1[e] += y[e];
+          mat_vec<NP, NFPE, E>(sL + f * NP * NFPE, sF2 + f * NFPE, NF * NFPE, i, y);
+#pragma unroll
+          for (int e = 0; e < E; ++e) l2[e] += y[e];
         }
-        sPre[i] = -(vol + l1) * inv_dt + l2;
+#pragma unroll
+        for (int e = 0; e < E; ++e) sPre[e * NPE + i] = -(vol[e] + l1[e]) * inv_dt + l2[e];
       }
     }
     __syncwarp();
@@ -638,9 +662,11 @@ __global__ void __launch_bounds__(kProjWarps * 32) k_pr_rhs(const PrRhsArgs a) {
     for (int u = 0; u < NPL; ++u) {
       const int i = lane + 32 * u;
       if (i < NP) {
-        double y[1];
-        mat_vec<NP, NPE, 1>(sM, sPre, 0, i, y);
-        a.rhs[(size_t)e * NP + i] = J * y[0];
+        double y[E];
+        mat_vec<NP, NPE, E>(sM, sPre, NPE, i, y);
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+          if (valid[e]) a.rhs[(size_t)(e0 + e) * NP + i] = J[e] * y[e];
       }
     }
   }
@@ -649,7 +675,7 @@ __global__ void __launch_bounds__(kProjWarps * 32) k_pr_rhs(const PrRhsArgs a) {
 template <int D, int P>
 __host__ __device__ constexpr int pr_rhs_smem_doubles() {
   return proj_blob_doubles<D, P>() +
-         kProjWarps * ((D + 1) * proj_npe(D, P) + 2 * (D + 1) * proj_nfpe(D, P));
+         kProjWarps * proj_epw(D, P) * ((D + 1) * proj_npe(D, P) + 2 * (D + 1) * proj_nfpe(D, P));
 }
 
 // Reference-element matrices in the kernel's layouts, per (device, dim, order).
@@ -844,7 +870,8 @@ void launch_pr_rhs(const PrRhsArgs& a, cudaStream_t s) {
   static_assert(smem <= 227 * 1024, "pressure rhs shared memory");
   auto kern = k_pr_rhs<D, P>;
   const int per_sm = kernel_setup(kern, smem);
-  const int need = (a.K + kProjWarps - 1) / kProjWarps;
+  const int epc = kProjWarps * proj_epw(D, P);  // elements per CTA round
+  const int need = (a.K + epc - 1) / epc;
   const int grid = std::max(1, std::min(need, per_sm * num_sms()));
   kern<<<grid, kProjWarps * 32, smem, s>>>(a);
   SIPG_CUDA(cudaGetLastError());
