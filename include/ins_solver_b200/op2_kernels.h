@@ -1179,6 +1179,7 @@ template <int ORDER>
 SIPG_OP2_HD void ins_3d_proj_pen(const double *factor, const double *a0, const double *a1, const double *geof,
                                  const double *u0, const double *v0, const double *w0, const double *u1,
                                  const double *v1, const double *w1, const double *h, double *pen, double *pen_f) {
+  (void)a0, (void)a1, (void)geof, (void)u0, (void)v0, (void)w0, (void)u1, (void)v1, (void)w1;
   *pen = *factor * (*h / ((double)ORDER + 1.0));
   *pen_f = *factor;
 }
@@ -1187,6 +1188,7 @@ template <int ORDER>
 SIPG_OP2_HD void ins_2d_proj_pen(const double *factor, const double *a0, const double *a1, const double *geof,
                                  const double *u0, const double *v0, const double *u1, const double *v1,
                                  const double *h, double *pen, double *pen_f) {
+  (void)a0, (void)a1, (void)geof, (void)u0, (void)v0, (void)u1, (void)v1;
   *pen = *factor * (*h / ((double)ORDER + 1.0));
   *pen_f = *factor;
 }
@@ -1388,6 +1390,7 @@ template <int ORDER>
 SIPG_OP2_HD void mp_ins_3d_vis_0(const double *fact0, const double *fact1, const double *rho, double *mu,
                                  const double *art_vis, const double *u, const double *v, const double *w,
                                  double *rhs0, double *rhs1, double *rhs2, double *mm_factor) {
+  (void)mu, (void)art_vis;
   for (int i = 0; i < Dg<3, ORDER>::NP; ++i) {
     rhs0[i] = u[i] * *fact0 * rho[i];
     rhs1[i] = v[i] * *fact0 * rho[i];
