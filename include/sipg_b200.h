@@ -115,8 +115,12 @@ int sipg_op_apply_host(sipg_op *op, const double *x, double *y);
  * for callers that cannot allocate device memory at apply time. The first call
  * on each device (current device) does a one-time set-up, a symbol-address
  * lookup; make it before any stream capture. Operators whose scratch would
- * exceed the limit (K * (dim+1) face records of 2 * Nfp values, padded to
- * 16-byte multiples; at p = 3 in 3D: 209,715 elements FP32, 104,857 FP64) get SIPG_INVALID_ARG. There is one scratch per
+ * exceed the limit get SIPG_INVALID_ARG; the scratch holds
+ * K * (dim+1) * roundup(2 * roundup(Nfp, 2), 4) values of the precision's size
+ * (at p = 3 in 3D: 209,715 elements FP32, 104,857 FP64). With lazy module
+ * loading (the CUDA default) the array takes device memory from the first use
+ * of the library's kernels in a context; with CUDA_MODULE_LOADING=EAGER every
+ * context that loads the library reserves it at start-up. There is one scratch per
  * device: calls that overlap in time on one device race on it, so order them
  * on one stream or synchronise between them. Nothing in it needs to start at
  * zero. */

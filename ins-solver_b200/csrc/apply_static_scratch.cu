@@ -13,7 +13,9 @@
 // This entry point runs the same two kernels with the trace scratch in a
 // fixed-size array compiled into the library as a __device__ variable, so the
 // call allocates nothing. Its price is a fixed kScratchBytes of device memory
-// per device once the array is first used, and one scratch per device: two
+// per device (reserved when the library's module is loaded in a context: at the
+// first use of its kernels under lazy module loading, the CUDA default, or at
+// context creation under CUDA_MODULE_LOADING=EAGER), and one scratch per device: two
 // calls that overlap in time on the same device (different streams, different
 // host threads without ordering) race on it and give wrong results.
 #include <cuda_runtime.h>

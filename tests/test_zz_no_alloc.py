@@ -53,7 +53,11 @@ def test_static_scratch_apply_matches_apply_twice(dim, n, order, precision):
 
 def test_static_scratch_apply_allocates_no_device_memory():
     import torch
-    dim, n, order = 3, 5, 3
+    # 10^3 x 6 = 6,000 tets at p = 3: sipg_op_apply would allocate 3.84 MB (FP64) and
+    # 1.92 MB (FP32) of traces, above the 2 MiB granularity of device allocations,
+    # so a trace allocation shows up in the device's free memory.
+    dim, n, order = 3, 10, 3
+    trace_bytes = 6000 * 4 * 20 * (8 + 4)
     # warm-up on one operator: the one-time set-up and the first launch of each kernel
     mesh, t, e, om, x, f, m, bct = random_case(dim, n, order, 1, seed=5)
     warm = make_op(mesh, order, 1, f, None, bct=bct)
@@ -61,22 +65,29 @@ def test_static_scratch_apply_allocates_no_device_memory():
         xd = DevArray(x.astype(dtype_of(prec)))
         yd = DevArray(np.zeros_like(x, dtype=dtype_of(prec)))
         assert static_apply(warm, prec, xd, yd) == sipg.SIPG_OK
-    # a second operator that has never been applied: sipg_op_apply would allocate its traces
-    fresh = make_op(mesh, order, 1, f, None, bct=bct)
     bufs = {p: (DevArray(x.astype(dtype_of(p))), DevArray(np.zeros_like(x, dtype=dtype_of(p))))
             for p in (sipg.FP64, sipg.FP32)}
-    sipg.check(sipg.lib().sipg_device_synchronize())
-    free0 = torch.cuda.mem_get_info()[0]
-    outs = {}
-    for prec, (xd, yd) in bufs.items():
-        for _ in range(2):
-            assert static_apply(fresh, prec, xd, yd) == sipg.SIPG_OK
-        outs[prec] = yd.get().astype(np.float64)
-    sipg.check(sipg.lib().sipg_device_synchronize())
-    free1 = torch.cuda.mem_get_info()[0]
-    assert free1 == free0
-    for prec, tol in ((sipg.FP64, TOL_FP64), (sipg.FP32, TOL_FP32)):
-        assert rel_err(outs[prec], reference_apply(fresh, prec, x)) < tol
+    # The free-memory figure is device-wide, so an unrelated allocation in between
+    # (another process, an allocator growing its cache) can lower it: measure on a
+    # fresh, never-applied operator up to three times and accept any attempt in
+    # which free memory dropped by less than half the traces sipg_op_apply would take.
+    drops = []
+    for attempt in range(3):
+        fresh = make_op(mesh, order, 1, f, None, bct=bct)
+        sipg.check(sipg.lib().sipg_device_synchronize())
+        free0 = torch.cuda.mem_get_info()[0]
+        outs = {}
+        for prec, (xd, yd) in bufs.items():
+            for _ in range(2):
+                assert static_apply(fresh, prec, xd, yd) == sipg.SIPG_OK
+            outs[prec] = yd.get().astype(np.float64)
+        sipg.check(sipg.lib().sipg_device_synchronize())
+        drops.append(free0 - torch.cuda.mem_get_info()[0])
+        for prec, tol in ((sipg.FP64, TOL_FP64), (sipg.FP32, TOL_FP32)):
+            assert rel_err(outs[prec], reference_apply(fresh, prec, x)) < tol
+        if drops[-1] < trace_bytes // 2:
+            break
+    assert min(drops) < trace_bytes // 2, f"free device memory dropped by {drops} bytes"
 
 
 def test_static_scratch_rejects_operators_beyond_its_size():
