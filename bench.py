@@ -22,10 +22,16 @@ The operator setup (diagonals, eigenvalue estimates, coarse operators) runs once
 before timing; the coefficient does not change between steps and its setup time
 is reported separately.
 
---impl reference: the reference's own kernels (src/kernels/fvmf_3d_*.h of
-TobyFlynn/INS-Solver, compiled under oracle/_ref with OpenMP on all host cores)
-execute one outer iteration's worth of applies per step on the same mesh; solves/s
-= 1 / (step time x outer iterations of the FP64 path).
+--impl reference: one complete FP64 solve of the same workload on the host
+cores, every operator apply done by the reference's own kernels
+(src/kernels/fvmf_3d_*.h of TobyFlynn/INS-Solver compiled under oracle/_ref,
+OpenMP on all host cores) inside the oracle's p-multigrid FPCG (the reference's
+PETScPMultigrid is not vendored), timed end to end (set-up, coarse levels and
+vector updates included); solves/s = 1 / that time. Its inputs (mesh,
+reference element, workload, coarse hierarchy) come from oracle/ alone: that
+process never loads the CUDA library. Beside it: the 2D configuration solved
+with the reference's own block-Jacobi CG kernels on 1 core and on all cores,
+and the 48^3 x 6 p = 4 Helmholtz apply through the reference's kernels.
 """
 import argparse
 import ctypes as C
@@ -42,8 +48,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 for sub in ("ins-solver_b200", "oracle"):
     sys.path.insert(0, os.path.join(ROOT, sub))
 
-import sipg  # noqa: E402
-import workloads as W  # noqa: E402
+# The library binding (sipg, workloads) is imported by main() for this
+# repository's arm only: the reference arm runs without the CUDA library.
+sipg = W = None
+C2_FIXTURE = os.path.join(ROOT, "tests", "golden", "c2", "c2_oracle_solution.npz")
 
 METRIC = "SIPG apply GDOF/s; Poisson solves/s + p50/p99 latency, mixed vs FP64 @1e-8"
 N_HEAD = 24
@@ -115,6 +123,13 @@ def launches():
     n = C.c_ulonglong()
     sipg.check(sipg.lib().sipg_launch_count(C.byref(n)))
     return n.value
+
+
+def headline_config(K=82944, world=1):
+    return {"workload": "3D two-phase Poisson 24^3x6=82944 tets p=3, Neumann walls + nullspace projection, "
+                        "p-MG 3-2-1 Chebyshev(4), FPCG rel 1e-8",
+            "K": K, "dofs": K * 20, "parallelism": f"replicas{world}",
+            "l2_flush": "inputs larger than L2 across a solve (26 MB/vector, ~30 vectors live)"}
 
 
 def build_headline():
@@ -247,6 +262,7 @@ def run_ours(args):
     s64, setup64 = pmg_solver(op, sipg.FP64)
     # plain FP64 path (fewer steps; it is the slow one)
     ms64, inf64 = time_solves(s64, bd, xd, max(1, min(3, args.steps)), 1)
+    err64 = fixture_error(xd.cpu().numpy())
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
@@ -254,6 +270,7 @@ def run_ours(args):
     with ClockSampler(local) as clk:
         ms32, inf32 = time_solves(s32, bd, xd, args.steps, args.warmup)
     l1 = launches()
+    err32 = fixture_error(xd.cpu().numpy())
     n_launch = (l1 - l0) * args.steps // (args.steps + args.warmup)
     step_ms = float(np.mean(ms32))
     total_ms = float(np.sum(ms32))
@@ -277,6 +294,18 @@ def run_ours(args):
             sipg.check(st)
     e2e_ms = max_over_ranks(float(np.sum(e2e_t)) * 1e3, world, "cuda")
     e2e_val = replica_throughput(len(e2e_t), world, e2e_ms)
+    # one time step of an INS loop: the density (factor) changes, the operator and
+    # the V-cycle are set up again, then the solve (the reference re-sets the factor
+    # and the matrices before every pressure solve, mp_ins_solver.cpp:513-522, 616-632)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    op.set_factor(c["factor"])
+    s32.setup()
+    torch.cuda.synchronize()
+    resetup_ms = (time.perf_counter() - t0) * 1e3
+    xd.zero_()
+    torch.cuda.synchronize()
+    first_ms = s32.solve_device(bd.data_ptr(), xd.data_ptr()).solve_ms
     # dominant kernel: FP32 p=3 apply of the V-cycle (and the FP64 outer apply)
     a32 = time_apply(op, sipg.FP32, K, Np)
     a64 = time_apply(op, sipg.FP64, K, Np)
@@ -313,10 +342,7 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "fp32 V-cycle / fp64 outer CG",
         "data": "synthetic (seeded two-phase density and Gaussian random field RHS)",
-        "config": {"workload": "3D two-phase Poisson 24^3x6=82944 tets p=3, Neumann walls + nullspace projection, "
-                               "p-MG 3-2-1 Chebyshev(4), FPCG rel 1e-8",
-                   "K": K, "dofs": n, "parallelism": f"replicas{world}",
-                   "l2_flush": "inputs larger than L2 across a solve (26 MB/vector, ~30 vectors live)"},
+        "config": headline_config(K, world),
         "iters": int(inf32[-1].iters),
         "true_rel_res": float(inf32[-1].true_rel_res),
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
@@ -324,6 +350,10 @@ def run_ours(args):
                       "iters": int(inf64[-1].iters), "true_rel_res": float(inf64[-1].true_rel_res)},
         "mixed_vs_fp64_speedup": float(np.mean(ms64)) / step_ms,
         "setup_ms": {"mixed": setup32, "fp64": setup64},
+        "per_time_step": {"set_factor_and_setup_ms": resetup_ms, "first_solve_ms": first_ms,
+                          "total_ms": resetup_ms + first_ms,
+                          "what": "new factor, V-cycle set-up again, then the solve (graph re-capture included)"},
+        "error_vs_fp64_oracle": {"mixed": err32, "fp64": err64},
         "e2e": {"value": e2e_val, "unit": "solves/s", "h2d_bytes_per_step": int(2 * b.nbytes),
                 "d2h_bytes_per_step": int(b.nbytes)},
         "gpu_launches": int(n_launch),
@@ -342,7 +372,7 @@ def run_ours(args):
     if not args.skip_serving:
         out["serving"] = serving_sweep(seed=1234 + rank)
     if rank == 0 and world == 1 and not args.skip_cpu:
-        out["cpu_baseline"] = cpu_reference(c, op, int(inf64[-1].iters), sample_only=True)
+        out["cpu_baseline"] = cpu_baseline_sample(c, int(inf64[-1].iters))
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
@@ -621,37 +651,99 @@ def run_serving(seed, n_req=96, rate=400.0, slots=4):
             "speedup_vs_sequential_fp64": (n_req / served_s) / (n_req / seq_s)}
 
 
-def cpu_reference(c, op, outer_iters, sample_only=False, steps=1, warmup=0):
-    """Reference kernels on the host cores: one outer iteration of the p-MG solve =
-    1 FP64 apply at p=3 + 8 V-cycle applies (Chebyshev(4) before and after,
-    one residual) at each of p=3, 2, 1 (the algebraic coarse levels below p=1
-    are excluded), timed with the reference's own
-    kernels (oracle/_ref, OpenMP)."""
-    import oracle_py as O
+def omp_threads(n):
+    """Thread count of the CPU checkers' OpenMP loops (one libgomp instance is
+    shared by oracle/liboracle.so and oracle/_ref/libsipgref.so)."""
+    try:
+        C.CDLL("libgomp.so.1").omp_set_num_threads(int(n))
+    except (OSError, AttributeError):
+        os.environ["OMP_NUM_THREADS"] = str(n)
+
+
+def oracle_case(c):
+    """The headline workload as the oracle's p-multigrid takes it: the mesh and
+    reference element rebuilt by oracle/dg_oracle (equal to the library's, see
+    tests/test_dg_oracle.py), the coefficient and right-hand side as given."""
+    import dg_oracle as D
+    mesh = D.Mesh.box(3, N_HEAD, 0.1, 20261203)
+    t = D.ref_tables(3, ORDER)
+    return dict(mesh=mesh, export=mesh.export(ORDER, t), tables=t, factor=c["factor"], rhs=c["rhs"],
+                bc_types=c["bc_types"], pin=None)
+
+
+def cpu_baseline_sample(c, outer_iters):
+    """Bounded sample of the reference CPU path on all host cores: the set-up and
+    two outer iterations of the same FP64 p-multigrid FPCG, every operator apply
+    by the reference's own kernels (oracle/_ref); solve time = set-up + (outer
+    iterations of this run's GPU FP64 solve, the same algorithm) x the measured
+    seconds per iteration."""
+    import pmg_oracle as P
     cores = os.cpu_count() or 1
-    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    mesh = c["mesh"]
-    counts = {3: 1 + 8, 2: 8, 1: 8}
-    per = {}
-    rng = np.random.default_rng(0)
-    for p, cnt in counts.items():
-        t = sipg.ref_tables(3, p)
-        e = mesh.export(p)
-        om = O.OMesh(t, e)
-        I = sipg.interp_matrix(3, ORDER, p)
-        f = c["factor"] @ I.T
-        x = rng.uniform(-1, 1, (1, mesh.K, t["Np"]))
-        O.mult(om, x, c["bc_types"], f, use_ref=True)  # warm
-        t0 = time.perf_counter()
-        O.mult(om, x, c["bc_types"], f, use_ref=True)
-        per[p] = time.perf_counter() - t0
-    step_s = sum(per[p] * counts[p] for p in counts)
-    return {"value": 1.0 / (step_s * outer_iters), "unit": "solves/s", "cores": cores, "kind": "reference",
-            "sample": (f"one outer p-MG iteration of applies with the reference kernels (oracle/_ref, "
-                       f"OpenMP {cores} threads): per-apply s {{p3: {per[3]:.3f}, p2: {per[2]:.3f}, "
-                       f"p1: {per[1]:.3f}}} x counts {counts} = {step_s:.2f} s, scaled by {outer_iters} "
-                       f"outer iterations; vector updates excluded"),
-            "step_s": step_s}
+    omp_threads(cores)
+    case = oracle_case(c)
+    t0 = time.perf_counter()
+    _, info, _ = P.solve_poisson(case, max_iter=2, ref_applies=True)
+    wall = time.perf_counter() - t0
+    setup = wall - info.solve_s
+    est = setup + outer_iters * info.iter_s
+    return {"value": 1.0 / est, "unit": "solves/s", "cores": cores, "kind": "reference",
+            "sample": (f"set-up ({setup:.1f} s) and 2 outer FP64 p-MG FPCG iterations ({info.iter_s:.2f} s each) "
+                       f"with every apply by the reference's kernels (oracle/_ref, OpenMP {cores} threads), "
+                       f"solve = set-up + {outer_iters} iterations (this run's GPU FP64 iteration count)"),
+            "setup_s": setup, "iter_s": info.iter_s, "wall_s": wall}
+
+
+def reference_2d(threads):
+    """The 2D configuration (64^2 x 2 = 8,192 triangles, p = 3, zero Dirichlet,
+    M (8 pi^2 sin sin)) solved by the reference's own block-Jacobi CG kernels
+    (cg_*.h, the 2D ViscousSolver loop in oracle/_ref) to ||r|| <= 1e-10 ||b||."""
+    import dg_oracle as D
+    import oracle_py as O
+    omp_threads(threads)
+    mesh = D.Mesh.box(2, 64)
+    t = D.ref_tables(2, 3)
+    e = mesh.export(3, t)
+    f = 8 * np.pi ** 2 * np.sin(2 * np.pi * e["x"]) * np.sin(2 * np.pi * e["y"])
+    b = D.mass_apply(e, t, f)[None]
+    bct = np.zeros((1, e["Kb"]), np.int32)
+    om = O.OMesh(t, e)
+    t0 = time.perf_counter()
+    x, info = O.solve(om, b, bct, O.PRE_BLOCK_JACOBI, abs_tol=1e-10 * float(np.linalg.norm(b)), rel_tol=0.0,
+                      max_iter=5000, use_ref=True)
+    dt = time.perf_counter() - t0
+    exact = np.sin(2 * np.pi * e["x"]) * np.sin(2 * np.pi * e["y"])
+    return {"threads": threads, "ms_per_solve": dt * 1e3, "iters": int(info.iters),
+            "max_error_vs_exact": float(np.abs(x[0] - exact).max())}
+
+
+def reference_c3_apply(reps=2):
+    """The 48^3 x 6 p = 4 Helmholtz operator applied by the reference's kernels on
+    all host cores (a sample of `reps` applies of the 200-apply workload)."""
+    import dg_oracle as D
+    import oracle_py as O
+    omp_threads(os.cpu_count() or 1)
+    h = D.helmholtz3d(48, order=4)
+    t = D.ref_tables(3, 4)
+    om = O.OMesh(t, h["mesh"].export(4, t))
+    O.mult(om, h["x"], h["bc_types"], None, None, h["mm"], use_ref=True)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        O.mult(om, h["x"], h["bc_types"], None, None, h["mm"], use_ref=True)
+    dt = (time.perf_counter() - t0) / reps
+    return {"ms_per_apply": dt * 1e3, "gdofs": h["x"].size / dt / 1e9, "sample": f"{reps} applies after one warm-up"}
+
+
+def fixture_error(x):
+    """Relative L2 distance of a solution to the committed FP64 oracle solution
+    of the headline workload (tests/golden/c2/make_c2_oracle.py)."""
+    if not os.path.exists(C2_FIXTURE):
+        return None
+    g = np.load(C2_FIXTURE)
+    ref = g["x"].astype(np.float64).reshape(-1)
+    x = np.asarray(x, dtype=np.float64).reshape(-1)
+    return {"rel_l2": float(np.linalg.norm(x - ref) / np.linalg.norm(ref)), "oracle_iters": int(g["iters"]),
+            "oracle_rel_res": float(g["rel_res"]),
+            "fixture": "tests/golden/c2/c2_oracle_solution.npz (FP64 oracle solution stored in FP32)"}
 
 
 def run_reference(args):
@@ -662,24 +754,34 @@ def run_reference(args):
     if not O.have_ref():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libsipgref.so was not built"}))
         return
-    c = W.poisson3d_two_phase(N_HEAD, order=ORDER, n_modes=256, pin=False)
-    outer = 22  # outer iterations of the FP64 p-MG path on this workload (measured on the GPU)
-    step_times = []
-    for i in range(args.warmup + args.steps):
-        r = cpu_reference(c, None, outer)
-        if i >= args.warmup:
-            step_times.append(r["step_s"])
-    step = float(np.mean(step_times))
-    val = 1.0 / (step * outer)
+    import dg_oracle as D
+    import pmg_oracle as P
+    cores = os.cpu_count() or 1
+    omp_threads(cores)
+    case = D.poisson3d_two_phase(N_HEAD, order=ORDER, n_modes=256, pin=False)
+    # warm-up: fine-level applies through the reference's kernels (page-in, thread pool)
+    om = O.OMesh(case["tables"], case["export"])
+    for _ in range(args.warmup):
+        O.mult(om, case["rhs"], case["bc_types"], case["factor"], use_ref=True)
+    t0 = time.perf_counter()
+    x, info, _ = P.solve_poisson(case, ref_applies=True)
+    total = time.perf_counter() - t0
+    val = 1.0 / total
+    sample = (f"one complete FP64 p-MG FPCG solve of this workload ({info.iters} outer iterations to relative "
+              f"residual {info.rel_res:.2e}), every apply by the reference's kernels (oracle/_ref, OpenMP "
+              f"{cores} threads), set-up included, timed end to end ({total:.1f} s); ms_per_step = that time / steps")
+    extra = {"reference_solve": {"total_s": total, "iters": int(info.iters), "rel_res": float(info.rel_res),
+                                 "oracle_setup_s": float(info.setup_s), "iter_s": float(info.iter_s),
+                                 "error_vs_fixture": fixture_error(x)},
+             "config_2d": {"one_core": reference_2d(1), "all_cores": reference_2d(cores)},
+             "apply_c3": reference_c3_apply()}
     out = {"metric": METRIC, "value": val, "unit": "solves/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
-           "steps": args.steps, "warmup": args.warmup, "ms_per_step": step * 1e3, "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "fp64", "data": "synthetic",
-           "config": {"workload": "3D two-phase Poisson 24^3x6=82944 tets p=3, Neumann walls + nullspace projection, "
-                                  "p-MG 3-2-1 Chebyshev(4), FPCG rel 1e-8"},
-           "impl": "reference",
-           "cpu_baseline": {"value": val, "unit": "solves/s", "cores": r["cores"], "kind": "reference",
-                            "sample": r["sample"]},
-           "e2e": {"value": val, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": total * 1e3 / args.steps,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": headline_config(), "impl": "reference",
+           "cpu_baseline": {"value": val, "unit": "solves/s", "cores": cores, "kind": "reference", "sample": sample},
+           "e2e": {"value": val, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           **extra}
     print(json.dumps(out))
 
 
@@ -775,6 +877,11 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-serving", action="store_true")
     args = ap.parse_args()
+    if args.impl == "ours" or args.profile:
+        global sipg, W
+        import sipg as _sipg
+        import workloads as _workloads
+        sipg, W = _sipg, _workloads
     if args.profile:
         run_profile(args)
     elif args.impl == "reference":

@@ -33,7 +33,8 @@ class OracleMesh(C.Structure):
 
 class SolveInfo(C.Structure):
     _fields_ = [("iters", C.c_int), ("abs_res", C.c_double), ("rel_res", C.c_double),
-                ("converged", C.c_int)]
+                ("converged", C.c_int), ("setup_s", C.c_double), ("solve_s", C.c_double),
+                ("iter_s", C.c_double)]
 
 
 class OracleCsr(C.Structure):
@@ -51,7 +52,8 @@ class SolverOpts(C.Structure):
                 ("eig_iters", C.c_int), ("coarse_iters", C.c_int), ("coarse_kind", C.c_int),
                 ("amg_nlevels", C.c_int), ("amg_A", C.POINTER(OracleCsr)), ("amg_P", C.POINTER(OracleCsr)),
                 ("amg_R", C.POINTER(OracleCsr)), ("amg_Pdg", C.POINTER(OracleCsr)),
-                ("amg_Rdg", C.POINTER(OracleCsr)), ("amg_coarse_inv", DP), ("amg_coarse_n", C.c_int)]
+                ("amg_Rdg", C.POINTER(OracleCsr)), ("amg_coarse_inv", DP), ("amg_coarse_n", C.c_int),
+                ("smoother", C.c_int), ("amg_cheb_order", C.c_int), ("mult", C.c_void_p)]
 
 
 _libs = {}
@@ -179,10 +181,13 @@ def block_diag(om, ncomp, bc_types, factor=None, mm=None, mm_scalar=0.0, flags=0
 
 def solve(om, b, bc_types, precond=PRE_NONE, factor=None, mm=None, mm_scalar=0.0, flags=0,
           abs_tol=1e-9, rel_tol=1e-8, max_iter=500, inv_mass_factor=1.0, pin_dof=-1, nullspace=0,
-          x0=None, pmg=None, use_ref=False):
+          x0=None, pmg=None, use_ref=False, ref_applies=False):
     """Solve with the oracle (or the reference-kernel harness). pmg: dict with
     orders, meshes (OMesh per level), factors, prolong, cheb_order, eig_safety,
-    eig_ratio, eig_iters, coarse_iters."""
+    eig_ratio, eig_iters, coarse_iters, smoother (0 Jacobi, 1 element-block
+    Jacobi), amg_cheb_order and amg (a hierarchy with the csr / coarse_inverse
+    accessors). ref_applies: the oracle's solver with every operator apply
+    done by the reference's own kernels (oracle/_ref ref_mult)."""
     b = np.ascontiguousarray(b, dtype=np.float64)
     x = np.zeros_like(b) if x0 is None else np.ascontiguousarray(x0, dtype=np.float64).copy()
     bct = np.ascontiguousarray(bc_types, dtype=np.int32).reshape(-1)
@@ -222,6 +227,8 @@ def solve(om, b, bc_types, precond=PRE_NONE, factor=None, mm=None, mm_scalar=0.0
         o.eig_ratio = pmg.get("eig_ratio", 30.0)
         o.eig_iters = pmg.get("eig_iters", 20)
         o.coarse_iters = pmg.get("coarse_iters", 20)
+        o.smoother = pmg.get("smoother", 0)
+        o.amg_cheb_order = pmg.get("amg_cheb_order", 0)
         amg = pmg.get("amg")
         if amg is not None:
             nl = amg.nlevels
@@ -245,6 +252,8 @@ def solve(om, b, bc_types, precond=PRE_NONE, factor=None, mm=None, mm_scalar=0.0
             o.amg_A, o.amg_P, o.amg_R = A, P, R
             o.amg_coarse_inv = _d(inv)
             o.amg_coarse_n = amg.coarse_n
+    if ref_applies:
+        o.mult = C.cast(ref_lib().ref_mult, C.c_void_p).value
     info = SolveInfo()
     if use_ref:
         assert ref_lib().ref_solve(C.byref(om.s), C.byref(o), _d(b), _d(x), C.byref(info)) == 0

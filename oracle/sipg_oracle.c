@@ -8,14 +8,22 @@
  *   mass(q)  : q <- J * M * q
  *   op2_gemv : per element y = alpha * A x + beta * y (A^T when transposed)
  */
+#define _POSIX_C_SOURCE 199309L
 #include "sipg_oracle.h"
 
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 
 #define IDX(e, i, n) ((size_t)(e) * (n) + (i))
+
+static double wall_s(void) {
+  struct timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
 
 static int ngeof(const oracle_mesh *m) { return m->dim == 3 ? 10 : 5; }
 
@@ -90,6 +98,7 @@ void oracle_mult(const oracle_mesh *m, int ncomp, const int *bc_types, const dou
   }
   for (int c = 0; c < ncomp; ++c) {
     /* op2_gemv_halo_exchange(DR/DS/DT), :109-117 */
+#pragma omp parallel for schedule(static)
     for (int e = 0; e < K; ++e)
       for (int d = 0; d < dim; ++d)
         for (int i = 0; i < Np; ++i) {
@@ -98,6 +107,7 @@ void oracle_mult(const oracle_mesh *m, int ncomp, const int *bc_types, const dou
           q[c][d][IDX(e, i, Np)] = s;
         }
     /* fvmf_3d_grad, :119-130 (fvmf_3d_grad.h:13-33) */
+#pragma omp parallel for schedule(static)
     for (int e = 0; e < K; ++e) {
       double G[3][3], J;
       geo_unpack(m, e, G, &J);
@@ -113,7 +123,9 @@ void oracle_mult(const oracle_mesh *m, int ncomp, const int *bc_types, const dou
       }
     }
   }
-  /* mesh->jump / mesh->avg over interior faces, :165-176 */
+  /* mesh->jump / mesh->avg over interior faces, :165-176 (every element face
+   * belongs to one face: the loop writes disjoint slots) */
+#pragma omp parallel for schedule(static)
   for (int fc = 0; fc < m->F; ++fc) {
     int eL = m->face2cells[2 * fc], eR = m->face2cells[2 * fc + 1];
     int fL = m->faceNum[2 * fc], fR = m->faceNum[2 * fc + 1];
@@ -163,6 +175,7 @@ void oracle_mult(const oracle_mesh *m, int ncomp, const int *bc_types, const dou
     }
   }
   /* fvmf_3d_mult_flux, :213-231 (fvmf_3d_mult_flux.h:6-24; vmf_3d_mult_flux.h with the flag) */
+#pragma omp parallel for schedule(static)
   for (int e = 0; e < K; ++e)
     for (int f = 0; f < Nf; ++f) {
       double n[3] = {m->nx[IDX(e, f, Nf)], m->ny[IDX(e, f, Nf)], dim == 3 ? m->nz[IDX(e, f, Nf)] : 0.0};
@@ -181,9 +194,10 @@ void oracle_mult(const oracle_mesh *m, int ncomp, const int *bc_types, const dou
       }
     }
   /* mesh->mass, EMAT lifts, geometric transform, D^T and mm term, :233-286 */
-  double *tmp = (double *)malloc(sizeof(double) * Np);
   for (int c = 0; c < ncomp; ++c) {
+#pragma omp parallel for schedule(static)
     for (int e = 0; e < K; ++e) {
+      double tmp[64];
       double G[3][3], J;
       geo_unpack(m, e, G, &J);
       double w[3][64];
@@ -233,7 +247,6 @@ void oracle_mult(const oracle_mesh *m, int ncomp, const int *bc_types, const dou
       }
     }
   }
-  free(tmp);
   for (int c = 0; c < ncomp; ++c) {
     free(jump[c]);
     for (int d = 0; d < dim; ++d) { free(q[c][d]); free(avg[c][d]); }
@@ -396,7 +409,9 @@ void oracle_block_diag(const oracle_mesh *m, int ncomp, const int *bc_types,
   const int Np = m->Np, Nf = m->Nf, K = m->K, NN = Np * Np;
   double *D = (double *)malloc(sizeof(double) * NN);
   double *blk = (double *)malloc(sizeof(double) * NN);
+#pragma omp parallel for schedule(static)
   for (int e = 0; e < K; ++e) {
+    double *blk = blocks + (size_t)e * NN; /* built in the first component's slot */
     volume_block(m, e, factor, flags, blk); /* fvmf_3d_op1 */
     /* mass term: the operator scales columns (fvmf_3d_mult_mm_geof.h:12); the
      * reference's block scales rows (fvmf_3d_mm_block_diag.h:7) */
@@ -408,7 +423,7 @@ void oracle_block_diag(const oracle_mesh *m, int ncomp, const int *bc_types,
           blk[i * Np + j] += (mm_factor ? mm_factor[IDX(e, (flags & ORACLE_REF_BLOCK_DIAG) ? i : j, Np)]
                                         : mm_scalar) * J * m->M[i * Np + j];
     }
-    for (int c = 0; c < ncomp; ++c) memcpy(blocks + ((size_t)c * K + e) * NN, blk, sizeof(double) * NN);
+    for (int c = 1; c < ncomp; ++c) memcpy(blocks + ((size_t)c * K + e) * NN, blk, sizeof(double) * NN);
   }
   /* fvmf_3d_op2_block_diag over interior faces */
   for (int fc = 0; fc < m->F; ++fc) {
@@ -500,6 +515,7 @@ typedef struct {
   int flags;
   int pin_dof;
   double pin_scale;
+  oracle_mult_fn mult;  /* NULL: oracle_mult */
 } op_ctx;
 
 static size_t vec_len(const op_ctx *o) { return (size_t)o->ncomp * o->m->K * o->m->Np; }
@@ -519,7 +535,12 @@ static void op_apply(const op_ctx *o, const double *x, double *y) {
     x = xc;
   }
   for (int c = 0; c < o->ncomp; ++c) { xs[c] = x + c * per; ys[c] = y + c * per; }
-  oracle_mult(o->m, o->ncomp, o->bc_types, o->factor, o->mm_factor, o->mm_scalar, o->flags, xs, ys);
+  if (o->mult) {
+    if (o->mult(o->m, o->ncomp, o->bc_types, o->factor, o->mm_factor, o->mm_scalar, o->flags, xs, ys) != 0)
+      memset(y, 0xff, sizeof(double) * n); /* NaN: an apply the hook cannot do poisons the solve */
+  } else {
+    oracle_mult(o->m, o->ncomp, o->bc_types, o->factor, o->mm_factor, o->mm_scalar, o->flags, xs, ys);
+  }
   if (xc) {
     y[o->pin_dof] = o->pin_scale * xpin;
     free(xc);
@@ -542,10 +563,31 @@ static double dot(const double *a, const double *b, size_t n) {
 typedef struct {
   op_ctx op;
   double *dinv;
+  double *binv;    /* smoother 1: inverse diagonal blocks, row-major per element (else NULL) */
   double lmax;
   const double *P; /* prolongation from the next level */
   int np_next;
 } pmg_level;
+
+/* out = S in for the level's smoother S: D^-1 (Jacobi) or the inverse diagonal
+ * blocks (element-block Jacobi). */
+static void smoother_apply(const op_ctx *o, const double *dinv, const double *binv, const double *in,
+                           double *out) {
+  size_t n = (size_t)o->ncomp * o->m->K * o->m->Np;
+  if (!binv) {
+    for (size_t i = 0; i < n; ++i) out[i] = dinv[i] * in[i];
+    return;
+  }
+  const int Np = o->m->Np;
+  const size_t nb = n / Np;
+#pragma omp parallel for schedule(static)
+  for (size_t b = 0; b < nb; ++b)
+    for (int i = 0; i < Np; ++i) {
+      double s = 0.0;
+      for (int j = 0; j < Np; ++j) s += binv[(b * Np + i) * Np + j] * in[b * Np + j];
+      out[b * Np + i] = s;
+    }
+}
 
 static uint64_t smix(uint64_t *s) {
   uint64_t z = (*s += 0x9E3779B97F4A7C15ull);
@@ -554,24 +596,27 @@ static uint64_t smix(uint64_t *s) {
   return z ^ (z >> 31);
 }
 
-/* Power iteration on D^-1 A from start vector v0_i = U(-1,1) (splitmix64 seed
- * 0x5eed); lambda = ||D^-1 A v|| / ||v|| after `iters` normalised steps. */
-static double power_lmax(const op_ctx *o, const double *dinv, int iters) {
+/* Power iteration on S A (S the smoother: D^-1, or the inverse diagonal blocks
+ * when binv != NULL) from start vector v0_i = U(-1,1) (splitmix64 seed 0x5eed);
+ * lambda = ||S A v|| / ||v|| after `iters` normalised steps. */
+static double power_lmax(const op_ctx *o, const double *dinv, const double *binv, int iters) {
   size_t n = vec_len(o);
   double *v = (double *)malloc(sizeof(double) * n), *w = (double *)malloc(sizeof(double) * n);
+  double *t = (double *)malloc(sizeof(double) * n);
   uint64_t s = 0x5eedull;
   for (size_t i = 0; i < n; ++i) v[i] = 2.0 * ((smix(&s) >> 11) * (1.0 / 9007199254740992.0)) - 1.0;
   double lam = 0.0;
   for (int it = 0; it < iters; ++it) {
     double nv = sqrt(dot(v, v, n));
     for (size_t i = 0; i < n; ++i) v[i] /= nv;
-    op_apply(o, v, w);
-    for (size_t i = 0; i < n; ++i) w[i] *= dinv[i];
+    op_apply(o, v, t);
+    smoother_apply(o, dinv, binv, t, w);
     lam = sqrt(dot(w, w, n));
-    double *t = v; v = w; w = t;
+    double *tt = v; v = w; w = tt;
   }
   free(v);
   free(w);
+  free(t);
   return lam;
 }
 
@@ -583,12 +628,12 @@ static void compute_dinv(const op_ctx *o, double *dinv) {
 
 double oracle_pmg_lambda_max(const oracle_mesh *m, const int *bc_types, const double *factor,
                              int pin_dof, int iters) {
-  op_ctx o = {m, 1, bc_types, factor, NULL, 0.0, 0, pin_dof, 0.0};
+  op_ctx o = {m, 1, bc_types, factor, NULL, 0.0, 0, pin_dof, 0.0, NULL};
   size_t n = vec_len(&o);
   double *dinv = (double *)malloc(sizeof(double) * n);
   compute_dinv(&o, dinv);
   if (pin_dof >= 0) o.pin_scale = 1.0 / dinv[pin_dof];
-  double l = power_lmax(&o, dinv, iters);
+  double l = power_lmax(&o, dinv, NULL, iters);
   free(dinv);
   return l;
 }
@@ -601,12 +646,15 @@ static void chebyshev(const pmg_level *L, int k, double safety, double ratio, do
   double hi = L->lmax * safety, lo = hi / ratio;
   double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
   double *d = (double *)malloc(sizeof(double) * n), *Ad = (double *)malloc(sizeof(double) * n);
+  double *sr = (double *)malloc(sizeof(double) * n);
   double rho_old = 1.0 / sigma;
-  for (size_t i = 0; i < n; ++i) d[i] = L->dinv[i] * res[i] / theta;
+  smoother_apply(&L->op, L->dinv, L->binv, res, sr);
+  for (size_t i = 0; i < n; ++i) d[i] = sr[i] / theta;
   for (int it = 0; it < k; ++it) {
     if (it > 0) {
       double rho = 1.0 / (2.0 * sigma - rho_old);
-      for (size_t i = 0; i < n; ++i) d[i] = rho * rho_old * d[i] + (2.0 * rho / delta) * L->dinv[i] * res[i];
+      smoother_apply(&L->op, L->dinv, L->binv, res, sr);
+      for (size_t i = 0; i < n; ++i) d[i] = rho * rho_old * d[i] + (2.0 * rho / delta) * sr[i];
       rho_old = rho;
     }
     for (size_t i = 0; i < n; ++i) z[i] += d[i];
@@ -617,6 +665,7 @@ static void chebyshev(const pmg_level *L, int k, double safety, double ratio, do
   }
   free(d);
   free(Ad);
+  free(sr);
 }
 
 /* Fixed-count Jacobi-preconditioned CG from zero (coarsest level). */
@@ -719,14 +768,15 @@ static void amg_vcycle(const oracle_solver_opts *o, const amg_level *al, int l, 
   double *rc = (double *)malloc(sizeof(double) * nc), *zc = (double *)malloc(sizeof(double) * nc);
   memset(z, 0, sizeof(double) * n);
   memcpy(res, r, sizeof(double) * n);
-  csr_chebyshev(A, &al[l], o->cheb_order, o->eig_safety, o->eig_ratio, z, res, 1);
+  const int deg = o->amg_cheb_order > 0 ? o->amg_cheb_order : o->cheb_order;
+  csr_chebyshev(A, &al[l], deg, o->eig_safety, o->eig_ratio, z, res, 1);
   csr_mv(&o->amg_R[l], res, rc);
   amg_vcycle(o, al, l + 1, rc, zc);
   csr_mv(&o->amg_P[l], zc, tmp);
   for (size_t i = 0; i < n; ++i) z[i] += tmp[i];
   csr_mv(A, z, tmp);
   for (size_t i = 0; i < n; ++i) res[i] = r[i] - tmp[i];
-  csr_chebyshev(A, &al[l], o->cheb_order, o->eig_safety, o->eig_ratio, z, res, 0);
+  csr_chebyshev(A, &al[l], deg, o->eig_safety, o->eig_ratio, z, res, 0);
   free(res); free(tmp); free(rc); free(zc);
 }
 
@@ -806,9 +856,11 @@ static void project_mean(double *v, size_t n) {
  * (viscous_solver.cpp:116-117), which is rel_tol = 0. */
 void oracle_solve(const oracle_mesh *m, const oracle_solver_opts *o, const double *b, double *x,
                   oracle_solve_info *info) {
-  op_ctx op = {m, o->ncomp, o->bc_types, o->factor, o->mm_factor, o->mm_scalar, o->flags, o->pin_dof, 0.0};
+  op_ctx op = {m, o->ncomp, o->bc_types, o->factor, o->mm_factor, o->mm_scalar, o->flags, o->pin_dof, 0.0,
+               o->mult};
   size_t n = vec_len(&op);
   const int Np = m->Np, K = m->K;
+  const double t_setup = wall_s();
   double *dinv = NULL, *blocks = NULL;
   pmg_level *lv = NULL;
   amg_level *al = NULL;
@@ -826,14 +878,33 @@ void oracle_solve(const oracle_mesh *m, const oracle_solver_opts *o, const doubl
     nl = o->pmg_nlevels;
     lv = (pmg_level *)calloc(nl, sizeof(pmg_level));
     for (int l = 0; l < nl; ++l) {
-      op_ctx ol = {&o->pmg_meshes[l], o->ncomp, o->bc_types, o->pmg_factors[l], NULL, 0.0, 0, o->pin_dof, 0.0};
+      op_ctx ol = {&o->pmg_meshes[l], o->ncomp, o->bc_types, o->pmg_factors[l], NULL, 0.0, 0, o->pin_dof, 0.0,
+                   o->mult};
       if (o->pin_dof >= 0) ol.pin_dof = (o->pin_dof / Np) * o->pmg_meshes[l].Np + (o->pin_dof % Np);
       lv[l].op = ol;
       size_t nlv = vec_len(&ol);
       lv[l].dinv = (double *)malloc(sizeof(double) * nlv);
       compute_dinv(&lv[l].op, lv[l].dinv);
       if (ol.pin_dof >= 0) lv[l].op.pin_scale = 1.0 / lv[l].dinv[ol.pin_dof];
-      lv[l].lmax = power_lmax(&lv[l].op, lv[l].dinv, o->eig_iters);
+      lv[l].binv = NULL;
+      if (o->smoother == 1) {
+        /* inverse diagonal blocks of the pinned operator: the pinned row and
+         * column of its element's block become pin_scale * identity */
+        const oracle_mesh *lm = &o->pmg_meshes[l];
+        const int Npl = lm->Np;
+        lv[l].binv = (double *)malloc(sizeof(double) * nlv * Npl);
+        oracle_block_diag(lm, o->ncomp, o->bc_types, o->pmg_factors[l], NULL, 0.0, 0, 0, lv[l].binv);
+        if (ol.pin_dof >= 0) {
+          double *B = lv[l].binv + (size_t)(ol.pin_dof / Npl) * Npl * Npl;
+          const int pn = ol.pin_dof % Npl;
+          for (int i = 0; i < Npl; ++i)
+            if (i != pn) { B[pn * Npl + i] = 0.0; B[i * Npl + pn] = 0.0; }
+          B[pn * Npl + pn] = lv[l].op.pin_scale;
+        }
+#pragma omp parallel for schedule(static)
+        for (size_t b = 0; b < nlv / Npl; ++b) invert_inplace(lv[l].binv + b * Npl * Npl, Npl);
+      }
+      lv[l].lmax = power_lmax(&lv[l].op, lv[l].dinv, lv[l].binv, o->eig_iters);
       lv[l].P = l < nl - 1 ? o->pmg_prolong[l] : NULL;
     }
     if (o->coarse_kind == 1) {
@@ -851,6 +922,7 @@ void oracle_solve(const oracle_mesh *m, const oracle_solver_opts *o, const doubl
       }
     }
   }
+  const double t_solve = wall_s();
   double *r = (double *)malloc(sizeof(double) * n), *z = (double *)malloc(sizeof(double) * n);
   double *zo = (double *)malloc(sizeof(double) * n), *p = (double *)malloc(sizeof(double) * n);
   double *Ap = (double *)malloc(sizeof(double) * n);
@@ -903,6 +975,7 @@ void oracle_solve(const oracle_mesh *m, const oracle_solver_opts *o, const doubl
     invert_inplace(minv, Np);
   }
   int iter = 0;
+  double t_iter = wall_s();
   if (o->precond == ORACLE_PRE_NONE) {
     memcpy(p, r, sizeof(double) * n);
     while (res > tol && iter < o->max_iter) {
@@ -923,6 +996,7 @@ void oracle_solve(const oracle_mesh *m, const oracle_solver_opts *o, const doubl
   } else {
     PRECOND(r, z);
     memcpy(p, z, sizeof(double) * n);
+    t_iter = wall_s();
     while (res > tol && iter < o->max_iter) {
       op_apply(&op, p, Ap);
       double a0 = dot(r, z, n), a1 = dot(p, Ap, n);  /* cg3_alpha_pre.h */
@@ -946,10 +1020,16 @@ void oracle_solve(const oracle_mesh *m, const oracle_solver_opts *o, const doubl
   info->abs_res = res;
   info->rel_res = bnorm > 0 ? res / bnorm : res;
   info->converged = res <= tol;
+  info->setup_s = t_solve - t_setup;
+  info->solve_s = wall_s() - t_solve;
+  info->iter_s = iter > 0 ? (wall_s() - t_iter) / iter : 0.0;
   free(r); free(z); free(zo); free(p); free(Ap);
   free(dinv); free(blocks); free(minv);
   if (lv) {
-    for (int l = 0; l < nl; ++l) free(lv[l].dinv);
+    for (int l = 0; l < nl; ++l) {
+      free(lv[l].dinv);
+      free(lv[l].binv);
+    }
     free(lv);
   }
   if (al) {

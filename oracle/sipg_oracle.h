@@ -90,7 +90,17 @@ typedef struct {
   double abs_res;      /* final ||r||_2 */
   double rel_res;      /* final ||r||_2 / ||b||_2 */
   int converged;
+  double setup_s;      /* wall seconds of the preconditioner set-up */
+  double solve_s;      /* wall seconds of the iterations (initial residual included) */
+  double iter_s;       /* wall seconds per iteration after the first preconditioner application */
 } oracle_solve_info;
+
+/* Operator apply with oracle_mult's arguments; returns 0 on success. Lets a
+ * solve run on another implementation of the same apply (the reference's own
+ * kernels in oracle/_ref, ref_mult). */
+typedef int (*oracle_mult_fn)(const oracle_mesh *m, int ncomp, const int *bc_types, const double *factor,
+                              const double *mm_factor, double mm_scalar, int flags, const double *const *x,
+                              double *const *y);
 
 typedef struct {
   int ncomp;
@@ -124,6 +134,11 @@ typedef struct {
   const oracle_csr *amg_Pdg, *amg_Rdg;     /* last-order DG unknowns <-> algebraic level 0 */
   const double *amg_coarse_inv;            /* dense inverse of the coarsest operator */
   int amg_coarse_n;
+  /* smoother of the order levels: 0 Jacobi (inverse diagonal), 1 element-block
+   * Jacobi (inverse diagonal blocks of the operator, pinned DOF included) */
+  int smoother;
+  int amg_cheb_order;        /* Chebyshev degree on the algebraic levels (0: cheb_order) */
+  oracle_mult_fn mult;       /* every operator apply of the solve (NULL: oracle_mult) */
 } oracle_solver_opts;
 
 /* Solve A x = b (x holds the initial guess on entry). ncomp components are
