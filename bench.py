@@ -794,6 +794,10 @@ def run_profile(args):
     projection: the velocity projection workload at --n (3 launches of k_proj_cg).
     pressure: the pressure step kernels at --n: sipg_pressure_rhs and
            sipg_pressure_projection alternately, 3 launches each.
+    c3apply: the Helmholtz operator (I/(nu dt) - Laplacian) at --n, order --order,
+           --precision: 3 applies.
+    c3pcg: the inverse-mass preconditioned CG on that operator, FP64: a warm-up
+           solve of 3 iterations, then a counted one (kernel by kernel, no graphs).
     solve: the headline mixed solve: one warm-up solve, then the captured solve;
            prints the number of kernels launched before it (ncu -s) and in it (-c).
            The outer iterations replay one host-launched graph each (graphs = 1):
@@ -830,6 +834,36 @@ def run_profile(args):
         sipg.check(sipg.lib().sipg_device_synchronize())
         print("done", mesh.K)
         return
+    if args.profile in ("c3apply", "c3pcg"):
+        # the Helmholtz configuration at --n (48: 663,552 tets), order --order (4)
+        h = W.helmholtz3d(args.n, order=args.order)
+        op = sipg.Operator(h["mesh"], args.order, 1)
+        op.set_bc_types(h["bc_types"])
+        op.set_mm(sipg.MM_SCALAR, h["mm"])
+        K, Np = h["mesh"].K, op.Np
+        if args.profile == "c3apply":
+            t = np.float32 if args.precision == 32 else np.float64
+            x = sipg.DeviceVector(h["x"].reshape(-1).astype(t))
+            y = sipg.DeviceVector(np.zeros(K * Np, t))
+            for _ in range(3):
+                op.apply_device(args.precision, x.ptr, y.ptr)
+        else:
+            # inverse-mass PCG (PETScInvMassSolver): one warm-up solve, then 3 iterations
+            o = sipg.default_opts(sipg.SOLVER_INV_MASS)
+            o.rel_tol, o.abs_tol, o.max_iter, o.graphs = 1e-8, 0.0, 3, 0
+            o.inv_mass_factor = 1.0 / h["mm"]
+            s = sipg.Solver(op, sipg.SOLVER_INV_MASS, o)
+            b = sipg.DeviceVector(np.random.default_rng(11).uniform(-1, 1, K * Np))
+            x = sipg.DeviceVector(np.zeros(K * Np))
+            s.solve_device(b.ptr, x.ptr)
+            sipg.check(sipg.lib().sipg_device_synchronize())
+            n1 = launches()
+            x = sipg.DeviceVector(np.zeros(K * Np))
+            info = s.solve_device(b.ptr, x.ptr)
+            print("skip", n1, "count", launches() - n1, "iters", info.iters)
+        sipg.check(sipg.lib().sipg_device_synchronize())
+        print("done", K)
+        return
     c = W.poisson3d_two_phase(args.n, order=ORDER, n_modes=256, pin=False)
     if args.profile == "apply":
         op = sipg.Operator(c["mesh"], args.order, 1)
@@ -864,7 +898,7 @@ def run_profile(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--profile", choices=["apply", "solve", "projection", "pressure"], default=None,
+    ap.add_argument("--profile", choices=["apply", "solve", "projection", "pressure", "c3apply", "c3pcg"], default=None,
                     help="run a small fixed workload for an ncu capture instead of the benchmark")
     ap.add_argument("--n", type=int, default=N_HEAD)
     ap.add_argument("--order", type=int, default=ORDER)

@@ -127,8 +127,11 @@ int sipg_op_apply_host(sipg_op *op, const double *x, double *y);
 #define SIPG_STATIC_SCRATCH_BYTES (64u << 20)
 int sipg_op_apply_static_scratch(sipg_op *op, int precision, const void *x, void *y, void *stream);
 /* Kernel selection of apply(): 0 tensor cores where the operator allows it
- * (scalar operators: TF32 MMAs for SIPG_FP32, FP64 MMAs for SIPG_FP64), 1 the
- * CUDA-core kernel. No reference counterpart (the reference has one OP2 path). */
+ * (scalar operators: SIPG_FP32 on tcgen05 TF32 MMAs with TMEM accumulators where
+ * the order has that kernel, else mma.sync TF32; SIPG_FP64 on FP64 MMAs), 1 the
+ * CUDA-core kernel, 2 the mma.sync tensor-core kernels for every order (the
+ * previous generation, kept for comparison). No reference counterpart (the
+ * reference has one OP2 path). */
 int sipg_op_set_kernel(sipg_op *op, int kind);
 /* apply_bc (factor_viscous_matrix.cpp:47-68): rhs += lifted bc data; host buffers,
  * bc: ncomp x Kb x Nfp, rhs: ncomp x K x Np (updated in place). */
@@ -355,6 +358,11 @@ int sipg_pressure_rhs_host(sipg_mesh *m, int order, double dt, double b0, double
 /* Number of kernels this library has launched so far in the process
  * (diagnostics for benchmarks; no reference counterpart). */
 int sipg_launch_count(unsigned long long *n);
+
+/* Bounded waits inside the library's kernels on the current device that ran
+ * out (an MMA completion never arrived); the kernel that saw one stopped its
+ * work. 0 in a healthy run (diagnostics; no reference counterpart). */
+int sipg_kernel_wait_timeouts(unsigned long long *n);
 
 #ifdef __cplusplus
 }

@@ -925,6 +925,10 @@ cudaError_t launch_tc_t(const ApplyArgs<T>& a, const T* blob, T* trace, int num_
   constexpr int WA = warps1<T, DIM, P>(), W2D = warps2<T, DIM, P, 2>(), W2S = warps2<T, DIM, P, 1>();
   if (W2D < 1) return cudaErrorInvalidConfiguration;
   using X = Tc<T, DIM, P>;
+  if constexpr (std::is_same<T, float>::value) {
+    // FP32: the tcgen05 kernels (their constants follow the mma.sync blob)
+    if (a.tcgen05 && tc5_supported(DIM, P)) return launch_apply_tc5(DIM, P, a, blob + X::NALL, trace, num_sms, s);
+  }
   // the kernels copy caller vectors in 16-byte pieces: other alignments take the CUDA-core kernel
   if (!aligned16(a.x) || !aligned16(a.y) || !aligned16(trace) || (a.factor && !aligned16(a.factor)) ||
       (a.beta != T(0) && !aligned16(a.c)))
@@ -974,6 +978,11 @@ void build_tc_consts_t(const RefElement& r, std::vector<double>& out) {
     for (int n = 0; n < NP; ++n)
       for (int k = 0; k < KF; ++k)
         put(X::BF + rr * NT * FT * X::BLK, FT, n, k, D[rr][r.fmask[k] * NP + n]);  // BF_r[n][k] = D_r[m(k)][n]
+  if (std::is_same<T, float>::value && tc5_supported(DIM, P)) {
+    std::vector<double> t5;
+    build_tc5_consts(DIM, P, r, t5);
+    out.insert(out.end(), t5.begin(), t5.end());
+  }
 }
 
 }  // namespace

@@ -31,4 +31,15 @@ size_t tc_geom_values(int dim, int K);
 template <typename T>
 cudaError_t launch_tc_geom(int dim, const T* geof, int K, T* out, cudaStream_t s);
 
+// tcgen05 kernels of the FP32 scalar apply (apply_tc5.cu): their constants follow
+// the mma.sync blob of build_tc_consts<float> (appended by it), the face traces
+// use the same scratch layout (tc_trace_values).
+bool tc5_supported(int dim, int order);
+size_t tc5_const_values(int dim, int order);
+void build_tc5_consts(int dim, int order, const RefElement& r, std::vector<double>& out);
+cudaError_t launch_apply_tc5(int dim, int order, const ApplyArgs<float>& a, const float* blob, float* trace,
+                             int num_sms, cudaStream_t s);
+// MMA waits of the tcgen05 kernels that ran out (0 unless something hung).
+unsigned tc5_timeouts();
+
 }  // namespace sipg

@@ -22,6 +22,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <type_traits>
@@ -174,6 +176,23 @@ double host_csr_lmax(const Csr& A, const std::vector<double>& dinv, int iters) {
 }
 
 }  // namespace
+
+// Set-up phase timer: with SIPG_SETUP_TIMES set in the environment, each phase
+// of a solver set-up is synchronised and its wall time printed to stderr.
+struct PhaseTimer {
+  bool on = std::getenv("SIPG_SETUP_TIMES") != nullptr;
+  cudaStream_t s;
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+  explicit PhaseTimer(cudaStream_t st) : s(st) {}
+  void mark(const char* what, int level = -1) {
+    if (!on) return;
+    cudaStreamSynchronize(s);
+    const auto t1 = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "setup %-22s level %2d %8.2f ms\n", what, level,
+                 std::chrono::duration<double, std::milli>(t1 - t0).count());
+    t0 = t1;
+  }
+};
 
 // One capture at a time in the process (solvers of a serving loop capture from
 // several threads), and no capture while another thread runs a solver's first
@@ -344,6 +363,7 @@ void sipg_solver::setup_pmg() {
   const size_t ts = f32 ? sizeof(float) : sizeof(double);
   sipg_mesh* m = op->mesh;
   const int K = m->K, nc = op->ncomp, dim = m->dim;
+  PhaseTimer pt(stream);
   if (lv.empty()) {
     lv.resize(nl);
     for (int l = 0; l < nl; ++l) {
@@ -414,6 +434,7 @@ void sipg_solver::setup_pmg() {
     }
     SIPG_CUDA(cudaStreamSynchronize(stream));
   }
+  pt.mark("levels and factors");
   for (int l = 0; l < nl; ++l) {
     Level& L = lv[l];
     L.cheb = o.cheb_orders[l] > 0 ? o.cheb_orders[l] : o.cheb_order;
@@ -448,10 +469,13 @@ void sipg_solver::setup_pmg() {
         L.bc64 = DevBuf((size_t)nb * L.Np * L.Np * sizeof(double));
         block_transpose<double>(L.bc64.as<double>(), rows.as<double>(), nb, L.Np, stream);
       }
+      pt.mark("diagonal and blocks", l);
       L.lmax = power_lmax(L.op, nullptr, L.n, rows.as<double>(), L.Np);
     } else {
+      pt.mark("diagonal", l);
       L.lmax = power_lmax(L.op, L.dinv64.as<double>(), L.n);
     }
+    pt.mark("eigenvalue bound", l);
     L.bsr.reset();
     // -1: p = 2 and below in the FP32 V-cycle (p = 2 as scaled FP16 blocks: half the
     // bytes of the matrix-free apply's per-element work, same iteration counts), p = 1
@@ -465,6 +489,7 @@ void sipg_solver::setup_pmg() {
       // that one kernel per Chebyshev step after the first updates Bd^-1 r directly
       const bool fused = f32 && o.smoother == 1 && L.Np % 2 == 0;
       bsr_assemble(L.op, *L.bsr, f32, stream, fused ? rows.as<double>() : nullptr, L.bsym);
+      pt.mark("assembled blocks", l);
       if (L.bsr->c16.p) {
         L.d2 = DevBuf(L.n * sizeof(float));
         L.sres = DevBuf(L.n * sizeof(float));
@@ -473,6 +498,7 @@ void sipg_solver::setup_pmg() {
   }
   use_amg = o.coarse_kind == 1 && nc == 1 && lv.back().order == 1;
   if (use_amg) setup_amg();
+  pt.mark("algebraic levels");
 }
 
 void sipg_solver::setup_amg() {
@@ -499,12 +525,15 @@ void sipg_solver::setup_amg() {
     bd[b] = op->bct_host[b] == SIPG_BC_DIRICHLET;
     any_dirichlet |= bd[b] != 0;
   }
+  PhaseTimer pt(stream);
   Csr A0, Pd;
   p1c_operator(dev_ref(m->dim, 1).ref, K, m->Nv, h.geof.data(), h.e2v.data(), fac1.empty() ? nullptr : fac1.data(),
                tau1.data(), h.sJ.data(), h.nx.data(), h.ny.data(), h.nz.data(), h.nbr.data(), bd, lop->mm_mode,
                lop->mm_scalar, mm1.empty() ? nullptr : mm1.data(), &A0, &Pd);
   const bool singular = !any_dirichlet && lop->mm_mode == SIPG_MM_NONE;
+  pt.mark("P1 operator (host)");
   AmgHierarchy H = build_amg(A0, Pd, std::max(2, o.amg_coarse_max), o.amg_strength, singular);
+  pt.mark("aggregation (host)");
   const bool f32 = o.precision == SIPG_FP32;
   const size_t ts = f32 ? sizeof(float) : sizeof(double);
   Pdg.upload(H.Pdg);
@@ -1186,6 +1215,13 @@ int sipg_launch_count(unsigned long long* n) {
   return guarded([&] {
     if (!n) throw Error(SIPG_INVALID_ARG, "null pointer");
     *n = launch_count();
+  });
+}
+
+int sipg_kernel_wait_timeouts(unsigned long long* n) {
+  return guarded([&] {
+    if (!n) throw Error(SIPG_INVALID_ARG, "null pointer");
+    *n = tc5_timeouts();
   });
 }
 

@@ -574,6 +574,43 @@ __global__ void k_inv_mass(T* y, const T* x, const T* Minv, const T* geof, int n
   }
 }
 
+// Fixed-size inverse mass: a block stages the rows of 128 elements with coalesced
+// loads, each thread applies M^-1 (shared, broadcast reads) to one element's row
+// and the block stores the rows back coalesced.
+template <typename T, int NP>
+__global__ void __launch_bounds__(128) k_inv_mass_n(T* __restrict__ y, const T* __restrict__ x,
+                                                     const T* __restrict__ Minv, const T* __restrict__ geof,
+                                                     int ngeof, int jidx, int K, int nrows, T scale) {
+  __shared__ T sM[NP * NP];
+  __shared__ T sx[128 * NP];
+  for (int i = threadIdx.x; i < NP * NP; i += blockDim.x) sM[i] = Minv[i];  // set-up data
+  pdl_enter();
+  for (size_t b0 = (size_t)blockIdx.x * 128; b0 < (size_t)nrows; b0 += (size_t)gridDim.x * 128) {
+    const int nb = (int)min((size_t)128, (size_t)nrows - b0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < nb * NP; i += blockDim.x) sx[i] = x[b0 * NP + i];
+    __syncthreads();
+    if ((int)threadIdx.x < nb) {
+      const size_t be = b0 + threadIdx.x;
+      const T* xr = sx + threadIdx.x * NP;
+      T xv[NP];
+#pragma unroll
+      for (int j = 0; j < NP; ++j) xv[j] = xr[j];
+      const T sc = scale / geof[(be % (size_t)K) * ngeof + jidx];
+      T* yr = sx + threadIdx.x * NP;
+#pragma unroll
+      for (int r = 0; r < NP; ++r) {
+        T s = T(0);
+#pragma unroll
+        for (int j = 0; j < NP; ++j) s += sM[r * NP + j] * xv[j];
+        yr[r] = sc * s;
+      }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nb * NP; i += blockDim.x) y[b0 * NP + i] = sx[i];
+  }
+}
+
 template <typename T>
 __global__ void k_restrict(T* rc, const T* r, const T* P, int K, int Npf, int Npc, int ncomp) {
   pdl_enter();
@@ -936,7 +973,17 @@ void block_matvec(T* y, const T* B, const T* x, int nb, int Np, cudaStream_t s) 
 template <typename T>
 void inv_mass(T* y, const T* x, const T* Minv, const T* geof, int ngeof, int jidx, int K, int Np,
               int ncomp, T scale, cudaStream_t s) {
-  pdl_launch(k_inv_mass<T>, dim3(grid_for((size_t)ncomp * K * Np)), dim3(256), 0, s, y, x, Minv, geof, ngeof, jidx, K, Np, ncomp, scale);
+  const int nrows = ncomp * K;
+  const dim3 g((unsigned)std::max(1, std::min((nrows + 127) / 128, 148 * 8))), b(128);
+  switch (Np) {  // 3D orders 2..4 and 2D orders 3..4: element rows staged in shared memory
+    case 10: pdl_launch(k_inv_mass_n<T, 10>, g, b, 0, s, y, x, Minv, geof, ngeof, jidx, K, nrows, scale); break;
+    case 15: pdl_launch(k_inv_mass_n<T, 15>, g, b, 0, s, y, x, Minv, geof, ngeof, jidx, K, nrows, scale); break;
+    case 20: pdl_launch(k_inv_mass_n<T, 20>, g, b, 0, s, y, x, Minv, geof, ngeof, jidx, K, nrows, scale); break;
+    case 35: pdl_launch(k_inv_mass_n<T, 35>, g, b, 0, s, y, x, Minv, geof, ngeof, jidx, K, nrows, scale); break;
+    default:
+      pdl_launch(k_inv_mass<T>, dim3(grid_for((size_t)ncomp * K * Np)), dim3(256), 0, s, y, x, Minv, geof, ngeof, jidx,
+                 K, Np, ncomp, scale);
+  }
   note_launch();
 }
 template <typename T>
