@@ -220,10 +220,18 @@ def apply_bytes_per_elem(Np, ts, factor, ngeof=10, nf=4, gface=5):
     return ts * (2 * Np + (Np if factor else 0) + ngeof + nf * gface) + 4 * 2 * nf
 
 
-# DRAM traffic of one FP32 p=3 apply (trace + apply kernels) at the headline
-# size, ncu capture with flushed caches (dram__bytes_read.sum + dram__bytes_write.sum
-# of both launches): profiles/apply_tc_fp32_p3_24cube.txt
-APPLY_P3_FP32_TRAFFIC = 16.627e6 + 0.006e6 + 46.210e6 + 0.449e6
+def profile_value(name, key):
+    """A `key = value` figure of a committed ncu summary under profiles/ (the
+    DRAM traffic the roofline blocks quote comes from the capture itself)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", name)) as f:
+            for line in f:
+                k, _, v = line.partition("=")
+                if k.strip() == key and v.strip():
+                    return float(v.split()[0])
+    except OSError:
+        pass
+    return None
 
 
 def max_over_ranks(x, world, device):
@@ -309,6 +317,9 @@ def run_ours(args):
     # dominant kernel: FP32 p=3 apply of the V-cycle (and the FP64 outer apply)
     a32 = time_apply(op, sipg.FP32, K, Np)
     a64 = time_apply(op, sipg.FP64, K, Np)
+    op.set_kernel(3)  # the tcgen05 kernels (TMEM accumulators), for comparison
+    a32_tc5 = time_apply(op, sipg.FP32, K, Np)
+    op.set_kernel(0)
     hbm, peak_kind = peaks()
     bpe = apply_bytes_per_elem(Np, 4, True)
     achieved = bpe * K / (a32 * 1e-3) / 1e9
@@ -323,10 +334,18 @@ def run_ours(args):
         t64 = time_apply(op4, sipg.FP64, K4, Np4, 20)
         t32 = time_apply(op4, sipg.FP32, K4, Np4, 20)
         b4 = apply_bytes_per_elem(Np4, 4, False)
+        tpe = profile_value("apply_tc_fp32_p4_40cube.txt", "traffic_bytes_per_element")
         apply_c3 = {"workload": "3D Helmholtz I/(nu dt) - Lap, 48^3x6=663552 tets, p=4",
                     "fp64_gdofs": K4 * Np4 / (t64 * 1e-3) / 1e9, "fp32_gdofs": K4 * Np4 / (t32 * 1e-3) / 1e9,
                     "fp64_ms": t64, "fp32_ms": t32,
                     "fp32_hbm_frac": b4 * K4 / (t32 * 1e-3) / 1e9 / hbm,
+                    "roofline": {"kernel": "sipg_trace_kernel<float,3,4,9> + sipg_apply_tc_kernel<float,3,4,7,1>",
+                                 "bound": "hbm", "achieved": b4 * K4 / (t32 * 1e-3) / 1e9, "peak": hbm,
+                                 "peak_kind": peak_kind, "unit": "GB/s",
+                                 "frac": b4 * K4 / (t32 * 1e-3) / 1e9 / hbm,
+                                 "traffic": tpe * K4 if tpe else None, "bytes_per_elem": b4,
+                                 "traffic_source": "profiles/apply_tc_fp32_p4_40cube.txt (40^3x6 capture, "
+                                                   "per-element traffic scaled to 663,552 elements)"},
                     "inv_mass_pcg": c3_solve(op4, h["mm"], K4 * Np4)}
     lat = np.array(ms32)
     out = {
@@ -358,13 +377,16 @@ def run_ours(args):
                 "d2h_bytes_per_step": int(b.nbytes)},
         "gpu_launches": int(n_launch),
         "apply_p3": {"fp32_ms": a32, "fp64_ms": a64, "fp32_gdofs": n / (a32 * 1e-3) / 1e9,
-                     "fp64_gdofs": n / (a64 * 1e-3) / 1e9},
+                     "fp64_gdofs": n / (a64 * 1e-3) / 1e9, "fp32_tcgen05_ms": a32_tc5,
+                     "fp32_tcgen05_gdofs": n / (a32_tc5 * 1e-3) / 1e9},
         "apply_c3": apply_c3,
         "roofline": {"kernel": "sipg_trace_kernel<float,3,3> + sipg_apply_tc_kernel<float,3,3> "
                                "(one FP32 p=3 apply = 2 launches)",
                      "bound": "hbm", "achieved": achieved, "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": APPLY_P3_FP32_TRAFFIC, "bytes_per_elem": bpe,
-                     "apply_ms": a32, "elements": K},
+                     "frac": achieved / hbm,
+                     "traffic": profile_value("apply_tc_fp32_p3_24cube.txt", "traffic_bytes_per_apply"),
+                     "traffic_source": "profiles/apply_tc_fp32_p3_24cube.txt (ncu, caches flushed per pass)",
+                     "bytes_per_elem": bpe, "apply_ms": a32, "elements": K},
         "clocks": clk.summary(),
     }
     out["config_2d"] = run_config_2d()

@@ -127,11 +127,11 @@ int sipg_op_apply_host(sipg_op *op, const double *x, double *y);
 #define SIPG_STATIC_SCRATCH_BYTES (64u << 20)
 int sipg_op_apply_static_scratch(sipg_op *op, int precision, const void *x, void *y, void *stream);
 /* Kernel selection of apply(): 0 tensor cores where the operator allows it
- * (scalar operators: SIPG_FP32 on tcgen05 TF32 MMAs with TMEM accumulators where
- * the order has that kernel, else mma.sync TF32; SIPG_FP64 on FP64 MMAs), 1 the
- * CUDA-core kernel, 2 the mma.sync tensor-core kernels for every order (the
- * previous generation, kept for comparison). No reference counterpart (the
- * reference has one OP2 path). */
+ * (scalar operators: mma.sync TF32 MMAs for SIPG_FP32, FP64 MMAs for SIPG_FP64),
+ * 1 the CUDA-core kernel, 2 the same tensor-core kernels as 0, 3 SIPG_FP32 on
+ * tcgen05 TF32 MMAs with TMEM accumulators where the order has those kernels
+ * (3D p = 3; otherwise as 0). No reference counterpart (the reference has one
+ * OP2 path). */
 int sipg_op_set_kernel(sipg_op *op, int kind);
 /* apply_bc (factor_viscous_matrix.cpp:47-68): rhs += lifted bc data; host buffers,
  * bc: ncomp x Kb x Nfp, rhs: ncomp x K x Np (updated in place). */
@@ -182,7 +182,7 @@ typedef struct {
   int check_every;           /* host convergence check period (iterations) */
   int coarse_kind;           /* 0: Jacobi-PCG on the lowest order; 1: algebraic multigrid on the
                                 continuous piecewise-linear space (coarse_solver = petsc/amg) */
-  int amg_coarse_max;        /* unknowns of the densely inverted coarsest level */
+  int amg_coarse_max;        /* unknowns of the densely inverted coarsest level (default 2048; inverted on the device) */
   double amg_strength;       /* aggregation strength threshold */
   int graphs;                /* 2: the outer iterations after the first run inside one CUDA graph
                                 whose conditional while-node repeats an iteration until the
@@ -354,6 +354,19 @@ int sipg_pressure_rhs(sipg_mesh *m, int order, double dt, double b0, double b1, 
                       const double *dPdN, double *dPdN_old, double *rhs, void *stream);
 int sipg_pressure_rhs_host(sipg_mesh *m, int order, double dt, double b0, double b1, const double *velT,
                            const double *dPdN, double *dPdN_old, double *rhs);
+
+/* Viscous right-hand side of the two-phase time step, MPINSSolver3D::viscosity
+ * (src/solvers/3d/mp_ins_solver.cpp:669-694): mp_ins_3d_vis_0 then mesh->mass on
+ * each component, as one kernel. rhs_c = J M (fact0 rho velTT_c), mm_factor =
+ * fact1 rho (the mass factor of the viscous Helmholtz operator); fact0 =
+ * Re / dt, fact1 = g0 Re / dt. rho, mm_factor: K x Np; velTT, rhs: dim x K x Np
+ * (device pointers, or host pointers in the synchronous _host variant). The
+ * boundary data of ins_3d_vis_{x,y,z} come from the problem's callbacks and enter
+ * through sipg_op_apply_bc_host. */
+int sipg_viscous_rhs(sipg_mesh *m, int order, double fact0, double fact1, const double *rho, const double *velTT,
+                     double *rhs, double *mm_factor, void *stream);
+int sipg_viscous_rhs_host(sipg_mesh *m, int order, double fact0, double fact1, const double *rho,
+                          const double *velTT, double *rhs, double *mm_factor);
 
 /* Number of kernels this library has launched so far in the process
  * (diagnostics for benchmarks; no reference counterpart). */

@@ -4,7 +4,10 @@
 #include "refelem.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <stdexcept>
 
 namespace sipg {
@@ -39,16 +42,45 @@ Csr p0_operator(int K, int Nf, const double* sJ, const double* tau, const int* n
   return A;
 }
 
+P1Plan p1c_plan(int K, int Nv, int Np, const int* e2v) {
+  P1Plan pl;
+  pl.Nv = Nv;
+  std::vector<std::vector<int>> cols(Nv);
+  for (int e = 0; e < K; ++e)
+    for (int i = 0; i < Np; ++i)
+      for (int j = 0; j < Np; ++j) cols[e2v[(size_t)e * Np + i]].push_back(e2v[(size_t)e * Np + j]);
+  pl.ptr.assign(Nv + 1, 0);
+  for (int v = 0; v < Nv; ++v) {
+    std::sort(cols[v].begin(), cols[v].end());
+    cols[v].erase(std::unique(cols[v].begin(), cols[v].end()), cols[v].end());
+    pl.ptr[v + 1] = pl.ptr[v] + (int)cols[v].size();
+  }
+  pl.idx.resize(pl.ptr[Nv]);
+  for (int v = 0; v < Nv; ++v) std::copy(cols[v].begin(), cols[v].end(), pl.idx.begin() + pl.ptr[v]);
+  pl.slot.resize((size_t)K * Np * Np);
+  for (int e = 0; e < K; ++e)
+    for (int i = 0; i < Np; ++i) {
+      const int vi = e2v[(size_t)e * Np + i];
+      const int* b = pl.idx.data() + pl.ptr[vi];
+      const int* en = pl.idx.data() + pl.ptr[vi + 1];
+      for (int j = 0; j < Np; ++j)
+        pl.slot[((size_t)e * Np + i) * Np + j] = pl.ptr[vi] + (int)(std::lower_bound(b, en, e2v[(size_t)e * Np + j]) - b);
+    }
+  return pl;
+}
+
 void p1c_operator(const RefElement& r, int K, int Nv, const double* geof, const int* e2v,
                   const double* factor1, const double* tau1, const double* sJ, const double* nx,
                   const double* ny, const double* nz, const int* nbr,
                   const std::vector<uint8_t>& bc_dirichlet, int mm_mode, double mm_scalar,
-                  const double* mm1, Csr* Aout, Csr* Pout) {
+                  const double* mm1, Csr* Aout, Csr* Pout, const P1Plan* plan) {
   const int dim = r.dim, Np = r.Np, Nf = r.Nfaces, Nfp = r.Nfp, ng = dim == 3 ? 10 : 5;
   if (Np != dim + 1) throw std::runtime_error("p1c_operator needs the order-1 element");
   const double* Dm[3] = {r.Dr.data(), r.Ds.data(), r.Dt.data()};
-  // assemble with a per-row map (vertex graph)
-  std::vector<std::vector<std::pair<int, double>>> rows(Nv);
+  // assemble into the planned sparsity (element order) or, without a plan, with a
+  // per-row map of the vertex graph
+  std::vector<std::vector<std::pair<int, double>>> rows(plan ? 0 : Nv);
+  std::vector<double> pval(plan ? plan->idx.size() : 0, 0.0);
   std::vector<double> B(Np * Np), Dx(Np * Np), T(Np * Np), Dn(Np * Np);
   for (int e = 0; e < K; ++e) {
     const double* g = geof + (size_t)e * ng;
@@ -108,16 +140,28 @@ void p1c_operator(const RefElement& r, int K, int Nv, const double* geof, const 
         for (int j = 0; j < Np; ++j)
           B[i * Np + j] += J * r.M[i * Np + j] * (mm_mode == 1 ? mm_scalar : mm1[(size_t)e * Np + j]);
     const int* v = e2v + (size_t)e * Np;
-    for (int i = 0; i < Np; ++i)
-      for (int j = 0; j < Np; ++j) rows[v[i]].push_back({v[j], B[i * Np + j]});
+    if (plan) {
+      const int* sl = plan->slot.data() + (size_t)e * Np * Np;
+      for (int q = 0; q < Np * Np; ++q) pval[sl[q]] += B[q];
+    } else {
+      for (int i = 0; i < Np; ++i)
+        for (int j = 0; j < Np; ++j) rows[v[i]].push_back({v[j], B[i * Np + j]});
+    }
     (void)Nfp;
   }
   Csr& A = *Aout;
   A.rows = A.cols = Nv;
-  A.ptr.assign(Nv + 1, 0);
-  A.idx.clear();
-  A.val.clear();
-  for (int i = 0; i < Nv; ++i) {
+  if (plan) {
+    A.ptr = plan->ptr;
+    A.idx = plan->idx;
+    A.val = std::move(pval);
+  }
+  if (!plan) {
+    A.ptr.assign(Nv + 1, 0);
+    A.idx.clear();
+    A.val.clear();
+  }
+  for (int i = 0; i < Nv && !plan; ++i) {
     auto& rw = rows[i];
     std::sort(rw.begin(), rw.end());
     for (size_t k = 0; k < rw.size();) {
@@ -267,8 +311,25 @@ std::vector<double> dense_inverse(std::vector<double> a, int n) {
 constexpr double kMinCoarsening = 0.6;
 constexpr int kMaxDenseCoarse = 8192;
 
-AmgHierarchy build_amg(const Csr& A0, const Csr& Pdg, int coarse_max, double strength, bool singular) {
+namespace {
+struct HostTimer {
+  bool on = std::getenv("SIPG_SETUP_TIMES") != nullptr;
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+  void mark(const char* what, int level) {
+    if (!on) return;
+    const auto t1 = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "  amg %-20s level %2d %8.2f ms\n", what, level,
+                 std::chrono::duration<double, std::milli>(t1 - t0).count());
+    t0 = t1;
+  }
+};
+}  // namespace
+
+AmgHierarchy build_amg(const Csr& A0, const Csr& Pdg, int coarse_max, double strength, bool singular,
+                       bool host_inverse) {
+  HostTimer ht;
   AmgHierarchy H;
+  H.singular = singular;
   H.Pdg = Pdg;
   H.Rdg = transpose(Pdg);
   H.levels.push_back({A0, {}, {}});
@@ -284,6 +345,7 @@ AmgHierarchy build_amg(const Csr& A0, const Csr& Pdg, int coarse_max, double str
       agg = aggregate(A, theta, &na);
     }
     if (na > kMinCoarsening * A.rows || na < 1) break;
+    ht.mark("aggregate", (int)H.levels.size() - 1);
     // tentative prolongator: piecewise constant on aggregates
     Csr T;
     T.rows = A.rows;
@@ -318,7 +380,9 @@ AmgHierarchy build_amg(const Csr& A0, const Csr& Pdg, int coarse_max, double str
       }
     Csr P = spgemm(S, T);
     Csr R = transpose(P);
+    ht.mark("prolongator", (int)H.levels.size() - 1);
     Csr Ac = spgemm(R, spgemm(A, P));
+    ht.mark("galerkin product", (int)H.levels.size() - 1);
     H.levels.back().P = std::move(P);
     H.levels.back().R = std::move(R);
     H.levels.push_back({std::move(Ac), {}, {}});
@@ -336,7 +400,14 @@ AmgHierarchy build_amg(const Csr& A0, const Csr& Pdg, int coarse_max, double str
     }
   if (singular)
     for (int i = 0; i < n; ++i) dense[(size_t)i * n + i] += 1e-8 * dmax;
+  ht.mark("coarse matrix", -1);
+  H.coarse_n = n;
+  if (!host_inverse) {
+    H.coarse_dense = std::move(dense);
+    return H;
+  }
   std::vector<double> inv = dense_inverse(std::move(dense), n);
+  ht.mark("dense inverse", -1);
   if (singular) {
     // pseudo-inverse on the complement of the constants: Q inv Q with Q = I - 11^T/n,
     // so the coarsest correction neither sees nor produces the nullspace

@@ -34,6 +34,8 @@ struct AmgHierarchy {
   Csr Pdg, Rdg;                   // DG p=1 unknowns x level-0 unknowns, and its transpose
   std::vector<AmgLevel> levels;   // levels[0].A is the coarse-space operator; P/R of level l map l <-> l+1
   std::vector<double> coarse_inv; // dense inverse of the coarsest operator (n x n, row-major)
+  std::vector<double> coarse_dense;  // without the host inverse: the coarsest operator, dense (shifted when singular)
+  bool singular = false;
   int coarse_n = 0;
 };
 
@@ -53,16 +55,27 @@ Csr p0_operator(int K, int Nf, const double* sJ, const double* tau, const int* n
 // ref1: order-1 reference element; geof K x ngeof; e2v K x (dim+1);
 // factor1 K x Np1 (null: 1); tau1, sJ K x Nf; nbr K x Nf; mm: mode/scalar/nodal K x Np1.
 struct RefElement;
+// Sparsity of the continuous P1 operator of a mesh and, per element entry (e, i, j),
+// its position in the CSR values (built once per mesh, reused by every assembly).
+struct P1Plan {
+  int Nv = 0;
+  std::vector<int> ptr, idx, slot;
+};
+P1Plan p1c_plan(int K, int Nv, int Np, const int* e2v);
 void p1c_operator(const RefElement& ref1, int K, int Nv, const double* geof, const int* e2v,
                   const double* factor1, const double* tau1, const double* sJ, const double* nx,
                   const double* ny, const double* nz, const int* nbr,
                   const std::vector<uint8_t>& bc_dirichlet, int mm_mode, double mm_scalar,
-                  const double* mm1, Csr* A, Csr* Pdg);
+                  const double* mm1, Csr* A, Csr* Pdg, const P1Plan* plan = nullptr);
 
 // Smoothed-aggregation hierarchy down to at most `coarse_max` unknowns.
 // `singular` adds a tiny diagonal shift before inverting the coarsest level
 // (pure Neumann problems, whose constant nullspace the outer solver projects out).
-AmgHierarchy build_amg(const Csr& A0, const Csr& Pdg, int coarse_max, double strength, bool singular);
+// host_inverse = false leaves the inversion to the caller (coarse_dense holds the
+// matrix to invert, with the 1e-8 relative diagonal shift of a singular problem;
+// the inverse is then projected onto the complement of the constants).
+AmgHierarchy build_amg(const Csr& A0, const Csr& Pdg, int coarse_max, double strength, bool singular,
+                       bool host_inverse = true);
 
 Csr transpose(const Csr& A);
 Csr spgemm(const Csr& A, const Csr& B);

@@ -91,7 +91,7 @@ ApplyArgs<T> args_of(const sipg_op* op, const T* x, T* y) {
   a.beta = T(0);
   a.c = y;
   a.tcg = f64 ? (const T*)op->mesh->tcg64.p : (const T*)op->mesh->tcg32.p;
-  a.tcgen05 = op->kernel == 0;
+  a.tcgen05 = op->kernel == 3;
   return a;
 }
 
@@ -100,7 +100,7 @@ template <typename T>
 void apply_static(const sipg_op* op, const T* x, T* y, cudaStream_t s) {
   constexpr bool f64 = std::is_same<T, double>::value;
   const ApplyArgs<T> a = args_of<T>(op, x, y);
-  const bool tc = (op->kernel == 0 || op->kernel == 2) && op->ncomp == 1 &&
+  const bool tc = (op->kernel == 0 || op->kernel >= 2) && op->ncomp == 1 &&
                   (f64 ? op->dref->tc_ok64 : op->dref->tc_ok32);
   if (!tc) {  // the single-pass kernels need no scratch
     SIPG_CUDA(launch_apply<T>(op->mesh->dim, op->order, a, num_sms(), s));

@@ -10,7 +10,8 @@
 //
 //   pass 1: T = x . B1f (B1f: per face f and direction r the rows of D_r at the
 //           face nodes), g = f(m) sum_r c_r(f) T_r at the face nodes, trace
-//           record (u, g) per element face.
+//           record (u, g) per element face, written in the face-node order of
+//           the neighbour that reads it (so pass 2 reads it without permuting).
 //   pass 2: one MMA gives the reference gradients gr_r = x . D_r^T and the own
 //           face traces T; each thread row then builds
 //             w_r = J f sum_s K_rs gr_s                 (K = G G^T)
@@ -67,22 +68,25 @@ struct T5 {
   static constexpr int OFF_MM = OFF_F + NF * KFACE;
   static constexpr int K2 = rup5(OFF_MM + NP, 8);
   // trace records: the mma.sync kernels' layout (u at [0, NFP), g at [TRP, TRP + NFP))
-  static constexpr int TRP = rup5(NFP, 2), TR = rup5(2 * TRP, 4);
+  static constexpr int TRP = rup5(NFP, 2), TR = rup5(2 * TRP, 4), TRV = TR / 4;
   // constant blob (floats, MMA layout): B1 (N1 x K1), B2 (N2 x K2)
   static constexpr int CB1 = 0, CB2 = N1 * K1, CALL = CB2 + N2 * K2;
   // geometry blocks of the mma.sync kernels (launch_tc_geom, FP32: tiles of 16 elements)
   static constexpr int GTE = 16, GROWS = 24, GBLK = GROWS * GTE;
-  // shared memory (bytes)
+  static constexpr int XS = NP | 1;             // row stride of the staged x / factor rows (odd: no bank conflicts)
+  // pass-2 shared memory (bytes): constants, operands, x and factor rows, one
+  // neighbour trace record per thread, the int8 tables, barriers
   static constexpr int SB1 = 0, SB2 = SB1 + N1 * K1 * 4, SA1 = SB2 + N2 * K2 * 4, SA2 = SA1 + kM * K1 * 4;
-  static constexpr int SG = SA2 + kM * K2 * 4, STAU = SG + (kM / GTE) * GBLK * 4, SNBR = STAU + kM * NF * 4;
-  static constexpr int SCODE = SNBR + kM * NF * 4, SITAB = SCODE + kM * 4;
+  static constexpr int SX = SA2 + kM * K2 * 4, SF = SX + kM * XS * 4;
+  static constexpr int SITAB = SF + kM * XS * 4;
   static constexpr int SBAR = rup5(SITAB + NF * NFP + 6 * NFP, 16), SMEM2 = SBAR + 32;
-  // pass 1: face rows of B1, x, geometry
-  static constexpr int P1B = 0, P1A = P1B + NF * FT * K1 * 4, P1G = P1A + kM * K1 * 4;
-  static constexpr int P1I = P1G + (kM / GTE) * GBLK * 4, P1BAR = rup5(P1I + NF * NFP, 16), SMEM1 = P1BAR + 32;
+  // pass 1: face rows of B1, x operand, x and factor rows, one record per thread
+  // (reordered there), the int8 tables
+  static constexpr int P1B = 0, P1A = P1B + NF * FT * K1 * 4, P1X = P1A + kM * K1 * 4, P1F = P1X + kM * XS * 4;
+  static constexpr int P1S = P1F + kM * XS * 4, P1I = P1S + kThreads * TR * 4;
+  static constexpr int P1BAR = rup5(P1I + NF * NFP + 6 * NFP, 16), SMEM1 = P1BAR + 32;
   static constexpr int TMEM2 = N1 + N2 <= 256 ? 256 : 512;
   static constexpr int TMEM1 = NF * FT <= 128 ? 128 : 256;
-  static_assert(NP % 4 == 0 || P != 3, "row chunks");
   static_assert(KFACE % 4 == 0, "face sections are whole 16-byte chunks");
   static_assert(N1 <= 256 && N1 % 16 == 0 && N2 % 16 == 0, "one MMA per K step");
   static_assert(FT % 16 == 0, "TMEM loads of a face group");
@@ -162,95 +166,196 @@ __device__ __forceinline__ void copy_f4(float* dst, const float* src, int n, int
     *reinterpret_cast<float4*>(dst + i) = *reinterpret_cast<const float4*>(src + i);
 }
 
-// Stage a tile: x into the A1 operand (zero past the tile, past Np and at the
-// pinned DOF), the geometry blocks of its elements (zero past the mesh).
+// Face node -> volume node maps of the reference element (FMASK), as compile-time
+// tables so that the flux code reads the staged rows at fixed offsets. The host
+// checks them against the element the library builds (tc5_prepare); an order
+// whose table differs is not run on these kernels.
 template <int P>
-__device__ __forceinline__ void stage_x(const ApplyArgs<float>& a, float* sA1, int e0, int ne, int tid) {
-  using X = T5<P>;
-  for (int q = tid; q < kM * X::K1; q += kThreads) {
-    const int m = q / X::K1, k = q % X::K1;
-    float v = 0.0f;
-    if (m < ne && k < X::NP && !(e0 + m == a.pin_elem && k == a.pin_node)) v = a.x[(size_t)(e0 + m) * X::NP + k];
-    sA1[opidx(kM, m, k)] = tf32(v);
+struct FaceMask;
+template <>
+struct FaceMask<3> {
+  __host__ __device__ static constexpr int at(int f, int j) {
+    constexpr int8_t v[4][10] = {{9, 8, 6, 3, 7, 2, 5, 4, 1, 0},
+                                 {19, 17, 12, 3, 16, 2, 11, 10, 1, 0},
+                                 {19, 18, 15, 9, 17, 8, 14, 12, 6, 3},
+                                 {19, 18, 15, 9, 16, 7, 13, 10, 4, 0}};
+    return v[f][j];
   }
-}
+};
+
+// A tile's x and factor rows: thread m of half 0 loads row m of x, of half 1 row m
+// of the factor, into registers ahead of use (the next tile's while the current
+// one finishes); they are stored as rows of stride XS (zero past the tile; the
+// pinned DOF is zero, as in the operator's column) and the A1 operand (TF32,
+// zero past Np) is built from the x rows.
 template <int P>
-__device__ __forceinline__ void stage_geom(const ApplyArgs<float>& a, float* sG, int e0, int tid) {
+struct Rows {
+  float v[T5<P>::NP];
+};
+
+template <int P>
+__device__ __forceinline__ void load_rows(const ApplyArgs<float>& a, int e0, int ne, int m, int half, Rows<P>& r) {
   using X = T5<P>;
-  const int nt16 = (a.K + X::GTE - 1) / X::GTE;
-  const int b0 = e0 / X::GTE;
-  const int nvalid = max(0, min(kM / X::GTE, nt16 - b0)) * X::GBLK;
-  for (int i = tid * 4; i < (kM / X::GTE) * X::GBLK; i += kThreads * 4) {
-    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (i < nvalid) v = *reinterpret_cast<const float4*>(a.tcg + (size_t)b0 * X::GBLK + i);
-    *reinterpret_cast<float4*>(sG + i) = v;
+  constexpr int NP = X::NP;
+  const float* src = half == 0 ? a.x : a.factor;
+  if (half == 1 && !src) {
+#pragma unroll
+    for (int i = 0; i < NP; ++i) r.v[i] = 1.f;
+    return;
   }
-}
-// geometry row q of element m of the tile
-template <int P>
-__device__ __forceinline__ float geo(const float* sG, int q, int m) {
-  using X = T5<P>;
-  return sG[(m / X::GTE) * X::GBLK + q * X::GTE + (m % X::GTE)];
+  if (m >= ne) {
+#pragma unroll
+    for (int i = 0; i < NP; ++i) r.v[i] = 0.f;
+    return;
+  }
+  const float* row = src + (size_t)(e0 + m) * NP;
+  if constexpr (NP % 4 == 0) {
+#pragma unroll
+    for (int c = 0; c < NP / 4; ++c) {
+      const float4 q = __ldg(reinterpret_cast<const float4*>(row) + c);
+      r.v[4 * c] = q.x;
+      r.v[4 * c + 1] = q.y;
+      r.v[4 * c + 2] = q.z;
+      r.v[4 * c + 3] = q.w;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < NP; ++i) r.v[i] = __ldg(row + i);
+  }
 }
 
-// Face f of element row m: own traces from TMEM (T_r at the face nodes), the
-// neighbour's record, the fluxes; writes the face's A2 section [c_r S | Fu].
 template <int P>
-__device__ __forceinline__ void face_section(const ApplyArgs<float>& a, const float* __restrict__ trace, float* sA2,
-                                            const float* sA1, const float* sG, const float* stau, const int* snbr,
-                                            const uint32_t* scode, const int8_t* fmask, const int8_t* perm,
-                                            uint32_t tcol, int m, int row, int f, bool valid) {
+__device__ __forceinline__ void store_rows(const ApplyArgs<float>& a, const Rows<P>& r, float* sX, float* sF,
+                                           float* sA1, int e0, int m, int half) {
   using X = T5<P>;
-  constexpr int NFP = X::NFP, NF = X::NF;
+  constexpr int NP = X::NP, XS = X::XS;
+  float* dst = (half == 0 ? sX : sF) + m * XS;
+  const int pin = (half == 0 && e0 + m == a.pin_elem) ? a.pin_node : -1;
+#pragma unroll
+  for (int i = 0; i < NP; ++i) dst[i] = i == pin ? 0.f : r.v[i];
+  __syncthreads();
+  // the two threads of row m write alternate 16-byte chunks of its A1 row
+  const float* xr = sX + m * XS;
+#pragma unroll
+  for (int c = half * 4; c < X::K1; c += 8) {
+    float v[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) v[i] = c + i < NP ? xr[c + i] : 0.f;
+    st4(sA1, kM, m, c, v[0], v[1], v[2], v[3]);
+  }
+}
+
+// Element e's column of the per-mesh geometry blocks (rows q at stride GTE).
+template <int P>
+__device__ __forceinline__ const float* geo_col(const float* __restrict__ tcg, int e) {
+  using X = T5<P>;
+  return tcg + (size_t)(e / X::GTE) * X::GBLK + (e % X::GTE);
+}
+
+// Face data of one element face, loaded into registers ahead of use: sJ, c_r,
+// tau, the neighbour (or -(bface+1)) and its trace record.
+template <int P>
+struct FaceIn {
+  float sJ, c[3], tau;
+  int nb;
+  bool dir;
+  float4 rec[T5<P>::TRV];
+};
+
+template <int P>
+__device__ __forceinline__ void load_face(const ApplyArgs<float>& a, const float* __restrict__ trace, const float* g,
+                                          int e, int f, bool valid, FaceIn<P>& d) {
+  using X = T5<P>;
+  constexpr int NF = X::NF, GTE = X::GTE;
+  d.sJ = d.tau = d.c[0] = d.c[1] = d.c[2] = 0.f;
+  d.nb = -1;
+  d.dir = false;
+  if (!valid) return;
+  d.sJ = __ldg(g + (8 + f) * GTE);
+#pragma unroll
+  for (int r = 0; r < 3; ++r) d.c[r] = __ldg(g + (8 + (1 + r) * NF + f) * GTE);
+  d.tau = __ldg(a.tau + (size_t)e * NF + f);
+  d.nb = __ldg(a.nbr + (size_t)e * NF + f);
+  if (d.nb >= 0) {
+    const uint32_t code = __ldg(a.fcode + e);
+    const float4* src = reinterpret_cast<const float4*>(trace + ((size_t)d.nb * NF + ((code >> (8 * f)) & 3)) * X::TR);
+#pragma unroll
+    for (int c = 0; c < X::TRV; ++c) d.rec[c] = __ldg(src + c);
+  } else {
+    d.dir = a.bct[-d.nb - 1] == BC_DIRICHLET;
+  }
+}
+
+// Face F of element row m: own traces from TMEM (T_r at the face nodes), the
+// neighbour's record (already in this face's node order), the fluxes; writes the
+// face's A2 section [c_r S | Fu].
+template <int P, int F>
+__device__ __forceinline__ void face_section(float* sA2, const float* xr, const float* fr, const FaceIn<P>& d,
+                                             uint32_t tcol, int m) {
+  using X = T5<P>;
+  constexpr int NFP = X::NFP;
   float T[X::FT];
 #pragma unroll
   for (int c = 0; c < X::FT; c += 16) tmem_ld16(tcol + c, *reinterpret_cast<float(*)[16]>(&T[c]));
-  float sec[X::KFACE];
-  int nb = -1, code = 0;
-  float sJ = 0.f, tau = 0.f, cr[3] = {0.f, 0.f, 0.f};
-  if (valid) {
-    nb = snbr[m * NF + f];
-    code = (int)scode[m];
-    sJ = geo<P>(sG, 8 + f, m);
-#pragma unroll
-    for (int r = 0; r < 3; ++r) cr[r] = geo<P>(sG, 8 + (1 + r) * NF + f, m);
-    tau = stau[m * NF + f];
-  }
-  bool dir = false;
-  const float* rec = nullptr;
-  int pbase = 0;
-  if (valid && nb >= 0) {
-    rec = trace + ((size_t)nb * NF + ((code >> (8 * f)) & 3)) * X::TR;
-    pbase = ((code >> (8 * f + 2)) & 7) * NFP;
-  } else if (valid) {
-    dir = a.bct[-nb - 1] == BC_DIRICHLET;
-  }
+  const bool inner = d.nb >= 0;
+  const float* rec = reinterpret_cast<const float*>(d.rec);
   tmem_wait_ld();
+  float sec[X::KFACE];
 #pragma unroll
   for (int j = 0; j < NFP; ++j) {
-    const int mj = fmask[f * NFP + j];
-    const float fm = (valid && a.factor) ? __ldg(a.factor + (size_t)row * X::NP + mj) : 1.0f;
-    const float gm = fm * (cr[0] * T[j] + cr[1] * T[NFP + j] + cr[2] * T[2 * NFP + j]);
-    const float um = (valid && !(row == a.pin_elem && mj == a.pin_node)) ? __ldg(a.x + (size_t)row * X::NP + mj) : 0.f;
+    const int mj = FaceMask<P>::at(F, j);
+    const float fm = fr[mj];
+    const float gm = fm * (d.c[0] * T[j] + d.c[1] * T[NFP + j] + d.c[2] * T[2 * NFP + j]);
+    const float um = xr[mj];
     float jump = 0.f, navg = 0.f;
-    if (rec) {
-      const int kk = perm[pbase + j];
-      jump = um - __ldg(rec + kk);
-      navg = 0.5f * (gm - __ldg(rec + X::TRP + kk));
-    } else if (dir) {
+    if (inner) {
+      jump = um - rec[j];
+      navg = 0.5f * (gm - rec[X::TRP + j]);
+    } else if (d.dir) {
       jump = 2.0f * um;
       navg = gm;
     }
     const float h = 0.5f * jump;
-    const float s = -sJ * fm * h;
-    sec[j] = cr[0] * s;
-    sec[NFP + j] = cr[1] * s;
-    sec[2 * NFP + j] = cr[2] * s;
-    sec[3 * NFP + j] = sJ * (tau * h - navg);
+    const float sv = -d.sJ * fm * h;
+    sec[j] = d.c[0] * sv;
+    sec[NFP + j] = d.c[1] * sv;
+    sec[2 * NFP + j] = d.c[2] * sv;
+    sec[3 * NFP + j] = d.sJ * (d.tau * h - navg);
   }
-  const int k0 = X::OFF_F + f * X::KFACE;
+  constexpr int k0 = X::OFF_F + F * X::KFACE;
 #pragma unroll
   for (int c = 0; c < X::KFACE; c += 4) st4(sA2, kM, m, k0 + c, sec[c], sec[c + 1], sec[c + 2], sec[c + 3]);
+}
+
+// Pass-1 record of face F: u and g at the face nodes, stored in the face-node
+// order of the neighbour that reads it (position perm_pos[sigma][j] holds face
+// node j; sigma: this face's orientation code), through the thread's slot.
+template <int P, int F>
+__device__ __forceinline__ void trace_record(float* __restrict__ trace, float* slot, const int8_t* perm,
+                                             const float* xr, const float* fr, const float (&cg)[3], int pb,
+                                             uint32_t tcol, size_t e, bool valid) {
+  using X = T5<P>;
+  constexpr int NFP = X::NFP;
+  float T[X::FT];
+#pragma unroll
+  for (int c = 0; c < X::FT; c += 16) tmem_ld16(tcol + c, *reinterpret_cast<float(*)[16]>(&T[c]));
+  tmem_wait_ld();
+#pragma unroll
+  for (int i = NFP; i < X::TRP; ++i) slot[i] = slot[X::TRP + i] = 0.f;
+#pragma unroll
+  for (int i = 2 * X::TRP; i < X::TR; ++i) slot[i] = 0.f;
+#pragma unroll
+  for (int j = 0; j < NFP; ++j) {
+    const int mj = FaceMask<P>::at(F, j);
+    const int pos = pb >= 0 ? perm[pb + j] : j;
+    slot[pos] = xr[mj];
+    slot[X::TRP + pos] = fr[mj] * (cg[0] * T[j] + cg[1] * T[NFP + j] + cg[2] * T[2 * NFP + j]);
+  }
+  if (valid) {
+    float4* dst = reinterpret_cast<float4*>(trace + (e * X::NF + F) * X::TR);
+#pragma unroll
+    for (int c = 0; c < X::TRV; ++c) dst[c] = reinterpret_cast<const float4*>(slot)[c];
+  }
 }
 
 // ---------------------------------------------------------------- pass 1
@@ -258,16 +363,19 @@ template <int P>
 __global__ void __launch_bounds__(kThreads, 2) sipg_tc5_trace(ApplyArgs<float> a, const float* __restrict__ blob,
                                                              float* __restrict__ trace) {
   using X = T5<P>;
-  constexpr int NP = X::NP, NFP = X::NFP, NF = X::NF, K1 = X::K1;
+  constexpr int NFP = X::NFP, NF = X::NF, K1 = X::K1, XS = X::XS, GTE = X::GTE;
   extern __shared__ __align__(128) unsigned char smem[];
   float* sB = reinterpret_cast<float*>(smem + X::P1B);  // face rows of B1: NF*FT x K1
   float* sA1 = reinterpret_cast<float*>(smem + X::P1A);
-  float* sG = reinterpret_cast<float*>(smem + X::P1G);
-  int8_t* fmask = reinterpret_cast<int8_t*>(smem + X::P1I);
+  float* sX = reinterpret_cast<float*>(smem + X::P1X);
+  float* sF = reinterpret_cast<float*>(smem + X::P1F);
+  int8_t* itab = reinterpret_cast<int8_t*>(smem + X::P1I);
+  const int8_t* perm = itab + NF * NFP;
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + X::P1BAR);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + X::P1BAR + 8);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m = 32 * (warp & 3) + lane, half = warp >> 2;
+  float* slot = reinterpret_cast<float*>(smem + X::P1S) + tid * X::TR;
   constexpr int NB = NF * X::FT;
   pdl_trigger();
   // face rows of B1 (rows NG .. N1 of the N1 x K1 operand) as an NB-row operand
@@ -275,7 +383,7 @@ __global__ void __launch_bounds__(kThreads, 2) sipg_tc5_trace(ApplyArgs<float> a
     const int n = q / K1, k = q % K1;
     sB[opidx(NB, n, k)] = blob[X::CB1 + opidx(X::N1, X::NG + n, k)];
   }
-  for (int i = tid; i < NF * NFP; i += kThreads) fmask[i] = a.itab[i];
+  for (int i = tid; i < NF * NFP + 6 * NFP; i += kThreads) itab[i] = a.itab[i];
   if (tid == 0) {
     mbar_init(smem_u32(bar));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -294,14 +402,21 @@ __global__ void __launch_bounds__(kThreads, 2) sipg_tc5_trace(ApplyArgs<float> a
   const int ntiles = (a.K + kM - 1) / kM;
   bool ok = true;
   uint32_t phase = 0;
+  Rows<P> rows;
+  if ((int)blockIdx.x < ntiles) load_rows<P>(a, blockIdx.x * kM, min(kM, a.K - (int)blockIdx.x * kM), m, half, rows);
   for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, phase ^= 1) {
     const int e0 = tile * kM, ne = min(kM, a.K - e0);
-    stage_x<P>(a, sA1, e0, ne, tid);
-    stage_geom<P>(a, sG, e0, tid);
+    const bool valid = m < ne;
+    const int e = e0 + m;
+    store_rows<P>(a, rows, sX, sF, sA1, e0, m, half);
     fence_async_smem();
     tc_before_sync();
     __syncthreads();
     tc_after_sync();
+    {
+      const int next = tile + gridDim.x;
+      if (next < ntiles) load_rows<P>(a, next * kM, min(kM, a.K - next * kM), m, half, rows);
+    }
     if (tid == 0) {
       const uint32_t a0 = smem_u32(sA1), b0 = smem_u32(sB);
 #pragma unroll
@@ -310,46 +425,37 @@ __global__ void __launch_bounds__(kThreads, 2) sipg_tc5_trace(ApplyArgs<float> a
                  idesc_tf32(NB), kk > 0);
       mma_commit(smem_u32(bar));
     }
-    const bool valid = m < ne;
-    ok = __syncthreads_and(mbar_wait(smem_u32(bar), phase)) != 0;  // the whole CTA stops on a timeout
+    // the face geometry and orientation while the MMA runs
+    float cg[2][3];
+    int pb[2] = {-1, -1};
+    const float* g = geo_col<P>(a.tcg, e);
+    const uint32_t code = valid ? __ldg(a.fcode + e) : 0u;
+#pragma unroll
+    for (int fi = 0; fi < 2; ++fi) {
+      const int f = 2 * half + fi;
+#pragma unroll
+      for (int r = 0; r < 3; ++r) cg[fi][r] = valid ? __ldg(g + (8 + (1 + r) * NF + f) * GTE) : 0.f;
+      if (valid && __ldg(a.nbr + (size_t)e * NF + f) >= 0) pb[fi] = (int)((code >> (8 * f + 2)) & 7) * NFP;
+    }
+    // one thread polls the MMA barrier, the others wait at the CTA barrier;
+    // the whole CTA stops on a timeout
+    ok = __syncthreads_and(tid == 0 ? mbar_wait(smem_u32(bar), phase) : true) != 0;
     tc_after_sync();
     if (!ok) {
       if (tid == 0) atomicAdd(&g_tc5_timeouts, 1u);
       break;
     }
-#pragma unroll
-    for (int fi = 0; fi < 2; ++fi) {
-      const int f = 2 * half + fi;
-      float T[X::FT];
-#pragma unroll
-      for (int c = 0; c < X::FT; c += 16)
-        tmem_ld16(lane_base + f * X::FT + c, *reinterpret_cast<float(*)[16]>(&T[c]));
-      tmem_wait_ld();
-      float c0 = 0.f, c1 = 0.f, c2 = 0.f;
-      if (valid) {
-        c0 = geo<P>(sG, 8 + NF + f, m);
-        c1 = geo<P>(sG, 8 + 2 * NF + f, m);
-        c2 = geo<P>(sG, 8 + 3 * NF + f, m);
-      }
-      float rec[X::TR];
-#pragma unroll
-      for (int i = 0; i < X::TR; ++i) rec[i] = 0.f;
-#pragma unroll
-      for (int j = 0; j < NFP; ++j) {
-        const int mj = fmask[f * NFP + j];
-        rec[j] = valid ? a.x[(size_t)(e0 + m) * NP + mj] * ((e0 + m == a.pin_elem && mj == a.pin_node) ? 0.f : 1.f)
-                       : 0.f;
-        const float fm = (valid && a.factor) ? __ldg(a.factor + (size_t)(e0 + m) * NP + mj) : 1.0f;
-        rec[X::TRP + j] = fm * (c0 * T[j] + c1 * T[NFP + j] + c2 * T[2 * NFP + j]);
-      }
-      if (valid) {
-        float4* dst = reinterpret_cast<float4*>(trace + ((size_t)(e0 + m) * NF + f) * X::TR);
-#pragma unroll
-        for (int c = 0; c < X::TR / 4; ++c) dst[c] = make_float4(rec[4 * c], rec[4 * c + 1], rec[4 * c + 2], rec[4 * c + 3]);
-      }
+    const float* xr = sX + m * XS;
+    const float* fr = sF + m * XS;
+    if (half == 0) {
+      trace_record<P, 0>(trace, slot, perm, xr, fr, cg[0], pb[0], lane_base + 0 * X::FT, (size_t)e, valid);
+      trace_record<P, 1>(trace, slot, perm, xr, fr, cg[1], pb[1], lane_base + 1 * X::FT, (size_t)e, valid);
+    } else {
+      trace_record<P, 2>(trace, slot, perm, xr, fr, cg[0], pb[0], lane_base + 2 * X::FT, (size_t)e, valid);
+      trace_record<P, 3>(trace, slot, perm, xr, fr, cg[1], pb[1], lane_base + 3 * X::FT, (size_t)e, valid);
     }
     tc_before_sync();
-    __syncthreads();  // the next tile's staging overwrites sA1 / sG, its MMA the accumulator
+    __syncthreads();  // the next tile's staging overwrites the rows, its MMA the accumulator
     tc_after_sync();
   }
   tc_before_sync();
@@ -362,16 +468,14 @@ template <int P>
 __global__ void __launch_bounds__(kThreads, 1) sipg_tc5_apply(ApplyArgs<float> a, const float* __restrict__ blob,
                                                              const float* __restrict__ trace) {
   using X = T5<P>;
-  constexpr int NP = X::NP, NFP = X::NFP, NF = X::NF, K1 = X::K1, N1 = X::N1, N2 = X::N2;
+  constexpr int NP = X::NP, NFP = X::NFP, NF = X::NF, K1 = X::K1, N1 = X::N1, N2 = X::N2, XS = X::XS;
   extern __shared__ __align__(128) unsigned char smem[];
   float* sB1 = reinterpret_cast<float*>(smem + X::SB1);
   float* sB2 = reinterpret_cast<float*>(smem + X::SB2);
   float* sA1 = reinterpret_cast<float*>(smem + X::SA1);
   float* sA2 = reinterpret_cast<float*>(smem + X::SA2);
-  float* sG = reinterpret_cast<float*>(smem + X::SG);
-  float* stau = reinterpret_cast<float*>(smem + X::STAU);
-  int* snbr = reinterpret_cast<int*>(smem + X::SNBR);
-  uint32_t* scode = reinterpret_cast<uint32_t*>(smem + X::SCODE);
+  float* sX = reinterpret_cast<float*>(smem + X::SX);
+  float* sF = reinterpret_cast<float*>(smem + X::SF);
   int8_t* itab = reinterpret_cast<int8_t*>(smem + X::SITAB);
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + X::SBAR);  // [0] MMA 1, [1] MMA 2
   uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + X::SBAR + 16);
@@ -397,24 +501,18 @@ __global__ void __launch_bounds__(kThreads, 1) sipg_tc5_apply(ApplyArgs<float> a
   tc_after_sync();
   const uint32_t tmem = *tslot;
   const uint32_t lane_base = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
-  const int8_t* fmask = itab;
-  const int8_t* perm = itab + NF * NFP;
   const bool has_mm = a.mm_mode != MM_NONE;
   const int k2 = has_mm ? X::K2 : X::OFF_MM;
   const int ntiles = (a.K + kM - 1) / kM;
   bool ok = true;
   uint32_t phase = 0;
+  Rows<P> rows;
+  if ((int)blockIdx.x < ntiles) load_rows<P>(a, blockIdx.x * kM, min(kM, a.K - (int)blockIdx.x * kM), m, half, rows);
   for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, phase ^= 1) {
     const int e0 = tile * kM, ne = min(kM, a.K - e0);
     const bool valid = m < ne;
-    stage_x<P>(a, sA1, e0, ne, tid);
-    stage_geom<P>(a, sG, e0, tid);
-    for (int i = tid; i < kM * NF; i += kThreads) {
-      const bool v = i < ne * NF;
-      stau[i] = v ? a.tau[(size_t)e0 * NF + i] : 0.f;
-      snbr[i] = v ? a.nbr[(size_t)e0 * NF + i] : -1;
-    }
-    for (int i = tid; i < kM; i += kThreads) scode[i] = i < ne ? a.fcode[e0 + i] : 0u;
+    const int e = e0 + m;
+    store_rows<P>(a, rows, sX, sF, sA1, e0, m, half);
     fence_async_smem();
     tc_before_sync();
     __syncthreads();
@@ -427,71 +525,80 @@ __global__ void __launch_bounds__(kThreads, 1) sipg_tc5_apply(ApplyArgs<float> a
                  idesc_tf32(N1), kk > 0);
       mma_commit(smem_u32(bar));
     }
-    // per-row data while MMA 1 runs
-    float fac[NP];
+    // this thread's faces (half 0: face 0 and the volume terms, half 1: faces 1..3)
+    // and geometry, loaded while MMA 1 runs
+    const float* g = geo_col<P>(a.tcg, e);
+    constexpr int NFH = NF - 1;
+    FaceIn<P> fd[NFH];
+    if (half == 0) {
+      load_face<P>(a, trace, g, e, 0, valid, fd[0]);
+    } else {
 #pragma unroll
-    for (int i = 0; i < NP; ++i)
-      fac[i] = (half == 0 && valid && a.factor) ? __ldg(a.factor + (size_t)(e0 + m) * NP + i) : 1.0f;
+      for (int i = 0; i < NFH; ++i) load_face<P>(a, trace, g, e, 1 + i, valid, fd[i]);
+    }
     float J = 0.f, Km[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
     if (half == 0 && valid) {
-      J = geo<P>(sG, 0, m);
+      J = __ldg(g);
       int q = 1;
 #pragma unroll
       for (int r = 0; r < 3; ++r)
 #pragma unroll
-        for (int s = r; s < 3; ++s) {
-          Km[r][s] = Km[s][r] = geo<P>(sG, q, m);
+        for (int s2 = r; s2 < 3; ++s2) {
+          Km[r][s2] = Km[s2][r] = __ldg(g + q * X::GTE);
           ++q;
         }
     }
-    ok = __syncthreads_and(mbar_wait(smem_u32(bar), phase)) != 0;  // the whole CTA stops on a timeout
+    // one thread polls the MMA barrier, the others wait at the CTA barrier;
+    // the whole CTA stops on a timeout
+    ok = __syncthreads_and(tid == 0 ? mbar_wait(smem_u32(bar), phase) : true) != 0;
     tc_after_sync();
     if (!ok) {
       if (tid == 0) atomicAdd(&g_tc5_timeouts, 1u);
       break;
     }
+    const float* xr = sX + m * XS;
+    const float* fr = sF + m * XS;
     if (half == 0) {
-      // w_r = J f sum_s K_rs gr_s, four nodes (one 16-byte chunk per direction) at a time
+      // w_r = J f sum_s K_rs gr_s
       float gr[X::NG];
 #pragma unroll
       for (int c = 0; c < X::NG; c += 16) tmem_ld16(lane_base + c, *reinterpret_cast<float(*)[16]>(&gr[c]));
       tmem_wait_ld();
-      float wv[3 * NP];
-#pragma unroll
-      for (int n = 0; n < NP; ++n) {
-        const float fJ = J * fac[n];
-        const float g0 = gr[n], g1 = gr[NP + n], g2 = gr[2 * NP + n];
-#pragma unroll
-        for (int r = 0; r < 3; ++r) wv[r * NP + n] = fJ * (Km[r][0] * g0 + Km[r][1] * g1 + Km[r][2] * g2);
-      }
 #pragma unroll
       for (int c = 0; c < X::OFF_F; c += 4) {
         float v[4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) v[i] = c + i < 3 * NP ? wv[c + i] : 0.f;
+        for (int i = 0; i < 4; ++i) {
+          const int k = c + i;
+          v[i] = 0.f;
+          if (k < 3 * NP) {
+            const int r = k / NP, n = k % NP;
+            v[i] = J * fr[n] * (Km[r][0] * gr[n] + Km[r][1] * gr[NP + n] + Km[r][2] * gr[2 * NP + n]);
+          }
+        }
         st4(sA2, kM, m, c, v[0], v[1], v[2], v[3]);
       }
       if (has_mm) {
-        float mv[X::K2 - X::OFF_MM];
 #pragma unroll
-        for (int n = 0; n < X::K2 - X::OFF_MM; ++n) {
-          float v = 0.f;
-          if (n < NP && valid) {
-            const float mmv = a.mm_mode == MM_SCALAR ? a.mm_scalar : a.mm[(size_t)(e0 + m) * NP + n];
-            v = J * mmv * sA1[opidx(kM, m, n)];
+        for (int c = 0; c < X::K2 - X::OFF_MM; c += 4) {
+          float v[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const int n = c + i;
+            v[i] = 0.f;
+            if (n < NP && valid) {
+              const float mmv = a.mm_mode == MM_SCALAR ? a.mm_scalar : __ldg(a.mm + (size_t)e * NP + n);
+              v[i] = J * mmv * xr[n];
+            }
           }
-          mv[n] = v;
+          st4(sA2, kM, m, X::OFF_MM + c, v[0], v[1], v[2], v[3]);
         }
-#pragma unroll
-        for (int c = 0; c < X::K2 - X::OFF_MM; c += 4) st4(sA2, kM, m, X::OFF_MM + c, mv[c], mv[c + 1], mv[c + 2], mv[c + 3]);
       }
-      face_section<P>(a, trace, sA2, sA1, sG, stau, snbr, scode, fmask, perm, lane_base + X::NG, m, e0 + m, 0,
-                      valid);
+      face_section<P, 0>(sA2, xr, fr, fd[0], lane_base + X::NG, m);
     } else {
-#pragma unroll 1
-      for (int f = 1; f < NF; ++f)
-        face_section<P>(a, trace, sA2, sA1, sG, stau, snbr, scode, fmask, perm, lane_base + X::NG + f * X::FT,
-                        m, e0 + m, f, valid);
+      face_section<P, 1>(sA2, xr, fr, fd[0], lane_base + X::NG + 1 * X::FT, m);
+      face_section<P, 2>(sA2, xr, fr, fd[1], lane_base + X::NG + 2 * X::FT, m);
+      face_section<P, 3>(sA2, xr, fr, fd[2], lane_base + X::NG + 3 * X::FT, m);
     }
     fence_async_smem();
     tc_before_sync();
@@ -504,41 +611,50 @@ __global__ void __launch_bounds__(kThreads, 1) sipg_tc5_apply(ApplyArgs<float> a
                  idesc_tf32(N2), kk > 0);
       mma_commit(smem_u32(bar + 1));
     }
-    // c for the epilogue while MMA 2 runs
-    constexpr int HALFN = N2 / 2;
-    const int n0 = half * HALFN;
-    float yold[HALFN];
-#pragma unroll
-    for (int i = 0; i < HALFN; ++i)
-      yold[i] = (a.beta != 0.f && valid && n0 + i < NP) ? a.c[(size_t)(e0 + m) * NP + n0 + i] : 0.f;
-    ok = __syncthreads_and(mbar_wait(smem_u32(bar + 1), phase)) != 0;
+    // the next tile's rows, and c for the epilogue (into the factor rows, free
+    // now), while MMA 2 runs
+    {
+      const int next = tile + gridDim.x;
+      if (next < ntiles) load_rows<P>(a, next * kM, min(kM, a.K - next * kM), m, half, rows);
+    }
+    if (a.beta != 0.f)
+      for (int i = tid; i < ne * NP; i += kThreads) {
+        const int mm_ = i / NP;
+        sF[mm_ * XS + (i - mm_ * NP)] = __ldg(a.c + (size_t)e0 * NP + i);
+      }
+    ok = __syncthreads_and(tid == 0 ? mbar_wait(smem_u32(bar + 1), phase) : true) != 0;
     tc_after_sync();
     if (!ok) {
       if (tid == 0) atomicAdd(&g_tc5_timeouts, 1u);
       break;
     }
+    constexpr int HALFN = N2 / 2;
+    const int n0 = half * HALFN;
     float acc[HALFN];
 #pragma unroll
     for (int c = 0; c < HALFN; c += 16)
       tmem_ld16(lane_base + N1 + n0 + c, *reinterpret_cast<float(*)[16]>(&acc[c]));
     tmem_wait_ld();
-    if (valid) {
-      float* yrow = a.y + (size_t)(e0 + m) * NP;
-      const bool pin_row = e0 + m == a.pin_elem;
+    // y row into the x rows (free now), then a coalesced store of the tile
+    float* yr = sX + m * XS;
 #pragma unroll
-      for (int i = 0; i < HALFN; ++i) {
-        const int n = n0 + i;
-        if (n < NP) {
-          float v = acc[i];
-          if (pin_row && n == a.pin_node) v = a.pin_scale * a.x[(size_t)(e0 + m) * NP + n];
-          v *= a.alpha;
-          if (a.beta != 0.f) v += a.beta * yold[i];
-          yrow[n] = v;
-        }
+    for (int i = 0; i < HALFN; ++i) {
+      const int n = n0 + i;
+      if (n < NP) {
+        float v = acc[i];
+        if (e == a.pin_elem && n == a.pin_node) v = a.pin_scale * __ldg(a.x + (size_t)e * NP + n);
+        v *= a.alpha;
+        if (a.beta != 0.f) v += a.beta * fr[n];
+        yr[n] = v;
       }
     }
+    __syncthreads();
+    for (int i = tid; i < ne * NP; i += kThreads) {
+      const int mm_ = i / NP;
+      a.y[(size_t)e0 * NP + i] = sX[mm_ * XS + (i - mm_ * NP)];
+    }
     tc_before_sync();
-    __syncthreads();  // smem operands and accumulators are free for the next tile
+    __syncthreads();  // shared operands, rows and accumulators are free for the next tile
     tc_after_sync();
   }
   tc_before_sync();
@@ -619,7 +735,11 @@ void build_t(const RefElement& r, std::vector<double>& out) {
 
 }  // namespace
 
-bool tc5_supported(int dim, int order) { return dim == 3 && order == 3; }
+// Orders whose reference element matched the compile-time face masks (set by
+// build_tc5_consts, which runs before any apply of that order).
+static std::atomic<int> g_tc5_ready[5];
+
+bool tc5_supported(int dim, int order) { return dim == 3 && order == 3 && g_tc5_ready[order].load() == 1; }
 
 size_t tc5_const_values(int dim, int order) {
   if (dim == 3 && order == 3) return T5<3>::CALL;
@@ -627,8 +747,16 @@ size_t tc5_const_values(int dim, int order) {
 }
 
 void build_tc5_consts(int dim, int order, const RefElement& r, std::vector<double>& out) {
-  if (dim == 3 && order == 3) build_t<3>(r, out);
-  else out.clear();
+  out.clear();
+  if (dim != 3 || order != 3) return;
+  for (int f = 0; f < 4; ++f)
+    for (int j = 0; j < T5<3>::NFP; ++j)
+      if (r.fmask[f * T5<3>::NFP + j] != FaceMask<3>::at(f, j)) {
+        g_tc5_ready[order].store(-1);
+        return;
+      }
+  build_t<3>(r, out);
+  g_tc5_ready[order].store(1);
 }
 
 cudaError_t launch_apply_tc5(int dim, int order, const ApplyArgs<float>& a, const float* blob, float* trace,

@@ -267,29 +267,41 @@ void bsr_assemble(sipg_op* op, BsrOp& B, bool want32, cudaStream_t s, const doub
   if (op->ncomp != 1) throw Error(SIPG_INVALID_ARG, "assembled blocks need a scalar operator");
   sipg_mesh* m = op->mesh;
   const int K = m->K, Np = op->Np, NF = m->dim + 1;
-  const Mesh& h = m->host_order(1);
-  int nc = 0;
-  std::vector<int> col = distance2_colours(K, NF, h.nbr.data(), &nc);
-  std::vector<int> off(nc + 1, 0), list(K);
-  for (int e = 0; e < K; ++e) ++off[col[e] + 1];
-  for (int c = 0; c < nc; ++c) off[c + 1] += off[c];
+  // the colouring depends on the mesh only: built once, kept on the mesh
   {
-    std::vector<int> fill(off.begin(), off.end() - 1);
-    for (int e = 0; e < K; ++e) list[fill[col[e]]++] = e;
+    std::lock_guard<std::mutex> lk(m->probe_mu);
+    if (m->probe_off.empty()) {
+      const Mesh& h = m->host_order(1);
+      int ncol = 0;
+      std::vector<int> col = distance2_colours(K, NF, h.nbr.data(), &ncol);
+      std::vector<int> o(ncol + 1, 0), list(K);
+      for (int e = 0; e < K; ++e) ++o[col[e] + 1];
+      for (int c = 0; c < ncol; ++c) o[c + 1] += o[c];
+      std::vector<int> fill(o.begin(), o.end() - 1);
+      for (int e = 0; e < K; ++e) list[fill[col[e]]++] = e;
+      DevBuf dl((size_t)K * sizeof(int));
+      dl.upload(list.data(), (size_t)K * sizeof(int));
+      m->probe_list = std::move(dl);
+      m->probe_off = std::move(o);
+    }
   }
+  const std::vector<int>& off = m->probe_off;
+  const int nc = (int)off.size() - 1;
   B.K = K;
   B.Np = Np;
   B.NF = NF;
   B.dim = m->dim;
   B.nbr = m->nbr.as<int>();
   const size_t nv = (size_t)(NF + 1) * Np * Np * K;
-  B.v64 = DevBuf(nv * sizeof(double));
+  ensure(B.v64, nv * sizeof(double));
   SIPG_CUDA(cudaMemsetAsync(B.v64.p, 0, nv * sizeof(double), s));
-  DevBuf dl((size_t)K * sizeof(int)), x((size_t)K * Np * sizeof(double)), y((size_t)K * Np * sizeof(double));
-  SIPG_CUDA(cudaMemcpyAsync(dl.p, list.data(), (size_t)K * sizeof(int), cudaMemcpyHostToDevice, s));
+  ensure(B.probe_x, (size_t)K * Np * sizeof(double));
+  ensure(B.probe_y, (size_t)K * Np * sizeof(double));
+  DevBuf& x = B.probe_x;
+  DevBuf& y = B.probe_y;
   for (int c = 0; c < nc; ++c) {
     const int n = off[c + 1] - off[c];
-    const int* lc = dl.as<int>() + off[c];
+    const int* lc = m->probe_list.as<int>() + off[c];
     for (int i = 0; i < Np; ++i) {
       SIPG_CUDA(cudaMemsetAsync(x.p, 0, (size_t)K * Np * sizeof(double), s));
       k_probe_set<<<grid_of(n), 256, 0, s>>>(x.as<double>(), lc, n, i, Np);
@@ -302,31 +314,29 @@ void bsr_assemble(sipg_op* op, BsrOp& B, bool want32, cudaStream_t s, const doub
   }
   const bool half = want32 && Np % 2 == 0;  // two rows per thread in k_bsr16
   if (half) {
-    B.v16 = DevBuf(nv * sizeof(__half));
-    B.scale16 = DevBuf((size_t)K * sizeof(float));
+    ensure(B.v16, nv * sizeof(__half));
+    ensure(B.scale16, (size_t)K * sizeof(float));
     k_bsr16_pack<<<grid_of(K), 256, 0, s>>>(B.v64.as<double>(), K, Np, NF + 1, B.v16.as<__half>(),
                                             B.scale16.as<float>());
     note_launch();
     if (binv_rows) {
-      DevBuf c64(nv * sizeof(double));
+      ensure(B.c64, nv * sizeof(double));
+      DevBuf& c64 = B.c64;
       k_bsr_precond<<<grid_of(nv), 256, 0, s>>>(B.v64.as<double>(), binv_rows, K, Np, NF + 1, binv_sym ? 1 : 0,
                                                 c64.as<double>());
       note_launch();
-      B.c16 = DevBuf(nv * sizeof(__half));
-      B.cscale16 = DevBuf((size_t)K * sizeof(float));
+      ensure(B.c16, nv * sizeof(__half));
+      ensure(B.cscale16, (size_t)K * sizeof(float));
       k_bsr16_pack<<<grid_of(K), 256, 0, s>>>(c64.as<double>(), K, Np, NF + 1, B.c16.as<__half>(),
                                               B.cscale16.as<float>());
       note_launch();
-      SIPG_CUDA(cudaStreamSynchronize(s));  // c64 is freed on scope exit
     }
   } else if (want32) {
-    B.v32 = DevBuf(nv * sizeof(float));
+    ensure(B.v32, nv * sizeof(float));
     k_d2f<<<grid_of(nv), 256, 0, s>>>(B.v32.as<float>(), B.v64.as<double>(), nv);
     note_launch();
   }
   SIPG_CUDA(cudaGetLastError());
-  SIPG_CUDA(cudaStreamSynchronize(s));  // the probe buffers are freed on return
-  if (half) B.v64 = DevBuf();            // the FP32 V-cycle reads the FP16 copy only
 }
 
 template <typename T>

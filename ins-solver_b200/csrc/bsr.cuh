@@ -36,6 +36,7 @@ struct BsrOp {
   // element row), same layout and scaling as v16: one kernel per Chebyshev step
   // (k_bsr16_cheb) then updates the preconditioned residual directly
   DevBuf c16, cscale16;
+  DevBuf probe_x, probe_y, c64;  // assembly workspace, kept for the next set-up
   const int* nbr = nullptr;  // mesh K x NF (device)
 };
 

@@ -39,6 +39,7 @@
 
 #include "../../include/sipg_b200.h"
 #include "capi_util.hpp"
+#include "pdl.cuh"
 #include "vecops.cuh"
 
 namespace sipg {
@@ -914,6 +915,95 @@ void pressure_rhs_device(sipg_mesh* m, int order, double dt, double b0, double b
   }
 }
 
+// Viscous right-hand side of the two-phase time step in one pass
+// (MPINSSolver3D::viscosity, src/solvers/3d/mp_ins_solver.cpp:669-694:
+// mp_ins_3d_vis_0 then mesh->mass on each component): per element
+//   rhs_c = J M (fact0 rho u_c)  (c = 0 .. dim-1),   mm_factor = fact1 rho.
+// A block takes 32 elements: their rho and velocity rows are staged with
+// coalesced loads, thread (c, e) applies M (shared, broadcast reads) to one
+// component of one element, and the rows go back coalesced.
+template <int NP, int DIM>
+__global__ void __launch_bounds__(96) k_vis_rhs(int K, const double* __restrict__ Mm, int ldm,
+                                                 const double* __restrict__ geof, int ngeof, double fact0,
+                                                 double fact1, const double* __restrict__ rho,
+                                                 const double* __restrict__ vel, double* __restrict__ rhs,
+                                                 double* __restrict__ mm) {
+  constexpr int EB = 32;
+  __shared__ double sM[NP * NP];
+  __shared__ double sr[EB * NP];
+  __shared__ double sv[3 * EB * NP];
+  for (int i = threadIdx.x; i < NP * NP; i += blockDim.x) sM[i] = Mm[(i / NP) * ldm + i % NP];  // set-up data
+  pdl_enter();
+  for (int e0 = blockIdx.x * EB; e0 < K; e0 += gridDim.x * EB) {
+    const int ne = min(EB, K - e0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < ne * NP; i += blockDim.x) {
+      const double r = rho[(size_t)e0 * NP + i];
+      sr[i] = r;
+      mm[(size_t)e0 * NP + i] = fact1 * r;
+    }
+    for (int c = 0; c < DIM; ++c)
+      for (int i = threadIdx.x; i < ne * NP; i += blockDim.x)
+        sv[c * EB * NP + i] = vel[((size_t)c * K + e0) * NP + i];
+    __syncthreads();
+    const int c = threadIdx.x / EB, el = threadIdx.x % EB;
+    if (c < DIM && el < ne) {
+      double w[NP];
+      const double* ur = sv + c * EB * NP + el * NP;
+      const double* rr = sr + el * NP;
+#pragma unroll
+      for (int j = 0; j < NP; ++j) w[j] = fact0 * rr[j] * ur[j];
+      const double J = geof[(size_t)(e0 + el) * ngeof + ngeof - 1];
+      double* out = sv + c * EB * NP + el * NP;  // each thread overwrites only its own row
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        double acc = 0.0;
+#pragma unroll
+        for (int j = 0; j < NP; ++j) acc += sM[i * NP + j] * w[j];
+        out[i] = J * acc;
+      }
+    }
+    __syncthreads();
+    for (int cc = 0; cc < DIM; ++cc)
+      for (int i = threadIdx.x; i < ne * NP; i += blockDim.x)
+        rhs[((size_t)cc * K + e0) * NP + i] = sv[cc * EB * NP + i];
+  }
+}
+
+template <int DIM, int P>
+void launch_vis_rhs(sipg_mesh* m, const double* Mm, int ldm, double fact0, double fact1, const double* rho,
+                    const double* vel, double* rhs, double* mm, cudaStream_t s) {
+  constexpr int NP = DIM == 2 ? (P + 1) * (P + 2) / 2 : (P + 1) * (P + 2) * (P + 3) / 6;
+  const int grid = std::max(1, std::min((m->K + 31) / 32, 148 * 16));
+  SIPG_CUDA(pdl_launch(k_vis_rhs<NP, DIM>, dim3(grid), dim3(96), 0, s, m->K, Mm, ldm, m->geof64.as<double>(),
+                       DIM == 3 ? 10 : 5, fact0, fact1, rho, vel, rhs, mm));
+  note_launch();
+}
+
+void viscous_rhs_device(sipg_mesh* m, int order, double fact0, double fact1, const double* rho, const double* vel,
+                        double* rhs, double* mm, cudaStream_t s) {
+  if (!m || order < 1 || order > 4 || !rho || !vel || !rhs || !mm)
+    throw Error(SIPG_INVALID_ARG, "viscous_rhs: null mesh/array or order outside 1..4");
+  if (!std::isfinite(fact0) || !std::isfinite(fact1)) throw Error(SIPG_INVALID_ARG, "viscous_rhs: factors");
+  if (rhs == vel || mm == rho) throw Error(SIPG_INVALID_ARG, "viscous_rhs: aliasing");
+  m->ensure_device();
+  if (m->K == 0) return;
+  const DevRef& dr = dev_ref(m->dim, order);
+  const int Np = dr.Np, ld = Np | 1;
+  const double* Mm = dr.c64.as<double>() + (size_t)m->dim * Np * ld;  // mass block of the constant blob
+  switch (m->dim * 10 + order) {
+    case 21: launch_vis_rhs<2, 1>(m, Mm, ld, fact0, fact1, rho, vel, rhs, mm, s); break;
+    case 22: launch_vis_rhs<2, 2>(m, Mm, ld, fact0, fact1, rho, vel, rhs, mm, s); break;
+    case 23: launch_vis_rhs<2, 3>(m, Mm, ld, fact0, fact1, rho, vel, rhs, mm, s); break;
+    case 24: launch_vis_rhs<2, 4>(m, Mm, ld, fact0, fact1, rho, vel, rhs, mm, s); break;
+    case 31: launch_vis_rhs<3, 1>(m, Mm, ld, fact0, fact1, rho, vel, rhs, mm, s); break;
+    case 32: launch_vis_rhs<3, 2>(m, Mm, ld, fact0, fact1, rho, vel, rhs, mm, s); break;
+    case 33: launch_vis_rhs<3, 3>(m, Mm, ld, fact0, fact1, rho, vel, rhs, mm, s); break;
+    case 34: launch_vis_rhs<3, 4>(m, Mm, ld, fact0, fact1, rho, vel, rhs, mm, s); break;
+    default: throw Error(SIPG_INVALID_ARG, "viscous_rhs: dimension");
+  }
+}
+
 }  // namespace
 }  // namespace sipg
 
@@ -983,5 +1073,36 @@ extern "C" int sipg_pressure_rhs_host(sipg_mesh* m, int order, double dt, double
     pressure_rhs_device(m, order, dt, b0, b1, d_v, d_n, d_o, d_rhs, 0);
     SIPG_CUDA(cudaMemcpy(rhs, d_rhs, sb, cudaMemcpyDeviceToHost));
     if (d_o) SIPG_CUDA(cudaMemcpy(dPdN_old, d_o, fb, cudaMemcpyDeviceToHost));
+  });
+}
+
+extern "C" int sipg_viscous_rhs(sipg_mesh* m, int order, double fact0, double fact1, const double* rho,
+                                const double* velTT, double* rhs, double* mm_factor, void* stream) {
+  return guarded([&] { viscous_rhs_device(m, order, fact0, fact1, rho, velTT, rhs, mm_factor, (cudaStream_t)stream); });
+}
+
+extern "C" int sipg_viscous_rhs_host(sipg_mesh* m, int order, double fact0, double fact1, const double* rho,
+                                     const double* velTT, double* rhs, double* mm_factor) {
+  return guarded([&] {
+    if (!m || order < 1 || order > 4 || !rho || !velTT || !rhs || !mm_factor)
+      throw Error(SIPG_INVALID_ARG, "viscous_rhs: null mesh/array or order outside 1..4");
+    const int Np = np_of(m->dim, order);
+    const size_t sb = (size_t)m->K * Np * sizeof(double), vb = (size_t)m->dim * sb;
+    std::lock_guard<std::mutex> lk(m->proj_mu);
+    const size_t need = 2 * vb + 2 * sb;
+    if (m->proj_io.bytes < need) {
+      m->proj_io = DevBuf();
+      m->proj_io = DevBuf(need);
+    }
+    char* base = m->proj_io.as<char>();
+    double* d_v = reinterpret_cast<double*>(base);
+    double* d_rhs = reinterpret_cast<double*>(base + vb);
+    double* d_rho = reinterpret_cast<double*>(base + 2 * vb);
+    double* d_mm = reinterpret_cast<double*>(base + 2 * vb + sb);
+    SIPG_CUDA(cudaMemcpy(d_v, velTT, vb, cudaMemcpyHostToDevice));
+    SIPG_CUDA(cudaMemcpy(d_rho, rho, sb, cudaMemcpyHostToDevice));
+    viscous_rhs_device(m, order, fact0, fact1, d_rho, d_v, d_rhs, d_mm, 0);
+    SIPG_CUDA(cudaMemcpy(rhs, d_rhs, vb, cudaMemcpyDeviceToHost));
+    SIPG_CUDA(cudaMemcpy(mm_factor, d_mm, sb, cudaMemcpyDeviceToHost));
   });
 }

@@ -210,8 +210,8 @@ void sipg_op::apply(const T* x, T* y, cudaStream_t s, T alpha, T beta, const T* 
   a.beta = beta;
   a.c = c ? c : y;
   a.tcg = f64 ? (const T*)mesh->tcg64.p : (const T*)mesh->tcg32.p;
-  a.tcgen05 = kernel == 0;
-  const bool tc = (kernel == 0 || kernel == 2) && ncomp == 1 && (f64 ? dref->tc_ok64 : dref->tc_ok32);
+  a.tcgen05 = kernel == 3;
+  const bool tc = (kernel == 0 || kernel >= 2) && ncomp == 1 && (f64 ? dref->tc_ok64 : dref->tc_ok32);
   if (tc) {
     const T* tcc = f64 ? (const T*)dref->tc64.p : (const T*)dref->tc32.p;
     DevBuf& tr = f64 ? trace64 : trace32;
@@ -558,7 +558,7 @@ int sipg_op_apply(sipg_op* op, int precision, const void* x, void* y, void* stre
 
 int sipg_op_set_kernel(sipg_op* op, int kind) {
   return guarded([&] {
-    if (!op || kind < 0 || kind > 2) throw Error(SIPG_INVALID_ARG, "set_kernel");
+    if (!op || kind < 0 || kind > 3) throw Error(SIPG_INVALID_ARG, "set_kernel");
     ++op->version;
     op->kernel = kind;
   });

@@ -9,6 +9,7 @@
 #include <string>
 #include <vector>
 
+#include "amg.hpp"
 #include "mesh.hpp"
 #include "refelem.hpp"
 #include "sipg_apply.cuh"
@@ -41,6 +42,13 @@ struct DevBuf {
   void upload(const void* src, size_t n, cudaStream_t s = 0);
 };
 
+// Keep b at exactly n bytes, reallocating only when the size changes (set-up
+// buffers are rebuilt at every time step: no allocation, no implicit
+// synchronisation of cudaFree when the mesh stays the same).
+inline void ensure(DevBuf& b, size_t n) {
+  if (b.bytes != n) b = DevBuf(n);
+}
+
 // Order-specific reference tables on the device (FP64 and FP32 copies).
 struct DevRef {
   RefElement ref;
@@ -63,6 +71,10 @@ struct sipg_mesh {
   std::mutex host_mu;
   sipg::DevBuf geof64, geof32, nbr, fcode, belems;
   sipg::DevBuf tcg64, tcg32;  // geometry blocks of the tensor-core apply (launch_tc_geom)
+  std::shared_ptr<sipg::P1Plan> p1_plan;  // algebraic coarse space: sparsity of the P1 operator (set-up cache)
+  sipg::DevBuf probe_list;    // assembled levels: elements grouped by distance-2 colour (set-up cache)
+  std::vector<int> probe_off;  // colour c: probe_list[probe_off[c] .. probe_off[c+1])
+  std::mutex probe_mu;
   sipg::DevBuf proj_h;        // velocity projection: 1 / max interior-face fscale per element
   sipg::DevBuf proj_io;       // velocity projection: device copies for the host-buffer entry point
   std::mutex proj_mu;         // serialises host-buffer projections on this mesh

@@ -77,7 +77,7 @@ struct ApplyArgs {
   T alpha, beta;          // y = alpha * A x + beta * c (beta == 0: c is not read)
   const T* c;             // ncomp x K x NP; y unless the caller gives another vector
   const T* tcg;           // tensor-core path: tile-major element and face geometry (launch_tc_geom)
-  int tcgen05 = 1;        // tensor-core path, FP32: tcgen05 kernels where the order has them (else mma.sync)
+  int tcgen05 = 0;        // tensor-core path, FP32: tcgen05 kernels where the order has them (else mma.sync)
 };
 
 // Host-side launchers (sipg_apply.cu).

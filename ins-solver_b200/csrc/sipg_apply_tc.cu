@@ -978,8 +978,8 @@ void build_tc_consts_t(const RefElement& r, std::vector<double>& out) {
     for (int n = 0; n < NP; ++n)
       for (int k = 0; k < KF; ++k)
         put(X::BF + rr * NT * FT * X::BLK, FT, n, k, D[rr][r.fmask[k] * NP + n]);  // BF_r[n][k] = D_r[m(k)][n]
-  if (std::is_same<T, float>::value && tc5_supported(DIM, P)) {
-    std::vector<double> t5;
+  if (std::is_same<T, float>::value) {
+    std::vector<double> t5;  // empty where the order has no tcgen05 kernels
     build_tc5_consts(DIM, P, r, t5);
     out.insert(out.end(), t5.begin(), t5.end());
   }

@@ -242,8 +242,10 @@ struct sipg_solver {
   std::vector<Level> lv;
   std::vector<AmgDevLevel> al;
   DevCsr Pdg, Rdg;
-  DevBuf cinv64, cinv32;
+  DevBuf cinv64, cinv32, cinv_work;
   int cinv_n = 0;
+  DevBuf rows_ws;  // set-up workspace: FP64 inverse diagonal blocks of a level
+  DevBuf pl_v, pl_w, pl_t;  // set-up workspace: power iteration
   bool use_amg = false;
   bool dirty = true;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -326,30 +328,36 @@ static void op_diag(sipg_op* op, double* out, cudaStream_t s) {
 double sipg_solver::power_lmax(sipg_op* lop, const double* dinv64, size_t nl, const double* blocks, int Np) {
   // Power iteration on D^-1 A (D the diagonal, or the diagonal blocks when `blocks`
   // holds their inverses row by row) from v0_i = U(-1,1), splitmix64 seed 0x5eed.
-  std::vector<double> h(nl);
-  uint64_t st = 0x5eedull;
-  for (size_t i = 0; i < nl; ++i) h[i] = 2.0 * ((smix(&st) >> 11) * (1.0 / 9007199254740992.0)) - 1.0;
-  DevBuf v(nl * sizeof(double)), w(nl * sizeof(double)), tb(blocks ? nl * sizeof(double) : 0);
-  SIPG_CUDA(cudaMemcpyAsync(v.p, h.data(), nl * sizeof(double), cudaMemcpyHostToDevice, stream));
+  // work vectors kept across set-ups; the start vector is generated on the device
+  if (pl_v.bytes < nl * sizeof(double)) {
+    pl_v = DevBuf(nl * sizeof(double));
+    pl_w = DevBuf(nl * sizeof(double));
+    pl_t = DevBuf(nl * sizeof(double));
+  }
+  double* v = pl_v.as<double>();
+  double* w = pl_w.as<double>();
+  double* tb = pl_t.as<double>();
+  splitmix_uniform_device(v, nl, 0x5eedull, stream);
   double lam = 0.0;
   for (int it = 0; it < o.eig_iters; ++it) {
-    const double* a[1] = {v.as<double>()};
+    const double* a[1] = {v};
     multi_dot<double>(a, a, 1, nl, S() + S_TMP, 1, rw, stream);
-    k_scale<<<grid_for(nl), 256, 0, stream>>>(v.as<double>(), nl, S(), S_TMP);
-      note_launch();
+    k_scale<<<grid_for(nl), 256, 0, stream>>>(v, nl, S(), S_TMP);
+    note_launch();
     if (blocks) {
-      lop->apply<double>(v.as<double>(), tb.as<double>(), stream);
-      block_matvec<double>(w.as<double>(), blocks, tb.as<double>(), (int)(nl / Np), Np, stream);
+      lop->apply<double>(v, tb, stream);
+      block_matvec<double>(w, blocks, tb, (int)(nl / Np), Np, stream);
     } else {
-      lop->apply<double>(v.as<double>(), w.as<double>(), stream);
-      k_mul<<<grid_for(nl), 256, 0, stream>>>(w.as<double>(), dinv64, nl);
+      lop->apply<double>(v, w, stream);
+      k_mul<<<grid_for(nl), 256, 0, stream>>>(w, dinv64, nl);
       note_launch();
     }
-    const double* b[1] = {w.as<double>()};
-    multi_dot<double>(b, b, 1, nl, S() + S_TMP, 1, rw, stream);
-    lam = std::sqrt(read_scalar(S_TMP));
     std::swap(v, w);
   }
+  // lambda = ||S A v|| of the last step (no host synchronisation before it)
+  const double* b[1] = {v};
+  multi_dot<double>(b, b, 1, nl, S() + S_TMP, 1, rw, stream);
+  lam = std::sqrt(read_scalar(S_TMP));
   return lam;
 }
 
@@ -444,9 +452,7 @@ void sipg_solver::setup_pmg() {
     k_recip<<<grid_for(L.n), 256, 0, stream>>>(L.dinv64.as<double>(), L.n);
       note_launch();
     if (f32) to_f32(L.dinv32.as<float>(), L.dinv64.as<double>(), L.n, stream);
-    L.bc64 = DevBuf();
-    L.bc32 = DevBuf();
-    DevBuf rows;  // FP64 inverse diagonal blocks, row-major per element (block-Jacobi smoothing)
+    DevBuf& rows = rows_ws;  // FP64 inverse diagonal blocks, row-major per element (block-Jacobi smoothing)
     if (o.smoother == 1) {
       // element-block Jacobi: inverse diagonal blocks in the level precision (BF16 for
       // the FP32 V-cycle: the smoother tolerates 8 mantissa bits). Large meshes store
@@ -454,46 +460,48 @@ void sipg_solver::setup_pmg() {
       // small ones as full column-major blocks (ten threads per block at p = 3).
       const int nb = (int)(L.n / L.Np);
       L.bsym = block_sym_supported(L.Np) && nb >= kSymMinBlocks;
-      rows = DevBuf((size_t)nb * L.Np * L.Np * sizeof(double));
+      const size_t rb = (size_t)nb * L.Np * L.Np * sizeof(double);
+      if (rows.bytes < rb) rows = DevBuf(rb);  // shared by the levels, kept across set-ups
       SIPG_CUDA(launch_blocks(dim, L.order, L.op->block_args(BLOCK_INVERSE, 0, rows.as<double>(), true), stream));
       if (f32 && L.bsym) {
-        L.bc32 = DevBuf(block_sym_values<__nv_bfloat16>(nb, L.Np) * sizeof(__nv_bfloat16));
+        ensure(L.bc32, block_sym_values<__nv_bfloat16>(nb, L.Np) * sizeof(__nv_bfloat16));
         block_pack_sym<__nv_bfloat16>(L.bc32.as<__nv_bfloat16>(), rows.as<double>(), nb, L.Np, stream);
       } else if (f32) {
-        L.bc32 = DevBuf((size_t)nb * L.Np * L.Np * sizeof(__nv_bfloat16));
+        ensure(L.bc32, (size_t)nb * L.Np * L.Np * sizeof(__nv_bfloat16));
         block_transpose<__nv_bfloat16>(L.bc32.as<__nv_bfloat16>(), rows.as<double>(), nb, L.Np, stream);
       } else if (L.bsym) {
-        L.bc64 = DevBuf(block_sym_values<double>(nb, L.Np) * sizeof(double));
+        ensure(L.bc64, block_sym_values<double>(nb, L.Np) * sizeof(double));
         block_pack_sym<double>(L.bc64.as<double>(), rows.as<double>(), nb, L.Np, stream);
       } else {
-        L.bc64 = DevBuf((size_t)nb * L.Np * L.Np * sizeof(double));
+        ensure(L.bc64, (size_t)nb * L.Np * L.Np * sizeof(double));
         block_transpose<double>(L.bc64.as<double>(), rows.as<double>(), nb, L.Np, stream);
       }
       pt.mark("diagonal and blocks", l);
       L.lmax = power_lmax(L.op, nullptr, L.n, rows.as<double>(), L.Np);
     } else {
+      L.bc64 = DevBuf();
+      L.bc32 = DevBuf();
       pt.mark("diagonal", l);
       L.lmax = power_lmax(L.op, L.dinv64.as<double>(), L.n);
     }
     pt.mark("eigenvalue bound", l);
-    L.bsr.reset();
     // -1: p = 2 and below in the FP32 V-cycle (p = 2 as scaled FP16 blocks: half the
     // bytes of the matrix-free apply's per-element work, same iteration counts), p = 1
     // in the FP64 V-cycle (FP64 blocks at p = 2 move more bytes than the matrix-free apply)
     const int amo = o.assembled_max_order >= 0 ? o.assembled_max_order : (f32 ? 2 : 1);
-    L.d2 = DevBuf();
-    L.sres = DevBuf();
     if (l > 0 && L.order <= amo && bsr_supported(dim, L.order, nc)) {
-      L.bsr = std::make_unique<BsrOp>();
+      if (!L.bsr) L.bsr = std::make_unique<BsrOp>();  // its buffers are reused by later set-ups
       // FP32 V-cycle with packed symmetric block-Jacobi smoothing: also C = Bd^-1 A, so
       // that one kernel per Chebyshev step after the first updates Bd^-1 r directly
       const bool fused = f32 && o.smoother == 1 && L.Np % 2 == 0;
       bsr_assemble(L.op, *L.bsr, f32, stream, fused ? rows.as<double>() : nullptr, L.bsym);
       pt.mark("assembled blocks", l);
       if (L.bsr->c16.p) {
-        L.d2 = DevBuf(L.n * sizeof(float));
-        L.sres = DevBuf(L.n * sizeof(float));
+        ensure(L.d2, L.n * sizeof(float));
+        ensure(L.sres, L.n * sizeof(float));
       }
+    } else {
+      L.bsr.reset();
     }
   }
   use_amg = o.coarse_kind == 1 && nc == 1 && lv.back().order == 1;
@@ -526,13 +534,17 @@ void sipg_solver::setup_amg() {
     any_dirichlet |= bd[b] != 0;
   }
   PhaseTimer pt(stream);
+  {
+    std::lock_guard<std::mutex> lk(m->probe_mu);
+    if (!m->p1_plan) m->p1_plan = std::make_shared<P1Plan>(p1c_plan(K, m->Nv, Np1, h.e2v.data()));
+  }
   Csr A0, Pd;
   p1c_operator(dev_ref(m->dim, 1).ref, K, m->Nv, h.geof.data(), h.e2v.data(), fac1.empty() ? nullptr : fac1.data(),
                tau1.data(), h.sJ.data(), h.nx.data(), h.ny.data(), h.nz.data(), h.nbr.data(), bd, lop->mm_mode,
-               lop->mm_scalar, mm1.empty() ? nullptr : mm1.data(), &A0, &Pd);
+               lop->mm_scalar, mm1.empty() ? nullptr : mm1.data(), &A0, &Pd, m->p1_plan.get());
   const bool singular = !any_dirichlet && lop->mm_mode == SIPG_MM_NONE;
   pt.mark("P1 operator (host)");
-  AmgHierarchy H = build_amg(A0, Pd, std::max(2, o.amg_coarse_max), o.amg_strength, singular);
+  AmgHierarchy H = build_amg(A0, Pd, std::max(2, o.amg_coarse_max), o.amg_strength, singular, false);
   pt.mark("aggregation (host)");
   const bool f32 = o.precision == SIPG_FP32;
   const size_t ts = f32 ? sizeof(float) : sizeof(double);
@@ -566,12 +578,17 @@ void sipg_solver::setup_amg() {
     D.res2 = DevBuf(D.n * ts);
     D.d2 = DevBuf(D.n * ts);
   }
+  // the coarsest level is inverted on the device (FP64 Gauss-Jordan), then copied to FP32
+  const size_t nn = (size_t)H.coarse_n * H.coarse_n;
+  ensure(cinv64, nn * sizeof(double));
+  ensure(cinv32, nn * sizeof(float));
+  ensure(cinv_work, (size_t)2 * H.coarse_n * sizeof(double));
   cinv_n = H.coarse_n;
-  cinv64 = DevBuf(H.coarse_inv.size() * sizeof(double));
-  cinv64.upload(H.coarse_inv.data(), H.coarse_inv.size() * sizeof(double));
-  std::vector<float> c32(H.coarse_inv.begin(), H.coarse_inv.end());
-  cinv32 = DevBuf(c32.size() * sizeof(float));
-  cinv32.upload(c32.data(), c32.size() * sizeof(float));
+  SIPG_CUDA(cudaMemcpyAsync(cinv64.p, H.coarse_dense.data(), nn * sizeof(double), cudaMemcpyHostToDevice, stream));
+  dense_inverse_device(cinv64.as<double>(), cinv_n, H.singular, cinv_work.as<double>(), stream);
+  to_f32(cinv32.as<float>(), cinv64.as<double>(), nn, stream);
+  SIPG_CUDA(cudaStreamSynchronize(stream));  // the host matrix goes out of scope
+  pt.mark("coarsest inverse (device)");
 }
 
 // A set-up that fails part-way leaves no half-built levels behind: the next
@@ -1146,7 +1163,7 @@ int sipg_solver_default_opts(int kind, sipg_solver_opts* o) {
     o->coarse_iters = 20;
     o->check_every = 1;
     o->coarse_kind = 1;
-    o->amg_coarse_max = 1000;
+    o->amg_coarse_max = 2048;
     o->amg_strength = 0.08;
     o->graphs = 2;
     o->assembled_max_order = -1;

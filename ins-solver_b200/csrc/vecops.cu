@@ -1,4 +1,9 @@
 // Vector kernels for the solvers. See vecops.cuh.
+#include <cooperative_groups.h>
+
+#include <stdexcept>
+#include <string>
+
 #include <algorithm>
 #include <atomic>
 
@@ -6,6 +11,8 @@
 
 #include "pdl.cuh"
 #include "vecops.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace sipg {
 
@@ -598,16 +605,96 @@ __global__ void __launch_bounds__(128) k_inv_mass_n(T* __restrict__ y, const T* 
       for (int j = 0; j < NP; ++j) xv[j] = xr[j];
       const T sc = scale / geof[(be % (size_t)K) * ngeof + jidx];
       T* yr = sx + threadIdx.x * NP;
+      // four rows at a time: independent accumulators hide the FMA latency
+      constexpr int R4 = NP / 4 * 4;
 #pragma unroll
-      for (int r = 0; r < NP; ++r) {
-        T s = T(0);
+      for (int r = 0; r < R4; r += 4) {
+        T s0 = T(0), s1 = T(0), s2 = T(0), s3 = T(0);
 #pragma unroll
-        for (int j = 0; j < NP; ++j) s += sM[r * NP + j] * xv[j];
-        yr[r] = sc * s;
+        for (int j = 0; j < NP; ++j) {
+          const T v = xv[j];
+          s0 += sM[r * NP + j] * v;
+          s1 += sM[(r + 1) * NP + j] * v;
+          s2 += sM[(r + 2) * NP + j] * v;
+          s3 += sM[(r + 3) * NP + j] * v;
+        }
+        yr[r] = sc * s0;
+        yr[r + 1] = sc * s1;
+        yr[r + 2] = sc * s2;
+        yr[r + 3] = sc * s3;
+      }
+#pragma unroll
+      for (int r = R4; r < NP; ++r) {
+        T s0 = T(0);
+#pragma unroll
+        for (int j = 0; j < NP; ++j) s0 += sM[r * NP + j] * xv[j];
+        yr[r] = sc * s0;
       }
     }
     __syncthreads();
     for (int i = threadIdx.x; i < nb * NP; i += blockDim.x) y[b0 * NP + i] = sx[i];
+  }
+}
+
+// In-place Gauss-Jordan inversion of a dense n x n matrix (row-major, FP64) on
+// the device as one cooperative kernel (grid-wide barriers between the phases
+// instead of three launches per pivot). Pivot k:
+//   row:    a[k][j] *= 1 / a[k][k]           (j != k)
+//   update: a[i][j] -= a[i][k] a[k][j]       (i, j != k; a warp per row)
+//   column: a[i][k] *= -1 / a[k][k], a[k][k] = 1 / a[k][k]
+// No pivoting: the coarsest algebraic operator is symmetric positive definite
+// (a singular one is shifted first), so every pivot is positive.
+__global__ void __launch_bounds__(256) k_gj_coop(double* a, int n) {
+  cg::grid_group grid = cg::this_grid();
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  const int lane = threadIdx.x & 31, warp = tid >> 5, nwarps = nth >> 5;
+  for (int k = 0; k < n; ++k) {
+    const double r = 1.0 / a[(size_t)k * n + k];  // nobody writes a[k][k] before the column phase
+    for (int t = tid; t < n; t += nth)
+      if (t != k) a[(size_t)k * n + t] *= r;
+    grid.sync();
+    const double* rowk = a + (size_t)k * n;
+    for (int i = warp; i < n; i += nwarps) {
+      if (i == k) continue;
+      double* rowi = a + (size_t)i * n;
+      const double f = rowi[k];
+      for (int j = lane; j < n; j += 32)
+        if (j != k) rowi[j] -= f * rowk[j];
+    }
+    grid.sync();
+    for (int t = tid; t < n; t += nth) {
+      if (t != k) a[(size_t)t * n + k] *= -r;
+      else a[(size_t)k * n + k] = r;
+    }
+    grid.sync();
+  }
+}
+// Row sums, column sums and the total of a dense matrix (one thread per row /
+// column; the total from the row sums in a fixed order).
+__global__ void k_dense_sums(const double* a, int n, double* rs, double* cs) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 2 * n; t += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    if (t < n)
+      for (int j = 0; j < n; ++j) s += a[(size_t)t * n + j];
+    else
+      for (int i = 0; i < n; ++i) s += a[(size_t)i * n + (t - n)];
+    (t < n ? rs[t] : cs[t - n]) = s;
+  }
+}
+// Q a Q with Q = I - 11^T / n: a_ij - rs_i / n - cs_j / n + total / n^2.
+__global__ void k_dense_project(double* a, int n, const double* rs, const double* cs) {
+  __shared__ double total;
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int i = 0; i < n; ++i) s += rs[i];
+    total = s;
+  }
+  __syncthreads();
+  const double dn = (double)n;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < (size_t)n * n;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(t / n), j = (int)(t - (size_t)i * n);
+    a[t] += -rs[i] / dn - cs[j] / dn + total / (dn * dn);
   }
 }
 
@@ -1039,6 +1126,49 @@ void csr_cheb(int rows, const int* ptr, const int* idx, const T* val, const T* d
              (int)first);
   note_launch();
 }
+void dense_inverse_device(double* a, int n, bool project_constants, double* work, cudaStream_t s) {
+  const size_t nn = (size_t)n * n;
+  const int g2 = (int)std::min<size_t>((nn + 255) / 256, 148 * 8);
+  // every block of the cooperative kernel must be resident at once
+  static int per_sm = 0;
+  if (per_sm == 0) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gj_coop, 256, 0) != cudaSuccess || per_sm < 1)
+      per_sm = 1;
+  }
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = std::max(1, std::min(sms * std::min(per_sm, 4), (n + 7) / 8));
+  void* args[] = {&a, &n};
+  const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_gj_coop, dim3(grid), dim3(256), args, 0, s);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw std::runtime_error(std::string("dense inverse: cooperative launch failed: ") + cudaGetErrorString(e));
+  }
+  note_launch();
+  if (project_constants) {
+    k_dense_sums<<<(2 * n + 255) / 256, 256, 0, s>>>(a, n, work, work + n);
+    k_dense_project<<<g2, 256, 0, s>>>(a, n, work, work + n);
+    note_launch(2);
+  }
+}
+
+// v_i = 2 U_i - 1 with U_i the i-th splitmix64 draw of `seed` (top 53 bits), as
+// the host generator SplitMix64 gives them one after the other.
+__global__ void k_splitmix_uniform(double* v, size_t n, unsigned long long seed) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    unsigned long long z = seed + (unsigned long long)(i + 1) * 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    v[i] = 2.0 * ((double)(z >> 11) * (1.0 / 9007199254740992.0)) - 1.0;
+  }
+}
+void splitmix_uniform_device(double* v, size_t n, unsigned long long seed, cudaStream_t s) {
+  k_splitmix_uniform<<<grid_for(n), 256, 0, s>>>(v, n, seed);
+  note_launch();
+}
+
 template <typename T>
 void dense_mv(int n, const T* M, const T* x, T* y, cudaStream_t s) {
   int blocks = std::max(1, std::min((n * 32 + 255) / 256, 148 * 8));

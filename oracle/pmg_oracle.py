@@ -12,7 +12,7 @@ eigen_val_saftey_factor) with the library's default choices for the rest:
 orders 3 -> 2 -> 1, Chebyshev(4) on the element-block Jacobi preconditioned
 operator, eigenvalue bound from 20 power iterations x 1.1, lower bound / 30,
 one pre- and one post-smoothing sweep, a continuous-P1 smoothed-aggregation
-coarse hierarchy to 1000 unknowns with Chebyshev(2) smoothing on its levels.
+coarse hierarchy to at most 2048 unknowns with Chebyshev(2) smoothing on its levels.
 """
 import ctypes as C
 
@@ -23,7 +23,7 @@ import dg_oracle as D
 import oracle_py as O
 
 DEFAULTS = dict(cheb_order=4, eig_safety=1.1, eig_ratio=30.0, eig_iters=20, coarse_iters=20, smoother=1,
-                amg_cheb_order=2, amg_coarse_max=1000, amg_strength=0.08)
+                amg_cheb_order=2, amg_coarse_max=2048, amg_strength=0.08)
 
 
 def levels(mesh, dim, orders, factor, bc_types, **over):

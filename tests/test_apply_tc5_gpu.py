@@ -1,6 +1,6 @@
-"""The tcgen05 FP32 apply (TF32 MMAs with TMEM accumulators, kernel 0 at p = 3
+"""The tcgen05 FP32 apply (TF32 MMAs with TMEM accumulators, kernel 3 at p = 3
 in 3D) against the FP64 oracle and against the mma.sync tensor-core kernels
-(kernel 2), on meshes from a partial first tile to several tiles per CTA, with
+(kernel 0), on meshes from a partial first tile to several tiles per CTA, with
 a nodal factor, nodal and scalar mass terms, mixed Dirichlet / Neumann walls
 and a pinned DOF."""
 import ctypes as C
@@ -48,8 +48,8 @@ def test_tcgen05_apply_matches_oracle_and_mma_sync(n, variant):
     scalar = 2.5e3 if variant == "helmholtz_scalar" else 0.0
     op = make_op(mesh, 3, 1, f, m, mm_scalar=scalar, bct=bct)
     want = O.mult(om, x, bct, f, m, scalar)
-    got = fp32_apply(op, x, 0)
-    prev = fp32_apply(op, x, 2)
+    got = fp32_apply(op, x, 3)
+    prev = fp32_apply(op, x, 0)
     err = rel_err(got, want)
     print(f"{variant} n={n}: tcgen05 {err:.2e}, mma.sync {rel_err(prev, want):.2e}")
     assert err < TOL_TC5
@@ -67,16 +67,18 @@ def test_tcgen05_apply_pinned_dof():
     want = O.mult(om, xs, bct, f)
     d = O.diag(om, 1, bct, f)
     want[0, pe, pn] = d[0, pe, pn] * x[0, pe, pn]
-    assert rel_err(fp32_apply(op, x, 0), want) < TOL_TC5
+    assert rel_err(fp32_apply(op, x, 3), want) < TOL_TC5
     assert timeouts() == 0
 
 
 def test_tcgen05_static_scratch_entry_point_matches_apply():
     mesh, t, e, om, x, f, m, bct = random_case(3, 8, 3, 1, seed=12)
     op = make_op(mesh, 3, 1, f, bct=bct)
-    want = fp32_apply(op, x, 0)
+    want = fp32_apply(op, x, 3)
+    op.set_kernel(3)
     xd = DevArray(x.astype(np.float32))
     yd = DevArray(np.zeros(x.shape, np.float32))
     st = sipg.lib().sipg_op_apply_static_scratch(op.h, sipg.FP32, C.c_void_p(xd.p), C.c_void_p(yd.p), C.c_void_p(0))
+    op.set_kernel(0)
     assert st == sipg.SIPG_OK
     assert np.array_equal(yd.get().astype(np.float64), want)

@@ -302,3 +302,39 @@ def test_gpu_pressure_rhs_exact_divergence():
     got, _ = sipg.pressure_rhs(mesh, order, 0.01, u)
     want = e["geof"][:, -1][:, None] * ((-div / 0.01) @ t["M"].T)
     assert np.abs(got - want).max() < 1e-9 * np.abs(want).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dim,n,order", [(3, 4, 3), (3, 3, 4), (2, 8, 3), (3, 3, 2)])
+def test_viscous_rhs_matches_the_reference_kernel_and_mass(dim, n, order):
+    """sipg_viscous_rhs_host: mp_ins_3d_vis_0 then mesh->mass on each component
+    (src/solvers/3d/mp_ins_solver.cpp:669-694) as one kernel, against the
+    reference's own mp_ins_3d_vis_0 (oracle/_ref) followed by J M per element."""
+    import ctypes as C
+    mesh = sipg.Mesh.box(dim, n, jitter=0.1, seed=3 + order)
+    t, e = sipg.ref_tables(dim, order), mesh.export(order)
+    K, Np = mesh.K, t["Np"]
+    rng = np.random.default_rng(order + 10 * dim)
+    rho = rng.uniform(1.0, 1000.0, (K, Np))
+    vel = rng.uniform(-1.0, 1.0, (dim, K, Np))
+    fact0, fact1 = 1e3 / 1e-3, 1.5 * 1e3 / 1e-3
+    rhs = np.zeros_like(vel)
+    mm = np.zeros_like(rho)
+    sipg.check(sipg.lib().sipg_viscous_rhs_host(mesh.h, order, C.c_double(fact0), C.c_double(fact1),
+                                                O._d(rho), O._d(np.ascontiguousarray(vel)), O._d(rhs), O._d(mm)))
+    J = e["geof"][:, -1]
+    want = J[None, :, None] * ((fact0 * rho[None] * vel) @ t["M"].T)
+    assert np.abs(rhs - want).max() <= 1e-13 * np.abs(want).max()
+    assert np.abs(mm - fact1 * rho).max() <= 1e-15 * np.abs(fact1 * rho).max()
+    if dim == 3 and O.have_ref():
+        # the reference's kernel on the first elements, then the mass
+        om = O.OMesh(t, e)
+        for el in range(4):
+            args = [np.array([fact0]), np.array([fact1]), rho[el].copy(), np.zeros(Np), np.zeros(1)]
+            args += [vel[c, el].copy() for c in range(3)] + [np.zeros(Np) for _ in range(4)]
+            ptrs = (C.c_void_p * len(args))(*[a.ctypes.data_as(C.c_void_p) for a in args])
+            assert O.ref_lib().ref_kernel(C.byref(om.s), b"mp_ins_3d_vis_0", ptrs) == 0
+            for c in range(3):
+                ref = J[el] * (t["M"] @ args[8 + c])
+                assert np.abs(rhs[c, el] - ref).max() <= 1e-13 * np.abs(ref).max()
+            assert np.abs(mm[el] - args[11]).max() <= 1e-15 * np.abs(args[11]).max()

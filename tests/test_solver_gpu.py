@@ -51,7 +51,7 @@ def _pmg_oracle_levels(mesh, orders, factor, bct, amg=True):
         f1 = np.ascontiguousarray(facs[-1])
         O.oracle_lib().oracle_tau(C.byref(meshes[-1].s), O._d(f1), O._d(tau1))
         bd = (np.asarray(bct)[0] == sipg.BC_DIRICHLET).astype(np.int32)
-        out["amg"] = sipg.Amg.p1(mesh, f1, tau1, bd, coarse_max=1000, strength=0.08, singular=not bd.any())
+        out["amg"] = sipg.Amg.p1(mesh, f1, tau1, bd, coarse_max=2048, strength=0.08, singular=not bd.any())
     return out
 
 
