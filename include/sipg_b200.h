@@ -208,6 +208,12 @@ typedef struct {
   int amg_cheb_order;        /* Chebyshev degree on the algebraic coarse levels (0: cheb_order);
                                 default 2 (the coarse correction needs no more at C2: same
                                 iteration count as degree 4) */
+  int amg_reuse_interpolation; /* [petsc-amg] reuse-interpolation (examples/3d/oscillating_droplet/
+                                config.ini:59, default 1): later set-ups keep the aggregates and
+                                prolongators of the first and recompute only the level operators
+                                (Galerkin products), their smoother data and the coarsest inverse,
+                                all on the device; 0: aggregate again at every set-up. A change of
+                                the boundary types or of the problem's singularity aggregates again. */
 } sipg_solver_opts;
 
 int sipg_solver_default_opts(int kind, sipg_solver_opts *o);

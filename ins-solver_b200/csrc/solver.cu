@@ -31,6 +31,7 @@
 
 #include "../../include/sipg_b200.h"
 #include "amg.hpp"
+#include "amg_setup.cuh"
 #include "capi_util.hpp"
 #include "bsr.cuh"
 #include "runtime.hpp"
@@ -129,51 +130,39 @@ struct DevCsr {
   }
 };
 
+// Fixed term lists on the device (TermPlan): out[i] = sum_t in[idx[t]] * coef[t].
+struct DevTerms {
+  int n = 0;
+  DevBuf ptr, idx, coef;
+  void upload(const TermPlan& t) {
+    n = (int)t.ptr.size() - 1;
+    ptr = DevBuf(t.ptr.size() * sizeof(int));
+    ptr.upload(t.ptr.data(), t.ptr.size() * sizeof(int));
+    idx = DevBuf(std::max<size_t>(1, t.idx.size()) * sizeof(int));
+    if (!t.idx.empty()) idx.upload(t.idx.data(), t.idx.size() * sizeof(int));
+    coef = DevBuf();
+    if (!t.coef.empty()) {
+      coef = DevBuf(t.coef.size() * sizeof(double));
+      coef.upload(t.coef.data(), t.coef.size() * sizeof(double));
+    }
+  }
+  void run(const double* in, double* out, float* out32, cudaStream_t s) const {
+    term_sum_device(n, ptr.as<int>(), idx.as<int>(), coef.p ? coef.as<double>() : nullptr, in, out, out32, s);
+  }
+};
+
 struct AmgDevLevel {
   int n = 0;
   DevCsr A, P, R;
+  DevTerms ap, rap;  // Galerkin product with the stored P: AP = A P, then R (AP) = the next level's operator
+  DevBuf apv;        // values of A P
   DevBuf dinv64, dinv32;
   double lmax = 0.0;
   DevBuf rhs, z, res, d;
   DevBuf res2, d2;  // the fused Chebyshev steps alternate between (d, res) and (d2, res2)
 };
 
-// Power iteration on D^-1 A for a host CSR matrix, same start vector and steps as
-// the order levels (splitmix64 seed 0x5eed, U(-1,1)).
-double host_csr_lmax(const Csr& A, const std::vector<double>& dinv, int iters);
-
 int grid_for(size_t n) { return (int)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, 148 * 16)); }
-
-uint64_t smix(uint64_t* s) {
-  uint64_t z = (*s += 0x9E3779B97F4A7C15ull);
-  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-  return z ^ (z >> 31);
-}
-
-double host_csr_lmax(const Csr& A, const std::vector<double>& dinv, int iters) {
-  const size_t n = (size_t)A.rows;
-  std::vector<double> v(n), w(n);
-  uint64_t st = 0x5eedull;
-  for (size_t i = 0; i < n; ++i) v[i] = 2.0 * ((smix(&st) >> 11) * (1.0 / 9007199254740992.0)) - 1.0;
-  double lam = 0.0;
-  for (int it = 0; it < iters; ++it) {
-    double nv = 0.0;
-    for (size_t i = 0; i < n; ++i) nv += v[i] * v[i];
-    nv = std::sqrt(nv);
-    for (size_t i = 0; i < n; ++i) v[i] /= nv;
-    for (size_t i = 0; i < n; ++i) {
-      double s = 0.0;
-      for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) s += A.val[k] * v[A.idx[k]];
-      w[i] = s * dinv[i];
-    }
-    double ww = 0.0;
-    for (size_t i = 0; i < n; ++i) ww += w[i] * w[i];
-    lam = std::sqrt(ww);
-    std::swap(v, w);
-  }
-  return lam;
-}
 
 }  // namespace
 
@@ -246,6 +235,12 @@ struct sipg_solver {
   int cinv_n = 0;
   DevBuf rows_ws;  // set-up workspace: FP64 inverse diagonal blocks of a level
   DevBuf pl_v, pl_w, pl_t;  // set-up workspace: power iteration
+  DevBuf p1_blk, a0_tmp;     // set-up workspace: P1 element blocks, level-0 values before the hierarchy exists
+  // the algebraic hierarchy (aggregates and prolongators) is kept across set-ups
+  // while these stay the same (amg_reuse_interpolation)
+  bool amg_frozen = false;
+  std::vector<int> amg_bct;
+  bool amg_singular = false;
   bool use_amg = false;
   bool dirty = true;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -318,6 +313,7 @@ struct sipg_solver {
   void precondition(const double* rin, double* zout);
   int solve(const double* b, double* x, sipg_solve_info* info);
   double power_lmax(sipg_op* lop, const double* dinv64, size_t nl, const double* blocks = nullptr, int Np = 0);
+  double power_lmax_csr(const AmgDevLevel& D);
 };
 
 // Diagonal of an operator (FP64), with its pinned DOF.
@@ -359,6 +355,32 @@ double sipg_solver::power_lmax(sipg_op* lop, const double* dinv64, size_t nl, co
   multi_dot<double>(b, b, 1, nl, S() + S_TMP, 1, rw, stream);
   lam = std::sqrt(read_scalar(S_TMP));
   return lam;
+}
+
+// The same power iteration on D^-1 A for an algebraic level (CSR, FP64).
+double sipg_solver::power_lmax_csr(const AmgDevLevel& D) {
+  const size_t nl = (size_t)D.n;
+  if (pl_v.bytes < nl * sizeof(double)) {
+    pl_v = DevBuf(nl * sizeof(double));
+    pl_w = DevBuf(nl * sizeof(double));
+    pl_t = DevBuf(nl * sizeof(double));
+  }
+  double* v = pl_v.as<double>();
+  double* w = pl_w.as<double>();
+  splitmix_uniform_device(v, nl, 0x5eedull, stream);
+  for (int it = 0; it < o.eig_iters; ++it) {
+    const double* a[1] = {v};
+    multi_dot<double>(a, a, 1, nl, S() + S_TMP, 1, rw, stream);
+    k_scale<<<grid_for(nl), 256, 0, stream>>>(v, nl, S(), S_TMP);
+    note_launch();
+    D.A.mv<double>(v, w, 1.0, 0.0, stream);
+    k_mul<<<grid_for(nl), 256, 0, stream>>>(w, D.dinv64.as<double>(), nl);
+    note_launch();
+    std::swap(v, w);
+  }
+  const double* b[1] = {v};
+  multi_dot<double>(b, b, 1, nl, S() + S_TMP, 1, rw, stream);
+  return std::sqrt(read_scalar(S_TMP));
 }
 
 void sipg_solver::setup_pmg() {
@@ -509,85 +531,124 @@ void sipg_solver::setup_pmg() {
   pt.mark("algebraic levels");
 }
 
+// Algebraic levels below the p = 1 level. The continuous P1 operator is assembled
+// on the device from the level's factor and penalty. The first set-up (and any
+// set-up after the boundary types or the singularity of the problem changed, or
+// every set-up with amg_reuse_interpolation = 0) aggregates on the host and stores
+// the prolongators and the Galerkin term lists; every set-up then recomputes the
+// level operators, their inverse diagonals and eigenvalue bounds and the coarsest
+// inverse on the device.
 void sipg_solver::setup_amg() {
   Level& L = lv.back();
   sipg_op* lop = L.op;
   sipg_mesh* m = op->mesh;
-  const int K = m->K, Np1 = L.Np, Nf = m->dim + 1;
-  std::vector<double> tau1((size_t)K * Nf), fac1;
-  SIPG_CUDA(cudaMemcpyAsync(tau1.data(), lop->tau64.p, tau1.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
-  if (lop->has_factor) {
-    fac1.resize((size_t)K * Np1);
-    SIPG_CUDA(cudaMemcpyAsync(fac1.data(), lop->factor64.p, fac1.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
-  }
-  std::vector<double> mm1;
-  if (lop->mm_mode == SIPG_MM_NODAL) {
-    mm1.resize((size_t)K * Np1);
-    SIPG_CUDA(cudaMemcpyAsync(mm1.data(), lop->mm64.p, mm1.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
-  }
-  SIPG_CUDA(cudaStreamSynchronize(stream));
-  const Mesh& h = m->host_order(1);
-  std::vector<uint8_t> bd(m->Kb);
+  const int K = m->K, Np1 = L.Np;
   bool any_dirichlet = false;
-  for (int b = 0; b < m->Kb; ++b) {
-    bd[b] = op->bct_host[b] == SIPG_BC_DIRICHLET;
-    any_dirichlet |= bd[b] != 0;
-  }
+  for (int b = 0; b < m->Kb; ++b) any_dirichlet |= op->bct_host[b] == SIPG_BC_DIRICHLET;
+  const bool singular = !any_dirichlet && lop->mm_mode == SIPG_MM_NONE;
   PhaseTimer pt(stream);
   {
     std::lock_guard<std::mutex> lk(m->probe_mu);
-    if (!m->p1_plan) m->p1_plan = std::make_shared<P1Plan>(p1c_plan(K, m->Nv, Np1, h.e2v.data()));
+    if (!m->p1_plan) m->p1_plan = std::make_shared<P1Plan>(p1c_plan(K, m->Nv, Np1, m->e2v.data()));
+    if (!m->p1_gather) {
+      auto g = std::make_shared<DevTerms>();
+      g->upload(p1c_gather_plan(*m->p1_plan, K, Np1));
+      m->p1_gather = g;
+    }
   }
-  Csr A0, Pd;
-  p1c_operator(dev_ref(m->dim, 1).ref, K, m->Nv, h.geof.data(), h.e2v.data(), fac1.empty() ? nullptr : fac1.data(),
-               tau1.data(), h.sJ.data(), h.nx.data(), h.ny.data(), h.nz.data(), h.nbr.data(), bd, lop->mm_mode,
-               lop->mm_scalar, mm1.empty() ? nullptr : mm1.data(), &A0, &Pd, m->p1_plan.get());
-  const bool singular = !any_dirichlet && lop->mm_mode == SIPG_MM_NONE;
-  pt.mark("P1 operator (host)");
-  AmgHierarchy H = build_amg(A0, Pd, std::max(2, o.amg_coarse_max), o.amg_strength, singular, false);
-  pt.mark("aggregation (host)");
+  const P1Plan& plan = *m->p1_plan;
+  const DevTerms& gather = *std::static_pointer_cast<DevTerms>(m->p1_gather);
+  const size_t nnz0 = plan.idx.size();
+  ensure(p1_blk, (size_t)K * Np1 * Np1 * sizeof(double));
+  p1c_blocks_device(p1_tables(dev_ref(m->dim, 1).ref), K, m->geof64.as<double>(),
+                    lop->has_factor ? lop->factor64.as<double>() : nullptr, lop->tau64.as<double>(), m->nbr.as<int>(),
+                    lop->bct.as<unsigned char>(), lop->mm_mode, lop->mm_scalar,
+                    lop->mm_mode == SIPG_MM_NODAL ? lop->mm64.as<double>() : nullptr, p1_blk.as<double>(), stream);
+  const bool reuse = o.amg_reuse_interpolation != 0 && amg_frozen && !al.empty() && amg_bct == op->bct_host &&
+                     amg_singular == singular;
   const bool f32 = o.precision == SIPG_FP32;
   const size_t ts = f32 ? sizeof(float) : sizeof(double);
-  Pdg.upload(H.Pdg);
-  Rdg.upload(H.Rdg);
-  al.clear();
-  al.resize(H.levels.size());
-  for (size_t l = 0; l < H.levels.size(); ++l) {
-    AmgDevLevel& D = al[l];
-    const AmgLevel& HL = H.levels[l];
-    D.n = HL.A.rows;
-    D.A.upload(HL.A);
-    if (l + 1 < H.levels.size()) {
-      D.P.upload(HL.P);
-      D.R.upload(HL.R);
-      std::vector<double> dinv(D.n, 0.0);
-      for (int i = 0; i < D.n; ++i)
-        for (int k = HL.A.ptr[i]; k < HL.A.ptr[i + 1]; ++k)
-          if (HL.A.idx[k] == i) dinv[i] = 1.0 / HL.A.val[k];
-      D.lmax = host_csr_lmax(HL.A, dinv, o.eig_iters);
-      D.dinv64 = DevBuf(D.n * sizeof(double));
-      D.dinv64.upload(dinv.data(), D.n * sizeof(double));
-      std::vector<float> d32(dinv.begin(), dinv.end());
-      D.dinv32 = DevBuf(D.n * sizeof(float));
-      D.dinv32.upload(d32.data(), D.n * sizeof(float));
+  if (!reuse) {
+    amg_frozen = false;
+    ensure(a0_tmp, nnz0 * sizeof(double));
+    gather.run(p1_blk.as<double>(), a0_tmp.as<double>(), nullptr, stream);
+    Csr A0;
+    A0.rows = A0.cols = m->Nv;
+    A0.ptr = plan.ptr;
+    A0.idx = plan.idx;
+    A0.val.resize(nnz0);
+    SIPG_CUDA(cudaMemcpyAsync(A0.val.data(), a0_tmp.p, nnz0 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    SIPG_CUDA(cudaStreamSynchronize(stream));
+    // injection of vertex values into the p = 1 nodes: row (e, i) has one entry at e2v[e][i]
+    Csr Pd;
+    Pd.rows = K * Np1;
+    Pd.cols = m->Nv;
+    Pd.ptr.resize(Pd.rows + 1);
+    for (int k = 0; k <= Pd.rows; ++k) Pd.ptr[k] = k;
+    Pd.idx.assign(m->e2v.begin(), m->e2v.begin() + Pd.rows);
+    Pd.val.assign(Pd.rows, 1.0);
+    pt.mark("P1 operator (device)");
+    AmgHierarchy H = build_amg(A0, Pd, std::max(2, o.amg_coarse_max), o.amg_strength, singular, false);
+    pt.mark("aggregation (host)");
+    Pdg.upload(H.Pdg);
+    Rdg.upload(H.Rdg);
+    al.clear();
+    al.resize(H.levels.size());
+    for (size_t l = 0; l < H.levels.size(); ++l) {
+      AmgDevLevel& D = al[l];
+      const AmgLevel& HL = H.levels[l];
+      D.n = HL.A.rows;
+      D.A.upload(HL.A);
+      if (l + 1 < H.levels.size()) {
+        D.P.upload(HL.P);
+        D.R.upload(HL.R);
+        Csr APs, RAPs;
+        const TermPlan tap = spgemm_plan(HL.A, HL.P, true, &APs);
+        const TermPlan trap = spgemm_plan(HL.R, APs, false, &RAPs);
+        const Csr& next = H.levels[l + 1].A;
+        if (RAPs.ptr != next.ptr || RAPs.idx != next.idx)
+          throw Error(SIPG_CUDA_ERROR, "algebraic set-up: Galerkin term lists do not match the coarse operator");
+        D.ap.upload(tap);
+        D.rap.upload(trap);
+        D.apv = DevBuf(std::max<size_t>(1, APs.nnz()) * sizeof(double));
+        D.dinv64 = DevBuf(D.n * sizeof(double));
+        D.dinv32 = DevBuf(D.n * sizeof(float));
+      }
+      D.rhs = DevBuf(D.n * ts);
+      D.z = DevBuf(D.n * ts);
+      D.res = DevBuf(D.n * ts);
+      D.d = DevBuf(D.n * ts);
+      D.res2 = DevBuf(D.n * ts);
+      D.d2 = DevBuf(D.n * ts);
     }
-    D.rhs = DevBuf(D.n * ts);
-    D.z = DevBuf(D.n * ts);
-    D.res = DevBuf(D.n * ts);
-    D.d = DevBuf(D.n * ts);
-    D.res2 = DevBuf(D.n * ts);
-    D.d2 = DevBuf(D.n * ts);
+    cinv_n = H.coarse_n;
+    const size_t nn = (size_t)cinv_n * cinv_n;
+    ensure(cinv64, nn * sizeof(double));
+    ensure(cinv32, nn * sizeof(float));
+    ensure(cinv_work, ((size_t)2 * cinv_n + 1024) * sizeof(double));
+    amg_bct = op->bct_host;
+    amg_singular = singular;
+    amg_frozen = true;
+    pt.mark("hierarchy upload");
   }
-  // the coarsest level is inverted on the device (FP64 Gauss-Jordan), then copied to FP32
-  const size_t nn = (size_t)H.coarse_n * H.coarse_n;
-  ensure(cinv64, nn * sizeof(double));
-  ensure(cinv32, nn * sizeof(float));
-  ensure(cinv_work, (size_t)2 * H.coarse_n * sizeof(double));
-  cinv_n = H.coarse_n;
-  SIPG_CUDA(cudaMemcpyAsync(cinv64.p, H.coarse_dense.data(), nn * sizeof(double), cudaMemcpyHostToDevice, stream));
-  dense_inverse_device(cinv64.as<double>(), cinv_n, H.singular, cinv_work.as<double>(), stream);
+  // level operators from the stored prolongators (Galerkin products on the device)
+  gather.run(p1_blk.as<double>(), al[0].A.v64.as<double>(), al[0].A.v32.as<float>(), stream);
+  for (size_t l = 0; l + 1 < al.size(); ++l) {
+    AmgDevLevel& D = al[l];
+    D.ap.run(D.A.v64.as<double>(), D.apv.as<double>(), nullptr, stream);
+    D.rap.run(D.apv.as<double>(), al[l + 1].A.v64.as<double>(), al[l + 1].A.v32.as<float>(), stream);
+    csr_dinv_device(D.n, D.A.ptr.as<int>(), D.A.idx.as<int>(), D.A.v64.as<double>(), D.dinv64.as<double>(),
+                    D.dinv32.as<float>(), stream);
+    D.lmax = power_lmax_csr(D);
+  }
+  pt.mark("algebraic levels (device)");
+  // the coarsest level is inverted on the device (FP64 blocked Gauss-Jordan), then copied to FP32
+  const AmgDevLevel& C = al.back();
+  const size_t nn = (size_t)cinv_n * cinv_n;
+  csr_to_dense_device(cinv_n, C.A.ptr.as<int>(), C.A.idx.as<int>(), C.A.v64.as<double>(), cinv64.as<double>(),
+                      singular, stream);
+  dense_inverse_device(cinv64.as<double>(), cinv_n, singular, cinv_work.as<double>(), stream);
   to_f32(cinv32.as<float>(), cinv64.as<double>(), nn, stream);
-  SIPG_CUDA(cudaStreamSynchronize(stream));  // the host matrix goes out of scope
   pt.mark("coarsest inverse (device)");
 }
 
@@ -601,6 +662,7 @@ void sipg_solver::setup() {
   } catch (...) {
     lv.clear();
     al.clear();
+    amg_frozen = false;
     use_amg = false;
     dirty = true;
     throw;
@@ -1169,6 +1231,7 @@ int sipg_solver_default_opts(int kind, sipg_solver_opts* o) {
     o->assembled_max_order = -1;
     o->smoother = 1;
     o->amg_cheb_order = 2;
+    o->amg_reuse_interpolation = 1;
     for (int l = 0; l < 4; ++l) {
       o->cheb_orders[l] = 0;
       o->pre_it[l] = 1;

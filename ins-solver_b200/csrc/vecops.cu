@@ -1,5 +1,4 @@
 // Vector kernels for the solvers. See vecops.cuh.
-#include <cooperative_groups.h>
 
 #include <stdexcept>
 #include <string>
@@ -11,8 +10,6 @@
 
 #include "pdl.cuh"
 #include "vecops.cuh"
-
-namespace cg = cooperative_groups;
 
 namespace sipg {
 
@@ -636,37 +633,135 @@ __global__ void __launch_bounds__(128) k_inv_mass_n(T* __restrict__ y, const T* 
   }
 }
 
-// In-place Gauss-Jordan inversion of a dense n x n matrix (row-major, FP64) on
-// the device as one cooperative kernel (grid-wide barriers between the phases
-// instead of three launches per pivot). Pivot k:
-//   row:    a[k][j] *= 1 / a[k][k]           (j != k)
-//   update: a[i][j] -= a[i][k] a[k][j]       (i, j != k; a warp per row)
-//   column: a[i][k] *= -1 / a[k][k], a[k][k] = 1 / a[k][k]
+// In-place blocked Gauss-Jordan inversion of a dense n x n matrix (row-major,
+// FP64). For each pivot block K of GJB rows and columns, with P = A_KK^-1:
+//   A_Kj <- P A_Kj                  (j not in K; k_gjb_row)
+//   A_ij <- A_ij - A_iK A_Kj        (i, j not in K, with the new A_Kj; k_gjb_update)
+//   A_iK <- -A_iK P, A_KK <- P      (i not in K; k_gjb_col)
+// which is scalar Gauss-Jordan applied GJB pivots at a time: the trailing update
+// is a rank-GJB product over 64 x 64 tiles instead of n rank-1 passes.
 // No pivoting: the coarsest algebraic operator is symmetric positive definite
-// (a singular one is shifted first), so every pivot is positive.
-__global__ void __launch_bounds__(256) k_gj_coop(double* a, int n) {
-  cg::grid_group grid = cg::this_grid();
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
-  const int lane = threadIdx.x & 31, warp = tid >> 5, nwarps = nth >> 5;
-  for (int k = 0; k < n; ++k) {
-    const double r = 1.0 / a[(size_t)k * n + k];  // nobody writes a[k][k] before the column phase
-    for (int t = tid; t < n; t += nth)
-      if (t != k) a[(size_t)k * n + t] *= r;
-    grid.sync();
-    const double* rowk = a + (size_t)k * n;
-    for (int i = warp; i < n; i += nwarps) {
-      if (i == k) continue;
-      double* rowi = a + (size_t)i * n;
-      const double f = rowi[k];
-      for (int j = lane; j < n; j += 32)
-        if (j != k) rowi[j] -= f * rowk[j];
+// (a singular one is shifted first), so every pivot block is.
+constexpr int GJB = 32;
+
+// P = A_KK^-1 by scalar Gauss-Jordan in shared memory (one block); P is GJB x GJB.
+__global__ void __launch_bounds__(256) k_gjb_pivot(const double* __restrict__ a, int n, int k0, int bs,
+                                                   double* __restrict__ P) {
+  __shared__ double sa[GJB][GJB + 1];
+  for (int t = threadIdx.x; t < bs * bs; t += blockDim.x) {
+    const int i = t / bs, j = t - (t / bs) * bs;
+    sa[i][j] = a[(size_t)(k0 + i) * n + k0 + j];
+  }
+  __syncthreads();
+  for (int k = 0; k < bs; ++k) {
+    const double r = 1.0 / sa[k][k];
+    __syncthreads();
+    for (int j = threadIdx.x; j < bs; j += blockDim.x)
+      if (j != k) sa[k][j] *= r;
+    __syncthreads();
+    for (int t = threadIdx.x; t < bs * bs; t += blockDim.x) {
+      const int i = t / bs, j = t - (t / bs) * bs;
+      if (i != k && j != k) sa[i][j] -= sa[i][k] * sa[k][j];
     }
-    grid.sync();
-    for (int t = tid; t < n; t += nth) {
-      if (t != k) a[(size_t)t * n + k] *= -r;
-      else a[(size_t)k * n + k] = r;
+    __syncthreads();
+    for (int i = threadIdx.x; i < bs; i += blockDim.x) {
+      if (i != k) sa[i][k] *= -r;
+      else sa[k][k] = r;
     }
-    grid.sync();
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < GJB * GJB; t += blockDim.x) {
+    const int i = t / GJB, j = t % GJB;
+    P[t] = (i < bs && j < bs) ? sa[i][j] : 0.0;
+  }
+}
+
+// Row panel: one thread per column j outside K.
+__global__ void __launch_bounds__(256) k_gjb_row(double* __restrict__ a, int n, int k0, int bs,
+                                                 const double* __restrict__ P) {
+  __shared__ double sp[GJB * GJB];
+  for (int t = threadIdx.x; t < GJB * GJB; t += blockDim.x) sp[t] = P[t];
+  __syncthreads();
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n || (j >= k0 && j < k0 + bs)) return;
+  double col[GJB];
+#pragma unroll
+  for (int m = 0; m < GJB; ++m) col[m] = m < bs ? a[(size_t)(k0 + m) * n + j] : 0.0;
+#pragma unroll
+  for (int i = 0; i < GJB; ++i) {
+    if (i >= bs) break;
+    double s = 0.0;
+#pragma unroll
+    for (int m = 0; m < GJB; ++m) s += sp[i * GJB + m] * col[m];
+    a[(size_t)(k0 + i) * n + j] = s;
+  }
+}
+
+// Trailing update over 64 x 64 tiles, 256 threads, 4 x 4 entries per thread
+// (rows ty + 16 u, columns tx + 16 v: coalesced loads and stores).
+__global__ void __launch_bounds__(256) k_gjb_update(double* __restrict__ a, int n, int k0, int bs) {
+  __shared__ double sc[64][GJB + 1];  // A_iK of the tile's rows
+  __shared__ double sw[GJB][64 + 1];  // A_Kj of the tile's columns
+  const int i0 = blockIdx.y * 64, j0 = blockIdx.x * 64;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  for (int t = threadIdx.x; t < 64 * GJB; t += 256) {
+    const int r = t / GJB, m = t % GJB;
+    sc[r][m] = (i0 + r < n && m < bs) ? a[(size_t)(i0 + r) * n + k0 + m] : 0.0;
+  }
+  for (int t = threadIdx.x; t < GJB * 64; t += 256) {
+    const int m = t / 64, c = t % 64;
+    sw[m][c] = (j0 + c < n && m < bs) ? a[(size_t)(k0 + m) * n + j0 + c] : 0.0;
+  }
+  __syncthreads();
+  double acc[4][4] = {};
+#pragma unroll 8
+  for (int m = 0; m < GJB; ++m) {
+    double cv[4], wv[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) cv[u] = sc[ty + 16 * u][m];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) wv[v] = sw[m][tx + 16 * v];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) acc[u][v] += cv[u] * wv[v];
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const int i = i0 + ty + 16 * u;
+    if (i >= n || (i >= k0 && i < k0 + bs)) continue;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int j = j0 + tx + 16 * v;
+      if (j >= n || (j >= k0 && j < k0 + bs)) continue;
+      a[(size_t)i * n + j] -= acc[u][v];
+    }
+  }
+}
+
+// Column panel: one thread per row i; rows of K receive P.
+__global__ void __launch_bounds__(128) k_gjb_col(double* __restrict__ a, int n, int k0, int bs,
+                                                 const double* __restrict__ P) {
+  __shared__ double sp[GJB * GJB];
+  for (int t = threadIdx.x; t < GJB * GJB; t += blockDim.x) sp[t] = P[t];
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double* row = a + (size_t)i * n + k0;
+  if (i >= k0 && i < k0 + bs) {
+    for (int j = 0; j < bs; ++j) row[j] = sp[(i - k0) * GJB + j];
+    return;
+  }
+  double rv[GJB];
+#pragma unroll
+  for (int m = 0; m < GJB; ++m) rv[m] = m < bs ? row[m] : 0.0;
+#pragma unroll
+  for (int j = 0; j < GJB; ++j) {
+    if (j >= bs) break;
+    double s = 0.0;
+#pragma unroll
+    for (int m = 0; m < GJB; ++m) s += rv[m] * sp[m * GJB + j];
+    row[j] = -s;
   }
 }
 // Row sums, column sums and the total of a dense matrix (one thread per row /
@@ -1129,23 +1224,18 @@ void csr_cheb(int rows, const int* ptr, const int* idx, const T* val, const T* d
 void dense_inverse_device(double* a, int n, bool project_constants, double* work, cudaStream_t s) {
   const size_t nn = (size_t)n * n;
   const int g2 = (int)std::min<size_t>((nn + 255) / 256, 148 * 8);
-  // every block of the cooperative kernel must be resident at once
-  static int per_sm = 0;
-  if (per_sm == 0) {
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gj_coop, 256, 0) != cudaSuccess || per_sm < 1)
-      per_sm = 1;
+  double* P = work + 2 * (size_t)n;  // GJB x GJB pivot-block inverse
+  const int tiles = (n + 63) / 64;
+  for (int k0 = 0; k0 < n; k0 += GJB) {
+    const int bs = std::min(GJB, n - k0);
+    k_gjb_pivot<<<1, 256, 0, s>>>(a, n, k0, bs, P);
+    k_gjb_row<<<(n + 255) / 256, 256, 0, s>>>(a, n, k0, bs, P);
+    k_gjb_update<<<dim3(tiles, tiles), 256, 0, s>>>(a, n, k0, bs);
+    k_gjb_col<<<(n + 127) / 128, 128, 0, s>>>(a, n, k0, bs, P);
+    note_launch(4);
   }
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int grid = std::max(1, std::min(sms * std::min(per_sm, 4), (n + 7) / 8));
-  void* args[] = {&a, &n};
-  const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_gj_coop, dim3(grid), dim3(256), args, 0, s);
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    throw std::runtime_error(std::string("dense inverse: cooperative launch failed: ") + cudaGetErrorString(e));
-  }
-  note_launch();
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) throw std::runtime_error(std::string("dense inverse: ") + cudaGetErrorString(e));
   if (project_constants) {
     k_dense_sums<<<(2 * n + 255) / 256, 256, 0, s>>>(a, n, work, work + n);
     k_dense_project<<<g2, 256, 0, s>>>(a, n, work, work + n);

@@ -166,9 +166,9 @@ void csr_cheb(int rows, const int* ptr, const int* idx, const T* val, const T* d
 // y = M x for a dense row-major n x n matrix
 template <typename T>
 void dense_mv(int n, const T* M, const T* x, T* y, cudaStream_t s);
-// In-place inverse of the dense SPD matrix a (n x n, FP64) by Gauss-Jordan
-// elimination; project_constants applies Q a Q, Q = I - 11^T/n, after it.
-// work: 2n doubles. One cooperative launch (grid-wide barriers between phases).
+// In-place inverse of the dense SPD matrix a (n x n, FP64) by blocked Gauss-Jordan
+// elimination (32 pivots per step, the trailing update as 64 x 64 tiles);
+// project_constants applies Q a Q, Q = I - 11^T/n, after it. work: 2n + 1024 doubles.
 void dense_inverse_device(double* a, int n, bool project_constants, double* work, cudaStream_t s);
 // v_i = 2 U_i - 1, U_i the i-th splitmix64 draw from `seed` (the host SplitMix64 sequence).
 void splitmix_uniform_device(double* v, size_t n, unsigned long long seed, cudaStream_t s);

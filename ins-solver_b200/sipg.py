@@ -50,7 +50,7 @@ class SolverOpts(C.Structure):
                 ("coarse_kind", C.c_int), ("amg_coarse_max", C.c_int), ("amg_strength", C.c_double),
                 ("graphs", C.c_int), ("assembled_max_order", C.c_int), ("smoother", C.c_int),
                 ("cheb_orders", C.c_int * 4), ("pre_it", C.c_int * 4), ("post_it", C.c_int * 4),
-                ("amg_cheb_order", C.c_int)]
+                ("amg_cheb_order", C.c_int), ("amg_reuse_interpolation", C.c_int)]
 
 
 def lib():

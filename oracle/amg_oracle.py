@@ -142,6 +142,27 @@ class Hierarchy:
             self.P.append(P)
             self.R.append(R)
             self.A.append(Ac)
+        self.singular = singular
+        self._coarse()
+
+    def reuse(self, A0):
+        """The hierarchy of a new level-0 operator with the same sparsity, keeping
+        this one's aggregates and prolongators (PETSc GAMG with reuse-interpolation,
+        the reference's `[petsc-amg] reuse-interpolation = 1`,
+        examples/3d/oscillating_droplet/config.ini:59): only the Galerkin
+        products and the coarsest inverse are recomputed."""
+        h = object.__new__(Hierarchy)
+        h.P, h.R, h.Pdg, h.Rdg, h.singular = self.P, self.R, self.Pdg, self.Rdg, self.singular
+        h.A = [A0.tocsr()]
+        for P, R in zip(self.P, self.R):
+            Ac = (R @ (h.A[-1] @ P)).tocsr()
+            Ac.sort_indices()
+            h.A.append(Ac)
+        h._coarse()
+        return h
+
+    def _coarse(self):
+        singular = self.singular
         C = self.A[-1].toarray()
         n = C.shape[0]
         if n > MAX_DENSE_COARSE:

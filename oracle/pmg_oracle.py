@@ -26,9 +26,11 @@ DEFAULTS = dict(cheb_order=4, eig_safety=1.1, eig_ratio=30.0, eig_iters=20, coar
                 amg_cheb_order=2, amg_coarse_max=2048, amg_strength=0.08)
 
 
-def levels(mesh, dim, orders, factor, bc_types, **over):
+def levels(mesh, dim, orders, factor, bc_types, reuse=None, **over):
     """pmg dict for oracle_py.solve: per-order meshes, interpolated factors,
-    prolongations, the AMG hierarchy and the smoother settings."""
+    prolongations, the AMG hierarchy and the smoother settings. reuse: the pmg
+    dict of an earlier set-up on the same mesh whose aggregates and prolongators
+    the new hierarchy keeps (reuse-interpolation)."""
     cfg = dict(DEFAULTS, **over)
     meshes, facs, prol = [], [], []
     for lv, p in enumerate(orders):
@@ -48,16 +50,20 @@ def levels(mesh, dim, orders, factor, bc_types, **over):
         bd = (bct == D.BC_DIRICHLET).astype(np.int32)
         t1 = D.ref_tables(dim, 1)
         A0, Pdg = A.p1_continuous_operator(t1, mesh, f1, tau1, bd)
-        out["amg"] = A.Hierarchy(A0, Pdg, cfg["amg_coarse_max"], cfg["amg_strength"], singular=not bd.any())
+        if reuse is not None:
+            out["amg"] = reuse["amg"].reuse(A0)
+        else:
+            out["amg"] = A.Hierarchy(A0, Pdg, cfg["amg_coarse_max"], cfg["amg_strength"], singular=not bd.any())
     return out
 
 
-def solve_poisson(case, orders=(3, 2, 1), rel_tol=1e-8, max_iter=200, ref_applies=False, **over):
+def solve_poisson(case, orders=(3, 2, 1), rel_tol=1e-8, max_iter=200, ref_applies=False, reuse=None, **over):
     """FP64 p-multigrid FPCG of a dg_oracle workload (pinned DOF or nullspace
-    projection as the case says). Returns (x, info, pmg)."""
+    projection as the case says). reuse: the pmg dict of an earlier solve on the
+    same mesh whose algebraic prolongators are kept. Returns (x, info, pmg)."""
     mesh, e, t = case["mesh"], case["export"], case["tables"]
     om = O.OMesh(t, e)
-    pmg = levels(mesh, e["dim"], orders, case["factor"], case["bc_types"], **over)
+    pmg = levels(mesh, e["dim"], orders, case["factor"], case["bc_types"], reuse=reuse, **over)
     pin = case.get("pin")
     pin_dof = -1 if pin is None else pin[0] * t["Np"] + pin[1]
     x, info = O.solve(om, case["rhs"], case["bc_types"], O.PRE_PMG, case["factor"], abs_tol=0.0,

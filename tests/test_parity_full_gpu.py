@@ -94,6 +94,71 @@ def test_default_pmultigrid_mixed_against_oracle(n):
     assert err <= MIXED_C2_BOUND
 
 
+# ------------------------------------------- the next time step: set-up again
+def moved_factor(case, n, shift):
+    """1 / rho of the two-phase case with the heavy sphere moved by (shift, 0, -shift)."""
+    e = case["export"]
+    return 1.0 / D.two_phase_rho(e["x"], e["y"], e["z"], 1.0 / n, center=(0.5 + shift, 0.5, 0.5 - shift))
+
+
+@pytest.mark.parametrize("precision", [sipg.FP64, sipg.FP32], ids=["fp64", "mixed"])
+def test_second_time_step_reuses_interpolation_like_the_oracle(precision):
+    """A solve, then the density moves and the solver is set up again (the
+    reference's per-step reset before the pressure solve). The library keeps the
+    first set-up's aggregates and prolongators and recomputes the level operators,
+    smoother data and coarsest inverse on the device; the oracle's hierarchy does
+    the same from its own first set-up (Hierarchy.reuse). A coarse limit of 40
+    unknowns gives three algebraic levels at 6^3 x 6."""
+    n, cmax, shift = 6, 40, 0.08
+    gc = W.poisson3d_two_phase(n, order=3, n_modes=64, pin=False)
+    oc = D.poisson3d_two_phase(n, order=3, n_modes=64, pin=False)
+    _, io1, pmg1 = P.solve_poisson(oc, amg_coarse_max=cmax)
+    assert pmg1["amg"].nlevels >= 3
+    oc2 = dict(oc, factor=moved_factor(oc, n, shift))
+    xo, io, _ = P.solve_poisson(oc2, reuse=pmg1, amg_coarse_max=cmax)
+    assert io1.converged and io.converged
+    op = sipg.Operator(gc["mesh"], 3, 1)
+    op.set_bc_types(gc["bc_types"])
+    op.set_factor(gc["factor"])
+    o = sipg.default_opts(sipg.SOLVER_PMULTIGRID)
+    o.precision, o.rel_tol, o.abs_tol, o.max_iter, o.nullspace = precision, 1e-8, 0.0, 500, 1
+    o.amg_coarse_max = cmax
+    s = sipg.Solver(op, sipg.SOLVER_PMULTIGRID, o)
+    _, i1 = s.solve_host(gc["rhs"])
+    assert i1.status == sipg.SIPG_OK and abs(i1.iters - io1.iters) <= 1
+    op.set_factor(moved_factor(gc, n, shift))
+    s.setup()
+    x, info = s.solve_host(gc["rhs"])
+    assert info.status == sipg.SIPG_OK
+    assert abs(info.iters - io.iters) <= 1
+    assert info.true_rel_res <= 1e-8
+    assert rel_l2(x, xo) <= (1e-9 if precision == sipg.FP64 else MIXED_C2_BOUND)
+
+
+def test_set_up_without_reuse_equals_a_fresh_solver():
+    """amg_reuse_interpolation = 0 aggregates again at every set-up: a solver set
+    up a second time on a new factor gives the iterates of a solver created on it."""
+    n, shift = 6, 0.08
+    gc = W.poisson3d_two_phase(n, order=3, n_modes=64, pin=False)
+    f2 = moved_factor(gc, n, shift)
+    res = []
+    for fresh in (False, True):
+        op = sipg.Operator(gc["mesh"], 3, 1)
+        op.set_bc_types(gc["bc_types"])
+        op.set_factor(f2 if fresh else gc["factor"])
+        o = sipg.default_opts(sipg.SOLVER_PMULTIGRID)
+        o.precision, o.rel_tol, o.abs_tol, o.max_iter, o.nullspace = sipg.FP64, 1e-8, 0.0, 500, 1
+        o.amg_coarse_max, o.amg_reuse_interpolation = 40, 0
+        s = sipg.Solver(op, sipg.SOLVER_PMULTIGRID, o)
+        if not fresh:
+            s.solve_host(gc["rhs"])
+            op.set_factor(f2)
+            s.setup()
+        res.append(s.solve_host(gc["rhs"]))
+    (xa, ia), (xb, ib) = res
+    assert ia.iters == ib.iters and np.array_equal(xa, xb)
+
+
 # ------------------------------------------------------- full-size applies
 @pytest.fixture(scope="module")
 def c2():
