@@ -142,6 +142,14 @@ int sipg_op_diag_host(sipg_op *op, double *diag);
  * invert != 0 returns the inverses. ref_volume_block != 0 reproduces the
  * reference's volume block formula (fvmf_3d_op1.h:17-18). */
 int sipg_op_block_diag_host(sipg_op *op, int invert, int ref_volume_block, double *blocks);
+/* The assembled form of a scalar operator of order 1 or 2: per element row e its
+ * Np x Np blocks against itself (s = 0) and against the neighbour across each
+ * face f (s = 1 + f; zero on boundary faces), columns in the neighbour's node
+ * order, layout blocks[((s * Np + r) * Np + c) * K + e], (dim + 2) Np^2 K values.
+ * These are the element-block matrices the p-multigrid applies on its low-order
+ * levels; they stand in for the assembled coarse matrices of OP2-DG-Toolkit
+ * (PoissonCoarseMatrix, unvendored) behind the reference's PETSc coarse solve. */
+int sipg_op_element_blocks_host(sipg_op *op, double *blocks);
 int sipg_op_sizes(const sipg_op *op, int *K, int *Np, int *Nfp, int *ncomp);
 void sipg_op_destroy(sipg_op *op);
 

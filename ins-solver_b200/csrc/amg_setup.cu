@@ -6,6 +6,7 @@
 #include <stdexcept>
 
 #include "refelem.hpp"
+#include "sipg_apply.cuh"
 #include "vecops.cuh"
 
 namespace sipg {
@@ -25,37 +26,6 @@ P1Tables p1_tables(const RefElement& r) {
 }
 
 namespace {
-
-// Outward unit normal and surface Jacobian of face f of an affine simplex from
-// its geometric factors (rx ry rz sx sy sz tx ty tz J / rx ry sx sy J), as the
-// host mesh computes them.
-template <int DIM>
-__device__ void p1_face_normal(const double* g, int f, double n[3], double* sJ) {
-  n[2] = 0.0;
-  if (DIM == 3) {
-    for (int d = 0; d < 3; ++d) {
-      double v;
-      if (f == 0) v = -g[6 + d];
-      else if (f == 1) v = -g[3 + d];
-      else if (f == 2) v = (g[d] + g[3 + d]) + g[6 + d];
-      else v = -g[d];
-      n[d] = v;
-    }
-  } else {
-    for (int d = 0; d < 2; ++d) {
-      double v;
-      if (f == 0) v = -g[2 + d];
-      else if (f == 1) v = g[d] + g[2 + d];
-      else v = -g[d];
-      n[d] = v;
-    }
-  }
-  const double len = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
-  n[0] /= len;
-  n[1] /= len;
-  n[2] /= len;
-  *sJ = len * g[DIM == 3 ? 9 : 4];
-}
 
 // One thread per element; the block stays in registers (Np <= 4).
 template <int DIM>
@@ -108,7 +78,7 @@ __global__ void k_p1c_blocks(P1Tables t, int K, const double* __restrict__ geof,
     const int nb = nbr[(size_t)e * NF + f];
     if (nb >= 0 || bct[-nb - 1] != 0) continue;  // interior jumps vanish; Neumann and slip add nothing
     double n[3], sJ;
-    p1_face_normal<DIM>(g, f, n, &sJ);
+    simplex_face_normal<DIM>(g, f, n, &sJ);
     double rf[3] = {0.0, 0.0, 0.0};
 #pragma unroll
     for (int r = 0; r < DIM; ++r)

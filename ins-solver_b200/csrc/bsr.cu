@@ -1,4 +1,4 @@
-// Element-block form of low-order SIPG operators: probing assembly and apply.
+// Element-block form of low-order SIPG operators: assembly and apply.
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -9,7 +9,9 @@
 
 #include "../../include/sipg_b200.h"
 #include "bsr.cuh"
+#include "capi_util.hpp"
 #include "pdl.cuh"
+#include "sipg_blocks.cuh"
 #include "vecops.cuh"
 
 namespace sipg {
@@ -17,27 +19,194 @@ namespace {
 
 int grid_of(size_t n) { return (int)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, 148 * 16)); }
 
-__global__ void k_probe_set(double* x, const int* list, int n, int node, int Np) {
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
-    x[(size_t)list[j] * Np + node] = 1.0;
-}
-
-// Column (e, node) of the blocks of every row element k adjacent to a probed element e.
-__global__ void k_probe_extract(const double* y, const int* list, int n, int node, const int* nbr,
-                                const uint32_t* fcode, int K, int Np, int NF, double* v) {
-  const int per = (NF + 1) * Np;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n * per; t += gridDim.x * blockDim.x) {
-    const int j = t / per, q = t % per;
-    const int s = q / Np, r = q % Np;
-    const int e = list[j];
-    int k = e, slot = 0;
-    if (s > 0) {
-      k = nbr[(size_t)e * NF + s - 1];
-      if (k < 0) continue;
-      slot = 1 + (int)((fcode[e] >> (8 * (s - 1))) & 3u);
-    }
-    v[((size_t)(slot * Np + r) * Np + node) * K + k] = y[(size_t)k * Np + r];
+// Element-row blocks of the operator straight from the terms of the apply
+// (sipg_apply.cu; FactorViscousMatrix3D::mult, factor_viscous_matrix.cpp:96-310),
+// one thread per (row r, element e), e fastest (coalesced block stores), 64 per block. With
+// Dx_d = sum_r G[r][d] D_r, Dn = sum_r (n . G[r]) D_r, F the nodal factor, MF the
+// face mass, m_j / m+_j the own / neighbour node at face node j, scale = sJ / 2 on
+// interior faces and sJ on Dirichlet faces (jump 2u, average n.q):
+//   self:      J sum_d Dx_d^T M F Dx_d + J M diag(mm)
+//              + rows on the face: scale MF (tau I - F Dn) at the face nodes
+//              + columns m_j:      -scale f(m_j) sum_a Dn[m_a][r] MF[a][j]
+//   neighbour: rows on the face:   -scale MF (tau I + F+ Dn+) at the matched nodes
+//              columns m+_j:       +scale f(m_j) sum_a Dn[m_a][r] MF[a][j]
+// (Dn+ built from the neighbour's G with this element's normal). The apply reads
+// a pinned DOF as zero and returns pin_scale times it in its row: its column is
+// zero and its row holds pin_scale on the diagonal only.
+template <int DIM, int P>
+__global__ void __launch_bounds__(64) k_bsr_direct(BlockArgs a, const uint32_t* __restrict__ fcode,
+                                                    double* __restrict__ v) {
+  using C = Cfg<DIM, P>;
+  constexpr int NP = C::NP, NFP = C::NFP, NF = C::NF, LD = C::LD, NG = C::NG, NPERM = C::NPERM;
+  __shared__ double sD[DIM][NP][NP], sM[NP][NP], sMF[NF][NFP][NFP];
+  __shared__ int sfm[NF][NFP], sperm[NPERM][NFP];
+  // the thread's row of every block, one shared-memory column per thread (the
+  // entries are addressed through the face-node tables)
+  __shared__ double sacc[(NF + 1) * NP][64];
+#define ACC(s_, c_) sacc[(s_) * NP + (c_)][threadIdx.x]
+  for (int t = threadIdx.x; t < DIM * NP * NP; t += blockDim.x) {
+    const int d = t / (NP * NP), i = (t / NP) % NP, j = t % NP;
+    sD[d][i][j] = a.consts[C::OFF_D + d * NP * LD + i * LD + j];
   }
+  for (int t = threadIdx.x; t < NP * NP; t += blockDim.x) sM[t / NP][t % NP] = a.consts[C::OFF_M + (t / NP) * LD + t % NP];
+  for (int t = threadIdx.x; t < NF * NFP * NFP; t += blockDim.x) (&sMF[0][0][0])[t] = a.mf[t];
+  for (int t = threadIdx.x; t < NF * NFP; t += blockDim.x) (&sfm[0][0])[t] = a.itab[t];
+  for (int t = threadIdx.x; t < NPERM * NFP; t += blockDim.x) (&sperm[0][0])[t] = a.itab[NF * NFP + t];
+  __syncthreads();
+  const size_t K = (size_t)a.K;
+  for (size_t tid = blockIdx.x * (size_t)blockDim.x + threadIdx.x; tid < K * NP; tid += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(tid / K), e = (int)(tid - (size_t)r * K);
+    double g[NG], f[NP];
+#pragma unroll
+    for (int i = 0; i < NG; ++i) g[i] = a.geof[(size_t)e * NG + i];
+#pragma unroll
+    for (int i = 0; i < NP; ++i) f[i] = a.factor ? a.factor[(size_t)e * NP + i] : 1.0;
+    for (int q = 0; q < (NF + 1) * NP; ++q) sacc[q][threadIdx.x] = 0.0;
+    const double J = g[DIM == 3 ? 9 : 4];
+    // volume row r: J sum_d sum_q t_d[q] Dx_d[q][p], t_d[q] = f(q) sum_m Dx_d[m][r] M[m][q],
+    // summed as sum_rr sum_q u_rr[q] D_rr[q][p] with u_rr[q] = sum_d G[rr][d] t_d[q]
+    {
+      double u[DIM][NP];
+      {
+        double t[DIM][NP];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+          double col[NP];
+#pragma unroll
+          for (int m = 0; m < NP; ++m) {
+            double s = 0.0;
+#pragma unroll
+            for (int rr = 0; rr < DIM; ++rr) s += g[rr * DIM + d] * sD[rr][m][r];
+            col[m] = s;
+          }
+#pragma unroll
+          for (int q = 0; q < NP; ++q) {
+            double s = 0.0;
+#pragma unroll
+            for (int m = 0; m < NP; ++m) s += col[m] * sM[m][q];
+            t[d][q] = J * f[q] * s;
+          }
+        }
+#pragma unroll
+        for (int rr = 0; rr < DIM; ++rr)
+#pragma unroll
+          for (int q = 0; q < NP; ++q) {
+            double s = 0.0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) s += g[rr * DIM + d] * t[d][q];
+            u[rr][q] = s;
+          }
+      }
+#pragma unroll 1
+      for (int p = 0; p < NP; ++p) {
+        double s = 0.0;
+#pragma unroll
+        for (int rr = 0; rr < DIM; ++rr)
+#pragma unroll
+          for (int q = 0; q < NP; ++q) s += u[rr][q] * sD[rr][q][p];
+        ACC(0, p) += s;
+      }
+    }
+#pragma unroll 1
+    for (int fc = 0; fc < NF; ++fc) {
+      const int nb = a.nbr[(size_t)e * NF + fc];
+      if (nb < 0 && a.bct[-nb - 1] != BC_DIRICHLET) continue;  // Neumann (and scalar slip): no face terms
+      double n[3], sJ;
+      simplex_face_normal<DIM>(g, fc, n, &sJ);
+      const double scale = nb >= 0 ? 0.5 * sJ : sJ;
+      const double tau = a.tau[(size_t)e * NF + fc];
+      double rf[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+      for (int rr = 0; rr < DIM; ++rr)
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) rf[rr] += n[d] * g[rr * DIM + d];
+      // neighbour data: matched nodes, factor, geometry
+      int nm[NFP];
+      double rfn[3] = {0.0, 0.0, 0.0};
+      const double* gn = nullptr;
+      if (nb >= 0) {
+        const int code = (fcode[e] >> (8 * fc)) & 0xff;
+#pragma unroll
+        for (int j = 0; j < NFP; ++j) nm[j] = sfm[code & 3][sperm[code >> 2][j]];
+        gn = a.geof + (size_t)nb * NG;
+#pragma unroll
+        for (int rr = 0; rr < DIM; ++rr)
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) rfn[rr] += n[d] * gn[rr * DIM + d];
+      }
+      // columns: -/+ scale f(m_j) sum_a Dn[m_a][r] MF[a][j]
+      double dnr[NFP];
+#pragma unroll
+      for (int aa = 0; aa < NFP; ++aa) {
+        double s = 0.0;
+#pragma unroll
+        for (int rr = 0; rr < DIM; ++rr) s += rf[rr] * sD[rr][sfm[fc][aa]][r];
+        dnr[aa] = s;
+      }
+#pragma unroll
+      for (int j = 0; j < NFP; ++j) {
+        double cj = 0.0;
+#pragma unroll
+        for (int aa = 0; aa < NFP; ++aa) cj += dnr[aa] * sMF[fc][aa][j];
+        const double w = scale * f[sfm[fc][j]] * cj;
+        ACC(0, sfm[fc][j]) -= w;
+        if (nb >= 0) ACC(1 + fc, nm[j]) += w;
+      }
+      // rows on the face
+      int ar = -1;
+#pragma unroll
+      for (int aa = 0; aa < NFP; ++aa)
+        if (sfm[fc][aa] == r) ar = aa;
+      if (ar < 0) continue;
+#pragma unroll 1
+      for (int j = 0; j < NFP; ++j) {
+        const double w = scale * sMF[fc][ar][j];
+        const int mj = sfm[fc][j];
+        ACC(0, mj) += w * tau;
+        const double wf = w * f[mj];
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+          double dn = 0.0;
+#pragma unroll
+          for (int rr = 0; rr < DIM; ++rr) dn += rf[rr] * sD[rr][mj][p];
+          ACC(0, p) -= wf * dn;
+        }
+        if (nb >= 0) {
+          const int q = nm[j];
+          ACC(1 + fc, q) -= w * tau;
+          const double wfn = w * (a.factor ? a.factor[(size_t)nb * NP + q] : 1.0);
+#pragma unroll
+          for (int c = 0; c < NP; ++c) {
+            double dn = 0.0;
+#pragma unroll
+            for (int rr = 0; rr < DIM; ++rr) dn += rfn[rr] * sD[rr][q][c];
+            ACC(1 + fc, c) -= wfn * dn;
+          }
+        }
+      }
+    }
+    if (a.mm_mode != MM_NONE)
+#pragma unroll
+      for (int p = 0; p < NP; ++p) ACC(0, p) += J * sM[r][p] * (a.mm_mode == MM_SCALAR ? a.mm_scalar : a.mm[(size_t)e * NP + p]);
+    // the pinned DOF is read as zero by every row (its column vanishes) ...
+    if (a.pin_elem >= 0) {
+      if (e == a.pin_elem) ACC(0, a.pin_node) = 0.0;
+      for (int fc = 0; fc < NF; ++fc)
+        if (a.nbr[(size_t)e * NF + fc] == a.pin_elem) ACC(1 + fc, a.pin_node) = 0.0;
+    }
+    // ... and its own row is pin_scale times itself
+    if (e == a.pin_elem && r == a.pin_node) {
+#pragma unroll
+      for (int s = 0; s <= NF; ++s)
+#pragma unroll
+        for (int c = 0; c < NP; ++c) ACC(s, c) = (s == 0 && c == r) ? a.pin_scale : 0.0;
+    }
+#pragma unroll
+    for (int s = 0; s <= NF; ++s)
+#pragma unroll
+      for (int c = 0; c < NP; ++c) v[((size_t)(s * NP + r) * NP + c) * K + e] = ACC(s, c);
+  }
+#undef ACC
 }
 
 __global__ void k_d2f(float* dst, const double* src, size_t n) {
@@ -236,57 +405,28 @@ __global__ void __launch_bounds__(256, 2) k_bsr16_cheb(int K, const __half* __re
 
 }  // namespace
 
-std::vector<int> distance2_colours(int K, int NF, const int* nbr, int* ncolours) {
-  std::vector<int> col(K, -1);
-  std::vector<int> stamp(64 * 4 + 64, -1);
-  int nc = 0;
-  for (int e = 0; e < K; ++e) {
-    // colours used within distance 2 of e
-    auto mark = [&](int k) {
-      if (k >= 0 && col[k] >= 0) {
-        if (col[k] >= (int)stamp.size()) stamp.resize(col[k] + 1, -1);
-        stamp[col[k]] = e;
-      }
-    };
-    for (int f = 0; f < NF; ++f) {
-      const int k = nbr[(size_t)e * NF + f];
-      if (k < 0) continue;
-      mark(k);
-      for (int g = 0; g < NF; ++g) mark(nbr[(size_t)k * NF + g]);
-    }
-    int c = 0;
-    while (c < (int)stamp.size() && stamp[c] == e) ++c;
-    col[e] = c;
-    nc = std::max(nc, c + 1);
+void element_blocks_device(const sipg_op* op, double* v, cudaStream_t s) {
+  if (op->ncomp != 1) throw Error(SIPG_INVALID_ARG, "element blocks need a scalar operator");
+  const sipg_mesh* m = op->mesh;
+  const BlockArgs a = op->block_args(BLOCK_FULL, 0, v, true);
+  const size_t n = (size_t)m->K * op->Np;
+  const int g = (int)std::max<size_t>(1, std::min<size_t>((n + 63) / 64, 148 * 32));
+  const uint32_t* fc = m->fcode.as<uint32_t>();
+  switch (m->dim * 10 + op->order) {
+    case 21: k_bsr_direct<2, 1><<<g, 64, 0, s>>>(a, fc, v); break;
+    case 22: k_bsr_direct<2, 2><<<g, 64, 0, s>>>(a, fc, v); break;
+    case 31: k_bsr_direct<3, 1><<<g, 64, 0, s>>>(a, fc, v); break;
+    case 32: k_bsr_direct<3, 2><<<g, 64, 0, s>>>(a, fc, v); break;
+    default: throw Error(SIPG_INVALID_ARG, "element blocks: orders 1 and 2 only");
   }
-  *ncolours = nc;
-  return col;
+  note_launch();
+  SIPG_CUDA(cudaGetLastError());
 }
 
 void bsr_assemble(sipg_op* op, BsrOp& B, bool want32, cudaStream_t s, const double* binv_rows, bool binv_sym) {
   if (op->ncomp != 1) throw Error(SIPG_INVALID_ARG, "assembled blocks need a scalar operator");
   sipg_mesh* m = op->mesh;
   const int K = m->K, Np = op->Np, NF = m->dim + 1;
-  // the colouring depends on the mesh only: built once, kept on the mesh
-  {
-    std::lock_guard<std::mutex> lk(m->probe_mu);
-    if (m->probe_off.empty()) {
-      const Mesh& h = m->host_order(1);
-      int ncol = 0;
-      std::vector<int> col = distance2_colours(K, NF, h.nbr.data(), &ncol);
-      std::vector<int> o(ncol + 1, 0), list(K);
-      for (int e = 0; e < K; ++e) ++o[col[e] + 1];
-      for (int c = 0; c < ncol; ++c) o[c + 1] += o[c];
-      std::vector<int> fill(o.begin(), o.end() - 1);
-      for (int e = 0; e < K; ++e) list[fill[col[e]]++] = e;
-      DevBuf dl((size_t)K * sizeof(int));
-      dl.upload(list.data(), (size_t)K * sizeof(int));
-      m->probe_list = std::move(dl);
-      m->probe_off = std::move(o);
-    }
-  }
-  const std::vector<int>& off = m->probe_off;
-  const int nc = (int)off.size() - 1;
   B.K = K;
   B.Np = Np;
   B.NF = NF;
@@ -294,24 +434,7 @@ void bsr_assemble(sipg_op* op, BsrOp& B, bool want32, cudaStream_t s, const doub
   B.nbr = m->nbr.as<int>();
   const size_t nv = (size_t)(NF + 1) * Np * Np * K;
   ensure(B.v64, nv * sizeof(double));
-  SIPG_CUDA(cudaMemsetAsync(B.v64.p, 0, nv * sizeof(double), s));
-  ensure(B.probe_x, (size_t)K * Np * sizeof(double));
-  ensure(B.probe_y, (size_t)K * Np * sizeof(double));
-  DevBuf& x = B.probe_x;
-  DevBuf& y = B.probe_y;
-  for (int c = 0; c < nc; ++c) {
-    const int n = off[c + 1] - off[c];
-    const int* lc = m->probe_list.as<int>() + off[c];
-    for (int i = 0; i < Np; ++i) {
-      SIPG_CUDA(cudaMemsetAsync(x.p, 0, (size_t)K * Np * sizeof(double), s));
-      k_probe_set<<<grid_of(n), 256, 0, s>>>(x.as<double>(), lc, n, i, Np);
-      note_launch();
-      op->apply<double>(x.as<double>(), y.as<double>(), s);
-      k_probe_extract<<<grid_of((size_t)n * (NF + 1) * Np), 256, 0, s>>>(
-          y.as<double>(), lc, n, i, m->nbr.as<int>(), m->fcode.as<uint32_t>(), K, Np, NF, B.v64.as<double>());
-      note_launch();
-    }
-  }
+  element_blocks_device(op, B.v64.as<double>(), s);
   const bool half = want32 && Np % 2 == 0;  // two rows per thread in k_bsr16
   if (half) {
     ensure(B.v16, nv * sizeof(__half));
@@ -402,3 +525,14 @@ template void bsr_apply<double>(const BsrOp&, const double*, double*, double, do
 template void bsr_apply<float>(const BsrOp&, const float*, float*, float, float, cudaStream_t, const float*);
 
 }  // namespace sipg
+
+extern "C" int sipg_op_element_blocks_host(sipg_op* op, double* blocks) {
+  using namespace sipg;
+  return guarded([&] {
+    if (!op || !blocks) throw Error(SIPG_INVALID_ARG, "element_blocks arguments");
+    const size_t n = (size_t)(op->mesh->dim + 2) * op->Np * op->Np * op->mesh->K;
+    DevBuf d(n * sizeof(double));
+    element_blocks_device(op, d.as<double>(), 0);
+    SIPG_CUDA(cudaMemcpy(blocks, d.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+  });
+}

@@ -8,11 +8,9 @@
 // chosen order store these blocks once and apply them as a block-sparse
 // product (one thread per element row, coalesced block reads).
 //
-// The blocks are assembled by probing the matrix-free apply in FP64: elements
-// are coloured so that no two elements of one colour share a face neighbour
-// (distance-2 colouring of the face graph); for every colour c and local node i
-// the apply of the indicator vector sum_{e in c} e_(e,i) gives column (e, i) of
-// the blocks of every row element adjacent to e, without overlap.
+// The blocks are computed in FP64 by one kernel straight from the terms of the
+// matrix-free apply (volume, face fluxes with the neighbour's factor and
+// geometry, mass, pinned row), a thread per element row.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -36,14 +34,18 @@ struct BsrOp {
   // element row), same layout and scaling as v16: one kernel per Chebyshev step
   // (k_bsr16_cheb) then updates the preconditioned residual directly
   DevBuf c16, cscale16;
-  DevBuf probe_x, probe_y, c64;  // assembly workspace, kept for the next set-up
+  DevBuf c64;  // assembly workspace, kept for the next set-up
   const int* nbr = nullptr;  // mesh K x NF (device)
 };
 
 // Orders whose element blocks have an assembled apply (Np x Np registers per thread).
 inline bool bsr_supported(int dim, int order, int ncomp) { return ncomp == 1 && order >= 1 && order <= 2 && dim >= 2; }
 
-// Assemble from the operator's FP64 apply; want32: also the FP32 V-cycle's copy
+// Element-row blocks of a scalar operator of order 1 or 2 (FP64, the values
+// layout above) on the device.
+void element_blocks_device(const sipg_op* op, double* v, cudaStream_t s);
+
+// Assemble in FP64; want32: also the FP32 V-cycle's copy
 // (scaled FP16 for even Np, the FP64 values then released; FP32 otherwise).
 // binv_rows (FP32 V-cycle, even Np): the inverse diagonal blocks, row-major per
 // element, for the preconditioned copy C (binv_sym: with their symmetric part, as
@@ -63,7 +65,5 @@ void bsr_apply(const BsrOp& B, const T* x, T* y, T alpha, T beta, cudaStream_t s
 void bsr_cheb_step(const BsrOp& B, const float* din, float* dout, float* sres, float* z, float c1, float c2,
                    float s0_scale, cudaStream_t s);
 
-// Greedy distance-2 colouring of the face graph (nbr: K x NF, negative = boundary).
-std::vector<int> distance2_colours(int K, int NF, const int* nbr, int* ncolours);
 
 }  // namespace sipg

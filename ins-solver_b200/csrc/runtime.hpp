@@ -73,9 +73,7 @@ struct sipg_mesh {
   sipg::DevBuf tcg64, tcg32;  // geometry blocks of the tensor-core apply (launch_tc_geom)
   std::shared_ptr<sipg::P1Plan> p1_plan;  // algebraic coarse space: sparsity of the P1 operator (set-up cache)
   std::shared_ptr<void> p1_gather;        // its assembly from element blocks as device term lists (set-up cache)
-  sipg::DevBuf probe_list;    // assembled levels: elements grouped by distance-2 colour (set-up cache)
-  std::vector<int> probe_off;  // colour c: probe_list[probe_off[c] .. probe_off[c+1])
-  std::mutex probe_mu;
+  std::mutex probe_mu;         // guards the set-up caches above
   sipg::DevBuf proj_h;        // velocity projection: 1 / max interior-face fscale per element
   sipg::DevBuf proj_io;       // velocity projection: device copies for the host-buffer entry point
   std::mutex proj_mu;         // serialises host-buffer projections on this mesh

@@ -47,6 +47,34 @@ struct Cfg {
   static constexpr int ITAB = NF * NFP + NPERM * NFP;
 };
 
+#ifdef __CUDACC__
+// Outward unit normal n and surface Jacobian sJ of face f of an affine simplex
+// from its geometric factors g (3D rx ry rz sx sy sz tx ty tz J, faces t = -1,
+// s = -1, r + s + t = -1, r = -1; 2D rx ry sx sy J, faces s = -1, r + s = 0, r = -1).
+template <int DIM>
+__device__ __forceinline__ void simplex_face_normal(const double* g, int f, double n[3], double* sJ) {
+  n[2] = 0.0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    const double* gr = g;        // d r / d x
+    const double* gs = g + DIM;  // d s / d x
+    double v;
+    if (DIM == 3) {
+      const double* gt = g + 6;
+      v = f == 0 ? -gt[d] : f == 1 ? -gs[d] : f == 2 ? (gr[d] + gs[d]) + gt[d] : -gr[d];
+    } else {
+      v = f == 0 ? -gs[d] : f == 1 ? gr[d] + gs[d] : -gr[d];
+    }
+    n[d] = v;
+  }
+  const double len = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+  n[0] /= len;
+  n[1] /= len;
+  n[2] /= len;
+  *sJ = len * g[DIM == 3 ? 9 : 4];
+}
+#endif
+
 // Boundary condition types (problem_specific_3d.h: 0 Dirichlet, 1 Neumann; slip 2).
 enum : int { BC_DIRICHLET = 0, BC_NEUMANN = 1, BC_SLIP = 2 };
 

@@ -89,8 +89,9 @@ __global__ void k_recip(double* d, size_t n) {
     d[i] = 1.0 / d[i];
 }
 
-__global__ void k_scale(double* v, size_t n, const double* scal, int slot) {
-  const double inv = 1.0 / sqrt(scal[slot]);
+template <typename T>
+__global__ void k_scale(T* v, size_t n, const double* scal, int slot) {
+  const T inv = (T)(1.0 / sqrt(scal[slot]));
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     v[i] *= inv;
 }
@@ -314,6 +315,7 @@ struct sipg_solver {
   int solve(const double* b, double* x, sipg_solve_info* info);
   double power_lmax(sipg_op* lop, const double* dinv64, size_t nl, const double* blocks = nullptr, int Np = 0);
   double power_lmax_csr(const AmgDevLevel& D);
+  double power_lmax_f32(Level& L);
 };
 
 // Diagonal of an operator (FP64), with its pinned DOF.
@@ -338,7 +340,7 @@ double sipg_solver::power_lmax(sipg_op* lop, const double* dinv64, size_t nl, co
   for (int it = 0; it < o.eig_iters; ++it) {
     const double* a[1] = {v};
     multi_dot<double>(a, a, 1, nl, S() + S_TMP, 1, rw, stream);
-    k_scale<<<grid_for(nl), 256, 0, stream>>>(v, nl, S(), S_TMP);
+    k_scale<double><<<grid_for(nl), 256, 0, stream>>>(v, nl, S(), S_TMP);
     note_launch();
     if (blocks) {
       lop->apply<double>(v, tb, stream);
@@ -357,6 +359,42 @@ double sipg_solver::power_lmax(sipg_op* lop, const double* dinv64, size_t nl, co
   return lam;
 }
 
+// The FP32 V-cycle's levels with element-block Jacobi smoothing: the same power
+// iteration on the operator the smoother sees, B^-1 A with the level's FP32 apply
+// (TF32 matrix-free, or the assembled FP16 blocks) and its BF16 inverse blocks.
+double sipg_solver::power_lmax_f32(Level& L) {
+  const size_t nl = L.n;
+  if (pl_v.bytes < nl * sizeof(double)) {
+    pl_v = DevBuf(nl * sizeof(double));
+    pl_w = DevBuf(nl * sizeof(double));
+    pl_t = DevBuf(nl * sizeof(double));
+  }
+  float* v = pl_v.as<float>();
+  float* w = pl_w.as<float>();
+  float* t = pl_t.as<float>();
+  splitmix_uniform_device(pl_w.as<double>(), nl, 0x5eedull, stream);
+  to_f32(v, pl_w.as<double>(), nl, stream);
+  const int nb = (int)(nl / L.Np);
+  for (int it = 0; it < o.eig_iters; ++it) {
+    const float* a[1] = {v};
+    multi_dot<float>(a, a, 1, nl, S() + S_TMP, 1, rw, stream);
+    k_scale<float><<<grid_for(nl), 256, 0, stream>>>(v, nl, S(), S_TMP);
+    note_launch();
+    L.apply<float>(v, t, stream);
+    // w = B^-1 t (a first Chebyshev step with c2 = 1; the level's z is scratch here)
+    if (L.bsym)
+      cheb_step_sym<float, __nv_bfloat16>(w, L.z.as<float>(), t, L.bc32.as<__nv_bfloat16>(), 0.0f, 1.0f, nb, L.Np,
+                                          stream, true);
+    else
+      cheb_step_block<float, __nv_bfloat16>(w, L.z.as<float>(), t, L.bc32.as<__nv_bfloat16>(), 0.0f, 1.0f, nb,
+                                            L.Np, stream, true);
+    std::swap(v, w);
+  }
+  const float* b[1] = {v};
+  multi_dot<float>(b, b, 1, nl, S() + S_TMP, 1, rw, stream);
+  return std::sqrt(read_scalar(S_TMP));
+}
+
 // The same power iteration on D^-1 A for an algebraic level (CSR, FP64).
 double sipg_solver::power_lmax_csr(const AmgDevLevel& D) {
   const size_t nl = (size_t)D.n;
@@ -371,7 +409,7 @@ double sipg_solver::power_lmax_csr(const AmgDevLevel& D) {
   for (int it = 0; it < o.eig_iters; ++it) {
     const double* a[1] = {v};
     multi_dot<double>(a, a, 1, nl, S() + S_TMP, 1, rw, stream);
-    k_scale<<<grid_for(nl), 256, 0, stream>>>(v, nl, S(), S_TMP);
+    k_scale<double><<<grid_for(nl), 256, 0, stream>>>(v, nl, S(), S_TMP);
     note_launch();
     D.A.mv<double>(v, w, 1.0, 0.0, stream);
     k_mul<<<grid_for(nl), 256, 0, stream>>>(w, D.dinv64.as<double>(), nl);
@@ -499,14 +537,15 @@ void sipg_solver::setup_pmg() {
         block_transpose<double>(L.bc64.as<double>(), rows.as<double>(), nb, L.Np, stream);
       }
       pt.mark("diagonal and blocks", l);
-      L.lmax = power_lmax(L.op, nullptr, L.n, rows.as<double>(), L.Np);
+      // the FP32 V-cycle estimates its bound after the assembly, on its own operator
+      if (!f32) L.lmax = power_lmax(L.op, nullptr, L.n, rows.as<double>(), L.Np);
     } else {
       L.bc64 = DevBuf();
       L.bc32 = DevBuf();
       pt.mark("diagonal", l);
       L.lmax = power_lmax(L.op, L.dinv64.as<double>(), L.n);
     }
-    pt.mark("eigenvalue bound", l);
+    if (!(f32 && o.smoother == 1)) pt.mark("eigenvalue bound", l);
     // -1: p = 2 and below in the FP32 V-cycle (p = 2 as scaled FP16 blocks: half the
     // bytes of the matrix-free apply's per-element work, same iteration counts), p = 1
     // in the FP64 V-cycle (FP64 blocks at p = 2 move more bytes than the matrix-free apply)
@@ -524,6 +563,10 @@ void sipg_solver::setup_pmg() {
       }
     } else {
       L.bsr.reset();
+    }
+    if (f32 && o.smoother == 1) {
+      L.lmax = power_lmax_f32(L);
+      pt.mark("eigenvalue bound", l);
     }
   }
   use_amg = o.coarse_kind == 1 && nc == 1 && lv.back().order == 1;

@@ -344,6 +344,16 @@ class Operator:
         check(lib().sipg_op_block_diag_host(self.h, int(invert), int(ref_volume_block), _dp(b)))
         return b
 
+    def element_blocks_host(self):
+        """Assembled element-row blocks (order 1 or 2, scalar): array
+        [1 + Nf, Np (row), Np (column), K]; block s = 1 + f couples to the
+        neighbour across face f in that neighbour's node order."""
+        K = self.mesh.K
+        nf = self.mesh.dim + 1
+        b = np.zeros((nf + 1, self.Np, self.Np, K))
+        check(lib().sipg_op_element_blocks_host(self.h, _dp(b)))
+        return b
+
     def __del__(self):
         if getattr(self, "h", None) and self.h:
             lib().sipg_op_destroy(self.h)
