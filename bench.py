@@ -391,8 +391,8 @@ def run_ours(args):
     }
     out["config_2d"] = run_config_2d()
     out["projection"] = run_projection(cpu=rank == 0 and world == 1 and not args.skip_cpu)
-    if not args.skip_serving:
-        out["serving"] = serving_sweep(seed=1234 + rank)
+    if not args.skip_serving and world == 1:
+        out["serving"] = run_serving(slots=args.serve_slots)
     if rank == 0 and world == 1 and not args.skip_cpu:
         out["cpu_baseline"] = cpu_baseline_sample(c, int(inf64[-1].iters))
     if world > 1:
@@ -584,26 +584,11 @@ def run_config_2d(reps=5):
             "max_error_vs_exact": err}
 
 
-def serving_problems(rng):
-    """A pool of resident problems for the served stream: 2D and 3D jittered boxes,
-    orders 2 and 3, constant or two-phase (ratio 1000) coefficient, element counts
-    from 2e3 to 1.1e4 (a scaled-down form of the served-stream configuration)."""
-    probs = []
-    for dim, n, order in ((3, 8, 2), (3, 10, 3), (3, 12, 2), (2, 32, 3), (2, 64, 2), (2, 48, 3)):
-        if dim == 3:
-            c = W.poisson3d_two_phase(n, order=order, n_modes=64, pin=False)
-            factor = c["factor"] if rng.random() < 0.5 else None
-            bct, rhs = c["bc_types"], c["rhs"].reshape(-1)
-        else:
-            c = W.poisson2d_manufactured(n, order=order)
-            factor, bct, rhs = None, c["bc_types"], c["rhs"].reshape(-1)
-        op = sipg.Operator(c["mesh"], order, 1)
-        op.set_bc_types(bct)
-        if factor is not None:
-            op.set_factor(factor)
-        singular = dim == 3
-        probs.append((op, rhs, singular, order))
-    return probs
+SERVE_RATES = (50.0, 100.0, 200.0, 500.0, 1000.0, 2000.0)
+SERVE_REQUESTS = 512
+SERVE_POOL = 32
+SERVE_SLOTS = 4
+SERVE_BUDGET = 150 * 10**9
 
 
 def serving_opts(order, singular, precision):
@@ -615,29 +600,11 @@ def serving_opts(order, singular, precision):
     return o
 
 
-def serving_sweep(seed):
-    """The served stream below capacity (400 arrivals/s: latency) and above it
-    (2000/s: the throughput the server sustains); the headline fields are the
-    saturated run's."""
-    low = run_serving(seed, n_req=96, rate=400.0)
-    high = run_serving(seed, n_req=192, rate=2000.0)
-    keys = ("solves_per_s", "p50_ms", "p99_ms", "failed")
-    return {**high, "sweep": [{"rate_per_s": 400.0, **{k: low[k] for k in keys}},
-                              {"rate_per_s": 2000.0, **{k: high[k] for k in keys}}]}
-
-
-def run_serving(seed, n_req=96, rate=400.0, slots=4):
-    """Served stream: n_req requests with Poisson arrivals at `rate` per second over
-    the problem pool, mixed-precision p-multigrid to 1e-8, `slots` concurrent solves;
-    against the same requests solved one at a time on the plain FP64 path."""
-    rng = np.random.default_rng(seed)
-    probs = serving_problems(rng)
+def serving_stream(srv, probs, ops, rate, n_req, rng):
+    """n_req requests with Poisson arrivals at `rate` per second, each a solve of a
+    problem drawn uniformly from the pool; returns the stream's record and its picks."""
     pick = rng.integers(0, len(probs), n_req)
     gaps = rng.exponential(1.0 / rate, n_req)
-    srv = sipg.Server(slots=slots)
-    # resident solver states: one warm request per problem (set-up is not part of the stream)
-    for op, rhs, sing, order in probs:
-        srv.wait(srv.submit(op, sipg.SOLVER_PMULTIGRID, serving_opts(order, sing, sipg.FP32), rhs))
     ids = []
     t0 = time.perf_counter()
     t_next = t0
@@ -645,32 +612,78 @@ def run_serving(seed, n_req=96, rate=400.0, slots=4):
         t_next += gaps[i]
         while time.perf_counter() < t_next:
             time.sleep(max(0.0, min(0.001, t_next - time.perf_counter())))
-        op, rhs, sing, order = probs[pick[i]]
-        ids.append(srv.submit(op, sipg.SOLVER_PMULTIGRID, serving_opts(order, sing, sipg.FP32), rhs))
-    lat, bad = [], 0
+        p = probs[pick[i]]
+        ids.append(srv.submit(ops[pick[i]], sipg.SOLVER_PMULTIGRID, serving_opts(p["order"], True, sipg.FP32),
+                              p["rhs"]))
+    lat, bad, iters = [], 0, []
     for rid in ids:
         _, res = srv.wait(rid)
         lat.append(res.total_ms)
+        iters.append(res.info.iters)
         bad += res.status != sipg.SIPG_OK
     served_s = time.perf_counter() - t0
-    srv.close()
-    # sequential plain FP64 solves of the same requests (solvers set up beforehand)
-    seq = [sipg.Solver(op, sipg.SOLVER_PMULTIGRID, serving_opts(order, sing, sipg.FP64)) for op, _, sing, order in probs]
-    for (op, rhs, _, _), s in zip(probs, seq):
-        s.solve_host(rhs)
-    t1 = time.perf_counter()
-    for i in range(n_req):
-        op, rhs, _, _ = probs[pick[i]]
-        seq[pick[i]].solve_host(rhs)
-    seq_s = time.perf_counter() - t1
     lat = np.array(lat)
-    return {"workload": f"{n_req} requests, Poisson arrivals {rate:g}/s, {len(probs)} resident problems "
-                        "(2D/3D, p=2/3, K 2048..10368, constant or two-phase coefficient), mixed p-MG to 1e-8, "
-                        f"{slots} slots",
-            "solves_per_s": n_req / served_s, "p50_ms": float(np.percentile(lat, 50)),
+    return {"rate_per_s": rate, "solves_per_s": n_req / served_s, "p50_ms": float(np.percentile(lat, 50)),
             "p99_ms": float(np.percentile(lat, 99)), "failed": int(bad),
-            "sequential_fp64_solves_per_s": n_req / seq_s,
-            "speedup_vs_sequential_fp64": (n_req / served_s) / (n_req / seq_s)}
+            "mean_iters": float(np.mean(iters))}, pick
+
+
+def sequential_solves(probs, ops, pick, precision):
+    """The same requests solved one at a time through the host-buffer solve
+    (solvers set up and warmed beforehand): solves/s."""
+    solvers = [sipg.Solver(op, sipg.SOLVER_PMULTIGRID, serving_opts(p["order"], True, precision))
+               for p, op in zip(probs, ops)]
+    for p, s in zip(probs, solvers):
+        s.solve_host(p["rhs"])
+    t0 = time.perf_counter()
+    for i in pick:
+        solvers[i].solve_host(probs[i]["rhs"])
+    return len(pick) / (time.perf_counter() - t0)
+
+
+def run_serving(seed=1234, slots=SERVE_SLOTS):
+    """The served solve stream at its stated size: SERVE_REQUESTS requests per
+    arrival rate in SERVE_RATES over a pool of SERVE_POOL distinct resident
+    problems drawn from the stream's distribution (2D 60 % / 3D 40 %, K
+    log-uniform in [2e3, 3e5], p in {2, 3, 4}, two-phase with probability 0.5,
+    Gaussian random field right-hand sides), mixed p-multigrid to 1e-8 with
+    `slots` concurrent solves under a 150 GB HBM budget. Baselines: the
+    saturated stream's requests solved one at a time on the FP64 path and on the
+    same mixed path (the second isolates the gain of overlapping solves)."""
+    probs = W.served_stream_pool(SERVE_POOL)
+    ops = []
+    for p in probs:
+        op = sipg.Operator(p["mesh"], p["order"], 1)
+        op.set_bc_types(p["bc_types"])
+        if p["factor"] is not None:
+            op.set_factor(p["factor"])
+        ops.append(op)
+    srv = sipg.Server(slots=slots, hbm_budget_bytes=SERVE_BUDGET)
+    # resident solver states: one request per problem first (set-up is not part of the stream)
+    for p, op in zip(probs, ops):
+        srv.wait(srv.submit(op, sipg.SOLVER_PMULTIGRID, serving_opts(p["order"], True, sipg.FP32), p["rhs"]))
+    rng = np.random.default_rng(seed)
+    sweep, pick = [], None
+    for rate in SERVE_RATES:
+        rec, pick = serving_stream(srv, probs, ops, rate, SERVE_REQUESTS, rng)
+        sweep.append(rec)
+    resident = srv.stats()
+    srv.close()
+    seq64 = sequential_solves(probs, ops, pick, sipg.FP64)
+    seq32 = sequential_solves(probs, ops, pick, sipg.FP32)
+    top = sweep[-1]
+    Ks = np.array([p["K"] for p in probs])
+    return {"workload": f"{SERVE_REQUESTS} requests per rate, Poisson arrivals at {list(SERVE_RATES)}/s, "
+                        f"{len(probs)} resident problems (2D {sum(p['dim'] == 2 for p in probs)} / 3D "
+                        f"{sum(p['dim'] == 3 for p in probs)}, K {int(Ks.min())}..{int(Ks.max())} log-uniform in "
+                        "[2e3, 3e5], p in {2,3,4}, two-phase or constant coefficient, GRF right-hand sides), "
+                        f"mixed p-MG to 1e-8, {slots} slots, HBM budget 150 GB",
+            "solves_per_s": top["solves_per_s"], "p50_ms": top["p50_ms"], "p99_ms": top["p99_ms"],
+            "failed": int(sum(r["failed"] for r in sweep)),
+            "sequential_fp64_solves_per_s": seq64, "sequential_mixed_solves_per_s": seq32,
+            "speedup_vs_sequential_fp64": top["solves_per_s"] / seq64,
+            "speedup_vs_sequential_mixed": top["solves_per_s"] / seq32,
+            "resident_bytes": int(resident["resident_bytes"]), "sweep": sweep}
 
 
 def omp_threads(n):
@@ -932,6 +945,8 @@ def main():
     ap.add_argument("--skip-c3", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-serving", action="store_true")
+    ap.add_argument("--serving-only", action="store_true", help="run only the served stream; print its record")
+    ap.add_argument("--serve-slots", type=int, default=SERVE_SLOTS, help="concurrent solves of the served stream")
     args = ap.parse_args()
     if args.impl == "ours" or args.profile:
         global sipg, W
@@ -940,6 +955,8 @@ def main():
         sipg, W = _sipg, _workloads
     if args.profile:
         run_profile(args)
+    elif args.serving_only:
+        print(json.dumps({"serving": run_serving(slots=args.serve_slots)}))
     elif args.impl == "reference":
         run_reference(args)
     else:

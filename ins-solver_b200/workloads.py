@@ -62,6 +62,47 @@ def poisson3d_two_phase(n, order=3, jitter=0.1, seed=20261203, rhs_seed=7, n_mod
                 pin=(0, 0) if pin else None, rho=rho)
 
 
+def served_poisson(dim, n, order, two_phase, seed, n_modes=32):
+    """One problem of the served stream: a box of 2 n^2 triangles or 6 n^3 tets,
+    interior vertices jittered +-0.1h (seed), Neumann walls (constants projected
+    out), right-hand side J M (Gaussian random field with correlation length 0.1
+    minus its mean, seed + 1), factor 1/rho with rho = 1000 in a ball (disc) of
+    radius 0.25 at the centre and 1 outside, or constant 1."""
+    mesh = sipg.Mesh.box(dim, n, jitter=0.1, seed=seed)
+    e = mesh.export(order)
+    t = sipg.ref_tables(dim, order)
+    coords = [e["x"], e["y"]] + ([e["z"]] if dim == 3 else [])
+    factor = None
+    if two_phase:
+        zc = e["z"] if dim == 3 else np.full_like(e["x"], 0.5)
+        factor = 1.0 / two_phase_rho(e["x"], e["y"], zc, 1.0 / n)
+    pts = np.stack([c.ravel() for c in coords], 1)
+    f = grf(pts, 0.1, n_modes, seed + 1).reshape(e["K"], t["Np"])
+    b = mass_apply(e, t, f)
+    f = f - b.sum() / mass_apply(e, t, np.ones_like(f)).sum()
+    b = mass_apply(e, t, f)
+    bct = np.full((1, e["Kb"]), sipg.BC_NEUMANN, np.int32)
+    return dict(mesh=mesh, dim=dim, order=order, K=e["K"], factor=factor, rhs=b.reshape(-1), bc_types=bct,
+                two_phase=bool(two_phase))
+
+
+def served_stream_pool(n_problems, seed=4):
+    """Distinct problems drawn from the served-stream distribution: 2D with
+    probability 0.6 (else 3D), element count log-uniform in [2e3, 3e5] (the box
+    size nearest to it), order uniform in {2, 3, 4}, two-phase coefficient with
+    probability 0.5."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_problems):
+        dim = 2 if rng.random() < 0.6 else 3
+        K = float(np.exp(rng.uniform(np.log(2e3), np.log(3e5))))
+        order = int(rng.integers(2, 5))
+        two = bool(rng.random() < 0.5)
+        n = max(4, int(round((K / 2) ** 0.5))) if dim == 2 else max(3, int(round((K / 6) ** (1.0 / 3.0))))
+        out.append(served_poisson(dim, n, order, two, seed=1000 + 17 * i))
+    return out
+
+
 def poisson2d_manufactured(n, order=3):
     """2D Poisson with zero Dirichlet data and exact solution sin(2 pi x) sin(2 pi y)."""
     mesh = sipg.Mesh.box(2, n, jitter=0.0, seed=0)
