@@ -142,6 +142,28 @@ int sipg_op_diag_host(sipg_op *op, double *diag);
  * invert != 0 returns the inverses. ref_volume_block != 0 reproduces the
  * reference's volume block formula (fvmf_3d_op1.h:17-18). */
 int sipg_op_block_diag_host(sipg_op *op, int invert, int ref_volume_block, double *blocks);
+/* ---- over-integrated factor: FactorPoissonMatrixFreeDiagOI3D (OP2-DG-Toolkit,
+ * unvendored), selected by [pressure-solve] over_int (src/solvers/3d/
+ * mp_ins_solver.cpp:81-88) and set in update_pressure_matrices_oi (:524-544).
+ * The factor (1/rho) is given at nq volume cubature points per element
+ * (mat_free_set_factor_oi) and at nqs surface cubature points per element face
+ * (mat_free_set_factor_surf_oi); the operator integrates every SIPG term with
+ * these points (the symmetric form: each face term that carries one side's
+ * factor uses that side's points) and uses the L2 projection of the volume
+ * values as its nodal factor (set_factor(CUB3D_PROJ f), the coarse levels'
+ * factor). The rules are the library's own (collapsed Gauss-Legendre, exact to
+ * degree 2p + 1 in the volume and 2p on the faces; the toolkit's are not in the
+ * reference tree): sipg_op_oi_points_host gives their physical coordinates,
+ * where the caller evaluates rho (getRhoVolOI / getRhoSurfOI). Scalar operators;
+ * sipg_op_set_factor returns to the nodal factor. */
+int sipg_op_oi_sizes(const sipg_op *op, int *nq, int *nqs);
+/* xyz_vol: dim x K x nq, xyz_surf: dim x K x (dim + 1) x nqs (either may be NULL). */
+int sipg_op_oi_points_host(sipg_op *op, double *xyz_vol, double *xyz_surf);
+/* fvol: K x nq, fsurf: K x (dim + 1) x nqs, host pointers (synchronous) ... */
+int sipg_op_set_factor_oi(sipg_op *op, const double *fvol, const double *fsurf);
+/* ... or device pointers, ordered on `stream`. */
+int sipg_op_set_factor_oi_device(sipg_op *op, const double *fvol, const double *fsurf, void *stream);
+
 /* The assembled form of a scalar operator of order 1 or 2: per element row e its
  * Np x Np blocks against itself (s = 0) and against the neighbour across each
  * face f (s = 1 + f; zero on boundary faces), columns in the neighbour's node

@@ -126,6 +126,12 @@ extern "C" int sipg_op_apply_static_scratch(sipg_op* op, int precision, const vo
   return guarded([&] {
     if (!op || !x || !y) throw Error(SIPG_INVALID_ARG, "apply arguments");
     cudaStream_t s = (cudaStream_t)stream;
+    if (op->oi) {  // the over-integrated operator's block-sparse apply needs no scratch
+      if (precision == SIPG_FP64) op->apply<double>((const double*)x, (double*)y, s);
+      else if (precision == SIPG_FP32) op->apply<float>((const float*)x, (float*)y, s);
+      else throw Error(SIPG_INVALID_ARG, "precision must be 64 or 32");
+      return;
+    }
     if (precision == SIPG_FP64) apply_static<double>(op, (const double*)x, (double*)y, s);
     else if (precision == SIPG_FP32) apply_static<float>(op, (const float*)x, (float*)y, s);
     else throw Error(SIPG_INVALID_ARG, "precision must be 64 or 32");

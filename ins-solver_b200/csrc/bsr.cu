@@ -495,6 +495,11 @@ void bsr_apply(const BsrOp& B, const T* x, T* y, T alpha, T beta, cudaStream_t s
   else if (B.dim == 3 && B.Np == 10) pdl_launch(k_bsr<T, 10, 4>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta, c);
   else if (B.dim == 2 && B.Np == 3) pdl_launch(k_bsr<T, 3, 3>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta, c);
   else if (B.dim == 2 && B.Np == 6) pdl_launch(k_bsr<T, 6, 3>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta, c);
+  // orders 3 and 4 (the over-integrated operator's blocks)
+  else if (B.dim == 3 && B.Np == 20) pdl_launch(k_bsr<T, 20, 4>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta, c);
+  else if (B.dim == 3 && B.Np == 35) pdl_launch(k_bsr<T, 35, 4>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta, c);
+  else if (B.dim == 2 && B.Np == 10) pdl_launch(k_bsr<T, 10, 3>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta, c);
+  else if (B.dim == 2 && B.Np == 15) pdl_launch(k_bsr<T, 15, 3>, dim3(g), dim3(256), 0, s, B.K, v, B.nbr, x, y, alpha, beta, c);
   else throw Error(SIPG_INVALID_ARG, "no assembled apply for this element");
   note_launch();
   SIPG_CUDA(cudaGetLastError());

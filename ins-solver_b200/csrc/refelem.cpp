@@ -358,6 +358,69 @@ static void lagrange_at(const RefElement& e, const std::vector<double>& Vinv, do
   }
 }
 
+void collapsed_rule(int dim, int n, std::vector<double>& qr, std::vector<double>& qs, std::vector<double>& qt,
+                    std::vector<double>& qw) {
+  // Gauss-Legendre nodes in ascending order, the first collapsed direction outermost
+  std::vector<double> x, w;
+  gauss_legendre(n, x, w);
+  std::vector<int> ord(n);
+  for (int i = 0; i < n; ++i) ord[i] = i;
+  std::sort(ord.begin(), ord.end(), [&](int a, int b) { return x[a] < x[b]; });
+  std::vector<double> xs(n), ws(n);
+  for (int i = 0; i < n; ++i) { xs[i] = x[ord[i]]; ws[i] = w[ord[i]]; }
+  qr.clear(); qs.clear(); qt.clear(); qw.clear();
+  if (dim == 1) {
+    qr = xs;
+    qw = ws;
+    qs.assign(n, 0.0);
+    qt.assign(n, 0.0);
+    return;
+  }
+  if (dim == 2) {
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j) {
+        const double a = xs[i], b = xs[j];
+        qr.push_back((1 + a) * (1 - b) / 2 - 1);
+        qs.push_back(b);
+        qt.push_back(0.0);
+        qw.push_back(ws[i] * ws[j] * (1 - b) / 2);
+      }
+    return;
+  }
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j)
+      for (int k = 0; k < n; ++k) {
+        const double a = xs[i], b = xs[j], c = xs[k];
+        qr.push_back((1 + a) * (1 - b) * (1 - c) / 4 - 1);
+        qs.push_back((1 + b) * (1 - c) / 2 - 1);
+        qt.push_back(c);
+        qw.push_back(ws[i] * ws[j] * ws[k] * (1 - b) * (1 - c) * (1 - c) / 8);
+      }
+}
+
+void face_param_point(int dim, int f, double a, double b, double* r, double* s, double* t) {
+  face_point(dim, f, a, b, r, s, t);
+}
+
+void lagrange_at_points(const RefElement& e, const std::vector<double>& r, const std::vector<double>& s,
+                        const std::vector<double>& t, std::vector<double>& phi, std::vector<double>* dphi) {
+  const int Np = e.Np;
+  const size_t n = r.size();
+  const std::vector<double> Vinv = inverse(e.V, Np);
+  phi.assign(n * Np, 0.0);
+  if (dphi) dphi->assign(3 * n * Np, 0.0);
+  std::vector<double> dr(Np), ds(Np), dt(Np);
+  for (size_t q = 0; q < n; ++q) {
+    lagrange_at(e, Vinv, r[q], s[q], t.empty() ? 0.0 : t[q], &phi[q * Np], dr.data(), ds.data(), dt.data());
+    if (dphi)
+      for (int i = 0; i < Np; ++i) {
+        (*dphi)[(0 * n + q) * Np + i] = dr[i];
+        (*dphi)[(1 * n + q) * Np + i] = ds[i];
+        (*dphi)[(2 * n + q) * Np + i] = e.dim == 3 ? dt[i] : 0.0;
+      }
+  }
+}
+
 RefElement build_ref_element(int dim, int order) {
   if ((dim != 2 && dim != 3) || order < 1 || order > kMaxOrder)
     throw std::runtime_error("unsupported element: dim=" + std::to_string(dim) +

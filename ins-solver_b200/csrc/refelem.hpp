@@ -60,6 +60,20 @@ std::vector<double> interp_matrix(int dim, int q, int p);
 // position a on this face to position sigma[a] on the neighbour's face.
 const int* face_vertex_perm(int dim, int sigma);
 
+// Collapsed Gauss-Legendre rule with n points per direction on the reference
+// simplex (weights sum to its volume; exact for degree 2n - 3 in 3D, 2n - 2 in
+// 2D; dim 1: the Gauss-Legendre rule on [-1, 1], exact for 2n - 1). Nodes a, b, c
+// ascending, a outermost: r = (1+a)(1-b)(1-c)/4 - 1, s = (1+b)(1-c)/2 - 1, t = c
+// (2D: r = (1+a)(1-b)/2 - 1, s = b).
+void collapsed_rule(int dim, int n, std::vector<double>& qr, std::vector<double>& qs, std::vector<double>& qt,
+                    std::vector<double>& qw);
+// Reference coordinates of the face-parameter point (a, b) on face f (the
+// parameter domain is the reference triangle in 3D, [-1, 1] in 2D).
+void face_param_point(int dim, int f, double a, double b, double* r, double* s, double* t);
+// Nodal basis (and its reference derivatives, 3 x n x Np, d/dr d/ds d/dt) at n points.
+void lagrange_at_points(const RefElement& e, const std::vector<double>& r, const std::vector<double>& s,
+                        const std::vector<double>& t, std::vector<double>& phi, std::vector<double>* dphi);
+
 inline int np_of(int dim, int p) {
   return dim == 2 ? (p + 1) * (p + 2) / 2 : (p + 1) * (p + 2) * (p + 3) / 6;
 }

@@ -8,6 +8,7 @@
 
 #include "../../include/sipg_b200.h"
 #include "capi_util.hpp"
+#include "bsr.cuh"
 #include "runtime.hpp"
 #include "sipg_blocks.cuh"
 #include "vecops.cuh"
@@ -185,6 +186,10 @@ void sipg_mesh::ensure_device() {
 template <typename T>
 void sipg_op::apply(const T* x, T* y, cudaStream_t s, T alpha, T beta, const T* c) const {
   constexpr bool f64 = std::is_same<T, double>::value;
+  if (oi) {  // over-integrated factor: the assembled element blocks
+    bsr_apply<T>(*oi_blocks, x, y, alpha, beta, s, c);
+    return;
+  }
   ApplyArgs<T> a;
   a.consts = f64 ? (const T*)dref->c64.p : (const T*)dref->c32.p;
   a.itab = dref->itab.as<int8_t>();
@@ -479,6 +484,7 @@ int sipg_op_set_factor(sipg_op* op, const double* factor) {
   return guarded([&] {
     if (!op) throw Error(SIPG_INVALID_ARG, "null op");
     ++op->version;
+    op->oi = false;  // a nodal factor replaces a cubature-point one
     size_t n = (size_t)op->mesh->K * op->Np;
     if (!factor) {
       op->has_factor = false;
@@ -515,6 +521,10 @@ int sipg_op_set_mm(sipg_op* op, int mode, double scalar, const double* mm) {
       op->mm32.upload(m32.data(), n * sizeof(float));
     }
     op->refresh_pin(0);
+    if (op->oi) {
+      oi_assemble(op, 0);
+      SIPG_CUDA(cudaDeviceSynchronize());
+    }
   });
 }
 
@@ -531,6 +541,10 @@ int sipg_op_set_bc_types(sipg_op* op, const int* types) {
     }
     if (n) op->bct.upload(b.data(), n);
     op->refresh_pin(0);
+    if (op->oi) {
+      oi_assemble(op, 0);
+      SIPG_CUDA(cudaDeviceSynchronize());
+    }
   });
 }
 
@@ -538,11 +552,19 @@ int sipg_op_set_pin(sipg_op* op, int elem, int node) {
   return guarded([&] {
     if (!op) throw Error(SIPG_INVALID_ARG, "null op");
     ++op->version;
-    if (elem < 0) { op->pin_elem = -1; op->pin_node = -1; return; }
-    if (elem >= op->mesh->K || node < 0 || node >= op->Np) throw Error(SIPG_INVALID_ARG, "pin out of range");
-    op->pin_elem = elem;
-    op->pin_node = node;
-    op->refresh_pin(0);
+    if (elem < 0) {
+      op->pin_elem = -1;
+      op->pin_node = -1;
+    } else {
+      if (elem >= op->mesh->K || node < 0 || node >= op->Np) throw Error(SIPG_INVALID_ARG, "pin out of range");
+      op->pin_elem = elem;
+      op->pin_node = node;
+      op->refresh_pin(0);
+    }
+    if (op->oi) {
+      oi_assemble(op, 0);
+      SIPG_CUDA(cudaDeviceSynchronize());
+    }
   });
 }
 

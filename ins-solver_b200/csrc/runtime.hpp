@@ -84,6 +84,10 @@ struct sipg_mesh {
   void ensure_device();  // upload geometry/connectivity on first device use
 };
 
+namespace sipg {
+struct BsrOp;
+}
+
 struct sipg_op {
   sipg_mesh* mesh = nullptr;
   int order = 0, ncomp = 1, Np = 0, Nfp = 0;
@@ -101,6 +105,12 @@ struct sipg_op {
   int kernel = 0;  // 0: tensor cores where available, 1: CUDA cores
   unsigned version = 0;  // bumped by every setter: solvers re-capture their graphs
   mutable sipg::DevBuf trace64, trace32;  // face traces of the two-pass tensor-core apply
+  // over-integrated factor (sipg_op_set_factor_oi): the factor at the volume and
+  // surface cubature points, and the element blocks the operator then applies;
+  // factor64 holds its nodal projection (the p-multigrid levels' factor)
+  bool oi = false;
+  sipg::DevBuf oi_fvol, oi_fsurf;
+  std::shared_ptr<sipg::BsrOp> oi_blocks;
   // Apply on device buffers in precision T.
   template <typename T>
   // y = alpha A x + beta c, c = y when null (beta == 0: c is not read)
@@ -116,4 +126,9 @@ std::unique_ptr<sipg_op> create_op(sipg_mesh* m, int order, int ncomp);
 void set_factor_device(sipg_op* op, const double* f64, cudaStream_t s);
 void set_mm_device(sipg_op* op, int mode, double scalar, const double* mm64, cudaStream_t s);
 void set_bc_types_host(sipg_op* op, const std::vector<int>& types);
+// Over-integrated factor (oi.cu): copy the cubature-point factor (K x nq and
+// K x Nf x nqs, host or device pointers), then assemble; oi_assemble again from
+// the stored factor after the boundary types, mass term or pinned DOF change.
+void set_factor_oi_device(sipg_op* op, const double* fvol, const double* fsurf, cudaStream_t s);
+void oi_assemble(sipg_op* op, cudaStream_t s);
 }  // namespace sipg

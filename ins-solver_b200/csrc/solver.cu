@@ -432,12 +432,17 @@ void sipg_solver::setup_pmg() {
   sipg_mesh* m = op->mesh;
   const int K = m->K, nc = op->ncomp, dim = m->dim;
   PhaseTimer pt(stream);
+  if (!lv.empty() && op->oi != (lv[0].own != nullptr)) {  // nodal <-> over-integrated factor: levels anew
+    lv.clear();
+    al.clear();
+    amg_frozen = false;
+  }
   if (lv.empty()) {
     lv.resize(nl);
     for (int l = 0; l < nl; ++l) {
       Level& L = lv[l];
       L.order = o.orders[l];
-      if (l == 0) {
+      if (l == 0 && !op->oi) {
         L.op = op;
       } else {
         L.own = create_op(m, L.order, nc);
@@ -466,6 +471,26 @@ void sipg_solver::setup_pmg() {
         L.P32.upload(P32.data(), P32.size() * sizeof(float));
       }
     }
+  }
+  // An over-integrated operator is the outer solver's; the V-cycle's finest level
+  // is its nodal twin with the projected factor (the factor of the reference's
+  // coarse levels, mp_ins_solver.cpp:538-543), kept current here.
+  if (op->oi) {
+    Level& L0 = lv[0];
+    set_bc_types_host(L0.op, op->bct_host);
+    set_factor_device(L0.op, op->factor64.as<double>(), stream);
+    if (op->mm_mode == SIPG_MM_NODAL) {
+      if (!L0.mm64.p) L0.mm64 = DevBuf((size_t)K * L0.Np * sizeof(double));
+      SIPG_CUDA(cudaMemcpyAsync(L0.mm64.p, op->mm64.p, (size_t)K * L0.Np * sizeof(double), cudaMemcpyDeviceToDevice,
+                                stream));
+      set_mm_device(L0.op, SIPG_MM_NODAL, 0.0, L0.mm64.as<double>(), stream);
+    } else {
+      set_mm_device(L0.op, op->mm_mode, op->mm_scalar, nullptr, stream);
+    }
+    L0.op->pin_elem = op->pin_elem;
+    L0.op->pin_node = op->pin_node;
+    SIPG_CUDA(cudaStreamSynchronize(stream));
+    if (op->pin_elem >= 0) L0.op->refresh_pin(stream);
   }
   // Coefficients of the coarse levels: interpolate the fine nodal factor / mm.
   for (int l = 1; l < nl; ++l) {

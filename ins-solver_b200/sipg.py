@@ -344,6 +344,29 @@ class Operator:
         check(lib().sipg_op_block_diag_host(self.h, int(invert), int(ref_volume_block), _dp(b)))
         return b
 
+    def oi_sizes(self):
+        """(nq, nqs): volume and per-face surface cubature points of the
+        over-integrated factor."""
+        nq, nqs = C.c_int(), C.c_int()
+        check(lib().sipg_op_oi_sizes(self.h, C.byref(nq), C.byref(nqs)))
+        return nq.value, nqs.value
+
+    def oi_points(self):
+        """Physical coordinates of the cubature points: (dim, K, nq) and (dim, K, Nf, nqs)."""
+        nq, nqs = self.oi_sizes()
+        d, K = self.mesh.dim, self.mesh.K
+        xv = np.zeros((d, K, nq))
+        xs = np.zeros((d, K, d + 1, nqs))
+        check(lib().sipg_op_oi_points_host(self.h, _dp(xv), _dp(xs)))
+        return xv, xs
+
+    def set_factor_oi(self, fvol, fsurf):
+        """Over-integrated factor: fvol (K, nq) and fsurf (K, Nf, nqs) at the
+        points of oi_points()."""
+        fvol = np.ascontiguousarray(fvol, dtype=np.float64)
+        fsurf = np.ascontiguousarray(fsurf, dtype=np.float64)
+        check(lib().sipg_op_set_factor_oi(self.h, _dp(fvol), _dp(fsurf)))
+
     def element_blocks_host(self):
         """Assembled element-row blocks (order 1 or 2, scalar): array
         [1 + Nf, Np (row), Np (column), K]; block s = 1 + f couples to the

@@ -53,7 +53,8 @@ class SolverOpts(C.Structure):
                 ("amg_nlevels", C.c_int), ("amg_A", C.POINTER(OracleCsr)), ("amg_P", C.POINTER(OracleCsr)),
                 ("amg_R", C.POINTER(OracleCsr)), ("amg_Pdg", C.POINTER(OracleCsr)),
                 ("amg_Rdg", C.POINTER(OracleCsr)), ("amg_coarse_inv", DP), ("amg_coarse_n", C.c_int),
-                ("smoother", C.c_int), ("amg_cheb_order", C.c_int), ("mult", C.c_void_p)]
+                ("smoother", C.c_int), ("amg_cheb_order", C.c_int), ("mult", C.c_void_p),
+                ("outer_mult", C.c_void_p)]
 
 
 _libs = {}
@@ -181,13 +182,14 @@ def block_diag(om, ncomp, bc_types, factor=None, mm=None, mm_scalar=0.0, flags=0
 
 def solve(om, b, bc_types, precond=PRE_NONE, factor=None, mm=None, mm_scalar=0.0, flags=0,
           abs_tol=1e-9, rel_tol=1e-8, max_iter=500, inv_mass_factor=1.0, pin_dof=-1, nullspace=0,
-          x0=None, pmg=None, use_ref=False, ref_applies=False):
+          x0=None, pmg=None, use_ref=False, ref_applies=False, outer_mult=None):
     """Solve with the oracle (or the reference-kernel harness). pmg: dict with
     orders, meshes (OMesh per level), factors, prolong, cheb_order, eig_safety,
     eig_ratio, eig_iters, coarse_iters, smoother (0 Jacobi, 1 element-block
     Jacobi), amg_cheb_order and amg (a hierarchy with the csr / coarse_inverse
     accessors). ref_applies: the oracle's solver with every operator apply
-    done by the reference's own kernels (oracle/_ref ref_mult)."""
+    done by the reference's own kernels (oracle/_ref ref_mult). outer_mult: an
+    oracle_mult_fn (ctypes function) for the outer operator alone."""
     b = np.ascontiguousarray(b, dtype=np.float64)
     x = np.zeros_like(b) if x0 is None else np.ascontiguousarray(x0, dtype=np.float64).copy()
     bct = np.ascontiguousarray(bc_types, dtype=np.int32).reshape(-1)
@@ -254,6 +256,8 @@ def solve(om, b, bc_types, precond=PRE_NONE, factor=None, mm=None, mm_scalar=0.0
             o.amg_coarse_n = amg.coarse_n
     if ref_applies:
         o.mult = C.cast(ref_lib().ref_mult, C.c_void_p).value
+    if outer_mult is not None:
+        o.outer_mult = C.cast(outer_mult, C.c_void_p).value
     info = SolveInfo()
     if use_ref:
         assert ref_lib().ref_solve(C.byref(om.s), C.byref(o), _d(b), _d(x), C.byref(info)) == 0

@@ -57,10 +57,14 @@ def levels(mesh, dim, orders, factor, bc_types, reuse=None, **over):
     return out
 
 
-def solve_poisson(case, orders=(3, 2, 1), rel_tol=1e-8, max_iter=200, ref_applies=False, reuse=None, **over):
+def solve_poisson(case, orders=(3, 2, 1), rel_tol=1e-8, max_iter=200, ref_applies=False, reuse=None,
+                  outer_mult=None, **over):
     """FP64 p-multigrid FPCG of a dg_oracle workload (pinned DOF or nullspace
     projection as the case says). reuse: the pmg dict of an earlier solve on the
-    same mesh whose algebraic prolongators are kept. Returns (x, info, pmg)."""
+    same mesh whose algebraic prolongators are kept. outer_mult: the outer
+    operator when it is not the nodal one of case["factor"] (the over-integrated
+    operator, oi_oracle.outer_mult; the levels keep the nodal factor). Returns
+    (x, info, pmg)."""
     mesh, e, t = case["mesh"], case["export"], case["tables"]
     om = O.OMesh(t, e)
     pmg = levels(mesh, e["dim"], orders, case["factor"], case["bc_types"], reuse=reuse, **over)
@@ -68,5 +72,5 @@ def solve_poisson(case, orders=(3, 2, 1), rel_tol=1e-8, max_iter=200, ref_applie
     pin_dof = -1 if pin is None else pin[0] * t["Np"] + pin[1]
     x, info = O.solve(om, case["rhs"], case["bc_types"], O.PRE_PMG, case["factor"], abs_tol=0.0,
                       rel_tol=rel_tol, max_iter=max_iter, pin_dof=pin_dof, nullspace=0 if pin else 1,
-                      pmg=pmg, ref_applies=ref_applies)
+                      pmg=pmg, ref_applies=ref_applies, outer_mult=outer_mult)
     return x, info, pmg

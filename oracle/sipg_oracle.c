@@ -857,7 +857,7 @@ static void project_mean(double *v, size_t n) {
 void oracle_solve(const oracle_mesh *m, const oracle_solver_opts *o, const double *b, double *x,
                   oracle_solve_info *info) {
   op_ctx op = {m, o->ncomp, o->bc_types, o->factor, o->mm_factor, o->mm_scalar, o->flags, o->pin_dof, 0.0,
-               o->mult};
+               o->outer_mult ? o->outer_mult : o->mult};
   size_t n = vec_len(&op);
   const int Np = m->Np, K = m->K;
   const double t_setup = wall_s();

@@ -139,6 +139,8 @@ typedef struct {
   int smoother;
   int amg_cheb_order;        /* Chebyshev degree on the algebraic levels (0: cheb_order) */
   oracle_mult_fn mult;       /* every operator apply of the solve (NULL: oracle_mult) */
+  oracle_mult_fn outer_mult; /* the outer Krylov operator only, when it differs from the
+                                preconditioner's (the over-integrated operator); NULL: mult */
 } oracle_solver_opts;
 
 /* Solve A x = b (x holds the initial guess on entry). ncomp components are
