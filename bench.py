@@ -211,6 +211,51 @@ def c3_solve(op, c, n, reps=3):
             "status": int(info.status)}
 
 
+def run_over_integrated(c, steps=5, warmup=3):
+    """The headline problem with the factor at the cubature points
+    (sipg_op_set_factor_oi, FactorPoissonMatrixFreeDiagOI3D's inputs): 1/rho of
+    the same two-phase density at 125 volume and 4 x 16 surface points per
+    element. Assembly time (device-resident inputs, and from host buffers),
+    the mixed p-multigrid solve (outer CG on the over-integrated operator, V-cycle
+    on its nodal projection) against the nodal factor's, and the FP64 block-sparse
+    apply with its roofline ((NF + 1) Np^2 FP64 block values, x and y per element)."""
+    import torch
+    mesh = c["mesh"]
+    K, n = mesh.K, N_HEAD
+    op = sipg.Operator(mesh, ORDER, 1)
+    op.set_bc_types(c["bc_types"])
+    xv, xs = op.oi_points()
+    fv = 1.0 / W.two_phase_rho(xv[0], xv[1], xv[2], 1.0 / n)
+    fs = 1.0 / W.two_phase_rho(xs[0], xs[1], xs[2], 1.0 / n)
+    t0 = time.perf_counter()
+    op.set_factor_oi(fv, fs)
+    host_ms = (time.perf_counter() - t0) * 1e3
+    fvd, fsd = torch.from_numpy(fv).cuda(), torch.from_numpy(fs).cuda()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sipg.check(sipg.lib().sipg_op_set_factor_oi_device(op.h, C.c_void_p(fvd.data_ptr()), C.c_void_p(fsd.data_ptr()),
+                                                       None))
+    torch.cuda.synchronize()
+    dev_ms = (time.perf_counter() - t0) * 1e3
+    s, setup_ms = pmg_solver(op, sipg.FP32)
+    bd = torch.from_numpy(c["rhs"].reshape(-1)).cuda()
+    xd = torch.zeros_like(bd)
+    ms, infos = time_solves(s, bd, xd, steps, warmup)
+    Np = op.Np
+    t64 = time_apply(op, sipg.FP64, K, Np)
+    hbm, peak_kind = peaks()
+    bpe = (5 * Np * Np + 2 * Np) * 8
+    return {"workload": "24^3x6 = 82,944 tets, p = 3, 1/rho (two-phase, ratio 1000) at 125 volume and 4 x 16 "
+                        "surface cubature points per element, GRF right-hand side, Neumann walls",
+            "assemble_ms_device_inputs": dev_ms, "set_factor_oi_host_ms": host_ms, "solver_setup_ms": setup_ms,
+            "mixed_ms_per_solve": float(np.mean(ms)), "iters": int(infos[-1].iters),
+            "true_rel_res": float(infos[-1].true_rel_res),
+            "apply_fp64_ms": t64,
+            "roofline": {"kernel": "k_bsr<double,20,4> (over-integrated element blocks)", "bound": "hbm",
+                         "achieved": bpe * K / (t64 * 1e-3) / 1e9, "peak": hbm, "peak_kind": peak_kind,
+                         "unit": "GB/s", "frac": bpe * K / (t64 * 1e-3) / 1e9 / hbm, "bytes_per_elem": bpe}}
+
+
 def apply_bytes_per_elem(Np, ts, factor, ngeof=10, nf=4, gface=5):
     """Algorithmic HBM bytes of one scalar apply per element: read x, write y,
     the nodal factor (if any), the volume geometric factors and nf faces of
@@ -389,12 +434,13 @@ def run_ours(args):
                      "bytes_per_elem": bpe, "apply_ms": a32, "elements": K},
         "clocks": clk.summary(),
     }
+    out["over_integrated"] = run_over_integrated(c)
     out["config_2d"] = run_config_2d()
     out["projection"] = run_projection(cpu=rank == 0 and world == 1 and not args.skip_cpu)
     if not args.skip_serving and world == 1:
         out["serving"] = run_serving(slots=args.serve_slots)
     if rank == 0 and world == 1 and not args.skip_cpu:
-        out["cpu_baseline"] = cpu_baseline_sample(c, int(inf64[-1].iters))
+        out["cpu_baseline"] = cpu_baseline_sample(int(inf64[-1].iters))
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
@@ -706,26 +752,39 @@ def oracle_case(c):
                 bc_types=c["bc_types"], pin=None)
 
 
-def cpu_baseline_sample(c, outer_iters):
+def cpu_baseline_sample(outer_iters):
     """Bounded sample of the reference CPU path on all host cores: the set-up and
     two outer iterations of the same FP64 p-multigrid FPCG, every operator apply
     by the reference's own kernels (oracle/_ref); solve time = set-up + (outer
     iterations of this run's GPU FP64 solve, the same algorithm) x the measured
-    seconds per iteration."""
+    seconds per iteration. Runs in a fresh process built from oracle/ alone (no
+    GPU context or other OpenMP runtime in it)."""
+    out = subprocess.run([sys.executable, os.path.abspath(__file__), "--cpu-sample", str(outer_iters)],
+                         capture_output=True, text=True, timeout=1800)
+    lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
+    if out.returncode != 0 or not lines:
+        return {"unavailable": f"CPU sample failed: {out.stderr.strip()[-300:]}"}
+    return json.loads(lines[-1])
+
+
+def cpu_sample_main(outer_iters):
+    import dg_oracle as D
     import pmg_oracle as P
     cores = os.cpu_count() or 1
     omp_threads(cores)
-    case = oracle_case(c)
+    case = D.poisson3d_two_phase(N_HEAD, order=ORDER, n_modes=256, pin=False)
     t0 = time.perf_counter()
     _, info, _ = P.solve_poisson(case, max_iter=2, ref_applies=True)
     wall = time.perf_counter() - t0
     setup = wall - info.solve_s
     est = setup + outer_iters * info.iter_s
-    return {"value": 1.0 / est, "unit": "solves/s", "cores": cores, "kind": "reference",
-            "sample": (f"set-up ({setup:.1f} s) and 2 outer FP64 p-MG FPCG iterations ({info.iter_s:.2f} s each) "
-                       f"with every apply by the reference's kernels (oracle/_ref, OpenMP {cores} threads), "
-                       f"solve = set-up + {outer_iters} iterations (this run's GPU FP64 iteration count)"),
-            "setup_s": setup, "iter_s": info.iter_s, "wall_s": wall}
+    print(json.dumps({"value": 1.0 / est, "unit": "solves/s", "cores": cores, "kind": "reference",
+                      "sample": (f"set-up ({setup:.1f} s) and 2 outer FP64 p-MG FPCG iterations ({info.iter_s:.2f} s "
+                                 f"each) with every apply by the reference's kernels (oracle/_ref, OpenMP {cores} "
+                                 f"threads), solve = set-up + {outer_iters} iterations (this run's GPU FP64 "
+                                 "iteration count)"),
+                      "setup_s": setup, "iter_s": info.iter_s, "wall_s": wall, "sample_iters": int(info.iters),
+                      "sample_rel_res": float(info.rel_res)}))
 
 
 def reference_2d(threads):
@@ -801,6 +860,17 @@ def run_reference(args):
     t0 = time.perf_counter()
     x, info, _ = P.solve_poisson(case, ref_applies=True)
     total = time.perf_counter() - t0
+    # one core: the fine-level apply through the reference's kernels at 1 thread and
+    # at all threads; the 1-core solve is the all-core solve scaled by their ratio
+    apply_s = {}
+    for th in (1, cores):
+        omp_threads(th)
+        O.mult(om, case["rhs"], case["bc_types"], case["factor"], use_ref=True)
+        t1 = time.perf_counter()
+        for _ in range(3):
+            O.mult(om, case["rhs"], case["bc_types"], case["factor"], use_ref=True)
+        apply_s[th] = (time.perf_counter() - t1) / 3
+    omp_threads(cores)
     val = 1.0 / total
     sample = (f"one complete FP64 p-MG FPCG solve of this workload ({info.iters} outer iterations to relative "
               f"residual {info.rel_res:.2e}), every apply by the reference's kernels (oracle/_ref, OpenMP "
@@ -808,6 +878,10 @@ def run_reference(args):
     extra = {"reference_solve": {"total_s": total, "iters": int(info.iters), "rel_res": float(info.rel_res),
                                  "oracle_setup_s": float(info.setup_s), "iter_s": float(info.iter_s),
                                  "error_vs_fixture": fixture_error(x)},
+             "reference_c2_one_core": {"apply_s_1_thread": apply_s[1], f"apply_s_{cores}_threads": apply_s[cores],
+                                       "solve_s_estimate": total * apply_s[1] / apply_s[cores],
+                                       "how": "the all-core solve time scaled by the fine-level apply's 1-thread / "
+                                              "all-thread time ratio (a full 1-thread solve takes over 20 min)"},
              "config_2d": {"one_core": reference_2d(1), "all_cores": reference_2d(cores)},
              "apply_c3": reference_c3_apply()}
     out = {"metric": METRIC, "value": val, "unit": "solves/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
@@ -947,7 +1021,11 @@ def main():
     ap.add_argument("--skip-serving", action="store_true")
     ap.add_argument("--serving-only", action="store_true", help="run only the served stream; print its record")
     ap.add_argument("--serve-slots", type=int, default=SERVE_SLOTS, help="concurrent solves of the served stream")
+    ap.add_argument("--cpu-sample", type=int, default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.cpu_sample is not None:
+        cpu_sample_main(args.cpu_sample)
+        return
     if args.impl == "ours" or args.profile:
         global sipg, W
         import sipg as _sipg
