@@ -211,6 +211,58 @@ def c3_solve(op, c, n, reps=3):
             "status": int(info.status)}
 
 
+def run_viscous(steps=3):
+    """The viscous step of the rising-bubble configuration (32^3 x 6 = 196,608
+    tets, p = 3, the bubble of radius 0.25 at (0.5, 0.3, 0.5), density ratio 1000,
+    viscosity ratio 100): the vector Helmholtz operator rho g0 Re / dt M + the
+    mu-weighted SIPG operator on (u, v, w) (FactorViscousMatrix3D, ncomp = 3), slip
+    on the x and z walls and no-slip on the y walls, right-hand side from the
+    fused viscous right-hand side kernel (mp_ins_3d_vis_0 + mass) of seeded
+    U(-1, 1) velocities, ViscousSolver3D's Jacobi-preconditioned CG to 1e-8
+    relative. FP64 applies on the tensor cores (three scalar applies and the slip
+    coupling terms) and on the CUDA cores, and the solve."""
+    import torch
+    n, order, dt, Re, g0 = PROJ_N, 3, 1e-3, 100.0, 1.5
+    mesh = sipg.Mesh.box(3, n, jitter=0.1, seed=20261203)
+    e = mesh.export(order)
+    K, Np = mesh.K, sipg.ref_sizes(3, order)[0]
+    center = (0.5, 0.3, 0.5)
+    rho = W.two_phase_rho(e["x"], e["y"], e["z"], 1.0 / n, ratio=1000.0, center=center)
+    mu = W.two_phase_rho(e["x"], e["y"], e["z"], 1.0 / n, ratio=100.0, center=center)
+    yb = e["bface_centroid"][:, 1]
+    wall = np.where((yb < 1e-9) | (yb > 1 - 1e-9), sipg.BC_DIRICHLET, sipg.BC_SLIP).astype(np.int32)
+    bct = np.ascontiguousarray(np.repeat(wall[None], 3, axis=0))
+    vel = np.random.default_rng(5).uniform(-1.0, 1.0, (3, K, Np))
+    rhs = np.zeros_like(vel)
+    mm = np.zeros((K, Np))
+    fact0, fact1 = Re / dt, g0 * Re / dt
+    sipg.check(sipg.lib().sipg_viscous_rhs_host(mesh.h, order, C.c_double(fact0), C.c_double(fact1),
+                                                rho.ctypes.data_as(C.c_void_p), vel.ctypes.data_as(C.c_void_p),
+                                                rhs.ctypes.data_as(C.c_void_p), mm.ctypes.data_as(C.c_void_p)))
+    op = sipg.Operator(mesh, order, 3)
+    op.set_bc_types(bct)
+    op.set_factor(mu)
+    op.set_mm(sipg.MM_NODAL, 0.0, mm)
+    t_tc = time_apply(op, sipg.FP64, K, 3 * Np, 10)
+    op.set_kernel(1)
+    t_cc = time_apply(op, sipg.FP64, K, 3 * Np, 10)
+    op.set_kernel(0)
+    # the reference's default for slip walls: Jacobi-preconditioned ViscousSolver3D
+    # ([viscous-solve] preconditioner = jacobi, mp_ins_solver.cpp:97-104), r_tol 1e-8
+    o = sipg.default_opts(sipg.SOLVER_JACOBI)
+    o.rel_tol, o.abs_tol, o.max_iter = 1e-8, 0.0, 5000
+    s = sipg.Solver(op, sipg.SOLVER_JACOBI, o)
+    bd = torch.from_numpy(rhs.reshape(-1)).cuda()
+    xd = torch.zeros_like(bd)
+    ms, infos = time_solves(s, bd, xd, steps, 1)
+    dofs = 3 * K * Np
+    return {"workload": "32^3x6 = 196,608 tets, p = 3, (u, v, w): rho g0 Re/dt M + SIPG(mu), density ratio 1000, "
+                        "viscosity ratio 100, slip x/z walls, no-slip y walls, Jacobi PCG to 1e-8",
+            "apply_fp64_tensor_cores_ms": t_tc, "apply_fp64_cuda_cores_ms": t_cc,
+            "apply_fp64_gdofs": dofs / (t_tc * 1e-3) / 1e9, "solve_ms": float(np.mean(ms)),
+            "iters": int(infos[-1].iters), "true_rel_res": float(infos[-1].true_rel_res)}
+
+
 def run_over_integrated(c, steps=5, warmup=3):
     """The headline problem with the factor at the cubature points
     (sipg_op_set_factor_oi, FactorPoissonMatrixFreeDiagOI3D's inputs): 1/rho of
@@ -435,6 +487,7 @@ def run_ours(args):
         "clocks": clk.summary(),
     }
     out["over_integrated"] = run_over_integrated(c)
+    out["viscous"] = run_viscous()
     out["config_2d"] = run_config_2d()
     out["projection"] = run_projection(cpu=rank == 0 and world == 1 and not args.skip_cpu)
     if not args.skip_serving and world == 1:

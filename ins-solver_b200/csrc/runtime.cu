@@ -216,7 +216,27 @@ void sipg_op::apply(const T* x, T* y, cudaStream_t s, T alpha, T beta, const T* 
   a.c = c ? c : y;
   a.tcg = f64 ? (const T*)mesh->tcg64.p : (const T*)mesh->tcg32.p;
   a.tcgen05 = kernel == 3;
-  const bool tc = (kernel == 0 || kernel >= 2) && ncomp == 1 && (f64 ? dref->tc_ok64 : dref->tc_ok32);
+  const bool tc_ok = (kernel == 0 || kernel >= 2) && (f64 ? dref->tc_ok64 : dref->tc_ok32);
+  if (tc_ok && ncomp > 1 && pin_elem < 0) {
+    // vector operator: one tensor-core scalar apply per component (its own boundary
+    // types; slip faces get no face terms there), then the slip faces' coupling terms
+    const T* tcc = f64 ? (const T*)dref->tc64.p : (const T*)dref->tc32.p;
+    DevBuf& tr = f64 ? trace64 : trace32;
+    if (!tr.p) tr = DevBuf(tc_trace_values(mesh->dim, order, mesh->K) * sizeof(T));
+    const size_t per = (size_t)mesh->K * Np;
+    for (int comp = 0; comp < ncomp; ++comp) {
+      ApplyArgs<T> ac = a;
+      ac.ncomp = 1;
+      ac.x = x + comp * per;
+      ac.y = y + comp * per;
+      ac.c = a.c + comp * per;
+      ac.bct = bct.as<uint8_t>() + (size_t)comp * mesh->Kb;
+      SIPG_CUDA(launch_apply_tc<T>(mesh->dim, order, ac, tcc, tr.as<T>(), num_sms(), s));
+    }
+    SIPG_CUDA(launch_slip<T>(mesh->dim, order, a, mesh->belems.as<int>(), mesh->n_belem, s));
+    return;
+  }
+  const bool tc = tc_ok && ncomp == 1;
   if (tc) {
     const T* tcc = f64 ? (const T*)dref->tc64.p : (const T*)dref->tc32.p;
     DevBuf& tr = f64 ? trace64 : trace32;

@@ -396,6 +396,109 @@ __global__ void sipg_tau_kernel(const int8_t* itab, const T* geof, const int* nb
   }
 }
 
+// Slip faces of the vector operator (every component of a boundary face of type 2,
+// vmf_3d_mult_avg_jump.h:9-41): the face terms that couple the components,
+//   un = n . u,  nqn = sum_c n_c (n . f grad u_c)  at each face node,
+//   Fu_c = sJ (tau n_c un - n_c nqn),  Fq_(c,d) = -n_d sJ f n_c un,
+// lifted as y_c += EMAT Fu_c + sum_r D_r^T EMAT (G Fq_c)_r. Added (times alpha) to
+// per-component scalar applies, which give a slip face no face terms. One CTA per
+// element that owns a boundary face.
+template <typename T, int DIM, int P>
+__global__ void __launch_bounds__(128) sipg_slip_kernel(ApplyArgs<T> a, const int* __restrict__ belems,
+                                                        int n_belem) {
+  using C = Cfg<DIM, P>;
+  constexpr int NP = C::NP, NFP = C::NFP, NF = C::NF, NFNFP = C::NFNFP, LD = C::LD, LDE = C::LDE, NG = C::NG;
+  __shared__ T u[DIM][NP], fac[NP], g[NG], W[DIM][DIM][NP];
+  __shared__ T fu[DIM][NFNFP], ft[DIM][DIM][NFNFP];
+  __shared__ int slipf[NF];
+  const T* Dm = a.consts + C::OFF_D;
+  const T* Em = a.consts + C::OFF_E;
+  const int8_t* fmask = a.itab;
+  const size_t K = (size_t)a.K;
+  for (int it = blockIdx.x; it < n_belem; it += gridDim.x) {
+    const int e = belems[it];
+    __syncthreads();
+    if (threadIdx.x < NF) {
+      const int nb = a.nbr[(size_t)e * NF + threadIdx.x];
+      int sl = 0;
+      if (nb < 0) {
+        sl = 1;
+        for (int c = 0; c < DIM; ++c) sl &= a.bct[(size_t)c * a.Kb + (-nb - 1)] == BC_SLIP;
+      }
+      slipf[threadIdx.x] = sl;
+    }
+    for (int i = threadIdx.x; i < DIM * NP; i += blockDim.x) u[i / NP][i % NP] = a.x[((size_t)(i / NP) * K + e) * NP + i % NP];
+    for (int i = threadIdx.x; i < NP; i += blockDim.x) fac[i] = a.factor ? a.factor[(size_t)e * NP + i] : T(1);
+    for (int i = threadIdx.x; i < NG; i += blockDim.x) g[i] = a.geof[(size_t)e * NG + i];
+    __syncthreads();
+    bool any = false;
+    for (int f = 0; f < NF; ++f) any |= slipf[f] != 0;
+    if (!any) continue;
+    for (int k = threadIdx.x; k < NFNFP; k += blockDim.x) {
+      const int f = k / NFP, j = k - (k / NFP) * NFP;
+      if (!slipf[f]) {
+        for (int c = 0; c < DIM; ++c) {
+          fu[c][k] = T(0);
+          for (int r = 0; r < DIM; ++r) ft[c][r][k] = T(0);
+        }
+        continue;
+      }
+      const int m = fmask[f * NFP + j];
+      T n[3], sJ;
+      face_normal<DIM>(g, f, n, &sJ);
+      const T tau = a.tau[(size_t)e * NF + f];
+      T un = T(0), nqn = T(0);
+      for (int c = 0; c < DIM; ++c) {
+        T gr[3] = {T(0), T(0), T(0)};
+        for (int q = 0; q < NP; ++q)
+          for (int r = 0; r < DIM; ++r) gr[r] += Dm[r * NP * LD + m * LD + q] * u[c][q];
+        T nq = T(0);
+        for (int d = 0; d < DIM; ++d) {
+          T qd = T(0);
+          for (int r = 0; r < DIM; ++r) qd += geo_G<DIM>(g, r, d) * gr[r];
+          nq += n[d] * qd;
+        }
+        un += n[c] * u[c][m];
+        nqn += n[c] * (fac[m] * nq);
+      }
+      for (int c = 0; c < DIM; ++c) {
+        fu[c][k] = sJ * (tau * n[c] * un - n[c] * nqn);
+        for (int r = 0; r < DIM; ++r) {
+          T s2 = T(0);
+          for (int d = 0; d < DIM; ++d) s2 += geo_G<DIM>(g, r, d) * (-n[d] * sJ * fac[m] * n[c] * un);
+          ft[c][r][k] = s2;
+        }
+      }
+    }
+    __syncthreads();
+    // W_(c,r) = EMAT ft_(c,r)
+    for (int t = threadIdx.x; t < DIM * DIM * NP; t += blockDim.x) {
+      const int c = t / (DIM * NP), r = (t / NP) % DIM, q = t % NP;
+      T s2 = T(0);
+      for (int k = 0; k < NFNFP; ++k) s2 += Em[q * LDE + k] * ft[c][r][k];
+      W[c][r][q] = s2;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < DIM * NP; t += blockDim.x) {
+      const int c = t / NP, i = t % NP;
+      T acc = T(0);
+      for (int k = 0; k < NFNFP; ++k) acc += Em[i * LDE + k] * fu[c][k];
+      for (int r = 0; r < DIM; ++r)
+        for (int q = 0; q < NP; ++q) acc += Dm[r * NP * LD + q * LD + i] * W[c][r][q];
+      a.y[((size_t)c * K + e) * NP + i] += a.alpha * acc;
+    }
+  }
+}
+
+template <typename T, int DIM, int P>
+cudaError_t launch_slip_t(const ApplyArgs<T>& a, const int* belems, int n_belem, cudaStream_t s) {
+  if (n_belem <= 0) return cudaSuccess;
+  const int grid = std::max(1, std::min(n_belem, 148 * 16));
+  sipg_slip_kernel<T, DIM, P><<<grid, 128, 0, s>>>(a, belems, n_belem);
+  note_launch();
+  return cudaGetLastError();
+}
+
 template <typename T, int DIM, int P>
 cudaError_t launch_apply_t(const ApplyArgs<T>& a, int num_sms, cudaStream_t s) {
   using C = Cfg<DIM, P>;
@@ -454,6 +557,12 @@ cudaError_t launch_apply(int dim, int order, const ApplyArgs<T>& a, int num_sms,
   return cudaErrorInvalidValue;
 }
 
+template <typename T>
+cudaError_t launch_slip(int dim, int order, const ApplyArgs<T>& a, const int* belems, int n_belem, cudaStream_t s) {
+  SIPG_DISPATCH(dim, order, return (launch_slip_t<T, D, P>(a, belems, n_belem, s)));
+  return cudaErrorInvalidValue;
+}
+
 size_t apply_smem_bytes(int dim, int order, int ncomp, int eb, bool fp64) {
   SIPG_DISPATCH(dim, order, return smem_bytes_t<D, P>(ncomp, eb, fp64));
   return 0;
@@ -480,6 +589,8 @@ cudaError_t launch_tau(int dim, int order, const int8_t* itab, const T* geof, co
 
 template cudaError_t launch_apply<double>(int, int, const ApplyArgs<double>&, int, cudaStream_t);
 template cudaError_t launch_apply<float>(int, int, const ApplyArgs<float>&, int, cudaStream_t);
+template cudaError_t launch_slip<double>(int, int, const ApplyArgs<double>&, const int*, int, cudaStream_t);
+template cudaError_t launch_slip<float>(int, int, const ApplyArgs<float>&, const int*, int, cudaStream_t);
 template cudaError_t launch_tau<double>(int, int, const int8_t*, const double*, const int*,
                                         const uint32_t*, const double*, int, double*, cudaStream_t);
 template cudaError_t launch_tau<float>(int, int, const int8_t*, const float*, const int*,

@@ -113,6 +113,11 @@ template <typename T>
 cudaError_t launch_apply(int dim, int order, const ApplyArgs<T>& a, int num_sms, cudaStream_t s);
 size_t apply_smem_bytes(int dim, int order, int ncomp, int eb, bool fp64);
 int apply_pick_eb(int dim, int order, int ncomp, bool fp64);
+// Vector operator (ncomp = dim): y_c += alpha x the component-coupling slip-face
+// terms, over the elements that own boundary faces (after per-component scalar
+// applies, which give slip faces no face terms).
+template <typename T>
+cudaError_t launch_slip(int dim, int order, const ApplyArgs<T>& a, const int* belems, int n_belem, cudaStream_t s);
 
 // tau per element face (fvmf_3d_calc_tau_faces.h / fvmf_3d_calc_tau_bfaces.h).
 template <typename T>
