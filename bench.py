@@ -960,12 +960,31 @@ def run_profile(args):
            --precision: 3 applies.
     c3pcg: the inverse-mass preconditioned CG on that operator, FP64: a warm-up
            solve of 3 iterations, then a counted one (kernel by kernel, no graphs).
+    oiapply: the over-integrated operator at --n, p = 3 (two-phase factor at the
+           cubature points): 3 FP64 applies of its element blocks.
     solve: the headline mixed solve: one warm-up solve, then the captured solve;
            prints the number of kernels launched before it (ncu -s) and in it (-c).
            The outer iterations replay one host-launched graph each (graphs = 1):
            the kernels of the device-resident loop, which the profiler then sees
            as ordinary graph launches.
     """
+    if args.profile == "oiapply":
+        # the over-integrated operator (two-phase 1/rho at the cubature points) at
+        # --n, p = 3: 3 FP64 applies of its element blocks after the assembly
+        c = W.poisson3d_two_phase(args.n, order=ORDER, n_modes=64, pin=False)
+        op = sipg.Operator(c["mesh"], ORDER, 1)
+        op.set_bc_types(c["bc_types"])
+        xv, xs = op.oi_points()
+        op.set_factor_oi(1.0 / W.two_phase_rho(xv[0], xv[1], xv[2], 1.0 / args.n),
+                         1.0 / W.two_phase_rho(xs[0], xs[1], xs[2], 1.0 / args.n))
+        K, Np = c["mesh"].K, op.Np
+        x = sipg.DeviceVector(np.random.default_rng(3).uniform(-1, 1, K * Np))
+        y = sipg.DeviceVector(np.zeros(K * Np))
+        for _ in range(3):
+            op.apply_device(sipg.FP64, x.ptr, y.ptr)
+        sipg.check(sipg.lib().sipg_device_synchronize())
+        print("done", K)
+        return
     if args.profile == "pressure":
         mesh, velT, dp = projection_inputs(args.n)
         K, Np = mesh.K, velT.shape[2]
@@ -1060,7 +1079,8 @@ def run_profile(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--profile", choices=["apply", "solve", "projection", "pressure", "c3apply", "c3pcg"], default=None,
+    ap.add_argument("--profile", choices=["apply", "solve", "projection", "pressure", "c3apply", "c3pcg", "oiapply"],
+                    default=None,
                     help="run a small fixed workload for an ncu capture instead of the benchmark")
     ap.add_argument("--n", type=int, default=N_HEAD)
     ap.add_argument("--order", type=int, default=ORDER)
