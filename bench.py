@@ -305,7 +305,11 @@ def run_over_integrated(c, steps=5, warmup=3):
             "apply_fp64_ms": t64,
             "roofline": {"kernel": "k_bsr<double,20,4> (over-integrated element blocks)", "bound": "hbm",
                          "achieved": bpe * K / (t64 * 1e-3) / 1e9, "peak": hbm, "peak_kind": peak_kind,
-                         "unit": "GB/s", "frac": bpe * K / (t64 * 1e-3) / 1e9 / hbm, "bytes_per_elem": bpe}}
+                         "unit": "GB/s", "frac": bpe * K / (t64 * 1e-3) / 1e9 / hbm, "bytes_per_elem": bpe,
+                         "traffic": (tpe * K if (tpe := profile_value("oi_block_apply_fp64_p3_16cube.txt",
+                                                                      "traffic_bytes_per_element")) else None),
+                         "traffic_source": "profiles/oi_block_apply_fp64_p3_16cube.txt (16^3x6 capture, "
+                                           "per-element traffic scaled to 82,944 elements)"}}
 
 
 def apply_bytes_per_elem(Np, ts, factor, ngeof=10, nf=4, gface=5):
