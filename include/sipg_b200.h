@@ -404,6 +404,20 @@ int sipg_viscous_rhs(sipg_mesh *m, int order, double fact0, double fact1, const 
 int sipg_viscous_rhs_host(sipg_mesh *m, int order, double fact0, double fact1, const double *rho,
                           const double *velTT, double *rhs, double *mm_factor);
 
+/* Non-linear advection step of the 3D time step, INSSolverBase3D::advec_current_non_linear
+ * and advec_standard (src/solvers/3d/ins_solver_base.cpp:224-329, 451-480): N = div(u (x) u)
+ * with Lax-Friedrichs face fluxes (ins_3d_advec_0/1/2 and LIFT) and the extrapolated
+ * velocity velT = a0 u + a1 u_old - dt (b0 N + b1 N_old) (ins_3d_advec_3), in one kernel.
+ * vel, vel_old, N_old, N, velT: 3 x K x Np; vel_bc: Kb velocity boundary types of the
+ * reference's problem_specific_3d.h (0 no-slip, 1 slip, 2 natural outflow). Device
+ * pointers on `stream`, or host pointers in the synchronous _host variant. */
+int sipg_ins_advection(sipg_mesh *m, int order, double dt, double a0, double a1, double b0, double b1,
+                       const double *vel, const double *vel_old, const double *N_old, const int *vel_bc,
+                       double *N, double *velT, void *stream);
+int sipg_ins_advection_host(sipg_mesh *m, int order, double dt, double a0, double a1, double b0, double b1,
+                            const double *vel, const double *vel_old, const double *N_old, const int *vel_bc,
+                            double *N, double *velT);
+
 /* Number of kernels this library has launched so far in the process
  * (diagnostics for benchmarks; no reference counterpart). */
 int sipg_launch_count(unsigned long long *n);

@@ -1,0 +1,284 @@
+// Non-linear advection step of the 3D incompressible time step, fused into one
+// kernel: INSSolverBase3D::advec_current_non_linear + advec_standard
+// (src/solvers/3d/ins_solver_base.cpp:224-329, 451-480), i.e. the flux tensor
+// u (x) u (ins_3d_advec_0), its strong-form divergence (mesh->div), the
+// Lax-Friedrichs face fluxes (ins_3d_advec_1 interior, ins_3d_advec_2 boundary:
+// no-slip, slip, natural outflow), their LIFT, and the extrapolated velocity
+// (ins_3d_advec_3): velT = a0 u + a1 u_old - dt (b0 N + b1 N_old).
+// One warp per element (lane = node / face node), FP64; the reference matrices
+// D_r and LIFT sit in shared memory. The boundary kernel's wave speed is the
+// floor of the largest |n . u| over the face (the reference stores it in an int,
+// ins_3d_advec_2.h:44), kept here so the results are the reference's.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <map>
+#include <memory>
+#include <mutex>
+
+#include "../../include/sipg_b200.h"
+#include "capi_util.hpp"
+#include "runtime.hpp"
+#include "sipg_apply.cuh"
+#include "vecops.cuh"
+
+namespace sipg {
+namespace {
+
+constexpr int kAdvWarps = 8;
+
+struct AdvTables {
+  DevBuf mats;  // Dr, Ds, Dt (Np x Np), LIFT (Np x Nf Nfp), row-major
+};
+
+const AdvTables& adv_tables(int order) {
+  static std::mutex mu;
+  static std::map<std::pair<int, int>, std::unique_ptr<AdvTables>> cache;
+  int dev = 0;
+  SIPG_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  auto& slot = cache[{dev, order}];
+  if (slot) return *slot;
+  const RefElement& r = dev_ref(3, order).ref;
+  std::vector<double> m;
+  m.insert(m.end(), r.Dr.begin(), r.Dr.end());
+  m.insert(m.end(), r.Ds.begin(), r.Ds.end());
+  m.insert(m.end(), r.Dt.begin(), r.Dt.end());
+  m.insert(m.end(), r.LIFT.begin(), r.LIFT.end());
+  auto t = std::make_unique<AdvTables>();
+  t->mats = DevBuf(m.size() * sizeof(double));
+  t->mats.upload(m.data(), m.size() * sizeof(double));
+  slot = std::move(t);
+  return *slot;
+}
+
+struct AdvArgs {
+  const double* mats;
+  const int8_t* itab;  // fmask, perm_pos
+  const double* geof;
+  const int* nbr;
+  const uint32_t* fcode;
+  const int* vel_bc;  // Kb: 0 no-slip, 1 slip, 2 natural outflow
+  const double *u, *u_old, *N_old;
+  double *N, *velT;
+  double dt, a0, a1, b0, b1;
+  int K;
+};
+
+template <int P>
+__global__ void __launch_bounds__(kAdvWarps * 32) k_advection(const AdvArgs a) {
+  using Cf = Cfg<3, P>;
+  constexpr int NP = Cf::NP, NFP = Cf::NFP, NF = 4, NFNFP = NF * NFP, NG = 10;
+  extern __shared__ double sm[];
+  const double* sD = sm;                       // 3 x NP x NP
+  const double* sL = sm + 3 * NP * NP;         // NP x NFNFP
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* sU = sm + 3 * NP * NP + NP * NFNFP + warp * (12 * NP + 4 * NFNFP);
+  double* sH = sU + 3 * NP;    // [3][3][NP]: H[c][r] = sum_d G[r][d] u_c u_d
+  double* sF = sH + 9 * NP;    // [3][NFNFP] face fluxes
+  double* sS = sF + 3 * NFNFP; // [NFNFP] boundary wave speeds
+  for (int i = threadIdx.x; i < 3 * NP * NP + NP * NFNFP; i += blockDim.x) sm[i] = a.mats[i];
+  __syncthreads();
+  const int8_t* fmask = a.itab;
+  const int8_t* perm = a.itab + NF * NFP;
+  const size_t n = (size_t)a.K * NP;
+  for (int e = blockIdx.x * kAdvWarps + warp; e < a.K; e += gridDim.x * kAdvWarps) {
+    double g[NG];
+#pragma unroll
+    for (int k = 0; k < NG; ++k) g[k] = __ldg(a.geof + (size_t)e * NG + k);
+    __syncwarp();
+    for (int i = lane; i < NP; i += 32) {
+      double uc[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        uc[c] = a.u[c * n + (size_t)e * NP + i];
+        sU[c * NP + i] = uc[c];
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+          double s = 0.0;
+#pragma unroll
+          for (int d = 0; d < 3; ++d) s += g[r * 3 + d] * (uc[c] * uc[d]);
+          sH[(c * 3 + r) * NP + i] = s;
+        }
+    }
+    __syncwarp();
+    // face fluxes (ins_3d_advec_1 / ins_3d_advec_2)
+    for (int m = lane; m < NFNFP; m += 32) {
+      const int f = m / NFP, j = m - f * NFP;
+      double nv[3], sJ;
+      simplex_face_normal<3>(g, f, nv, &sJ);
+      const double fs = sJ / g[9];
+      const int o = fmask[f * NFP + j];
+      const double uM[3] = {sU[o], sU[NP + o], sU[2 * NP + o]};
+      const double lvel = nv[0] * uM[0] + nv[1] * uM[1] + nv[2] * uM[2];
+      const int nb = __ldg(a.nbr + (size_t)e * NF + f);
+      if (nb >= 0) {
+        const int code = (__ldg(a.fcode + e) >> (8 * f)) & 0xff;
+        const int gf = code & 3, sg = code >> 2;
+        const int nn = fmask[gf * NFP + perm[sg * NFP + j]];
+        double uP[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) uP[c] = a.u[c * n + (size_t)nb * NP + nn];
+        double gn[NG], np_[3], sJn;
+#pragma unroll
+        for (int k = 0; k < NG; ++k) gn[k] = __ldg(a.geof + (size_t)nb * NG + k);
+        simplex_face_normal<3>(gn, gf, np_, &sJn);
+        const double rvel = np_[0] * uP[0] + np_[1] * uP[1] + np_[2] * uP[2];
+        const double nuP = nv[0] * uP[0] + nv[1] * uP[1] + nv[2] * uP[2];
+        const double lam = fmax(fabs(lvel), fabs(rvel));
+#pragma unroll
+        for (int c = 0; c < 3; ++c) sF[c * NFNFP + m] = 0.5 * fs * (-(uM[c] * lvel - uP[c] * nuP) - lam * (uP[c] - uM[c]));
+        sS[m] = -1.0;
+      } else {
+        const int kind = __ldg(a.vel_bc + (-nb - 1));
+        double uR[3];
+        if (kind == 0) {
+          uR[0] = uR[1] = uR[2] = 0.0;
+        } else if (kind == 1) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) uR[c] = uM[c] - lvel * nv[c];
+        } else {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) uR[c] = uM[c];
+        }
+        const double rvel = nv[0] * uR[0] + nv[1] * uR[1] + nv[2] * uR[2];
+        sS[m] = fmax(fabs(lvel), fabs(rvel));
+#pragma unroll
+        for (int c = 0; c < 3; ++c) sF[c * NFNFP + m] = 0.5 * fs * (-(uM[c] * lvel - uR[c] * rvel));  // + wave term below
+      }
+    }
+    __syncwarp();
+    // boundary wave term: - floor(max over the face of the speeds) (uR - uM)
+    for (int m = lane; m < NFNFP; m += 32) {
+      if (sS[m] < 0.0) continue;
+      const int f = m / NFP, j = m - f * NFP;
+      double mx = 0.0;
+      for (int k = 0; k < NFP; ++k) mx = fmax(mx, sS[f * NFP + k]);
+      const double lam = (double)(int)mx;
+      if (lam == 0.0) continue;
+      double nv[3], sJ;
+      simplex_face_normal<3>(g, f, nv, &sJ);
+      const double fs = sJ / g[9];
+      const int o = fmask[f * NFP + j];
+      const double uM[3] = {sU[o], sU[NP + o], sU[2 * NP + o]};
+      const double lvel = nv[0] * uM[0] + nv[1] * uM[1] + nv[2] * uM[2];
+      const int kind = __ldg(a.vel_bc + (-__ldg(a.nbr + (size_t)e * NF + f) - 1));
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const double uR = kind == 0 ? 0.0 : kind == 1 ? uM[c] - lvel * nv[c] : uM[c];
+        sF[c * NFNFP + m] += 0.5 * fs * (-lam * (uR - uM[c]));
+      }
+    }
+    __syncwarp();
+    // N = sum_r D_r H_r + LIFT flux, then velT
+    for (int i = lane; i < NP; i += 32) {
+      double Nc[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        const double* Dr = sD + r * NP * NP + i * NP;
+        for (int k = 0; k < NP; ++k) {
+          const double dv = Dr[k];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) Nc[c] += dv * sH[(c * 3 + r) * NP + k];
+        }
+      }
+      const double* Li = sL + i * NFNFP;
+      for (int k = 0; k < NFNFP; ++k) {
+        const double lv = Li[k];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) Nc[c] += lv * sF[c * NFNFP + k];
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const size_t idx = c * n + (size_t)e * NP + i;
+        a.N[idx] = Nc[c];
+        a.velT[idx] = (a.a0 * sU[c * NP + i] + a.a1 * a.u_old[idx]) - a.dt * (a.b0 * Nc[c] + a.b1 * a.N_old[idx]);
+      }
+    }
+  }
+}
+
+template <int P>
+void launch_advection_t(const AdvArgs& a, cudaStream_t s) {
+  using Cf = Cfg<3, P>;
+  constexpr int NP = Cf::NP, NFNFP = 4 * Cf::NFP;
+  const size_t smem = (size_t)(3 * NP * NP + NP * NFNFP + kAdvWarps * (12 * NP + 4 * NFNFP)) * sizeof(double);
+  auto k = k_advection<P>;
+  SIPG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int grid = std::max(1, std::min((a.K + kAdvWarps - 1) / kAdvWarps, num_sms() * 8));
+  k<<<grid, kAdvWarps * 32, smem, s>>>(a);
+  note_launch();
+  SIPG_CUDA(cudaGetLastError());
+}
+
+void advection_device(sipg_mesh* m, int order, double dt, double a0, double a1, double b0, double b1,
+                      const double* u, const double* u_old, const double* N_old, const int* vel_bc, double* N,
+                      double* velT, cudaStream_t s) {
+  if (m->dim != 3) throw Error(SIPG_INVALID_ARG, "the advection step is 3D");
+  if (order < 1 || order > 4) throw Error(SIPG_INVALID_ARG, "order must be 1..4");
+  m->ensure_device();
+  AdvArgs a;
+  a.mats = adv_tables(order).mats.as<double>();
+  a.itab = dev_ref(3, order).itab.as<int8_t>();
+  a.geof = m->geof64.as<double>();
+  a.nbr = m->nbr.as<int>();
+  a.fcode = m->fcode.as<uint32_t>();
+  a.vel_bc = vel_bc;
+  a.u = u;
+  a.u_old = u_old;
+  a.N_old = N_old;
+  a.N = N;
+  a.velT = velT;
+  a.dt = dt;
+  a.a0 = a0;
+  a.a1 = a1;
+  a.b0 = b0;
+  a.b1 = b1;
+  a.K = m->K;
+  switch (order) {
+    case 1: launch_advection_t<1>(a, s); break;
+    case 2: launch_advection_t<2>(a, s); break;
+    case 3: launch_advection_t<3>(a, s); break;
+    default: launch_advection_t<4>(a, s); break;
+  }
+}
+
+}  // namespace
+}  // namespace sipg
+
+using namespace sipg;
+
+extern "C" {
+
+int sipg_ins_advection(sipg_mesh* m, int order, double dt, double a0, double a1, double b0, double b1,
+                       const double* vel, const double* vel_old, const double* N_old, const int* vel_bc, double* N,
+                       double* velT, void* stream) {
+  return guarded([&] {
+    if (!m || !vel || !vel_old || !N_old || !vel_bc || !N || !velT) throw Error(SIPG_INVALID_ARG, "advection arguments");
+    advection_device(m, order, dt, a0, a1, b0, b1, vel, vel_old, N_old, vel_bc, N, velT, (cudaStream_t)stream);
+  });
+}
+
+int sipg_ins_advection_host(sipg_mesh* m, int order, double dt, double a0, double a1, double b0, double b1,
+                            const double* vel, const double* vel_old, const double* N_old, const int* vel_bc,
+                            double* N, double* velT) {
+  return guarded([&] {
+    if (!m || !vel || !vel_old || !N_old || !vel_bc || !N || !velT) throw Error(SIPG_INVALID_ARG, "advection arguments");
+    m->ensure_device();
+    const size_t n = (size_t)3 * m->K * np_of(3, order), bytes = n * sizeof(double);
+    DevBuf du(bytes), duo(bytes), dno(bytes), dn(bytes), dv(bytes), db(std::max<size_t>(1, m->Kb) * sizeof(int));
+    du.upload(vel, bytes);
+    duo.upload(vel_old, bytes);
+    dno.upload(N_old, bytes);
+    if (m->Kb) db.upload(vel_bc, m->Kb * sizeof(int));
+    advection_device(m, order, dt, a0, a1, b0, b1, du.as<double>(), duo.as<double>(), dno.as<double>(), db.as<int>(),
+                     dn.as<double>(), dv.as<double>(), 0);
+    SIPG_CUDA(cudaMemcpy(N, dn.p, bytes, cudaMemcpyDeviceToHost));
+    SIPG_CUDA(cudaMemcpy(velT, dv.p, bytes, cudaMemcpyDeviceToHost));
+  });
+}
+
+}  // extern "C"

@@ -225,6 +225,20 @@ class Mesh:
 
 
 
+def ins_advection(mesh, order, dt, a0, a1, b0, b1, vel, vel_old, N_old, vel_bc):
+    """Non-linear advection step (sipg_ins_advection_host): returns (N, velT),
+    each (3, K, Np); vel_bc: Kb velocity boundary types (0 no-slip, 1 slip,
+    2 natural outflow)."""
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (vel, vel_old, N_old)]
+    bc = np.ascontiguousarray(vel_bc, dtype=np.int32).reshape(-1)
+    N = np.zeros_like(arrs[0])
+    velT = np.zeros_like(arrs[0])
+    check(lib().sipg_ins_advection_host(mesh.h, order, C.c_double(dt), C.c_double(a0), C.c_double(a1),
+                                        C.c_double(b0), C.c_double(b1), _dp(arrs[0]), _dp(arrs[1]), _dp(arrs[2]),
+                                        _ip(bc), _dp(N), _dp(velT)))
+    return N, velT
+
+
 def projection_factor(dim, dt):
     """The penalty factor INSSolverBase{3D,2D}::project_velocity passes to the
     element-local solve: dt in 3D (src/solvers/3d/ins_solver_base.cpp:1082),

@@ -1,0 +1,105 @@
+"""The time-step oracle (oracle/ins_oracle.py) against the reference's own
+kernels: the non-linear advection step of INSSolverBase3D::advec_current_non_linear
+/ advec_standard (src/solvers/3d/ins_solver_base.cpp:224-329, 451-480) run through
+ins_3d_advec_0 (cells), ins_3d_advec_1 (interior faces), ins_3d_advec_2 (boundary
+faces: no-slip, slip, natural outflow) and ins_3d_advec_3 (cells) compiled in
+oracle/_ref, with the toolkit glue (mesh->div, the LIFT op2_gemv) restated."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import dg_oracle as D
+import ins_oracle as I
+import oracle_py as O
+
+pytestmark = pytest.mark.skipif(not O.have_ref(), reason="oracle/_ref not built")
+
+
+def call(om, name, args):
+    keep = []
+    ptrs = []
+    for a in args:
+        if isinstance(a, list):  # a face argument: pointers to the two cells' data
+            arr = (C.c_void_p * len(a))(*[x.ctypes.data_as(C.c_void_p) for x in a])
+            keep.append(arr)
+            ptrs.append(C.cast(arr, C.c_void_p))
+        else:
+            ptrs.append(a.ctypes.data_as(C.c_void_p))
+    pa = (C.c_void_p * len(ptrs))(*ptrs)
+    assert O.ref_lib().ref_kernel(C.byref(om.s), name.encode(), pa) == 0, name
+
+
+def reference_advection(mesh, t, om, dt, a0, a1, b0, b1, u, u_old, N_old, vel_bc):
+    K, Np, Nf, Nfp = mesh.K, t["Np"], t["Nf"], t["Nfp"]
+    fm, pp = t["fmask"], t["perm_pos"]
+    F = np.zeros((3, 3, K, Np))
+    for e in range(K):
+        outs = [np.zeros(Np) for _ in range(9)]
+        call(om, "ins_3d_advec_0", [u[0, e].copy(), u[1, e].copy(), u[2, e].copy()] + outs)
+        for c in range(3):
+            for d in range(3):
+                F[c, d, e] = outs[3 * c + d]
+    N = np.stack([I.divergence(mesh, I._tables(t["order"]), F[c]) for c in range(3)])
+    flux = np.zeros((3, K, Nf * Nfp))
+    rows = [[np.ascontiguousarray(u[c, e]) for e in range(K)] for c in range(3)]
+    fl = [[np.zeros(Nf * Nfp) for _ in range(K)] for _ in range(3)]
+    nrm = np.stack([mesh.nx, mesh.ny, mesh.nz], 2)
+    for (L, R), (fL, fR), sLR, sRL in zip(mesh.face2cells, mesh.faceNum, mesh.sLR, mesh.sRL):
+        fmL_corr = np.ascontiguousarray(fm[fL][pp[sRL]], dtype=np.int32)  # L nodes in R's face order
+        fmR_corr = np.ascontiguousarray(fm[fR][pp[sLR]], dtype=np.int32)  # R nodes in L's face order
+        args = [np.array([fL, fR], np.int32), fmL_corr, fmR_corr,
+                np.array([nrm[L, fL, 0], nrm[R, fR, 0]]), np.array([nrm[L, fL, 1], nrm[R, fR, 1]]),
+                np.array([nrm[L, fL, 2], nrm[R, fR, 2]]), np.array([mesh.fscale[L, fL], mesh.fscale[R, fR]]),
+                [rows[0][L], rows[0][R]], [rows[1][L], rows[1][R]], [rows[2][L], rows[2][R]],
+                [fl[0][L], fl[0][R]], [fl[1][L], fl[1][R]], [fl[2][L], fl[2][R]]]
+        call(om, "ins_3d_advec_1", args)
+    bct = np.asarray(vel_bc).reshape(-1)
+    e_x = mesh.export(t["order"], t)
+    for b, (e, f) in enumerate(zip(mesh.bface2cell, mesh.bfaceNum)):
+        args = [np.array([0.0]), np.array([bct[b]], np.int32), np.array([f], np.int32),
+                np.array([nrm[e, f, 0]]), np.array([nrm[e, f, 1]]), np.array([nrm[e, f, 2]]),
+                np.array([mesh.fscale[e, f]]), e_x["x"][e].copy(), e_x["y"][e].copy(), e_x["z"][e].copy(),
+                rows[0][e], rows[1][e], rows[2][e], fl[0][e], fl[1][e], fl[2][e]]
+        call(om, "ins_3d_advec_2", args)
+    for c in range(3):
+        for e in range(K):
+            flux[c, e] = fl[c][e]
+    LIFT = I._tables(t["order"])["LIFT"]
+    N = N + flux @ LIFT.T
+    velT = np.zeros_like(u)
+    for e in range(K):
+        outs = [np.zeros(Np) for _ in range(3)]
+        args = [np.array([a0]), np.array([a1]), np.array([b0]), np.array([b1]), np.array([dt])]
+        args += [u[c, e].copy() for c in range(3)] + [u_old[c, e].copy() for c in range(3)]
+        args += [N[c, e].copy() for c in range(3)] + [N_old[c, e].copy() for c in range(3)] + outs
+        call(om, "ins_3d_advec_3", args)
+        for c in range(3):
+            velT[c, e] = outs[c]
+    return N, velT
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+@pytest.mark.parametrize("scale", [0.5, 3.0], ids=["slow", "fast"])
+def test_advection_matches_the_reference_kernels(p, scale):
+    mesh = D.Mesh.box(3, 3, 0.1, 5)
+    t = D.ref_tables(3, p)
+    om = O.OMesh(t, mesh.export(p, t))
+    rng = np.random.default_rng(p)
+    u, u_old, N_old = rng.uniform(-scale, scale, (3, 3, mesh.K, t["Np"]))
+    vel_bc = (np.arange(mesh.Kb) % 3).astype(np.int32)  # no-slip, slip, outflow
+    dt, a0, a1, b0, b1 = 1e-3, 2.0, -0.5, 2.0, -1.0
+    N, velT = I.advection(mesh, p, dt, a0, a1, b0, b1, u, u_old, N_old, vel_bc)
+    Nr, velTr = reference_advection(mesh, t, om, dt, a0, a1, b0, b1, u, u_old, N_old, vel_bc)
+    assert np.abs(N - Nr).max() <= 1e-12 * np.abs(Nr).max()
+    assert np.abs(velT - velTr).max() <= 1e-12 * np.abs(velTr).max()
+
+
+def test_advection_of_a_uniform_flow_vanishes_inside():
+    """u constant: u (x) u is constant, its divergence zero, interior jumps zero."""
+    mesh = D.Mesh.box(3, 3, 0.1, 5)
+    t = D.ref_tables(3, 2)
+    u = np.zeros((3, mesh.K, t["Np"]))
+    u[0], u[1], u[2] = 0.3, -0.2, 0.1
+    N = I.nonlinear(mesh, 2, u, np.full(mesh.Kb, I.BC_OUTFLOW, np.int32))
+    assert np.abs(N).max() < 1e-12

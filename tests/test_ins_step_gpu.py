@@ -1,0 +1,32 @@
+"""The time-step kernels around the solves against the time-step oracle
+(oracle/ins_oracle.py, itself pinned against the reference's kernels in
+tests/test_ins_oracle.py): the fused non-linear advection step."""
+import numpy as np
+import pytest
+
+import dg_oracle as D
+import ins_oracle as I
+import sipg
+from helpers import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 4])
+@pytest.mark.parametrize("scale", [0.5, 3.0], ids=["slow", "fast"])
+def test_advection_matches_the_oracle(p, scale):
+    n = 3
+    gm = sipg.Mesh.box(3, n, jitter=0.1, seed=5)
+    om = D.Mesh.box(3, n, 0.1, 5)
+    Np = sipg.ref_sizes(3, p)[0]
+    rng = np.random.default_rng(10 + p)
+    u, u_old, N_old = rng.uniform(-scale, scale, (3, 3, gm.K, Np))
+    vel_bc = (np.arange(gm.Kb) % 3).astype(np.int32)
+    args = (1e-3, 2.0, -0.5, 2.0, -1.0)
+    N, velT = sipg.ins_advection(gm, p, *args, u, u_old, N_old, vel_bc)
+    Nw, velTw = I.advection(om, p, *args, u, u_old, N_old, vel_bc)
+    # p = 4: the oracle's monomial-basis reference tables agree with the library's to
+    # about 1e-13, which the derivatives of the quadratic flux amplify (1.1e-11 measured)
+    tol = 1e-12 if p < 4 else 1e-10
+    assert rel_err(N, Nw) < tol
+    assert rel_err(velT, velTw) < tol
