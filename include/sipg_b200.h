@@ -418,6 +418,16 @@ int sipg_ins_advection_host(sipg_mesh *m, int order, double dt, double a0, doubl
                             const double *vel, const double *vel_old, const double *N_old, const int *vel_bc,
                             double *N, double *velT);
 
+/* Curl-curl Neumann data of the multiphase pressure step, MPINSSolver3D::
+ * apply_pressure_neumann_bc (src/solvers/3d/mp_ins_solver.cpp:450-493): on no-slip and
+ * slip walls dPdN = fscale n . (-N - curl(mu curl u) / (Re rho)) at the face nodes
+ * (mesh->curl, mp_ins_3d_pr_mu, mp_ins_3d_pr_0), zero on the other faces; the input
+ * of sipg_pressure_rhs. vel, N: 3 x K x Np; mu, rho: K x Np; dPdN: K x 4 x Nfp. */
+int sipg_ins_pressure_neumann(sipg_mesh *m, int order, double reynolds, const double *vel, const double *N,
+                              const double *mu, const double *rho, const int *vel_bc, double *dPdN, void *stream);
+int sipg_ins_pressure_neumann_host(sipg_mesh *m, int order, double reynolds, const double *vel, const double *N,
+                                   const double *mu, const double *rho, const int *vel_bc, double *dPdN);
+
 /* Number of kernels this library has launched so far in the process
  * (diagnostics for benchmarks; no reference counterpart). */
 int sipg_launch_count(unsigned long long *n);

@@ -1,5 +1,5 @@
-// Non-linear advection step of the 3D incompressible time step, fused into one
-// kernel: INSSolverBase3D::advec_current_non_linear + advec_standard
+// Steps of the 3D incompressible time step around the solves. Non-linear
+// advection, fused into one kernel: INSSolverBase3D::advec_current_non_linear + advec_standard
 // (src/solvers/3d/ins_solver_base.cpp:224-329, 451-480), i.e. the flux tensor
 // u (x) u (ins_3d_advec_0), its strong-form divergence (mesh->div), the
 // Lax-Friedrichs face fluxes (ins_3d_advec_1 interior, ins_3d_advec_2 boundary:
@@ -201,6 +201,142 @@ __global__ void __launch_bounds__(kAdvWarps * 32) k_advection(const AdvArgs a) {
   }
 }
 
+struct PnArgs {
+  const double* mats;  // Dr, Ds, Dt first
+  const int8_t* itab;
+  const double* geof;
+  const int* nbr;
+  const int* belems;
+  int n_belem;
+  const int* vel_bc;
+  const double *u, *N, *mu, *rho;
+  double* dPdN;  // K x 4 x Nfp, zeroed before
+  double reynolds;
+  int K;
+};
+
+// Curl-curl Neumann data of the multiphase pressure step
+// (MPINSSolver3D::apply_pressure_neumann_bc, src/solvers/3d/mp_ins_solver.cpp:450-493):
+// w = mu curl u (mesh->curl, mp_ins_3d_pr_mu), then on no-slip and slip walls
+// (mp_ins_3d_pr_0) dPdN = fscale n . (-N - curl w / (Re rho)) at the face nodes. One
+// warp per element that owns a boundary face; the curls are the element-local
+// strong-form derivatives.
+template <int P>
+__global__ void __launch_bounds__(kAdvWarps * 32) k_pressure_neumann(const PnArgs a) {
+  using Cf = Cfg<3, P>;
+  constexpr int NP = Cf::NP, NFP = Cf::NFP, NF = 4, NG = 10;
+  extern __shared__ double sm[];
+  const double* sD = sm;  // 3 x NP x NP
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* sU = sm + 3 * NP * NP + warp * 6 * NP;  // [3][NP] u
+  double* sW = sU + 3 * NP;                       // [3][NP] mu curl u
+  for (int i = threadIdx.x; i < 3 * NP * NP; i += blockDim.x) sm[i] = a.mats[i];
+  __syncthreads();
+  const int8_t* fmask = a.itab;
+  const size_t n = (size_t)a.K * NP;
+  for (int it = blockIdx.x * kAdvWarps + warp; it < a.n_belem; it += gridDim.x * kAdvWarps) {
+    const int e = __ldg(a.belems + it);
+    double g[NG];
+#pragma unroll
+    for (int k = 0; k < NG; ++k) g[k] = __ldg(a.geof + (size_t)e * NG + k);
+    __syncwarp();
+    for (int i = lane; i < 3 * NP; i += 32) sU[i] = a.u[(i / NP) * n + (size_t)e * NP + i % NP];
+    __syncwarp();
+    // w = mu curl u at every node
+    for (int i = lane; i < NP; i += 32) {
+      double gr[3][3];  // gr[c][d] = d u_c / dx_d
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        double dr[3] = {0.0, 0.0, 0.0};
+        for (int k = 0; k < NP; ++k) {
+          const double uk = sU[c * NP + k];
+#pragma unroll
+          for (int r = 0; r < 3; ++r) dr[r] += sD[r * NP * NP + i * NP + k] * uk;
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) gr[c][d] = g[d] * dr[0] + g[3 + d] * dr[1] + g[6 + d] * dr[2];
+      }
+      const double mu = a.mu[(size_t)e * NP + i];
+      sW[0 * NP + i] = mu * (gr[2][1] - gr[1][2]);
+      sW[1 * NP + i] = mu * (gr[0][2] - gr[2][0]);
+      sW[2 * NP + i] = mu * (gr[1][0] - gr[0][1]);
+    }
+    __syncwarp();
+    for (int m = lane; m < NF * NFP; m += 32) {
+      const int f = m / NFP, j = m - f * NFP;
+      const int nb = __ldg(a.nbr + (size_t)e * NF + f);
+      if (nb >= 0) continue;
+      const int kind = __ldg(a.vel_bc + (-nb - 1));
+      if (kind != 0 && kind != 1) continue;  // natural outflow: no Neumann data
+      const int i = fmask[f * NFP + j];
+      double gr[3][3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        double dr[3] = {0.0, 0.0, 0.0};
+        for (int k = 0; k < NP; ++k) {
+          const double wk = sW[c * NP + k];
+#pragma unroll
+          for (int r = 0; r < 3; ++r) dr[r] += sD[r * NP * NP + i * NP + k] * wk;
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) gr[c][d] = g[d] * dr[0] + g[3 + d] * dr[1] + g[6 + d] * dr[2];
+      }
+      const double c2[3] = {gr[2][1] - gr[1][2], gr[0][2] - gr[2][0], gr[1][0] - gr[0][1]};
+      double nv[3], sJ;
+      simplex_face_normal<3>(g, f, nv, &sJ);
+      const double fs = sJ / g[9];
+      const double rr = a.reynolds * a.rho[(size_t)e * NP + i];
+      double s = 0.0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) s += nv[c] * (-a.N[c * n + (size_t)e * NP + i] - c2[c] / rr);
+      a.dPdN[((size_t)e * NF + f) * NFP + j] = fs * s;
+    }
+  }
+}
+
+template <int P>
+void launch_pressure_neumann_t(const PnArgs& a, cudaStream_t s) {
+  constexpr int NP = Cfg<3, P>::NP;
+  const size_t smem = (size_t)(3 * NP * NP + kAdvWarps * 6 * NP) * sizeof(double);
+  auto k = k_pressure_neumann<P>;
+  SIPG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int grid = std::max(1, std::min((a.n_belem + kAdvWarps - 1) / kAdvWarps, num_sms() * 8));
+  k<<<grid, kAdvWarps * 32, smem, s>>>(a);
+  note_launch();
+  SIPG_CUDA(cudaGetLastError());
+}
+
+void pressure_neumann_device(sipg_mesh* m, int order, double reynolds, const double* u, const double* N,
+                             const double* mu, const double* rho, const int* vel_bc, double* dPdN, cudaStream_t s) {
+  if (m->dim != 3) throw Error(SIPG_INVALID_ARG, "the pressure Neumann data are 3D");
+  if (order < 1 || order > 4) throw Error(SIPG_INVALID_ARG, "order must be 1..4");
+  m->ensure_device();
+  const int Nfp = nfp_of(3, order);
+  SIPG_CUDA(cudaMemsetAsync(dPdN, 0, (size_t)m->K * 4 * Nfp * sizeof(double), s));
+  if (m->n_belem == 0) return;
+  PnArgs a;
+  a.mats = adv_tables(order).mats.as<double>();
+  a.itab = dev_ref(3, order).itab.as<int8_t>();
+  a.geof = m->geof64.as<double>();
+  a.nbr = m->nbr.as<int>();
+  a.belems = m->belems.as<int>();
+  a.n_belem = m->n_belem;
+  a.vel_bc = vel_bc;
+  a.u = u;
+  a.N = N;
+  a.mu = mu;
+  a.rho = rho;
+  a.dPdN = dPdN;
+  a.reynolds = reynolds;
+  a.K = m->K;
+  switch (order) {
+    case 1: launch_pressure_neumann_t<1>(a, s); break;
+    case 2: launch_pressure_neumann_t<2>(a, s); break;
+    case 3: launch_pressure_neumann_t<3>(a, s); break;
+    default: launch_pressure_neumann_t<4>(a, s); break;
+  }
+}
+
 template <int P>
 void launch_advection_t(const AdvArgs& a, cudaStream_t s) {
   using Cf = Cfg<3, P>;
@@ -278,6 +414,36 @@ int sipg_ins_advection_host(sipg_mesh* m, int order, double dt, double a0, doubl
                      dn.as<double>(), dv.as<double>(), 0);
     SIPG_CUDA(cudaMemcpy(N, dn.p, bytes, cudaMemcpyDeviceToHost));
     SIPG_CUDA(cudaMemcpy(velT, dv.p, bytes, cudaMemcpyDeviceToHost));
+  });
+}
+
+int sipg_ins_pressure_neumann(sipg_mesh* m, int order, double reynolds, const double* vel, const double* N,
+                              const double* mu, const double* rho, const int* vel_bc, double* dPdN, void* stream) {
+  return guarded([&] {
+    if (!m || !vel || !N || !mu || !rho || !vel_bc || !dPdN || !(reynolds > 0.0))
+      throw Error(SIPG_INVALID_ARG, "pressure Neumann data arguments");
+    pressure_neumann_device(m, order, reynolds, vel, N, mu, rho, vel_bc, dPdN, (cudaStream_t)stream);
+  });
+}
+
+int sipg_ins_pressure_neumann_host(sipg_mesh* m, int order, double reynolds, const double* vel, const double* N,
+                                   const double* mu, const double* rho, const int* vel_bc, double* dPdN) {
+  return guarded([&] {
+    if (!m || !vel || !N || !mu || !rho || !vel_bc || !dPdN || !(reynolds > 0.0))
+      throw Error(SIPG_INVALID_ARG, "pressure Neumann data arguments");
+    m->ensure_device();
+    const int Np = np_of(3, order), Nfp = nfp_of(3, order);
+    const size_t nv = (size_t)3 * m->K * Np * sizeof(double), ns = (size_t)m->K * Np * sizeof(double);
+    const size_t nd = (size_t)m->K * 4 * Nfp * sizeof(double);
+    DevBuf du(nv), dn(nv), dmu(ns), drho(ns), dd(nd), db(std::max<size_t>(1, m->Kb) * sizeof(int));
+    du.upload(vel, nv);
+    dn.upload(N, nv);
+    dmu.upload(mu, ns);
+    drho.upload(rho, ns);
+    if (m->Kb) db.upload(vel_bc, m->Kb * sizeof(int));
+    pressure_neumann_device(m, order, reynolds, du.as<double>(), dn.as<double>(), dmu.as<double>(),
+                            drho.as<double>(), db.as<int>(), dd.as<double>(), 0);
+    SIPG_CUDA(cudaMemcpy(dPdN, dd.p, nd, cudaMemcpyDeviceToHost));
   });
 }
 

@@ -239,6 +239,20 @@ def ins_advection(mesh, order, dt, a0, a1, b0, b1, vel, vel_old, N_old, vel_bc):
     return N, velT
 
 
+def ins_pressure_neumann(mesh, order, reynolds, vel, N, mu, rho, vel_bc):
+    """Curl-curl Neumann data of the multiphase pressure step
+    (sipg_ins_pressure_neumann_host): returns dPdN (K, 4, Nfp), nonzero on the
+    no-slip and slip wall faces; vel, N: (3, K, Np); mu, rho: (K, Np)."""
+    v, n = (np.ascontiguousarray(a, dtype=np.float64) for a in (vel, N))
+    m, r = (np.ascontiguousarray(a, dtype=np.float64) for a in (mu, rho))
+    bc = np.ascontiguousarray(vel_bc, dtype=np.int32).reshape(-1)
+    nfp = (order + 1) * (order + 2) // 2
+    out = np.zeros((v.shape[1], 4, nfp))
+    check(lib().sipg_ins_pressure_neumann_host(mesh.h, order, C.c_double(reynolds), _dp(v), _dp(n), _dp(m),
+                                               _dp(r), _ip(bc), _dp(out)))
+    return out
+
+
 def projection_factor(dim, dt):
     """The penalty factor INSSolverBase{3D,2D}::project_velocity passes to the
     element-local solve: dt in 3D (src/solvers/3d/ins_solver_base.cpp:1082),

@@ -2,6 +2,9 @@
 solves, restated in numpy. TEST INFRASTRUCTURE ONLY (tests/, the CPU legs of
 the benchmark).
 
+pressure_neumann: the curl-curl Neumann data of the multiphase pressure step,
+MPINSSolver3D::apply_pressure_neumann_bc (src/solvers/3d/mp_ins_solver.cpp:450-493).
+
 advection: INSSolverBase3D::advec_current_non_linear and advec_standard
 (src/solvers/3d/ins_solver_base.cpp:224-329, 451-480): the flux tensor
 u (x) u at the nodes (ins_3d_advec_0), its strong-form divergence (mesh->div of
@@ -82,6 +85,42 @@ def nonlinear(mesh, p, u, vel_bc):
     N = np.stack([divergence(mesh, t, F[c]) for c in range(3)])
     fl = face_flux(mesh, t, u, vel_bc).reshape(3, mesh.K, -1)
     return N + fl @ t["LIFT"].T
+
+
+def gradient(mesh, t, f):
+    """(3, K, Np): d f / dx_d, strong form, element-local."""
+    Dm = [t["Dr"], t["Ds"], t["Dt"]]
+    return np.stack([sum(mesh.G[:, r, d][:, None] * (f @ Dm[r].T) for r in range(3)) for d in range(3)])
+
+
+def curl(mesh, t, u):
+    """mesh->curl (OP2-DG-Toolkit, unvendored, restated): the strong-form,
+    element-local curl of a nodal vector field (3, K, Np)."""
+    g = [gradient(mesh, t, u[c]) for c in range(3)]  # g[c][d] = d u_c / dx_d
+    return np.stack([g[2][1] - g[1][2], g[0][2] - g[2][0], g[1][0] - g[0][1]])
+
+
+def pressure_neumann(mesh, p, u, N, mu, rho, vel_bc, reynolds):
+    """dPdN (K, Nf, Nfp) of MPINSSolver3D::apply_pressure_neumann_bc
+    (src/solvers/3d/mp_ins_solver.cpp:450-493): curl(mu curl u) (mesh->curl,
+    mp_ins_3d_pr_mu, mesh->curl), then on no-slip and slip walls (mp_ins_3d_pr_0)
+    fscale n . (-N - curl2 / (Re rho)) at the face nodes; zero elsewhere (natural
+    outflow and interior faces)."""
+    t = _tables(p)
+    c2 = curl(mesh, t, curl(mesh, t, u) * mu[None])
+    K, Nf, Nfp = mesh.K, t["Nf"], t["Nfp"]
+    out = np.zeros((K, Nf, Nfp))
+    bct = np.asarray(vel_bc).reshape(-1)
+    nrm = np.stack([mesh.nx, mesh.ny, mesh.nz], 2)
+    for e in range(K):
+        for f in range(Nf):
+            nb = mesh.nbr[e, f]
+            if nb >= 0 or bct[-nb - 1] not in (BC_NO_SLIP, BC_SLIP):
+                continue
+            m = t["fmask"][f]
+            res = -N[:, e, m] - c2[:, e, m] / (reynolds * rho[e, m])
+            out[e, f] = mesh.fscale[e, f] * (nrm[e, f] @ res)
+    return out
 
 
 def advection(mesh, p, dt, a0, a1, b0, b1, u, u_old, N_old, vel_bc):

@@ -102,6 +102,11 @@ namespace d3p4 { constexpr int ORDER = 4, NP = 35, NPF = 15, NF = 4;
   }
 
 extern "C" {
+// The Reynolds number of the multiphase pressure boundary kernel, every build.
+void ref_set_reynolds(double re) {
+  d2p1::r_ynolds = d2p2::r_ynolds = d2p3::r_ynolds = d2p4::r_ynolds = re;
+  d3p1::r_ynolds = d3p2::r_ynolds = d3p3::r_ynolds = d3p4::r_ynolds = re;
+}
 int ref_mult(const oracle_mesh *m, int ncomp, const int *bc_types, const double *factor,
              const double *mm_factor, double mm_scalar, int flags, const double *const *x,
              double *const *y) {

@@ -103,3 +103,39 @@ def test_advection_of_a_uniform_flow_vanishes_inside():
     u[0], u[1], u[2] = 0.3, -0.2, 0.1
     N = I.nonlinear(mesh, 2, u, np.full(mesh.Kb, I.BC_OUTFLOW, np.int32))
     assert np.abs(N).max() < 1e-12
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+def test_pressure_neumann_data_matches_the_reference_kernels(p):
+    """curl, mp_ins_3d_pr_mu, curl, then mp_ins_3d_pr_0 on every boundary face
+    (the curls are the restated toolkit glue, as in the oracle)."""
+    mesh = D.Mesh.box(3, 3, 0.1, 5)
+    t = D.ref_tables(3, p)
+    e_x = mesh.export(p, t)
+    om = O.OMesh(t, e_x)
+    rng = np.random.default_rng(20 + p)
+    u, N = rng.uniform(-1, 1, (2, 3, mesh.K, t["Np"]))
+    mu = rng.uniform(1.0, 100.0, (mesh.K, t["Np"]))
+    rho = rng.uniform(1.0, 1000.0, (mesh.K, t["Np"]))
+    vel_bc = (np.arange(mesh.Kb) % 3).astype(np.int32)
+    re = 123.0
+    want = I.pressure_neumann(mesh, p, u, N, mu, rho, vel_bc, re)
+    tt = I._tables(p)
+    cu = I.curl(mesh, tt, u)
+    for e in range(mesh.K):
+        rows = [np.ascontiguousarray(cu[c, e]) for c in range(3)]
+        call(om, "mp_ins_3d_pr_mu", [mu[e].copy()] + rows)
+        for c in range(3):
+            cu[c, e] = rows[c]
+    c2 = I.curl(mesh, tt, cu)
+    O.ref_lib().ref_set_reynolds(C.c_double(re))
+    got = np.zeros((mesh.K, t["Nf"] * t["Nfp"]))
+    nrm = np.stack([mesh.nx, mesh.ny, mesh.nz], 2)
+    for b, (e, f) in enumerate(zip(mesh.bface2cell, mesh.bfaceNum)):
+        args = [np.array([0.0]), np.array([vel_bc[b]], np.int32), np.array([f], np.int32),
+                np.array([nrm[e, f, 0]]), np.array([nrm[e, f, 1]]), np.array([nrm[e, f, 2]]),
+                np.array([mesh.fscale[e, f]]), e_x["x"][e].copy(), e_x["y"][e].copy(), e_x["z"][e].copy(),
+                N[0, e].copy(), N[1, e].copy(), N[2, e].copy(), c2[0, e].copy(), c2[1, e].copy(), c2[2, e].copy(),
+                rho[e].copy(), got[e]]
+        call(om, "mp_ins_3d_pr_0", args)
+    assert np.abs(got.reshape(want.shape) - want).max() <= 1e-12 * np.abs(want).max()

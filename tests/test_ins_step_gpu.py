@@ -1,6 +1,7 @@
 """The time-step kernels around the solves against the time-step oracle
 (oracle/ins_oracle.py, itself pinned against the reference's kernels in
-tests/test_ins_oracle.py): the fused non-linear advection step."""
+tests/test_ins_oracle.py): the fused non-linear advection step and the
+curl-curl pressure Neumann data."""
 import numpy as np
 import pytest
 
@@ -30,3 +31,32 @@ def test_advection_matches_the_oracle(p, scale):
     tol = 1e-12 if p < 4 else 1e-10
     assert rel_err(N, Nw) < tol
     assert rel_err(velT, velTw) < tol
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 4])
+def test_pressure_neumann_data_match_the_oracle(p):
+    n = 3
+    gm = sipg.Mesh.box(3, n, jitter=0.1, seed=5)
+    om = D.Mesh.box(3, n, 0.1, 5)
+    Np = sipg.ref_sizes(3, p)[0]
+    rng = np.random.default_rng(30 + p)
+    u, N = rng.uniform(-1, 1, (2, 3, gm.K, Np))
+    mu = rng.uniform(1.0, 100.0, (gm.K, Np))
+    rho = rng.uniform(1.0, 1000.0, (gm.K, Np))
+    vel_bc = (np.arange(gm.Kb) % 3).astype(np.int32)
+    got = sipg.ins_pressure_neumann(gm, p, 123.0, u, N, mu, rho, vel_bc)
+    want = I.pressure_neumann(om, p, u, N, mu, rho, vel_bc, 123.0)
+    # two derivative passes amplify the last-bit differences of the reference tables
+    assert rel_err(got, want) < (1e-12 if p < 4 else 1e-10)
+    # outflow faces and interior faces carry no data
+    assert np.all(got[want == 0.0] == 0.0)
+
+
+def test_pressure_neumann_data_vanish_without_walls():
+    gm = sipg.Mesh.box(3, 2, jitter=0.1, seed=1)
+    Np = sipg.ref_sizes(3, 2)[0]
+    rng = np.random.default_rng(3)
+    u, N = rng.uniform(-1, 1, (2, 3, gm.K, Np))
+    ones = np.ones((gm.K, Np))
+    got = sipg.ins_pressure_neumann(gm, 2, 10.0, u, N, ones, ones, np.full(gm.Kb, 2, np.int32))
+    assert not got.any()
