@@ -263,6 +263,63 @@ def run_viscous(steps=3):
             "iters": int(infos[-1].iters), "true_rel_res": float(infos[-1].true_rel_res)}
 
 
+TWO_PHASE_STEPS = 100
+
+
+def rising_bubble(n=32, order=3):
+    """The rising-bubble case: 32^3 x 6 tets, level set of the sphere r = 0.25 at
+    (0.5, 0.3, 0.5) (negative inside: the light phase), at rest, no-slip walls."""
+    mesh = sipg.Mesh.box(3, n, jitter=0.1, seed=20261203)
+    e = mesh.export(order)
+    s = np.sqrt((e["x"] - 0.5) ** 2 + (e["y"] - 0.3) ** 2 + (e["z"] - 0.5) ** 2) - 0.25
+    vel = np.zeros((3,) + s.shape)
+    return mesh, s, vel, np.zeros(mesh.Kb, np.int32)
+
+
+def run_two_phase(steps=TWO_PHASE_STEPS):
+    """The full two-phase time-step loop (sipg_ins3d_step): rising bubble, density
+    ratio 1000, viscosity ratio 100, gravity 9.81 along -y, Re 100, CFL 0.5 (of the
+    reference's dt = h / ((p+1)^2 max |u|)), `steps` steps of advection, pressure
+    (mixed or FP64 p-multigrid), viscosity (three Jacobi-PCG solves) and level-set
+    advection; the mixed run's velocity and level set against the FP64 run's."""
+    mesh, s, vel, vel_bc = rising_bubble()
+    consts = dict(order=3, reynolds=100.0, rho0=1.0, rho1=1e-3, mu0=1.0, mu1=1e-2, gravity=9.81, ls_alpha=2.0,
+                  cfl=0.5)
+    runs = {}
+    for name, prec in (("fp64", sipg.FP64), ("mixed", sipg.FP32)):
+        ins = sipg.Ins3D(mesh, vel_bc, **consts, precision=prec)
+        ins.set_state(vel, s)
+        ins.step(1)  # first step: set-up of the solvers' workspaces
+        t0 = time.perf_counter()
+        parts = np.zeros(4)
+        it_pr, it_vis = [], []
+        for _ in range(steps - 1):
+            info = ins.step(1)
+            parts += [info.ms_advection, info.ms_pressure, info.ms_viscosity, info.ms_surface]
+            it_pr.append(info.pr_iters)
+            it_vis.append(sum(info.vis_iters))
+        wall = (time.perf_counter() - t0) * 1e3 / (steps - 1)
+        st = ins.state()
+        runs[name] = dict(ms_per_step=wall, parts_ms=(parts / (steps - 1)).tolist(), pr_iters=float(np.mean(it_pr)),
+                          vis_iters=float(np.mean(it_vis)), time=info.time, dt=info.dt, max_vel=info.max_vel,
+                          proj_converged=int(info.proj_converged), state=st)
+        ins.close()
+    a, b = runs["fp64"]["state"], runs["mixed"]["state"]
+    rel = lambda x, y: float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
+    up = float(a["vel"][1][s < 0].mean())
+    for r in runs.values():
+        r.pop("state")
+    return {"workload": f"rising bubble 32^3x6 = {mesh.K:,} tets, p = 3, {steps} steps at CFL 0.5, density ratio "
+                        "1000, viscosity ratio 100, gravity 9.81 along -y, Re 100, no-slip walls; level set "
+                        "advected, not reinitialised",
+            "steps": steps, "fp64": runs["fp64"], "mixed": runs["mixed"],
+            "mixed_vs_fp64_step_speedup": runs["fp64"]["ms_per_step"] / runs["mixed"]["ms_per_step"],
+            "parts": ["advection", "pressure", "viscosity", "surface"],
+            "mixed_vs_fp64": {"velocity_rel_l2": rel(b["vel"], a["vel"]), "level_set_rel_l2": rel(b["s"], a["s"]),
+                              "pressure_rel_l2": rel(b["pr"] - b["pr"].mean(), a["pr"] - a["pr"].mean())},
+            "mean_v_in_bubble_fp64": up}
+
+
 def run_over_integrated(c, steps=5, warmup=3):
     """The headline problem with the factor at the cubature points
     (sipg_op_set_factor_oi, FactorPoissonMatrixFreeDiagOI3D's inputs): 1/rho of
@@ -492,6 +549,8 @@ def run_ours(args):
     }
     out["over_integrated"] = run_over_integrated(c)
     out["viscous"] = run_viscous()
+    if not args.skip_two_phase and world == 1:
+        out["two_phase_step"] = run_two_phase(args.two_phase_steps)
     out["config_2d"] = run_config_2d()
     out["projection"] = run_projection(cpu=rank == 0 and world == 1 and not args.skip_cpu)
     if not args.skip_serving and world == 1:
@@ -1096,6 +1155,9 @@ def main():
     ap.add_argument("--skip-c3", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-serving", action="store_true")
+    ap.add_argument("--skip-two-phase", action="store_true")
+    ap.add_argument("--two-phase-steps", type=int, default=TWO_PHASE_STEPS)
+    ap.add_argument("--two-phase-only", action="store_true", help="run only the two-phase time-step loop")
     ap.add_argument("--serving-only", action="store_true", help="run only the served stream; print its record")
     ap.add_argument("--serve-slots", type=int, default=SERVE_SLOTS, help="concurrent solves of the served stream")
     ap.add_argument("--cpu-sample", type=int, default=None, help=argparse.SUPPRESS)
@@ -1112,6 +1174,8 @@ def main():
         run_profile(args)
     elif args.serving_only:
         print(json.dumps({"serving": run_serving(slots=args.serve_slots)}))
+    elif args.two_phase_only:
+        print(json.dumps({"two_phase_step": run_two_phase(args.two_phase_steps)}))
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -428,6 +428,66 @@ int sipg_ins_pressure_neumann(sipg_mesh *m, int order, double reynolds, const do
 int sipg_ins_pressure_neumann_host(sipg_mesh *m, int order, double reynolds, const double *vel, const double *N,
                                    const double *mu, const double *rho, const int *vel_bc, double *dPdN);
 
+/* ---- two-phase time step: replaces MPINSSolver3D (src/solvers/3d/mp_ins_solver.cpp:
+ * 182-285: init, step = advection, pressure, viscosity, surface) with its level set
+ * (LevelSetSolver3D, src/solvers/3d/ls_solver.cpp:106-257) for problems with no-slip
+ * walls and natural outflow, no surface tension, sub-cycling, filtering or shock
+ * capturing. Every field stays on the device; a step runs
+ *   advection     sipg_ins_advection's kernel, plus the body force;
+ *   pressure      Neumann data (sipg_ins_pressure_neumann), right-hand side
+ *                 (sipg_pressure_rhs), factor 1/rho, p-multigrid set-up and solve from
+ *                 the extrapolated initial guess, sipg_pressure_projection;
+ *   viscosity     sipg_viscous_rhs, factor mu and mass factor g0 Re rho / dt, set-up and
+ *                 three Jacobi-PCG solves (FactorMMPoissonMatrixFreeDiag3D +
+ *                 PETScJacobiSolver) with zero Dirichlet data on no-slip walls;
+ *   surface       the level-set advection (three Runge-Kutta stages), then rho and mu;
+ * then dt = cfl h / ((p+1)^2 max(1, max |u|)) (INSSolverBase3D::max_vel) and the second-
+ * order coefficients (a0, a1, b0, b1, g0) = (2, -0.5, 2, -1, 1.5) after the first step.
+ * The level-set reinitialisation (LevelSetSolver3D::reinitLS) is not part of it. */
+typedef struct {
+  int order;                 /* DG order */
+  double reynolds;           /* r_ynolds */
+  double rho0, rho1;         /* density where s > 0 and where s < 0 (fluid-constants) */
+  double mu0, mu1;           /* viscosity likewise */
+  double gravity;            /* body force -gravity along y; 0: none, as the reference's 3D
+                                solver (the 2D solver's gravity adds it to N_y,
+                                ins_advec_intermediate_vel_grav_2d.h; here also to the
+                                pressure Neumann data) */
+  double ls_alpha;           /* interface half-width alpha in units of the largest element
+                                size (level-set-options alpha, default 24) */
+  double cfl;                /* multiplies the reference's time step (1) */
+  int precision;             /* pressure p-multigrid preconditioner: SIPG_FP64 or SIPG_FP32 */
+  int extrapolate_history;   /* pressure initial guess from this many past solutions (3);
+                                0: the previous pressure */
+  double pr_rel_tol, pr_abs_tol;
+  int pr_max_iter;
+  double vis_rel_tol, vis_abs_tol;
+  int vis_max_iter;
+} sipg_ins3d_opts;
+
+typedef struct {
+  double time, dt;           /* after the step: the time reached and the next dt */
+  int pr_iters, vis_iters[3];
+  double pr_rel_res, vis_rel_res[3];
+  double max_vel;            /* max(1, max |u|) after the step */
+  double ms_advection, ms_pressure, ms_viscosity, ms_surface; /* device time per part */
+  unsigned long long proj_converged; /* elements whose velocity projection converged */
+} sipg_ins3d_step_info;
+
+typedef struct sipg_ins3d sipg_ins3d;
+int sipg_ins3d_default_opts(sipg_ins3d_opts *o);
+/* vel_bc: Kb velocity boundary types (0 no-slip, 2 natural outflow). */
+int sipg_ins3d_create(sipg_mesh *m, const sipg_ins3d_opts *o, const int *vel_bc, sipg_ins3d **out);
+/* Initial velocity (3 x K x Np) and level set (K x Np), host arrays: the reference's
+ * ps3d_set_ic / ps3d_set_surface callbacks evaluated by the caller. Sets time 0, the
+ * first-order coefficients, rho and mu, and the first dt. */
+int sipg_ins3d_set_state_host(sipg_ins3d *ins, const double *vel, const double *s);
+/* nsteps steps; info (may be NULL) describes the last one. */
+int sipg_ins3d_step(sipg_ins3d *ins, int nsteps, sipg_ins3d_step_info *info);
+/* Copies of the current fields (NULL: skipped): vel 3 x K x Np, pr, s, rho, mu K x Np. */
+int sipg_ins3d_get_state_host(sipg_ins3d *ins, double *vel, double *pr, double *s, double *rho, double *mu);
+void sipg_ins3d_destroy(sipg_ins3d *ins);
+
 /* Number of kernels this library has launched so far in the process
  * (diagnostics for benchmarks; no reference counterpart). */
 int sipg_launch_count(unsigned long long *n);

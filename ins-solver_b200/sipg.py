@@ -253,6 +253,70 @@ def ins_pressure_neumann(mesh, order, reynolds, vel, N, mu, rho, vel_bc):
     return out
 
 
+class Ins3DOpts(C.Structure):
+    """sipg_ins3d_opts: the MPINSSolver3D configuration of the two-phase time step."""
+    _fields_ = [("order", C.c_int), ("reynolds", C.c_double), ("rho0", C.c_double), ("rho1", C.c_double),
+                ("mu0", C.c_double), ("mu1", C.c_double), ("gravity", C.c_double), ("ls_alpha", C.c_double),
+                ("cfl", C.c_double), ("precision", C.c_int), ("extrapolate_history", C.c_int),
+                ("pr_rel_tol", C.c_double), ("pr_abs_tol", C.c_double), ("pr_max_iter", C.c_int),
+                ("vis_rel_tol", C.c_double), ("vis_abs_tol", C.c_double), ("vis_max_iter", C.c_int)]
+
+
+class Ins3DStepInfo(C.Structure):
+    _fields_ = [("time", C.c_double), ("dt", C.c_double), ("pr_iters", C.c_int), ("vis_iters", C.c_int * 3),
+                ("pr_rel_res", C.c_double), ("vis_rel_res", C.c_double * 3), ("max_vel", C.c_double),
+                ("ms_advection", C.c_double), ("ms_pressure", C.c_double), ("ms_viscosity", C.c_double),
+                ("ms_surface", C.c_double), ("proj_converged", C.c_ulonglong)]
+
+
+def ins3d_default_opts(**kw):
+    o = Ins3DOpts()
+    check(lib().sipg_ins3d_default_opts(C.byref(o)))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+class Ins3D:
+    """Two-phase 3D time step on the device (sipg_ins3d_*): MPINSSolver3D's init /
+    step / field access with its level set, no-slip walls and natural outflow."""
+
+    def __init__(self, mesh, vel_bc, opts=None, **kw):
+        self.mesh = mesh
+        self.o = opts if opts is not None else ins3d_default_opts(**kw)
+        self.Np = ref_sizes(3, self.o.order)[0]
+        bc = np.ascontiguousarray(vel_bc, dtype=np.int32).reshape(-1)
+        self.h = C.c_void_p()
+        check(lib().sipg_ins3d_create(mesh.h, C.byref(self.o), _ip(bc), C.byref(self.h)))
+
+    def set_state(self, vel, s):
+        v = np.ascontiguousarray(vel, dtype=np.float64)
+        q = np.ascontiguousarray(s, dtype=np.float64)
+        check(lib().sipg_ins3d_set_state_host(self.h, _dp(v), _dp(q)))
+
+    def step(self, nsteps=1):
+        info = Ins3DStepInfo()
+        check(lib().sipg_ins3d_step(self.h, nsteps, C.byref(info)))
+        return info
+
+    def state(self):
+        K, Np = self.mesh.K, self.Np
+        vel, pr, s, rho, mu = np.zeros((3, K, Np)), *(np.zeros((K, Np)) for _ in range(4))
+        check(lib().sipg_ins3d_get_state_host(self.h, _dp(vel), _dp(pr), _dp(s), _dp(rho), _dp(mu)))
+        return dict(vel=vel, pr=pr, s=s, rho=rho, mu=mu)
+
+    def close(self):
+        if self.h:
+            lib().sipg_ins3d_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def projection_factor(dim, dt):
     """The penalty factor INSSolverBase{3D,2D}::project_velocity passes to the
     element-local solve: dt in 3D (src/solvers/3d/ins_solver_base.cpp:1082),

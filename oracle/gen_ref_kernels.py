@@ -31,6 +31,7 @@ KERNELS_3D = [
     "ins_3d_proj_rhs", "ins_3d_proj_pen", "ins_3d_proj_cg_precon", "ins_proj_setup_0", "ins_proj_setup_1",
     "ins_3d_pr_1", "mp_ins_3d_pr_2", "mp_ins_pr_bc_dpdn_factors", "mp_ins_pr_div_factor", "mp_ins_3d_vis_0",
     "ins_3d_advec_0", "ins_3d_advec_1", "ins_3d_advec_2", "ins_3d_advec_3", "mp_ins_3d_pr_mu", "mp_ins_3d_pr_0",
+    "advec_3d_0", "advec_3d_flux", "ls_advec_3d_bc", "runge_kutta_0", "runge_kutta_1", "ls_step",
 ]
 KERNELS_2D = [
     "fvmf_2d_grad", "fvmf_2d_calc_tau_faces", "fvmf_2d_calc_tau_bfaces", "vmf_2d_mult_avg_jump",

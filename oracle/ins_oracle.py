@@ -2,8 +2,20 @@
 solves, restated in numpy. TEST INFRASTRUCTURE ONLY (tests/, the CPU legs of
 the benchmark).
 
+ls_advect / ls_props: the level-set step of LevelSetSolver3D::step and getRhoMu
+(src/solvers/3d/ls_solver.cpp:192-200, 243-257): AdvectionSolver3D::step's three
+Runge-Kutta stages (src/solvers/3d/advection_solver.cpp:24-72, runge_kutta_0/1) of
+rhs = div_weak(u q) - LIFT(flux) (advection_solver.cpp:84-120: advec_3d_0,
+mesh->div_weak of OP2-DG-Toolkit, unvendored, restated as M^-1 D_r^T M, the upwind
+advec_3d_flux and ls_advec_3d_bc), then ls_step's smoothed Heaviside.
+
 pressure_neumann: the curl-curl Neumann data of the multiphase pressure step,
 MPINSSolver3D::apply_pressure_neumann_bc (src/solvers/3d/mp_ins_solver.cpp:450-493).
+
+TwoPhaseStep: MPINSSolver3D::step (src/solvers/3d/mp_ins_solver.cpp:245-285) composed
+of the pieces above, the oracle's pressure right-hand side, gradient, velocity
+projection and conjugate-gradient solves (oracle/oracle_py.py) run to a tight
+tolerance, and the level-set step.
 
 advection: INSSolverBase3D::advec_current_non_linear and advec_standard
 (src/solvers/3d/ins_solver_base.cpp:224-329, 451-480): the flux tensor
@@ -20,6 +32,7 @@ the restatement keeps that.
 import numpy as np
 
 import dg_oracle as D
+import oracle_py as O
 
 BC_NO_SLIP, BC_SLIP, BC_OUTFLOW = 0, 1, 2
 
@@ -100,7 +113,7 @@ def curl(mesh, t, u):
     return np.stack([g[2][1] - g[1][2], g[0][2] - g[2][0], g[1][0] - g[0][1]])
 
 
-def pressure_neumann(mesh, p, u, N, mu, rho, vel_bc, reynolds):
+def pressure_neumann(mesh, p, u, N, mu, rho, vel_bc, reynolds, grav=0.0):
     """dPdN (K, Nf, Nfp) of MPINSSolver3D::apply_pressure_neumann_bc
     (src/solvers/3d/mp_ins_solver.cpp:450-493): curl(mu curl u) (mesh->curl,
     mp_ins_3d_pr_mu, mesh->curl), then on no-slip and slip walls (mp_ins_3d_pr_0)
@@ -118,13 +131,169 @@ def pressure_neumann(mesh, p, u, N, mu, rho, vel_bc, reynolds):
             if nb >= 0 or bct[-nb - 1] not in (BC_NO_SLIP, BC_SLIP):
                 continue
             m = t["fmask"][f]
-            res = -N[:, e, m] - c2[:, e, m] / (reynolds * rho[e, m])
+            res = -(N[:, e, m] + _gravity(grav)[:, None]) - c2[:, e, m] / (reynolds * rho[e, m])
             out[e, f] = mesh.fscale[e, f] * (nrm[e, f] @ res)
     return out
 
 
-def advection(mesh, p, dt, a0, a1, b0, b1, u, u_old, N_old, vel_bc):
-    """(N, velT) of one advection step."""
+def _gravity(grav):
+    """The body force -grav along y as the term added to N (the 2D solver's
+    ins_advec_intermediate_vel_grav_2d.h adds 1 / Fr^2 to N_y)."""
+    return np.array([0.0, grav, 0.0])
+
+
+def advection(mesh, p, dt, a0, a1, b0, b1, u, u_old, N_old, vel_bc, grav=0.0):
+    """(N, velT) of one advection step; grav: body force -grav along y, added to
+    N_y in the extrapolation only."""
     N = nonlinear(mesh, p, u, vel_bc)
-    velT = (a0 * u + a1 * u_old) - dt * (b0 * N + b1 * N_old)
+    G = _gravity(grav)[:, None, None]
+    velT = (a0 * u + a1 * u_old) - dt * (b0 * (N + G) + b1 * (N_old + G))
     return N, velT
+
+
+def weak_divergence(mesh, t, F):
+    """mesh->div_weak (OP2-DG-Toolkit, unvendored, restated): the weak-form
+    divergence M^-1 int grad(phi) . F of F (3, K, Np), i.e. sum_d sum_r dr/dx_d
+    Dw_r F_d with the weak derivatives Dw_r = M^-1 D_r^T M."""
+    Minv = np.linalg.inv(t["M"])
+    out = np.zeros(F.shape[1:])
+    for r, Dm in enumerate([t["Dr"], t["Ds"], t["Dt"]]):
+        Dw = Minv @ Dm.T @ t["M"]
+        for d in range(3):
+            out += mesh.G[:, r, d][:, None] * (F[d] @ Dw.T)
+    return out
+
+
+def ls_face_flux(mesh, t, q, u, vel_bc):
+    """(K, Nf, Nfp): advec_3d_flux on interior faces (upwind on the element's own
+    normal velocity) and ls_advec_3d_bc on no-slip, slip and outflow faces."""
+    K, Nf = mesh.K, t["Nf"]
+    fm, pp = t["fmask"], t["perm_pos"]
+    nrm = np.stack([mesh.nx, mesh.ny, mesh.nz], 2)
+    out = np.zeros((K, Nf, t["Nfp"]))
+    bct = np.asarray(vel_bc).reshape(-1)
+    for e in range(K):
+        for f in range(Nf):
+            m = fm[f]
+            un = nrm[e, f] @ u[:, e, m]
+            qM = q[e, m]
+            nb = mesh.nbr[e, f]
+            if nb >= 0:
+                qP = q[nb, fm[mesh.nbr_face[e, f]][pp[mesh.nbr_perm[e, f]]]]
+                out[e, f] = mesh.fscale[e, f] * (un * 0.5 * (qM + qP) + 0.5 * np.abs(un) * (qM - qP))
+            else:
+                assert bct[-nb - 1] in (BC_NO_SLIP, BC_SLIP, BC_OUTFLOW)
+                out[e, f] = mesh.fscale[e, f] * un * qM
+    return out
+
+
+def ls_rhs(mesh, p, q, u, vel_bc):
+    """div_weak(u q) - LIFT(flux), (K, Np)."""
+    t = _tables(p)
+    out = weak_divergence(mesh, t, u * q[None])
+    return out - ls_face_flux(mesh, t, q, u, vel_bc).reshape(mesh.K, -1) @ t["LIFT"].T
+
+
+def ls_advect(mesh, p, dt, s, u, vel_bc):
+    """One AdvectionSolver3D::step: the stages of runge_kutta_0 / runge_kutta_1, the
+    second stage point being s + 0.5 dt (rk0 / 4 + rk1 / 4) as the reference has it."""
+    rk0 = ls_rhs(mesh, p, s, u, vel_bc)
+    rk1 = ls_rhs(mesh, p, s + dt * rk0, u, vel_bc)
+    rk2 = ls_rhs(mesh, p, s + 0.5 * dt * (rk0 / 4.0 + rk1 / 4.0), u, vel_bc)
+    return s + dt * (rk0 / 6.0 + rk1 / 6.0 + 2.0 * rk2 / 3.0)
+
+
+def ls_props(s, alpha, rho0, rho1, mu0, mu1):
+    """ls_step: rho, mu from the smoothed Heaviside tanh(pi s / alpha)."""
+    step = np.tanh(np.pi * s / alpha)
+    return 0.5 * rho0 * (1 + step) + 0.5 * rho1 * (1 - step), 0.5 * mu0 * (1 + step) + 0.5 * mu1 * (1 - step)
+
+
+def lagrange_extrapolate(times, fields, t):
+    """The initial guess through the pressure history (initial_guess_extrapolation)."""
+    out = np.zeros_like(fields[0])
+    for i, (ti, fi) in enumerate(zip(times, fields)):
+        w = 1.0
+        for j, tj in enumerate(times):
+            if j != i:
+                w *= (t - tj) / (ti - tj)
+        out += w * fi
+    return out
+
+
+class TwoPhaseStep:
+    """MPINSSolver3D::step on host arrays: advection (+ body force), pressure
+    (Neumann data, right-hand side, solve with factor 1/rho, gradient / rho and the
+    velocity projection), viscosity (right-hand side, three Helmholtz solves with
+    factor mu and mass factor g0 Re rho / dt, zero Dirichlet data on no-slip
+    walls), the level-set step, then the time-step update. Solves run to rel_tol."""
+
+    def __init__(self, mesh, p, vel_bc, reynolds, rho0, rho1, mu0, mu1, gravity=0.0, ls_alpha=24.0, cfl=1.0,
+                 history=3, rel_tol=1e-11):
+        self.mesh, self.p = mesh, p
+        self.t = D.ref_tables(3, p)
+        self.om = O.OMesh(self.t, mesh.export(p, self.t))
+        self.vel_bc = np.asarray(vel_bc, np.int32).reshape(-1)
+        assert np.all((self.vel_bc == BC_NO_SLIP) | (self.vel_bc == BC_OUTFLOW))
+        self.pr_bct = np.where(self.vel_bc == BC_NO_SLIP, 1, 0).astype(np.int32)  # Neumann / Dirichlet
+        self.vis_bct = np.where(self.vel_bc == BC_NO_SLIP, 0, 1).astype(np.int32)
+        self.nullspace = int(np.all(self.pr_bct == 1))
+        self.re, self.rho0, self.rho1, self.mu0, self.mu1 = reynolds, rho0, rho1, mu0, mu1
+        self.grav, self.cfl, self.history, self.rel_tol = gravity, cfl, history, rel_tol
+        fs = mesh.fscale[mesh.nbr >= 0]
+        self.h = 1.0 / fs.max()
+        self.alpha = ls_alpha / fs.min()
+
+    def _props(self):
+        self.rho, self.mu = ls_props(self.s, self.alpha, self.rho0, self.rho1, self.mu0, self.mu1)
+
+    def _next_dt(self):
+        self.max_vel = max(1.0, float(np.sqrt(np.max(np.sum(self.vel ** 2, axis=0)))))
+        self.dt = self.cfl * self.h / ((self.p + 1) ** 2 * self.max_vel)
+
+    def set_state(self, vel, s):
+        self.vel = np.array(vel, dtype=np.float64)
+        self.vel_old = self.vel.copy()
+        self.s = np.array(s, dtype=np.float64)
+        K, Np, Nfp = self.mesh.K, self.t["Np"], self.t["Nfp"]
+        self.N_old = np.zeros((3, K, Np))
+        self.dPdN_old = np.zeros((K, 4, Nfp))
+        self.pr = np.zeros((K, Np))
+        self.hist = []
+        self.time = 0.0
+        self.a0, self.a1, self.b0, self.b1, self.g0 = 1.0, 0.0, 1.0, 0.0, 1.0
+        self._props()
+        self._next_dt()
+
+    def _solve(self, b, bct, x0, **kw):
+        x, info = O.solve(self.om, b[None], bct, precond=O.PRE_JACOBI, rel_tol=self.rel_tol, abs_tol=1e-300,
+                          max_iter=20000, x0=x0[None], **kw)
+        return x[0], info
+
+    def step(self):
+        m, p, dt = self.mesh, self.p, self.dt
+        N, velT = advection(m, p, dt, self.a0, self.a1, self.b0, self.b1, self.vel, self.vel_old, self.N_old,
+                            self.vel_bc, self.grav)
+        dPdN = pressure_neumann(m, p, self.vel, N, self.mu, self.rho, self.vel_bc, self.re, self.grav)
+        rhs, _ = O.pressure_rhs(self.om, dt, velT, dPdN, self.dPdN_old, self.b0, self.b1)
+        if self.history and self.hist:
+            x0 = lagrange_extrapolate([h[0] for h in self.hist], [h[1] for h in self.hist], self.time + dt)
+        else:
+            x0 = self.pr
+        self.pr, self.pr_info = self._solve(rhs, self.pr_bct, x0, factor=1.0 / self.rho, nullspace=self.nullspace)
+        if self.history:
+            self.hist = (self.hist + [(self.time + dt, self.pr.copy())])[-self.history:]
+        dp = O.grad_central(self.om, self.pr) / self.rho[None]
+        velTT, _ = O.project_velocity(self.om, dt, dt, dp, velT)
+        M, J = self.t["M"], m.J
+        mmf = self.g0 * self.re / dt * self.rho
+        vel_new = np.zeros_like(self.vel)
+        for c in range(3):
+            b = J[:, None] * ((self.re / dt * self.rho * velTT[c]) @ M.T)
+            vel_new[c], _ = self._solve(b, self.vis_bct, self.vel_old[c], factor=self.mu, mm=mmf)
+        self.s = ls_advect(m, p, dt, self.s, vel_new, self.vel_bc)
+        self._props()
+        self.vel_old, self.vel, self.N_old, self.dPdN_old = self.vel, vel_new, N, dPdN
+        self.time += dt
+        self.a0, self.a1, self.b0, self.b1, self.g0 = 2.0, -0.5, 2.0, -1.0, 1.5
+        self._next_dt()

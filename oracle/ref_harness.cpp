@@ -107,6 +107,13 @@ void ref_set_reynolds(double re) {
   d2p1::r_ynolds = d2p2::r_ynolds = d2p3::r_ynolds = d2p4::r_ynolds = re;
   d3p1::r_ynolds = d3p2::r_ynolds = d3p3::r_ynolds = d3p4::r_ynolds = re;
 }
+// The fluid constants of ls_step, every 3D build.
+void ref_set_fluid(double r0, double r1, double m0, double m1) {
+  d3p1::rho0 = d3p2::rho0 = d3p3::rho0 = d3p4::rho0 = r0;
+  d3p1::rho1 = d3p2::rho1 = d3p3::rho1 = d3p4::rho1 = r1;
+  d3p1::mu0 = d3p2::mu0 = d3p3::mu0 = d3p4::mu0 = m0;
+  d3p1::mu1 = d3p2::mu1 = d3p3::mu1 = d3p4::mu1 = m1;
+}
 int ref_mult(const oracle_mesh *m, int ncomp, const int *bc_types, const double *factor,
              const double *mm_factor, double mm_scalar, int flags, const double *const *x,
              double *const *y) {

@@ -1,0 +1,77 @@
+"""The two-phase time step on the device (sipg_ins3d_*) against the composed
+oracle step (oracle/ins_oracle.py TwoPhaseStep, whose pieces are pinned against the
+reference's kernels in tests/test_ins_oracle.py and tests/test_projection.py), and
+the mixed-precision pressure solve against the FP64 one."""
+import numpy as np
+import pytest
+
+import dg_oracle as D
+import ins_oracle as I
+import sipg
+from helpers import rel_err
+
+pytestmark = pytest.mark.gpu
+
+CONSTS = dict(reynolds=100.0, rho0=1.0, rho1=1e-3, mu0=1.0, mu1=1e-2, gravity=9.81, ls_alpha=2.0)
+
+
+def _case(n, p, open_top):
+    gm = sipg.Mesh.box(3, n, jitter=0.1, seed=5)
+    om = D.Mesh.box(3, n, 0.1, 5)
+    t = D.ref_tables(3, p)
+    e = om.export(p, t)
+    s = np.sqrt((e["x"] - 0.5) ** 2 + (e["y"] - 0.3) ** 2 + (e["z"] - 0.5) ** 2) - 0.25
+    # a smooth start that vanishes on the walls, so that advection has work to do
+    w = 0.3 * np.sin(np.pi * e["x"]) * np.sin(np.pi * e["y"]) * np.sin(np.pi * e["z"])
+    vel = np.stack([w, -0.5 * w, 0.25 * w])
+    vel_bc = np.zeros(om.Kb, np.int32)
+    if open_top:
+        vel_bc[om.bface_centroid[:, 1] > 1.0 - 1e-9] = I.BC_OUTFLOW
+    return gm, om, s, vel, vel_bc
+
+
+def _mean_free(p):
+    return p - p.mean()
+
+
+@pytest.mark.parametrize("p", [2, 3])
+@pytest.mark.parametrize("open_top", [False, True], ids=["closed", "open-top"])
+def test_two_phase_steps_match_the_oracle(p, open_top):
+    gm, om, s, vel, vel_bc = _case(3, p, open_top)
+    tol = dict(pr_rel_tol=1e-11, pr_abs_tol=1e-300, vis_rel_tol=1e-11, vis_abs_tol=1e-300)
+    ins = sipg.Ins3D(gm, vel_bc, order=p, precision=sipg.FP64, **tol, **CONSTS)
+    ins.set_state(vel, s)
+    ref = I.TwoPhaseStep(om, p, vel_bc, **CONSTS)
+    ref.set_state(vel, s)
+    for k in range(3):
+        info = ins.step()
+        ref.step()
+        assert info.proj_converged == gm.K
+        assert info.time == pytest.approx(ref.time, rel=1e-12)
+        assert info.dt == pytest.approx(ref.dt, rel=1e-9)
+    got = ins.state()
+    # solves stop at 1e-11 relative residual on both sides
+    assert rel_err(got["vel"], ref.vel) < 1e-7
+    assert rel_err(got["s"], ref.s) < 1e-9
+    pg, pw = (got["pr"], ref.pr) if open_top else (_mean_free(got["pr"]), _mean_free(ref.pr))
+    assert rel_err(pg, pw) < 1e-7
+    assert rel_err(got["rho"], ref.rho) < 1e-9 and rel_err(got["mu"], ref.mu) < 1e-9
+
+
+def test_mixed_pressure_preconditioner_steps_match_fp64():
+    """The time step with the FP32 p-multigrid V-cycle inside the FP64 outer Krylov
+    solve against the all-FP64 one, both at the reference's tolerances."""
+    gm, _, s, vel, vel_bc = _case(4, 3, False)
+    runs = {}
+    for prec in (sipg.FP64, sipg.FP32):
+        ins = sipg.Ins3D(gm, vel_bc, order=3, precision=prec, **CONSTS)
+        ins.set_state(vel, s)
+        infos = [ins.step() for _ in range(4)]
+        runs[prec] = (ins.state(), infos)
+    a, b = runs[sipg.FP64][0], runs[sipg.FP32][0]
+    assert rel_err(b["vel"], a["vel"]) < 1e-5
+    assert rel_err(b["s"], a["s"]) < 1e-7
+    for i64, i32 in zip(runs[sipg.FP64][1], runs[sipg.FP32][1]):
+        assert abs(i64.pr_iters - i32.pr_iters) <= 2
+    # the light bubble rises
+    assert a["vel"][1][s < 0].mean() > 0
