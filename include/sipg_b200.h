@@ -456,13 +456,21 @@ typedef struct {
   double ls_alpha;           /* interface half-width alpha in units of the largest element
                                 size (level-set-options alpha, default 24) */
   double cfl;                /* multiplies the reference's time step (1) */
-  int precision;             /* pressure p-multigrid preconditioner: SIPG_FP64 or SIPG_FP32 */
   int extrapolate_history;   /* pressure initial guess from this many past solutions (3);
                                 0: the previous pressure */
-  double pr_rel_tol, pr_abs_tol;
-  int pr_max_iter;
-  double vis_rel_tol, vis_abs_tol;
-  int vis_max_iter;
+  int pr_over_int;           /* [pressure-solve] over_int: 1/rho at the cubature points of the
+                                over-integrated operator (update_pressure_matrices_oi,
+                                mp_ins_solver.cpp:524-544), the V-cycle on its nodal
+                                projection; 0: the nodal factor 1/rho. The pressure gradient
+                                of the projection step is the nodal one either way. */
+  /* The pressure p-multigrid (SIPG_SOLVER_PMULTIGRID: precision of the V-cycle,
+   * tolerances, [p-multigrid] keys; n_levels 0 = orders p, p-1, ..., 1; nullspace is
+   * set from the boundary types) and the viscous Jacobi-PCG options. Defaults: the
+   * tolerances of setup_pressure_viscous_solvers (ins_solver_base.cpp:149-184) and
+   * eigen_val_saftey_factor 2.5 of the reference's 3D two-phase examples
+   * (examples/3d/oscillating_droplet/config.ini:30). */
+  sipg_solver_opts pressure;
+  sipg_solver_opts viscous;
 } sipg_ins3d_opts;
 
 typedef struct {
@@ -471,6 +479,9 @@ typedef struct {
   double pr_rel_res, vis_rel_res[3];
   double max_vel;            /* max(1, max |u|) after the step */
   double ms_advection, ms_pressure, ms_viscosity, ms_surface; /* device time per part */
+  double ms_pressure_setup;  /* of ms_pressure: new factor (and over-integrated blocks) and the
+                                p-multigrid set-up */
+  double ms_pressure_solve;  /* of ms_pressure: the solve */
   unsigned long long proj_converged; /* elements whose velocity projection converged */
 } sipg_ins3d_step_info;
 

@@ -8,7 +8,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <vector>
@@ -24,6 +26,16 @@ namespace {
 
 void ok(int status, const char* what) {
   if (status != SIPG_OK) throw Error(status, std::string(what) + ": " + sipg_last_error());
+}
+
+// A linear solve that stops short is an error of the step, as the reference's
+// dg_abort("Pressure solve failed to converge") is.
+void solved(int status, const char* what, const sipg_solve_info& i) {
+  if (status == SIPG_OK) return;
+  char buf[160];
+  std::snprintf(buf, sizeof(buf), "%s: status %d after %d iterations, relative residual %.3e", what, status, i.iters,
+                i.rel_res);
+  throw Error(status, buf);
 }
 
 struct Timer {
@@ -146,12 +158,18 @@ struct sipg_ins3d {
     ok(sipg_pressure_rhs(m, o.order, dt, b0, b1, velT.as<double>(), dPdN[cur].as<double>(), dPdN[nw].as<double>(),
                          rhs.as<double>(), st),
        "pressure right-hand side");
-    set_factor_device(pop, rrho.as<double>(), st);
+    SIPG_CUDA(cudaStreamSynchronize(st));
+    const auto c0 = std::chrono::steady_clock::now();
+    if (o.pr_over_int)
+      set_factor_oi_level_set(pop, s.as<double>(), alpha, o.rho0, o.rho1, st);
+    else
+      set_factor_device(pop, rrho.as<double>(), st);
     pressure_guess();
     SIPG_CUDA(cudaStreamSynchronize(st));
     ok(sipg_solver_setup(psol), "pressure set-up");
+    const auto c1 = std::chrono::steady_clock::now();
     sipg_solve_info pi{};
-    ok(sipg_solver_solve(psol, rhs.as<double>(), pr.as<double>(), &pi), "pressure solve");
+    solved(sipg_solver_solve(psol, rhs.as<double>(), pr.as<double>(), &pi), "pressure solve", pi);
     add_history();
     ok(sipg_pressure_projection(m, o.order, dt, dt, pr.as<double>(), rho.as<double>(), velT.as<double>(),
                                 velTT.as<double>(), stats.as<unsigned long long>(), st),
@@ -168,7 +186,7 @@ struct sipg_ins3d {
     ok(sipg_solver_setup(vsol), "viscous set-up");
     sipg_solve_info vi[3]{};
     for (int c = 0; c < 3; ++c)
-      ok(sipg_solver_solve(vsol, rhs.as<double>() + c * n, u_new + c * n, &vi[c]), "viscous solve");
+      solved(sipg_solver_solve(vsol, rhs.as<double>() + c * n, u_new + c * n, &vi[c]), "viscous solve", vi[c]);
     SIPG_CUDA(cudaEventRecord(t_vis.b, st));
     // surface (level set, then rho and mu)
     SIPG_CUDA(cudaEventRecord(t_surf.a, st));
@@ -206,6 +224,8 @@ struct sipg_ins3d {
       SIPG_CUDA(cudaEventElapsedTime(&ms, t_surf.a, t_surf.b));
       info->ms_surface = ms;
       info->proj_converged = cs[0];
+      info->ms_pressure_setup = std::chrono::duration<double, std::milli>(c1 - c0).count();
+      info->ms_pressure_solve = pi.solve_ms;
     }
   }
 };
@@ -221,15 +241,18 @@ int sipg_ins3d_default_opts(sipg_ins3d_opts* o) {
     o->rho0 = o->rho1 = o->mu0 = o->mu1 = 1.0;
     o->ls_alpha = 24.0;  // level-set-options alpha (ls_solver.cpp:137)
     o->cfl = 1.0;
-    o->precision = SIPG_FP64;
     o->extrapolate_history = 3;
     // setup_pressure_viscous_solvers (ins_solver_base.cpp:149-184)
-    o->pr_rel_tol = 1e-8;
-    o->pr_abs_tol = 1e-9;
-    o->pr_max_iter = 500;
-    o->vis_rel_tol = 1e-8;
-    o->vis_abs_tol = 1e-9;
-    o->vis_max_iter = 5000;
+    ok(sipg_solver_default_opts(SIPG_SOLVER_PMULTIGRID, &o->pressure), "pressure options");
+    o->pressure.rel_tol = 1e-8;
+    o->pressure.abs_tol = 1e-9;
+    o->pressure.max_iter = 500;
+    o->pressure.n_levels = 0;
+    o->pressure.eig_safety = 2.5;
+    ok(sipg_solver_default_opts(SIPG_SOLVER_JACOBI, &o->viscous), "viscous options");
+    o->viscous.rel_tol = 1e-8;
+    o->viscous.abs_tol = 1e-9;
+    o->viscous.max_iter = 5000;
   });
 }
 
@@ -241,7 +264,6 @@ int sipg_ins3d_create(sipg_mesh* m, const sipg_ins3d_opts* o, const int* vel_bc,
     if (!(o->reynolds > 0.0) || !(o->rho0 > 0.0) || !(o->rho1 > 0.0) || !(o->mu0 > 0.0) || !(o->mu1 > 0.0) ||
         !(o->ls_alpha > 0.0) || !(o->cfl > 0.0))
       throw Error(SIPG_INVALID_ARG, "ins3d constants must be positive");
-    if (o->precision != SIPG_FP64 && o->precision != SIPG_FP32) throw Error(SIPG_INVALID_ARG, "precision");
     if (o->extrapolate_history < 0 || o->extrapolate_history > 8)
       throw Error(SIPG_INVALID_ARG, "extrapolate_history must be 0..8");
     bool dirichlet_pr = false;
@@ -298,22 +320,17 @@ int sipg_ins3d_create(sipg_mesh* m, const sipg_ins3d_opts* o, const int* vel_bc,
     // pressure: FactorPoissonMatrixFreeDiag3D + PETScPMultigrid, nullspace without Dirichlet faces
     ok(sipg_op_create(m, o->order, 1, &ins->pop), "pressure operator");
     ok(sipg_op_set_bc_types(ins->pop, prt.data()), "pressure boundary types");
-    sipg_solver_opts po;
-    ok(sipg_solver_default_opts(SIPG_SOLVER_PMULTIGRID, &po), "pressure options");
-    po.rel_tol = o->pr_rel_tol;
-    po.abs_tol = o->pr_abs_tol;
-    po.max_iter = o->pr_max_iter;
-    po.precision = o->precision;
+    sipg_solver_opts po = o->pressure;
     po.nullspace = dirichlet_pr ? 0 : 1;
+    if (po.n_levels == 0) {  // p-multigrid orders p, p-1, ..., 1 (the [p-multigrid] orders key)
+      po.n_levels = o->order;
+      for (int l = 0; l < 4; ++l) po.orders[l] = l < o->order ? o->order - l : 0;
+    }
     ok(sipg_solver_create(ins->pop, SIPG_SOLVER_PMULTIGRID, &po, &ins->psol), "pressure solver");
     // viscosity: FactorMMPoissonMatrixFreeDiag3D + PETScJacobiSolver, one component at a time
     ok(sipg_op_create(m, o->order, 1, &ins->vop), "viscous operator");
     ok(sipg_op_set_bc_types(ins->vop, vst.data()), "viscous boundary types");
-    sipg_solver_opts vo;
-    ok(sipg_solver_default_opts(SIPG_SOLVER_JACOBI, &vo), "viscous options");
-    vo.rel_tol = o->vis_rel_tol;
-    vo.abs_tol = o->vis_abs_tol;
-    vo.max_iter = o->vis_max_iter;
+    sipg_solver_opts vo = o->viscous;
     ok(sipg_solver_create(ins->vop, SIPG_SOLVER_JACOBI, &vo, &ins->vsol), "viscous solver");
     *out = ins.release();
   });

@@ -24,7 +24,7 @@ namespace sipg {
 
 struct OiDev {
   OiTables t;
-  DevBuf vdphi, wq, ws, fphi, fdphi, xphi, xdphi, yphi, proj, mass;
+  DevBuf vphi, vdphi, wq, ws, fphi, fdphi, xphi, xdphi, yphi, proj, mass;
 };
 
 namespace {
@@ -43,6 +43,7 @@ const OiDev& oi_dev(int dim, int order) {
     b = DevBuf(std::max<size_t>(1, v.size()) * sizeof(double));
     if (!v.empty()) b.upload(v.data(), v.size() * sizeof(double));
   };
+  up(d->vphi, d->t.vphi);
   up(d->vdphi, d->t.vdphi);
   up(d->wq, d->t.wq);
   up(d->ws, d->t.ws);
@@ -294,6 +295,51 @@ void oi_sizes(int dim, int order, int* nq, int* nqs) {
   const OiDev& d = oi_dev(dim, order);
   if (nq) *nq = d.t.nq;
   if (nqs) *nqs = d.t.nqs;
+}
+
+// 1/rho of the level set at the volume and surface cubature points:
+// LevelSetSolver3D::getRhoVolOI / getRhoSurfOI (src/solvers/3d/ls_solver.cpp:202-233:
+// s interpolated to the points, then ls_3d_step_rho_vol_oi / ls_3d_step_surf_oi_1)
+// followed by mp_ins_3d_pr_fact_oi_0/1 (1 / rho). The surface values come from the
+// element's own polynomial, whose trace the reference interpolates from the face
+// nodes. One thread per point.
+__global__ void k_oi_ls_factor(const double* __restrict__ vphi, const double* __restrict__ fphi,
+                               const double* __restrict__ s, int K, int Np, int nq, int nfq, double alpha,
+                               double rho0, double rho1, double* __restrict__ fvol, double* __restrict__ fsurf) {
+  const size_t nv = (size_t)K * nq, ns = (size_t)K * nfq;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nv + ns; i += (size_t)gridDim.x * blockDim.x) {
+    const bool vol = i < nv;
+    const size_t j = vol ? i : i - nv;
+    const int per = vol ? nq : nfq;
+    const size_t e = j / per;
+    const int q = (int)(j - e * per);
+    const double* phi = (vol ? vphi : fphi) + (size_t)q * Np;
+    const double* se = s + e * Np;
+    double sv = 0.0;
+    for (int k = 0; k < Np; ++k) sv += phi[k] * se[k];
+    const double step = tanh(3.141592653589793238463 * sv / alpha);
+    const double rho = 0.5 * rho0 * (1.0 + step) + 0.5 * rho1 * (1.0 - step);
+    (vol ? fvol : fsurf)[j] = 1.0 / rho;
+  }
+}
+
+void set_factor_oi_level_set(sipg_op* op, const double* s, double alpha, double rho0, double rho1,
+                             cudaStream_t st) {
+  if (op->ncomp != 1) throw Error(SIPG_INVALID_ARG, "the over-integrated operator is scalar");
+  sipg_mesh* m = op->mesh;
+  const int K = m->K, NF = m->dim + 1;
+  const OiDev& d = oi_dev(m->dim, op->order);
+  const int nq = d.t.nq, nqs = d.t.nqs;
+  ensure(op->oi_fvol, (size_t)K * nq * sizeof(double));
+  ensure(op->oi_fsurf, (size_t)K * NF * nqs * sizeof(double));
+  const size_t n = (size_t)K * (nq + NF * nqs);
+  const int g = (int)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, (size_t)num_sms() * 16));
+  k_oi_ls_factor<<<g, 256, 0, st>>>(d.vphi.as<double>(), d.fphi.as<double>(), s, K, op->Np, nq, NF * nqs, alpha,
+                                    rho0, rho1, op->oi_fvol.as<double>(), op->oi_fsurf.as<double>());
+  note_launch();
+  SIPG_CUDA(cudaGetLastError());
+  ++op->version;
+  oi_assemble(op, st);
 }
 
 // Set the operator's cubature-point factor (host or device pointers): penalty,

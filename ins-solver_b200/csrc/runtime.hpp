@@ -131,4 +131,7 @@ void set_bc_types_host(sipg_op* op, const std::vector<int>& types);
 // the stored factor after the boundary types, mass term or pinned DOF change.
 void set_factor_oi_device(sipg_op* op, const double* fvol, const double* fsurf, cudaStream_t s);
 void oi_assemble(sipg_op* op, cudaStream_t s);
+// The two-phase pressure factor 1/rho(s) at the cubature points straight from the
+// level set s (K x Np, device), rho = the smoothed Heaviside of ls_step; then assemble.
+void set_factor_oi_level_set(sipg_op* op, const double* s, double alpha, double rho0, double rho1, cudaStream_t st);
 }  // namespace sipg

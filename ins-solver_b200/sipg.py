@@ -254,26 +254,40 @@ def ins_pressure_neumann(mesh, order, reynolds, vel, N, mu, rho, vel_bc):
 
 
 class Ins3DOpts(C.Structure):
-    """sipg_ins3d_opts: the MPINSSolver3D configuration of the two-phase time step."""
+    """sipg_ins3d_opts: the MPINSSolver3D configuration of the two-phase time step,
+    with the pressure (p-multigrid) and viscous (Jacobi-PCG) solver options."""
     _fields_ = [("order", C.c_int), ("reynolds", C.c_double), ("rho0", C.c_double), ("rho1", C.c_double),
                 ("mu0", C.c_double), ("mu1", C.c_double), ("gravity", C.c_double), ("ls_alpha", C.c_double),
-                ("cfl", C.c_double), ("precision", C.c_int), ("extrapolate_history", C.c_int),
-                ("pr_rel_tol", C.c_double), ("pr_abs_tol", C.c_double), ("pr_max_iter", C.c_int),
-                ("vis_rel_tol", C.c_double), ("vis_abs_tol", C.c_double), ("vis_max_iter", C.c_int)]
+                ("cfl", C.c_double), ("extrapolate_history", C.c_int), ("pr_over_int", C.c_int),
+                ("pressure", SolverOpts),
+                ("viscous", SolverOpts)]
 
 
 class Ins3DStepInfo(C.Structure):
     _fields_ = [("time", C.c_double), ("dt", C.c_double), ("pr_iters", C.c_int), ("vis_iters", C.c_int * 3),
                 ("pr_rel_res", C.c_double), ("vis_rel_res", C.c_double * 3), ("max_vel", C.c_double),
                 ("ms_advection", C.c_double), ("ms_pressure", C.c_double), ("ms_viscosity", C.c_double),
-                ("ms_surface", C.c_double), ("proj_converged", C.c_ulonglong)]
+                ("ms_surface", C.c_double), ("ms_pressure_setup", C.c_double),
+                ("ms_pressure_solve", C.c_double), ("proj_converged", C.c_ulonglong)]
 
 
 def ins3d_default_opts(**kw):
+    """Defaults of sipg_ins3d_default_opts with overrides: plain fields by name,
+    precision (the pressure V-cycle's), and pr_<field> / vis_<field> for the
+    pressure and viscous solver options (pr_rel_tol, vis_max_iter, pr_cheb_order ...)."""
     o = Ins3DOpts()
     check(lib().sipg_ins3d_default_opts(C.byref(o)))
     for k, v in kw.items():
-        setattr(o, k, v)
+        if k == "precision":
+            o.pressure.precision = v
+        elif k == "pr_over_int":
+            o.pr_over_int = v
+        elif k.startswith("pr_"):
+            setattr(o.pressure, k[3:], v)
+        elif k.startswith("vis_"):
+            setattr(o.viscous, k[4:], v)
+        else:
+            setattr(o, k, v)
     return o
 
 
