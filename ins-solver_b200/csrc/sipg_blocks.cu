@@ -47,39 +47,63 @@ __device__ void face_normal_d(const double* g, int f, double n[3], double* sJ) {
   }
 }
 
-// consts64 layout of the apply (Cfg): Dr, Ds, [Dt], M with row stride LD.
+// One warp builds one element's block: the reference matrices (consts64 layout of
+// the apply, Cfg: Dr, Ds, [Dt], M with row stride LD) and the face masses are staged
+// once per CTA, each warp keeps its element's block B and two Np x Np work arrays,
+// and only warp barriers separate the steps (lanes stride over the entries, each
+// entry summed in the same order as a plain loop).
+template <int P>
+struct BlockWarps {
+  static constexpr int W = P >= 4 ? 2 : 4;
+};
+
 template <int DIM, int P>
-__global__ void __launch_bounds__(128) block_kernel(BlockArgs a) {
+__host__ __device__ constexpr size_t block_smem_doubles() {
+  using C = Cfg<DIM, P>;
+  return (size_t)(DIM + 1) * C::NP * C::LD + (size_t)C::NF * C::NFP * C::NFP +
+         (size_t)BlockWarps<P>::W * (3 * C::NP * C::NP + 2 * C::NP + C::NG);
+}
+
+template <int DIM, int P>
+__global__ void __launch_bounds__(32 * BlockWarps<P>::W) block_kernel(BlockArgs a) {
   using C = Cfg<DIM, P>;
   constexpr int NP = C::NP, NFP = C::NFP, NF = C::NF, LD = C::LD, NG = C::NG, NPP = NP * NP;
-  __shared__ double B[NPP], X[NPP], T[NPP], MF[NF * NFP * NFP];
-  __shared__ double g[NG], fac[NP];
+  constexpr int W = BlockWarps<P>::W;
+  extern __shared__ double smb[];
   __shared__ int fm[NF * NFP];
-  __shared__ int piv_row;
-  __shared__ double fcol[NP];
-  const double* Dm = a.consts + C::OFF_D;
-  const double* Mm = a.consts + C::OFF_M;
+  double* Dm = smb;                               // DIM x NP x LD
+  double* Mm = Dm + DIM * NP * LD;                // NP x LD
+  double* MF = Mm + NP * LD;                      // NF x NFP x NFP
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* B = MF + NF * NFP * NFP + (size_t)warp * (3 * NPP + 2 * NP + NG);
+  double* X = B + NPP;
+  double* T = X + NPP;
+  double* fac = T + NPP;
+  double* fcol = fac + NP;
+  double* g = fcol + NP;
+  for (int i = threadIdx.x; i < (DIM + 1) * NP * LD; i += blockDim.x) Dm[i] = a.consts[C::OFF_D + i];
   for (int i = threadIdx.x; i < NF * NFP * NFP; i += blockDim.x) MF[i] = a.mf[i];
   for (int i = threadIdx.x; i < NF * NFP; i += blockDim.x) fm[i] = a.itab[i];
+  __syncthreads();
   const int total = a.K * a.ncomp;
-  for (int item = blockIdx.x; item < total; item += gridDim.x) {
+  for (int item = blockIdx.x * W + warp; item < total; item += gridDim.x * W) {
     const int e = item % a.K, c = item / a.K;
-    __syncthreads();
-    for (int i = threadIdx.x; i < NG; i += blockDim.x) g[i] = a.geof[(size_t)e * NG + i];
-    for (int i = threadIdx.x; i < NP; i += blockDim.x) fac[i] = a.factor ? a.factor[(size_t)e * NP + i] : 1.0;
-    for (int i = threadIdx.x; i < NPP; i += blockDim.x) B[i] = 0.0;
-    __syncthreads();
+    __syncwarp();
+    for (int i = lane; i < NG; i += 32) g[i] = a.geof[(size_t)e * NG + i];
+    for (int i = lane; i < NP; i += 32) fac[i] = a.factor ? a.factor[(size_t)e * NP + i] : 1.0;
+    for (int i = lane; i < NPP; i += 32) B[i] = 0.0;
+    __syncwarp();
     const double J = g[DIM == 3 ? 9 : 4];
     // volume: sum_d J Dx_d^T M F Dx_d (fvmf_3d_op1.h / fvmf_3d_op1_diag.h)
     for (int d = 0; d < DIM; ++d) {
-      for (int i = threadIdx.x; i < NPP; i += blockDim.x) {
+      for (int i = lane; i < NPP; i += 32) {
         int r = i / NP, cc = i % NP;
         double s = 0.0;
         for (int rr = 0; rr < DIM; ++rr) s += g[rr * DIM + d] * Dm[rr * NP * LD + r * LD + cc];
         X[i] = s;
       }
-      __syncthreads();
-      for (int i = threadIdx.x; i < NPP; i += blockDim.x) {
+      __syncwarp();
+      for (int i = lane; i < NPP; i += 32) {
         int r = i / NP, cc = i % NP;
         double s = 0.0;
         if (a.ref_volume && DIM == 2) {
@@ -90,8 +114,8 @@ __global__ void __launch_bounds__(128) block_kernel(BlockArgs a) {
         }
         T[i] = J * s;
       }
-      __syncthreads();
-      for (int i = threadIdx.x; i < NPP; i += blockDim.x) {
+      __syncwarp();
+      for (int i = lane; i < NPP; i += 32) {
         int r = i / NP, cc = i % NP;
         double s = 0.0;
         if (a.ref_volume && DIM == 3)
@@ -100,7 +124,7 @@ __global__ void __launch_bounds__(128) block_kernel(BlockArgs a) {
           for (int k = 0; k < NP; ++k) s += X[k * NP + r] * T[k * NP + cc];
         B[i] += s;
       }
-      __syncthreads();
+      __syncwarp();
     }
     // faces (fvmf_3d_op2_block_diag.h, fvmf_3d_bop_block_diag.h)
     for (int f = 0; f < NF; ++f) {
@@ -123,103 +147,105 @@ __global__ void __launch_bounds__(128) block_kernel(BlockArgs a) {
       double rf[3] = {0.0, 0.0, 0.0};
       for (int rr = 0; rr < DIM; ++rr)
         for (int d = 0; d < DIM; ++d) rf[rr] += n[d] * g[rr * DIM + d];
-      __syncthreads();
-      for (int i = threadIdx.x; i < NPP; i += blockDim.x) {
+      for (int i = lane; i < NPP; i += 32) {
         int r = i / NP, cc = i % NP;
         double s = 0.0;
         for (int rr = 0; rr < DIM; ++rr) s += rf[rr] * Dm[rr * NP * LD + r * LD + cc];
         X[i] = s * fac[r];
       }
-      __syncthreads();
+      __syncwarp();
       const double* mf = MF + f * NFP * NFP;
       const int* fmf = fm + f * NFP;
       // rows on the face: -scale * (MF D_n)[a][j]; and the penalty on face-face entries
-      for (int i = threadIdx.x; i < NFP * NP; i += blockDim.x) {
+      for (int i = lane; i < NFP * NP; i += 32) {
         int aa = i / NP, j = i % NP;
         double s = 0.0;
         for (int bb = 0; bb < NFP; ++bb) s += mf[aa * NFP + bb] * X[fmf[bb] * NP + j];
         B[fmf[aa] * NP + j] -= scale * s;
       }
-      __syncthreads();
+      __syncwarp();
       // columns on the face: -scale * (D_n^T MF)[i][b]
-      for (int i = threadIdx.x; i < NP * NFP; i += blockDim.x) {
+      for (int i = lane; i < NP * NFP; i += 32) {
         int r = i / NFP, bb = i % NFP;
         double s = 0.0;
         for (int aa = 0; aa < NFP; ++aa) s += X[fmf[aa] * NP + r] * mf[aa * NFP + bb];
         B[r * NP + fmf[bb]] -= scale * s;
       }
-      __syncthreads();
-      for (int i = threadIdx.x; i < NFP * NFP; i += blockDim.x) {
+      __syncwarp();
+      for (int i = lane; i < NFP * NFP; i += 32) {
         int aa = i / NFP, bb = i % NFP;
         B[fmf[aa] * NP + fmf[bb]] += scale * gtau * mf[i];
       }
-      __syncthreads();
+      __syncwarp();
     }
     // mass term (fvmf_3d_mm_block_diag.h: the reference scales rows; the operator scales columns)
     if (a.mm_mode != 0) {
-      for (int i = threadIdx.x; i < NPP; i += blockDim.x) {
+      for (int i = lane; i < NPP; i += 32) {
         int r = i / NP, cc = i % NP;
         int k = a.ref_volume ? r : cc;
         double mmv = a.mm_mode == 1 ? a.mm_scalar : a.mm[(size_t)e * NP + k];
         B[i] += J * Mm[r * LD + cc] * mmv;
       }
-      __syncthreads();
+      __syncwarp();
     }
     if (e == a.pin_elem) {
       const int pn = a.pin_node;
-      for (int i = threadIdx.x; i < NP; i += blockDim.x) {
+      for (int i = lane; i < NP; i += 32) {
         if (i != pn) { B[pn * NP + i] = 0.0; B[i * NP + pn] = 0.0; }
       }
-      if (threadIdx.x == 0) B[pn * NP + pn] = a.pin_scale;
-      __syncthreads();
+      __syncwarp();
+      if (lane == 0) B[pn * NP + pn] = a.pin_scale;
+      __syncwarp();
     }
     double* out_base = a.out + (size_t)item * (a.mode == BLOCK_DIAG_ONLY ? NP : NPP);
     if (a.mode == BLOCK_DIAG_ONLY) {
-      for (int i = threadIdx.x; i < NP; i += blockDim.x) out_base[i] = B[i * NP + i];
+      for (int i = lane; i < NP; i += 32) out_base[i] = B[i * NP + i];
       continue;
     }
     if (a.mode == BLOCK_INVERSE) {
       // Gauss-Jordan with partial pivoting: B -> I, X -> B^-1
-      for (int i = threadIdx.x; i < NPP; i += blockDim.x) X[i] = (i / NP == i % NP) ? 1.0 : 0.0;
-      __syncthreads();
+      for (int i = lane; i < NPP; i += 32) X[i] = (i / NP == i % NP) ? 1.0 : 0.0;
+      __syncwarp();
       for (int col = 0; col < NP; ++col) {
-        if (threadIdx.x == 0) {
-          int p = col;
-          double best = fabs(B[col * NP + col]);
-          for (int r = col + 1; r < NP; ++r) {
-            double v = fabs(B[r * NP + col]);
-            if (v > best) { best = v; p = r; }
-          }
-          piv_row = p;
+        // pivot: the first row (from col down) of largest |B[r][col]|, as a serial scan picks it
+        double best = -1.0;
+        int p = NP;
+        for (int r = col + lane; r < NP; r += 32) {
+          const double v = fabs(B[r * NP + col]);
+          if (v > best) { best = v; p = r; }
         }
-        __syncthreads();
-        const int p = piv_row;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+          const int op = __shfl_xor_sync(0xffffffffu, p, o);
+          if (ob > best || (ob == best && op < p)) { best = ob; p = op; }
+        }
         if (p != col)
-          for (int j = threadIdx.x; j < NP; j += blockDim.x) {
+          for (int j = lane; j < NP; j += 32) {
             double t0 = B[col * NP + j]; B[col * NP + j] = B[p * NP + j]; B[p * NP + j] = t0;
             double t1 = X[col * NP + j]; X[col * NP + j] = X[p * NP + j]; X[p * NP + j] = t1;
           }
-        __syncthreads();
+        __syncwarp();
         const double dinv = 1.0 / B[col * NP + col];
-        __syncthreads();
-        for (int j = threadIdx.x; j < NP; j += blockDim.x) {
+        __syncwarp();
+        for (int j = lane; j < NP; j += 32) {
           B[col * NP + j] *= dinv;
           X[col * NP + j] *= dinv;
         }
-        __syncthreads();
-        for (int r = threadIdx.x; r < NP; r += blockDim.x) fcol[r] = B[r * NP + col];
-        __syncthreads();
-        for (int i = threadIdx.x; i < NPP; i += blockDim.x) {
+        __syncwarp();
+        for (int r = lane; r < NP; r += 32) fcol[r] = B[r * NP + col];
+        __syncwarp();
+        for (int i = lane; i < NPP; i += 32) {
           int r = i / NP, j = i % NP;
           if (r == col) continue;
           B[i] -= fcol[r] * B[col * NP + j];
           X[i] -= fcol[r] * X[col * NP + j];
         }
-        __syncthreads();
+        __syncwarp();
       }
-      for (int i = threadIdx.x; i < NPP; i += blockDim.x) out_base[i] = X[i];
+      for (int i = lane; i < NPP; i += 32) out_base[i] = X[i];
     } else {
-      for (int i = threadIdx.x; i < NPP; i += blockDim.x) out_base[i] = B[i];
+      for (int i = lane; i < NPP; i += 32) out_base[i] = B[i];
     }
   }
 }
@@ -309,8 +335,17 @@ __global__ void __launch_bounds__(128) apply_bc_kernel(ApplyBcArgs a) {
 cudaError_t launch_blocks(int dim, int order, const BlockArgs& a, cudaStream_t s) {
   int total = a.K * a.ncomp;
   if (total <= 0) return cudaSuccess;
-  int grid = std::min(total, 148 * 16);
-  SIPG_DISPATCH_B(dim, order, block_kernel<D, P><<<grid, 128, 0, s>>>(a); note_launch(); return cudaGetLastError());
+  SIPG_DISPATCH_B(dim, order, {
+    constexpr int W = BlockWarps<P>::W;
+    const size_t smem = block_smem_doubles<D, P>() * sizeof(double);
+    auto k = block_kernel<D, P>;
+    cudaError_t err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return err;
+    const int grid = std::max(1, std::min((total + W - 1) / W, 148 * 8));
+    k<<<grid, 32 * W, smem, s>>>(a);
+    note_launch();
+    return cudaGetLastError();
+  });
   return cudaErrorInvalidValue;
 }
 

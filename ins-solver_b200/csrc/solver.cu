@@ -528,15 +528,21 @@ void sipg_solver::setup_pmg() {
     SIPG_CUDA(cudaStreamSynchronize(stream));
   }
   pt.mark("levels and factors");
+  // the point-Jacobi diagonal is read by the Chebyshev smoother without element blocks
+  // and by the Jacobi-PCG on the lowest order; the element-block smoother with the
+  // algebraic coarse solve reads none
+  const bool amg_below = o.coarse_kind == 1 && nc == 1 && lv.back().order == 1;
   for (int l = 0; l < nl; ++l) {
     Level& L = lv[l];
     L.cheb = o.cheb_orders[l] > 0 ? o.cheb_orders[l] : o.cheb_order;
     L.pre = std::max(0, o.pre_it[l]);
     L.post = std::max(0, o.post_it[l]);
-    op_diag(L.op, L.dinv64.as<double>(), stream);
-    k_recip<<<grid_for(L.n), 256, 0, stream>>>(L.dinv64.as<double>(), L.n);
+    if (o.smoother != 1 || (l == nl - 1 && !amg_below)) {
+      op_diag(L.op, L.dinv64.as<double>(), stream);
+      k_recip<<<grid_for(L.n), 256, 0, stream>>>(L.dinv64.as<double>(), L.n);
       note_launch();
-    if (f32) to_f32(L.dinv32.as<float>(), L.dinv64.as<double>(), L.n, stream);
+      if (f32) to_f32(L.dinv32.as<float>(), L.dinv64.as<double>(), L.n, stream);
+    }
     DevBuf& rows = rows_ws;  // FP64 inverse diagonal blocks, row-major per element (block-Jacobi smoothing)
     if (o.smoother == 1) {
       // element-block Jacobi: inverse diagonal blocks in the level precision (BF16 for
