@@ -120,171 +120,218 @@ __global__ void k_oi_project(const double* __restrict__ proj, const double* __re
   }
 }
 
-constexpr int OI_THREADS = 128, OI_QC = 32;
+constexpr int OI_QC = 32;
 
-// Element blocks, one CTA per element (grid-stride). Each thread owns the entries
-// (i, j) = t, t + 128, ... of a block; the volume term runs over the cubature
-// points in chunks of OI_QC whose physical gradients are staged in shared memory.
+// One warp assembles one element's blocks. Every block is a sum of outer products
+// over cubature points,
+//   volume        sum_{q,d} a_q Y_d[q][i] Y_d[q][j]       (Y_d = dphi/dx_d, a_q = w_q J f_q)
+//   self, face    sum_s P[s][i] Q[s][j] + E[s][i] P[s][j]  (P = phi, E = -h sJ f- dn,
+//                                                          Q = E + h sJ tau w P)
+//   neighbour     sum_s U[s][i] PS[s][j] + CH[s][i] DM[s][j]
+//                 (U = sJ (f- dn - tau w phi) / 2, PS = the neighbour's basis, CH = the own
+//                  basis at the neighbour's points, DM = -sJ f+ dn+ / 2),
+// so the factors are staged per point chunk or face in the warp's shared area
+// (rows padded to NPP4, a multiple of 4) and each lane accumulates a 4 x 4 tile of the
+// Np x Np block in registers: 16 FMAs per 8 staged values. Tiles beyond 32 per
+// block (p = 4 in 3D) take further rounds over the element.
+template <int NP>
+struct OiTile {
+  static constexpr int NPP4 = (NP + 3) / 4 * 4, NTI = NPP4 / 4, NT = NTI * NTI;
+  static constexpr int W = NP > 20 ? 2 : 4;  // warps per CTA
+};
+
+template <int NP>
+__device__ __forceinline__ void oi_outer(double (&acc)[16], const double* L, const double* R, const double* w,
+                                         int nk, int i0, int j0) {
+  constexpr int S = OiTile<NP>::NPP4;
+  for (int k = 0; k < nk; ++k) {
+    const double2 l01 = *reinterpret_cast<const double2*>(L + k * S + i0);
+    const double2 l23 = *reinterpret_cast<const double2*>(L + k * S + i0 + 2);
+    const double2 r01 = *reinterpret_cast<const double2*>(R + k * S + j0);
+    const double2 r23 = *reinterpret_cast<const double2*>(R + k * S + j0 + 2);
+    const double ws = w ? w[k] : 1.0;
+    const double l[4] = {ws * l01.x, ws * l01.y, ws * l23.x, ws * l23.y};
+    const double r[4] = {r01.x, r01.y, r23.x, r23.y};
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a * 4 + b] = fma(l[a], r[b], acc[a * 4 + b]);
+  }
+}
+
+// doubles of one warp's shared area: a volume chunk (Y and its weights) or the seven
+// face arrays, whichever is larger
 template <int DIM, int NP>
-__global__ void __launch_bounds__(OI_THREADS) k_oi_blocks(OiArgs a) {
-  constexpr int NF = DIM + 1, NG = DIM == 3 ? 10 : 5, NE = (NP * NP + OI_THREADS - 1) / OI_THREADS;
+__host__ __device__ size_t oi_warp_doubles(int nqs) {
+  constexpr int S = OiTile<NP>::NPP4;
+  const size_t vol = (size_t)OI_QC * DIM * S + OI_QC * DIM;
+  const size_t face = (size_t)7 * nqs * S;
+  return vol > face ? vol : face;
+}
+
+template <int DIM, int NP>
+__global__ void __launch_bounds__(32 * OiTile<NP>::W) k_oi_blocks(OiArgs a) {
+  constexpr int NF = DIM + 1, NG = DIM == 3 ? 10 : 5, S = OiTile<NP>::NPP4, NTI = OiTile<NP>::NTI;
+  constexpr int NT = OiTile<NP>::NT, W = OiTile<NP>::W;
   extern __shared__ double sm[];
-  const int nqs = a.nqs;
-  double* Y = sm;                           // [DIM][OI_QC][NP]
-  double* aq = Y + DIM * OI_QC * NP;        // [OI_QC]
-  double* ph = aq + OI_QC;                  // [nqs][NP] own basis at own points
-  double* dn = ph + nqs * NP;               // [nqs][NP] own normal derivative at own points
-  double* ps = dn + nqs * NP;               // [nqs][NP] neighbour basis at own points
-  double* dp = ps + nqs * NP;               // [nqs][NP] neighbour normal derivative at its points
-  double* ch = dp + nqs * NP;               // [nqs][NP] own basis at the neighbour's points
-  double* fm = ch + nqs * NP;               // [nqs] own factor x weight
-  double* fp = fm + nqs;                    // [nqs] neighbour factor x weight
-  double* g = fp + nqs;                     // [NG] own geometry
-  double* gn = g + NG;                      // [NG] neighbour geometry
+  const int nqs = a.nqs, nq = a.nq;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* Z = sm + (size_t)warp * oi_warp_doubles<DIM, NP>(nqs);
+  // volume chunk: Y[(q * DIM + d) * S + i], weights wv[q * DIM + d]
+  double* Y = Z;
+  double* wv = Z + (size_t)OI_QC * DIM * S;
+  // face arrays, nqs x S each
+  double* P = Z;
+  double* E = P + nqs * S;
+  double* Q = E + nqs * S;
+  double* U = Q + nqs * S;
+  double* PS = U + nqs * S;
+  double* CH = PS + nqs * S;
+  double* DM = CH + nqs * S;
   const size_t K = (size_t)a.K;
-  for (int e = blockIdx.x; e < a.K; e += gridDim.x) {
-    __syncthreads();
-    if (threadIdx.x < NG) g[threadIdx.x] = a.geof[(size_t)e * NG + threadIdx.x];
-    __syncthreads();
+  for (int e = blockIdx.x * W + warp; e < a.K; e += gridDim.x * W) {
+    double g[NG];
+#pragma unroll
+    for (int k = 0; k < NG; ++k) g[k] = __ldg(a.geof + (size_t)e * NG + k);
     const double J = oi_J<DIM>(g);
-    double acc[NE];
+    for (int t0 = 0; t0 < NT; t0 += 32) {
+      const int t = t0 + lane;
+      const bool act = t < NT;
+      const int i0 = act ? 4 * (t / NTI) : 0, j0 = act ? 4 * (t % NTI) : 0;
+      double acc[16];
 #pragma unroll
-    for (int k = 0; k < NE; ++k) acc[k] = 0.0;
-    // volume: sum_q w_q J f_q sum_d (dphi_i / dx_d)(dphi_j / dx_d)
-    for (int q0 = 0; q0 < a.nq; q0 += OI_QC) {
-      const int nc = min(OI_QC, a.nq - q0);
-      for (int t = threadIdx.x; t < DIM * nc * NP; t += blockDim.x) {
-        const int d = t / (nc * NP), qq = (t / NP) % nc, i = t % NP;
-        double s = 0.0;
+      for (int k = 0; k < 16; ++k) acc[k] = 0.0;
+      // volume
+      for (int q0 = 0; q0 < nq; q0 += OI_QC) {
+        const int nc = min(OI_QC, nq - q0);
+        __syncwarp();
+        for (int idx = lane; idx < nc * DIM * S; idx += 32) {
+          const int i = idx % S, d = (idx / S) % DIM, qq = idx / (S * DIM);
+          double v = 0.0;
+          if (i < NP)
 #pragma unroll
-        for (int r = 0; r < DIM; ++r) s += g[r * DIM + d] * a.vdphi[((size_t)r * a.nq + q0 + qq) * NP + i];
-        Y[(d * OI_QC + qq) * NP + i] = s;
-      }
-      for (int qq = threadIdx.x; qq < nc; qq += blockDim.x)
-        aq[qq] = a.wq[q0 + qq] * J * a.fvol[(size_t)e * a.nq + q0 + qq];
-      __syncthreads();
-#pragma unroll
-      for (int k = 0; k < NE; ++k) {
-        const int ent = threadIdx.x + k * OI_THREADS;
-        if (ent >= NP * NP) break;
-        const int i = ent / NP, j = ent % NP;
-        double s = 0.0;
-        for (int qq = 0; qq < nc; ++qq) {
-          double t = 0.0;
-#pragma unroll
-          for (int d = 0; d < DIM; ++d) t += Y[(d * OI_QC + qq) * NP + i] * Y[(d * OI_QC + qq) * NP + j];
-          s += aq[qq] * t;
+            for (int r = 0; r < DIM; ++r) v += g[r * DIM + d] * __ldg(a.vdphi + ((size_t)r * nq + q0 + qq) * NP + i);
+          Y[idx] = v;
         }
-        acc[k] += s;
+        for (int idx = lane; idx < nc * DIM; idx += 32) {
+          const int qq = idx / DIM;
+          wv[idx] = __ldg(a.wq + q0 + qq) * J * a.fvol[(size_t)e * nq + q0 + qq];
+        }
+        __syncwarp();
+        if (act) oi_outer<NP>(acc, Y, Y, wv, nc * DIM, i0, j0);
       }
-      __syncthreads();
-    }
-    // faces
-    for (int f = 0; f < NF; ++f) {
-      const int nb = a.nbr[(size_t)e * NF + f];
-      if (nb < 0 && a.bct[-nb - 1] != BC_DIRICHLET) continue;  // Neumann and (scalar) slip faces add nothing
-      double n[3], sJ;
-      simplex_face_normal<DIM>(g, f, n, &sJ);
-      const double h = nb >= 0 ? 0.5 : 1.0, tau = a.tau[(size_t)e * NF + f];
-      double cr[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-      for (int r = 0; r < DIM; ++r)
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) cr[r] += n[d] * g[r * DIM + d];
-      int gf = 0, sg = 0;
-      if (nb >= 0) {
-        const int code = (a.fcode[e] >> (8 * f)) & 0xff;
-        gf = code & 3;
-        sg = code >> 2;
-        if (threadIdx.x < NG) gn[threadIdx.x] = a.geof[(size_t)nb * NG + threadIdx.x];
-      }
-      __syncthreads();
-      double cn[3] = {0.0, 0.0, 0.0};
-      if (nb >= 0)
+      // faces
+      for (int f = 0; f < NF; ++f) {
+        const int nb = a.nbr[(size_t)e * NF + f];
+        const bool dir = nb < 0 && a.bct[-nb - 1] == BC_DIRICHLET;
+        if (nb < 0 && !dir) continue;  // Neumann and (scalar) slip faces add nothing
+        double n[3], sJ;
+        simplex_face_normal<DIM>(g, f, n, &sJ);
+        const double h = nb >= 0 ? 0.5 : 1.0, tau = a.tau[(size_t)e * NF + f];
+        double cr[3] = {0.0, 0.0, 0.0}, cn[3] = {0.0, 0.0, 0.0};
 #pragma unroll
         for (int r = 0; r < DIM; ++r)
 #pragma unroll
-          for (int d = 0; d < DIM; ++d) cn[r] += n[d] * gn[r * DIM + d];
-      for (int t = threadIdx.x; t < nqs * NP; t += blockDim.x) {
-        const int s = t / NP, i = t % NP;
-        ph[t] = a.fphi[((size_t)f * nqs + s) * NP + i];
-        double v = 0.0;
-#pragma unroll
-        for (int r = 0; r < DIM; ++r) v += cr[r] * a.fdphi[(((size_t)f * 3 + r) * nqs + s) * NP + i];
-        dn[t] = v;
+          for (int d = 0; d < DIM; ++d) cr[r] += n[d] * g[r * DIM + d];
+        int gf = 0, sg = 0;
         if (nb >= 0) {
-          ps[t] = a.xphi[(((size_t)gf * a.nperm + sg) * nqs + s) * NP + i];
-          double w = 0.0;
+          const int code = (a.fcode[e] >> (8 * f)) & 0xff;
+          gf = code & 3;
+          sg = code >> 2;
 #pragma unroll
-          for (int r = 0; r < DIM; ++r) w += cn[r] * a.fdphi[(((size_t)gf * 3 + r) * nqs + s) * NP + i];
-          dp[t] = w;
-          ch[t] = a.yphi[(((size_t)f * a.nperm + sg) * nqs + s) * NP + i];
-        }
-      }
-      for (int s = threadIdx.x; s < nqs; s += blockDim.x) {
-        fm[s] = a.ws[s] * a.fsurf[((size_t)e * NF + f) * nqs + s];
-        if (nb >= 0) fp[s] = a.ws[s] * a.fsurf[((size_t)nb * NF + gf) * nqs + s];
-      }
-      __syncthreads();
-      // self: sJ sum_s [-h f- (dn_j phi_i + dn_i phi_j) + h tau phi_i phi_j]
+          for (int r = 0; r < DIM; ++r)
 #pragma unroll
-      for (int k = 0; k < NE; ++k) {
-        const int ent = threadIdx.x + k * OI_THREADS;
-        if (ent >= NP * NP) break;
-        const int i = ent / NP, j = ent % NP;
-        double s1 = 0.0;
-        for (int s = 0; s < nqs; ++s) {
-          const double pi = ph[s * NP + i], pj = ph[s * NP + j];
-          s1 += -h * fm[s] * (dn[s * NP + j] * pi + dn[s * NP + i] * pj) + h * tau * a.ws[s] * pi * pj;
+            for (int d = 0; d < DIM; ++d) cn[r] += n[d] * __ldg(a.geof + (size_t)nb * NG + r * DIM + d);
         }
-        acc[k] += sJ * s1;
-      }
-      if (nb >= 0) {
-        // neighbour: sJ [sum_s (f- dn_i psi_j - tau phi_i psi_j) / 2 - sum_t f+_t dn+_j(t) chi_i(t) / 2]
-        for (int ent = threadIdx.x; ent < NP * NP; ent += blockDim.x) {
-          const int i = ent / NP, j = ent % NP;
-          double s1 = 0.0, s2 = 0.0;
-          for (int s = 0; s < nqs; ++s) {
-            s1 += (fm[s] * dn[s * NP + i] - tau * a.ws[s] * ph[s * NP + i]) * ps[s * NP + j];
-            s2 += fp[s] * dp[s * NP + j] * ch[s * NP + i];
+        __syncwarp();
+        for (int idx = lane; idx < nqs * S; idx += 32) {
+          const int sq = idx / S, i = idx % S;
+          double ph = 0.0, dn = 0.0, ps = 0.0, ch = 0.0, dp = 0.0;
+          if (i < NP) {
+            ph = __ldg(a.fphi + ((size_t)f * nqs + sq) * NP + i);
+#pragma unroll
+            for (int r = 0; r < DIM; ++r) dn += cr[r] * __ldg(a.fdphi + (((size_t)f * 3 + r) * nqs + sq) * NP + i);
+            if (nb >= 0) {
+              ps = __ldg(a.xphi + (((size_t)gf * a.nperm + sg) * nqs + sq) * NP + i);
+#pragma unroll
+              for (int r = 0; r < DIM; ++r)
+                dp += cn[r] * __ldg(a.fdphi + (((size_t)gf * 3 + r) * nqs + sq) * NP + i);
+              ch = __ldg(a.yphi + (((size_t)f * a.nperm + sg) * nqs + sq) * NP + i);
+            }
           }
-          double val = 0.5 * sJ * (s1 - s2);
-          if ((nb == a.pin_elem && j == a.pin_node) || (e == a.pin_elem && i == a.pin_node)) val = 0.0;
-          a.v[((size_t)((1 + f) * NP + i) * NP + j) * K + e] = val;
+          const double ws = __ldg(a.ws + sq);
+          const double fm = ws * a.fsurf[((size_t)e * NF + f) * nqs + sq];
+          const double ev = -h * sJ * fm * dn;
+          P[idx] = ph;
+          E[idx] = ev;
+          Q[idx] = ev + h * sJ * tau * ws * ph;
+          if (nb >= 0) {
+            const double fp = ws * a.fsurf[((size_t)nb * NF + gf) * nqs + sq];
+            U[idx] = 0.5 * sJ * (fm * dn - tau * ws * ph);
+            PS[idx] = ps;
+            CH[idx] = ch;
+            DM[idx] = -0.5 * sJ * fp * dp;
+          }
+        }
+        __syncwarp();
+        if (act) {
+          oi_outer<NP>(acc, P, Q, nullptr, nqs, i0, j0);
+          oi_outer<NP>(acc, E, P, nullptr, nqs, i0, j0);
+        }
+        if (nb >= 0 && act) {
+          double nacc[16];
+#pragma unroll
+          for (int k = 0; k < 16; ++k) nacc[k] = 0.0;
+          oi_outer<NP>(nacc, U, PS, nullptr, nqs, i0, j0);
+          oi_outer<NP>(nacc, CH, DM, nullptr, nqs, i0, j0);
+#pragma unroll
+          for (int aa = 0; aa < 4; ++aa)
+#pragma unroll
+            for (int bb = 0; bb < 4; ++bb) {
+              const int i = i0 + aa, j = j0 + bb;
+              if (i >= NP || j >= NP) continue;
+              double val = nacc[aa * 4 + bb];
+              if ((nb == a.pin_elem && j == a.pin_node) || (e == a.pin_elem && i == a.pin_node)) val = 0.0;
+              a.v[((size_t)((1 + f) * NP + i) * NP + j) * K + e] = val;
+            }
         }
       }
-      __syncthreads();
-    }
-    for (int f = 0; f < NF; ++f)
-      if (a.nbr[(size_t)e * NF + f] < 0)
-        for (int ent = threadIdx.x; ent < NP * NP; ent += blockDim.x)
-          a.v[((size_t)((1 + f) * NP + ent / NP) * NP + ent % NP) * K + e] = 0.0;
+      if (act) {
+        for (int f = 0; f < NF; ++f)
+          if (a.nbr[(size_t)e * NF + f] < 0)
 #pragma unroll
-    for (int k = 0; k < NE; ++k) {
-      const int ent = threadIdx.x + k * OI_THREADS;
-      if (ent >= NP * NP) break;
-      const int i = ent / NP, j = ent % NP;
-      double val = acc[k];
-      if (a.mm_mode != MM_NONE)
-        val += J * a.mass[i * NP + j] * (a.mm_mode == MM_SCALAR ? a.mm_scalar : a.mm[(size_t)e * NP + j]);
-      // the pinned DOF: column zero, its row keeps only its own diagonal
-      if (e == a.pin_elem && (j == a.pin_node || i == a.pin_node) && i != j) val = 0.0;
-      a.v[((size_t)i * NP + j) * K + e] = val;
+            for (int aa = 0; aa < 4; ++aa)
+#pragma unroll
+              for (int bb = 0; bb < 4; ++bb) {
+                const int i = i0 + aa, j = j0 + bb;
+                if (i < NP && j < NP) a.v[((size_t)((1 + f) * NP + i) * NP + j) * K + e] = 0.0;
+              }
+#pragma unroll
+        for (int aa = 0; aa < 4; ++aa)
+#pragma unroll
+          for (int bb = 0; bb < 4; ++bb) {
+            const int i = i0 + aa, j = j0 + bb;
+            if (i >= NP || j >= NP) continue;
+            double val = acc[aa * 4 + bb];
+            if (a.mm_mode != MM_NONE)
+              val += J * a.mass[i * NP + j] * (a.mm_mode == MM_SCALAR ? a.mm_scalar : a.mm[(size_t)e * NP + j]);
+            // the pinned DOF: column zero, its row keeps only its own diagonal
+            if (e == a.pin_elem && (j == a.pin_node || i == a.pin_node) && i != j) val = 0.0;
+            a.v[((size_t)i * NP + j) * K + e] = val;
+          }
+      }
     }
   }
 }
 
-size_t oi_smem(int dim, int Np, int nqs) {
-  const int NG = dim == 3 ? 10 : 5;
-  return (size_t)(dim * OI_QC * Np + OI_QC + 5 * nqs * Np + 2 * nqs + 2 * NG) * sizeof(double);
-}
-
 template <int DIM, int NP>
-void launch_oi_blocks_t(const OiArgs& a, size_t smem, cudaStream_t s) {
+void launch_oi_blocks_t(const OiArgs& a, cudaStream_t s) {
+  constexpr int W = OiTile<NP>::W;
+  const size_t smem = (size_t)W * oi_warp_doubles<DIM, NP>(a.nqs) * sizeof(double);
   auto k = k_oi_blocks<DIM, NP>;
   SIPG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const int grid = std::max(1, std::min(a.K, num_sms() * 16));
-  k<<<grid, OI_THREADS, smem, s>>>(a);
+  const int grid = std::max(1, std::min((a.K + W - 1) / W, num_sms() * 16));
+  k<<<grid, 32 * W, smem, s>>>(a);
   note_launch();
   SIPG_CUDA(cudaGetLastError());
 }
@@ -422,16 +469,15 @@ void oi_assemble(sipg_op* op, cudaStream_t s) {
   a.pin_elem = op->pin_elem;
   a.pin_node = op->pin_node;
   a.v = B.v64.as<double>();
-  const size_t smem = oi_smem(dim, Np, nqs);
   switch (dim * 100 + Np) {
-    case 203: launch_oi_blocks_t<2, 3>(a, smem, s); break;
-    case 206: launch_oi_blocks_t<2, 6>(a, smem, s); break;
-    case 210: launch_oi_blocks_t<2, 10>(a, smem, s); break;
-    case 215: launch_oi_blocks_t<2, 15>(a, smem, s); break;
-    case 304: launch_oi_blocks_t<3, 4>(a, smem, s); break;
-    case 310: launch_oi_blocks_t<3, 10>(a, smem, s); break;
-    case 320: launch_oi_blocks_t<3, 20>(a, smem, s); break;
-    case 335: launch_oi_blocks_t<3, 35>(a, smem, s); break;
+    case 203: launch_oi_blocks_t<2, 3>(a, s); break;
+    case 206: launch_oi_blocks_t<2, 6>(a, s); break;
+    case 210: launch_oi_blocks_t<2, 10>(a, s); break;
+    case 215: launch_oi_blocks_t<2, 15>(a, s); break;
+    case 304: launch_oi_blocks_t<3, 4>(a, s); break;
+    case 310: launch_oi_blocks_t<3, 10>(a, s); break;
+    case 320: launch_oi_blocks_t<3, 20>(a, s); break;
+    case 335: launch_oi_blocks_t<3, 35>(a, s); break;
     default: throw Error(SIPG_INVALID_ARG, "over-integrated operator: unsupported element");
   }
   to_f32(B.v32.as<float>(), B.v64.as<double>(), nv, s);
