@@ -288,8 +288,9 @@ def run_two_phase(steps=TWO_PHASE_STEPS):
     consts = dict(order=3, reynolds=100.0, rho0=1.0, rho1=1e-3, mu0=1.0, mu1=1e-2, gravity=9.81, cfl=0.5,
                   pr_over_int=1)
     runs = {}
-    for name, prec in (("fp64", sipg.FP64), ("mixed", sipg.FP32)):
-        ins = sipg.Ins3D(mesh, vel_bc, **consts, precision=prec)
+    arms = (("fp64", sipg.FP64, sipg.SOLVER_JACOBI), ("mixed", sipg.FP32, sipg.SOLVER_JACOBI))
+    for name, prec, vk in arms:
+        ins = sipg.Ins3D(mesh, vel_bc, **consts, precision=prec, viscous_kind=vk)
         ins.set_state(vel, s)
         ins.step(1)  # first step: set-up of the solvers' workspaces
         t0 = time.perf_counter()
@@ -316,6 +317,7 @@ def run_two_phase(steps=TWO_PHASE_STEPS):
                         "1000, viscosity ratio 100, gravity 9.81 along -y, Re 100, no-slip walls, over-integrated "
                         "pressure operator, level-set alpha 24 h; level set advected, not reinitialised",
             "steps": steps, "fp64": runs["fp64"], "mixed": runs["mixed"],
+            "viscous_preconditioner": "Jacobi ([viscous-solve] preconditioner = jacobi, the reference's default)",
             "mixed_vs_fp64_step_speedup": runs["fp64"]["ms_per_step"] / runs["mixed"]["ms_per_step"],
             "parts": ["advection", "pressure", "viscosity", "surface", "pressure: factor and set-up",
                       "pressure: solve"],
@@ -1029,6 +1031,8 @@ def run_profile(args):
            solve of 3 iterations, then a counted one (kernel by kernel, no graphs).
     oiapply: the over-integrated operator at --n, p = 3 (two-phase factor at the
            cubature points): 3 FP64 applies of its element blocks.
+    setup: the headline solver's set-up for a new factor (set_factor, then setup)
+           after a warm-up solve; prints ncu's -s and -c for it like solve.
     solve: the headline mixed solve: one warm-up solve, then the captured solve;
            prints the number of kernels launched before it (ncu -s) and in it (-c).
            The outer iterations replay one host-launched graph each (graphs = 1):
@@ -1127,6 +1131,21 @@ def run_profile(args):
         sipg.check(sipg.lib().sipg_device_synchronize())
         print("done", K)
         return
+    if args.profile == "setup":
+        # the per-time-step set-up of the headline solve: one warm-up solve (first
+        # set-up included), then a new factor and the set-up again, counted
+        c2, op = build_headline()
+        s, _ = pmg_solver(op, args.precision, graphs=1)
+        b = sipg.DeviceVector(c2["rhs"].reshape(-1))
+        x = sipg.DeviceVector(np.zeros(c2["rhs"].size))
+        s.solve_device(b.ptr, x.ptr)
+        sipg.check(sipg.lib().sipg_device_synchronize())
+        n1 = launches()
+        op.set_factor(c2["factor"])
+        s.setup()
+        sipg.check(sipg.lib().sipg_device_synchronize())
+        print("skip", n1, "count", launches() - n1)
+        return
     c2, op = build_headline() if args.n == N_HEAD else (c, None)
     if op is None:
         op = sipg.Operator(c["mesh"], ORDER, 1)
@@ -1146,7 +1165,8 @@ def run_profile(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--profile", choices=["apply", "solve", "projection", "pressure", "c3apply", "c3pcg", "oiapply"],
+    ap.add_argument("--profile", choices=["apply", "solve", "setup", "projection", "pressure", "c3apply", "c3pcg",
+                                          "oiapply"],
                     default=None,
                     help="run a small fixed workload for an ncu capture instead of the benchmark")
     ap.add_argument("--n", type=int, default=N_HEAD)

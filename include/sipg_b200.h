@@ -463,6 +463,9 @@ typedef struct {
                                 mp_ins_solver.cpp:524-544), the V-cycle on its nodal
                                 projection; 0: the nodal factor 1/rho. The pressure gradient
                                 of the projection step is the nodal one either way. */
+  int viscous_kind;          /* [viscous-solve] preconditioner: SIPG_SOLVER_JACOBI (default,
+                                PETScJacobiSolver) or SIPG_SOLVER_BLOCK_JACOBI
+                                (PETScBlockJacobiSolver, mp_ins_solver.cpp:113-121) */
   /* The pressure p-multigrid (SIPG_SOLVER_PMULTIGRID: precision of the V-cycle,
    * tolerances, [p-multigrid] keys; n_levels 0 = orders p, p-1, ..., 1; nullspace is
    * set from the boundary types) and the viscous Jacobi-PCG options. Defaults: the

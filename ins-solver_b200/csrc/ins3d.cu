@@ -242,6 +242,7 @@ int sipg_ins3d_default_opts(sipg_ins3d_opts* o) {
     o->ls_alpha = 24.0;  // level-set-options alpha (ls_solver.cpp:137)
     o->cfl = 1.0;
     o->extrapolate_history = 3;
+    o->viscous_kind = SIPG_SOLVER_JACOBI;
     // setup_pressure_viscous_solvers (ins_solver_base.cpp:149-184)
     ok(sipg_solver_default_opts(SIPG_SOLVER_PMULTIGRID, &o->pressure), "pressure options");
     o->pressure.rel_tol = 1e-8;
@@ -330,8 +331,10 @@ int sipg_ins3d_create(sipg_mesh* m, const sipg_ins3d_opts* o, const int* vel_bc,
     // viscosity: FactorMMPoissonMatrixFreeDiag3D + PETScJacobiSolver, one component at a time
     ok(sipg_op_create(m, o->order, 1, &ins->vop), "viscous operator");
     ok(sipg_op_set_bc_types(ins->vop, vst.data()), "viscous boundary types");
+    if (o->viscous_kind != SIPG_SOLVER_JACOBI && o->viscous_kind != SIPG_SOLVER_BLOCK_JACOBI)
+      throw Error(SIPG_INVALID_ARG, "viscous_kind must be SIPG_SOLVER_JACOBI or SIPG_SOLVER_BLOCK_JACOBI");
     sipg_solver_opts vo = o->viscous;
-    ok(sipg_solver_create(ins->vop, SIPG_SOLVER_JACOBI, &vo, &ins->vsol), "viscous solver");
+    ok(sipg_solver_create(ins->vop, o->viscous_kind, &vo, &ins->vsol), "viscous solver");
     *out = ins.release();
   });
 }

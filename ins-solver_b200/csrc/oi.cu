@@ -173,10 +173,10 @@ template <int DIM, int NP>
 __global__ void __launch_bounds__(32 * OiTile<NP>::W) k_oi_blocks(OiArgs a) {
   constexpr int NF = DIM + 1, NG = DIM == 3 ? 10 : 5, S = OiTile<NP>::NPP4, NTI = OiTile<NP>::NTI;
   constexpr int NT = OiTile<NP>::NT, W = OiTile<NP>::W;
-  extern __shared__ double sm[];
+  extern __shared__ __align__(16) double sm[];
   const int nqs = a.nqs, nq = a.nq;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double* Z = sm + (size_t)warp * oi_warp_doubles<DIM, NP>(nqs);
+  double* Z = sm + (size_t)warp * oi_warp_doubles<DIM, NP>(nqs);  // even sizes: 16-byte aligned tiles
   // volume chunk: Y[(q * DIM + d) * S + i], weights wv[q * DIM + d]
   double* Y = Z;
   double* wv = Z + (size_t)OI_QC * DIM * S;

@@ -57,11 +57,47 @@ struct BlockWarps {
   static constexpr int W = P >= 4 ? 2 : 4;
 };
 
+template <int NP>
+struct BlockTile {
+  static constexpr int S = (NP + 3) / 4 * 4, NTI = S / 4, NT = NTI * NTI;
+};
+
+// Shared-memory layout of block_kernel in doubles, every part starting on an even
+// index (16 bytes) for the tiles' double2 loads: the staged reference matrices and
+// face masses, then per warp the block B, the staging area (LT, Xd, Ts) and fac, fcol, g.
+__host__ __device__ constexpr size_t even_up(size_t n) { return (n + 1) / 2 * 2; }
+
+template <int DIM, int P>
+struct BlockSmem {
+  using C = Cfg<DIM, P>;
+  static constexpr size_t BASE = even_up((size_t)(DIM + 1) * C::NP * C::LD + (size_t)C::NF * C::NFP * C::NFP);
+  static constexpr size_t OFF_LT = even_up((size_t)C::NP * C::NP);
+  static constexpr size_t WARP = OFF_LT + 3 * (size_t)C::NP * BlockTile<C::NP>::S + even_up(2 * C::NP + C::NG);
+};
+
 template <int DIM, int P>
 __host__ __device__ constexpr size_t block_smem_doubles() {
-  using C = Cfg<DIM, P>;
-  return (size_t)(DIM + 1) * C::NP * C::LD + (size_t)C::NF * C::NFP * C::NFP +
-         (size_t)BlockWarps<P>::W * (3 * C::NP * C::NP + 2 * C::NP + C::NG);
+  return BlockSmem<DIM, P>::BASE + (size_t)BlockWarps<P>::W * BlockSmem<DIM, P>::WARP;
+}
+
+// acc (4 x 4 tile at rows i0, columns j0) = sum_k L[k][i] R[k][j], rows of stride S
+template <int S>
+__device__ __forceinline__ void block_outer(double (&acc)[16], const double* L, const double* R, int nk, int i0,
+                                            int j0) {
+#pragma unroll
+  for (int k = 0; k < 16; ++k) acc[k] = 0.0;
+  for (int k = 0; k < nk; ++k) {
+    const double2 l01 = *reinterpret_cast<const double2*>(L + k * S + i0);
+    const double2 l23 = *reinterpret_cast<const double2*>(L + k * S + i0 + 2);
+    const double2 r01 = *reinterpret_cast<const double2*>(R + k * S + j0);
+    const double2 r23 = *reinterpret_cast<const double2*>(R + k * S + j0 + 2);
+    const double l[4] = {l01.x, l01.y, l23.x, l23.y};
+    const double r[4] = {r01.x, r01.y, r23.x, r23.y};
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a * 4 + b] = fma(l[a], r[b], acc[a * 4 + b]);
+  }
 }
 
 template <int DIM, int P>
@@ -69,16 +105,23 @@ __global__ void __launch_bounds__(32 * BlockWarps<P>::W) block_kernel(BlockArgs 
   using C = Cfg<DIM, P>;
   constexpr int NP = C::NP, NFP = C::NFP, NF = C::NF, LD = C::LD, NG = C::NG, NPP = NP * NP;
   constexpr int W = BlockWarps<P>::W;
-  extern __shared__ double smb[];
+  extern __shared__ __align__(16) double smb[];
   __shared__ int fm[NF * NFP];
   double* Dm = smb;                               // DIM x NP x LD
   double* Mm = Dm + DIM * NP * LD;                // NP x LD
   double* MF = Mm + NP * LD;                      // NF x NFP x NFP
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double* B = MF + NF * NFP * NFP + (size_t)warp * (3 * NPP + 2 * NP + NG);
-  double* X = B + NPP;
-  double* T = X + NPP;
-  double* fac = T + NPP;
+  constexpr int S = BlockTile<NP>::S, NTI = BlockTile<NP>::NTI, NT = BlockTile<NP>::NT;
+  using L = BlockSmem<DIM, P>;
+  double* B = smb + L::BASE + (size_t)warp * L::WARP;
+  double* LT = B + L::OFF_LT;  // NP x S: (J M F)^T
+  double* Xd = LT + NP * S;  // NP x S: X_d
+  double* Ts = Xd + NP * S;  // NP x S: T = J M F X_d
+  // Np x Np work arrays of the face terms and of the reference's volume variants,
+  // over the staging area (NP * S >= NPP)
+  double* X = LT;
+  double* T = Xd;
+  double* fac = Ts + NP * S;
   double* fcol = fac + NP;
   double* g = fcol + NP;
   for (int i = threadIdx.x; i < (DIM + 1) * NP * LD; i += blockDim.x) Dm[i] = a.consts[C::OFF_D + i];
@@ -94,8 +137,47 @@ __global__ void __launch_bounds__(32 * BlockWarps<P>::W) block_kernel(BlockArgs 
     for (int i = lane; i < NPP; i += 32) B[i] = 0.0;
     __syncwarp();
     const double J = g[DIM == 3 ? 9 : 4];
-    // volume: sum_d J Dx_d^T M F Dx_d (fvmf_3d_op1.h / fvmf_3d_op1_diag.h)
-    for (int d = 0; d < DIM; ++d) {
+    // volume: sum_d J Dx_d^T M F Dx_d (fvmf_3d_op1.h / fvmf_3d_op1_diag.h); the operator's
+    // form as outer products in 4 x 4 lane tiles, the reference's variants entry by entry
+    if (!a.ref_volume) {
+      for (int i = lane; i < NP * S; i += 32) {
+        const int k = i / S, r = i % S;
+        LT[i] = r < NP ? J * Mm[r * LD + k] * fac[k] : 0.0;
+      }
+      for (int d = 0; d < DIM; ++d) {
+        for (int i = lane; i < NP * S; i += 32) {
+          const int k = i / S, cc = i % S;
+          double v = 0.0;
+          if (cc < NP)
+            for (int rr = 0; rr < DIM; ++rr) v += g[rr * DIM + d] * Dm[rr * NP * LD + k * LD + cc];
+          Xd[i] = v;
+        }
+        __syncwarp();
+        for (int t = lane; t < NT; t += 32) {
+          const int i0 = 4 * (t / NTI), j0 = 4 * (t % NTI);
+          double acc[16];
+          block_outer<S>(acc, LT, Xd, NP, i0, j0);
+#pragma unroll
+          for (int aa = 0; aa < 4; ++aa)
+#pragma unroll
+            for (int bb = 0; bb < 4; ++bb)
+              if (i0 + aa < NP) Ts[(i0 + aa) * S + j0 + bb] = acc[aa * 4 + bb];
+        }
+        __syncwarp();
+        for (int t = lane; t < NT; t += 32) {
+          const int i0 = 4 * (t / NTI), j0 = 4 * (t % NTI);
+          double acc[16];
+          block_outer<S>(acc, Xd, Ts, NP, i0, j0);
+#pragma unroll
+          for (int aa = 0; aa < 4; ++aa)
+#pragma unroll
+            for (int bb = 0; bb < 4; ++bb)
+              if (i0 + aa < NP && j0 + bb < NP) B[(i0 + aa) * NP + j0 + bb] += acc[aa * 4 + bb];
+        }
+        __syncwarp();
+      }
+    }
+    for (int d = 0; d < (a.ref_volume ? DIM : 0); ++d) {
       for (int i = lane; i < NPP; i += 32) {
         int r = i / NP, cc = i % NP;
         double s = 0.0;

@@ -259,6 +259,7 @@ class Ins3DOpts(C.Structure):
     _fields_ = [("order", C.c_int), ("reynolds", C.c_double), ("rho0", C.c_double), ("rho1", C.c_double),
                 ("mu0", C.c_double), ("mu1", C.c_double), ("gravity", C.c_double), ("ls_alpha", C.c_double),
                 ("cfl", C.c_double), ("extrapolate_history", C.c_int), ("pr_over_int", C.c_int),
+                ("viscous_kind", C.c_int),
                 ("pressure", SolverOpts),
                 ("viscous", SolverOpts)]
 
@@ -280,8 +281,8 @@ def ins3d_default_opts(**kw):
     for k, v in kw.items():
         if k == "precision":
             o.pressure.precision = v
-        elif k == "pr_over_int":
-            o.pr_over_int = v
+        elif k in ("pr_over_int", "viscous_kind"):
+            setattr(o, k, v)
         elif k.startswith("pr_"):
             setattr(o.pressure, k[3:], v)
         elif k.startswith("vis_"):

@@ -104,3 +104,18 @@ def test_over_integrated_two_phase_steps_converge_and_lift_the_bubble(precision)
         assert info.pr_iters < 500 and info.pr_rel_res <= 1e-8
     st = ins.state()
     assert st["vel"][1][s < 0].mean() > 0
+
+
+def test_block_jacobi_viscous_solves_give_the_jacobi_steps():
+    """[viscous-solve] preconditioner = block-jacobi: the same step to the solver tolerance."""
+    gm, _, s, vel, vel_bc = _case(3, 2, False)
+    tol = dict(pr_rel_tol=1e-11, pr_abs_tol=1e-300, vis_rel_tol=1e-11, vis_abs_tol=1e-300)
+    got, iters = [], []
+    for vk in (sipg.SOLVER_JACOBI, sipg.SOLVER_BLOCK_JACOBI):
+        ins = sipg.Ins3D(gm, vel_bc, order=2, precision=sipg.FP64, viscous_kind=vk, **tol, **CONSTS)
+        ins.set_state(vel, s)
+        info = ins.step(2)
+        got.append(ins.state())
+        iters.append(sum(info.vis_iters))
+    assert rel_err(got[1]["vel"], got[0]["vel"]) < 1e-8
+    assert iters[1] < iters[0]
