@@ -440,10 +440,10 @@ int sipg_ins_pressure_neumann_host(sipg_mesh *m, int order, double reynolds, con
  *   viscosity     sipg_viscous_rhs, factor mu and mass factor g0 Re rho / dt, set-up and
  *                 three Jacobi-PCG solves (FactorMMPoissonMatrixFreeDiag3D +
  *                 PETScJacobiSolver) with zero Dirichlet data on no-slip walls;
- *   surface       the level-set advection (three Runge-Kutta stages), then rho and mu;
+ *   surface       the level-set advection (three Runge-Kutta stages), every reinit_freq
+ *                 steps its reinitialisation (sipg_ls_reinit_host), then rho and mu;
  * then dt = cfl h / ((p+1)^2 max(1, max |u|)) (INSSolverBase3D::max_vel) and the second-
- * order coefficients (a0, a1, b0, b1, g0) = (2, -0.5, 2, -1, 1.5) after the first step.
- * The level-set reinitialisation (LevelSetSolver3D::reinitLS) is not part of it. */
+ * order coefficients (a0, a1, b0, b1, g0) = (2, -0.5, 2, -1, 1.5) after the first step. */
 typedef struct {
   int order;                 /* DG order */
   double reynolds;           /* r_ynolds */
@@ -463,6 +463,10 @@ typedef struct {
                                 mp_ins_solver.cpp:524-544), the V-cycle on its nodal
                                 projection; 0: the nodal factor 1/rho. The pressure gradient
                                 of the projection step is the nodal one either way. */
+  int reinit_freq;           /* level-set-options reinit_freq: reinitialise every this many steps
+                                (24); 0: never */
+  int reinit_ic;             /* level-set-options reinit_ic: reinitialise the initial level set (1) */
+  double ls_cap;             /* LS_CAP of problem_specific_3d.h (1): the reinitialised level set's bound */
   int viscous_kind;          /* [viscous-solve] preconditioner: SIPG_SOLVER_JACOBI (default,
                                 PETScJacobiSolver) or SIPG_SOLVER_BLOCK_JACOBI
                                 (PETScBlockJacobiSolver, mp_ins_solver.cpp:113-121) */
@@ -490,6 +494,12 @@ typedef struct {
 
 typedef struct sipg_ins3d sipg_ins3d;
 int sipg_ins3d_default_opts(sipg_ins3d_opts *o);
+/* Closest-point reinitialisation of a level set alone, LevelSetSolver3D::reinitLS
+ * (src/solvers/3d/ls_solver.cpp:719-860) as the time step runs it: the zero set sampled
+ * in the elements where s changes sign, each node's closest sample, a Newton
+ * closest-point iteration on that element's polynomial, s = +-distance clamped to
+ * +-ls_cap (ls_post_reinit). s: K x Np host array, in place. */
+int sipg_ls_reinit_host(sipg_mesh *m, int order, double ls_cap, double *s);
 /* vel_bc: Kb velocity boundary types (0 no-slip, 2 natural outflow). */
 int sipg_ins3d_create(sipg_mesh *m, const sipg_ins3d_opts *o, const int *vel_bc, sipg_ins3d **out);
 /* Initial velocity (3 x K x Np) and level set (K x Np), host arrays: the reference's

@@ -60,7 +60,10 @@ struct sipg_ins3d {
   cudaStream_t st = nullptr;
   DevBuf vel[2], N[2], velT, velTT, pr, dPdN[2];
   DevBuf s, qa, qb, rk0, rk1, rho, mu, rrho;
-  DevBuf rhs, mmf, vbc, vmax, stats;
+  DevBuf rhs, mmf, vbc, vmax, stats, xyz;
+  ReinitWork rw;
+  double h_ls = 0.0;
+  int reinit_counter = 0;
   std::vector<DevBuf> hist;      // pressure history (ring), newest last in hist_order
   std::vector<double> hist_t;
   std::vector<int> hist_order;
@@ -141,6 +144,13 @@ struct sipg_ins3d {
     hist_order.push_back(slot);
   }
 
+  // LevelSetSolver3D::step's reinitialisation and ls_post_reinit, then rho, mu and max |u|
+  // again from the new level set
+  void reinit(const double* u) {
+    ls_reinit_device(m, o.order, xyz.as<double>(), s.as<double>(), h_ls, o.ls_cap, rw, st);
+    ls_props_device(m, o.order, ls_fields(u), st);
+  }
+
   void step(sipg_ins3d_step_info* info) {
     const int nw = 1 - cur;
     double* u = vel[cur].as<double>();
@@ -191,6 +201,10 @@ struct sipg_ins3d {
     // surface (level set, then rho and mu)
     SIPG_CUDA(cudaEventRecord(t_surf.a, st));
     ls_step_device(m, o.order, dt, ls_fields(u_new), st);
+    if (o.reinit_freq > 0 && ++reinit_counter >= o.reinit_freq) {
+      reinit(u_new);
+      reinit_counter = 0;
+    }
     SIPG_CUDA(cudaEventRecord(t_surf.b, st));
     max_vel = read_max_vel();
     // update_time and the second-order coefficients (MPINSSolver3D::step)
@@ -243,6 +257,9 @@ int sipg_ins3d_default_opts(sipg_ins3d_opts* o) {
     o->cfl = 1.0;
     o->extrapolate_history = 3;
     o->viscous_kind = SIPG_SOLVER_JACOBI;
+    o->reinit_freq = 24;  // level-set-options reinit_freq (ls_solver.cpp:146-148)
+    o->reinit_ic = 1;     // reinit_ic (:158-159)
+    o->ls_cap = 1.0;      // LS_CAP, include/problem_specific_3d.h
     // setup_pressure_viscous_solvers (ins_solver_base.cpp:149-184)
     ok(sipg_solver_default_opts(SIPG_SOLVER_PMULTIGRID, &o->pressure), "pressure options");
     o->pressure.rel_tol = 1e-8;
@@ -300,7 +317,9 @@ int sipg_ins3d_create(sipg_mesh* m, const sipg_ins3d_opts* o, const int* vel_bc,
         }
     if (fmax_ <= 0.0) throw Error(SIPG_INVALID_ARG, "mesh without interior faces");
     ins->h = 1.0 / fmax_;
+    ins->h_ls = 1.0 / fmin_;
     ins->alpha = o->ls_alpha / fmin_;
+    if (!(o->ls_cap > 0.0) || o->reinit_freq < 0) throw Error(SIPG_INVALID_ARG, "ls_cap > 0 and reinit_freq >= 0");
     SIPG_CUDA(cudaStreamCreateWithFlags(&ins->st, cudaStreamNonBlocking));
     const size_t nb = ins->n * sizeof(double), nf = (size_t)m->K * 4 * hm.Nfp * sizeof(double);
     for (int i = 0; i < 2; ++i) {
@@ -317,6 +336,14 @@ int sipg_ins3d_create(sipg_mesh* m, const sipg_ins3d_opts* o, const int* vel_bc,
     ins->vbc = DevBuf(std::max<size_t>(1, m->Kb) * sizeof(int));
     if (m->Kb) ins->vbc.upload(vel_bc, m->Kb * sizeof(int));
     ins->vmax = DevBuf(sizeof(unsigned long long));
+    {
+      std::vector<double> xyz(3 * ins->n);
+      std::copy(hm.x.begin(), hm.x.end(), xyz.begin());
+      std::copy(hm.y.begin(), hm.y.end(), xyz.begin() + ins->n);
+      std::copy(hm.z.begin(), hm.z.end(), xyz.begin() + 2 * ins->n);
+      ins->xyz = DevBuf(3 * nb);
+      ins->xyz.upload(xyz.data(), 3 * nb);
+    }
     ins->stats = DevBuf(2 * sizeof(unsigned long long));
     // pressure: FactorPoissonMatrixFreeDiag3D + PETScPMultigrid, nullspace without Dirichlet faces
     ok(sipg_op_create(m, o->order, 1, &ins->pop), "pressure operator");
@@ -358,7 +385,11 @@ int sipg_ins3d_set_state_host(sipg_ins3d* ins, const double* vel, const double* 
     ins->b0 = 1.0;
     ins->b1 = 0.0;
     ins->g0 = 1.0;
-    ls_props_device(ins->m, ins->o.order, ins->ls_fields(ins->vel[0].as<double>()), ins->st);
+    ins->reinit_counter = 0;
+    if (ins->o.reinit_ic)
+      ins->reinit(ins->vel[0].as<double>());
+    else
+      ls_props_device(ins->m, ins->o.order, ins->ls_fields(ins->vel[0].as<double>()), ins->st);
     ins->max_vel = ins->read_max_vel();
     ins->dt = ins->next_dt();
     ins->have_state = true;
@@ -387,5 +418,31 @@ int sipg_ins3d_get_state_host(sipg_ins3d* ins, double* vel, double* pr, double* 
 }
 
 void sipg_ins3d_destroy(sipg_ins3d* ins) { delete ins; }
+
+int sipg_ls_reinit_host(sipg_mesh* m, int order, double ls_cap, double* s) {
+  return guarded([&] {
+    if (!m || !s || !(ls_cap > 0.0)) throw Error(SIPG_INVALID_ARG, "ls_reinit arguments");
+    if (m->dim != 3) throw Error(SIPG_INVALID_ARG, "the level-set reinitialisation is 3D");
+    if (order < 1 || order > 4) throw Error(SIPG_INVALID_ARG, "order must be 1..4");
+    m->ensure_device();
+    const Mesh& hm = m->host_order(order);
+    const size_t n = (size_t)m->K * hm.Np;
+    double fmin_ = 1e300;
+    for (int e = 0; e < m->K; ++e)
+      for (int f = 0; f < 4; ++f)
+        if (hm.nbr[(size_t)e * 4 + f] >= 0) fmin_ = std::min(fmin_, hm.fscale[(size_t)e * 4 + f]);
+    if (fmin_ >= 1e300) throw Error(SIPG_INVALID_ARG, "mesh without interior faces");
+    std::vector<double> xyz(3 * n);
+    std::copy(hm.x.begin(), hm.x.end(), xyz.begin());
+    std::copy(hm.y.begin(), hm.y.end(), xyz.begin() + n);
+    std::copy(hm.z.begin(), hm.z.end(), xyz.begin() + 2 * n);
+    DevBuf dx(3 * n * sizeof(double)), ds(n * sizeof(double));
+    dx.upload(xyz.data(), 3 * n * sizeof(double));
+    ds.upload(s, n * sizeof(double));
+    ReinitWork w;
+    ls_reinit_device(m, order, dx.as<double>(), ds.as<double>(), 1.0 / fmin_, ls_cap, w, 0);
+    SIPG_CUDA(cudaMemcpy(s, ds.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+  });
+}
 
 }  // extern "C"

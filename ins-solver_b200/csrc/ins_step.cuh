@@ -33,4 +33,15 @@ void ls_step_device(sipg_mesh* m, int order, double dt, const LsFields& f, cudaS
 // rho, mu, 1 / rho from s and max |u|^2 alone.
 void ls_props_device(sipg_mesh* m, int order, const LsFields& f, cudaStream_t s);
 
+// Work buffers of the level-set reinitialisation, kept across calls.
+struct ReinitWork {
+  DevBuf cells, count, samples, nearest, s_old;
+};
+
+// Closest-point reinitialisation of s (K x Np, in place): xyz the node coordinates
+// (3 x K x Np), h the level set's length (1 / the smallest interior-face fscale),
+// values clamped to +-ls_cap.
+void ls_reinit_device(sipg_mesh* m, int order, const double* xyz, double* s, double h, double ls_cap,
+                      ReinitWork& w, cudaStream_t st);
+
 }  // namespace sipg

@@ -259,6 +259,7 @@ class Ins3DOpts(C.Structure):
     _fields_ = [("order", C.c_int), ("reynolds", C.c_double), ("rho0", C.c_double), ("rho1", C.c_double),
                 ("mu0", C.c_double), ("mu1", C.c_double), ("gravity", C.c_double), ("ls_alpha", C.c_double),
                 ("cfl", C.c_double), ("extrapolate_history", C.c_int), ("pr_over_int", C.c_int),
+                ("reinit_freq", C.c_int), ("reinit_ic", C.c_int), ("ls_cap", C.c_double),
                 ("viscous_kind", C.c_int),
                 ("pressure", SolverOpts),
                 ("viscous", SolverOpts)]
@@ -281,7 +282,7 @@ def ins3d_default_opts(**kw):
     for k, v in kw.items():
         if k == "precision":
             o.pressure.precision = v
-        elif k in ("pr_over_int", "viscous_kind"):
+        elif k in ("pr_over_int", "viscous_kind", "reinit_freq", "reinit_ic", "ls_cap"):
             setattr(o, k, v)
         elif k.startswith("pr_"):
             setattr(o.pressure, k[3:], v)
@@ -330,6 +331,14 @@ class Ins3D:
             self.close()
         except Exception:
             pass
+
+
+def ls_reinit(mesh, order, s, ls_cap=1.0):
+    """Closest-point reinitialisation of a level set (sipg_ls_reinit_host): returns the
+    new (K, Np) values."""
+    out = np.array(s, dtype=np.float64, order="C", copy=True)
+    check(lib().sipg_ls_reinit_host(mesh.h, order, C.c_double(ls_cap), _dp(out)))
+    return out
 
 
 def projection_factor(dim, dt):

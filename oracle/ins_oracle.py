@@ -229,7 +229,7 @@ class TwoPhaseStep:
     walls), the level-set step, then the time-step update. Solves run to rel_tol."""
 
     def __init__(self, mesh, p, vel_bc, reynolds, rho0, rho1, mu0, mu1, gravity=0.0, ls_alpha=24.0, cfl=1.0,
-                 history=3, rel_tol=1e-11):
+                 history=3, rel_tol=1e-11, reinit_freq=24, reinit_ic=1, ls_cap=1.0):
         self.mesh, self.p = mesh, p
         self.t = D.ref_tables(3, p)
         self.om = O.OMesh(self.t, mesh.export(p, self.t))
@@ -240,6 +240,7 @@ class TwoPhaseStep:
         self.nullspace = int(np.all(self.pr_bct == 1))
         self.re, self.rho0, self.rho1, self.mu0, self.mu1 = reynolds, rho0, rho1, mu0, mu1
         self.grav, self.cfl, self.history, self.rel_tol = gravity, cfl, history, rel_tol
+        self.reinit_freq, self.reinit_ic, self.ls_cap = reinit_freq, reinit_ic, ls_cap
         fs = mesh.fscale[mesh.nbr >= 0]
         self.h = 1.0 / fs.max()
         self.alpha = ls_alpha / fs.min()
@@ -262,6 +263,9 @@ class TwoPhaseStep:
         self.hist = []
         self.time = 0.0
         self.a0, self.a1, self.b0, self.b1, self.g0 = 1.0, 0.0, 1.0, 0.0, 1.0
+        self.reinit_counter = 0
+        if self.reinit_ic:
+            self.s = ls_reinit(self.mesh, self.p, self.s, self.ls_cap)
         self._props()
         self._next_dt()
 
@@ -292,8 +296,183 @@ class TwoPhaseStep:
             b = J[:, None] * ((self.re / dt * self.rho * velTT[c]) @ M.T)
             vel_new[c], _ = self._solve(b, self.vis_bct, self.vel_old[c], factor=self.mu, mm=mmf)
         self.s = ls_advect(m, p, dt, self.s, vel_new, self.vel_bc)
+        self.reinit_counter += 1
+        if self.reinit_freq > 0 and self.reinit_counter >= self.reinit_freq:
+            self.s = ls_reinit(m, p, self.s, self.ls_cap)
+            self.reinit_counter = 0
         self._props()
         self.vel_old, self.vel, self.N_old, self.dPdN_old = self.vel, vel_new, N, dPdN
         self.time += dt
         self.a0, self.a1, self.b0, self.b1, self.g0 = 2.0, -0.5, 2.0, -1.0, 1.5
         self._next_dt()
+
+
+# ---- level-set reinitialisation (LevelSetSolver3D::reinitLS, src/solvers/3d/ls_solver.cpp:
+# 719-860; sampleInterface and simplified_newton, src/solvers/3d/ls_solver_cpu.cpp:291-487;
+# newton_kernel and newton_method, ls_solver.cpp:259-480), in the deterministic form the
+# library runs: each element's own polynomial instead of the stencil fit, samples started at
+# the reference nodes scaled by 0.75 and dropped when the sampling Newton fails (no random
+# restarts), brute-force closest samples instead of the KD-tree, no kink detection.
+
+def _mono_exps(p):
+    return [(a, b, n - a - b) for n in range(p + 1) for a in range(n, -1, -1) for b in range(n - a, -1, -1)]
+
+
+class _ElementPoly:
+    """The nodal interpolant of one element as a polynomial in its reference coordinates,
+    evaluated at physical points: value, gradient and Hessian (xx, yy, zz, xy, xz, yz)."""
+
+    def __init__(self, t, G, x0, sval):
+        self.ex = _mono_exps(t["order"])
+        r0 = np.array([t["r"][0], t["s"][0], t["t"][0]])
+        self.r0, self.G, self.x0 = r0, G, x0
+        V = np.array([[t["r"][i] ** a * t["s"][i] ** b * t["t"][i] ** c for (a, b, c) in self.ex]
+                      for i in range(t["Np"])])
+        self.c = np.linalg.solve(V, sval)
+
+    def ref(self, x):
+        return self.r0 + self.G @ (np.asarray(x) - self.x0)
+
+    def to_phys(self, r):
+        return self.x0 + np.linalg.solve(self.G, np.asarray(r) - self.r0)
+
+    def eval(self, x):
+        r = self.ref(x)
+        v, g, H = 0.0, np.zeros(3), np.zeros((3, 3))
+        for ck, e in zip(self.c, self.ex):
+            p = [r[d] ** e[d] for d in range(3)]
+            dp = [e[d] * r[d] ** (e[d] - 1) if e[d] > 0 else 0.0 for d in range(3)]
+            ddp = [e[d] * (e[d] - 1) * r[d] ** (e[d] - 2) if e[d] > 1 else 0.0 for d in range(3)]
+            v += ck * p[0] * p[1] * p[2]
+            g += ck * np.array([dp[0] * p[1] * p[2], p[0] * dp[1] * p[2], p[0] * p[1] * dp[2]])
+            for i in range(3):
+                for j in range(3):
+                    f = [p[0], p[1], p[2]]
+                    if i == j:
+                        f[i] = ddp[i]
+                    else:
+                        f[i], f[j] = dp[i], dp[j]
+                    H[i, j] += ck * f[0] * f[1] * f[2]
+        gx = self.G.T @ g
+        Hx = self.G.T @ H @ self.G
+        return v, gx, np.array([Hx[0, 0], Hx[1, 1], Hx[2, 2], Hx[0, 1], Hx[0, 2], Hx[1, 2]])
+
+    def inside(self, x, eps=1e-10):
+        r = self.ref(x)
+        return r[0] >= -1 - eps and r[1] >= -1 - eps and r[2] >= -1 - eps and r.sum() <= -1 + eps
+
+
+def _solve4(A, b):
+    """newtoncp_gepp (ls_solver.cpp:259-295): Gaussian elimination with partial pivoting."""
+    A, b = A.copy(), b.copy()
+    for i in range(4):
+        j = i + int(np.argmax(np.abs(A[i:, i])))
+        if abs(A[j, i]) <= abs(A[i, i]):
+            j = i
+        if j != i:
+            A[[i, j]] = A[[j, i]]
+            b[[i, j]] = b[[j, i]]
+        if abs(A[i, i]) < 1.0e4 * np.finfo(float).eps:
+            return None
+        f = 1.0 / A[i, i]
+        A[i + 1:, i] *= f
+        for r in range(i + 1, 4):
+            A[r, i + 1:] -= A[r, i] * A[i, i + 1:]
+            b[r] -= A[r, i] * b[i]
+    for i in range(3, -1, -1):
+        b[i] = (b[i] - A[i, i + 1:] @ b[i + 1:]) / A[i, i]
+    return b
+
+
+def ls_reinit(mesh, p, s, ls_cap=1.0):
+    """The reinitialised level set (K, Np) of s (K, Np)."""
+    t = D.ref_tables(3, p)
+    e_x = mesh.export(p, t)
+    xyz = np.stack([e_x["x"], e_x["y"], e_x["z"]], -1)  # K x Np x 3
+    K, Np = s.shape
+    h = 1.0 / mesh.fscale[mesh.nbr >= 0].min()
+    tol = max(1e-18, 1e-4 * h * h)
+    polys, samples, scell = {}, [], []
+    cells = [e for e in range(K) if np.any((s[e] >= 0.0) != (s[e, 0] >= 0.0))]
+    for e in cells:
+        pol = _ElementPoly(t, mesh.G[e], xyz[e, 0], s[e])
+        polys[e] = pol
+        for j in range(Np):
+            x = pol.to_phys(0.75 * np.array([t["r"][j], t["s"][j], t["t"][j]]))
+            conv = False
+            for _ in range(100):
+                v, g, _h = pol.eval(x)
+                sq = g @ g
+                if sq > 1e-14:
+                    g = g * (v / sq)
+                x = x - g
+                if g @ g < tol:
+                    conv = True
+                    break
+            samples.append(x if conv and pol.inside(x) else np.full(3, np.nan))
+            scell.append(e)
+    out = np.where(s < 0.0, -ls_cap, ls_cap).astype(float)
+    if not samples:
+        return out
+    S = np.array(samples)
+    Sf = np.where(np.isnan(S), np.inf, S)
+    pts = xyz.reshape(-1, 3)
+    near = np.empty(len(pts), dtype=int)
+    for i0 in range(0, len(pts), 4096):
+        d2 = ((pts[i0:i0 + 4096, None, :] - Sf[None]) ** 2).sum(-1)
+        near[i0:i0 + 4096] = np.argmin(d2, axis=1)
+    valid = ~np.isnan(S[:, 0])
+    w = ls_cap + 2.0 * h
+    flat = s.reshape(-1)
+    res = out.reshape(-1)
+    for node in range(len(pts)):
+        first = node // Np * Np
+        b0, bi = near[first], near[node]
+        if not (valid[b0] and valid[bi]):
+            continue
+        d0 = ((S[b0] - pts[first]) ** 2).sum()
+        if d0 >= w * w:
+            continue
+        d1 = ((S[bi] - pts[node]) ** 2).sum()
+        pol = polys[scell[bi]]
+        nx = pts[node]
+        pt = S[bi].copy()
+        init = pt.copy()
+        lam, conv = 0.0, False
+        for step in range(50):
+            old = pt.copy()
+            v, g, hx = pol.eval(pt)
+            g2 = g @ g
+            if g2 < 1e-14:
+                break
+            if step == 0:
+                lam = ((nx - pt) @ g) / g2
+            f = np.array([*(pt - nx + lam * g), v])
+            H = np.array([[1 + lam * hx[0], lam * hx[3], lam * hx[4], g[0]],
+                          [lam * hx[3], 1 + lam * hx[1], lam * hx[5], g[1]],
+                          [lam * hx[4], lam * hx[5], 1 + lam * hx[2], g[2]],
+                          [g[0], g[1], g[2], 0.0]])
+            sol = _solve4(H, f)
+            if sol is None:
+                lam = ((nx - pt) @ g) / g2
+                d1v = (v / g2) * g
+                d2v = pt - nx + lam * g
+                m2 = d2v @ d2v
+                if m2 > 0.01 * h * h:
+                    d2v = d2v * (0.1 * h / np.sqrt(m2))
+                pt = pt - (d1v + d2v)
+            else:
+                m2 = sol[:3] @ sol[:3]
+                if m2 > 0.25 * h * h:
+                    sol = sol * (0.5 * h / np.sqrt(m2))
+                pt = pt - sol[:3]
+                lam -= sol[3]
+            if ((init - pt) ** 2).sum() > 2.25 * h * h:
+                pt = old
+                break
+            if ((old - pt) ** 2).sum() < 1e-24:
+                conv = True
+                break
+        dist2 = ((pt - nx) ** 2).sum() if conv else d1
+        res[node] = (-1.0 if flat[node] < 0.0 else 1.0) * np.sqrt(dist2)
+    return np.clip(res.reshape(K, Np), -ls_cap, ls_cap)

@@ -254,3 +254,31 @@ def test_two_phase_step_oracle_lifts_a_light_bubble():
     assert 0 < ups[0] < ups[1] < ups[2]
     assert st.vel[1][s > 0.1].mean() < 0
     assert st.time == pytest.approx(3 * st.dt)
+
+
+def _plane_distance(e, nrm=(0.3, 1.0, -0.2), y0=0.45):
+    n = np.asarray(nrm) / np.linalg.norm(nrm)
+    return n[0] * (e["x"] - 0.5) + n[1] * (e["y"] - y0) + n[2] * (e["z"] - 0.5)
+
+
+@pytest.mark.parametrize("p", [2, 3])
+def test_reinit_recovers_the_distance_to_a_plane(p):
+    """A linear level set is its own polynomial in every element: the closest points are
+    exact, so three times the distance comes back as the distance."""
+    mesh = D.Mesh.box(3, 3, 0.1, 5)
+    e = mesh.export(p, D.ref_tables(3, p))
+    dist = _plane_distance(e)
+    got = I.ls_reinit(mesh, p, 3.0 * dist)
+    assert np.abs(got - np.clip(dist, -1.0, 1.0)).max() < 1e-12
+
+
+def test_reinit_converges_to_the_distance_to_a_sphere():
+    errs = []
+    for n in (3, 5):
+        mesh = D.Mesh.box(3, n, 0.1, 5)
+        e = mesh.export(2, D.ref_tables(3, 2))
+        d = np.sqrt((e["x"] - 0.5) ** 2 + (e["y"] - 0.45) ** 2 + (e["z"] - 0.5) ** 2) - 0.3
+        got = I.ls_reinit(mesh, 2, 2.0 * d)
+        assert np.all(np.sign(got) == np.sign(d))
+        errs.append(np.abs(got - d)[np.abs(d) < 0.1].max())
+    assert errs[0] < 0.02 and errs[1] < errs[0] / 2

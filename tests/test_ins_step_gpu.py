@@ -1,7 +1,7 @@
 """The time-step kernels around the solves against the time-step oracle
 (oracle/ins_oracle.py, itself pinned against the reference's kernels in
-tests/test_ins_oracle.py): the fused non-linear advection step and the
-curl-curl pressure Neumann data."""
+tests/test_ins_oracle.py): the fused non-linear advection step, the curl-curl
+pressure Neumann data and the level-set reinitialisation."""
 import numpy as np
 import pytest
 
@@ -60,3 +60,27 @@ def test_pressure_neumann_data_vanish_without_walls():
     ones = np.ones((gm.K, Np))
     got = sipg.ins_pressure_neumann(gm, 2, 10.0, u, N, ones, ones, np.full(gm.Kb, 2, np.int32))
     assert not got.any()
+
+
+def _reinit_case(n, p):
+    gm = sipg.Mesh.box(3, n, jitter=0.1, seed=5)
+    om = D.Mesh.box(3, n, 0.1, 5)
+    e = om.export(p, D.ref_tables(3, p))
+    d = np.sqrt((e["x"] - 0.5) ** 2 + (e["y"] - 0.3) ** 2 + (e["z"] - 0.5) ** 2) - 0.25
+    return gm, om, e, 2.0 * d + 0.05 * np.sin(5.0 * e["x"]) * np.cos(3.0 * e["z"])
+
+
+@pytest.mark.parametrize("p", [2, 3])
+def test_reinit_matches_the_oracle(p):
+    gm, om, _, s = _reinit_case(3, p)
+    got = sipg.ls_reinit(gm, p, s)
+    want = I.ls_reinit(om, p, s)
+    assert rel_err(got, want) < 1e-9
+
+
+def test_reinit_recovers_the_distance_to_a_plane():
+    gm, om, e, _ = _reinit_case(4, 3)
+    nrm = np.array([0.3, 1.0, -0.2]) / np.linalg.norm([0.3, 1.0, -0.2])
+    dist = nrm[0] * (e["x"] - 0.5) + nrm[1] * (e["y"] - 0.45) + nrm[2] * (e["z"] - 0.5)
+    got = sipg.ls_reinit(gm, 3, 3.0 * dist)
+    assert np.abs(got - dist).max() < 1e-12
