@@ -35,7 +35,7 @@ void ls_props_device(sipg_mesh* m, int order, const LsFields& f, cudaStream_t s)
 
 // Work buffers of the level-set reinitialisation, kept across calls.
 struct ReinitWork {
-  DevBuf cells, count, samples, nearest, s_old;
+  DevBuf cells, count, samples, nearest, s_old, kept, flat;
 };
 
 // Closest-point reinitialisation of s (K x Np, in place): xyz the node coordinates

@@ -1,16 +1,17 @@
 // Level-set reinitialisation on the device: the closest-point reinitialisation of
 // LevelSetSolver3D::reinitLS (src/solvers/3d/ls_solver.cpp:719-860,
 // sampleInterface and the sampling Newton of src/solvers/3d/ls_solver_cpu.cpp:
-// 291-316, 318-487, the closest-point Newton of ls_solver.cpp:259-480), in five
-// launches:
+// 291-316, 318-487, the closest-point Newton of ls_solver.cpp:259-480), in four
+// launches and a host pass that keeps the converged samples:
 //   cells    the elements whose nodal values change sign (s >= 0 against s < 0);
 //   sample   Np points per such element, started at the reference nodes scaled by
 //            0.75, moved onto the zero set of the element's polynomial by the
 //            simplified Newton x -= s grad s / |grad s|^2 (100 steps, converged when
 //            the step^2 < max(1e-18, 1e-4 h^2)) and kept if converged inside the
 //            element;
-//   nearest  the closest sample to every node, by brute force over the samples
-//            staged through shared memory (the reference queries a KD-tree);
+//   nearest  the closest kept sample to every node, by brute force over the samples
+//            staged through shared memory, four nodes per thread (the reference
+//            queries a KD-tree);
 //   newton   from that sample, the Lagrange-multiplier Newton iteration for the
 //            closest point of the zero set of the sample element's polynomial (4 x 4
 //            pivoted solve, steps clamped to h / 2, a fall-back step when the system
@@ -133,6 +134,8 @@ struct ReinitArgs {
   int* cells;          // interface elements
   int* ncells;
   double* samples;     // ncells x Np x 3 (NaN: dropped)
+  const double* csamples;  // the kept samples, in order (x, y, z)
+  const int* cflat;        // their flat sample indices
   int* nearest;        // K x Np: flat sample index, or -1
   double h, ls_cap, tol;
   int K, Np, order;
@@ -297,33 +300,49 @@ __global__ void __launch_bounds__(kRThreads) k_reinit_sample(ReinitArgs a, int n
   }
 }
 
-// closest sample to every node (brute force, samples staged through shared memory)
-__global__ void __launch_bounds__(kRThreads) k_reinit_nearest(ReinitArgs a, int nsamples) {
+// closest kept sample to every node: brute force, the samples staged through shared
+// memory and compared against NPT nodes per thread; ties go to the first sample
+constexpr int kNpt = 4;
+__global__ void __launch_bounds__(kRThreads) k_reinit_nearest(ReinitArgs a, int nkept) {
   __shared__ double sx[kRThreads], sy[kRThreads], sz[kRThreads];
   const size_t n = (size_t)a.K * a.Np;
-  const size_t node = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  const bool act = node < n;
-  const double px = act ? a.xyz[node] : 0.0, py = act ? a.xyz[n + node] : 0.0, pz = act ? a.xyz[2 * n + node] : 0.0;
-  double best = INFINITY;
-  int bi = -1;
-  for (int s0 = 0; s0 < nsamples; s0 += kRThreads) {
+  const size_t node0 = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) * kNpt;
+  double px[kNpt], py[kNpt], pz[kNpt], best[kNpt];
+  int bi[kNpt];
+#pragma unroll
+  for (int q = 0; q < kNpt; ++q) {
+    const size_t node = node0 + q;
+    const bool act = node < n;
+    px[q] = act ? a.xyz[node] : 0.0;
+    py[q] = act ? a.xyz[n + node] : 0.0;
+    pz[q] = act ? a.xyz[2 * n + node] : 0.0;
+    best[q] = INFINITY;
+    bi[q] = -1;
+  }
+  for (int s0 = 0; s0 < nkept; s0 += kRThreads) {
     __syncthreads();
     const int sidx = s0 + threadIdx.x;
-    sx[threadIdx.x] = sidx < nsamples ? a.samples[(size_t)sidx * 3] : qnan();
-    sy[threadIdx.x] = sidx < nsamples ? a.samples[(size_t)sidx * 3 + 1] : qnan();
-    sz[threadIdx.x] = sidx < nsamples ? a.samples[(size_t)sidx * 3 + 2] : qnan();
+    sx[threadIdx.x] = sidx < nkept ? a.csamples[(size_t)sidx * 3] : 0.0;
+    sy[threadIdx.x] = sidx < nkept ? a.csamples[(size_t)sidx * 3 + 1] : 0.0;
+    sz[threadIdx.x] = sidx < nkept ? a.csamples[(size_t)sidx * 3 + 2] : 0.0;
     __syncthreads();
-    const int m = min(kRThreads, nsamples - s0);
+    const int m = min(kRThreads, nkept - s0);
     for (int k = 0; k < m; ++k) {
-      const double dx = sx[k] - px, dy = sy[k] - py, dz = sz[k] - pz;
-      const double d2 = dx * dx + dy * dy + dz * dz;
-      if (d2 < best) {  // NaN samples never compare smaller
-        best = d2;
-        bi = s0 + k;
+      const double qx = sx[k], qy = sy[k], qz = sz[k];
+#pragma unroll
+      for (int q = 0; q < kNpt; ++q) {
+        const double dx = qx - px[q], dy = qy - py[q], dz = qz - pz[q];
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        if (d2 < best[q]) {
+          best[q] = d2;
+          bi[q] = s0 + k;
+        }
       }
     }
   }
-  if (act) a.nearest[node] = bi;
+#pragma unroll
+  for (int q = 0; q < kNpt; ++q)
+    if (node0 + q < n) a.nearest[node0 + q] = bi[q] >= 0 ? a.cflat[bi[q]] : -1;
 }
 
 // 4 x 4 solve with partial pivoting; false when a pivot is below 1e4 machine epsilon
@@ -513,8 +532,30 @@ void ls_reinit_device(sipg_mesh* m, int order, const double* xyz, double* s, dou
     note_launch();
     SIPG_CUDA(cudaGetLastError());
   }
-  const int g3 = (int)((n + kRThreads - 1) / kRThreads);
-  k_reinit_nearest<<<g3, kRThreads, 0, st>>>(a, nsamples);
+  // keep the converged samples, in order (a host pass over the sample list)
+  std::vector<double> hs((size_t)nsamples * 3), kept;
+  std::vector<int> flat;
+  if (nsamples) {
+    SIPG_CUDA(cudaMemcpyAsync(hs.data(), w.samples.p, hs.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    SIPG_CUDA(cudaStreamSynchronize(st));
+  }
+  for (int i = 0; i < nsamples; ++i)
+    if (!std::isnan(hs[(size_t)i * 3])) {
+      kept.insert(kept.end(), hs.begin() + (size_t)i * 3, hs.begin() + (size_t)i * 3 + 3);
+      flat.push_back(i);
+    }
+  const int nkept = (int)flat.size();
+  ensure(w.kept, std::max<size_t>(1, kept.size()) * sizeof(double));
+  ensure(w.flat, std::max<size_t>(1, flat.size()) * sizeof(int));
+  if (nkept) {
+    w.kept.upload(kept.data(), kept.size() * sizeof(double), st);
+    w.flat.upload(flat.data(), flat.size() * sizeof(int), st);
+  }
+  a.csamples = w.kept.as<double>();
+  a.cflat = w.flat.as<int>();
+  const size_t nthreads = (n + kNpt - 1) / kNpt;
+  const int g3 = (int)((nthreads + kRThreads - 1) / kRThreads);
+  k_reinit_nearest<<<g3, kRThreads, 0, st>>>(a, nkept);
   note_launch();
   SIPG_CUDA(cudaGetLastError());
   const int g4 = (int)std::max<size_t>(1, std::min<size_t>((n + kRThreads - 1) / kRThreads, (size_t)num_sms() * 16));
