@@ -332,19 +332,27 @@ __global__ void __launch_bounds__(256, 2) k_bsr16(int K, const __half* __restric
 // smoother stores it: its symmetric part when sym (packed triangles,
 // k_block_pack_sym), else as is. C[s][r][c][e] = sum_m Bi_e[r][m] A[s][m][c][e],
 // one thread per (block entry, element), element fastest.
-__global__ void k_bsr_precond(const double* __restrict__ A, const double* __restrict__ binv, int K, int Np, int NS,
-                              int sym, double* __restrict__ C) {
-  const size_t K_ = (size_t)K, total = (size_t)NS * Np * Np * K_;
+// C = Bd^-1 A block by block: one thread per (element, row r, block s) holds row r of
+// the element's inverse diagonal block in registers (symmetrised when sym) and writes
+// the Np entries of row r of C's block s; the loads of A and the stores of C are
+// coalesced over the elements.
+template <int NP>
+__global__ void k_bsr_precond(const double* __restrict__ A, const double* __restrict__ binv, int K, int NS, int sym,
+                              double* __restrict__ C) {
+  const size_t K_ = (size_t)K, total = (size_t)NS * NP * K_;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
     const size_t e = i % K_, q = i / K_;
-    const int c = (int)(q % Np), r = (int)((q / Np) % Np), s = (int)(q / ((size_t)Np * Np));
-    const double* be = binv + e * Np * Np;
-    double acc = 0.0;
-    for (int m = 0; m < Np; ++m) {
-      const double b = sym ? 0.5 * (be[(size_t)r * Np + m] + be[(size_t)m * Np + r]) : be[(size_t)r * Np + m];
-      acc += b * A[(((size_t)s * Np + m) * Np + c) * K_ + e];
+    const int r = (int)(q % NP), s = (int)(q / NP);
+    const double* be = binv + e * NP * NP;
+    double b[NP];
+#pragma unroll
+    for (int m = 0; m < NP; ++m) b[m] = sym ? 0.5 * (be[r * NP + m] + be[m * NP + r]) : be[r * NP + m];
+    for (int c = 0; c < NP; ++c) {
+      double acc = 0.0;
+#pragma unroll
+      for (int m = 0; m < NP; ++m) acc += b[m] * A[(((size_t)s * NP + m) * NP + c) * K_ + e];
+      C[(((size_t)s * NP + r) * NP + c) * K_ + e] = acc;
     }
-    C[i] = acc;
   }
 }
 
@@ -445,9 +453,17 @@ void bsr_assemble(sipg_op* op, BsrOp& B, bool want32, cudaStream_t s, const doub
     if (binv_rows) {
       ensure(B.c64, nv * sizeof(double));
       DevBuf& c64 = B.c64;
-      k_bsr_precond<<<grid_of(nv), 256, 0, s>>>(B.v64.as<double>(), binv_rows, K, Np, NF + 1, binv_sym ? 1 : 0,
-                                                c64.as<double>());
+      const size_t nrows = (size_t)(NF + 1) * Np * K;
+      const int sy = binv_sym ? 1 : 0;
+      switch (Np) {  // the even orders that reach here: two rows per thread in k_bsr16
+        case 4: k_bsr_precond<4><<<grid_of(nrows), 256, 0, s>>>(B.v64.as<double>(), binv_rows, K, NF + 1, sy, c64.as<double>()); break;
+        case 6: k_bsr_precond<6><<<grid_of(nrows), 256, 0, s>>>(B.v64.as<double>(), binv_rows, K, NF + 1, sy, c64.as<double>()); break;
+        case 10: k_bsr_precond<10><<<grid_of(nrows), 256, 0, s>>>(B.v64.as<double>(), binv_rows, K, NF + 1, sy, c64.as<double>()); break;
+        case 20: k_bsr_precond<20><<<grid_of(nrows), 256, 0, s>>>(B.v64.as<double>(), binv_rows, K, NF + 1, sy, c64.as<double>()); break;
+        default: throw Error(SIPG_INVALID_ARG, "block-preconditioned assembled level: unsupported Np");
+      }
       note_launch();
+      SIPG_CUDA(cudaGetLastError());
       ensure(B.c16, nv * sizeof(__half));
       ensure(B.cscale16, (size_t)K * sizeof(float));
       k_bsr16_pack<<<grid_of(K), 256, 0, s>>>(c64.as<double>(), K, Np, NF + 1, B.c16.as<__half>(),
