@@ -380,8 +380,8 @@ int sipg_pressure_projection_host(sipg_mesh *m, int order, double dt, double fac
  *   rhs = J M ( -div_c(velT) / dt + LIFT (b0 dPdN + b1 dPdN_old) ),
  * div_c = sum_d d(u_d)/dx_d + LIFT (fscale n . (u+ - u-) / 2) over interior faces
  * (central flux; boundary faces add nothing). dPdN_old is updated in place. The
- * Neumann data dPdN (the curl-curl boundary term the caller assembles,
- * ins_3d_pr_0.h / mp_ins_3d_pr_0.h) and dPdN_old are K x (dim + 1) x Nfp in the
+ * Neumann data dPdN (the curl-curl boundary term of ins_3d_pr_0.h / mp_ins_3d_pr_0.h:
+ * sipg_ins_pressure_neumann in 3D, else the caller's) and dPdN_old are K x (dim + 1) x Nfp in the
  * face-node order of the reference's FMASK, or NULL (zero; dPdN_old NULL is not
  * written). velT: dim x K x Np; rhs: K x Np. The Dirichlet data of
  * ins_3d_pr_dirichlet enter through sipg_op_apply_bc_host as before. Device
@@ -422,7 +422,9 @@ int sipg_ins_advection_host(sipg_mesh *m, int order, double dt, double a0, doubl
  * apply_pressure_neumann_bc (src/solvers/3d/mp_ins_solver.cpp:450-493): on no-slip and
  * slip walls dPdN = fscale n . (-N - curl(mu curl u) / (Re rho)) at the face nodes
  * (mesh->curl, mp_ins_3d_pr_mu, mp_ins_3d_pr_0), zero on the other faces; the input
- * of sipg_pressure_rhs. vel, N: 3 x K x Np; mu, rho: K x Np; dPdN: K x 4 x Nfp. */
+ * of sipg_pressure_rhs. With mu = rho = 1 it is the single-phase INSSolver3D's
+ * ins_3d_pr_0 (src/kernels/ins_3d_pr_0.h). vel, N: 3 x K x Np; mu, rho: K x Np;
+ * dPdN: K x 4 x Nfp. */
 int sipg_ins_pressure_neumann(sipg_mesh *m, int order, double reynolds, const double *vel, const double *N,
                               const double *mu, const double *rho, const int *vel_bc, double *dPdN, void *stream);
 int sipg_ins_pressure_neumann_host(sipg_mesh *m, int order, double reynolds, const double *vel, const double *N,
