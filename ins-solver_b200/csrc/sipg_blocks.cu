@@ -11,7 +11,12 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <vector>
 
+#include "runtime.hpp"
 #include "sipg_blocks.cuh"
 #include "vecops.cuh"
 
@@ -101,7 +106,7 @@ __device__ __forceinline__ void block_outer(double (&acc)[16], const double* L, 
 }
 
 template <int DIM, int P>
-__global__ void __launch_bounds__(32 * BlockWarps<P>::W) block_kernel(BlockArgs a) {
+__global__ void __launch_bounds__(32 * BlockWarps<P>::W) block_kernel(BlockArgs a, const double* __restrict__ U) {
   using C = Cfg<DIM, P>;
   constexpr int NP = C::NP, NFP = C::NFP, NF = C::NF, LD = C::LD, NG = C::NG, NPP = NP * NP;
   constexpr int W = BlockWarps<P>::W;
@@ -137,6 +142,70 @@ __global__ void __launch_bounds__(32 * BlockWarps<P>::W) block_kernel(BlockArgs 
     for (int i = lane; i < NPP; i += 32) B[i] = 0.0;
     __syncwarp();
     const double J = g[DIM == 3 ? 9 : 4];
+    if (a.mode == BLOCK_DIAG_ONLY && !a.ref_volume) {
+      // the diagonal alone: J sum_l f_l sum_{r<=s} K_rs U_rs[i][l] for the volume, with
+      // K = G G^T and U_rs[i][l] = E_r[i][l] D_s[l][i] (+ the (s, r) term for r < s),
+      // E_r = D_r^T M; the face terms touch the face nodes only (MF is symmetric)
+      constexpr int NQ = DIM * (DIM + 1) / 2;
+      double Kq[NQ];
+      {
+        int q = 0;
+        for (int r = 0; r < DIM; ++r)
+          for (int s2 = r; s2 < DIM; ++s2, ++q) {
+            double v = 0.0;
+            for (int d = 0; d < DIM; ++d) v += g[r * DIM + d] * g[s2 * DIM + d];
+            Kq[q] = v;
+          }
+      }
+      double* out_base = a.out + (size_t)item * NP;
+      for (int i = lane; i < NP; i += 32) {
+        double dv = 0.0;
+        for (int l = 0; l < NP; ++l) {
+          double u = 0.0;
+#pragma unroll
+          for (int q = 0; q < NQ; ++q) u += Kq[q] * __ldg(U + ((size_t)q * NP + i) * NP + l);
+          dv += fac[l] * u;
+        }
+        dv *= J;
+        for (int f = 0; f < NF; ++f) {
+          const int nb = a.nbr[(size_t)e * NF + f];
+          double n[3], sJ;
+          face_normal_d<DIM>(g, f, n, &sJ);
+          double scale;
+          if (nb >= 0) {
+            scale = 0.5 * sJ;
+          } else {
+            const int b = -nb - 1;
+            bool all_slip = a.ncomp == DIM;
+            for (int k = 0; k < a.ncomp; ++k) all_slip = all_slip && a.bct[(size_t)k * a.Kb + b] == 2;
+            if (all_slip) scale = sJ * n[c] * n[c];
+            else if (a.bct[(size_t)c * a.Kb + b] == 0) scale = sJ;
+            else continue;  // Neumann
+          }
+          int aa = -1;
+          for (int k = 0; k < NFP; ++k)
+            if (fm[f * NFP + k] == i) aa = k;
+          if (aa < 0) continue;
+          double rf[3] = {0.0, 0.0, 0.0};
+          for (int rr = 0; rr < DIM; ++rr)
+            for (int d = 0; d < DIM; ++d) rf[rr] += n[d] * g[rr * DIM + d];
+          const double* mf = MF + f * NFP * NFP;
+          double s1 = 0.0;
+          for (int bb = 0; bb < NFP; ++bb) {
+            const int jn = fm[f * NFP + bb];
+            double xv = 0.0;
+            for (int rr = 0; rr < DIM; ++rr) xv += rf[rr] * Dm[rr * NP * LD + jn * LD + i];
+            s1 += mf[aa * NFP + bb] * (xv * fac[jn]);
+          }
+          dv -= 2.0 * scale * s1;
+          dv += scale * a.tau[(size_t)e * NF + f] * mf[aa * NFP + aa];
+        }
+        if (a.mm_mode != 0) dv += J * Mm[i * LD + i] * (a.mm_mode == 1 ? a.mm_scalar : a.mm[(size_t)e * NP + i]);
+        if (e == a.pin_elem && i == a.pin_node) dv = a.pin_scale;
+        out_base[i] = dv;
+      }
+      continue;
+    }
     // volume: sum_d J Dx_d^T M F Dx_d (fvmf_3d_op1.h / fvmf_3d_op1_diag.h); the operator's
     // form as outer products in 4 x 4 lane tiles, the reference's variants entry by entry
     if (!a.ref_volume) {
@@ -414,6 +483,41 @@ __global__ void __launch_bounds__(128) apply_bc_kernel(ApplyBcArgs a) {
     default: break;                                                \
   }
 
+// U_rs[i][l] = E_r[i][l] D_s[l][i] (+ E_s[i][l] D_r[l][i] for r < s), E_r = D_r^T M: the
+// volume diagonal's tables, per order (pairs r <= s in order), cached per device
+static const double* diag_tables(int dim, int order) {
+  static std::mutex mu;
+  static std::map<std::pair<int, int>, std::unique_ptr<DevBuf>> cache;
+  int dev = 0;
+  SIPG_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  auto& slot = cache[{dev, dim * 10 + order}];
+  if (slot) return slot->as<double>();
+  const RefElement& r = dev_ref(dim, order).ref;
+  const int Np = r.Np;
+  const std::vector<double>* D[3] = {&r.Dr, &r.Ds, &r.Dt};
+  std::vector<std::vector<double>> E(dim, std::vector<double>((size_t)Np * Np, 0.0));
+  for (int q = 0; q < dim; ++q)
+    for (int i = 0; i < Np; ++i)
+      for (int l = 0; l < Np; ++l) {
+        double v = 0.0;
+        for (int k = 0; k < Np; ++k) v += (*D[q])[(size_t)k * Np + i] * r.M[(size_t)k * Np + l];
+        E[q][(size_t)i * Np + l] = v;
+      }
+  std::vector<double> U;
+  for (int a = 0; a < dim; ++a)
+    for (int b = a; b < dim; ++b)
+      for (int i = 0; i < Np; ++i)
+        for (int l = 0; l < Np; ++l) {
+          double v = E[a][(size_t)i * Np + l] * (*D[b])[(size_t)l * Np + i];
+          if (b != a) v += E[b][(size_t)i * Np + l] * (*D[a])[(size_t)l * Np + i];
+          U.push_back(v);
+        }
+  slot = std::make_unique<DevBuf>(U.size() * sizeof(double));
+  slot->upload(U.data(), U.size() * sizeof(double));
+  return slot->as<double>();
+}
+
 cudaError_t launch_blocks(int dim, int order, const BlockArgs& a, cudaStream_t s) {
   int total = a.K * a.ncomp;
   if (total <= 0) return cudaSuccess;
@@ -424,7 +528,8 @@ cudaError_t launch_blocks(int dim, int order, const BlockArgs& a, cudaStream_t s
     cudaError_t err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return err;
     const int grid = std::max(1, std::min((total + W - 1) / W, 148 * 8));
-    k<<<grid, 32 * W, smem, s>>>(a);
+    const double* U = a.mode == BLOCK_DIAG_ONLY ? diag_tables(D, P) : nullptr;
+    k<<<grid, 32 * W, smem, s>>>(a, U);
     note_launch();
     return cudaGetLastError();
   });
