@@ -205,13 +205,19 @@ __global__ void __launch_bounds__(32 * OiTile<NP>::W) k_oi_blocks(OiArgs a) {
       for (int q0 = 0; q0 < nq; q0 += OI_QC) {
         const int nc = min(OI_QC, nq - q0);
         __syncwarp();
-        for (int idx = lane; idx < nc * DIM * S; idx += 32) {
-          const int i = idx % S, d = (idx / S) % DIM, qq = idx / (S * DIM);
-          double v = 0.0;
-          if (i < NP)
+        // each reference derivative is loaded once and serves the DIM physical ones
+        for (int idx = lane; idx < nc * S; idx += 32) {
+          const int i = idx % S, qq = idx / S;
+          double dr[DIM];
 #pragma unroll
-            for (int r = 0; r < DIM; ++r) v += g[r * DIM + d] * __ldg(a.vdphi + ((size_t)r * nq + q0 + qq) * NP + i);
-          Y[idx] = v;
+          for (int r = 0; r < DIM; ++r) dr[r] = i < NP ? __ldg(a.vdphi + ((size_t)r * nq + q0 + qq) * NP + i) : 0.0;
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) {
+            double v = 0.0;
+#pragma unroll
+            for (int r = 0; r < DIM; ++r) v += g[r * DIM + d] * dr[r];
+            Y[(qq * DIM + d) * S + i] = v;
+          }
         }
         for (int idx = lane; idx < nc * DIM; idx += 32) {
           const int qq = idx / DIM;
