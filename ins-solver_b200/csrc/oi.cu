@@ -170,7 +170,7 @@ __host__ __device__ size_t oi_warp_doubles(int nqs) {
 }
 
 template <int DIM, int NP>
-__global__ void __launch_bounds__(32 * OiTile<NP>::W) k_oi_blocks(OiArgs a) {
+__global__ void __launch_bounds__(32 * OiTile<NP>::W, OiTile<NP>::W == 4 ? 3 : 1) k_oi_blocks(OiArgs a) {
   constexpr int NF = DIM + 1, NG = DIM == 3 ? 10 : 5, S = OiTile<NP>::NPP4, NTI = OiTile<NP>::NTI;
   constexpr int NT = OiTile<NP>::NT, W = OiTile<NP>::W;
   extern __shared__ __align__(16) double sm[];
