@@ -284,6 +284,9 @@ int sipg_ins3d_create(sipg_mesh* m, const sipg_ins3d_opts* o, const int* vel_bc,
       throw Error(SIPG_INVALID_ARG, "ins3d constants must be positive");
     if (o->extrapolate_history < 0 || o->extrapolate_history > 8)
       throw Error(SIPG_INVALID_ARG, "extrapolate_history must be 0..8");
+    if (!(o->ls_cap > 0.0) || o->reinit_freq < 0) throw Error(SIPG_INVALID_ARG, "ls_cap > 0 and reinit_freq >= 0");
+    if (o->viscous_kind != SIPG_SOLVER_JACOBI && o->viscous_kind != SIPG_SOLVER_BLOCK_JACOBI)
+      throw Error(SIPG_INVALID_ARG, "viscous_kind must be SIPG_SOLVER_JACOBI or SIPG_SOLVER_BLOCK_JACOBI");
     bool dirichlet_pr = false;
     std::vector<int> prt(m->Kb), vst(m->Kb);
     for (int b = 0; b < m->Kb; ++b) {
@@ -319,7 +322,6 @@ int sipg_ins3d_create(sipg_mesh* m, const sipg_ins3d_opts* o, const int* vel_bc,
     ins->h = 1.0 / fmax_;
     ins->h_ls = 1.0 / fmin_;
     ins->alpha = o->ls_alpha / fmin_;
-    if (!(o->ls_cap > 0.0) || o->reinit_freq < 0) throw Error(SIPG_INVALID_ARG, "ls_cap > 0 and reinit_freq >= 0");
     SIPG_CUDA(cudaStreamCreateWithFlags(&ins->st, cudaStreamNonBlocking));
     const size_t nb = ins->n * sizeof(double), nf = (size_t)m->K * 4 * hm.Nfp * sizeof(double);
     for (int i = 0; i < 2; ++i) {
@@ -358,8 +360,6 @@ int sipg_ins3d_create(sipg_mesh* m, const sipg_ins3d_opts* o, const int* vel_bc,
     // viscosity: FactorMMPoissonMatrixFreeDiag3D + PETScJacobiSolver, one component at a time
     ok(sipg_op_create(m, o->order, 1, &ins->vop), "viscous operator");
     ok(sipg_op_set_bc_types(ins->vop, vst.data()), "viscous boundary types");
-    if (o->viscous_kind != SIPG_SOLVER_JACOBI && o->viscous_kind != SIPG_SOLVER_BLOCK_JACOBI)
-      throw Error(SIPG_INVALID_ARG, "viscous_kind must be SIPG_SOLVER_JACOBI or SIPG_SOLVER_BLOCK_JACOBI");
     sipg_solver_opts vo = o->viscous;
     ok(sipg_solver_create(ins->vop, o->viscous_kind, &vo, &ins->vsol), "viscous solver");
     *out = ins.release();
