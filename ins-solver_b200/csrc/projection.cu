@@ -600,37 +600,74 @@ __global__ void __launch_bounds__(kProjWarps * 32) k_pr_rhs(const PrRhsArgs a) {
           }
         }
       }
-#pragma unroll
-    for (int e = 0; e < E; ++e)
-      for (int m = lane; m < NF * NFP; m += 32) {
-        const int f = m / NFP, k = m - f * NFP;
-        double un = 0.0, dn = 0.0;
-        if (valid[e]) {
-          const int el = e0 + e;
-          const int nb = __ldg(a.nbr + (size_t)el * NF + f);
-          if (nb >= 0) {
-            const int code = (__ldg(a.fcode + el) >> (8 * f)) & 0xff;
-            const int fr = code & 3, sg = code >> 2;
-            const int nn = fmask[fr * NFP + npos[sg * NFP + k]], o = fmask[f * NFP + k];
-#pragma unroll
-            for (int d = 0; d < D; ++d) {
-              double v;  // fscale n_d of face f (the unnormalised outward normal)
-              if (D == 3)
-                v = f == 0 ? -G[e][2][d] : f == 1 ? -G[e][1][d] : f == 2 ? (G[e][0][d] + G[e][1][d]) + G[e][2][d]
-                                                                           : -G[e][0][d];
-              else
-                v = f == 0 ? -G[e][1][d] : f == 1 ? G[e][0][d] + G[e][1][d] : -G[e][0][d];
-              un += v * (0.5 * (__ldg(a.velT + d * n + (size_t)nb * NP + nn) -
-                                __ldg(a.velT + d * n + (size_t)el * NP + o)));
-            }
-          }
-          const size_t fi = (size_t)el * NF * NFP + m;
-          dn = (a.dPdN ? a.b0 * a.dPdN[fi] : 0.0) + (a.dPdN_old ? a.b1 * a.dPdN_old[fi] : 0.0);
-          if (a.dPdN_old) a.dPdN_old[fi] = dn;
-        }
-        sF1[(e * NF + f) * NFPE + k] = un;
-        sF2[(e * NF + f) * NFPE + k] = dn;
+    // face terms: the warp's neighbour indices and face codes first (one lane per
+    // element face), then every lane issues all of its face nodes' loads before it uses
+    // any of them (the neighbour's velocities wait on the neighbour index)
+    constexpr int NFN = NF * NFP, ITEMS = (E * NFN + 31) / 32;
+    int nbv = -1;
+    uint32_t codev = 0;
+    if (lane < E * NF) {
+      const int e = lane / NF, f = lane - (lane / NF) * NF;
+      if (e0 + e < a.K) {
+        nbv = __ldg(a.nbr + (size_t)(e0 + e) * NF + f);
+        codev = __ldg(a.fcode + e0 + e);
       }
+    }
+    double vP[ITEMS][D], vM[ITEMS][D], dnv[ITEMS];
+    int nbi[ITEMS];
+#pragma unroll
+    for (int u = 0; u < ITEMS; ++u) {
+      const int it = lane + 32 * u;
+      const int e = min(it / NFN, E - 1), m = it - (it / NFN) * NFN, f = m / NFP, k = m - f * NFP;
+      const bool act = it < E * NFN && e0 + e < a.K;
+      const int nb = __shfl_sync(0xffffffffu, nbv, e * NF + f);
+      const uint32_t code = __shfl_sync(0xffffffffu, codev, e * NF + f);
+      nbi[u] = act ? nb : -1;
+      dnv[u] = 0.0;
+#pragma unroll
+      for (int d = 0; d < D; ++d) vP[u][d] = vM[u][d] = 0.0;
+      if (act) {
+        const int el = e0 + e;
+        if (nb >= 0) {
+          const int cf = (code >> (8 * f)) & 0xff;
+          const int fr = cf & 3, sg = cf >> 2;
+          const int nn = fmask[fr * NFP + npos[sg * NFP + k]], o = fmask[f * NFP + k];
+#pragma unroll
+          for (int d = 0; d < D; ++d) {
+            vP[u][d] = __ldg(a.velT + d * n + (size_t)nb * NP + nn);
+            vM[u][d] = __ldg(a.velT + d * n + (size_t)el * NP + o);
+          }
+        }
+        const size_t fi = (size_t)el * NF * NFP + m;
+        dnv[u] = (a.dPdN ? a.b0 * a.dPdN[fi] : 0.0) + (a.dPdN_old ? a.b1 * a.dPdN_old[fi] : 0.0);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < ITEMS; ++u) {
+      const int it = lane + 32 * u;
+      if (it >= E * NFN) continue;
+      const int e = it / NFN, m = it - e * NFN, f = m / NFP, k = m - f * NFP;
+      double un = 0.0;
+      if (nbi[u] >= 0) {
+#pragma unroll
+        for (int ee = 0; ee < E; ++ee) {
+          if (ee != e) continue;
+#pragma unroll
+          for (int d = 0; d < D; ++d) {
+            double v;  // fscale n_d of face f (the unnormalised outward normal)
+            if (D == 3)
+              v = f == 0 ? -G[ee][2][d] : f == 1 ? -G[ee][1][d] : f == 2 ? (G[ee][0][d] + G[ee][1][d]) + G[ee][2][d]
+                                                                           : -G[ee][0][d];
+            else
+              v = f == 0 ? -G[ee][1][d] : f == 1 ? G[ee][0][d] + G[ee][1][d] : -G[ee][0][d];
+            un += v * (0.5 * (vP[u][d] - vM[u][d]));
+          }
+        }
+      }
+      if (e0 + e < a.K && a.dPdN_old) a.dPdN_old[(size_t)(e0 + e) * NF * NFP + m] = dnv[u];
+      sF1[(e * NF + f) * NFPE + k] = un;
+      sF2[(e * NF + f) * NFPE + k] = dnv[u];
+    }
     __syncwarp();
 #pragma unroll
     for (int u = 0; u < NPL; ++u) {
