@@ -229,7 +229,7 @@ class TwoPhaseStep:
     walls), the level-set step, then the time-step update. Solves run to rel_tol."""
 
     def __init__(self, mesh, p, vel_bc, reynolds, rho0, rho1, mu0, mu1, gravity=0.0, ls_alpha=24.0, cfl=1.0,
-                 history=3, rel_tol=1e-11, reinit_freq=24, reinit_ic=1, ls_cap=1.0):
+                 history=3, rel_tol=1e-11, reinit_freq=24, reinit_ic=1, ls_cap=1.0, over_int=False):
         self.mesh, self.p = mesh, p
         self.t = D.ref_tables(3, p)
         self.om = O.OMesh(self.t, mesh.export(p, self.t))
@@ -241,6 +241,7 @@ class TwoPhaseStep:
         self.re, self.rho0, self.rho1, self.mu0, self.mu1 = reynolds, rho0, rho1, mu0, mu1
         self.grav, self.cfl, self.history, self.rel_tol = gravity, cfl, history, rel_tol
         self.reinit_freq, self.reinit_ic, self.ls_cap = reinit_freq, reinit_ic, ls_cap
+        self.over_int = over_int
         fs = mesh.fscale[mesh.nbr >= 0]
         self.h = 1.0 / fs.max()
         self.alpha = ls_alpha / fs.min()
@@ -274,6 +275,30 @@ class TwoPhaseStep:
                           max_iter=20000, x0=x0[None], **kw)
         return x[0], info
 
+    def _solve_oi(self, rhs, x0):
+        """update_pressure_matrices_oi (mp_ins_solver.cpp:524-544): 1/rho of the level
+        set at the volume and surface cubature points (the element's interpolant of s
+        there), the over-integrated operator as the solve's operator (its nodal
+        projection for the Jacobi preconditioner only)."""
+        import oi_oracle as OI
+        m, t = self.mesh, self.t
+        e_x = m.export(self.p, t)
+        xyz = np.stack([e_x["x"], e_x["y"], e_x["z"]], -1)
+        xv, xs = OI.points(m, self.p)  # 3 x K x nq, 3 x K x Nf x nqs
+        K, nq = xv.shape[1], xv.shape[2]
+        Nf, nqs = xs.shape[2], xs.shape[3]
+        sv, ss = np.zeros((K, nq)), np.zeros((K, Nf, nqs))
+        for e in range(K):
+            pol = _ElementPoly(t, m.G[e], xyz[e, 0], self.s[e])
+            sv[e] = pol.value(xv[:, e].T)
+            ss[e] = pol.value(xs[:, e].reshape(3, -1).T).reshape(Nf, nqs)
+        rho_v, _ = ls_props(sv, self.alpha, self.rho0, self.rho1, self.mu0, self.mu1)
+        rho_s, _ = ls_props(ss, self.alpha, self.rho0, self.rho1, self.mu0, self.mu1)
+        fv, fs = 1.0 / rho_v, 1.0 / rho_s
+        cb = OI.outer_mult(m, self.p, fv, fs, self.pr_bct)
+        nodal = fv @ OI.projection(3, self.p).T
+        return self._solve(rhs, self.pr_bct, x0, factor=nodal, nullspace=self.nullspace, outer_mult=cb)
+
     def step(self):
         m, p, dt = self.mesh, self.p, self.dt
         N, velT = advection(m, p, dt, self.a0, self.a1, self.b0, self.b1, self.vel, self.vel_old, self.N_old,
@@ -284,7 +309,10 @@ class TwoPhaseStep:
             x0 = lagrange_extrapolate([h[0] for h in self.hist], [h[1] for h in self.hist], self.time + dt)
         else:
             x0 = self.pr
-        self.pr, self.pr_info = self._solve(rhs, self.pr_bct, x0, factor=1.0 / self.rho, nullspace=self.nullspace)
+        if self.over_int:
+            self.pr, self.pr_info = self._solve_oi(rhs, x0)
+        else:
+            self.pr, self.pr_info = self._solve(rhs, self.pr_bct, x0, factor=1.0 / self.rho, nullspace=self.nullspace)
         if self.history:
             self.hist = (self.hist + [(self.time + dt, self.pr.copy())])[-self.history:]
         dp = O.grad_central(self.om, self.pr) / self.rho[None]
@@ -332,6 +360,11 @@ class _ElementPoly:
 
     def ref(self, x):
         return self.r0 + self.G @ (np.asarray(x) - self.x0)
+
+    def value(self, x):
+        """Values at the physical points x (n x 3)."""
+        r = self.r0[None] + (np.asarray(x) - self.x0[None]) @ self.G.T
+        return sum(ck * r[:, 0] ** a * r[:, 1] ** b * r[:, 2] ** c for ck, (a, b, c) in zip(self.c, self.ex))
 
     def to_phys(self, r):
         return self.x0 + np.linalg.solve(self.G, np.asarray(r) - self.r0)

@@ -119,3 +119,23 @@ def test_block_jacobi_viscous_solves_give_the_jacobi_steps():
         iters.append(sum(info.vis_iters))
     assert rel_err(got[1]["vel"], got[0]["vel"]) < 1e-8
     assert iters[1] < iters[0]
+
+
+@pytest.mark.parametrize("open_top", [False, True], ids=["closed", "open-top"])
+def test_over_integrated_two_phase_steps_match_the_oracle(open_top):
+    """[pressure-solve] over_int = 1: 1/rho at the cubature points from the level set and
+    the over-integrated operator in the pressure solve, against the oracle's step with
+    its over-integrated operator (oracle/oi_oracle.py) as the solve's operator."""
+    gm, om, s, vel, vel_bc = _case(3, 2, open_top)
+    tol = dict(pr_rel_tol=1e-11, pr_abs_tol=1e-300, vis_rel_tol=1e-11, vis_abs_tol=1e-300)
+    ins = sipg.Ins3D(gm, vel_bc, order=2, precision=sipg.FP64, pr_over_int=1, **tol, **CONSTS)
+    ins.set_state(vel, s)
+    ref = I.TwoPhaseStep(om, 2, vel_bc, over_int=True, **CONSTS)
+    ref.set_state(vel, s)
+    for _ in range(2):
+        ins.step()
+        ref.step()
+    got = ins.state()
+    assert rel_err(got["vel"], ref.vel) < 1e-7
+    pg, pw = (got["pr"], ref.pr) if open_top else (_mean_free(got["pr"]), _mean_free(ref.pr))
+    assert rel_err(pg, pw) < 1e-7
