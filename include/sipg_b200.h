@@ -433,15 +433,16 @@ int sipg_ins_pressure_neumann_host(sipg_mesh *m, int order, double reynolds, con
 /* ---- two-phase time step: replaces MPINSSolver3D (src/solvers/3d/mp_ins_solver.cpp:
  * 182-285: init, step = advection, pressure, viscosity, surface) with its level set
  * (LevelSetSolver3D, src/solvers/3d/ls_solver.cpp:106-257) for problems with no-slip
- * walls and natural outflow, no surface tension, sub-cycling, filtering or shock
- * capturing. Every field stays on the device; a step runs
+ * and slip walls and natural outflow, no surface tension, sub-cycling, filtering or
+ * shock capturing. Every field stays on the device; a step runs
  *   advection     sipg_ins_advection's kernel, plus the body force;
  *   pressure      Neumann data (sipg_ins_pressure_neumann), right-hand side
  *                 (sipg_pressure_rhs), factor 1/rho, p-multigrid set-up and solve from
  *                 the extrapolated initial guess, sipg_pressure_projection;
  *   viscosity     sipg_viscous_rhs, factor mu and mass factor g0 Re rho / dt, set-up and
  *                 three Jacobi-PCG solves (FactorMMPoissonMatrixFreeDiag3D +
- *                 PETScJacobiSolver) with zero Dirichlet data on no-slip walls;
+ *                 PETScJacobiSolver) with zero Dirichlet data on no-slip walls, or with
+ *                 slip walls one solve of the vector operator (ViscousSolver3D);
  *   surface       the level-set advection (three Runge-Kutta stages), every reinit_freq
  *                 steps its reinitialisation (sipg_ls_reinit_host), then rho and mu;
  * then dt = cfl h / ((p+1)^2 max(1, max |u|)) (INSSolverBase3D::max_vel) and the second-
@@ -502,7 +503,10 @@ int sipg_ins3d_default_opts(sipg_ins3d_opts *o);
  * closest-point iteration on that element's polynomial, s = +-distance clamped to
  * +-ls_cap (ls_post_reinit). s: K x Np host array, in place. */
 int sipg_ls_reinit_host(sipg_mesh *m, int order, double ls_cap, double *s);
-/* vel_bc: Kb velocity boundary types (0 no-slip, 2 natural outflow). */
+/* vel_bc: Kb velocity boundary types (0 no-slip, 1 slip, 2 natural outflow). With a slip
+ * wall the three velocity components are solved together on the vector operator
+ * (uses_slip_bcs: FactorViscousMatrix3D + ViscousSolver3D, mp_ins_solver.cpp:95-110, 699-790;
+ * vis_iters then repeats the one solve's count). */
 int sipg_ins3d_create(sipg_mesh *m, const sipg_ins3d_opts *o, const int *vel_bc, sipg_ins3d **out);
 /* Initial velocity (3 x K x Np) and level set (K x Np), host arrays: the reference's
  * ps3d_set_ic / ps3d_set_surface callbacks evaluated by the caller. Sets time 0, the

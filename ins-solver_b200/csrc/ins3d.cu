@@ -69,7 +69,7 @@ struct sipg_ins3d {
   std::vector<int> hist_order;
   sipg_op *pop = nullptr, *vop = nullptr;
   sipg_solver *psol = nullptr, *vsol = nullptr;
-  int cur = 0;
+  int cur = 0, vcomp = 1;
   double time = 0.0, dt = 0.0, a0 = 1.0, a1 = 0.0, b0 = 1.0, b1 = 0.0, g0 = 1.0;
   double h = 0.0, alpha = 0.0, max_vel = 1.0;
   bool have_state = false;
@@ -195,8 +195,13 @@ struct sipg_ins3d {
     SIPG_CUDA(cudaStreamSynchronize(st));
     ok(sipg_solver_setup(vsol), "viscous set-up");
     sipg_solve_info vi[3]{};
-    for (int c = 0; c < 3; ++c)
-      solved(sipg_solver_solve(vsol, rhs.as<double>() + c * n, u_new + c * n, &vi[c]), "viscous solve", vi[c]);
+    if (vcomp == 3) {
+      solved(sipg_solver_solve(vsol, rhs.as<double>(), u_new, &vi[0]), "viscous solve", vi[0]);
+      vi[1] = vi[2] = vi[0];
+    } else {
+      for (int c = 0; c < 3; ++c)
+        solved(sipg_solver_solve(vsol, rhs.as<double>() + c * n, u_new + c * n, &vi[c]), "viscous solve", vi[c]);
+    }
     SIPG_CUDA(cudaEventRecord(t_vis.b, st));
     // surface (level set, then rho and mu)
     SIPG_CUDA(cudaEventRecord(t_surf.a, st));
@@ -287,19 +292,27 @@ int sipg_ins3d_create(sipg_mesh* m, const sipg_ins3d_opts* o, const int* vel_bc,
     if (!(o->ls_cap > 0.0) || o->reinit_freq < 0) throw Error(SIPG_INVALID_ARG, "ls_cap > 0 and reinit_freq >= 0");
     if (o->viscous_kind != SIPG_SOLVER_JACOBI && o->viscous_kind != SIPG_SOLVER_BLOCK_JACOBI)
       throw Error(SIPG_INVALID_ARG, "viscous_kind must be SIPG_SOLVER_JACOBI or SIPG_SOLVER_BLOCK_JACOBI");
-    bool dirichlet_pr = false;
-    std::vector<int> prt(m->Kb), vst(m->Kb);
+    bool dirichlet_pr = false, slip = false;
     for (int b = 0; b < m->Kb; ++b) {
-      if (vel_bc[b] == 0) {  // no-slip: pressure Neumann, velocity Dirichlet (ins_3d_pr_dirichlet, ins_3d_vis_x)
-        prt[b] = SIPG_BC_NEUMANN;
-        vst[b] = SIPG_BC_DIRICHLET;
-      } else if (vel_bc[b] == 2) {  // natural outflow: pressure Dirichlet 0, velocity Neumann
+      if (vel_bc[b] < 0 || vel_bc[b] > 2)
+        throw Error(SIPG_INVALID_ARG, "ins3d supports no-slip (0), slip (1) and natural outflow (2) boundaries");
+      slip = slip || vel_bc[b] == 1;
+    }
+    // with slip walls the viscous solve is the coupled vector one (uses_slip_bcs:
+    // FactorViscousMatrix3D + ViscousSolver3D), otherwise one component at a time
+    const int vcomp = slip ? 3 : 1;
+    std::vector<int> prt(m->Kb), vst((size_t)vcomp * m->Kb);
+    for (int b = 0; b < m->Kb; ++b) {
+      int vt;
+      if (vel_bc[b] == 2) {  // natural outflow: pressure Dirichlet 0, velocity Neumann (ins_3d_pr_dirichlet)
         prt[b] = SIPG_BC_DIRICHLET;
-        vst[b] = SIPG_BC_NEUMANN;
+        vt = SIPG_BC_NEUMANN;
         dirichlet_pr = true;
-      } else {
-        throw Error(SIPG_INVALID_ARG, "ins3d supports no-slip (0) and natural outflow (2) boundaries");
+      } else {  // walls: pressure Neumann; velocity Dirichlet 0 (no-slip) or slip (ins_3d_vis_x)
+        prt[b] = SIPG_BC_NEUMANN;
+        vt = vel_bc[b] == 0 ? SIPG_BC_DIRICHLET : SIPG_BC_SLIP;
       }
+      for (int c = 0; c < vcomp; ++c) vst[(size_t)c * m->Kb + b] = vt;
     }
     auto ins = std::make_unique<sipg_ins3d>();
     ins->m = m;
@@ -357,8 +370,10 @@ int sipg_ins3d_create(sipg_mesh* m, const sipg_ins3d_opts* o, const int* vel_bc,
       for (int l = 0; l < 4; ++l) po.orders[l] = l < o->order ? o->order - l : 0;
     }
     ok(sipg_solver_create(ins->pop, SIPG_SOLVER_PMULTIGRID, &po, &ins->psol), "pressure solver");
-    // viscosity: FactorMMPoissonMatrixFreeDiag3D + PETScJacobiSolver, one component at a time
-    ok(sipg_op_create(m, o->order, 1, &ins->vop), "viscous operator");
+    // viscosity: FactorMMPoissonMatrixFreeDiag3D + PETScJacobiSolver, one component at a
+    // time, or with slip walls FactorViscousMatrix3D + ViscousSolver3D on (u, v, w)
+    ins->vcomp = vcomp;
+    ok(sipg_op_create(m, o->order, vcomp, &ins->vop), "viscous operator");
     ok(sipg_op_set_bc_types(ins->vop, vst.data()), "viscous boundary types");
     sipg_solver_opts vo = o->viscous;
     ok(sipg_solver_create(ins->vop, o->viscous_kind, &vo, &ins->vsol), "viscous solver");

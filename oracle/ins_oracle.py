@@ -234,9 +234,13 @@ class TwoPhaseStep:
         self.t = D.ref_tables(3, p)
         self.om = O.OMesh(self.t, mesh.export(p, self.t))
         self.vel_bc = np.asarray(vel_bc, np.int32).reshape(-1)
-        assert np.all((self.vel_bc == BC_NO_SLIP) | (self.vel_bc == BC_OUTFLOW))
-        self.pr_bct = np.where(self.vel_bc == BC_NO_SLIP, 1, 0).astype(np.int32)  # Neumann / Dirichlet
-        self.vis_bct = np.where(self.vel_bc == BC_NO_SLIP, 0, 1).astype(np.int32)
+        assert np.all((self.vel_bc >= BC_NO_SLIP) & (self.vel_bc <= BC_OUTFLOW))
+        self.pr_bct = np.where(self.vel_bc == BC_OUTFLOW, 0, 1).astype(np.int32)  # Dirichlet / Neumann
+        # velocity: Dirichlet 0 on no-slip walls, slip, Neumann on outflow; with a slip wall
+        # the three components are one vector solve (uses_slip_bcs, ViscousSolver3D)
+        self.slip = bool(np.any(self.vel_bc == BC_SLIP))
+        vt = np.select([self.vel_bc == BC_NO_SLIP, self.vel_bc == BC_SLIP], [0, 2], 1).astype(np.int32)
+        self.vis_bct = np.repeat(vt[None], 3, axis=0) if self.slip else vt
         self.nullspace = int(np.all(self.pr_bct == 1))
         self.re, self.rho0, self.rho1, self.mu0, self.mu1 = reynolds, rho0, rho1, mu0, mu1
         self.grav, self.cfl, self.history, self.rel_tol = gravity, cfl, history, rel_tol
@@ -320,9 +324,14 @@ class TwoPhaseStep:
         M, J = self.t["M"], m.J
         mmf = self.g0 * self.re / dt * self.rho
         vel_new = np.zeros_like(self.vel)
-        for c in range(3):
-            b = J[:, None] * ((self.re / dt * self.rho * velTT[c]) @ M.T)
-            vel_new[c], _ = self._solve(b, self.vis_bct, self.vel_old[c], factor=self.mu, mm=mmf)
+        b = np.stack([J[:, None] * ((self.re / dt * self.rho * velTT[c]) @ M.T) for c in range(3)])
+        if self.slip:
+            x, _ = O.solve(self.om, b, self.vis_bct, precond=O.PRE_JACOBI, rel_tol=self.rel_tol, abs_tol=1e-300,
+                           max_iter=20000, x0=self.vel_old, factor=self.mu, mm=mmf)
+            vel_new[:] = x
+        else:
+            for c in range(3):
+                vel_new[c], _ = self._solve(b[c], self.vis_bct, self.vel_old[c], factor=self.mu, mm=mmf)
         self.s = ls_advect(m, p, dt, self.s, vel_new, self.vel_bc)
         self.reinit_counter += 1
         if self.reinit_freq > 0 and self.reinit_counter >= self.reinit_freq:

@@ -37,8 +37,8 @@ def test_bad_options_are_refused(bad):
     assert st == sipg.SIPG_INVALID_ARG and not h.value
 
 
-def test_slip_walls_are_refused_by_the_scalar_viscous_driver():
+def test_unknown_boundary_types_are_refused():
     mesh = sipg.Mesh.box(3, 2, jitter=0.1, seed=1)
-    bc = np.ones(mesh.Kb, np.int32)  # slip
+    bc = np.full(mesh.Kb, 3, np.int32)  # a custom type of problem_specific_3d.h
     with pytest.raises(sipg.SipgError, match="no-slip"):
         sipg.Ins3D(mesh, bc)
