@@ -644,36 +644,36 @@ __global__ void __launch_bounds__(128) k_inv_mass_n(T* __restrict__ y, const T* 
 // (a singular one is shifted first), so every pivot block is.
 constexpr int GJB = 32;
 
-// P = A_KK^-1 by scalar Gauss-Jordan in shared memory (one block); P is GJB x GJB.
-__global__ void __launch_bounds__(256) k_gjb_pivot(const double* __restrict__ a, int n, int k0, int bs,
-                                                   double* __restrict__ P) {
-  __shared__ double sa[GJB][GJB + 1];
-  for (int t = threadIdx.x; t < bs * bs; t += blockDim.x) {
-    const int i = t / bs, j = t - (t / bs) * bs;
-    sa[i][j] = a[(size_t)(k0 + i) * n + k0 + j];
-  }
-  __syncthreads();
-  for (int k = 0; k < bs; ++k) {
-    const double r = 1.0 / sa[k][k];
-    __syncthreads();
-    for (int j = threadIdx.x; j < bs; j += blockDim.x)
-      if (j != k) sa[k][j] *= r;
-    __syncthreads();
-    for (int t = threadIdx.x; t < bs * bs; t += blockDim.x) {
-      const int i = t / bs, j = t - (t / bs) * bs;
-      if (i != k && j != k) sa[i][j] -= sa[i][k] * sa[k][j];
+// P = A_KK^-1 by scalar Gauss-Jordan in one warp: lane i holds row i of the pivot block
+// in registers and the pivot row reaches every lane by shuffles (no barriers); P is
+// GJB x GJB (GJB = 32, one row per lane), zero outside the bs x bs block.
+static_assert(GJB == 32, "one pivot-block row per lane");
+__global__ void __launch_bounds__(32) k_gjb_pivot(const double* __restrict__ a, int n, int k0, int bs,
+                                                  double* __restrict__ P) {
+  const int i = threadIdx.x;
+  double row[GJB];
+#pragma unroll
+  for (int j = 0; j < GJB; ++j) row[j] = (i < bs && j < bs) ? a[(size_t)(k0 + i) * n + k0 + j] : 0.0;
+#pragma unroll
+  for (int k = 0; k < GJB; ++k) {
+    if (k >= bs) break;  // uniform across the warp
+    const double r = 1.0 / __shfl_sync(0xffffffffu, row[k], k);
+    // the pivot row scaled by r (its column k stays until the column step)
+    if (i == k) {
+#pragma unroll
+      for (int j = 0; j < GJB; ++j)
+        if (j != k) row[j] *= r;
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < bs; i += blockDim.x) {
-      if (i != k) sa[i][k] *= -r;
-      else sa[k][k] = r;
+    const double aik = row[k];
+#pragma unroll
+    for (int j = 0; j < GJB; ++j) {
+      const double akj = __shfl_sync(0xffffffffu, row[j], k);
+      if (i != k && j != k) row[j] -= aik * akj;
     }
-    __syncthreads();
+    row[k] = i == k ? r : row[k] * -r;
   }
-  for (int t = threadIdx.x; t < GJB * GJB; t += blockDim.x) {
-    const int i = t / GJB, j = t % GJB;
-    P[t] = (i < bs && j < bs) ? sa[i][j] : 0.0;
-  }
+#pragma unroll
+  for (int j = 0; j < GJB; ++j) P[i * GJB + j] = (i < bs && j < bs) ? row[j] : 0.0;
 }
 
 // Row panel: one thread per column j outside K.
@@ -1228,7 +1228,7 @@ void dense_inverse_device(double* a, int n, bool project_constants, double* work
   const int tiles = (n + 63) / 64;
   for (int k0 = 0; k0 < n; k0 += GJB) {
     const int bs = std::min(GJB, n - k0);
-    k_gjb_pivot<<<1, 256, 0, s>>>(a, n, k0, bs, P);
+    k_gjb_pivot<<<1, 32, 0, s>>>(a, n, k0, bs, P);
     k_gjb_row<<<(n + 255) / 256, 256, 0, s>>>(a, n, k0, bs, P);
     k_gjb_update<<<dim3(tiles, tiles), 256, 0, s>>>(a, n, k0, bs);
     k_gjb_col<<<(n + 127) / 128, 128, 0, s>>>(a, n, k0, bs, P);
