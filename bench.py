@@ -189,6 +189,36 @@ def time_apply(op, precision, K, Np, iters=30):
     return e0.elapsed_time(e1) / iters
 
 
+def geometry_precision_c3(h, op64ref, reps=20):
+    """C3's comparison of the FP32 apply with FP32 and with BF16 geometric factors
+    against the FP64 apply: relative L2 error of y = A x for the workload's x, and the
+    FP32 apply time with BF16 factors (their bytes are stored in FP32 words: the apply
+    is issue-bound, so the storage would not change its time)."""
+    import torch
+    x64 = torch.from_numpy(h["x"].reshape(-1)).cuda()
+    K, Np = h["mesh"].K, op64ref.Np
+
+    def apply(op, prec):
+        x = x64 if prec == sipg.FP64 else x64.float()
+        y = torch.empty_like(x)
+        op.apply_device(prec, x.data_ptr(), y.data_ptr())
+        torch.cuda.synchronize()
+        return y.double()
+
+    ref = apply(op64ref, sipg.FP64)
+    err = lambda y: float(torch.linalg.norm(y - ref) / torch.linalg.norm(ref))
+    e32 = err(apply(op64ref, sipg.FP32))
+    hb = W.helmholtz3d(48, order=4, geometry_bits=16)
+    opb = sipg.Operator(hb["mesh"], 4, 1)
+    opb.set_bc_types(hb["bc_types"])
+    opb.set_mm(sipg.MM_SCALAR, hb["mm"])
+    eb = err(apply(opb, sipg.FP32))
+    tb = time_apply(opb, sipg.FP32, K, Np, reps)
+    return {"fp32_geometry_rel_l2": e32, "bf16_geometry_rel_l2": eb, "bf16_geometry_fp32_ms": tb,
+            "what": "FP32 (TF32 tensor-core) apply against the FP64 apply, geometric factors in FP32 "
+                    "and rounded to BF16"}
+
+
 def c3_solve(op, c, n, reps=3):
     """FP64 CG on the C3 Helmholtz operator preconditioned with (c M)^-1
     (PETScInvMassSolver::setFactor(1/c)) to a relative residual of 1e-8, from
@@ -324,6 +354,22 @@ def run_two_phase(steps=TWO_PHASE_STEPS):
             "mixed_vs_fp64": {"velocity_rel_l2": rel(b["vel"], a["vel"]), "level_set_rel_l2": rel(b["s"], a["s"]),
                               "pressure_rel_l2": rel(b["pr"] - b["pr"].mean(), a["pr"] - a["pr"].mean())},
             "mean_v_in_bubble_fp64": up}
+
+
+def run_geometry_bf16(steps=5, warmup=3):
+    """The headline mixed solve with the FP32 kernels' geometric factors in BF16 (the
+    V-cycle's p = 3 applies read them; the outer FP64 operator keeps FP64 factors)."""
+    import torch
+    c = W.poisson3d_two_phase(N_HEAD, order=ORDER, n_modes=256, pin=False, geometry_bits=16)
+    op = sipg.Operator(c["mesh"], ORDER, 1)
+    op.set_bc_types(c["bc_types"])
+    op.set_factor(c["factor"])
+    s, _ = pmg_solver(op, sipg.FP32)
+    b = torch.from_numpy(c["rhs"].reshape(-1)).cuda()
+    x = torch.zeros_like(b)
+    ms, infos = time_solves(s, b, x, steps, warmup)
+    return {"workload": "the headline problem, FP32 geometric factors rounded to BF16", "ms_per_solve": float(np.mean(ms)),
+            "iters": int(infos[-1].iters), "true_rel_res": float(infos[-1].true_rel_res)}
 
 
 def run_over_integrated(c, steps=5, warmup=3):
@@ -510,7 +556,8 @@ def run_ours(args):
                                  "traffic": tpe * K4 if tpe else None, "bytes_per_elem": b4,
                                  "traffic_source": "profiles/apply_tc_fp32_p4_40cube.txt (40^3x6 capture, "
                                                    "per-element traffic scaled to 663,552 elements)"},
-                    "inv_mass_pcg": c3_solve(op4, h["mm"], K4 * Np4)}
+                    "inv_mass_pcg": c3_solve(op4, h["mm"], K4 * Np4),
+                    "geometry_precision": geometry_precision_c3(h, op4)}
     lat = np.array(ms32)
     out = {
         "metric": METRIC,
@@ -554,6 +601,7 @@ def run_ours(args):
         "clocks": clk.summary(),
     }
     out["over_integrated"] = run_over_integrated(c)
+    out["geometry_bf16"] = run_geometry_bf16()
     out["viscous"] = run_viscous()
     if not args.skip_two_phase and world == 1:
         out["two_phase_step"] = run_two_phase(args.two_phase_steps)

@@ -78,6 +78,12 @@ int sipg_mesh_export(const sipg_mesh *m, int order, double *geof, double *nx, do
                      int *fmaskL, int *fmaskR, int *bface2cell, int *bfaceNum,
                      double *bface_centroid, double *x, double *y, double *z);
 int sipg_mesh_device_bytes(const sipg_mesh *m, size_t *bytes);
+/* Precision of the geometric factors the FP32 kernels read (no reference counterpart:
+ * the reference's geometric factors are DG_FP): 32 (default) or 16, the FP32 factors and
+ * the tensor-core geometry blocks derived from them rounded to BF16 (ties to even,
+ * stored in FP32 words); the FP64 kernels keep FP64 factors. Call before the mesh's
+ * first device use (SIPG_INVALID_ARG after). */
+int sipg_mesh_set_geometry_precision(sipg_mesh *m, int bits);
 void sipg_mesh_destroy(sipg_mesh *m);
 
 /* ---- operator: replaces PoissonMatrixFreeDiag3D / FactorPoissonMatrixFreeDiag3D /

@@ -147,12 +147,29 @@ const Mesh& sipg_mesh::host_order(int order) {
   return res.first->second;
 }
 
+namespace {
+// v rounded to the nearest BF16 value (ties to even), kept in an FP32 word
+float bf16_round(float v) {
+  uint32_t u;
+  std::memcpy(&u, &v, sizeof(u));
+  if ((u & 0x7f800000u) != 0x7f800000u) {  // finite
+    u += 0x7fffu + ((u >> 16) & 1u);
+    u &= 0xffff0000u;
+  }
+  float r;
+  std::memcpy(&r, &u, sizeof(r));
+  return r;
+}
+}  // namespace
+
 void sipg_mesh::ensure_device() {
   std::lock_guard<std::mutex> lk(dev_mu);
   if (device_ready) return;
   const Mesh& h = host_order(1);
   const int Nf = dim + 1, ng = h.ngeof();
   std::vector<float> g32(h.geof.begin(), h.geof.end());
+  if (geom_bf16)
+    for (float& v : g32) v = bf16_round(v);
   std::vector<uint32_t> code(K, 0);
   for (int e = 0; e < K; ++e)
     for (int f = 0; f < Nf; ++f) {
@@ -180,6 +197,12 @@ void sipg_mesh::ensure_device() {
   SIPG_CUDA(launch_tc_geom<double>(dim, geof64.as<double>(), K, tcg64.as<double>(), 0));
   SIPG_CUDA(launch_tc_geom<float>(dim, geof32.as<float>(), K, tcg32.as<float>(), 0));
   SIPG_CUDA(cudaDeviceSynchronize());
+  if (geom_bf16) {  // the derived geometry blocks are stored at the same precision
+    std::vector<float> t(tc_geom_values<float>(dim, K));
+    SIPG_CUDA(cudaMemcpy(t.data(), tcg32.p, t.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    for (float& v : t) v = bf16_round(v);
+    tcg32.upload(t.data(), t.size() * sizeof(float));
+  }
   device_ready = true;
 }
 
@@ -438,6 +461,15 @@ int sipg_box_mesh(int dim, int n, double jitter, uint64_t seed, double* vx, int*
     box_mesh(dim, n, jitter, seed, v, c);
     std::copy(v.begin(), v.end(), vx);
     std::copy(c.begin(), c.end(), e2v);
+  });
+}
+
+int sipg_mesh_set_geometry_precision(sipg_mesh* m, int bits) {
+  return guarded([&] {
+    if (!m || (bits != 16 && bits != 32)) throw Error(SIPG_INVALID_ARG, "geometry precision: 16 or 32 bits");
+    std::lock_guard<std::mutex> lk(m->dev_mu);
+    if (m->device_ready) throw Error(SIPG_INVALID_ARG, "geometry precision: set it before the mesh's first device use");
+    m->geom_bf16 = bits == 16;
   });
 }
 

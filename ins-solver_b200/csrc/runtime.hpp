@@ -78,6 +78,7 @@ struct sipg_mesh {
   sipg::DevBuf proj_io;       // velocity projection: device copies for the host-buffer entry point
   std::mutex proj_mu;         // serialises host-buffer projections on this mesh
   int n_belem = 0;
+  bool geom_bf16 = false;  // FP32 geometric data rounded to BF16 (sipg_mesh_set_geometry_precision)
   bool device_ready = false;
   std::mutex dev_mu;
   const sipg::Mesh& host_order(int order);

@@ -185,9 +185,17 @@ class Mesh:
         self.K, self.F, self.Kb = K.value, F.value, Kb.value
 
     @classmethod
-    def box(cls, dim, n, jitter=0.0, seed=0):
+    def box(cls, dim, n, jitter=0.0, seed=0, geometry_bits=32):
         vx, e2v = box_mesh(dim, n, jitter, seed)
-        return cls(dim, vx, e2v)
+        m = cls(dim, vx, e2v)
+        if geometry_bits != 32:
+            m.set_geometry_precision(geometry_bits)
+        return m
+
+    def set_geometry_precision(self, bits):
+        """Geometric factors of the FP32 kernels in BF16 (16) or FP32 (32), before the
+        mesh's first device use (sipg_mesh_set_geometry_precision)."""
+        check(lib().sipg_mesh_set_geometry_precision(self.h, bits))
 
     def export(self, order):
         """Per-order host data in the reference's form (dict of numpy arrays)."""

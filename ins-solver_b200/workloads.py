@@ -40,10 +40,11 @@ def two_phase_rho(x, y, z, h, ratio=1000.0, radius=0.25, center=(0.5, 0.5, 0.5),
     return 1.0 + (ratio - 1.0) * 0.5 * (1.0 + np.tanh((radius - r) / (width * h)))
 
 
-def poisson3d_two_phase(n, order=3, jitter=0.1, seed=20261203, rhs_seed=7, n_modes=256, pin=True):
+def poisson3d_two_phase(n, order=3, jitter=0.1, seed=20261203, rhs_seed=7, n_modes=256, pin=True, geometry_bits=32):
     """The 3D variable-density Poisson configuration on an n^3 x 6 tet box.
-    Returns dict(mesh, export, tables, factor, rhs, bc_types, pin)."""
-    mesh = sipg.Mesh.box(3, n, jitter=jitter, seed=seed)
+    Returns dict(mesh, export, tables, factor, rhs, bc_types, pin); geometry_bits 16: the
+    FP32 kernels' geometric factors in BF16."""
+    mesh = sipg.Mesh.box(3, n, jitter=jitter, seed=seed, geometry_bits=geometry_bits)
     e = mesh.export(order)
     t = sipg.ref_tables(3, order)
     h = 1.0 / n
@@ -115,9 +116,10 @@ def poisson2d_manufactured(n, order=3):
     return dict(mesh=mesh, export=e, tables=t, rhs=b[None], exact=exact[None], bc_types=bct)
 
 
-def helmholtz3d(n, order=4, nu=1e-3, dt=1e-3, seed=11, jitter=0.1):
-    """3D Helmholtz (I/(nu dt) - Laplacian) with Dirichlet walls, random input U(-1,1)."""
-    mesh = sipg.Mesh.box(3, n, jitter=jitter, seed=20261203)
+def helmholtz3d(n, order=4, nu=1e-3, dt=1e-3, seed=11, jitter=0.1, geometry_bits=32):
+    """3D Helmholtz (I/(nu dt) - Laplacian) with Dirichlet walls, random input U(-1,1);
+    geometry_bits 16: the FP32 kernels' geometric factors in BF16."""
+    mesh = sipg.Mesh.box(3, n, jitter=jitter, seed=20261203, geometry_bits=geometry_bits)
     Np = sipg.ref_sizes(3, order)[0]
     rng = np.random.default_rng(seed)
     x = rng.uniform(-1.0, 1.0, (1, mesh.K, Np))

@@ -110,3 +110,29 @@ def test_neumann_operator_annihilates_constants():
     op = make_op(mesh, 2, 1, f, bct=bct)
     y = op.apply_host(np.ones_like(x))
     assert np.abs(y).max() < 1e-11
+
+
+def test_bf16_geometric_factors_cost_three_digits_of_the_fp32_apply():
+    """sipg_mesh_set_geometry_precision(16): the FP32 kernels read BF16-rounded
+    geometric factors; the FP64 apply is unchanged, the FP32 one moves by about the
+    BF16 rounding (2^-9) of the factors, far above TF32's own error."""
+    import numpy as np
+    from helpers import rel_err
+    rng = np.random.default_rng(3)
+    m32 = sipg.Mesh.box(3, 4, jitter=0.1, seed=9)
+    m16 = sipg.Mesh.box(3, 4, jitter=0.1, seed=9, geometry_bits=16)
+    Np = sipg.ref_sizes(3, 3)[0]
+    x = rng.uniform(-1, 1, (1, m32.K, Np))
+    f = rng.uniform(0.5, 2.0, (m32.K, Np))
+    ys = {}
+    for name, m in (("32", m32), ("16", m16)):
+        op = sipg.Operator(m, 3, 1)
+        op.set_factor(f)
+        ys[name + "_64"] = op.apply_host(x)
+        xd = sipg.DeviceVector(x.reshape(-1).astype(np.float32))
+        yd = sipg.DeviceVector(np.zeros(x.size, np.float32))
+        op.apply_device(sipg.FP32, xd.ptr, yd.ptr)
+        ys[name + "_32"] = yd.get().reshape(x.shape).astype(np.float64)
+    assert rel_err(ys["16_64"], ys["32_64"]) < 1e-14
+    e32, e16 = rel_err(ys["32_32"], ys["32_64"]), rel_err(ys["16_32"], ys["32_64"])
+    assert e32 < 2e-3 and 5e-4 < e16 < 2e-2 and e16 > e32

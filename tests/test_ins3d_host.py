@@ -42,3 +42,11 @@ def test_unknown_boundary_types_are_refused():
     bc = np.full(mesh.Kb, 3, np.int32)  # a custom type of problem_specific_3d.h
     with pytest.raises(sipg.SipgError, match="no-slip"):
         sipg.Ins3D(mesh, bc)
+
+
+def test_geometry_precision_is_16_or_32_bits():
+    mesh = sipg.Mesh.box(3, 2, jitter=0.1, seed=1)
+    mesh.set_geometry_precision(16)
+    mesh.set_geometry_precision(32)
+    with pytest.raises(sipg.SipgError, match="16 or 32"):
+        mesh.set_geometry_precision(8)
