@@ -476,6 +476,12 @@ typedef struct {
                                 (24); 0: never */
   int reinit_ic;             /* level-set-options reinit_ic: reinitialise the initial level set (1) */
   double ls_cap;             /* LS_CAP of problem_specific_3d.h (1): the reinitialised level set's bound */
+  int pr_setup_every;        /* the pressure p-multigrid set up again every this many steps (1,
+                                the reference's update_pressure_matrices every step); between
+                                set-ups the outer operator (and in nodal mode the finest
+                                level) takes the new factor while the smoother blocks,
+                                eigenvalue bounds and coarse levels lag: a fixed
+                                preconditioner per solve, the same tolerance */
   int viscous_kind;          /* [viscous-solve] preconditioner: SIPG_SOLVER_JACOBI (default,
                                 PETScJacobiSolver) or SIPG_SOLVER_BLOCK_JACOBI
                                 (PETScBlockJacobiSolver, mp_ins_solver.cpp:113-121) */

@@ -70,6 +70,7 @@ struct sipg_ins3d {
   sipg_op *pop = nullptr, *vop = nullptr;
   sipg_solver *psol = nullptr, *vsol = nullptr;
   int cur = 0, vcomp = 1;
+  long long pr_setups = 0;  // pressure steps since set_state (the set-up runs every pr_setup_every)
   double time = 0.0, dt = 0.0, a0 = 1.0, a1 = 0.0, b0 = 1.0, b1 = 0.0, g0 = 1.0;
   double h = 0.0, alpha = 0.0, max_vel = 1.0;
   bool have_state = false;
@@ -176,7 +177,7 @@ struct sipg_ins3d {
       set_factor_device(pop, rrho.as<double>(), st);
     pressure_guess();
     SIPG_CUDA(cudaStreamSynchronize(st));
-    ok(sipg_solver_setup(psol), "pressure set-up");
+    if (pr_setups++ % o.pr_setup_every == 0) ok(sipg_solver_setup(psol), "pressure set-up");
     const auto c1 = std::chrono::steady_clock::now();
     sipg_solve_info pi{};
     solved(sipg_solver_solve(psol, rhs.as<double>(), pr.as<double>(), &pi), "pressure solve", pi);
@@ -262,6 +263,7 @@ int sipg_ins3d_default_opts(sipg_ins3d_opts* o) {
     o->cfl = 1.0;
     o->extrapolate_history = 3;
     o->viscous_kind = SIPG_SOLVER_JACOBI;
+    o->pr_setup_every = 1;
     o->reinit_freq = 24;  // level-set-options reinit_freq (ls_solver.cpp:146-148)
     o->reinit_ic = 1;     // reinit_ic (:158-159)
     o->ls_cap = 1.0;      // LS_CAP, include/problem_specific_3d.h
@@ -290,6 +292,7 @@ int sipg_ins3d_create(sipg_mesh* m, const sipg_ins3d_opts* o, const int* vel_bc,
     if (o->extrapolate_history < 0 || o->extrapolate_history > 8)
       throw Error(SIPG_INVALID_ARG, "extrapolate_history must be 0..8");
     if (!(o->ls_cap > 0.0) || o->reinit_freq < 0) throw Error(SIPG_INVALID_ARG, "ls_cap > 0 and reinit_freq >= 0");
+    if (o->pr_setup_every < 1) throw Error(SIPG_INVALID_ARG, "pr_setup_every must be >= 1");
     if (o->viscous_kind != SIPG_SOLVER_JACOBI && o->viscous_kind != SIPG_SOLVER_BLOCK_JACOBI)
       throw Error(SIPG_INVALID_ARG, "viscous_kind must be SIPG_SOLVER_JACOBI or SIPG_SOLVER_BLOCK_JACOBI");
     bool dirichlet_pr = false, slip = false;
@@ -401,6 +404,7 @@ int sipg_ins3d_set_state_host(sipg_ins3d* ins, const double* vel, const double* 
     ins->b1 = 0.0;
     ins->g0 = 1.0;
     ins->reinit_counter = 0;
+    ins->pr_setups = 0;
     if (ins->o.reinit_ic)
       ins->reinit(ins->vel[0].as<double>());
     else

@@ -268,7 +268,7 @@ class Ins3DOpts(C.Structure):
                 ("mu0", C.c_double), ("mu1", C.c_double), ("gravity", C.c_double), ("ls_alpha", C.c_double),
                 ("cfl", C.c_double), ("extrapolate_history", C.c_int), ("pr_over_int", C.c_int),
                 ("reinit_freq", C.c_int), ("reinit_ic", C.c_int), ("ls_cap", C.c_double),
-                ("viscous_kind", C.c_int),
+                ("pr_setup_every", C.c_int), ("viscous_kind", C.c_int),
                 ("pressure", SolverOpts),
                 ("viscous", SolverOpts)]
 
@@ -290,7 +290,7 @@ def ins3d_default_opts(**kw):
     for k, v in kw.items():
         if k == "precision":
             o.pressure.precision = v
-        elif k in ("pr_over_int", "viscous_kind", "reinit_freq", "reinit_ic", "ls_cap"):
+        elif k in ("pr_over_int", "pr_setup_every", "viscous_kind", "reinit_freq", "reinit_ic", "ls_cap"):
             setattr(o, k, v)
         elif k.startswith("pr_"):
             setattr(o.pressure, k[3:], v)

@@ -161,3 +161,21 @@ def test_slip_walls_two_phase_steps_match_the_oracle(open_top):
     got = ins.state()
     assert rel_err(got["vel"], ref.vel) < 1e-7
     assert rel_err(got["s"], ref.s) < 1e-9
+
+
+@pytest.mark.parametrize("over_int", [0, 1], ids=["nodal", "over-integrated"])
+def test_lagged_pressure_setup_gives_the_same_steps(over_int):
+    """pr_setup_every = 3: the V-cycle set up every third step only; the solves still reach
+    their tolerance, so the steps agree with the every-step set-up."""
+    gm, _, s, vel, vel_bc = _case(3, 2, False)
+    tol = dict(pr_rel_tol=1e-11, pr_abs_tol=1e-300, vis_rel_tol=1e-11, vis_abs_tol=1e-300)
+    got, iters = [], []
+    for every in (1, 3):
+        ins = sipg.Ins3D(gm, vel_bc, order=2, precision=sipg.FP32, pr_over_int=over_int, pr_setup_every=every,
+                         **tol, **CONSTS)
+        ins.set_state(vel, s)
+        its = [ins.step().pr_iters for _ in range(5)]
+        got.append(ins.state())
+        iters.append(its)
+    assert rel_err(got[1]["vel"], got[0]["vel"]) < 1e-7
+    assert max(iters[1]) <= 2 * max(iters[0]) + 5
