@@ -483,8 +483,13 @@ typedef struct {
                                 eigenvalue bounds and coarse levels lag: a fixed
                                 preconditioner per solve, the same tolerance */
   int viscous_kind;          /* [viscous-solve] preconditioner: SIPG_SOLVER_JACOBI (default,
-                                PETScJacobiSolver) or SIPG_SOLVER_BLOCK_JACOBI
-                                (PETScBlockJacobiSolver, mp_ins_solver.cpp:113-121) */
+                                PETScJacobiSolver), SIPG_SOLVER_BLOCK_JACOBI
+                                (PETScBlockJacobiSolver, mp_ins_solver.cpp:113-121), or
+                                SIPG_SOLVER_PMULTIGRID with viscous.n_levels 0: the FP64
+                                flexible PCG preconditioned by viscous.coarse_iters
+                                Jacobi-PCG iterations on the same operator in
+                                viscous.precision (SIPG_FP32: TF32 applies); no reference
+                                counterpart, same tolerance as the Jacobi solve */
   /* The pressure p-multigrid (SIPG_SOLVER_PMULTIGRID: precision of the V-cycle,
    * tolerances, [p-multigrid] keys; n_levels 0 = orders p, p-1, ..., 1; nullspace is
    * set from the boundary types) and the viscous Jacobi-PCG options. Defaults: the

@@ -293,8 +293,10 @@ int sipg_ins3d_create(sipg_mesh* m, const sipg_ins3d_opts* o, const int* vel_bc,
       throw Error(SIPG_INVALID_ARG, "extrapolate_history must be 0..8");
     if (!(o->ls_cap > 0.0) || o->reinit_freq < 0) throw Error(SIPG_INVALID_ARG, "ls_cap > 0 and reinit_freq >= 0");
     if (o->pr_setup_every < 1) throw Error(SIPG_INVALID_ARG, "pr_setup_every must be >= 1");
-    if (o->viscous_kind != SIPG_SOLVER_JACOBI && o->viscous_kind != SIPG_SOLVER_BLOCK_JACOBI)
-      throw Error(SIPG_INVALID_ARG, "viscous_kind must be SIPG_SOLVER_JACOBI or SIPG_SOLVER_BLOCK_JACOBI");
+    if (o->viscous_kind != SIPG_SOLVER_JACOBI && o->viscous_kind != SIPG_SOLVER_BLOCK_JACOBI &&
+        o->viscous_kind != SIPG_SOLVER_PMULTIGRID)
+      throw Error(SIPG_INVALID_ARG,
+                  "viscous_kind must be SIPG_SOLVER_JACOBI, SIPG_SOLVER_BLOCK_JACOBI or SIPG_SOLVER_PMULTIGRID");
     bool dirichlet_pr = false, slip = false;
     for (int b = 0; b < m->Kb; ++b) {
       if (vel_bc[b] < 0 || vel_bc[b] > 2)
@@ -379,6 +381,16 @@ int sipg_ins3d_create(sipg_mesh* m, const sipg_ins3d_opts* o, const int* vel_bc,
     ok(sipg_op_create(m, o->order, vcomp, &ins->vop), "viscous operator");
     ok(sipg_op_set_bc_types(ins->vop, vst.data()), "viscous boundary types");
     sipg_solver_opts vo = o->viscous;
+    if (o->viscous_kind == SIPG_SOLVER_PMULTIGRID && vo.n_levels == 0) {
+      // one level, no smoothing: the preconditioner is coarse_iters Jacobi-PCG iterations
+      // on the viscous operator itself, in the viscous precision (FP32: TF32 applies),
+      // inside the FP64 flexible PCG
+      vo.n_levels = 1;
+      vo.orders[0] = o->order;
+      vo.smoother = 0;
+      vo.coarse_kind = 0;
+      vo.pre_it[0] = vo.post_it[0] = 0;
+    }
     ok(sipg_solver_create(ins->vop, o->viscous_kind, &vo, &ins->vsol), "viscous solver");
     *out = ins.release();
   });

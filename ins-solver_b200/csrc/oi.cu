@@ -130,203 +130,220 @@ constexpr int OI_QC = 32;
 //   neighbour     sum_s U[s][i] PS[s][j] + CH[s][i] DM[s][j]
 //                 (U = sJ (f- dn - tau w phi) / 2, PS = the neighbour's basis, CH = the own
 //                  basis at the neighbour's points, DM = -sJ f+ dn+ / 2),
-// so the factors are staged per point chunk or face in the warp's shared area
-// (rows padded to NPP4, a multiple of 4) and each lane accumulates a 4 x 4 tile of the
-// Np x Np block in registers: 16 FMAs per 8 staged values. Tiles beyond 32 per
-// block (p = 4 in 3D) take further rounds over the element.
+// i.e. a product L^T R of two staged (points x Np) factors. The factors are staged per
+// point chunk or face in the warp's shared area (columns padded with zeros to NB 8-wide
+// tiles, rows SS apart) and the warp multiplies them on the FP64 tensor cores: one
+// m8n8k4 MMA per (8 x 8 tile of the block, 4 points), A = L^T and B = R read straight
+// from the staged rows (lane (g, t) reads row t, column g), accumulators in registers.
 template <int NP>
 struct OiTile {
-  static constexpr int NPP4 = (NP + 3) / 4 * 4, NTI = NPP4 / 4, NT = NTI * NTI;
+  static constexpr int NB = (NP + 7) / 8;  // 8-wide tiles per block side
+  static constexpr int S8 = NB * 8;        // staged columns (zeros beyond Np)
+  // row stride = 8 (mod 16) doubles: the four rows t of a fragment load fall in
+  // two distinct halves of the banks, two wavefronts per 32 x 8-byte load
+  static constexpr int SS = S8 % 16 == 0 ? S8 + 8 : S8;
   static constexpr int W = NP > 20 ? 2 : 4;  // warps per CTA
 };
 
+// acc[bi][bj] += (L^T R) tile (bi, bj) over rows 0..nk-1 of L and R (row k of L scaled by
+// w[k] when w is given). Lane (g = lane / 4, t = lane % 4) holds entries (8 bi + g,
+// 8 bj + 2t) and (8 bi + g, 8 bj + 2t + 1).
 template <int NP>
-__device__ __forceinline__ void oi_outer(double (&acc)[16], const double* L, const double* R, const double* w,
-                                         int nk, int i0, int j0) {
-  constexpr int S = OiTile<NP>::NPP4;
-  for (int k = 0; k < nk; ++k) {
-    const double2 l01 = *reinterpret_cast<const double2*>(L + k * S + i0);
-    const double2 l23 = *reinterpret_cast<const double2*>(L + k * S + i0 + 2);
-    const double2 r01 = *reinterpret_cast<const double2*>(R + k * S + j0);
-    const double2 r23 = *reinterpret_cast<const double2*>(R + k * S + j0 + 2);
-    const double ws = w ? w[k] : 1.0;
-    const double l[4] = {ws * l01.x, ws * l01.y, ws * l23.x, ws * l23.y};
-    const double r[4] = {r01.x, r01.y, r23.x, r23.y};
+__device__ __forceinline__ void oi_mma(double (&acc)[OiTile<NP>::NB][OiTile<NP>::NB][2], const double* L,
+                                       const double* R, const double* w, int nk, int lane) {
+  constexpr int NB = OiTile<NP>::NB, SS = OiTile<NP>::SS;
+  const int g = lane >> 2, t = lane & 3;
+  for (int k0 = 0; k0 < nk; k0 += 4) {
+    const int k = k0 + t;
+    const bool ok = k < nk;
+    const int kc = ok ? k : nk - 1;  // rows past nk are never read
+    const double ws = ok ? (w ? w[kc] : 1.0) : 0.0;
+    double av[NB], bv[NB];
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int b = 0; b < NB; ++b) {
+      const double l = L[kc * SS + b * 8 + g], r = R[kc * SS + b * 8 + g];
+      av[b] = ok ? ws * l : 0.0;
+      bv[b] = ok ? r : 0.0;
+    }
 #pragma unroll
-      for (int b = 0; b < 4; ++b) acc[a * 4 + b] = fma(l[a], r[b], acc[a * 4 + b]);
+    for (int bi = 0; bi < NB; ++bi)
+#pragma unroll
+      for (int bj = 0; bj < NB; ++bj)
+        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                     : "+d"(acc[bi][bj][0]), "+d"(acc[bi][bj][1])
+                     : "d"(av[bi]), "d"(bv[bj]));
   }
+}
+
+template <int NP>
+__device__ __forceinline__ void oi_zero(double (&acc)[OiTile<NP>::NB][OiTile<NP>::NB][2]) {
+#pragma unroll
+  for (int bi = 0; bi < OiTile<NP>::NB; ++bi)
+#pragma unroll
+    for (int bj = 0; bj < OiTile<NP>::NB; ++bj) acc[bi][bj][0] = acc[bi][bj][1] = 0.0;
+}
+
+// Writes this lane's entries (8 bi + lane / 4, 8 bj + 2 (lane % 4) + c) of block blk of
+// element e: 0 the self block, 1 + f the neighbour block of face f. mode 0 writes the
+// values, 1 a neighbour block with the pinned DOF's row and column zeroed, 2 the self
+// block with the mass term added and the pinned DOF's off-diagonal entries zeroed.
+template <int NP>
+__device__ __forceinline__ void oi_store(const OiArgs& a, const double (&c)[OiTile<NP>::NB][OiTile<NP>::NB][2],
+                                         int blk, int e, int nb, int mode, double J, int lane) {
+  constexpr int NB = OiTile<NP>::NB;
+  const size_t K = (size_t)a.K;
+  const int g8 = lane >> 2, t2 = 2 * (lane & 3);
+#pragma unroll
+  for (int bi = 0; bi < NB; ++bi)
+#pragma unroll
+    for (int bj = 0; bj < NB; ++bj)
+#pragma unroll
+      for (int cc = 0; cc < 2; ++cc) {
+        const int i = bi * 8 + g8, j = bj * 8 + t2 + cc;
+        if (i >= NP || j >= NP) continue;
+        double v = c[bi][bj][cc];
+        if (mode == 1 && ((nb == a.pin_elem && j == a.pin_node) || (e == a.pin_elem && i == a.pin_node))) v = 0.0;
+        if (mode == 2) {
+          if (a.mm_mode != MM_NONE)
+            v += J * a.mass[i * NP + j] * (a.mm_mode == MM_SCALAR ? a.mm_scalar : a.mm[(size_t)e * NP + j]);
+          // the pinned DOF: column zero, its row keeps only its own diagonal
+          if (e == a.pin_elem && (j == a.pin_node || i == a.pin_node) && i != j) v = 0.0;
+        }
+        a.v[((size_t)(blk * NP + i) * NP + j) * K + e] = v;
+      }
 }
 
 // doubles of one warp's shared area: a volume chunk (Y and its weights) or the seven
 // face arrays, whichever is larger
 template <int DIM, int NP>
 __host__ __device__ size_t oi_warp_doubles(int nqs) {
-  constexpr int S = OiTile<NP>::NPP4;
-  const size_t vol = (size_t)OI_QC * DIM * S + OI_QC * DIM;
-  const size_t face = (size_t)7 * nqs * S;
+  constexpr int SS = OiTile<NP>::SS;
+  const size_t vol = (size_t)OI_QC * DIM * SS + OI_QC * DIM;
+  const size_t face = (size_t)7 * nqs * SS;
   return vol > face ? vol : face;
 }
 
 template <int DIM, int NP>
-__global__ void __launch_bounds__(32 * OiTile<NP>::W, OiTile<NP>::W == 4 ? 3 : 1) k_oi_blocks(OiArgs a) {
-  constexpr int NF = DIM + 1, NG = DIM == 3 ? 10 : 5, S = OiTile<NP>::NPP4, NTI = OiTile<NP>::NTI;
-  constexpr int NT = OiTile<NP>::NT, W = OiTile<NP>::W;
+__global__ void __launch_bounds__(32 * OiTile<NP>::W) k_oi_blocks(OiArgs a) {
+  constexpr int NF = DIM + 1, NG = DIM == 3 ? 10 : 5, NB = OiTile<NP>::NB, S8 = OiTile<NP>::S8;
+  constexpr int SS = OiTile<NP>::SS, W = OiTile<NP>::W;
   extern __shared__ __align__(16) double sm[];
   const int nqs = a.nqs, nq = a.nq;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double* Z = sm + (size_t)warp * oi_warp_doubles<DIM, NP>(nqs);  // even sizes: 16-byte aligned tiles
-  // volume chunk: Y[(q * DIM + d) * S + i], weights wv[q * DIM + d]
+  double* Z = sm + (size_t)warp * oi_warp_doubles<DIM, NP>(nqs);
+  // volume chunk: Y[(q * DIM + d) * SS + i], weights wv[q * DIM + d]
   double* Y = Z;
-  double* wv = Z + (size_t)OI_QC * DIM * S;
-  // face arrays, nqs x S each
+  double* wv = Z + (size_t)OI_QC * DIM * SS;
+  // face arrays, nqs x SS each
   double* P = Z;
-  double* E = P + nqs * S;
-  double* Q = E + nqs * S;
-  double* U = Q + nqs * S;
-  double* PS = U + nqs * S;
-  double* CH = PS + nqs * S;
-  double* DM = CH + nqs * S;
-  const size_t K = (size_t)a.K;
+  double* E = P + nqs * SS;
+  double* Q = E + nqs * SS;
+  double* U = Q + nqs * SS;
+  double* PS = U + nqs * SS;
+  double* CH = PS + nqs * SS;
+  double* DM = CH + nqs * SS;
   for (int e = blockIdx.x * W + warp; e < a.K; e += gridDim.x * W) {
     double g[NG];
 #pragma unroll
     for (int k = 0; k < NG; ++k) g[k] = __ldg(a.geof + (size_t)e * NG + k);
     const double J = oi_J<DIM>(g);
-    for (int t0 = 0; t0 < NT; t0 += 32) {
-      const int t = t0 + lane;
-      const bool act = t < NT;
-      const int i0 = act ? 4 * (t / NTI) : 0, j0 = act ? 4 * (t % NTI) : 0;
-      double acc[16];
+    double acc[NB][NB][2];
+    oi_zero<NP>(acc);
+    // volume
+    for (int q0 = 0; q0 < nq; q0 += OI_QC) {
+      const int nc = min(OI_QC, nq - q0);
+      __syncwarp();
+      // each reference derivative is loaded once and serves the DIM physical ones
+      for (int idx = lane; idx < nc * S8; idx += 32) {
+        const int i = idx % S8, qq = idx / S8;
+        double dr[DIM];
 #pragma unroll
-      for (int k = 0; k < 16; ++k) acc[k] = 0.0;
-      // volume
-      for (int q0 = 0; q0 < nq; q0 += OI_QC) {
-        const int nc = min(OI_QC, nq - q0);
-        __syncwarp();
-        // each reference derivative is loaded once and serves the DIM physical ones
-        for (int idx = lane; idx < nc * S; idx += 32) {
-          const int i = idx % S, qq = idx / S;
-          double dr[DIM];
+        for (int r = 0; r < DIM; ++r) dr[r] = i < NP ? __ldg(a.vdphi + ((size_t)r * nq + q0 + qq) * NP + i) : 0.0;
 #pragma unroll
-          for (int r = 0; r < DIM; ++r) dr[r] = i < NP ? __ldg(a.vdphi + ((size_t)r * nq + q0 + qq) * NP + i) : 0.0;
+        for (int d = 0; d < DIM; ++d) {
+          double v = 0.0;
 #pragma unroll
-          for (int d = 0; d < DIM; ++d) {
-            double v = 0.0;
-#pragma unroll
-            for (int r = 0; r < DIM; ++r) v += g[r * DIM + d] * dr[r];
-            Y[(qq * DIM + d) * S + i] = v;
-          }
+          for (int r = 0; r < DIM; ++r) v += g[r * DIM + d] * dr[r];
+          Y[(qq * DIM + d) * SS + i] = v;
         }
-        for (int idx = lane; idx < nc * DIM; idx += 32) {
-          const int qq = idx / DIM;
-          wv[idx] = __ldg(a.wq + q0 + qq) * J * a.fvol[(size_t)e * nq + q0 + qq];
-        }
-        __syncwarp();
-        if (act) oi_outer<NP>(acc, Y, Y, wv, nc * DIM, i0, j0);
       }
-      // faces
-      for (int f = 0; f < NF; ++f) {
-        const int nb = a.nbr[(size_t)e * NF + f];
-        const bool dir = nb < 0 && a.bct[-nb - 1] == BC_DIRICHLET;
-        if (nb < 0 && !dir) continue;  // Neumann and (scalar) slip faces add nothing
-        double n[3], sJ;
-        simplex_face_normal<DIM>(g, f, n, &sJ);
-        const double h = nb >= 0 ? 0.5 : 1.0, tau = a.tau[(size_t)e * NF + f];
-        double cr[3] = {0.0, 0.0, 0.0}, cn[3] = {0.0, 0.0, 0.0};
+      for (int idx = lane; idx < nc * DIM; idx += 32) {
+        const int qq = idx / DIM;
+        wv[idx] = __ldg(a.wq + q0 + qq) * J * a.fvol[(size_t)e * nq + q0 + qq];
+      }
+      __syncwarp();
+      oi_mma<NP>(acc, Y, Y, wv, nc * DIM, lane);
+    }
+    // faces
+    for (int f = 0; f < NF; ++f) {
+      const int nb = a.nbr[(size_t)e * NF + f];
+      const bool dir = nb < 0 && a.bct[-nb - 1] == BC_DIRICHLET;
+      if (nb < 0) {
+        // no neighbour block on a boundary face
+        double zero[NB][NB][2];
+        oi_zero<NP>(zero);
+        oi_store<NP>(a, zero, 1 + f, e, nb, 0, J, lane);
+        if (!dir) continue;  // Neumann and (scalar) slip faces add nothing
+      }
+      double n[3], sJ;
+      simplex_face_normal<DIM>(g, f, n, &sJ);
+      const double h = nb >= 0 ? 0.5 : 1.0, tau = a.tau[(size_t)e * NF + f];
+      double cr[3] = {0.0, 0.0, 0.0}, cn[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+      for (int r = 0; r < DIM; ++r)
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) cr[r] += n[d] * g[r * DIM + d];
+      int gf = 0, sg = 0;
+      if (nb >= 0) {
+        const int code = (a.fcode[e] >> (8 * f)) & 0xff;
+        gf = code & 3;
+        sg = code >> 2;
 #pragma unroll
         for (int r = 0; r < DIM; ++r)
 #pragma unroll
-          for (int d = 0; d < DIM; ++d) cr[r] += n[d] * g[r * DIM + d];
-        int gf = 0, sg = 0;
-        if (nb >= 0) {
-          const int code = (a.fcode[e] >> (8 * f)) & 0xff;
-          gf = code & 3;
-          sg = code >> 2;
+          for (int d = 0; d < DIM; ++d) cn[r] += n[d] * __ldg(a.geof + (size_t)nb * NG + r * DIM + d);
+      }
+      __syncwarp();
+      for (int idx = lane; idx < nqs * S8; idx += 32) {
+        const int sq = idx / S8, i = idx % S8, o = sq * SS + i;
+        double ph = 0.0, dn = 0.0, ps = 0.0, ch = 0.0, dp = 0.0;
+        if (i < NP) {
+          ph = __ldg(a.fphi + ((size_t)f * nqs + sq) * NP + i);
 #pragma unroll
-          for (int r = 0; r < DIM; ++r)
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) cn[r] += n[d] * __ldg(a.geof + (size_t)nb * NG + r * DIM + d);
-        }
-        __syncwarp();
-        for (int idx = lane; idx < nqs * S; idx += 32) {
-          const int sq = idx / S, i = idx % S;
-          double ph = 0.0, dn = 0.0, ps = 0.0, ch = 0.0, dp = 0.0;
-          if (i < NP) {
-            ph = __ldg(a.fphi + ((size_t)f * nqs + sq) * NP + i);
-#pragma unroll
-            for (int r = 0; r < DIM; ++r) dn += cr[r] * __ldg(a.fdphi + (((size_t)f * 3 + r) * nqs + sq) * NP + i);
-            if (nb >= 0) {
-              ps = __ldg(a.xphi + (((size_t)gf * a.nperm + sg) * nqs + sq) * NP + i);
-#pragma unroll
-              for (int r = 0; r < DIM; ++r)
-                dp += cn[r] * __ldg(a.fdphi + (((size_t)gf * 3 + r) * nqs + sq) * NP + i);
-              ch = __ldg(a.yphi + (((size_t)f * a.nperm + sg) * nqs + sq) * NP + i);
-            }
-          }
-          const double ws = __ldg(a.ws + sq);
-          const double fm = ws * a.fsurf[((size_t)e * NF + f) * nqs + sq];
-          const double ev = -h * sJ * fm * dn;
-          P[idx] = ph;
-          E[idx] = ev;
-          Q[idx] = ev + h * sJ * tau * ws * ph;
+          for (int r = 0; r < DIM; ++r) dn += cr[r] * __ldg(a.fdphi + (((size_t)f * 3 + r) * nqs + sq) * NP + i);
           if (nb >= 0) {
-            const double fp = ws * a.fsurf[((size_t)nb * NF + gf) * nqs + sq];
-            U[idx] = 0.5 * sJ * (fm * dn - tau * ws * ph);
-            PS[idx] = ps;
-            CH[idx] = ch;
-            DM[idx] = -0.5 * sJ * fp * dp;
+            ps = __ldg(a.xphi + (((size_t)gf * a.nperm + sg) * nqs + sq) * NP + i);
+#pragma unroll
+            for (int r = 0; r < DIM; ++r) dp += cn[r] * __ldg(a.fdphi + (((size_t)gf * 3 + r) * nqs + sq) * NP + i);
+            ch = __ldg(a.yphi + (((size_t)f * a.nperm + sg) * nqs + sq) * NP + i);
           }
         }
-        __syncwarp();
-        if (act) {
-          oi_outer<NP>(acc, P, Q, nullptr, nqs, i0, j0);
-          oi_outer<NP>(acc, E, P, nullptr, nqs, i0, j0);
-        }
-        if (nb >= 0 && act) {
-          double nacc[16];
-#pragma unroll
-          for (int k = 0; k < 16; ++k) nacc[k] = 0.0;
-          oi_outer<NP>(nacc, U, PS, nullptr, nqs, i0, j0);
-          oi_outer<NP>(nacc, CH, DM, nullptr, nqs, i0, j0);
-#pragma unroll
-          for (int aa = 0; aa < 4; ++aa)
-#pragma unroll
-            for (int bb = 0; bb < 4; ++bb) {
-              const int i = i0 + aa, j = j0 + bb;
-              if (i >= NP || j >= NP) continue;
-              double val = nacc[aa * 4 + bb];
-              if ((nb == a.pin_elem && j == a.pin_node) || (e == a.pin_elem && i == a.pin_node)) val = 0.0;
-              a.v[((size_t)((1 + f) * NP + i) * NP + j) * K + e] = val;
-            }
+        const double ws = __ldg(a.ws + sq);
+        const double fm = ws * a.fsurf[((size_t)e * NF + f) * nqs + sq];
+        const double ev = -h * sJ * fm * dn;
+        P[o] = ph;
+        E[o] = ev;
+        Q[o] = ev + h * sJ * tau * ws * ph;
+        if (nb >= 0) {
+          const double fp = ws * a.fsurf[((size_t)nb * NF + gf) * nqs + sq];
+          U[o] = 0.5 * sJ * (fm * dn - tau * ws * ph);
+          PS[o] = ps;
+          CH[o] = ch;
+          DM[o] = -0.5 * sJ * fp * dp;
         }
       }
-      if (act) {
-        for (int f = 0; f < NF; ++f)
-          if (a.nbr[(size_t)e * NF + f] < 0)
-#pragma unroll
-            for (int aa = 0; aa < 4; ++aa)
-#pragma unroll
-              for (int bb = 0; bb < 4; ++bb) {
-                const int i = i0 + aa, j = j0 + bb;
-                if (i < NP && j < NP) a.v[((size_t)((1 + f) * NP + i) * NP + j) * K + e] = 0.0;
-              }
-#pragma unroll
-        for (int aa = 0; aa < 4; ++aa)
-#pragma unroll
-          for (int bb = 0; bb < 4; ++bb) {
-            const int i = i0 + aa, j = j0 + bb;
-            if (i >= NP || j >= NP) continue;
-            double val = acc[aa * 4 + bb];
-            if (a.mm_mode != MM_NONE)
-              val += J * a.mass[i * NP + j] * (a.mm_mode == MM_SCALAR ? a.mm_scalar : a.mm[(size_t)e * NP + j]);
-            // the pinned DOF: column zero, its row keeps only its own diagonal
-            if (e == a.pin_elem && (j == a.pin_node || i == a.pin_node) && i != j) val = 0.0;
-            a.v[((size_t)i * NP + j) * K + e] = val;
-          }
+      __syncwarp();
+      oi_mma<NP>(acc, P, Q, nullptr, nqs, lane);
+      oi_mma<NP>(acc, E, P, nullptr, nqs, lane);
+      if (nb >= 0) {
+        double nacc[NB][NB][2];
+        oi_zero<NP>(nacc);
+        oi_mma<NP>(nacc, U, PS, nullptr, nqs, lane);
+        oi_mma<NP>(nacc, CH, DM, nullptr, nqs, lane);
+        oi_store<NP>(a, nacc, 1 + f, e, nb, 1, J, lane);
       }
     }
+    oi_store<NP>(a, acc, 0, e, -1, 2, J, lane);
   }
 }
 

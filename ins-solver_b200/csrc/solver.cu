@@ -537,6 +537,9 @@ void sipg_solver::setup_pmg() {
     L.cheb = o.cheb_orders[l] > 0 ? o.cheb_orders[l] : o.cheb_order;
     L.pre = std::max(0, o.pre_it[l]);
     L.post = std::max(0, o.post_it[l]);
+    // the Chebyshev bound is read only by a level's smoothing sweeps (a single level with
+    // no sweeps is an inner Jacobi-PCG preconditioner)
+    const bool smooths = L.pre > 0 || L.post > 0;
     if (o.smoother != 1 || (l == nl - 1 && !amg_below)) {
       op_diag(L.op, L.dinv64.as<double>(), stream);
       k_recip<<<grid_for(L.n), 256, 0, stream>>>(L.dinv64.as<double>(), L.n);
@@ -569,12 +572,12 @@ void sipg_solver::setup_pmg() {
       }
       pt.mark("diagonal and blocks", l);
       // the FP32 V-cycle estimates its bound after the assembly, on its own operator
-      if (!f32) L.lmax = power_lmax(L.op, nullptr, L.n, rows.as<double>(), L.Np);
+      if (!f32 && smooths) L.lmax = power_lmax(L.op, nullptr, L.n, rows.as<double>(), L.Np);
     } else {
       L.bc64 = DevBuf();
       L.bc32 = DevBuf();
       pt.mark("diagonal", l);
-      L.lmax = power_lmax(L.op, L.dinv64.as<double>(), L.n);
+      if (smooths) L.lmax = power_lmax(L.op, L.dinv64.as<double>(), L.n);
     }
     if (!(f32 && o.smoother == 1)) pt.mark("eigenvalue bound", l);
     // -1: p = 2 and below in the FP32 V-cycle (p = 2 as scaled FP16 blocks: half the
@@ -595,7 +598,7 @@ void sipg_solver::setup_pmg() {
     } else {
       L.bsr.reset();
     }
-    if (f32 && o.smoother == 1) {
+    if (f32 && o.smoother == 1 && smooths) {
       L.lmax = power_lmax_f32(L);
       pt.mark("eigenvalue bound", l);
     }

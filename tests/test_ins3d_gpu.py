@@ -124,6 +124,28 @@ def test_block_jacobi_viscous_solves_give_the_jacobi_steps():
     assert iters[1] < iters[0]
 
 
+@pytest.mark.parametrize("slip", [False, True], ids=["no-slip", "slip-sides"])
+def test_inner_fp32_pcg_viscous_solves_give_the_jacobi_steps(slip):
+    """viscous_kind = p-multigrid with n_levels 0: the FP64 flexible PCG preconditioned by
+    six FP32 Jacobi-PCG iterations on the viscous operator reaches the Jacobi solve's
+    steps to the solver tolerance, in far fewer outer iterations; with slip side walls
+    through the coupled vector operator."""
+    gm, _, s, vel, vel_bc = _case(3, 2, False, slip_sides=slip)
+    tol = dict(pr_rel_tol=1e-11, pr_abs_tol=1e-300, vis_rel_tol=1e-11, vis_abs_tol=1e-300)
+    inner = dict(viscous_kind=sipg.SOLVER_PMULTIGRID, vis_precision=sipg.FP32, vis_n_levels=0, vis_coarse_iters=6)
+    got, iters = [], []
+    for kw in ({}, inner):
+        ins = sipg.Ins3D(gm, vel_bc, order=2, precision=sipg.FP64, **kw, **tol, **CONSTS)
+        ins.set_state(vel, s)
+        info = ins.step(2)
+        assert all(r <= 1e-11 for r in info.vis_rel_res[:(1 if slip else 3)])
+        got.append(ins.state())
+        iters.append(sum(info.vis_iters))
+        ins.close()
+    assert rel_err(got[1]["vel"], got[0]["vel"]) < 1e-8
+    assert 2 * iters[1] < iters[0]
+
+
 @pytest.mark.parametrize("open_top", [False, True], ids=["closed", "open-top"])
 def test_over_integrated_two_phase_steps_match_the_oracle(open_top):
     """[pressure-solve] over_int = 1: 1/rho at the cubature points from the level set and
