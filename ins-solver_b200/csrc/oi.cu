@@ -120,7 +120,7 @@ __global__ void k_oi_project(const double* __restrict__ proj, const double* __re
   }
 }
 
-constexpr int OI_QC = 32;
+constexpr int OI_QC = 16;
 
 // One warp assembles one element's blocks. Every block is a sum of outer products
 // over cubature points,
@@ -130,11 +130,14 @@ constexpr int OI_QC = 32;
 //   neighbour     sum_s U[s][i] PS[s][j] + CH[s][i] DM[s][j]
 //                 (U = sJ (f- dn - tau w phi) / 2, PS = the neighbour's basis, CH = the own
 //                  basis at the neighbour's points, DM = -sJ f+ dn+ / 2),
-// i.e. a product L^T R of two staged (points x Np) factors. The factors are staged per
-// point chunk or face in the warp's shared area (columns padded with zeros to NB 8-wide
-// tiles, rows SS apart) and the warp multiplies them on the FP64 tensor cores: one
-// m8n8k4 MMA per (8 x 8 tile of the block, 4 points), A = L^T and B = R read straight
-// from the staged rows (lane (g, t) reads row t, column g), accumulators in registers.
+// i.e. a product L^T R of two (points x Np) factors. The element-dependent factors
+// (Y, E, Q, U, DM) are staged per point chunk or face in the warp's shared area (columns
+// padded with zeros to NB 8-wide tiles, rows SS apart); the pure basis tables (P, PS, CH)
+// are read in place through the read-only cache, which keeps the shared area at 12 KB per
+// warp for p = 3 (four CTAs of four warps per SM). The warp multiplies them on the FP64
+// tensor cores: one m8n8k4 MMA per (8 x 8 tile of the block, 4 points), A = L^T and B = R
+// read straight from the rows (lane (g, t) reads row t, column g), accumulators in
+// registers.
 template <int NP>
 struct OiTile {
   static constexpr int NB = (NP + 7) / 8;  // 8-wide tiles per block side
@@ -147,11 +150,14 @@ struct OiTile {
 
 // acc[bi][bj] += (L^T R) tile (bi, bj) over rows 0..nk-1 of L and R (row k of L scaled by
 // w[k] when w is given). Lane (g = lane / 4, t = lane % 4) holds entries (8 bi + g,
-// 8 bj + 2t) and (8 bi + g, 8 bj + 2t + 1).
-template <int NP>
+// 8 bj + 2t) and (8 bi + g, 8 bj + 2t + 1). A staged operand has rows SS apart and zeros
+// beyond Np; a table operand (LT / RT: a basis table in global memory, rows Np apart)
+// is read through the read-only cache with the columns beyond Np masked.
+template <int NP, bool LT = false, bool RT = false>
 __device__ __forceinline__ void oi_mma(double (&acc)[OiTile<NP>::NB][OiTile<NP>::NB][2], const double* L,
                                        const double* R, const double* w, int nk, int lane) {
   constexpr int NB = OiTile<NP>::NB, SS = OiTile<NP>::SS;
+  constexpr int LL = LT ? NP : SS, LR = RT ? NP : SS;
   const int g = lane >> 2, t = lane & 3;
   for (int k0 = 0; k0 < nk; k0 += 4) {
     const int k = k0 + t;
@@ -161,7 +167,9 @@ __device__ __forceinline__ void oi_mma(double (&acc)[OiTile<NP>::NB][OiTile<NP>:
     double av[NB], bv[NB];
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
-      const double l = L[kc * SS + b * 8 + g], r = R[kc * SS + b * 8 + g];
+      const int c = b * 8 + g;
+      const double l = LT ? (c < NP ? __ldg(L + kc * LL + c) : 0.0) : L[kc * LL + c];
+      const double r = RT ? (c < NP ? __ldg(R + kc * LR + c) : 0.0) : R[kc * LR + c];
       av[b] = ok ? ws * l : 0.0;
       bv[b] = ok ? r : 0.0;
     }
@@ -213,18 +221,19 @@ __device__ __forceinline__ void oi_store(const OiArgs& a, const double (&c)[OiTi
       }
 }
 
-// doubles of one warp's shared area: a volume chunk (Y and its weights) or the seven
-// face arrays, whichever is larger
+// doubles of one warp's shared area: a volume chunk (Y and its weights) or the four
+// staged face arrays, whichever is larger (the basis P, the neighbour's basis PS and the
+// own basis at the neighbour's points CH are table rows, read in place)
 template <int DIM, int NP>
 __host__ __device__ size_t oi_warp_doubles(int nqs) {
   constexpr int SS = OiTile<NP>::SS;
   const size_t vol = (size_t)OI_QC * DIM * SS + OI_QC * DIM;
-  const size_t face = (size_t)7 * nqs * SS;
+  const size_t face = (size_t)4 * nqs * SS;
   return vol > face ? vol : face;
 }
 
 template <int DIM, int NP>
-__global__ void __launch_bounds__(32 * OiTile<NP>::W) k_oi_blocks(OiArgs a) {
+__global__ void __launch_bounds__(32 * OiTile<NP>::W, OiTile<NP>::W == 4 ? 4 : 1) k_oi_blocks(OiArgs a) {
   constexpr int NF = DIM + 1, NG = DIM == 3 ? 10 : 5, NB = OiTile<NP>::NB, S8 = OiTile<NP>::S8;
   constexpr int SS = OiTile<NP>::SS, W = OiTile<NP>::W;
   extern __shared__ __align__(16) double sm[];
@@ -235,13 +244,10 @@ __global__ void __launch_bounds__(32 * OiTile<NP>::W) k_oi_blocks(OiArgs a) {
   double* Y = Z;
   double* wv = Z + (size_t)OI_QC * DIM * SS;
   // face arrays, nqs x SS each
-  double* P = Z;
-  double* E = P + nqs * SS;
+  double* E = Z;
   double* Q = E + nqs * SS;
   double* U = Q + nqs * SS;
-  double* PS = U + nqs * SS;
-  double* CH = PS + nqs * SS;
-  double* DM = CH + nqs * SS;
+  double* DM = U + nqs * SS;
   for (int e = blockIdx.x * W + warp; e < a.K; e += gridDim.x * W) {
     double g[NG];
 #pragma unroll
@@ -306,40 +312,36 @@ __global__ void __launch_bounds__(32 * OiTile<NP>::W) k_oi_blocks(OiArgs a) {
       __syncwarp();
       for (int idx = lane; idx < nqs * S8; idx += 32) {
         const int sq = idx / S8, i = idx % S8, o = sq * SS + i;
-        double ph = 0.0, dn = 0.0, ps = 0.0, ch = 0.0, dp = 0.0;
+        double ph = 0.0, dn = 0.0, dp = 0.0;
         if (i < NP) {
           ph = __ldg(a.fphi + ((size_t)f * nqs + sq) * NP + i);
 #pragma unroll
           for (int r = 0; r < DIM; ++r) dn += cr[r] * __ldg(a.fdphi + (((size_t)f * 3 + r) * nqs + sq) * NP + i);
           if (nb >= 0) {
-            ps = __ldg(a.xphi + (((size_t)gf * a.nperm + sg) * nqs + sq) * NP + i);
 #pragma unroll
             for (int r = 0; r < DIM; ++r) dp += cn[r] * __ldg(a.fdphi + (((size_t)gf * 3 + r) * nqs + sq) * NP + i);
-            ch = __ldg(a.yphi + (((size_t)f * a.nperm + sg) * nqs + sq) * NP + i);
           }
         }
         const double ws = __ldg(a.ws + sq);
         const double fm = ws * a.fsurf[((size_t)e * NF + f) * nqs + sq];
         const double ev = -h * sJ * fm * dn;
-        P[o] = ph;
         E[o] = ev;
         Q[o] = ev + h * sJ * tau * ws * ph;
         if (nb >= 0) {
           const double fp = ws * a.fsurf[((size_t)nb * NF + gf) * nqs + sq];
           U[o] = 0.5 * sJ * (fm * dn - tau * ws * ph);
-          PS[o] = ps;
-          CH[o] = ch;
           DM[o] = -0.5 * sJ * fp * dp;
         }
       }
       __syncwarp();
-      oi_mma<NP>(acc, P, Q, nullptr, nqs, lane);
-      oi_mma<NP>(acc, E, P, nullptr, nqs, lane);
+      const double* P = a.fphi + (size_t)f * nqs * NP;
+      oi_mma<NP, true, false>(acc, P, Q, nullptr, nqs, lane);
+      oi_mma<NP, false, true>(acc, E, P, nullptr, nqs, lane);
       if (nb >= 0) {
         double nacc[NB][NB][2];
         oi_zero<NP>(nacc);
-        oi_mma<NP>(nacc, U, PS, nullptr, nqs, lane);
-        oi_mma<NP>(nacc, CH, DM, nullptr, nqs, lane);
+        oi_mma<NP, false, true>(nacc, U, a.xphi + ((size_t)gf * a.nperm + sg) * nqs * NP, nullptr, nqs, lane);
+        oi_mma<NP, true, false>(nacc, a.yphi + ((size_t)f * a.nperm + sg) * nqs * NP, DM, nullptr, nqs, lane);
         oi_store<NP>(a, nacc, 1 + f, e, nb, 1, J, lane);
       }
     }
