@@ -37,6 +37,21 @@ def test_bad_options_are_refused(bad):
     assert st == sipg.SIPG_INVALID_ARG and not h.value
 
 
+@pytest.mark.parametrize("kind", [sipg.SOLVER_JACOBI, sipg.SOLVER_BLOCK_JACOBI, sipg.SOLVER_PMULTIGRID])
+def test_viscous_kinds_the_driver_takes_pass_the_option_checks(kind):
+    """Jacobi, block-Jacobi and the FP32 inner Jacobi-PCG preconditioner (p-multigrid
+    kind with n_levels 0) get past the option checks; without a GPU the creation then
+    stops at the first device call, with a CUDA status rather than SIPG_INVALID_ARG."""
+    mesh = sipg.Mesh.box(3, 2, jitter=0.1, seed=1)
+    o = sipg.ins3d_default_opts(viscous_kind=kind, vis_precision=sipg.FP32, vis_n_levels=0, vis_coarse_iters=6)
+    h = C.c_void_p()
+    bc = np.zeros(mesh.Kb, np.int32)
+    st = sipg.lib().sipg_ins3d_create(mesh.h, C.byref(o), bc.ctypes.data_as(C.c_void_p), C.byref(h))
+    if h.value:
+        sipg.lib().sipg_ins3d_destroy(h)
+    assert st != sipg.SIPG_INVALID_ARG
+
+
 def test_unknown_boundary_types_are_refused():
     mesh = sipg.Mesh.box(3, 2, jitter=0.1, seed=1)
     bc = np.full(mesh.Kb, 3, np.int32)  # a custom type of problem_specific_3d.h
